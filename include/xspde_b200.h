@@ -1,0 +1,164 @@
+/* xspde_b200.h -- C ABI of the B200-native xSPDE ensemble-integration path.
+ *
+ * The library replaces the hooks through which xSPDE 4.21 drives one ensemble
+ * block (reference paths are relative to the xspde_matlab project root):
+ *
+ *   xs_run_path   replaces  p.path(a,nc,p)        Simulator/xpath.m:1, called at
+ *                           Simulator/xensemble.m:79, default set at
+ *                           Simulator/xpreferences.m:62.  The whole time loop
+ *                           (noise, method, observables) runs on the GPU.
+ *   xs_step       replaces  p.method(a,w,p)       Applications/SDE/MP.m:1, RK4.m:1,
+ *                           Euler.m:1, RK2.m:1, Implicit.m:1, called at
+ *                           Simulator/xpath.m:150.
+ *   xs_noise      replaces  p.noisegen(w1,nc,s,p) Simulator/xnoise.m:1 (one draw,
+ *                           before the coarse average of xnoise.m:33-35).
+ *   xs_random     replaces  p.randomgen(p)        Simulator/xrandom.m:1.
+ *
+ * The problem description mirrors the input struct fields of
+ * Simulator/xpreferences.m (dimensions, fields, points, ranges, origins,
+ * steps, checks, ensembles, noises, inrandoms, iterations, ipsteps, seed,
+ * boundaries, linear, deriv, initial, observe) after xSPDE's defaults have
+ * been applied.  Function-valued fields are passed as the text of the MATLAB
+ * anonymous function (what func2str returns), e.g.
+ *   deriv  = "@(a,w,p) 1i*a.*conj(a).*a + 0.01*(w(1,:)+1i*w(2,:))/sqrt(2)"
+ * The text is compiled into the fused kernel (NVRTC, sm_100a).  Expressions
+ * outside the supported grammar make xs_create fail with XS_ERR_GRAMMAR:
+ * there is no CPU fallback.
+ *
+ * Conventions: all host arrays are caller-owned, complex values are
+ * interleaved (re, im) FP64, and array layout is MATLAB column-major with the
+ * field index fastest and the ensemble index slowest: a(fields, space..., ens).
+ * The library owns its device buffers.  Every call returns XS_OK (0) or a
+ * negative XS_ERR_* code and never aborts; xs_last_error() gives the message
+ * of the calling thread's last failure.  One handle per host thread.
+ */
+#ifndef XSPDE_B200_H
+#define XSPDE_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+#define XS_EXTERN extern "C"
+#else
+#define XS_EXTERN extern
+#endif
+#define XS_API XS_EXTERN __attribute__((visibility("default")))
+
+typedef struct xs_handle xs_handle;
+typedef int xs_status;
+
+enum {
+  XS_OK = 0,
+  XS_ERR_SHAPE = -1,       /* sizes or layout not supported / inconsistent */
+  XS_ERR_GRAMMAR = -2,     /* MATLAB expression outside the device grammar */
+  XS_ERR_NVRTC = -3,       /* runtime compilation failed */
+  XS_ERR_CUDA = -4,        /* CUDA runtime/driver error */
+  XS_ERR_NAN = -5,         /* a trajectory produced a non-finite value */
+  XS_ERR_TIMEOUT = -6,     /* a bounded device wait gave up */
+  XS_ERR_ARG = -7,         /* invalid argument */
+  XS_ERR_NODEVICE = -8,    /* no CUDA device */
+  XS_ERR_UNSUPPORTED = -9  /* valid xSPDE input that this path does not cover */
+};
+
+enum { XS_METHOD_MP = 0, XS_METHOD_RK4 = 1, XS_METHOD_EULER = 2, XS_METHOD_RK2 = 3, XS_METHOD_IMPLICIT = 4 };
+enum { XS_PREC_FP64 = 0, XS_PREC_FP32 = 1 };
+
+#define XS_MAXDIM 4 /* p.dimensions up to 4: time + 3 space dimensions */
+
+typedef struct xs_problem {
+  int dimensions;              /* p.dimensions: 1 = SDE, 2..4 = SPDE with 1..3 space dims */
+  int fields;                  /* components of the single field cell, p.fields */
+  int noises;                  /* Gaussian x-space noises, p.noises */
+  int inrandoms;               /* initial Gaussian randoms, p.inrandoms */
+  int points[XS_MAXDIM];       /* p.points after space steps (xpreferences.m:137) */
+  double ranges[XS_MAXDIM];    /* p.ranges */
+  double origins[XS_MAXDIM];   /* p.origins */
+  int steps;                   /* p.steps(1) */
+  int checks;                  /* p.checks(1): 1 = step-halving fine/coarse passes */
+  int ensembles[3];            /* p.ensembles */
+  int method;                  /* XS_METHOD_* (p.method) */
+  int iterations;              /* p.iterations (MP, Implicit) */
+  int ipsteps;                 /* p.ipsteps: propagator is exp(L dtr/ipsteps) */
+  int precision;               /* XS_PREC_FP64 or XS_PREC_FP32 (fields/transforms/drift) */
+  unsigned long long seed;     /* p.seed */
+  const int* boundaries;       /* NULL: periodic; else [dimensions-1][fields][2] of p.boundaries{1,d}(i,b) */
+  const char* deriv;           /* p.deriv text, "@(a,w,p) ..." */
+  const char* initial;         /* p.initial text, "@(v,p) ..." */
+  const char* linear;          /* p.linear text "@(p) ..." or NULL/"" for none */
+  int nobserve;                /* number of observe functions (0 -> default "a") */
+  const char* const* observe;  /* p.observe texts, "@(a,p) ..." */
+  int nparams;                 /* named scalar constants readable as p.<name> */
+  const char* const* param_names;
+  const double* param_values;
+  int path_kind;               /* 0 = automatic, 1 = resident, 2 = streaming */
+} xs_problem;
+
+/* Create a handle: parse, generate and compile the kernels (NVRTC, cached).
+ * Replaces no single reference function: it is the one-time set-up that
+ * Simulator/xensemble.m:47 (p.propfactor) and the per-call evaluation of the
+ * user's handles amount to. */
+XS_API xs_status xs_create(const xs_problem* prob, xs_handle** out);
+XS_API void xs_destroy(xs_handle* h);
+
+/* Message of the calling thread's last failed call (truncated to n bytes).
+ * Returns the full message length. */
+XS_API size_t xs_last_error(char* buf, size_t n);
+
+/* Library version string. */
+XS_API const char* xs_version(void);
+
+/* Shape of observable o (0-based): lines, and spatial = 1 when the ensemble
+ * average keeps the lattice (av{o} is [lines, time, space...]) or 0 when it is
+ * [lines, time] (Int/Ave over all space).  Mirrors the observe sizing of
+ * Simulator/xpreferences.m:262-343. */
+XS_API xs_status xs_observe_info(const xs_handle* h, int o, int* lines, int* spatial);
+
+/* Bytes of av_out for nblocks blocks: sum over observables of
+ * lines*points(1)*(spatial ? nspace : 1) complex doubles, per block. */
+XS_API size_t xs_av_doubles_per_block(const xs_handle* h);
+
+/* p.path replacement (Simulator/xpath.m): integrate ensemble blocks
+ * first_block .. first_block+nblocks-1 (global block index
+ * npar-1 + (j-1)*ensembles(3), Simulator/xensemble.m:26) for check pass nc
+ * (1 = fine, 2 = coarse; Simulator/xensemble.m:27).
+ *   a_in   NULL: the initial field is p.initial(p.randomgen(p)) evaluated on the
+ *          device (Simulator/xensemble.m:53-64); else [fields, space, ens1*nblocks]
+ *          complex FP64 (the `a` that xensemble passes to p.path).
+ *   av_out per block, per observable o in order, the block mean av{o}
+ *          [lines, points(1), space] complex FP64 (Simulator/xpath.m:189).
+ *   a_out  NULL or the final field, same layout as a_in.
+ * Host pointers; copies are synchronous with respect to the caller. */
+XS_API xs_status xs_run_path(xs_handle* h, int first_block, int nblocks, int nc, const double* a_in,
+                             double* av_out, double* a_out);
+
+/* Same as xs_run_path with device pointers and a caller stream (cudaStream_t
+ * passed as void*); nothing is copied to or from the host and the call
+ * returns without synchronising.  av_dev uses the layout of av_out;
+ * a_in_dev/a_out_dev may be NULL. */
+XS_API xs_status xs_run_path_device(xs_handle* h, int first_block, int nblocks, int nc, const double* a_in_dev,
+                                    double* av_dev, double* a_out_dev, void* stream);
+
+/* Wait for the handle's work and report device-side status (XS_ERR_NAN when a
+ * trajectory became non-finite in the last run). */
+XS_API xs_status xs_sync(xs_handle* h);
+
+/* p.noisegen replacement, one draw (Simulator/xnoise.m:29-32): w_out =
+ * randn * sqrt(scale * noisefactor) as [noises, space, ens1] real FP64 for
+ * block `block`, draw index `draw` (1 = first call of a path).  The coarse
+ * average (xnoise.m:33-35) stays with the caller. */
+XS_API xs_status xs_noise(xs_handle* h, int block, int draw, double scale, double* w_out);
+
+/* p.randomgen replacement (Simulator/xrandom.m:20-23): [inrandoms, space, ens1]
+ * real FP64, randn * sqrt(noisefactor), Philox draw 0. */
+XS_API xs_status xs_random(xs_handle* h, int block, double* v_out);
+
+/* p.method replacement (Applications/SDE/<method>.m): one step of length dtr
+ * from time t on a [fields, space, ens1] complex FP64 field, in place, with
+ * the pre-scaled noise w [noises, space, ens1] (NULL: zero noise). */
+XS_API xs_status xs_step(xs_handle* h, double* a_inout, const double* w, double t, double dtr);
+
+/* Compile-only check (no device needed): parse and NVRTC-compile the kernels
+ * of a problem for sm_100a.  Writes the compile log (truncated to n). */
+XS_API xs_status xs_compile_check(const xs_problem* prob, char* log, size_t n);
+
+#endif /* XSPDE_B200_H */

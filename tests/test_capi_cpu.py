@@ -1,0 +1,67 @@
+"""CPU-only checks of the C ABI library: it loads, exports every declared
+symbol, reports errors, and NVRTC compiles problem kernels for sm_100a
+(compilation needs no GPU)."""
+import ctypes
+import os
+import re
+
+import pytest
+
+from xspde_matlab_b200 import _lib
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def test_header_exports_match():
+    hdr = open(os.path.join(ROOT, "include", "xspde_b200.h")).read()
+    declared = set(re.findall(r"XS_API\s+[\w\s\*]+?\b(xs_\w+)\s*\(", hdr))
+    assert declared == set(_lib.EXPORTS)
+    L = _lib.lib()
+    for name in declared:
+        assert hasattr(L, name), name
+
+
+def test_version_and_error_buffer():
+    L = _lib.lib()
+    assert b"sm_100a" in L.xs_version()
+    h = ctypes.c_void_p()
+    assert L.xs_create(None, ctypes.byref(h)) == -7
+    assert "null problem" in _lib.last_error()
+
+
+def _problem(**kw):
+    from tests.capi_problems import make_problem
+    return make_problem(**kw)
+
+
+def test_compile_check_cfg1(tmp_path, monkeypatch):
+    monkeypatch.setenv("XSPDE_B200_CACHE", str(tmp_path))
+    p, keep = _problem()
+    log = ctypes.create_string_buffer(1 << 16)
+    rc = _lib.lib().xs_compile_check(ctypes.byref(p), log, len(log))
+    assert rc == 0, _lib.last_error()
+    assert any(f.endswith(".cubin") for f in os.listdir(tmp_path))
+
+
+@pytest.mark.parametrize("deriv,frag", [
+    ("@(a,w,p) D2(a,2,p)", "unsupported function 'D2'"),
+    ("@(a,w,p) a.*q", "unknown identifier 'q'"),
+    ("@(a,w,p) a + p.gamma", "unknown parameter 'p.gamma'"),
+    ("@(a,w,p) a(3,:)", "out of range"),
+    ("@(a,w,p) a + 'x'", "strings"),
+])
+def test_grammar_rejections(deriv, frag, tmp_path, monkeypatch):
+    monkeypatch.setenv("XSPDE_B200_CACHE", str(tmp_path))
+    p, keep = _problem(deriv=deriv)
+    rc = _lib.lib().xs_compile_check(ctypes.byref(p), None, 0)
+    assert rc == -2
+    assert frag in _lib.last_error()
+
+
+def test_named_scalars_and_precision(tmp_path, monkeypatch):
+    monkeypatch.setenv("XSPDE_B200_CACHE", str(tmp_path))
+    p, keep = _problem(deriv="@(a,w,p) -p.gamma*a + p.eps*conj(a) + sqrt(-p.chi*a.^2).*w(1,:)", precision=1,
+                       params={"gamma": 1.0, "eps": 0.5, "chi": 1e-3}, noises=1, dimensions=1, linear="",
+                       initial="@(v,p) 1", observe=("@(a,p) a",))
+    rc = _lib.lib().xs_compile_check(ctypes.byref(p), None, 0)
+    assert rc == 0, _lib.last_error()

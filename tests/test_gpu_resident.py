@@ -1,0 +1,138 @@
+"""GPU parity of the resident path against the CPU oracle.
+
+Each case runs one or more ensemble blocks through the device p.path
+replacement (C ABI xs_run_path) and through the oracle's xpath with the same
+Philox noise, and compares the block-mean observables av.  Tolerances:
+FP64 fields: 1e-10 relative to the largest |av|; FP32 fields (FP64 tables and
+moments): 2e-4 relative.
+"""
+import numpy as np
+import pytest
+
+from oracle import xspde_ref as X
+from tests.gpu_util import oracle_block_av, rel_err
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = 1e-10
+FP32_TOL = 2e-4
+
+
+def _gpu(pdict, blocks, nc, a_in=None, a_out=False, path_kind=0):
+    from xspde_matlab_b200 import GpuPath, xpreferences
+    p = xpreferences([pdict])[0]
+    g = GpuPath(p, path_kind)
+    return g.run_path(blocks[0], len(blocks), nc, a_in=a_in, a_out=a_out)
+
+
+def _compare(pg, po, blocks, ncs, tol):
+    for nc in ncs:
+        av_g, _ = _gpu(pg, blocks, nc)
+        for i, b in enumerate(blocks):
+            av_o, _ = oracle_block_av(po, b, nc)
+            for o in range(len(av_o)):
+                e = rel_err(av_g[i][o].reshape(-1, order="F"), av_o[o].reshape(-1, order="F"))
+                assert e < tol, (nc, b, o, e)
+
+
+SNLS = dict(dimensions=2, points=[11, 64], ranges=[1.0, 10.0], steps=4, ensembles=[8, 2, 1], noises=2)
+
+
+def _snls(method, checks, precision="fp64", **kw):
+    g = dict(SNLS, method=method, checks=checks, precision=precision,
+             deriv="@(a,w,p) 1i*a.*conj(a).*a + 0.01*(w(1,:)+1i*w(2,:))/sqrt(2)",
+             initial="@(v,p) exp(-p.x.^2)", linear="@(p) 1i*p.Dx.^2",
+             observe=["@(a,p) a.*conj(a)", "@(a,p) real(a)"], **kw)
+    o = dict(SNLS, method=method, checks=checks,
+             deriv=lambda a, w, p: 1j * a * np.conj(a) * a + 0.01 * (w[0:1] + 1j * w[1:2]) / np.sqrt(2),
+             initial=lambda v, p: np.exp(-p.x ** 2), linear=lambda p: 1j * p.Dx ** 2,
+             observe=[lambda a, p: a * np.conj(a), lambda a, p: np.real(a)], **kw)
+    return g, o
+
+
+@pytest.mark.parametrize("method", ["MP", "RK4"])
+@pytest.mark.parametrize("checks", [0, 1])
+def test_snls_1d_fp64(method, checks):
+    g, o = _snls(method, checks)
+    _compare(g, o, [0, 1], [1, 2] if checks else [1], FP64_TOL)
+
+
+def test_snls_1d_fp32_bound():
+    g, o = _snls("MP", 1, precision="fp32")
+    _compare(g, o, [0, 1], [1, 2], FP32_TOL)
+
+
+@pytest.mark.parametrize("method", ["Euler", "RK2", "Implicit", "MP", "RK4"])
+def test_kubo_sde_methods(method):
+    base = dict(dimensions=1, points=[11], ranges=[2.0], steps=5, ensembles=[64, 2, 1], noises=1, method=method,
+                checks=1)
+    g = dict(base, deriv="@(a,w,p) 1i*w.*a", initial="@(w,p) 1+0*w",
+             observe=["@(a,p) real(a(1,:))", "@(a,p) a(1,:).*conj(a(1,:))"])
+    o = dict(base, deriv=lambda a, w, p: 1j * w * a, initial=lambda w, p: 1 + 0 * w,
+             observe=[lambda a, p: np.real(a[0:1]), lambda a, p: a[0:1] * np.conj(a[0:1])])
+    _compare(g, o, [0, 1], [1, 2], FP64_TOL)
+
+
+def test_dpo_positive_p_two_fields():
+    base = dict(dimensions=1, fields=2, noises=2, points=[6], ranges=[1.0], steps=20, ensembles=[32, 2, 1],
+                method="MP", checks=1)
+    g = dict(base, params={"gam": 1.0, "eps": 1.3, "chi": 1e-3},
+             deriv="@(a,w,p) [-p.gam*a(1,:)+p.eps*a(2,:)-p.chi*a(1,:).^2.*a(2,:)+sqrt(-p.chi*a(1,:).^2).*w(1,:);"
+                   " -p.gam*a(2,:)+p.eps*a(1,:)-p.chi*a(2,:).^2.*a(1,:)+sqrt(-p.chi*a(2,:).^2).*w(2,:)]",
+             initial="@(v,p) [1+0.5i+0*v(1,:); 1-0.5i+0*v(2,:)]",
+             observe=["@(a,p) real(a(1,:).*a(2,:))", "@(a,p) a"])
+    gam, eps, chi = 1.0, 1.3, 1e-3
+
+    def deriv(a, w, p):
+        a1, a2 = a[0:1], a[1:2]
+        return np.concatenate([-gam * a1 + eps * a2 - chi * a1 ** 2 * a2 + np.sqrt(-chi * a1 ** 2 + 0j) * w[0:1],
+                               -gam * a2 + eps * a1 - chi * a2 ** 2 * a1 + np.sqrt(-chi * a2 ** 2 + 0j) * w[1:2]])
+    o = dict(base, deriv=deriv,
+             initial=lambda v, p: np.concatenate([1 + 0.5j + 0 * v[0:1], 1 - 0.5j + 0 * v[1:2]]),
+             observe=[lambda a, p: np.real(a[0:1] * a[1:2]), lambda a, p: a])
+    _compare(g, o, [0, 1], [1, 2], FP64_TOL)
+
+
+def test_gpe_2d_small_periodic():
+    base = dict(dimensions=3, points=[6, 16, 12], ranges=[0.5, 8.0, 6.0], steps=3, ensembles=[4, 2, 1], noises=2,
+                method="MP", checks=1)
+    g = dict(base, deriv="@(a,w,p) (1-abs(a).^2).*a - 0.5i*abs(a).^2.*a + 0.05*(w(1,:)+1i*w(2,:))/sqrt(2)",
+             initial="@(v,p) 1 + 0.1*(v(1,:)+1i*v(2,:))/sqrt(2)", linear="@(p) (1i+0.1)*(p.Dx.^2+p.Dy.^2)",
+             observe=["@(a,p) abs(a).^2", "@(a,p) Int(abs(a).^2, p)", "@(a,p) Ave(real(a), p)"])
+    o = dict(base, deriv=lambda a, w, p: (1 - abs(a) ** 2) * a - 0.5j * abs(a) ** 2 * a
+             + 0.05 * (w[0:1] + 1j * w[1:2]) / np.sqrt(2),
+             initial=lambda v, p: 1 + 0.1 * (v[0:1] + 1j * v[1:2]) / np.sqrt(2),
+             linear=lambda p: (1j + 0.1) * (p.Dx ** 2 + p.Dy ** 2),
+             observe=[lambda a, p: abs(a) ** 2, lambda a, p: X.Int(abs(a) ** 2, p), lambda a, p: X.Ave(np.real(a), p)])
+    _compare(g, o, [0, 1], [1, 2], FP64_TOL)
+
+
+def test_all_boundary_types_stochastic_heat():
+    bnd = [[1, 1], [-1, -1], [1, -1], [-1, 1], [0, 0]]
+    base = dict(dimensions=2, fields=5, noises=5, points=[9, 21], ranges=[0.4, np.pi], origins=[0, 0], steps=2,
+                ensembles=[4, 2, 1], method="MP", checks=1, boundaries=[None, bnd])
+    g = dict(base, deriv="@(a,w,p) 0.1*w - 0.2*a.*conj(a).*a",
+             initial="@(v,p) [4*sin(p.x)+sin(2*p.x); 5+4*cos(p.x)+cos(2*p.x); 4*sin(p.x/2)+sin(3*p.x/2);"
+                     " 4*cos(p.x/2)+cos(3*p.x/2); 2+cos(2*p.x/1.02)+sin(4*p.x/1.02)]",
+             linear="@(p) p.Dx.^2", observe=["@(a,p) a", "@(a,p) Int(abs(a).^2, p.dx, [0 0; 0.5 2.5], p)"])
+    x = None
+
+    def init(v, p):
+        x = p.x
+        return np.concatenate([4 * np.sin(x) + np.sin(2 * x), 5 + 4 * np.cos(x) + np.cos(2 * x),
+                               4 * np.sin(x / 2) + np.sin(3 * x / 2), 4 * np.cos(x / 2) + np.cos(3 * x / 2),
+                               2 + np.cos(2 * x / 1.02) + np.sin(4 * x / 1.02)], axis=0)
+    o = dict(base, deriv=lambda a, w, p: 0.1 * w - 0.2 * a * np.conj(a) * a, initial=init,
+             linear=lambda p: p.Dx ** 2,
+             observe=[lambda a, p: a, lambda a, p: X.Int(abs(a) ** 2, p.dx, [[0, 0], [0.5, 2.5]], p)])
+    _compare(g, o, [0, 1], [1, 2], FP64_TOL)
+
+
+def test_a_in_a_out_roundtrip():
+    g, o = _snls("RK4", 0)
+    av_o, b_o = oracle_block_av(o, 1, 1)
+    inp = X.xpreferences([o])[0]
+    a0 = np.broadcast_to(np.exp(-inp.x ** 2), inp.ca).astype(complex)
+    av_g, a_g = _gpu(g, [1], 1, a_in=a0, a_out=True)
+    assert rel_err(a_g, b_o) < FP64_TOL
+    assert rel_err(av_g[0][0], av_o[0]) < FP64_TOL

@@ -1,0 +1,404 @@
+// Resident-path kernel: every trajectory's field lives in shared memory for the
+// whole time loop of one xpath call (Simulator/xpath.m:137-194).  One CTA owns
+// XS_G trajectories of one ensemble block; the time loop, noise draws
+// (Simulator/xnoise.m:29-38), interaction-picture steps (Applications/SDE/*.m,
+// Applications/SPDE/xprop.m) and observables (Simulator/xdata.m:339-393) run
+// on chip.  HBM sees only the initial/final fields and one partial-sum row of
+// observables per output time.  Transforms along each space dimension are
+// dense N x N matrices (FFT, DST-I/II/III, DCT-I/II/III alike), applied from
+// L1/L2-resident tables; the propagator table exp(L dt) is FP64.
+#pragma once
+
+struct XsPathArgs {
+  int ntraj;          // trajectories in this launch (multiple of XS_G)
+  int ens1;           // trajectories per ensemble block
+  int block0;         // global block index of the first trajectory
+  int nc;             // 1 = fine pass, 2 = coarse pass
+  int checks;         // p.checks(1)
+  int npoints;        // p.points(1)
+  int steps;          // p.steps(1)
+  int seq;            // sequence index (Philox counter)
+  u32 seed;
+  int pad0;
+  double wscale;      // sqrt(nscale * noisefactor)
+  double vscale;      // sqrt(noisefactor)
+  double dtr;         // step of this pass
+  double t0;          // origin
+  const double2* prop;  // [XS_PROP_COMPS][XS_NS] exp(L dtr / ipsteps)
+  const cx* tmat;       // dense transforms, see xs_transform_dim
+  int tmat_off[4];      // per space dim (index 1..3), element offsets
+  const double2* a_in;  // optional [ntraj][F][NS] initial field (FP64)
+  double2* a_out;       // optional [ntraj][F][NS] final field (FP64)
+  double2* obs;         // [npoints][nctas][XS_OBS_STRIDE] observable partial sums
+  int* status;          // bit 0: non-finite field
+};
+
+#define XS_STRIDE1 1
+#define XS_STRIDE2 (XS_N1)
+#define XS_STRIDE3 (XS_N1 * XS_N2)
+
+__device__ __forceinline__ void xs_site(int s, int& i1, int& i2, int& i3, real& x, real& y, real& z) {
+  i1 = s % XS_N1;
+  i2 = (s / XS_N1) % XS_N2;
+  i3 = s / (XS_N1 * XS_N2);
+  x = (real)(XS_O1 + XS_DX1 * (double)i1);
+  y = (real)(XS_O2 + XS_DX2 * (double)i2);
+  z = (real)(XS_O3 + XS_DX3 * (double)i3);
+}
+
+template <int D>
+__device__ __forceinline__ void xs_transform_dim(cx* X, cx* T, const XsPathArgs& P, int dir) {
+  constexpr int ND = D == 1 ? XS_N1 : (D == 2 ? XS_N2 : XS_N3);
+  constexpr int SD = D == 1 ? XS_STRIDE1 : (D == 2 ? XS_STRIDE2 : XS_STRIDE3);
+  if (ND <= 1) return;
+  const cx* M0 = P.tmat + P.tmat_off[D];
+  __syncthreads();
+  for (int i = threadIdx.x; i < XS_G * XS_F * XS_NS; i += blockDim.x) {
+    const int s = i % XS_NS;
+    const int gf = i / XS_NS;
+    const int f = gf % XS_F;
+    const int k = (s / SD) % ND;
+    const int base = gf * XS_NS + s - k * SD;
+    const cx* M = M0 + (size_t)(f * 2 + dir) * ND * ND;
+    real ar = 0, ai = 0;
+#pragma unroll 8
+    for (int n = 0; n < ND; ++n) {
+      const cx m = M[n * ND + k];
+      const cx v = X[base + n * SD];
+      ar += m.re * v.re - m.im * v.im;
+      ai += m.re * v.im + m.im * v.re;
+    }
+    T[i] = mkcx(ar, ai);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < XS_G * XS_F * XS_NS; i += blockDim.x) X[i] = T[i];
+  __syncthreads();
+}
+
+__device__ __forceinline__ void xs_setbound(cx* X) {
+#if XS_SETBOUND
+  for (int i = threadIdx.x; i < XS_G * XS_NS; i += blockDim.x) {
+    const int g = i / XS_NS, s = i % XS_NS;
+    int i1, i2, i3;
+    real x, y, z;
+    xs_site(s, i1, i2, i3, x, y, z);
+#pragma unroll
+    for (int f = 0; f < XS_F; ++f)
+      if (xs_dirichlet(f, i1, i2, i3)) X[(g * XS_F + f) * XS_NS + s] = mkcx((real)0, (real)0);
+  }
+  __syncthreads();
+#endif
+}
+
+// xprop (Applications/SPDE/xprop.m:76-104): transform, multiply by exp(L dt), inverse.
+__device__ __forceinline__ void xs_prop(cx* X, cx* T, const XsPathArgs& P) {
+#if XS_HAS_PROP
+  xs_transform_dim<1>(X, T, P, 0);
+  xs_transform_dim<2>(X, T, P, 0);
+  xs_transform_dim<3>(X, T, P, 0);
+  for (int i = threadIdx.x; i < XS_G * XS_F * XS_NS; i += blockDim.x) {
+    const int s = i % XS_NS;
+    const int f = (i / XS_NS) % XS_F;
+    const double2 pr = P.prop[(XS_PROP_COMPS > 1 ? f : 0) * XS_NS + s];
+    const cx v = X[i];
+    const double vr = (double)v.re, vi = (double)v.im;
+    X[i] = mkcx((real)(vr * pr.x - vi * pr.y), (real)(vr * pr.y + vi * pr.x));
+  }
+  xs_transform_dim<1>(X, T, P, 1);
+  xs_transform_dim<2>(X, T, P, 1);
+  xs_transform_dim<3>(X, T, P, 1);
+#endif
+  __syncthreads();
+  xs_setbound(X);
+  __syncthreads();
+}
+
+// dst = base + h * deriv(src, w, t), pointwise over sites (all components at once).
+__device__ __forceinline__ void xs_deriv_update(cx* dst, const cx* base, const cx* src, const real* W, real h, double t) {
+  for (int i = threadIdx.x; i < XS_G * XS_NS; i += blockDim.x) {
+    const int g = i / XS_NS, s = i % XS_NS;
+    int i1, i2, i3;
+    real x, y, z;
+    xs_site(s, i1, i2, i3, x, y, z);
+    cx a[XS_F], d[XS_F];
+    real w[XS_NW > 0 ? XS_NW : 1];
+#pragma unroll
+    for (int f = 0; f < XS_F; ++f) a[f] = src[(g * XS_F + f) * XS_NS + s];
+#pragma unroll
+    for (int c = 0; c < XS_NW; ++c) w[c] = W[(g * XS_NWS + c) * XS_NS + s];
+    xs_deriv(a, w, x, y, z, (real)t, d);
+#pragma unroll
+    for (int f = 0; f < XS_F; ++f) {
+      const int j = (g * XS_F + f) * XS_NS + s;
+      dst[j] = base[j] + h * d[f];
+    }
+  }
+  __syncthreads();
+}
+
+__device__ __forceinline__ void xs_axpby(cx* dst, real ca, const cx* A, real cb, const cx* B) {
+  for (int i = threadIdx.x; i < XS_G * XS_F * XS_NS; i += blockDim.x) dst[i] = ca * A[i] + cb * B[i];
+  __syncthreads();
+}
+__device__ __forceinline__ void xs_copy(cx* dst, const cx* src) {
+  for (int i = threadIdx.x; i < XS_G * XS_F * XS_NS; i += blockDim.x) dst[i] = src[i];
+  __syncthreads();
+}
+
+// One interaction-picture step of the selected method.  t is the time at the
+// start of the step (xpath's p.t).
+__device__ void xs_method(cx* A, cx* B1, cx* B2, cx* B3, cx* T, const real* W, const XsPathArgs& P, double t) {
+  const double dtr = P.dtr;
+#if XS_METHOD == 0
+  // MP (Applications/SDE/MP.m:10-27)
+  const real h = (real)(dtr * 0.5);
+  xs_prop(A, T, P);
+  xs_copy(B1, A);
+  for (int it = 0; it < XS_ITER; ++it) {
+    xs_deriv_update(A, B1, A, W, h, t + dtr * 0.5);
+    xs_setbound(A);
+  }
+  xs_axpby(A, (real)2, A, (real)-1, B1);
+  xs_prop(A, T, P);
+#elif XS_METHOD == 1
+  // RK4 (Applications/SDE/RK4.m:35-70)
+  const real h = (real)(dtr * 0.5);
+  xs_setbound(A);
+  xs_deriv_update(B1, A, A, W, h, t);
+  xs_prop(B1, T, P);
+  xs_prop(A, T, P);
+  xs_deriv_update(B2, A, B1, W, h, t + dtr * 0.5);
+  xs_setbound(B2);
+  xs_deriv_update(B3, A, B2, W, (real)(2 * (dtr * 0.5)), t + dtr * 0.5);
+  xs_setbound(B3);
+  for (int i = threadIdx.x; i < XS_G * XS_F * XS_NS; i += blockDim.x)
+    A[i] = (B1[i] + (real)2 * B2[i] + B3[i] - A[i]) / (real)3;
+  __syncthreads();
+  xs_prop(A, T, P);
+  xs_prop(B3, T, P);
+  xs_deriv_update(A, A, B3, W, (real)(dtr * 0.5 / 3.0), t + dtr);
+  xs_setbound(A);
+#elif XS_METHOD == 2
+  // Euler (Applications/SDE/Euler.m:77-81)
+  xs_deriv_update(A, A, A, W, (real)dtr, t);
+  xs_prop(A, T, P);
+#elif XS_METHOD == 3
+  // RK2 (Applications/SDE/RK2.m:89-107): B1 holds the predictor a.
+  xs_deriv_update(B1, A, A, W, (real)dtr, t);
+  xs_prop(A, T, P);
+  xs_prop(B1, T, P);
+  xs_deriv_update(A, A, B1, W, (real)dtr, t + dtr);
+  xs_axpby(A, (real)0.5, B1, (real)0.5, A);
+#elif XS_METHOD == 4
+  // Implicit (Applications/SDE/Implicit.m:116-125)
+  xs_copy(B1, A);
+  for (int it = 0; it < XS_ITER; ++it) xs_deriv_update(A, B1, A, W, (real)dtr, t + dtr);
+  xs_prop(A, T, P);
+#endif
+  __syncthreads();
+}
+
+// Noise of one p.noisegen call into W (coarse pass: averaged with Wp, xnoise.m:33-35).
+__device__ __forceinline__ void xs_noise(real* W, real* Wp, int mode, int draw, int g0, const XsPathArgs& P) {
+#if XS_NW > 0
+  for (int i = threadIdx.x; i < XS_G * XS_NS; i += blockDim.x) {
+    const int g = i / XS_NS, s = i % XS_NS;
+    const int e = g0 + g;
+    const u32 blk = (u32)(P.block0 + e / P.ens1);
+    const u32 el = (u32)(e % P.ens1);
+    real z[XS_NW];
+    xs_normals<XS_NW>(z, (u32)s, el, (u32)draw, (u32)P.seq, P.seed, blk);
+#pragma unroll
+    for (int c = 0; c < XS_NW; ++c) {
+      const int j = (g * XS_NWS + c) * XS_NS + s;
+      const real v = z[c] * (real)P.wscale;
+      if (mode == 0) W[j] = v;                          // fine draw
+      else if (mode == 1) Wp[j] = v;                    // first coarse draw
+      else W[j] = (v + Wp[j]) * (real)0.5;              // averaged coarse draw
+    }
+  }
+  __syncthreads();
+#endif
+}
+
+// Observables at one output time: per-CTA sums over its trajectories.
+__device__ void xs_observe(const cx* A, cx* RED, int n, double t, const XsPathArgs& P, double* wsum) {
+  const int cta = blockIdx.x;
+  const int nctas = gridDim.x;
+  double2* out = P.obs + ((size_t)n * nctas + cta) * XS_OBS_STRIDE;
+#if XS_NRED > 0
+  // full-space reductions (Int/Ave) per trajectory
+  for (int g = 0; g < XS_G; ++g) {
+    double acc[2 * XS_NRED];
+#pragma unroll
+    for (int k = 0; k < 2 * XS_NRED; ++k) acc[k] = 0;
+    for (int s = threadIdx.x; s < XS_NS; s += blockDim.x) {
+      int i1, i2, i3;
+      real x, y, z;
+      xs_site(s, i1, i2, i3, x, y, z);
+      cx a[XS_F], r[XS_NRED];
+#pragma unroll
+      for (int f = 0; f < XS_F; ++f) a[f] = A[(g * XS_F + f) * XS_NS + s];
+      xs_integrands(a, i1, i2, i3, x, y, z, (real)t, r);
+#pragma unroll
+      for (int k = 0; k < XS_NRED; ++k) { acc[2 * k] += (double)r[k].re; acc[2 * k + 1] += (double)r[k].im; }
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int k = 0; k < 2 * XS_NRED; ++k) {
+      double v = xs_warp_sum(acc[k]);
+      if (lane == 0) wsum[warp * 2 * XS_NRED + k] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 2 * XS_NRED) {
+      double v = 0;
+      for (int q = 0; q < nw; ++q) v += wsum[q * 2 * XS_NRED + threadIdx.x];
+      real* rr = (real*)(RED + g * XS_NRED);
+      rr[threadIdx.x] = (real)v;
+    }
+    __syncthreads();
+  }
+#endif
+#if XS_NOUT_SITE > 0
+  for (int s = threadIdx.x; s < XS_NS; s += blockDim.x) {
+    int i1, i2, i3;
+    real x, y, z;
+    xs_site(s, i1, i2, i3, x, y, z);
+    double sr[XS_NOUT_SITE], si[XS_NOUT_SITE];
+#pragma unroll
+    for (int k = 0; k < XS_NOUT_SITE; ++k) sr[k] = si[k] = 0;
+    for (int g = 0; g < XS_G; ++g) {
+      cx a[XS_F], o[XS_NOUT_SITE];
+#pragma unroll
+      for (int f = 0; f < XS_F; ++f) a[f] = A[(g * XS_F + f) * XS_NS + s];
+      xs_obs_site(a, RED + g * (XS_NRED > 0 ? XS_NRED : 1), x, y, z, (real)t, o);
+#pragma unroll
+      for (int k = 0; k < XS_NOUT_SITE; ++k) { sr[k] += (double)o[k].re; si[k] += (double)o[k].im; }
+    }
+#pragma unroll
+    for (int k = 0; k < XS_NOUT_SITE; ++k) out[(size_t)k * XS_NS + s] = make_double2(sr[k], si[k]);
+  }
+#endif
+#if XS_NOUT_SCALAR > 0
+  if (threadIdx.x == 0) {
+    double sr[XS_NOUT_SCALAR], si[XS_NOUT_SCALAR];
+    for (int k = 0; k < XS_NOUT_SCALAR; ++k) sr[k] = si[k] = 0;
+    for (int g = 0; g < XS_G; ++g) {
+      cx o[XS_NOUT_SCALAR];
+      xs_obs_scalar(RED + g * (XS_NRED > 0 ? XS_NRED : 1), (real)t, o);
+      for (int k = 0; k < XS_NOUT_SCALAR; ++k) { sr[k] += (double)o[k].re; si[k] += (double)o[k].im; }
+    }
+    for (int k = 0; k < XS_NOUT_SCALAR; ++k)
+      out[(size_t)XS_NOUT_SITE * XS_NS + k] = make_double2(sr[k], si[k]);
+  }
+#endif
+  __syncthreads();
+}
+
+extern "C" __global__ void __launch_bounds__(XS_THREADS) xs_resident(const XsPathArgs P) {
+  extern __shared__ __align__(16) unsigned char xs_smem[];
+  constexpr int GF = XS_G * XS_F * XS_NS;
+  cx* A = (cx*)xs_smem;
+  cx* B1 = A + GF;
+  cx* B2 = B1 + (XS_NARR >= 3 ? GF : 0);
+  cx* B3 = B2 + (XS_NARR >= 4 ? GF : 0);
+  cx* T = A + (XS_NARR - 1) * GF;     // transform scratch is the last array
+  cx* RED = A + XS_NARR * GF;         // [G][NRED]
+  double* wsum = (double*)(RED + XS_G * (XS_NRED > 0 ? XS_NRED : 1));  // [32][2*NRED]
+  real* W = (real*)(wsum + 32 * 2 * (XS_NRED > 0 ? XS_NRED : 1));
+  real* Wp = W + XS_G * XS_NWS * XS_NS;
+  const int g0 = blockIdx.x * XS_G;
+  {
+    // The layout above must fit the dynamic shared memory of this launch;
+    // refuse to run (status bit 1) rather than touch memory outside it.
+    u32 dyn;
+    asm volatile("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn));
+    const size_t need = (size_t)((unsigned char*)(Wp + XS_G * XS_NWS * XS_NS) - xs_smem);
+    if (need > (size_t)dyn || need != (size_t)XS_SMEM_BYTES || (int)blockDim.x != XS_THREADS ||
+        (blockIdx.x + 1) * XS_G > (unsigned)P.ntraj) {
+      if (threadIdx.x == 0) atomicOr(P.status, 2);
+      return;
+    }
+  }
+
+  // initial field: p.initial(v,p) with v = p.randomgen(p) (xensemble.m:53-64)
+  for (int i = threadIdx.x; i < XS_G * XS_NS; i += blockDim.x) {
+    const int g = i / XS_NS, s = i % XS_NS;
+    const int e = g0 + g;
+    cx a[XS_F];
+    if (P.a_in) {
+#pragma unroll
+      for (int f = 0; f < XS_F; ++f) {
+        const double2 v = P.a_in[((size_t)e * XS_F + f) * XS_NS + s];
+        a[f] = mkcx((real)v.x, (real)v.y);
+      }
+    } else {
+      int i1, i2, i3;
+      real x, y, z;
+      xs_site(s, i1, i2, i3, x, y, z);
+      real v[XS_NV > 0 ? XS_NV : 1];
+#if XS_NV > 0
+      xs_normals<XS_NV>(v, (u32)s, (u32)(e % P.ens1), 0u, (u32)P.seq, P.seed, (u32)(P.block0 + e / P.ens1));
+#pragma unroll
+      for (int c = 0; c < XS_NV; ++c) v[c] *= (real)P.vscale;
+#endif
+      xs_initial(v, x, y, z, a);
+    }
+#pragma unroll
+    for (int f = 0; f < XS_F; ++f) A[(g * XS_F + f) * XS_NS + s] = a[f];
+  }
+  __syncthreads();
+
+  double t = P.t0;
+  int draw = 0;
+  for (int n = 0; n < P.npoints; ++n) {
+    for (int step = 0; step < P.steps; ++step) {
+      if (n > 0 || step > 0 || P.npoints == 1) {
+        for (int chk = 0; chk <= P.checks; ++chk) {
+          ++draw;
+          int mode = 0;
+          if (P.nc == 2 && P.checks) mode = chk == 0 ? 1 : 2;
+          xs_noise(W, Wp, mode, draw, g0, P);
+          if (P.nc == 1 || chk == 1) {
+            __syncthreads();
+            xs_method(A, B1, B2, B3, T, W, P, t);
+            t += P.dtr;
+          }
+        }
+      }
+      if (step == 0) {
+        __syncthreads();
+        xs_observe(A, RED, n, t, P, wsum);
+      }
+    }
+  }
+  __syncthreads();
+  // final field and non-finite check
+  bool bad = false;
+  for (int i = threadIdx.x; i < GF; i += blockDim.x) {
+    const cx v = A[i];
+    if (!isfinite((double)v.re) || !isfinite((double)v.im)) bad = true;
+    if (P.a_out) {
+      const int g = i / (XS_F * XS_NS);
+      P.a_out[(size_t)(g0 + g) * XS_F * XS_NS + (i % (XS_F * XS_NS))] = make_double2((double)v.re, (double)v.im);
+    }
+  }
+  if (bad) atomicOr(P.status, 1);
+}
+
+// Block means over trajectories (xdata.m:84): av[b][n][k] = sum over the CTAs
+// of block b of obs partials, divided by ens1.  Fixed summation order.
+extern "C" __global__ void xs_obs_reduce(const double2* __restrict__ partial, double2* __restrict__ av,
+                                         int npoints, int nctas, int ctas_per_block, int stride, double inv_ens) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = blockIdx.y;
+  const int b = blockIdx.z;
+  if (k >= stride) return;
+  double sr = 0, si = 0;
+  for (int c = 0; c < ctas_per_block; ++c) {
+    const double2 v = partial[((size_t)n * nctas + (size_t)b * ctas_per_block + c) * stride + k];
+    sr += v.x;
+    si += v.y;
+  }
+  av[((size_t)b * npoints + n) * stride + k] = make_double2(sr * inv_ens, si * inv_ens);
+}

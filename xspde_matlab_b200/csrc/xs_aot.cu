@@ -1,0 +1,28 @@
+// Ahead-of-time kernels (compiled by nvcc for sm_100a) that do not depend on
+// the problem: layout conversion between the MATLAB host layout and the
+// device layout.  Problem kernels are generated and compiled by NVRTC.
+#include <cuda_runtime.h>
+
+// [F, NS, E] (MATLAB, field fastest) <-> [E][F][NS] (device), complex FP64.
+extern "C" __global__ void xs_aot_reorder(const double2* __restrict__ src, double2* __restrict__ dst, int F, int NS,
+                                          long long E, int to_device) {
+  const long long total = (long long)F * NS * E;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
+    const long long e = i / ((long long)F * NS);
+    const int r = (int)(i % ((long long)F * NS));
+    const int f = r / NS, s = r % NS;
+    const long long m = f + (long long)F * (s + (long long)NS * e);
+    if (to_device) dst[i] = src[m];
+    else dst[m] = src[i];
+  }
+}
+
+extern "C" int xs_aot_reorder_launch(const void* src, void* dst, int F, int NS, long long E, int to_device,
+                                      cudaStream_t st) {
+  const long long total = (long long)F * NS * E;
+  int blocks = (int)((total + 255) / 256);
+  if (blocks > 148 * 32) blocks = 148 * 32;
+  if (blocks < 1) blocks = 1;
+  xs_aot_reorder<<<blocks, 256, 0, st>>>((const double2*)src, (double2*)dst, F, NS, E, to_device);
+  return (int)cudaGetLastError();
+}

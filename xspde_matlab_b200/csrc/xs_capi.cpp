@@ -1,0 +1,1048 @@
+// Host side of the B200 xSPDE path: problem set-up (grids, FP64 tables),
+// kernel generation, NVRTC compilation with an on-disk cubin cache, device
+// buffers and launches.  Exposes the C ABI of include/xspde_b200.h.
+#include "xspde_b200.h"
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <nvrtc.h>
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <sstream>
+#include <string>
+#include <sys/stat.h>
+#include <unistd.h>
+#include <vector>
+
+#include "xs_expr.hpp"
+
+extern const char* xs_kernel_source_prelude;
+extern const char* xs_kernel_source_resident;
+extern const char* xs_kernel_source_stream;
+
+namespace {
+
+using cd = std::complex<double>;
+
+thread_local std::string g_err;
+
+struct XsError {
+  xs_status code;
+  std::string msg;
+};
+
+[[noreturn]] void raise(xs_status code, const std::string& msg) { throw XsError{code, msg}; }
+
+#define CUDA_CHECK(x)                                                                          \
+  do {                                                                                         \
+    cudaError_t e_ = (x);                                                                      \
+    if (e_ != cudaSuccess) raise(XS_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// Driver API entry points (resolved through the runtime; no link to libcuda)
+// ---------------------------------------------------------------------------
+typedef CUresult (*PFN_ModuleLoadData)(CUmodule*, const void*);
+typedef CUresult (*PFN_ModuleUnload)(CUmodule);
+typedef CUresult (*PFN_ModuleGetFunction)(CUfunction*, CUmodule, const char*);
+typedef CUresult (*PFN_FuncSetAttribute)(CUfunction, CUfunction_attribute, int);
+typedef CUresult (*PFN_LaunchKernel)(CUfunction, unsigned, unsigned, unsigned, unsigned, unsigned, unsigned,
+                                     unsigned, CUstream, void**, void**);
+typedef CUresult (*PFN_GetErrorString)(CUresult, const char**);
+
+struct Driver {
+  PFN_ModuleLoadData load = nullptr;
+  PFN_ModuleUnload unload = nullptr;
+  PFN_ModuleGetFunction getfn = nullptr;
+  PFN_FuncSetAttribute setattr = nullptr;
+  PFN_LaunchKernel launch = nullptr;
+  PFN_GetErrorString errstr = nullptr;
+};
+
+template <class T>
+void resolve(const char* name, T& fn) {
+  void* p = nullptr;
+  cudaDriverEntryPointQueryResult q;
+  cudaError_t e = cudaGetDriverEntryPointByVersion(name, &p, 12000, cudaEnableDefault, &q);
+  if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !p)
+    raise(XS_ERR_CUDA, std::string("cannot resolve driver entry point ") + name);
+  fn = reinterpret_cast<T>(p);
+}
+
+Driver& driver() {
+  static Driver d;
+  static std::once_flag once;
+  static std::string err;
+  std::call_once(once, [] {
+    try {
+      resolve("cuModuleLoadData", d.load);
+      resolve("cuModuleUnload", d.unload);
+      resolve("cuModuleGetFunction", d.getfn);
+      resolve("cuFuncSetAttribute", d.setattr);
+      resolve("cuLaunchKernel", d.launch);
+      resolve("cuGetErrorString", d.errstr);
+    } catch (const XsError& e) {
+      err = e.msg;
+    }
+  });
+  if (!err.empty()) raise(XS_ERR_CUDA, err);
+  return d;
+}
+
+void cu_check(CUresult r, const char* what) {
+  if (r == CUDA_SUCCESS) return;
+  const char* s = "?";
+  if (driver().errstr) driver().errstr(r, &s);
+  raise(XS_ERR_CUDA, std::string(what) + ": " + s);
+}
+
+void ensure_device() {
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0) raise(XS_ERR_NODEVICE, "no CUDA device available");
+  CUDA_CHECK(cudaFree(nullptr));  // create the primary context
+}
+
+// ---------------------------------------------------------------------------
+// NVRTC with on-disk cache
+// ---------------------------------------------------------------------------
+uint64_t fnv1a(const std::string& s, uint64_t h = 1469598103934665603ull) {
+  for (unsigned char c : s) {
+    h ^= c;
+    h *= 1099511628211ull;
+  }
+  return h;
+}
+
+std::string cache_dir() {
+  const char* e = getenv("XSPDE_B200_CACHE");
+  if (e && *e) return e;
+  const char* home = getenv("HOME");
+  return std::string(home && *home ? home : "/tmp") + "/.cache/xspde_b200";
+}
+
+void mkdirs(const std::string& path) {
+  std::string cur;
+  std::stringstream ss(path);
+  std::string part;
+  if (!path.empty() && path[0] == '/') cur = "/";
+  while (std::getline(ss, part, '/')) {
+    if (part.empty()) continue;
+    cur += part + "/";
+    mkdir(cur.c_str(), 0755);
+  }
+}
+
+std::string nvrtc_compile(const std::string& src, const std::string& name, std::string* log_out) {
+  std::vector<std::string> opts = {"--gpu-architecture=sm_100a", "-std=c++17", "--device-as-default-execution-space",
+                                   "-lineinfo", "--extra-device-vectorization", "-DXS_NVRTC=1"};
+  int maj = 0, min = 0;
+  nvrtcVersion(&maj, &min);
+  std::string key = src;
+  for (auto& o : opts) key += "\n" + o;
+  key += "\nnvrtc" + std::to_string(maj) + "." + std::to_string(min);
+  char hb[32];
+  snprintf(hb, sizeof hb, "%016llx", (unsigned long long)fnv1a(key));
+  std::string dir = cache_dir();
+  std::string path = dir + "/" + name + "_" + hb + ".cubin";
+  {
+    std::ifstream f(path, std::ios::binary);
+    if (f) {
+      std::string data((std::istreambuf_iterator<char>(f)), std::istreambuf_iterator<char>());
+      if (!data.empty()) return data;
+    }
+  }
+  nvrtcProgram prog;
+  if (nvrtcCreateProgram(&prog, src.c_str(), (name + ".cu").c_str(), 0, nullptr, nullptr) != NVRTC_SUCCESS)
+    raise(XS_ERR_NVRTC, "nvrtcCreateProgram failed");
+  std::vector<const char*> copts;
+  for (auto& o : opts) copts.push_back(o.c_str());
+  nvrtcResult r = nvrtcCompileProgram(prog, (int)copts.size(), copts.data());
+  size_t lsz = 0;
+  nvrtcGetProgramLogSize(prog, &lsz);
+  std::string log(lsz, '\0');
+  if (lsz) nvrtcGetProgramLog(prog, &log[0]);
+  if (log_out) *log_out = log;
+  if (r != NVRTC_SUCCESS) {
+    nvrtcDestroyProgram(&prog);
+    raise(XS_ERR_NVRTC, "NVRTC compilation failed:\n" + log);
+  }
+  size_t csz = 0;
+  nvrtcGetCUBINSize(prog, &csz);
+  std::string cubin(csz, '\0');
+  nvrtcGetCUBIN(prog, &cubin[0]);
+  nvrtcDestroyProgram(&prog);
+  mkdirs(dir);
+  std::string tmp = path + ".tmp" + std::to_string((long)getpid());
+  {
+    std::ofstream f(tmp, std::ios::binary);
+    f.write(cubin.data(), (std::streamsize)cubin.size());
+  }
+  rename(tmp.c_str(), path.c_str());
+  return cubin;
+}
+
+// ---------------------------------------------------------------------------
+// Problem description and FP64 host tables
+// ---------------------------------------------------------------------------
+struct ObsInfo {
+  int lines = 1;
+  bool spatial = true;
+  int red_off = 0;      // offset of its reductions in the combined red[] array
+  int out_off = 0;      // offset in the site (spatial) or scalar output lists
+  xs::Generated gen;
+};
+
+struct Problem {
+  xs_problem p{};
+  std::string deriv, initial, linear;
+  std::vector<std::string> observe;
+  xs::Scalars scalars;
+  std::vector<int> bnd;  // [D][F][2]
+  int D = 0, F = 1, NW = 0, NV = 0, NS = 1, E1 = 1;
+  int N[3] = {1, 1, 1};
+  double dx[XS_MAXDIM] = {1, 1, 1, 1}, dk[XS_MAXDIM] = {0, 0, 0, 0};
+  double dt = 0, nscale = 0, noisefactor = 1, dv = 1;
+  std::vector<double> xc[3];
+  std::vector<std::vector<std::vector<double>>> kprop;  // [F][D][N]
+  bool has_linear = false, setbound = false;
+  std::vector<cd> L;  // [Lc][NS]
+  int Lc = 1;
+  std::vector<ObsInfo> obs;
+  int nred = 0, nout_site = 0, nout_scalar = 0;
+  int type(int d, int f) const {  // boundary type b1 + 2*b2 (xtransform.m:134)
+    if (bnd.empty()) return 0;
+    return bnd[(d * F + f) * 2] + 2 * bnd[(d * F + f) * 2 + 1];
+  }
+};
+
+const char* method_name(int m) {
+  switch (m) {
+    case XS_METHOD_MP: return "MP";
+    case XS_METHOD_RK4: return "RK4";
+    case XS_METHOD_EULER: return "Euler";
+    case XS_METHOD_RK2: return "RK2";
+    case XS_METHOD_IMPLICIT: return "Implicit";
+  }
+  return "?";
+}
+
+void setup_problem(const xs_problem* in, Problem& P) {
+  if (!in) raise(XS_ERR_ARG, "null problem");
+  P.p = *in;
+  const xs_problem& p = P.p;
+  if (p.dimensions < 1 || p.dimensions > XS_MAXDIM)
+    raise(XS_ERR_UNSUPPORTED, "dimensions must be 1..4 (time + up to 3 space dimensions)");
+  if (p.fields < 1 || p.fields > 16) raise(XS_ERR_SHAPE, "fields must be 1..16");
+  if (p.noises < 0 || p.noises > 32 || p.inrandoms < 0 || p.inrandoms > 32) raise(XS_ERR_SHAPE, "noises/inrandoms must be 0..32");
+  if (p.steps < 1 || p.points[0] < 1) raise(XS_ERR_SHAPE, "points(1) and steps must be positive");
+  if (p.checks < 0 || p.checks > 1) raise(XS_ERR_SHAPE, "checks(1) must be 0 or 1");
+  if (p.method < 0 || p.method > 4) raise(XS_ERR_ARG, "unknown method");
+  if (p.iterations < 1) raise(XS_ERR_ARG, "iterations must be >= 1");
+  if (p.ipsteps < 1) raise(XS_ERR_ARG, "ipsteps must be >= 1");
+  for (int i = 0; i < 3; ++i)
+    if (p.ensembles[i] < 1) raise(XS_ERR_SHAPE, "ensembles must be >= 1");
+  P.D = p.dimensions - 1;
+  P.F = p.fields;
+  P.NW = p.noises;
+  P.NV = p.inrandoms;
+  P.E1 = p.ensembles[0];
+  P.NS = 1;
+  for (int d = 0; d < P.D; ++d) {
+    if (p.points[d + 1] < 1) raise(XS_ERR_SHAPE, "space points must be positive");
+    P.N[d] = p.points[d + 1];
+    P.NS *= P.N[d];
+  }
+  P.deriv = p.deriv ? p.deriv : "@(a,w,p) 0*a";
+  P.initial = p.initial ? p.initial : "@(v,p) 0";
+  P.linear = (p.linear && *p.linear) ? p.linear : "";
+  for (int i = 0; i < p.nobserve; ++i) P.observe.push_back(p.observe && p.observe[i] ? p.observe[i] : "@(a,p) a");
+  if (P.observe.empty()) P.observe.push_back("@(a,p) a");
+  for (int i = 0; i < p.nparams; ++i) P.scalars.values[p.param_names[i]] = p.param_values[i];
+  P.p.deriv = P.p.initial = P.p.linear = nullptr;
+  P.p.observe = nullptr;
+  P.p.param_names = nullptr;
+  P.p.param_values = nullptr;
+  if (p.boundaries) {
+    P.bnd.assign(in->boundaries, in->boundaries + (size_t)P.D * P.F * 2);
+    for (int v : P.bnd)
+      if (v < -1 || v > 1) raise(XS_ERR_ARG, "boundary flags must be -1, 0 or 1");
+    for (int d = 0; d < P.D; ++d)
+      for (int f = 0; f < P.F; ++f) {
+        int t = P.type(d, f);
+        if (t != 0 && t != 3 && t != -3 && t != 1 && t != -1)
+          raise(XS_ERR_ARG, "invalid boundary pair");
+        if (t != 0) P.setbound = true;
+      }
+  }
+  P.p.boundaries = nullptr;
+  // grid constants (Simulator/xpreferences.m:133-175, spdpreferences.m:190-244)
+  for (int d = 0; d < p.dimensions; ++d) {
+    int n = p.points[d];
+    P.dx[d] = n == 1 ? 1.0 : p.ranges[d] / std::max(1, n - 1);
+  }
+  P.dv = 1;
+  for (int d = 1; d < p.dimensions; ++d) P.dv *= P.dx[d];
+  P.noisefactor = 1.0 / P.dv;
+  for (int d = 1; d < p.dimensions; ++d) P.dk[d] = 2 * M_PI / (p.points[d] * P.dx[d]);
+  P.dk[0] = 2 * M_PI / (p.points[0] * P.dx[0]) / p.steps;
+  P.dt = p.ranges[0] / std::max(1, p.points[0] - 1);
+  P.nscale = p.steps * (1.0 + p.checks) / P.dt;
+  P.kprop.assign(P.F, std::vector<std::vector<double>>(P.D));
+  for (int d = 0; d < P.D; ++d) {
+    int n = P.N[d];
+    P.xc[d].resize(n);
+    for (int i = 0; i < n; ++i) P.xc[d][i] = p.origins[d + 1] + i * P.dx[d + 1];
+    double dkd = P.dk[d + 1];
+    double dkp = n > 1 ? M_PI / ((n - 1) * P.dx[d + 1]) : 0.0;
+    for (int f = 0; f < P.F; ++f) {
+      std::vector<double>& k = P.kprop[f][d];
+      k.resize(n);
+      int t = P.type(d, f);
+      for (int i = 0; i < n; ++i) {
+        if (t == 0) {
+          int j = (i + n / 2) % n;  // ifftshift of kc = (j - floor(n/2)) dk
+          k[i] = (j - n / 2) * dkd;
+        } else if (t == 3 || t == -3) {
+          k[i] = i * dkp;
+        } else if (t == -1) {
+          k[i] = i == 0 ? 0.0 : (i - 0.5) * dkp;
+        } else {  // t == 1
+          k[i] = i == n - 1 ? 0.0 : (i + 0.5) * dkp;
+        }
+      }
+    }
+  }
+  // linear operator -> L(k) in FP64 (xpropfactor.m:30-39)
+  if (!P.linear.empty()) {
+    xs::AnonFn fn = xs::parse_anon(P.linear);
+    if (P.D == 0) raise(XS_ERR_UNSUPPORTED, "p.linear needs at least one space dimension");
+    xs::GridInfo g;
+    g.ndim = P.D;
+    g.nfield = P.F;
+    for (int d = 0; d < P.D; ++d) {
+      g.n.push_back(P.N[d]);
+      g.x.push_back(P.xc[d]);
+    }
+    g.k.assign(P.F, std::vector<std::vector<double>>(P.D));
+    for (int f = 0; f < P.F; ++f)
+      for (int d = 0; d < P.D; ++d) g.k[f][d] = P.kprop[f][d];
+    P.L = xs::eval_linear(fn, g, P.scalars, &P.Lc);
+    P.has_linear = true;
+  }
+  if (P.D > 0 && !P.has_linear && P.setbound == false) {
+    // nothing: no propagation (xprop skips unit propagators)
+  }
+}
+
+// Host restatements of the reference's non-periodic transforms, applied to
+// unit vectors to obtain their (real) matrices.  They follow
+// Applications/SPDE/xdct1.m, xdst1.m, xdct2.m, xdct3.m, xdst2.m, xdst3.m with a
+// direct DFT in place of fft.
+std::vector<cd> dft(const std::vector<cd>& x) {
+  size_t M = x.size();
+  std::vector<cd> y(M);
+  for (size_t k = 0; k < M; ++k) {
+    cd acc = 0;
+    for (size_t n = 0; n < M; ++n) acc += x[n] * std::polar(1.0, -2 * M_PI * (double)((k * n) % M) / M);
+    y[k] = acc;
+  }
+  return y;
+}
+
+std::vector<double> transform_real(int type, bool inv, const std::vector<double>& a) {
+  int N = (int)a.size();
+  std::vector<double> out(N, 0.0);
+  if (N < 2) return a;
+  auto kind = type == -3 ? 0 : type == 3 ? 1 : type == -1 ? (inv ? 3 : 2) : (inv ? 5 : 4);
+  // 0 dct1, 1 dst1, 2 dst3 (fwd DN), 3 dst2 (inv DN), 4 dct3 (fwd ND), 5 dct2 (inv ND)
+  int M = N - 1;
+  if (kind == 0) {
+    std::vector<cd> e(2 * M);
+    for (int i = 0; i < N; ++i) e[i] = a[i];
+    for (int i = 1; i < N - 1; ++i) e[N - 1 + i] = a[N - 1 - i];
+    auto y = dft(e);
+    for (int k = 0; k < N; ++k) out[k] = y[k].real() * std::sqrt(1.0 / (2.0 * M));
+  } else if (kind == 1) {
+    std::vector<cd> e(2 * M);
+    for (int i = 1; i < N - 1; ++i) e[i] = a[i];
+    for (int i = 0; i < N - 2; ++i) e[N + i] = -a[N - 2 - i];
+    auto y = dft(e);
+    for (int k = 1; k < N - 1; ++k) out[k] = (y[k] * std::sqrt(2.0 / M) / cd(0, -2)).real();
+  } else if (kind == 5) {  // xdct2
+    std::vector<cd> e(2 * M);
+    for (int i = 0; i < M; ++i) e[i] = a[i];
+    auto y = dft(e);
+    for (int k = 0; k < M; ++k) out[k] = (y[k] * std::polar(1.0, -M_PI / (2.0 * M) * k)).real() * std::sqrt(2.0 / M);
+  } else if (kind == 4) {  // xdct3
+    std::vector<cd> e(2 * M);
+    for (int i = 1; i < M; ++i) e[i] = a[i] * std::polar(1.0, -M_PI / (2.0 * M) * i);
+    auto y = dft(e);
+    for (int k = 0; k < M; ++k) out[k] = (y[k].real() + 0.5 * a[0]) * std::sqrt(2.0 / M);
+  } else if (kind == 3) {  // xdst2
+    std::vector<cd> e(2 * M);
+    for (int i = 0; i < M; ++i) e[i] = a[i + 1] * std::polar(1.0, -M_PI / M * i);
+    auto y = dft(e);
+    for (int k = 0; k < M; ++k)
+      out[k + 1] = -(y[k] * std::polar(1.0, -M_PI / (2.0 * M) * (k + 1))).imag() * std::sqrt(2.0 / M);
+  } else {  // xdst3
+    std::vector<cd> e(2 * M);
+    for (int i = 0; i < M - 1; ++i) e[i] = a[i + 1] * std::polar(1.0, -M_PI / (2.0 * M) * i);
+    auto y = dft(e);
+    for (int k = 0; k < M; ++k) {
+      double alt = (k % 2 == 0) ? -1.0 : 1.0;  // cumprod(-ones): -1, +1, -1, ...
+      out[k + 1] = (-(y[k] * std::polar(1.0, -M_PI / M * (k + 0.5))).imag() - 0.5 * alt * a[N - 1]) * std::sqrt(2.0 / M);
+    }
+  }
+  return out;
+}
+
+// Matrix stored as M[n*N + k] = coefficient of input n in output k.
+std::vector<cd> transform_matrix(int type, bool inv, int N) {
+  std::vector<cd> M((size_t)N * N);
+  if (type == 0) {
+    for (int n = 0; n < N; ++n)
+      for (int k = 0; k < N; ++k) {
+        double ang = 2 * M_PI * (double)(((long long)k * n) % N) / N;
+        M[(size_t)n * N + k] = inv ? std::polar(1.0 / N, ang) : std::polar(1.0, -ang);
+      }
+    return M;
+  }
+  for (int n = 0; n < N; ++n) {
+    std::vector<double> e(N, 0.0);
+    e[n] = 1.0;
+    auto col = transform_real(type, inv, e);
+    for (int k = 0; k < N; ++k) M[(size_t)n * N + k] = col[k];
+  }
+  return M;
+}
+
+// ---------------------------------------------------------------------------
+// Code generation
+// ---------------------------------------------------------------------------
+std::string fmt(double v) {
+  char b[64];
+  snprintf(b, sizeof b, "%.17g", v);
+  return b;
+}
+
+xs::GenCtx make_ctx(const Problem& P, std::vector<xs::Role> roles, bool reduce) {
+  xs::GenCtx c;
+  c.roles = std::move(roles);
+  c.nfield = P.F;
+  c.nnoise = P.NW;
+  c.nrand = P.NV;
+  c.ndim = P.D;
+  c.allow_reduce = reduce;
+  c.scalars = &P.scalars;
+  for (int d = 0; d < P.p.dimensions; ++d) {
+    c.dx.push_back(P.dx[d]);
+    c.dk.push_back(P.dk[d]);
+    c.origins.push_back(P.p.origins[d]);
+    c.ranges.push_back(P.p.ranges[d]);
+  }
+  c.dt = P.dt;
+  return c;
+}
+
+void generate_functions(Problem& P, std::ostringstream& os) {
+  using xs::Role;
+  // deriv(a, w, p): xSPDE calls p.deriv{c}(a{:}, xi{:}, p) (MP.m:16)
+  {
+    auto fn = xs::parse_anon(P.deriv);
+    auto g = xs::generate(fn, make_ctx(P, {Role::Field, Role::Noise, Role::Params}, false));
+    if (g.len != P.F && g.len != 1)
+      raise(XS_ERR_SHAPE, "p.deriv returns " + std::to_string(g.len) + " components, fields = " + std::to_string(P.F));
+    os << "__device__ __forceinline__ void xs_deriv(const cx* __restrict__ a, const real* __restrict__ w, real x, real y, real z, real t, cx* __restrict__ out) {\n";
+    os << "  (void)a; (void)w; (void)x; (void)y; (void)z; (void)t;\n";
+    if (g.len == 1 && P.F > 1) {
+      os << "  cx o1[1];\n  { cx* out = o1;\n" << g.code << "  }\n";
+      os << "  for (int f = 0; f < " << P.F << "; ++f) out[f] = o1[0];\n";
+    } else {
+      os << g.code;
+    }
+    os << "}\n";
+  }
+  // initial(v, p) (xensemble.m:60)
+  {
+    auto fn = xs::parse_anon(P.initial);
+    auto g = xs::generate(fn, make_ctx(P, {Role::Random, Role::Params}, false));
+    if (g.len != P.F && g.len != 1)
+      raise(XS_ERR_SHAPE, "p.initial returns " + std::to_string(g.len) + " components, fields = " + std::to_string(P.F));
+    os << "__device__ __forceinline__ void xs_initial(const real* __restrict__ v, real x, real y, real z, cx* __restrict__ out) {\n";
+    os << "  (void)v; (void)x; (void)y; (void)z; const real t = (real)" << fmt(P.p.origins[0]) << "; (void)t;\n";
+    if (g.len == 1 && P.F > 1) {
+      os << "  cx o1[1];\n  { cx* out = o1;\n" << g.code << "  }\n";
+      os << "  for (int f = 0; f < " << P.F << "; ++f) out[f] = o1[0];\n";
+    } else {
+      os << g.code;
+    }
+    os << "}\n";
+  }
+  // observe{n}(a, p) (xdata.m:339)
+  P.obs.clear();
+  P.nred = P.nout_site = P.nout_scalar = 0;
+  for (auto& txt : P.observe) {
+    ObsInfo o;
+    auto fn = xs::parse_anon(txt);
+    o.gen = xs::generate(fn, make_ctx(P, {Role::Field, Role::Params}, true));
+    o.lines = o.gen.len;
+    o.spatial = o.gen.spatial;  // depends on the field or the site (0-D: one site)
+    o.red_off = P.nred;
+    for (auto& r : o.gen.reductions) {
+      if ((int)r.dims.size() != P.D)
+        raise(XS_ERR_UNSUPPORTED, "Int/Ave over a subset of the space dimensions is not supported on the device");
+      P.nred += r.lines;
+    }
+    if (o.spatial) {
+      o.out_off = P.nout_site;
+      P.nout_site += o.lines;
+    } else {
+      o.out_off = P.nout_scalar;
+      P.nout_scalar += o.lines;
+    }
+    P.obs.push_back(o);
+  }
+  os << "#define XS_NRED " << P.nred << "\n#define XS_NOUT_SITE " << P.nout_site << "\n#define XS_NOUT_SCALAR "
+     << P.nout_scalar << "\n#define XS_OBS_STRIDE (XS_NOUT_SITE * XS_NS + XS_NOUT_SCALAR)\n";
+  // integrands with bounds masks and weights
+  os << "__device__ __forceinline__ void xs_integrands(const cx* __restrict__ a, int i1, int i2, int i3, real x, real y, real z, real t, cx* __restrict__ rr) {\n";
+  os << "  (void)a; (void)i1; (void)i2; (void)i3; (void)x; (void)y; (void)z; (void)t; (void)rr;\n";
+  int off = 0;
+  for (auto& o : P.obs) {
+    for (auto& r : o.gen.reductions) {
+      double w = 1;
+      std::string mask = "true";
+      for (size_t q = 0; q < r.dims.size(); ++q) {
+        int d = r.dims[q] - 1;  // 0-based space dim
+        int n = P.N[d];
+        if (r.ave) w *= 1.0 / n;
+        else w *= r.weight[q];
+        double lo = r.lo[r.dims[q]], hi = r.hi[r.dims[q]];
+        if (!r.ave && lo < hi) {
+          // Int.m:273-277: j = 1+floor((lo-x(1))/d); while x(j) <= hi
+          double step = r.weight[q];
+          int j0 = (int)std::floor((lo - P.xc[d][0]) / step);
+          if (j0 < 0) j0 = 0;
+          int j = j0;
+          while (j < n && P.xc[d][j] <= hi) ++j;
+          const char* iv = d == 0 ? "i1" : d == 1 ? "i2" : "i3";
+          mask += std::string(" && ") + iv + " >= " + std::to_string(j0) + " && " + iv + " < " + std::to_string(j);
+        }
+      }
+      os << "  {\n    cx* r = rr + " << off << ";\n" << r.integrand_code;
+      os << "    const real wgt = (" << mask << ") ? (real)" << fmt(w) << " : (real)0;\n";
+      os << "    for (int k = 0; k < " << r.lines << "; ++k) r[k] = r[k] * wgt;\n  }\n";
+      off += r.lines;
+    }
+  }
+  os << "}\n";
+  os << "__device__ __forceinline__ void xs_obs_site(const cx* __restrict__ a, const cx* __restrict__ redall, real x, real y, real z, real t, cx* __restrict__ outall) {\n";
+  os << "  (void)a; (void)redall; (void)x; (void)y; (void)z; (void)t; (void)outall;\n";
+  for (auto& o : P.obs)
+    if (o.spatial)
+      os << "  {\n    const cx* red = redall + " << o.red_off << "; (void)red;\n    cx* out = outall + " << o.out_off
+         << ";\n" << o.gen.code << "  }\n";
+  os << "}\n";
+  os << "__device__ __forceinline__ void xs_obs_scalar(const cx* __restrict__ redall, real t, cx* __restrict__ outall) {\n";
+  os << "  (void)redall; (void)t; (void)outall; const cx* a = nullptr; const real x = 0, y = 0, z = 0; (void)a; (void)x; (void)y; (void)z;\n";
+  for (auto& o : P.obs)
+    if (!o.spatial)
+      os << "  {\n    const cx* red = redall + " << o.red_off << "; (void)red;\n    cx* out = outall + " << o.out_off
+         << ";\n" << o.gen.code << "  }\n";
+  os << "}\n";
+  // Dirichlet boundary mask (xsetbound.m:40-53, zero boundary values)
+  os << "__device__ __forceinline__ bool xs_dirichlet(int f, int i1, int i2, int i3) {\n  (void)f; (void)i1; (void)i2; (void)i3;\n";
+  if (!P.bnd.empty()) {
+    for (int f = 0; f < P.F; ++f) {
+      std::string cond = "false";
+      for (int d = 0; d < P.D; ++d) {
+        const char* iv = d == 0 ? "i1" : d == 1 ? "i2" : "i3";
+        if (P.N[d] <= 1) continue;
+        if (P.bnd[(d * P.F + f) * 2] == 1) cond += std::string(" || ") + iv + " == 0";
+        if (P.bnd[(d * P.F + f) * 2 + 1] == 1) cond += std::string(" || ") + iv + " == " + std::to_string(P.N[d] - 1);
+      }
+      os << "  if (f == " << f << ") return " << cond << ";\n";
+    }
+  }
+  os << "  return false;\n}\n";
+}
+
+// ---------------------------------------------------------------------------
+// Handle
+// ---------------------------------------------------------------------------
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  void ensure(size_t b) {
+    if (b <= bytes) return;
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+    CUDA_CHECK(cudaMalloc(&p, b));
+    bytes = b;
+  }
+  ~DevBuf() {
+    if (p) cudaFree(p);
+  }
+};
+
+struct ResidentPlan {
+  int G = 1, threads = 32, narr = 2;
+  size_t smem = 0;
+};
+
+}  // namespace
+
+struct xs_handle {
+  Problem P;
+  std::string header;     // generated problem header
+  std::string source;     // full kernel source
+  bool fp64 = true;
+  int kind = 1;           // 1 resident, 2 streaming
+  ResidentPlan rp;
+  // device state
+  bool loaded = false;
+  CUmodule mod = nullptr;
+  CUfunction f_resident = nullptr, f_reduce = nullptr, f_noise = nullptr;
+  cudaStream_t stream = nullptr;
+  DevBuf d_prop[2], d_tmat, d_obs, d_av, d_ain, d_aout, d_status, d_w;
+  double prop_dtr[2] = {-1, -1};
+  std::vector<int> tmat_off;
+  ~xs_handle() {
+    if (mod && driver().unload) driver().unload(mod);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+namespace {
+
+size_t resident_smem(const xs_handle& h, int G, int narr) {
+  const Problem& P = h.P;
+  size_t cxs = h.fp64 ? 16 : 8, rs = h.fp64 ? 8 : 4;
+  size_t nred = std::max(P.nred, 1);
+  size_t nws = std::max(P.NW, 1);
+  return (size_t)narr * G * P.F * P.NS * cxs + (size_t)G * nred * cxs + 32 * 2 * nred * 8 + 2 * (size_t)G * nws * P.NS * rs;
+}
+
+int method_arrays(int m) {
+  switch (m) {
+    case XS_METHOD_MP: return 3;
+    case XS_METHOD_RK4: return 5;
+    case XS_METHOD_EULER: return 2;
+    case XS_METHOD_RK2: return 3;
+    default: return 3;
+  }
+}
+
+void plan_resident(xs_handle& h, int total_traj) {
+  const Problem& P = h.P;
+  ResidentPlan rp;
+  rp.narr = method_arrays(P.p.method);
+  const size_t limit = 200 * 1024;
+  if (resident_smem(h, 1, rp.narr) > limit)
+    raise(XS_ERR_UNSUPPORTED, "field of one trajectory does not fit in shared memory for the resident path");
+  int best = 1;
+  for (int G = 1; G <= P.E1 && G <= 1024; ++G) {
+    if (P.E1 % G) continue;
+    if ((size_t)G * P.NS > 1024 && G > 1) break;
+    if (resident_smem(h, G, rp.narr) > limit) break;
+    if (G > 1 && total_traj / G < 296 && P.NS > 1) break;
+    best = G;
+  }
+  rp.G = best;
+  int items = rp.G * P.NS * P.F;
+  rp.threads = std::min(256, std::max(32, (items + 31) / 32 * 32));
+  rp.smem = resident_smem(h, rp.G, rp.narr);
+  h.rp = rp;
+}
+
+void build_source(xs_handle& h) {
+  Problem& P = h.P;
+  std::ostringstream fns;
+  generate_functions(P, fns);  // fixes P.nred / nout_* before the launch plan
+  plan_resident(h, P.E1 * P.p.ensembles[1] * P.p.ensembles[2]);
+  std::ostringstream os;
+  os << "// generated problem header\n";
+  os << "#define XS_FP64 " << (h.fp64 ? 1 : 0) << "\n#define XS_REAL " << (h.fp64 ? "double" : "float") << "\n";
+  os << xs_kernel_source_prelude << "\n";
+  os << "#define XS_F " << P.F << "\n#define XS_NW " << P.NW << "\n#define XS_NWS " << std::max(P.NW, 1)
+     << "\n#define XS_NV " << P.NV << "\n#define XS_ND " << P.D << "\n";
+  os << "#define XS_N1 " << P.N[0] << "\n#define XS_N2 " << P.N[1] << "\n#define XS_N3 " << P.N[2]
+     << "\n#define XS_NS " << P.NS << "\n";
+  for (int d = 0; d < 3; ++d) {
+    double o = d < P.D ? P.p.origins[d + 1] : 0.0;
+    double dx = d < P.D ? P.dx[d + 1] : 0.0;
+    os << "#define XS_O" << d + 1 << " " << fmt(o) << "\n#define XS_DX" << d + 1 << " " << fmt(dx) << "\n";
+  }
+  os << "#define XS_METHOD " << P.p.method << "\n#define XS_ITER " << P.p.iterations << "\n";
+  os << "#define XS_HAS_PROP " << ((P.has_linear && P.D > 0) ? 1 : 0) << "\n#define XS_PROP_COMPS " << P.Lc << "\n";
+  os << "#define XS_SETBOUND " << (P.setbound ? 1 : 0) << "\n";
+  os << "#define XS_G " << h.rp.G << "\n#define XS_THREADS " << h.rp.threads << "\n#define XS_NARR " << h.rp.narr << "\n";
+  os << "#define XS_SMEM_BYTES " << h.rp.smem << "\n";
+  os << fns.str();
+  os << xs_kernel_source_resident << "\n";
+  h.source = os.str();
+}
+
+void load_module(xs_handle& h) {
+  if (h.loaded) return;
+  ensure_device();
+  std::string cubin = nvrtc_compile(h.source, "xs_resident", nullptr);
+  Driver& d = driver();
+  cu_check(d.load(&h.mod, cubin.data()), "cuModuleLoadData");
+  cu_check(d.getfn(&h.f_resident, h.mod, "xs_resident"), "cuModuleGetFunction(xs_resident)");
+  cu_check(d.getfn(&h.f_reduce, h.mod, "xs_obs_reduce"), "cuModuleGetFunction(xs_obs_reduce)");
+  if (h.rp.smem > 48 * 1024)
+    cu_check(d.setattr(h.f_resident, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, (int)h.rp.smem),
+             "cuFuncSetAttribute(max dynamic smem)");
+  CUDA_CHECK(cudaStreamCreateWithFlags(&h.stream, cudaStreamNonBlocking));
+  // dense transform matrices (per space dim, per component, fwd/inv)
+  const Problem& P = h.P;
+  std::vector<cd> all;
+  h.tmat_off.assign(4, 0);
+  for (int d = 0; d < P.D; ++d) {
+    h.tmat_off[d + 1] = (int)all.size();
+    int n = P.N[d];
+    if (n <= 1) continue;
+    for (int f = 0; f < P.F; ++f)
+      for (int dir = 0; dir < 2; ++dir) {
+        auto M = transform_matrix(P.type(d, f), dir == 1, n);
+        all.insert(all.end(), M.begin(), M.end());
+      }
+  }
+  if (all.empty()) all.push_back(0);
+  if (h.fp64) {
+    h.d_tmat.ensure(all.size() * 16);
+    CUDA_CHECK(cudaMemcpy(h.d_tmat.p, all.data(), all.size() * 16, cudaMemcpyHostToDevice));
+  } else {
+    std::vector<float> f32(all.size() * 2);
+    for (size_t i = 0; i < all.size(); ++i) {
+      f32[2 * i] = (float)all[i].real();
+      f32[2 * i + 1] = (float)all[i].imag();
+    }
+    h.d_tmat.ensure(f32.size() * 4);
+    CUDA_CHECK(cudaMemcpy(h.d_tmat.p, f32.data(), f32.size() * 4, cudaMemcpyHostToDevice));
+  }
+  h.d_status.ensure(sizeof(int));
+  h.loaded = true;
+}
+
+double pass_dtr(const Problem& P, int nc) {
+  return (P.p.checks && nc != 2) ? P.dt / (2.0 * P.p.steps) : P.dt / P.p.steps;  // xensemble.m:41-45
+}
+
+const void* ensure_prop(xs_handle& h, int nc) {
+  const Problem& P = h.P;
+  int slot = nc == 2 ? 1 : 0;
+  double dtr = pass_dtr(P, nc);
+  if (!P.has_linear) {
+    h.d_prop[slot].ensure(16);
+    return h.d_prop[slot].p;
+  }
+  if (h.prop_dtr[slot] == dtr) return h.d_prop[slot].p;
+  double dt = dtr / P.p.ipsteps;  // xpropfactor.m:28
+  std::vector<cd> pr(P.L.size());
+  for (size_t i = 0; i < P.L.size(); ++i) pr[i] = std::exp(P.L[i] * dt);  // xpropfactor.m:39
+  h.d_prop[slot].ensure(pr.size() * 16);
+  CUDA_CHECK(cudaMemcpy(h.d_prop[slot].p, pr.data(), pr.size() * 16, cudaMemcpyHostToDevice));
+  h.prop_dtr[slot] = dtr;
+  return h.d_prop[slot].p;
+}
+
+struct PathArgsHost {
+  int ntraj, ens1, block0, nc, checks, npoints, steps, seq;
+  unsigned seed;
+  int pad0;
+  double wscale, vscale, dtr, t0;
+  const void* prop;
+  const void* tmat;
+  int tmat_off[4];
+  const void* a_in;
+  void* a_out;
+  void* obs;
+  int* status;
+};
+
+size_t av_stride(const Problem& P) { return (size_t)P.nout_site * P.NS + P.nout_scalar; }
+
+size_t av_doubles_per_block(const Problem& P) {
+  size_t n = 0;
+  for (auto& o : P.obs) n += (size_t)2 * o.lines * P.p.points[0] * (o.spatial ? P.NS : 1);
+  return n;
+}
+
+// Launch the resident path; av_dev receives [nblocks][npoints][stride] complex.
+void launch_resident(xs_handle& h, int first_block, int nblocks, int nc, const void* a_in_dev, void* av_dev,
+                     void* a_out_dev, cudaStream_t st) {
+  const Problem& P = h.P;
+  const int total = nblocks * P.E1;
+  const int G = h.rp.G;
+  const int nctas = total / G;
+  const size_t stride = av_stride(P);
+  const int npts = P.p.points[0];
+  h.d_obs.ensure(std::max<size_t>(1, (size_t)npts * nctas * stride) * 16);
+  PathArgsHost a{};
+  a.ntraj = total;
+  a.ens1 = P.E1;
+  a.block0 = first_block;
+  a.nc = nc;
+  a.checks = P.p.checks;
+  a.npoints = npts;
+  a.steps = P.p.steps;
+  a.seq = 0;
+  a.seed = (unsigned)(P.p.seed & 0xffffffffu);
+  a.wscale = std::sqrt(P.nscale * P.noisefactor);  // xnoise.m:32
+  a.vscale = std::sqrt(P.noisefactor);              // xrandom.m:23
+  a.dtr = pass_dtr(P, nc);
+  a.t0 = P.p.origins[0];
+  a.prop = ensure_prop(h, nc);
+  a.tmat = h.d_tmat.p;
+  for (int i = 0; i < 4; ++i) a.tmat_off[i] = h.tmat_off[i];
+  a.a_in = a_in_dev;
+  a.a_out = a_out_dev;
+  a.obs = h.d_obs.p;
+  a.status = (int*)h.d_status.p;
+  void* params[] = {&a};
+  cu_check(driver().launch(h.f_resident, nctas, 1, 1, h.rp.threads, 1, 1, (unsigned)h.rp.smem, (CUstream)st, params,
+                           nullptr),
+           "launch xs_resident");
+  if (stride > 0) {
+    const void* part = h.d_obs.p;
+    int ctas_per_block = P.E1 / G;
+    int strd = (int)stride;
+    double inv = 1.0 / P.E1;
+    void* rparams[] = {&part, &av_dev, (void*)&npts, (void*)&nctas, &ctas_per_block, &strd, &inv};
+    unsigned gx = (unsigned)((stride + 127) / 128);
+    cu_check(driver().launch(h.f_reduce, gx, (unsigned)npts, (unsigned)nblocks, 128, 1, 1, 0, (CUstream)st, rparams,
+                             nullptr),
+             "launch xs_obs_reduce");
+  }
+}
+
+// device [b][n][k] -> host MATLAB av{o} [lines, time, space] per block per observable
+void scatter_av(const Problem& P, const std::vector<double>& dev, int nblocks, double* out) {
+  const size_t stride = av_stride(P);
+  const int npts = P.p.points[0];
+  size_t o_off = 0;
+  size_t per_block = av_doubles_per_block(P);
+  for (int b = 0; b < nblocks; ++b) {
+    double* ob = out + (size_t)b * per_block;
+    o_off = 0;
+    for (auto& o : P.obs) {
+      size_t ns = o.spatial ? P.NS : 1;
+      for (int n = 0; n < npts; ++n)
+        for (size_t s = 0; s < ns; ++s)
+          for (int l = 0; l < o.lines; ++l) {
+            size_t k = o.spatial ? (size_t)(o.out_off + l) * P.NS + s : (size_t)P.nout_site * P.NS + o.out_off + l;
+            size_t src = (((size_t)b * npts + n) * stride + k) * 2;
+            size_t dst = o_off + ((size_t)l + (size_t)o.lines * ((size_t)n + (size_t)npts * s)) * 2;
+            ob[dst] = dev[src];
+            ob[dst + 1] = dev[src + 1];
+          }
+      o_off += (size_t)2 * o.lines * npts * ns;
+    }
+  }
+}
+
+template <class F>
+xs_status guard(F&& f) {
+  try {
+    return f();
+  } catch (const XsError& e) {
+    g_err = e.msg;
+    return e.code;
+  } catch (const xs::GrammarError& e) {
+    g_err = std::string("grammar: ") + e.what();
+    return XS_ERR_GRAMMAR;
+  } catch (const std::bad_alloc&) {
+    g_err = "host out of memory";
+    return XS_ERR_ARG;
+  } catch (const std::exception& e) {
+    g_err = e.what();
+    return XS_ERR_ARG;
+  }
+}
+
+void create_impl(const xs_problem* prob, xs_handle* h) {
+  setup_problem(prob, h->P);
+  h->fp64 = prob->precision != XS_PREC_FP32;
+  if (prob->path_kind == 2) raise(XS_ERR_UNSUPPORTED, "streaming path is not available for this problem");
+  h->kind = 1;
+  build_source(*h);
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+XS_API const char* xs_version(void) { return "xspde_b200 0.1 (sm_100a, NVRTC)"; }
+
+XS_API size_t xs_last_error(char* buf, size_t n) {
+  if (buf && n) {
+    size_t m = std::min(n - 1, g_err.size());
+    memcpy(buf, g_err.data(), m);
+    buf[m] = 0;
+  }
+  return g_err.size();
+}
+
+XS_API xs_status xs_create(const xs_problem* prob, xs_handle** out) {
+  if (!out) return XS_ERR_ARG;
+  *out = nullptr;
+  return guard([&]() -> xs_status {
+    auto h = std::make_unique<xs_handle>();
+    create_impl(prob, h.get());
+    *out = h.release();
+    return XS_OK;
+  });
+}
+
+XS_API void xs_destroy(xs_handle* h) { delete h; }
+
+XS_API xs_status xs_compile_check(const xs_problem* prob, char* log, size_t n) {
+  return guard([&]() -> xs_status {
+    xs_handle h;
+    create_impl(prob, &h);
+    std::string lg;
+    nvrtc_compile(h.source, "xs_resident", &lg);
+    if (log && n) {
+      size_t m = std::min(n - 1, lg.size());
+      memcpy(log, lg.data(), m);
+      log[m] = 0;
+    }
+    return XS_OK;
+  });
+}
+
+XS_API xs_status xs_observe_info(const xs_handle* h, int o, int* lines, int* spatial) {
+  if (!h || o < 0 || o >= (int)h->P.obs.size()) {
+    g_err = "bad handle or observable index";
+    return XS_ERR_ARG;
+  }
+  if (lines) *lines = h->P.obs[o].lines;
+  if (spatial) *spatial = h->P.obs[o].spatial ? 1 : 0;
+  return XS_OK;
+}
+
+XS_API size_t xs_av_doubles_per_block(const xs_handle* h) { return h ? av_doubles_per_block(h->P) : 0; }
+
+XS_API xs_status xs_run_path(xs_handle* h, int first_block, int nblocks, int nc, const double* a_in, double* av_out,
+                             double* a_out) {
+  return guard([&]() -> xs_status {
+    if (!h || nblocks < 1 || first_block < 0 || (nc != 1 && nc != 2)) raise(XS_ERR_ARG, "bad arguments to xs_run_path");
+    if (nc == 2 && !h->P.p.checks) raise(XS_ERR_ARG, "coarse pass requested without checks");
+    load_module(*h);
+    const Problem& P = h->P;
+    const size_t ntraj = (size_t)nblocks * P.E1;
+    const size_t fbytes = ntraj * P.F * P.NS * 16;
+    const void* din = nullptr;
+    void* dout = nullptr;
+    if (a_in) {
+      // host [F, space, ens] -> device [e][f][s] (identical when F == 1)
+      h->d_ain.ensure(fbytes);
+      if (P.F == 1) {
+        CUDA_CHECK(cudaMemcpyAsync(h->d_ain.p, a_in, fbytes, cudaMemcpyHostToDevice, h->stream));
+      } else {
+        std::vector<double> tmp(ntraj * P.F * P.NS * 2);
+        for (size_t e = 0; e < ntraj; ++e)
+          for (int f = 0; f < P.F; ++f)
+            for (int s = 0; s < P.NS; ++s) {
+              size_t src = (f + (size_t)P.F * (s + (size_t)P.NS * e)) * 2, dst = ((e * P.F + f) * P.NS + s) * 2;
+              tmp[dst] = a_in[src];
+              tmp[dst + 1] = a_in[src + 1];
+            }
+        CUDA_CHECK(cudaMemcpy(h->d_ain.p, tmp.data(), fbytes, cudaMemcpyHostToDevice));
+      }
+      din = h->d_ain.p;
+    }
+    if (a_out) {
+      h->d_aout.ensure(fbytes);
+      dout = h->d_aout.p;
+    }
+    const size_t stride = av_stride(P);
+    const size_t avd = (size_t)nblocks * P.p.points[0] * stride * 2;
+    h->d_av.ensure(std::max<size_t>(avd, 1) * 8);
+    CUDA_CHECK(cudaMemsetAsync(h->d_status.p, 0, sizeof(int), h->stream));
+    launch_resident(*h, first_block, nblocks, nc, din, h->d_av.p, dout, h->stream);
+    std::vector<double> av(avd);
+    if (avd) CUDA_CHECK(cudaMemcpyAsync(av.data(), h->d_av.p, avd * 8, cudaMemcpyDeviceToHost, h->stream));
+    int status = 0;
+    CUDA_CHECK(cudaMemcpyAsync(&status, h->d_status.p, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    if (a_out) {
+      if (P.F == 1) {
+        CUDA_CHECK(cudaMemcpyAsync(a_out, dout, fbytes, cudaMemcpyDeviceToHost, h->stream));
+        CUDA_CHECK(cudaStreamSynchronize(h->stream));
+      } else {
+        std::vector<double> tmp(ntraj * P.F * P.NS * 2);
+        CUDA_CHECK(cudaMemcpyAsync(tmp.data(), dout, fbytes, cudaMemcpyDeviceToHost, h->stream));
+        CUDA_CHECK(cudaStreamSynchronize(h->stream));
+        for (size_t e = 0; e < ntraj; ++e)
+          for (int f = 0; f < P.F; ++f)
+            for (int s = 0; s < P.NS; ++s) {
+              size_t dst = (f + (size_t)P.F * (s + (size_t)P.NS * e)) * 2, src = ((e * P.F + f) * P.NS + s) * 2;
+              a_out[dst] = tmp[src];
+              a_out[dst + 1] = tmp[src + 1];
+            }
+      }
+    }
+    CUDA_CHECK(cudaStreamSynchronize(h->stream));
+    if (av_out) scatter_av(P, av, nblocks, av_out);
+    if (status & 2) raise(XS_ERR_SHAPE, "kernel refused a launch whose shared-memory layout or grid did not match");
+    if (status & 1) raise(XS_ERR_NAN, "a trajectory became non-finite (NaN/Inf) during the path");
+    return XS_OK;
+  });
+}
+
+XS_API xs_status xs_run_path_device(xs_handle* h, int first_block, int nblocks, int nc, const double* a_in_dev,
+                                    double* av_dev, double* a_out_dev, void* stream) {
+  return guard([&]() -> xs_status {
+    if (!h || nblocks < 1 || first_block < 0 || (nc != 1 && nc != 2) || !av_dev)
+      raise(XS_ERR_ARG, "bad arguments to xs_run_path_device");
+    load_module(*h);
+    cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
+    CUDA_CHECK(cudaMemsetAsync(h->d_status.p, 0, sizeof(int), st));
+    launch_resident(*h, first_block, nblocks, nc, a_in_dev, av_dev, a_out_dev, st);
+    return XS_OK;
+  });
+}
+
+XS_API xs_status xs_sync(xs_handle* h) {
+  return guard([&]() -> xs_status {
+    if (!h || !h->loaded) raise(XS_ERR_ARG, "handle has not run");
+    CUDA_CHECK(cudaDeviceSynchronize());
+    int status = 0;
+    CUDA_CHECK(cudaMemcpy(&status, h->d_status.p, sizeof(int), cudaMemcpyDeviceToHost));
+    if (status & 2) raise(XS_ERR_SHAPE, "kernel refused a launch whose shared-memory layout or grid did not match");
+    if (status & 1) raise(XS_ERR_NAN, "a trajectory became non-finite (NaN/Inf) during the path");
+    return XS_OK;
+  });
+}
+
+XS_API xs_status xs_noise(xs_handle* h, int block, int draw, double scale, double* w_out) {
+  (void)h; (void)block; (void)draw; (void)scale; (void)w_out;
+  g_err = "xs_noise: not available yet";
+  return XS_ERR_UNSUPPORTED;
+}
+
+XS_API xs_status xs_random(xs_handle* h, int block, double* v_out) {
+  (void)h; (void)block; (void)v_out;
+  g_err = "xs_random: not available yet";
+  return XS_ERR_UNSUPPORTED;
+}
+
+XS_API xs_status xs_step(xs_handle* h, double* a_inout, const double* w, double t, double dtr) {
+  (void)h; (void)a_inout; (void)w; (void)t; (void)dtr;
+  g_err = "xs_step: not available yet";
+  return XS_ERR_UNSUPPORTED;
+}

@@ -1,0 +1,420 @@
+"""Host mirror of xSPDE's control layer over the GPU ensemble path.
+
+``xsim(p, ...)`` and ``xspde(p, ...)`` take the reference's input struct (a dict
+with the same field names: dimensions, fields, points, ranges, origins, steps,
+checks, ensembles, noises, inrandoms, method, iterations, ipsteps, order, seed,
+boundaries, linear, deriv, initial, observe, output, compare, axes ...) and
+return ``(error, data, input)`` as Simulator/xsim.m:1 does.  Functions that run
+on the device -- ``deriv`` (alias ``da``), ``initial``, ``observe``, ``linear``
+-- are given as the text of MATLAB anonymous functions; host-side functions
+-- ``output``, ``compare`` -- are Python callables, as in the reference where
+they run after the ensemble loop (Simulator/xensemble.m:88, xsim.m:170).
+
+The ensemble loop (Simulator/xensemble.m:25-108) calls the GPU's p.path
+replacement once per check pass for a group of blocks, then accumulates
+block moments and the step-error/sampling-error columns exactly as the
+reference does.  There is no CPU fallback: a problem the device path cannot
+run raises ``XsError``.
+"""
+import ctypes
+import math
+import time
+
+import numpy as np
+
+from . import _lib
+
+__all__ = ["xpreferences", "xsim", "xspde", "GpuPath", "Struct"]
+
+
+class Struct(dict):
+    """Attribute-access dict standing in for a MATLAB struct."""
+
+    def __getattr__(self, k):
+        try:
+            return self[k]
+        except KeyError as exc:
+            raise AttributeError(k) from exc
+
+    def __setattr__(self, k, v):
+        self[k] = v
+
+    def copy(self):
+        return Struct(self)
+
+
+_METHOD_ALIASES = {"xRK4": "RK4", "xMP": "MP", "xEuler": "Euler", "xRK2": "RK2", "xImplicit": "Implicit"}
+
+
+def _vec(v, n, fill):
+    v = [] if v is None else list(np.atleast_1d(v))
+    return v + [fill] * (n - len(v))
+
+
+def _fsize(a):
+    """MATLAB size: trailing singletons dropped (at least two entries)."""
+    s = list(np.shape(a))
+    while len(s) > 2 and s[-1] == 1:
+        s.pop()
+    return s + [1] * (2 - len(s))
+
+
+def xpreferences(inputs):
+    """Defaults of Simulator/xpreferences.m:11-414 for the fields this path uses."""
+    if isinstance(inputs, dict):
+        inputs = [inputs]
+    out = []
+    origin = 0.0
+    for s, pin in enumerate(inputs):
+        p = Struct(pin)
+        if "da" in p and "deriv" not in p:
+            p.deriv = p.da
+        if "step" in p and "method" not in p:
+            p.method = p.step
+        p.ensembles = [int(x) for x in _vec(p.get("ensembles"), 3, 1)]
+        p.tol = float(p.get("tol", 1e-20))
+        p.dimensions = int(p.get("dimensions", 1))
+        nd = max(1, p.dimensions)
+        p.fields = int(np.atleast_1d(p.get("fields", 1))[0])
+        dflt = [51] + [35] * (nd - 1)
+        pts = [int(x) for x in np.atleast_1d(p.get("points", dflt))]
+        pts = pts + dflt[len(pts):]
+        chk = [int(x) for x in np.atleast_1d(p.get("checks", [1] + [0] * (nd - 1)))]
+        p.checks = chk + [0] * (nd - len(chk))
+        if s > 0:
+            p.checks = out[0].checks
+        if any(p.checks[1:]):
+            raise _lib.XsError(-9, "space-step checks (checks(2:end)) are not supported")
+        p.iterations = int(p.get("iterations", 4))
+        nz = p.get("noises", None)
+        p.noises = int(np.atleast_1d(nz)[0]) if nz is not None else p.fields
+        rz = p.get("inrandoms", None)
+        p.inrandoms = int(np.atleast_1d(rz)[0]) if rz is not None else p.noises
+        p.ranges = [float(x) for x in _vec(p.get("ranges", [10.0] * nd), nd, 10.0)]
+        st = [int(x) for x in np.atleast_1d(p.get("steps", [1]))]
+        p.steps = st + [1] * (nd - len(st))
+        org = [origin] + [-r / 2 for r in p.ranges[1:]]
+        og = [float(x) for x in np.atleast_1d(p.get("origins", org))]
+        p.origins = og + org[len(og):]
+        for d in range(1, nd):
+            pts[d] = 1 + (pts[d] - 1) * p.steps[d]
+        p.points = pts
+        p.seed = int(p.get("seed", 0))
+        m = p.get("method", None)
+        if m is None:
+            m = "RK4" if int(np.prod(p.ensembles)) == 1 else "MP"
+        if callable(m):
+            m = m.__name__
+        p.method = _METHOD_ALIASES.get(m, m)
+        if p.method not in _lib.METHODS:
+            raise _lib.XsError(-9, "method %r is not available on the device path" % (m,))
+        p.ipsteps = int(p.get("ipsteps", 1 if p.method in ("Euler", "Implicit", "RK2") else 2))
+        p.order = int(p.get("order", 0))
+        p.relerr = int(p.get("relerr", 1))
+        p.precision = str(p.get("precision", "fp64")).lower()
+        for key in ("deriv", "initial", "linear"):
+            v = p.get(key, None)
+            if v is not None and not isinstance(v, str):
+                raise _lib.XsError(-2, "p.%s must be the text of a MATLAB anonymous function" % key)
+        obs = p.get("observe", None)
+        if obs is None:
+            obs = ["@(a,p) a"]
+        elif isinstance(obs, str):
+            obs = [obs]
+        for o in obs:
+            if not isinstance(o, str):
+                raise _lib.XsError(-2, "p.observe entries must be MATLAB anonymous-function text")
+        p.observe = list(obs)
+        outs = p.get("output", None)
+        outs = [outs] if callable(outs) else list(outs or [])
+        outs += [None] * (len(p.observe) - len(outs))
+        p.output = [o if o is not None else (lambda o, p, n=n: o[n]) for n, o in enumerate(outs)]
+        cmp = p.get("compare", None)
+        cmp = [cmp] if callable(cmp) else list(cmp or [])
+        p.compare = cmp + [None] * (len(p.output) - len(cmp))
+        cut = p.get("cutoff", -1e20)
+        p.cutoffs = list(p.get("cutoffs", [])) + [cut] * len(p.output)
+        ax = list(p.get("axes", None) or [])
+        ax += [None] * (len(p.output) - len(ax))
+        p.axes = [list(a) + [0] * (nd + 10 - len(a)) if a is not None else [0] * (nd + 10) for a in ax]
+        p.params = dict(p.get("params", {}))
+        bnd = p.get("boundaries", None)
+        if bnd is not None:
+            b = []
+            for d in range(1, nd):
+                bd = bnd[d] if d < len(bnd) and bnd[d] is not None else None
+                b.append(np.zeros((p.fields, 2), int) if bd is None else np.atleast_2d(np.asarray(bd, int)))
+            p.boundaries = b if any(np.any(x != 0) for x in b) else None
+        else:
+            p.boundaries = None
+        p.dt = p.ranges[0] / max(1, p.points[0] - 1)
+        p.nchk = 1 + sum(p.checks)
+        p.dx = [p.ranges[d] / max(1, p.points[d] - 1) if p.points[d] > 1 else 1.0 for d in range(nd)]
+        p.dk = [2 * math.pi / (p.points[d] * p.dx[d]) for d in range(nd)]
+        p.dk[0] /= p.steps[0]
+        p.space = p.points[1:]
+        p.nspace = int(np.prod(p.space)) if p.space else 1
+        p.xc = [p.origins[d] + np.arange(p.points[d]) * p.dx[d] for d in range(nd)]
+        p.kc = [(np.arange(p.points[d]) - p.points[d] // 2) * p.dk[d] for d in range(nd)]
+        p.kc[0] = (np.arange(p.points[0]) - p.points[0] // 2) * (2 * math.pi / (p.ranges[0] + p.dt))
+        out.append(p)
+        origin = p.origins[0] + p.ranges[0]
+    return out
+
+
+class GpuPath:
+    """One compiled device problem: the p.path/p.method replacements of one input."""
+
+    def __init__(self, p, path_kind=0):
+        L = _lib.lib()
+        pr = _lib.XsProblem()
+        pr.dimensions = p.dimensions
+        pr.fields = p.fields
+        pr.noises = p.noises
+        pr.inrandoms = p.inrandoms
+        for d in range(len(p.points)):
+            pr.points[d] = p.points[d]
+            pr.ranges[d] = p.ranges[d]
+            pr.origins[d] = p.origins[d]
+        pr.steps = p.steps[0]
+        pr.checks = p.checks[0]
+        for i in range(3):
+            pr.ensembles[i] = p.ensembles[i]
+        pr.method = _lib.METHODS[p.method]
+        pr.iterations = p.iterations
+        pr.ipsteps = p.ipsteps
+        pr.precision = 1 if p.precision in ("fp32", "single", "float32") else 0
+        pr.seed = p.seed & 0xFFFFFFFFFFFFFFFF
+        keep = []
+        if p.boundaries is not None:
+            flat = np.concatenate([np.asarray(b, np.int32).reshape(-1) for b in p.boundaries]).astype(np.int32)
+            arr = (ctypes.c_int * flat.size)(*flat.tolist())
+            keep.append(arr)
+            pr.boundaries = arr
+        pr.deriv = (p.get("deriv") or "@(a,w,p) 0*a").encode()
+        pr.initial = (p.get("initial") or "@(v,p) 0").encode()
+        pr.linear = (p.get("linear") or "").encode()
+        obs = (ctypes.c_char_p * len(p.observe))(*[o.encode() for o in p.observe])
+        keep.append(obs)
+        pr.nobserve = len(p.observe)
+        pr.observe = obs
+        names = list(p.params.keys())
+        if names:
+            nm = (ctypes.c_char_p * len(names))(*[n.encode() for n in names])
+            vals = (ctypes.c_double * len(names))(*[float(p.params[n]) for n in names])
+            keep += [nm, vals]
+            pr.nparams = len(names)
+            pr.param_names = nm
+            pr.param_values = vals
+        pr.path_kind = path_kind
+        h = ctypes.c_void_p()
+        _lib.check(L.xs_create(ctypes.byref(pr), ctypes.byref(h)))
+        self._keep = keep
+        self.h = h
+        self.p = p
+        self.obs = []
+        for o in range(len(p.observe)):
+            ln, sp = ctypes.c_int(), ctypes.c_int()
+            _lib.check(L.xs_observe_info(h, o, ctypes.byref(ln), ctypes.byref(sp)))
+            self.obs.append((ln.value, bool(sp.value)))
+        self.per_block = L.xs_av_doubles_per_block(h)
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h is not None and h.value:
+            try:
+                _lib.lib().xs_destroy(h)
+            except Exception:
+                pass
+            self.h = None
+
+    def av_shapes(self):
+        P = self.p
+        return [(ln, P.points[0]) + (tuple(P.space) if sp else ()) for ln, sp in self.obs]
+
+    def run_path(self, first_block, nblocks, nc, a_in=None, a_out=False):
+        """p.path for blocks [first_block, first_block+nblocks): returns
+        (av, a) with av[b][o] complex arrays of shape av_shapes()[o]."""
+        P = self.p
+        buf = np.empty(nblocks * self.per_block, dtype=np.float64)
+        ain = None
+        if a_in is not None:
+            ain = np.asfortranarray(np.asarray(a_in, dtype=np.complex128))
+        aout = None
+        if a_out:
+            aout = np.empty([P.fields] + list(P.space) + [P.ensembles[0] * nblocks], dtype=np.complex128, order="F")
+        _lib.check(_lib.lib().xs_run_path(self.h, first_block, nblocks, nc,
+                                          ain.ctypes.data if ain is not None else None,
+                                          buf.ctypes.data, aout.ctypes.data if aout is not None else None))
+        cbuf = buf.view(np.complex128)
+        av, pos = [], 0
+        for b in range(nblocks):
+            row = []
+            for shp in self.av_shapes():
+                n = int(np.prod(shp))
+                row.append(np.reshape(cbuf[pos:pos + n], shp, order="F"))
+                pos += n
+            av.append(row)
+        return av, aout
+
+
+def _xcompress(n, data, p, xk):
+    """Axis reduction of an output array (Applications/SPDE/xcompress.m:142-194)."""
+    axes = list(p.axes[n])
+    x = list(xk)
+    d = len(p.gpoints[n]) - 2
+    rank = data.ndim
+    shp = list(data.shape) + [1] * d
+    mid = [1 + v // 2 for v in shp]
+    for ax in range(d):
+        ind = axes[ax]
+        if np.size(x[ax]) > 1:
+            if np.size(ind) == 1:
+                ind = int(np.atleast_1d(ind)[0])
+                ind = (list(range(1, shp[ax + 1] + 1)) if ind == 0 else [mid[ax + 1]] if ind == -1
+                       else [shp[ax + 1]] if ind == -2 else [ind])
+            ind = [int(i) for i in np.atleast_1d(ind)]
+            if shp[ax + 1] > len(ind):
+                data = np.reshape(data, [int(np.prod(shp[:ax + 1])), shp[ax + 1], -1], order="F")[:, [i - 1 for i in ind], :]
+                shp[ax + 1] = len(ind)
+            else:
+                ind = ind[:shp[ax + 1]]
+            x[ax] = np.asarray(x[ax])[[i - 1 for i in ind]]
+    return np.reshape(data, shp[:rank], order="F"), x
+
+
+def _grid(xk):
+    """Output-grid broadcast coordinates for compare functions (Applications/SPDE/xgrid.m:320-327)."""
+    q = Struct()
+    d = len(xk)
+    r = []
+    for j in range(d):
+        sh = [1] * (d + 1)
+        sh[j + 1] = len(xk[j])
+        r.append(np.asarray(xk[j], dtype=float).reshape(sh))
+    r += [None] * (4 - len(r))
+    q.r = r
+    q.t, q.x, q.y, q.z = r[0], r[1], r[2], r[3]
+    return q
+
+
+def _ensembles(inp, paths):
+    """Block loop, check passes and moments (Simulator/xensemble.m:12-108) with
+    all blocks of a pass integrated by one device call."""
+    p1 = inp[0]
+    nb = p1.ensembles[1] * p1.ensembles[2]
+    m = p1.nchk
+    m1 = max(3, m + 1)
+    inv = 1.0 / nb
+    data = []
+    for s, p in enumerate(inp):
+        data.append([None] * len(p.output))
+    D = {}
+    chunk = max(1, min(nb, int(2 ** 27 // max(1, paths[0].per_block * 8))))
+    for b0 in range(0, nb, chunk):
+        nbk = min(chunk, nb - b0)
+        prev = None
+        for nc in range(1, p1.nchk + 1):
+            prev = None
+            for s, p in enumerate(inp):
+                a_in = prev if s > 0 else None
+                av, prev = paths[s].run_path(b0, nbk, nc, a_in=a_in, a_out=(s + 1 < len(inp)))
+                for b in range(nbk):
+                    for o in range(len(p.output)):
+                        Dv = np.real(np.asarray(p.output[o](av[b], p)))
+                        D[(s, b, nc, o)] = np.reshape(Dv, -1, order="F")
+        for s, p in enumerate(inp):
+            for b in range(nbk):
+                for o in range(len(p.output)):
+                    if p1.checks[0] and p.order > 0:
+                        d1, d2 = D[(s, b, 1, o)], D[(s, b, 2, o)]
+                        D[(s, b, 2, o)] = d1
+                        D[(s, b, 1, o)] = d1 + (d1 - d2) / (2 ** p.order - 1.0)
+                    if data[s][o] is None:
+                        data[s][o] = np.zeros((D[(s, b, 1, o)].size, m1))
+                    for n1 in range(1, m + 1):
+                        data[s][o][:, n1 - 1] += D[(s, b, n1, o)] * inv
+                    data[s][o][:, m1 - 1] += D[(s, b, 1, o)] ** 2 * inv
+        D.clear()
+    return data
+
+
+def xsim(*inputs, path_kind=0):
+    """Simulate and return (error, data, input) (Simulator/xsim.m:77-263).
+
+    error: [total RMS, step errors..., sampling, difference, chi^2/k, time]
+    data[s][o]: columns mean, step error, sampling error, comparison."""
+    t0 = time.perf_counter()
+    if len(inputs) == 1 and isinstance(inputs[0], (list, tuple)):
+        inputs = inputs[0]
+    inp = xpreferences(list(inputs))
+    paths = [GpuPath(p, path_kind) for p in inp]
+    for s, p in enumerate(inp):
+        if s > 0 and "transfer" in p and p.transfer is not None:
+            raise _lib.XsError(-9, "p.transfer functions are not supported on the device path")
+        shapes = paths[s].av_shapes()
+        O = [np.zeros(x) for x in shapes]
+        p.gpoints = []
+        for o in range(len(p.output)):
+            g = _fsize(p.output[o](O, p))
+            p.gpoints.append(g + [max(3, 1 + p.nchk)])
+        p.xk = [[p.xc[0]] + [p.xc[d] for d in range(1, len(p.points))] for _ in p.output]
+    data = _ensembles(inp, paths)
+    p = inp[0]
+    ne = p.ensembles[1] * p.ensembles[2]
+    sx = max(3, 1 + p.nchk)
+    rows = []
+    for s, p in enumerate(inp):
+        for n in range(len(p.output)):
+            d = np.reshape(np.real(data[s][n]), p.gpoints[n], order="F")
+            d, xkn = _xcompress(n, d, p, p.xk[n])
+            gp = list(d.shape[:-1])
+            nd_ = int(np.prod(gp))
+            d = np.reshape(d, [nd_, sx], order="F")
+            er = np.zeros(max(6, p.nchk + 4))
+            mx = np.max(np.abs(d[:, 0])) ** 2
+            if not (p.relerr and mx > p.tol):
+                mx = 1.0
+            d[:, sx - 1] = np.abs(np.sqrt((d[:, sx - 1] - d[:, 0] ** 2 + 0j) / (ne - 1))) if ne > 1 else 0.0
+            for nc in range(2, p.nchk + 1):
+                d[:, nc - 1] = np.abs(d[:, nc - 1] - d[:, 0])
+                er[nc - 1] = np.mean(d[:, nc - 1] ** 2)
+            esum = np.sum(d[:, 1:sx] ** 2, axis=1) + 1e-20
+            ept = (esum > p.tol) & (np.abs(d[:, 0]) > p.cutoffs[n])
+            if p.compare[n] is not None:
+                dif = np.asarray(p.compare[n](_grid(xkn)), dtype=float)
+                if dif.ndim < len(gp):
+                    dif = dif.reshape(dif.shape + (1,) * (len(gp) - dif.ndim))
+                while dif.ndim > len(gp) and dif.shape[-1] == 1:
+                    dif = dif[..., 0]
+                dif = np.reshape(np.broadcast_to(dif, gp), [nd_, 1], order="F")
+                d = np.concatenate([d, dif], axis=1)
+                ept = ept & (np.abs(d[:, sx]) > p.cutoffs[n])
+                mx = np.max(np.abs(d[:, sx]) ** 2)
+                if not (p.relerr and mx > p.tol):
+                    mx = 1.0
+                dif2 = (d[:, 0] - d[:, sx]) ** 2
+                er[sx] = np.mean(dif2) / mx
+                if ne > 1:
+                    er[sx + 1] = np.sum(ept * (dif2 / esum))
+                er[sx + 2] = np.sum(ept)
+            er[1:p.nchk] /= mx
+            er[sx - 1] = np.mean(d[:, sx - 1] ** 2) / mx
+            er[0] = np.sum(er[1:sx + 1]) / (1e-99 + np.sum(er[1:sx + 1] > 0))
+            er[0:sx + 1] = np.sqrt(er[0:sx + 1])
+            data[s][n] = d
+            rows.append(er)
+    er = np.array(rows)
+    error = np.zeros(max(6, sx + 4))
+    for c in range(1, sx + 1):
+        error[c] = math.sqrt(np.sum(er[:, c] ** 2) / (1e-99 + np.sum(er[:, c] > p.tol)))
+    error[0] = math.sqrt(np.sum(error[1:sx + 1] ** 2) / (1e-99 + np.sum(error[1:sx + 1] > p.tol)))
+    error[sx + 1:sx + 3] = np.sum(er[:, sx + 1:sx + 3], axis=0)
+    error[sx + 1] /= 1e-20 + error[sx + 2]
+    error[sx + 2] = time.perf_counter() - t0
+    return error, data, inp
+
+
+def xspde(*inputs, **kw):
+    """xSPDE control function without graphics (Simulator/xspde.m:8)."""
+    return xsim(*inputs, **kw)
