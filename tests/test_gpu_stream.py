@@ -1,0 +1,69 @@
+"""GPU parity of the streaming (HBM row/column pass) path against the oracle.
+
+A 64x64 periodic lattice is forced onto the streaming kernels (path_kind=2):
+the same x-row / y-column passes and FFT code that the 256x256 benchmark
+uses, at a size the oracle finishes in seconds.  FP64 tolerance 1e-10
+relative to max |av|; FP32 (FP64 propagator table, FP64 moments) 2e-4.
+"""
+import numpy as np
+import pytest
+
+from oracle import xspde_ref as X
+from tests.gpu_util import oracle_block_av, rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+def _case(checks, precision="fp64", points=(5, 64, 64), ens=(4, 2, 1), obs_int=True):
+    base = dict(dimensions=3, points=list(points), ranges=[0.2, 12.0, 10.0], steps=2, ensembles=list(ens), noises=2,
+                method="MP", checks=checks)
+    gobs = ["@(a,p) abs(a).^2", "@(a,p) real(a)"]
+    oobs = [lambda a, p: abs(a) ** 2, lambda a, p: np.real(a)]
+    if obs_int:
+        gobs.append("@(a,p) Int(abs(a).^2, p.dx, [0 0; -2 3; -1 2], p)")
+        oobs.append(lambda a, p: X.Int(abs(a) ** 2, p.dx, [[0, 0], [-2, 3], [-1, 2]], p))
+    g = dict(base, precision=precision,
+             deriv="@(a,w,p) (1-abs(a).^2).*a - 0.5i*abs(a).^2.*a + 0.05*(w(1,:)+1i*w(2,:))/sqrt(2)",
+             initial="@(v,p) 1 + 0.1*(v(1,:)+1i*v(2,:))/sqrt(2) + 0.2*exp(-p.x.^2-p.y.^2)",
+             linear="@(p) (1i+0.1)*(p.Dx.^2+p.Dy.^2)", observe=gobs)
+    o = dict(base, deriv=lambda a, w, p: (1 - abs(a) ** 2) * a - 0.5j * abs(a) ** 2 * a
+             + 0.05 * (w[0:1] + 1j * w[1:2]) / np.sqrt(2),
+             initial=lambda v, p: 1 + 0.1 * (v[0:1] + 1j * v[1:2]) / np.sqrt(2) + 0.2 * np.exp(-p.x ** 2 - p.y ** 2),
+             linear=lambda p: (1j + 0.1) * (p.Dx ** 2 + p.Dy ** 2), observe=oobs)
+    return g, o
+
+
+def _run(g, blocks, nc, a_in=None, a_out=False):
+    from xspde_matlab_b200 import GpuPath, xpreferences
+    path = GpuPath(xpreferences([g])[0], path_kind=2)
+    return path.run_path(blocks[0], len(blocks), nc, a_in=a_in, a_out=a_out)
+
+
+@pytest.mark.parametrize("checks", [0, 1])
+def test_stream_fp64_matches_oracle(checks):
+    g, o = _case(checks)
+    for nc in ([1, 2] if checks else [1]):
+        av_g, _ = _run(g, [0, 1], nc)
+        for i, b in enumerate([0, 1]):
+            av_o, _ = oracle_block_av(o, b, nc)
+            for k in range(len(av_o)):
+                e = rel_err(av_g[i][k].reshape(-1, order="F"), av_o[k].reshape(-1, order="F"))
+                assert e < 1e-10, (nc, b, k, e)
+
+
+def test_stream_fp32_bound():
+    g, o = _case(1, precision="fp32")
+    for nc in (1, 2):
+        av_g, _ = _run(g, [1], nc)
+        av_o, _ = oracle_block_av(o, 1, nc)
+        for k in range(len(av_o)):
+            e = rel_err(av_g[0][k].reshape(-1, order="F"), av_o[k].reshape(-1, order="F"))
+            assert e < 2e-4, (nc, k, e)
+
+
+def test_stream_final_field_and_rectangular_lattice():
+    g, o = _case(0, points=(4, 64, 256), ens=(2, 1, 1), obs_int=False)
+    av_o, b_o = oracle_block_av(o, 0, 1)
+    av_g, a_g = _run(g, [0], 1, a_out=True)
+    assert rel_err(a_g, b_o) < 1e-10
+    assert rel_err(av_g[0][0], av_o[0]) < 1e-10

@@ -1,1 +1,417 @@
-// streaming-path kernels (2D/3D lattices too large for one CTA)
+// Streaming-path kernels for 2D lattices whose field does not fit one CTA
+// (Simulator/xpath.m:137-194 with Applications/SDE/MP.m and the periodic
+// branch of Applications/SPDE/xprop.m / xtransform.m:149,164).
+//
+// Field layout in HBM: F[e][f][y][x], x fastest, complex `real`.  Between
+// passes the field is held with the x direction Fourier transformed
+// ("K state": kx, y).  One MP step (merged with its neighbour's half step):
+//   xs_s_pass   column pass: FFT_y, multiply by exp(L dtr/2)^m (FP64 table,
+//               m = 2 merges the previous step's second half with this step's
+//               first half), IFFT_y
+//   xs_x_nl     row pass: IFFT_x, midpoint iterations with the drift and
+//               Philox noise generated in registers, 2a - a0, FFT_x
+// Each pass reads and writes the field once: 4 N F s bytes per
+// trajectory-step.  Observables (xs_x_obs) read the field once per output
+// time and reduce over the trajectories of each block in a fixed order.
+//
+// 1D FFTs of length NX = RX*RX (and NY = RY*RY) use the four-step split:
+// thread t of a line holds elements t + R*j (j < R) in registers; DFT-R over
+// registers, twiddle W_N^(t k1), transpose through shared memory, DFT-R.
+// The output lands in the same thread/element layout (index t + R*k2).
+#pragma once
+
+struct XsStreamArgs {
+  int ntraj;      // trajectories in this launch
+  int ens1;       // trajectories per block
+  int block0;     // global index of the first block
+  int seq;        // sequence index (Philox counter)
+  u32 seed;
+  int draw0;      // Philox draw of this step
+  int draw1;      // >= 0: coarse pass, average draws draw0 and draw1 (xnoise.m:33-35)
+  int m;          // column pass: power of the half-step propagator (1 or 2)
+  int n;          // observation index
+  int npoints;
+  double wscale;  // sqrt(nscale * noisefactor)
+  double vscale;  // sqrt(noisefactor)
+  double dtr;     // step of this pass
+  double t;       // time at the start of this step (or of the observation)
+  cx* field;                 // [ntraj][F][NS]
+  const double2* prop1;      // [PC][NS] exp(L dtr/ipsteps), (ky, kx) order
+  const double2* prop2;      // [PC][NS] exp(2 L dtr/ipsteps)
+  const double2* a_in;       // [ntraj][F][NS] FP64 or null
+  double2* a_out;            // [ntraj][F][NS] FP64 or null
+  double2* av;               // [nblocks][npoints][XS_OBS_STRIDE]
+  double2* redpart;          // [ntraj][XS_NRG][XS_NRED] integrand sums per row group
+  int* status;
+};
+
+#define XS_RX XS_FFT_RX
+#define XS_RY XS_FFT_RY
+#define XS_NX XS_N1
+#define XS_NY XS_N2
+#define XS_XROWS (256 / XS_RX)          // rows per CTA in the row passes
+#define XS_TX (256 / XS_RY)             // columns per CTA in the column pass
+#define XS_OROWS XS_OBS_ROWS            // rows per CTA in the observation pass
+#define XS_NRG (XS_NY / XS_OROWS)       // row groups per trajectory
+
+extern __shared__ __align__(16) unsigned char xs_dsmem[];  // sizes set at launch
+template <int R> __device__ __forceinline__ void xs_dftR(cx (&v)[R]);
+
+__device__ __forceinline__ cx xs_cj(cx a) { return mkcx(a.re, -a.im); }
+
+// W_N^(t*k) for the four-step split, N = R*R: tw[t*R + k] = exp(-2 pi i t k / N)
+template <int R>
+__device__ __forceinline__ void xs_fill_twiddles(cx* tw) {
+  for (int i = threadIdx.x; i < R * R; i += blockDim.x) {
+    const int t = i / R, k = i % R;
+    double s, c;
+    sincospi(-2.0 * (double)(t * k) / (double)(R * R), &s, &c);
+    tw[i] = mkcx((real)c, (real)s);
+  }
+}
+
+// Forward DFT of N = R*R points held four-step style: thread t holds v[j] =
+// x[t + R*j].  `buf` is this line's (R x (R+1)) shared-memory scratch; `sync`
+// is the barrier that covers the threads of the line.  On return v[k2] =
+// X[t + R*k2].
+template <int R, class Sync>
+__device__ __forceinline__ void xs_fft4(cx (&v)[R], int t, const cx* __restrict__ tw, cx* buf, Sync sync) {
+  xs_dftR<R>(v);  // v[k1] = sum_j x[t + R j] W_R^(j k1)
+#pragma unroll
+  for (int k = 1; k < R; ++k) v[k] = v[k] * tw[t * R + k];
+#pragma unroll
+  for (int k = 0; k < R; ++k) buf[k * (R + 1) + t] = v[k];
+  sync();
+#pragma unroll
+  for (int n = 0; n < R; ++n) v[n] = buf[t * (R + 1) + n];
+  sync();
+  xs_dftR<R>(v);
+}
+
+template <int R, class Sync>
+__device__ __forceinline__ void xs_ifft4(cx (&v)[R], int t, const cx* __restrict__ tw, cx* buf, Sync sync) {
+#pragma unroll
+  for (int k = 0; k < R; ++k) v[k] = xs_cj(v[k]);
+  xs_fft4<R>(v, t, tw, buf, sync);
+  const real sc = (real)(1.0 / (double)(R * R));
+#pragma unroll
+  for (int k = 0; k < R; ++k) v[k] = mkcx(v[k].re * sc, -v[k].im * sc);
+}
+
+struct XsWarpSync {
+  __device__ __forceinline__ void operator()() const { __syncwarp(); }
+};
+struct XsBlockSync {
+  __device__ __forceinline__ void operator()() const { __syncthreads(); }
+};
+
+// ---- row passes -------------------------------------------------------------
+// Shared memory: twiddles (RX*RX) + per-row transpose scratch (RX*(RX+1)).
+#define XS_XSMEM (XS_RX * XS_RX + XS_XROWS * XS_RX * (XS_RX + 1))
+
+__device__ __forceinline__ void xs_row_coords(int y, int t, int j, real& x, real& yy) {
+  x = (real)(XS_O1 + XS_DX1 * (double)(t + XS_RX * j));
+  yy = (real)(XS_O2 + XS_DX2 * (double)y);
+}
+
+// MODE 0: initial field (expression or a_in) -> K state
+// MODE 1: one MP step in x space (K state in, K state out)
+// MODE 3: K state -> x-space a_out (FP64)
+template <int MODE>
+__device__ __forceinline__ void xs_xpass_body(const XsStreamArgs& A) {
+  // The grid covers ntraj*NY rows exactly; a CTA outside it leaves as a whole.
+  if ((size_t)(blockIdx.x + 1) * XS_XROWS > (size_t)A.ntraj * XS_NY) {
+    if (threadIdx.x == 0) atomicOr(A.status, 2);
+    return;
+  }
+  cx* smem = (cx*)xs_dsmem;
+  cx* tw = smem;
+  xs_fill_twiddles<XS_RX>(tw);
+  __syncthreads();
+  const int r = threadIdx.x / XS_RX, t = threadIdx.x % XS_RX;
+  cx* buf = tw + XS_RX * XS_RX + r * XS_RX * (XS_RX + 1);
+  const size_t row = (size_t)blockIdx.x * XS_XROWS + r;  // over ntraj * NY
+  const int e = (int)(row / XS_NY), y = (int)(row % XS_NY);
+  const u32 blk = (u32)(A.block0 + e / A.ens1), el = (u32)(e % A.ens1);
+  cx v[XS_F][XS_RX];
+  cx* base = A.field + ((size_t)e * XS_F) * XS_NS + (size_t)y * XS_NX + t;
+  XsWarpSync ws;
+  if (MODE == 0) {
+#pragma unroll
+    for (int j = 0; j < XS_RX; ++j) {
+      real x, yy;
+      xs_row_coords(y, t, j, x, yy);
+      const int s = y * XS_NX + t + XS_RX * j;
+      cx a[XS_F];
+      if (A.a_in) {
+#pragma unroll
+        for (int f = 0; f < XS_F; ++f) {
+          const double2 q = A.a_in[((size_t)e * XS_F + f) * XS_NS + s];
+          a[f] = mkcx((real)q.x, (real)q.y);
+        }
+      } else {
+        real vv[XS_NV > 0 ? XS_NV : 1];
+#if XS_NV > 0
+        xs_normals<XS_NV>(vv, (u32)s, el, 0u, (u32)A.seq, A.seed, blk);
+#pragma unroll
+        for (int c = 0; c < XS_NV; ++c) vv[c] *= (real)A.vscale;
+#endif
+        xs_initial(vv, x, yy, (real)0, a);
+      }
+#pragma unroll
+      for (int f = 0; f < XS_F; ++f) v[f][j] = a[f];
+    }
+  } else {
+#pragma unroll
+    for (int f = 0; f < XS_F; ++f)
+#pragma unroll
+      for (int j = 0; j < XS_RX; ++j) v[f][j] = base[(size_t)f * XS_NS + XS_RX * j];
+#pragma unroll
+    for (int f = 0; f < XS_F; ++f) xs_ifft4<XS_RX>(v[f], t, tw, buf, ws);
+  }
+  if (MODE == 1) {
+    // MP midpoint iterations (Applications/SDE/MP.m:13-23) at t + dtr/2.
+    const real h = (real)(A.dtr * 0.5);
+    const real tm = (real)(A.t + A.dtr * 0.5);
+#pragma unroll
+    for (int j = 0; j < XS_RX; ++j) {
+      real x, yy;
+      xs_row_coords(y, t, j, x, yy);
+      const u32 s = (u32)(y * XS_NX + t + XS_RX * j);
+      real w[XS_NW > 0 ? XS_NW : 1];
+#if XS_NW > 0
+      xs_normals<XS_NW>(w, s, el, (u32)A.draw0, (u32)A.seq, A.seed, blk);
+      if (A.draw1 >= 0) {
+        real w2[XS_NW];
+        xs_normals<XS_NW>(w2, s, el, (u32)A.draw1, (u32)A.seq, A.seed, blk);
+#pragma unroll
+        for (int c = 0; c < XS_NW; ++c) w[c] = (w[c] * (real)A.wscale + w2[c] * (real)A.wscale) * (real)0.5;
+      } else {
+#pragma unroll
+        for (int c = 0; c < XS_NW; ++c) w[c] = w[c] * (real)A.wscale;
+      }
+#endif
+      cx a0[XS_F], a[XS_F], d[XS_F];
+#pragma unroll
+      for (int f = 0; f < XS_F; ++f) a0[f] = a[f] = v[f][j];
+#pragma unroll
+      for (int it = 0; it < XS_ITER; ++it) {
+        xs_deriv(a, w, x, yy, (real)0, tm, d);
+#pragma unroll
+        for (int f = 0; f < XS_F; ++f) a[f] = a0[f] + h * d[f];
+      }
+#pragma unroll
+      for (int f = 0; f < XS_F; ++f) v[f][j] = (real)2 * a[f] - a0[f];
+    }
+  }
+  if (MODE == 3) {
+    bool bad = false;
+#pragma unroll
+    for (int f = 0; f < XS_F; ++f)
+#pragma unroll
+      for (int j = 0; j < XS_RX; ++j) {
+        const cx q = v[f][j];
+        if (!isfinite((double)q.re) || !isfinite((double)q.im)) bad = true;
+        if (A.a_out)
+          A.a_out[((size_t)e * XS_F + f) * XS_NS + (size_t)y * XS_NX + t + XS_RX * j] =
+              make_double2((double)q.re, (double)q.im);
+      }
+    if (bad) atomicOr(A.status, 1);
+    return;
+  }
+#pragma unroll
+  for (int f = 0; f < XS_F; ++f) xs_fft4<XS_RX>(v[f], t, tw, buf, ws);
+#pragma unroll
+  for (int f = 0; f < XS_F; ++f)
+#pragma unroll
+    for (int j = 0; j < XS_RX; ++j) base[(size_t)f * XS_NS + XS_RX * j] = v[f][j];
+}
+
+extern "C" __global__ void __launch_bounds__(256) xs_x_init(const XsStreamArgs A) { xs_xpass_body<0>(A); }
+extern "C" __global__ void __launch_bounds__(256) xs_x_nl(const XsStreamArgs A) { xs_xpass_body<1>(A); }
+extern "C" __global__ void __launch_bounds__(256) xs_x_final(const XsStreamArgs A) { xs_xpass_body<3>(A); }
+
+// ---- column pass ------------------------------------------------------------
+// CTA = TX consecutive kx columns of one (trajectory, component); thread
+// (c = tid % TX, t = tid / TX) holds y = t + RY*j of column c.
+#define XS_SSMEM (XS_RY * XS_RY + XS_TX * XS_RY * (XS_RY + 1))
+
+extern "C" __global__ void __launch_bounds__(256) xs_s_pass(const XsStreamArgs A) {
+  if ((size_t)blockIdx.x >= (size_t)A.ntraj * XS_F * (XS_NX / XS_TX)) {
+    if (threadIdx.x == 0) atomicOr(A.status, 2);
+    return;
+  }
+  cx* smem = (cx*)xs_dsmem;
+  cx* tw = smem;
+  xs_fill_twiddles<XS_RY>(tw);
+  const int c = threadIdx.x % XS_TX, t = threadIdx.x / XS_TX;
+  cx* buf = tw + XS_RY * XS_RY + c * XS_RY * (XS_RY + 1);
+  constexpr int TILES = XS_NX / XS_TX;
+  const size_t tile = blockIdx.x;  // over ntraj * F * TILES
+  const int x0 = (int)(tile % TILES) * XS_TX;
+  const size_t ef = tile / TILES;  // e * F + f
+  const int f = (int)(ef % XS_F);
+  cx* base = A.field + ef * XS_NS + x0 + c;
+  cx v[XS_RY];
+#pragma unroll
+  for (int j = 0; j < XS_RY; ++j) v[j] = base[(size_t)(t + XS_RY * j) * XS_NX];
+  __syncthreads();  // twiddles ready
+  XsBlockSync bs;
+  xs_fft4<XS_RY>(v, t, tw, buf, bs);
+  const double2* P = (A.m == 2 ? A.prop2 : A.prop1) + (XS_PROP_COMPS > 1 ? (size_t)f * XS_NS : 0);
+#pragma unroll
+  for (int k = 0; k < XS_RY; ++k) {
+    const double2 pr = P[(size_t)(t + XS_RY * k) * XS_NX + x0 + c];
+    const double vr = (double)v[k].re, vi = (double)v[k].im;
+    v[k] = mkcx((real)(vr * pr.x - vi * pr.y), (real)(vr * pr.y + vi * pr.x));
+  }
+  xs_ifft4<XS_RY>(v, t, tw, buf, bs);
+#pragma unroll
+  for (int j = 0; j < XS_RY; ++j) base[(size_t)(t + XS_RY * j) * XS_NX] = v[j];
+}
+
+// ---- observation pass ---------------------------------------------------------
+// CTA = (row group, block): OROWS rows of every trajectory of the block.
+// Site observables: block sums in FP64 registers, written as block means.
+// Reductions (Int/Ave): per-trajectory sums over the row group -> redpart.
+#define XS_OSMEM (XS_RX * XS_RX + XS_OROWS * XS_RX * (XS_RX + 1))
+
+extern "C" __global__ void __launch_bounds__(XS_OROWS * XS_RX) xs_x_obs(const XsStreamArgs A) {
+  if ((int)blockIdx.x >= XS_NRG || (size_t)(blockIdx.y + 1) * A.ens1 > (size_t)A.ntraj) {
+    if (threadIdx.x == 0) atomicOr(A.status, 2);
+    return;
+  }
+  cx* smem = (cx*)xs_dsmem;
+  __shared__ double wred[(XS_OROWS * XS_RX + 31) / 32][2 * (XS_NRED > 0 ? XS_NRED : 1)];
+  cx* tw = smem;
+  xs_fill_twiddles<XS_RX>(tw);
+  __syncthreads();
+  const int r = threadIdx.x / XS_RX, t = threadIdx.x % XS_RX;
+  cx* buf = tw + XS_RX * XS_RX + r * XS_RX * (XS_RX + 1);
+  const int rg = blockIdx.x;       // row group
+  const int b = blockIdx.y;        // block within the launch
+  const int y = rg * XS_OROWS + r;
+  const real tt = (real)A.t;
+  XsWarpSync ws;
+#if XS_NOUT_SITE > 0
+  double sr[XS_NOUT_SITE][XS_RX], si[XS_NOUT_SITE][XS_RX];
+#pragma unroll
+  for (int k = 0; k < XS_NOUT_SITE; ++k)
+#pragma unroll
+    for (int j = 0; j < XS_RX; ++j) sr[k][j] = si[k][j] = 0;
+#endif
+  for (int el = 0; el < A.ens1; ++el) {
+    const int e = b * A.ens1 + el;
+    cx v[XS_F][XS_RX];
+    const cx* base = A.field + ((size_t)e * XS_F) * XS_NS + (size_t)y * XS_NX + t;
+#pragma unroll
+    for (int f = 0; f < XS_F; ++f)
+#pragma unroll
+      for (int j = 0; j < XS_RX; ++j) v[f][j] = base[(size_t)f * XS_NS + XS_RX * j];
+#pragma unroll
+    for (int f = 0; f < XS_F; ++f) xs_ifft4<XS_RX>(v[f], t, tw, buf, ws);
+#if XS_NRED > 0
+    double acc[2 * XS_NRED];
+#pragma unroll
+    for (int k = 0; k < 2 * XS_NRED; ++k) acc[k] = 0;
+#endif
+#pragma unroll
+    for (int j = 0; j < XS_RX; ++j) {
+      real x, yy;
+      xs_row_coords(y, t, j, x, yy);
+      cx a[XS_F];
+#pragma unroll
+      for (int f = 0; f < XS_F; ++f) a[f] = v[f][j];
+#if XS_NRED > 0
+      cx rr[XS_NRED];
+      xs_integrands(a, t + XS_RX * j, y, 0, x, yy, (real)0, tt, rr);
+#pragma unroll
+      for (int k = 0; k < XS_NRED; ++k) { acc[2 * k] += (double)rr[k].re; acc[2 * k + 1] += (double)rr[k].im; }
+#endif
+#if XS_NOUT_SITE > 0
+      cx o[XS_NOUT_SITE];
+      xs_obs_site(a, (const cx*)nullptr, x, yy, (real)0, tt, o);
+#pragma unroll
+      for (int k = 0; k < XS_NOUT_SITE; ++k) { sr[k][j] += (double)o[k].re; si[k][j] += (double)o[k].im; }
+#endif
+    }
+#if XS_NRED > 0
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < 2 * XS_NRED; ++k) {
+      const double s = xs_warp_sum(acc[k]);
+      if (lane == 0) wred[warp][k] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x < XS_NRED) {
+      double re = 0, im = 0;
+      for (int q = 0; q < (XS_OROWS * XS_RX + 31) / 32; ++q) {
+        re += wred[q][2 * threadIdx.x];
+        im += wred[q][2 * threadIdx.x + 1];
+      }
+      A.redpart[((size_t)e * XS_NRG + rg) * XS_NRED + threadIdx.x] = make_double2(re, im);
+    }
+    __syncthreads();
+#endif
+  }
+#if XS_NOUT_SITE > 0
+  const double inv = 1.0 / (double)A.ens1;
+  double2* out = A.av + ((size_t)b * A.npoints + A.n) * XS_OBS_STRIDE;
+#pragma unroll
+  for (int k = 0; k < XS_NOUT_SITE; ++k)
+#pragma unroll
+    for (int j = 0; j < XS_RX; ++j)
+      out[(size_t)k * XS_NS + (size_t)y * XS_NX + t + XS_RX * j] = make_double2(sr[k][j] * inv, si[k][j] * inv);
+#endif
+}
+
+// Scalar observables from per-trajectory reductions: CTA per block, fixed
+// summation order over row groups and trajectories.
+extern "C" __global__ void __launch_bounds__(256) xs_stream_scalar(const XsStreamArgs A) {
+#if XS_NOUT_SCALAR > 0
+  __shared__ double part[8][2 * XS_NOUT_SCALAR];
+  const int b = blockIdx.x;
+  if ((size_t)(b + 1) * A.ens1 > (size_t)A.ntraj || blockDim.x > 256) {
+    if (threadIdx.x == 0) atomicOr(A.status, 2);
+    return;
+  }
+  double acc[2 * XS_NOUT_SCALAR];
+#pragma unroll
+  for (int k = 0; k < 2 * XS_NOUT_SCALAR; ++k) acc[k] = 0;
+  for (int el = threadIdx.x; el < A.ens1; el += blockDim.x) {
+    const int e = b * A.ens1 + el;
+    cx red[XS_NRED > 0 ? XS_NRED : 1];
+#pragma unroll
+    for (int k = 0; k < XS_NRED; ++k) {
+      double re = 0, im = 0;
+      for (int g = 0; g < XS_NRG; ++g) {
+        const double2 q = A.redpart[((size_t)e * XS_NRG + g) * XS_NRED + k];
+        re += q.x;
+        im += q.y;
+      }
+      red[k] = mkcx((real)re, (real)im);
+    }
+    cx o[XS_NOUT_SCALAR];
+    xs_obs_scalar(red, (real)A.t, o);
+#pragma unroll
+    for (int k = 0; k < XS_NOUT_SCALAR; ++k) { acc[2 * k] += (double)o[k].re; acc[2 * k + 1] += (double)o[k].im; }
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < 2 * XS_NOUT_SCALAR; ++k) {
+    const double s = xs_warp_sum(acc[k]);
+    if (lane == 0) part[warp][k] = s;
+  }
+  __syncthreads();
+  if (threadIdx.x < XS_NOUT_SCALAR) {
+    double re = 0, im = 0;
+    for (int q = 0; q < 8; ++q) {
+      re += part[q][2 * threadIdx.x];
+      im += part[q][2 * threadIdx.x + 1];
+    }
+    const double inv = 1.0 / (double)A.ens1;
+    A.av[((size_t)b * A.npoints + A.n) * XS_OBS_STRIDE + (size_t)XS_NOUT_SITE * XS_NS + threadIdx.x] =
+        make_double2(re * inv, im * inv);
+  }
+#endif
+}

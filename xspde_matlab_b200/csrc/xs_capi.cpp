@@ -145,6 +145,8 @@ void mkdirs(const std::string& path) {
 std::string nvrtc_compile(const std::string& src, const std::string& name, std::string* log_out) {
   std::vector<std::string> opts = {"--gpu-architecture=sm_100a", "-std=c++17", "--device-as-default-execution-space",
                                    "-lineinfo", "--extra-device-vectorization", "-DXS_NVRTC=1"};
+  if (const char* v = getenv("XSPDE_B200_PTXAS_VERBOSE"))
+    if (*v && *v != '0') opts.push_back("--ptxas-options=-v");
   int maj = 0, min = 0;
   nvrtcVersion(&maj, &min);
   std::string key = src;
@@ -601,6 +603,12 @@ struct ResidentPlan {
   size_t smem = 0;
 };
 
+// Streaming plan: 2D lattice with NX = RX^2, NY = RY^2 (RX, RY in {8, 16, 32}).
+struct StreamPlan {
+  int RX = 0, RY = 0, XROWS = 0, TX = 0, OROWS = 0;
+  size_t xsmem = 0, ssmem = 0, osmem = 0;
+};
+
 }  // namespace
 
 struct xs_handle {
@@ -614,9 +622,13 @@ struct xs_handle {
   bool loaded = false;
   CUmodule mod = nullptr;
   CUfunction f_resident = nullptr, f_reduce = nullptr, f_noise = nullptr;
+  CUfunction f_xinit = nullptr, f_xnl = nullptr, f_xfinal = nullptr, f_spass = nullptr, f_xobs = nullptr,
+             f_scalar = nullptr;
+  StreamPlan sp;
+  int path_kind = 0;
   cudaStream_t stream = nullptr;
-  DevBuf d_prop[2], d_tmat, d_obs, d_av, d_ain, d_aout, d_status, d_w;
-  double prop_dtr[2] = {-1, -1};
+  DevBuf d_prop[2], d_prop2[2], d_tmat, d_obs, d_av, d_ain, d_aout, d_status, d_w, d_field, d_redpart;
+  double prop_dtr[2] = {-1, -1}, prop2_dtr[2] = {-1, -1};
   std::vector<int> tmat_off;
   ~xs_handle() {
     if (mod && driver().unload) driver().unload(mod);
@@ -666,12 +678,87 @@ void plan_resident(xs_handle& h, int total_traj) {
   h.rp = rp;
 }
 
-void build_source(xs_handle& h) {
-  Problem& P = h.P;
-  std::ostringstream fns;
-  generate_functions(P, fns);  // fixes P.nred / nout_* before the launch plan
-  plan_resident(h, P.E1 * P.p.ensembles[1] * P.p.ensembles[2]);
+int isqrt_pow2(int n) {
+  for (int r : {8, 16, 32})
+    if (r * r == n) return r;
+  return 0;
+}
+
+// Reason why the streaming path cannot run this problem, or "" when it can.
+std::string stream_blocker(const Problem& P) {
+  if (P.D != 2) return "the streaming path covers two space dimensions";
+  if (!isqrt_pow2(P.N[0]) || !isqrt_pow2(P.N[1])) return "streaming lattices need 64, 256 or 1024 points per dimension";
+  for (int v : P.bnd)
+    if (v) return "the streaming path covers periodic boundaries";
+  if (P.p.method != XS_METHOD_MP) return "the streaming path integrates with MP";
+  if (!P.has_linear) return "the streaming path needs p.linear";
+  for (auto& o : P.obs)
+    if (o.spatial && !o.gen.reductions.empty()) return "site observables that use Int/Ave are not streamed";
+  return "";
+}
+
+// Straight-line radix-2 DIT DFT of R points (forward, exp(-2 pi i n k / R)),
+// emitted with literal twiddles; trivial twiddles (1, -i) cost no multiply.
+std::string gen_dft(int R) {
   std::ostringstream os;
+  int bits = 0;
+  while ((1 << bits) < R) ++bits;
+  auto rev = [&](int i) {
+    int r = 0;
+    for (int b = 0; b < bits; ++b)
+      if (i & (1 << b)) r |= 1 << (bits - 1 - b);
+    return r;
+  };
+  os << "template <> __device__ __forceinline__ void xs_dftR<" << R << ">(cx (&v)[" << R << "]) {\n";
+  std::vector<std::string> cur(R);
+  for (int i = 0; i < R; ++i) cur[i] = "v[" + std::to_string(rev(i)) + "]";
+  int tmp = 0;
+  for (int len = 2; len <= R; len <<= 1) {
+    std::vector<std::string> nxt(R);
+    for (int i = 0; i < R; i += len)
+      for (int k = 0; k < len / 2; ++k) {
+        int u = i + k, w = i + k + len / 2;
+        std::string tw = "q" + std::to_string(tmp++);
+        if (k == 0) {
+          os << "  const cx " << tw << " = " << cur[w] << ";\n";
+        } else if (4 * k == len) {
+          os << "  const cx " << tw << " = mkcx(" << cur[w] << ".im, -" << cur[w] << ".re);\n";
+        } else {
+          double c = std::cos(2 * M_PI * k / len), s = -std::sin(2 * M_PI * k / len);
+          os << "  const cx " << tw << " = " << cur[w] << " * mkcx((real)" << fmt(c) << ", (real)" << fmt(s) << ");\n";
+        }
+        std::string a = "q" + std::to_string(tmp++), b = "q" + std::to_string(tmp++);
+        os << "  const cx " << a << " = " << cur[u] << " + " << tw << ";\n";
+        os << "  const cx " << b << " = " << cur[u] << " - " << tw << ";\n";
+        nxt[u] = a;
+        nxt[w] = b;
+      }
+    cur = nxt;
+  }
+  for (int i = 0; i < R; ++i) os << "  v[" << i << "] = " << cur[i] << ";\n";
+  os << "}\n";
+  return os.str();
+}
+
+void plan_stream(xs_handle& h) {
+  const Problem& P = h.P;
+  StreamPlan sp;
+  sp.RX = isqrt_pow2(P.N[0]);
+  sp.RY = isqrt_pow2(P.N[1]);
+  sp.XROWS = 256 / sp.RX;
+  sp.TX = 256 / sp.RY;
+  sp.OROWS = std::max(1, 64 / sp.RX);
+  size_t cxs = h.fp64 ? 16 : 8;
+  sp.xsmem = (size_t)(sp.RX * sp.RX + sp.XROWS * sp.RX * (sp.RX + 1)) * cxs;
+  sp.ssmem = (size_t)(sp.RY * sp.RY + sp.TX * sp.RY * (sp.RY + 1)) * cxs;
+  sp.osmem = (size_t)(sp.RX * sp.RX + sp.OROWS * sp.RX * (sp.RX + 1)) * cxs;
+  if (P.N[1] % sp.XROWS || P.N[1] % sp.OROWS || P.N[0] % sp.TX)
+    raise(XS_ERR_SHAPE, "internal: streaming tile sizes do not divide the lattice");
+  h.sp = sp;
+}
+
+void emit_common_header(const xs_handle& h, std::ostringstream& os) {
+  const Problem& P = h.P;
   os << "// generated problem header\n";
   os << "#define XS_FP64 " << (h.fp64 ? 1 : 0) << "\n#define XS_REAL " << (h.fp64 ? "double" : "float") << "\n";
   os << xs_kernel_source_prelude << "\n";
@@ -687,6 +774,37 @@ void build_source(xs_handle& h) {
   os << "#define XS_METHOD " << P.p.method << "\n#define XS_ITER " << P.p.iterations << "\n";
   os << "#define XS_HAS_PROP " << ((P.has_linear && P.D > 0) ? 1 : 0) << "\n#define XS_PROP_COMPS " << P.Lc << "\n";
   os << "#define XS_SETBOUND " << (P.setbound ? 1 : 0) << "\n";
+}
+
+void build_source(xs_handle& h) {
+  Problem& P = h.P;
+  std::ostringstream fns;
+  generate_functions(P, fns);  // fixes P.nred / nout_* before the launch plan
+  const bool fits = resident_smem(h, 1, method_arrays(P.p.method)) <= 200 * 1024;
+  const std::string why = stream_blocker(P);
+  if (h.path_kind == 2 || (h.path_kind == 0 && !fits)) {
+    if (!why.empty()) {
+      if (!fits) raise(XS_ERR_UNSUPPORTED, "field too large for the resident path, and " + why);
+      raise(XS_ERR_UNSUPPORTED, why);
+    }
+    h.kind = 2;
+    plan_stream(h);
+    std::ostringstream os;
+    emit_common_header(h, os);
+    os << "#define XS_FFT_RX " << h.sp.RX << "\n#define XS_FFT_RY " << h.sp.RY << "\n#define XS_OBS_ROWS " << h.sp.OROWS
+       << "\n";
+    os << fns.str();
+    os << "template <int R> __device__ __forceinline__ void xs_dftR(cx (&v)[R]);\n";
+    os << gen_dft(h.sp.RX);
+    if (h.sp.RY != h.sp.RX) os << gen_dft(h.sp.RY);
+    os << xs_kernel_source_stream << "\n";
+    h.source = os.str();
+    return;
+  }
+  h.kind = 1;
+  plan_resident(h, P.E1 * P.p.ensembles[1] * P.p.ensembles[2]);
+  std::ostringstream os;
+  emit_common_header(h, os);
   os << "#define XS_G " << h.rp.G << "\n#define XS_THREADS " << h.rp.threads << "\n#define XS_NARR " << h.rp.narr << "\n";
   os << "#define XS_SMEM_BYTES " << h.rp.smem << "\n";
   os << fns.str();
@@ -697,6 +815,27 @@ void build_source(xs_handle& h) {
 void load_module(xs_handle& h) {
   if (h.loaded) return;
   ensure_device();
+  if (h.kind == 2) {
+    std::string cubin = nvrtc_compile(h.source, "xs_stream", nullptr);
+    Driver& d = driver();
+    cu_check(d.load(&h.mod, cubin.data()), "cuModuleLoadData");
+    struct {
+      CUfunction* f;
+      const char* name;
+      size_t smem;
+    } fns[] = {{&h.f_xinit, "xs_x_init", h.sp.xsmem}, {&h.f_xnl, "xs_x_nl", h.sp.xsmem},
+               {&h.f_xfinal, "xs_x_final", h.sp.xsmem}, {&h.f_spass, "xs_s_pass", h.sp.ssmem},
+               {&h.f_xobs, "xs_x_obs", h.sp.osmem}, {&h.f_scalar, "xs_stream_scalar", 0}};
+    for (auto& f : fns) {
+      cu_check(d.getfn(f.f, h.mod, f.name), f.name);
+      if (f.smem > 48 * 1024)
+        cu_check(d.setattr(*f.f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, (int)f.smem), f.name);
+    }
+    CUDA_CHECK(cudaStreamCreateWithFlags(&h.stream, cudaStreamNonBlocking));
+    h.d_status.ensure(sizeof(int));
+    h.loaded = true;
+    return;
+  }
   std::string cubin = nvrtc_compile(h.source, "xs_resident", nullptr);
   Driver& d = driver();
   cu_check(d.load(&h.mod, cubin.data()), "cuModuleLoadData");
@@ -829,6 +968,123 @@ void launch_resident(xs_handle& h, int first_block, int nblocks, int nc, const v
   }
 }
 
+// exp(2 L dtr/ipsteps): two consecutive half-step propagators merged into one.
+const void* ensure_prop2(xs_handle& h, int nc) {
+  const Problem& P = h.P;
+  int slot = nc == 2 ? 1 : 0;
+  ensure_prop(h, nc);
+  double dt = 2.0 * pass_dtr(P, nc) / P.p.ipsteps;
+  if (h.prop2_dtr[slot] == dt) return h.d_prop2[slot].p;
+  std::vector<cd> pr(P.L.size());
+  for (size_t i = 0; i < P.L.size(); ++i) pr[i] = std::exp(P.L[i] * dt);
+  h.d_prop2[slot].ensure(std::max<size_t>(pr.size(), 1) * 16);
+  CUDA_CHECK(cudaMemcpy(h.d_prop2[slot].p, pr.data(), pr.size() * 16, cudaMemcpyHostToDevice));
+  h.prop2_dtr[slot] = dt;
+  return h.d_prop2[slot].p;
+}
+
+struct StreamArgsHost {
+  int ntraj, ens1, block0, seq;
+  unsigned seed;
+  int draw0, draw1, m, n, npoints;
+  double wscale, vscale, dtr, t;
+  void* field;
+  const void* prop1;
+  const void* prop2;
+  const void* a_in;
+  void* a_out;
+  void* av;
+  void* redpart;
+  int* status;
+};
+
+// Streaming schedule of one xpath call (Simulator/xpath.m:137-194) for MP:
+// column passes apply the pending half-step propagators, row passes do the
+// midpoint step; observations need all half steps applied first.
+void launch_stream(xs_handle& h, int first_block, int nblocks, int nc, const void* a_in_dev, void* av_dev,
+                   void* a_out_dev, cudaStream_t st) {
+  const Problem& P = h.P;
+  const StreamPlan& sp = h.sp;
+  const int total = nblocks * P.E1;
+  const size_t cxs = h.fp64 ? 16 : 8;
+  h.d_field.ensure((size_t)total * P.F * P.NS * cxs);
+  const int nrg = P.N[1] / sp.OROWS;
+  if (P.nred) h.d_redpart.ensure((size_t)total * nrg * P.nred * 16);
+  StreamArgsHost a{};
+  a.ntraj = total;
+  a.ens1 = P.E1;
+  a.block0 = first_block;
+  a.seq = 0;
+  a.seed = (unsigned)(P.p.seed & 0xffffffffu);
+  a.draw0 = 0;
+  a.draw1 = -1;
+  a.npoints = P.p.points[0];
+  a.wscale = std::sqrt(P.nscale * P.noisefactor);
+  a.vscale = std::sqrt(P.noisefactor);
+  a.dtr = pass_dtr(P, nc);
+  a.t = P.p.origins[0];
+  a.field = h.d_field.p;
+  a.prop1 = ensure_prop(h, nc);
+  a.prop2 = ensure_prop2(h, nc);
+  a.a_in = a_in_dev;
+  a.a_out = a_out_dev;
+  a.av = av_dev;
+  a.redpart = h.d_redpart.p;
+  a.status = (int*)h.d_status.p;
+  Driver& d = driver();
+  void* params[] = {&a};
+  const unsigned xgrid = (unsigned)((size_t)total * P.N[1] / sp.XROWS);
+  const unsigned sgrid = (unsigned)((size_t)total * P.F * (P.N[0] / sp.TX));
+  auto row = [&](CUfunction f) {
+    cu_check(d.launch(f, xgrid, 1, 1, 256, 1, 1, (unsigned)sp.xsmem, (CUstream)st, params, nullptr), "row pass");
+  };
+  auto col = [&](int m) {
+    a.m = m;
+    cu_check(d.launch(h.f_spass, sgrid, 1, 1, 256, 1, 1, (unsigned)sp.ssmem, (CUstream)st, params, nullptr),
+             "column pass");
+  };
+  auto observe = [&](int n) {
+    a.n = n;
+    cu_check(d.launch(h.f_xobs, (unsigned)nrg, (unsigned)nblocks, 1, (unsigned)(sp.OROWS * sp.RX), 1, 1,
+                      (unsigned)sp.osmem, (CUstream)st, params, nullptr),
+             "observation pass");
+    if (P.nout_scalar)
+      cu_check(d.launch(h.f_scalar, (unsigned)nblocks, 1, 1, 256, 1, 1, 0, (CUstream)st, params, nullptr),
+               "scalar observables");
+  };
+  row(h.f_xinit);
+  int pending = 0, draw = 0, prev_draw = -1;
+  const int npts = P.p.points[0], S = P.p.steps, checks = P.p.checks;
+  for (int n = 0; n < npts; ++n) {
+    for (int step = 0; step < S; ++step) {
+      if (n > 0 || step > 0 || npts == 1) {
+        for (int chk = 0; chk <= checks; ++chk) {
+          ++draw;
+          if (nc == 2 && checks && chk == 0) {
+            prev_draw = draw;
+            continue;
+          }
+          col(pending + 1);
+          a.draw0 = draw;
+          a.draw1 = (nc == 2 && checks) ? prev_draw : -1;
+          row(h.f_xnl);
+          a.t += a.dtr;
+          pending = 1;
+        }
+      }
+      if (step == 0) {
+        if (pending) col(pending);
+        pending = 0;
+        observe(n);
+      }
+    }
+  }
+  if (a_out_dev) {
+    if (pending) col(pending);
+    row(h.f_xfinal);
+  }
+}
+
 // device [b][n][k] -> host MATLAB av{o} [lines, time, space] per block per observable
 void scatter_av(const Problem& P, const std::vector<double>& dev, int nblocks, double* out) {
   const size_t stride = av_stride(P);
@@ -876,8 +1132,8 @@ xs_status guard(F&& f) {
 void create_impl(const xs_problem* prob, xs_handle* h) {
   setup_problem(prob, h->P);
   h->fp64 = prob->precision != XS_PREC_FP32;
-  if (prob->path_kind == 2) raise(XS_ERR_UNSUPPORTED, "streaming path is not available for this problem");
-  h->kind = 1;
+  if (prob->path_kind < 0 || prob->path_kind > 2) raise(XS_ERR_ARG, "path_kind must be 0, 1 or 2");
+  h->path_kind = prob->path_kind;
   build_source(*h);
 }
 
@@ -915,7 +1171,7 @@ XS_API xs_status xs_compile_check(const xs_problem* prob, char* log, size_t n) {
     xs_handle h;
     create_impl(prob, &h);
     std::string lg;
-    nvrtc_compile(h.source, "xs_resident", &lg);
+    nvrtc_compile(h.source, h.kind == 2 ? "xs_stream" : "xs_resident", &lg);
     if (log && n) {
       size_t m = std::min(n - 1, lg.size());
       memcpy(log, lg.data(), m);
@@ -974,7 +1230,8 @@ XS_API xs_status xs_run_path(xs_handle* h, int first_block, int nblocks, int nc,
     const size_t avd = (size_t)nblocks * P.p.points[0] * stride * 2;
     h->d_av.ensure(std::max<size_t>(avd, 1) * 8);
     CUDA_CHECK(cudaMemsetAsync(h->d_status.p, 0, sizeof(int), h->stream));
-    launch_resident(*h, first_block, nblocks, nc, din, h->d_av.p, dout, h->stream);
+    if (h->kind == 2) launch_stream(*h, first_block, nblocks, nc, din, h->d_av.p, dout, h->stream);
+    else launch_resident(*h, first_block, nblocks, nc, din, h->d_av.p, dout, h->stream);
     std::vector<double> av(avd);
     if (avd) CUDA_CHECK(cudaMemcpyAsync(av.data(), h->d_av.p, avd * 8, cudaMemcpyDeviceToHost, h->stream));
     int status = 0;
@@ -1012,7 +1269,8 @@ XS_API xs_status xs_run_path_device(xs_handle* h, int first_block, int nblocks, 
     load_module(*h);
     cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
     CUDA_CHECK(cudaMemsetAsync(h->d_status.p, 0, sizeof(int), st));
-    launch_resident(*h, first_block, nblocks, nc, a_in_dev, av_dev, a_out_dev, st);
+    if (h->kind == 2) launch_stream(*h, first_block, nblocks, nc, a_in_dev, av_dev, a_out_dev, st);
+    else launch_resident(*h, first_block, nblocks, nc, a_in_dev, av_dev, a_out_dev, st);
     return XS_OK;
   });
 }
