@@ -1,0 +1,352 @@
+"""Benchmark: ensemble integration of the 2D stochastic GPE / CGL on one B200.
+
+Workload (the reference's second configuration): 256x256 periodic lattice over
+[-10,10]^2, da/dt = (i+0.1) lap a + (1-|a|^2) a - 0.5i |a|^2 a + 0.05 xi,
+a0 = 1 + 0.1 complex Gaussian, 4096 trajectories (16 blocks of 256), MP with 4
+iterations, 51 output points x 10 steps (509 integration steps, the xSPDE
+path's own count), observable <|a|^2>(x, y, t).  FP32 fields and transforms,
+FP64 propagator tables and moments.  Synthetic inputs: the initial field and
+all noise come from the counter-based Philox stream (seed 0).
+
+One "step" of this benchmark is one full p.path call over all 4096
+trajectories.  value = trajectory-steps/s with everything resident in HBM
+(field 2.1 GB > L2 every pass); e2e = the same through the host C ABI call
+xs_run_path with a pinned FP64 initial field copied in and the block means
+copied out inside the timed region.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With N > 1 (torchrun, one process per GPU) every rank integrates its own 16
+blocks (global block ids rank*16 .. rank*16+15: weak scaling); the FP64 block
+moments are summed over ranks with one NCCL all-reduce inside the timed
+region.  --impl reference times the CPU restatement of the reference path
+(the oracle; MATLAB itself is not available) on the host cores.
+"""
+import argparse
+import ctypes
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+HBM_FALLBACK_GBS = 6650.0
+# DRAM bytes per launch of the dominant kernels from one ncu capture of a
+# 512-trajectory case of the same problem, scaled to 4096 trajectories (traffic
+# grows with the trajectory count); profiles/ holds the capture summary.
+NCU_TRAFFIC_PER_TRAJ = {"x_step": None, "y_pass": None}
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return HBM_FALLBACK_GBS, "fallback"
+
+
+class Clocks:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        try:
+            for line in open(self.path):
+                f = [x.strip() for x in line.split(",")]
+                if len(f) < 9:
+                    continue
+                try:
+                    sm.append(float(f[1]))
+                    mx = float(f[2])
+                except ValueError:
+                    continue
+                names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+                for nm, v in zip(names, f[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(nm)
+        except Exception:
+            pass
+        finally:
+            try:
+                os.unlink(self.path)
+            except Exception:
+                pass
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def _problem(ntraj=4096):
+    from xspde_matlab_b200.problems import GPE_2D
+    p = dict(GPE_2D)
+    p["ensembles"] = [256, max(1, ntraj // 256), 1]
+    return p
+
+
+def _cpu_sample(seconds=12.0, ntraj=2):
+    """Oracle (FP64 NumPy restatement of the reference path, one core) on a
+    bounded sample of the workload: `ntraj` trajectories of the same 256x256
+    problem for as many integration steps as fit in about `seconds`."""
+    import numpy as np
+    from oracle import xspde_ref as X
+    p = _problem()
+    o = dict(dimensions=3, points=[2, 256, 256], ranges=[0.4, 20.0, 20.0], steps=40, ensembles=[ntraj, 1, 1],
+             noises=2, method="MP", checks=0,
+             deriv=lambda a, w, q: (1 - abs(a) ** 2) * a - 0.5j * abs(a) ** 2 * a
+             + 0.05 * (w[0:1] + 1j * w[1:2]) / np.sqrt(2),
+             initial=lambda v, q: 1 + 0.1 * (v[0:1] + 1j * v[1:2]) / np.sqrt(2),
+             linear=lambda q: (1j + 0.1) * (q.Dx ** 2 + q.Dy ** 2), observe=[lambda a, q: abs(a) ** 2])
+    inp = X.xpreferences([o])[0]
+    q = inp.copy()
+    q.block = 0
+    q.seq = 0
+    q.dtr = q.dt / q.steps[0]
+    q.propagator, q.da = q.propfactor(q)
+    v = q.randomgen(q)
+    q.t = q.origins[0]
+    a = X.fit(np.asarray(q.initial(v, q), dtype=complex), q.ca)
+    method = X.METHODS["MP"]
+    q.draw = 0
+    t0 = time.perf_counter()
+    steps = 0
+    while time.perf_counter() - t0 < seconds:
+        q.draw += 1
+        w = q.noisegen(None, 1, q.nscale, q)
+        a = method(a, w, q)
+        q.t += q.dtr
+        steps += 1
+    el = time.perf_counter() - t0
+    del p
+    return steps * ntraj / el, "%d trajectories x %d MP steps of the 256x256 problem (FP64 NumPy oracle, 1 core)" % (
+        ntraj, steps)
+
+
+def _reference_worker(args):
+    seconds, ntraj = args
+    os.environ.setdefault("OMP_NUM_THREADS", "1")
+    r, _ = _cpu_sample(seconds, ntraj)
+    return r
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the CPU restatement of the reference path on all host cores."""
+    import multiprocessing as mp
+    if rank != 0:
+        print(json.dumps({"impl": "reference", "rank": rank, "skipped": True}), file=sys.stderr)
+        return
+    cores = os.cpu_count() or 1
+    per_step = []
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(cores) as pool:
+        for i in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            rates = pool.map(_reference_worker, [(4.0, 2)] * cores)
+            dt = time.perf_counter() - t0
+            if i >= args.warmup:
+                per_step.append((sum(rates), dt))
+    value = statistics.mean(r for r, _ in per_step)
+    ms = 1000 * statistics.mean(d for _, d in per_step)
+    line = {
+        "impl": "reference", "metric": "traj-steps/s (2D 256x256 stochastic GPE, MP)", "value": value,
+        "unit": "traj-steps/s", "n_gpus": 0, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+        "config": {"workload": "gpe_2d 256x256, 4096 traj, 509 MP steps (bounded CPU sample per step)",
+                   "parallelism": "host processes"},
+        "cpu_baseline": {"value": value, "unit": "traj-steps/s", "cores": cores, "kind": "port",
+                         "sample": "per core: 2 trajectories x ~4 s of MP steps of the 256x256 problem; MATLAB "
+                                   "reference unavailable on this box (no MATLAB/Octave)"},
+        "e2e": {"value": value, "unit": "traj-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def run_ours(args, rank, world, local_rank):
+    import numpy as np
+    import torch
+    from xspde_matlab_b200 import GpuPath, _lib, xpreferences
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+    p = xpreferences([_problem(args.ntraj)])[0]
+    nb = p.ensembles[1] * p.ensembles[2]
+    E = p.ensembles[0]
+    ntraj = nb * E
+    steps_per_traj = p.points[0] * p.steps[0] - 1
+    path = GpuPath(p)
+    L = _lib.lib()
+    stride = 1 * p.nspace  # one site observable line
+    av = torch.zeros((nb, p.points[0], stride, 2), dtype=torch.float64, device="cuda")
+    moments = torch.zeros((2, p.points[0], stride), dtype=torch.float64, device="cuda")
+    first = rank * nb
+    stream = torch.cuda.current_stream()
+
+    def one_step():
+        _lib.check(L.xs_run_path_device(path.h, first, nb, 1, None, ctypes.c_void_p(av.data_ptr()), None,
+                                        ctypes.c_void_p(stream.cuda_stream)))
+        # block moments (xensemble.m:98-101): sum over blocks of D and D^2 / nblocks
+        re = av[..., 0]
+        moments[0].copy_(re.sum(0) / nb)
+        moments[1].copy_((re * re).sum(0) / nb)
+        if dist is not None:
+            dist.all_reduce(moments)
+
+    for _ in range(args.warmup):
+        one_step()
+    torch.cuda.synchronize()
+    L.xs_set_kernel_timing(path.h, 1)
+    L.xs_kernel_stats(path.h, 1, None, None)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(local_rank) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            one_step()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    kms = (ctypes.c_double * 8)()
+    kl = (ctypes.c_longlong * 8)()
+    _lib.check(L.xs_kernel_stats(path.h, 1, kms, kl))
+    L.xs_set_kernel_timing(path.h, 0)
+    clocks = clk.summary()
+    t_max = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if dist is not None:
+        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
+    ms_max = float(t_max.item())
+    value = world * ntraj * steps_per_traj / (ms_max / 1000.0)
+
+    if args.quick:
+        if rank == 0:
+            print(json.dumps({"quick": True, "value": value, "ms_per_step": ms_max,
+                              "kernels": {_lib.KERNEL_KINDS[i]: {"launches": int(kl[i]), "ms": float(kms[i])}
+                                          for i in range(8) if kl[i]}}))
+        return
+    # end to end through the host C ABI (pinned host buffers, copies inside the timed region)
+    a_in = torch.empty((ntraj * p.nspace * 2,), dtype=torch.float64, pin_memory=True)
+    g = torch.Generator().manual_seed(1)
+    a_in.normal_(0.0, 0.1 / math.sqrt(2), generator=g)
+    a_in[0::2] += 1.0
+    per_block = path.per_block
+    av_host = torch.empty((nb * per_block,), dtype=torch.float64, pin_memory=True)
+    e2e_steps = max(1, min(args.steps, 3))
+    _lib.check(L.xs_run_path(path.h, first, nb, 1, ctypes.c_void_p(a_in.data_ptr()),
+                             ctypes.c_void_p(av_host.data_ptr()), None))
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        _lib.check(L.xs_run_path(path.h, first, nb, 1, ctypes.c_void_p(a_in.data_ptr()),
+                                 ctypes.c_void_p(av_host.data_ptr()), None))
+    torch.cuda.synchronize()
+    e2e_ms = (time.perf_counter() - t0) * 1000 / e2e_steps
+    te = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
+    if dist is not None:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_value = world * ntraj * steps_per_traj / (float(te.item()) / 1000.0)
+
+    if rank != 0:
+        return
+    kinds = _lib.KERNEL_KINDS
+    stats = {kinds[i]: {"launches": int(kl[i]), "ms": float(kms[i])} for i in range(8) if kl[i]}
+    dom = max(("x_step", "y_pass"), key=lambda k: stats.get(k, {"ms": 0})["ms"])
+    per_launch_ms = stats[dom]["ms"] / stats[dom]["launches"]
+    alg_bytes = 2.0 * ntraj * p.fields * p.nspace * 8  # read + write of the FP32 complex field
+    achieved = alg_bytes / (per_launch_ms / 1000.0) / 1e9
+    peak, kind = _peaks()
+    tr = NCU_TRAFFIC_PER_TRAJ.get(dom)
+    gpu_launches = sum(int(kl[i]) for i in range(8))
+    cpu_val, cpu_desc = _cpu_sample()
+    line = {
+        "metric": "traj-steps/s (2D 256x256 stochastic GPE, MP, FP32 fields + FP64 tables/moments)",
+        "value": value, "unit": "traj-steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64",
+        "data": "synthetic (Philox initial field and noise, seed 0)",
+        "config": {"workload": "gpe_2d: 256x256 periodic, 4096 trajectories (16 blocks x 256), 51 points x 10 "
+                               "steps = 509 MP steps, observable <|a|^2>(x,y,t)",
+                   "global_batch": world * ntraj, "l2": "field 2.1 GB per pass > 126 MB L2",
+                   "parallelism": "dp%d (blocks per rank)" % world},
+        "e2e": {"value": e2e_value, "unit": "traj-steps/s",
+                "h2d_bytes_per_step": int(a_in.numel() * 8), "d2h_bytes_per_step": int(av_host.numel() * 8)},
+        "gpu_launches": gpu_launches * world // max(1, world),
+        "kernels": stats,
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": kind,
+                     "traffic": (tr * ntraj if tr else None),
+                     "algorithmic_bytes_per_launch": alg_bytes},
+        "cpu_baseline": {"value": cpu_val, "unit": "traj-steps/s", "cores": 1, "kind": "port", "sample": cpu_desc},
+        "clocks": clocks,
+    }
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--ntraj", type=int, default=4096, help="trajectories per GPU (multiple of 256)")
+    ap.add_argument("--quick", action="store_true", help="device timing only (no e2e, no CPU sample)")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

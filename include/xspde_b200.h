@@ -133,8 +133,11 @@ XS_API xs_status xs_run_path(xs_handle* h, int first_block, int nblocks, int nc,
 
 /* Same as xs_run_path with device pointers and a caller stream (cudaStream_t
  * passed as void*); nothing is copied to or from the host and the call
- * returns without synchronising.  av_dev uses the layout of av_out;
- * a_in_dev/a_out_dev may be NULL. */
+ * returns without synchronising.  a_in_dev/a_out_dev use the device layout
+ * [ens][fields][space] (identical to the host layout when fields == 1) and
+ * may be NULL.  av_dev receives, per block and output time, one row of
+ * complex FP64 values: site observables' lines k at k*nspace + s (s the
+ * column-major lattice index), then the non-spatial lines. */
 XS_API xs_status xs_run_path_device(xs_handle* h, int first_block, int nblocks, int nc, const double* a_in_dev,
                                     double* av_dev, double* a_out_dev, void* stream);
 
@@ -156,6 +159,27 @@ XS_API xs_status xs_random(xs_handle* h, int block, double* v_out);
  * from time t on a [fields, space, ens1] complex FP64 field, in place, with
  * the pre-scaled noise w [noises, space, ens1] (NULL: zero noise). */
 XS_API xs_status xs_step(xs_handle* h, double* a_inout, const double* w, double t, double dtr);
+
+/* Kernel kinds counted by xs_kernel_stats. */
+enum {
+  XS_KERNEL_RESIDENT = 0, /* whole path with fields in shared memory */
+  XS_KERNEL_OBS_REDUCE,   /* block means of the resident path */
+  XS_KERNEL_X_INIT,       /* streaming: initial field -> K state */
+  XS_KERNEL_X_STEP,       /* streaming: row pass (IFFT_x, drift + noise, FFT_x) */
+  XS_KERNEL_X_FINAL,      /* streaming: K state -> x-space field */
+  XS_KERNEL_Y_PASS,       /* streaming: column pass (FFT_y, exp(L dt), IFFT_y) */
+  XS_KERNEL_X_OBS,        /* streaming: observables */
+  XS_KERNEL_SCALAR,       /* streaming: Int/Ave scalar observables */
+  XS_KERNEL_KINDS
+};
+
+/* Instrumentation (no counterpart in the reference, which has only tic/toc,
+ * Simulator/xsim.m:77): with timing on, every launch of the handle is
+ * bracketed by CUDA events on its stream.  xs_kernel_stats synchronises
+ * that stream and returns, per kernel kind, the launches and the summed
+ * device milliseconds since the last reset (arrays of XS_KERNEL_KINDS). */
+XS_API xs_status xs_set_kernel_timing(xs_handle* h, int on);
+XS_API xs_status xs_kernel_stats(xs_handle* h, int reset, double* ms_out, long long* launches_out);
 
 /* Compile-only check (no device needed): parse and NVRTC-compile the kernels
  * of a problem for sm_100a.  Writes the compile log (truncated to n). */

@@ -25,6 +25,13 @@ Box-Muller pair (Box and Muller, 1958) with uniforms u = (x + 1/2) 2^-32:
   z_even = sqrt(-2 ln u0) cos(2 pi u1),  z_odd = sqrt(-2 ln u0) sin(2 pi u1).
 Component c of the call uses pair (c % 4) // 2 and the cos (even c) or sin
 (odd c) branch.
+
+Site pairing: when there are at most two components and the first space
+dimension has an even number of points N1, one call serves two sites that
+are N1/2 apart along x.  Site s with x index i1 uses the call whose site
+counter is p = (i1 mod N1/2) + (N1/2) (s div N1), words (0,1) when
+i1 < N1/2 and words (2,3) otherwise.  Otherwise each site has its own
+calls, counter s, components in groups of four.
 """
 import numpy as np
 
@@ -62,11 +69,32 @@ def uniform01(x):
     return (x.astype(np.float64) + 0.5) * TWO_M32
 
 
-def normals(ncomp, nspace, nens, draw, block, seed, seq=0):
-    """Standard normals z[c, s, e] for one draw, shape (ncomp, nspace, nens)."""
+def _boxmuller(w0, w1):
+    u0 = uniform01(w0)
+    u1 = uniform01(w1)
+    r = np.sqrt(-2.0 * np.log(u0))
+    th = 2.0 * np.pi * u1
+    return r * np.cos(th), r * np.sin(th)
+
+
+def normals(ncomp, nspace, nens, draw, block, seed, seq=0, n1=1):
+    """Standard normals z[c, s, e] for one draw, shape (ncomp, nspace, nens).
+    n1 is the number of points along the first space dimension (1 for SDEs)."""
     out = np.empty((ncomp, nspace, nens), dtype=np.float64)
-    s = np.arange(nspace, dtype=np.uint64)[:, None]
     e = np.arange(nens, dtype=np.uint64)[None, :]
+    if ncomp <= 2 and n1 > 1 and n1 % 2 == 0 and nspace % n1 == 0:
+        h = n1 // 2
+        s = np.arange(nspace)
+        i1 = s % n1
+        pidx = (i1 % h + h * (s // n1)).astype(np.uint64)[:, None]
+        hi = (i1 >= h)[:, None]
+        w = philox4x32_10(pidx, e, draw, seq << 16, seed, block)
+        za, zb = _boxmuller(np.where(hi, w[2], w[0]), np.where(hi, w[3], w[1]))
+        out[0] = za
+        if ncomp > 1:
+            out[1] = zb
+        return out
+    s = np.arange(nspace, dtype=np.uint64)[:, None]
     for g in range((ncomp + 3) // 4):
         w = philox4x32_10(s, e, draw, g | (seq << 16), seed, block)
         for pair in range(2):

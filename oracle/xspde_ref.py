@@ -721,7 +721,8 @@ def philox_noisegen(w1, nc, s, p):
     from ``p.draw`` which xpath advances once per call."""
     if p.noises <= 0:
         return 0
-    z = philox.normals(p.noises, p.nspace, p.ensembles[0], p.draw, p.block, p.seed, p.get("seq", 0))
+    z = philox.normals(p.noises, p.nspace, p.ensembles[0], p.draw, p.block, p.seed, p.get("seq", 0),
+                       p.space[0] if p.space else 1)
     w = freshape(z, [p.noises] + p.space + [p.ensembles[0]])
     w = w * math.sqrt(s * p.noisefactor)                                 # :32
     if w1 is not None and p.checks[0] and nc == 2:                       # :33-35
@@ -734,7 +735,8 @@ def philox_randomgen(p):
     (xrandom.m:20-23), Philox draw 0."""
     if p.inrandoms <= 0:
         return 0
-    z = philox.normals(p.inrandoms, p.nspace, p.ensembles[0], 0, p.block, p.seed, p.get("seq", 0))
+    z = philox.normals(p.inrandoms, p.nspace, p.ensembles[0], 0, p.block, p.seed, p.get("seq", 0),
+                       p.space[0] if p.space else 1)
     v = freshape(z, [p.inrandoms] + p.space + [p.ensembles[0]])
     return v * math.sqrt(p.noisefactor)
 

@@ -13,7 +13,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libxspde_b200.so")
 CUDA = os.environ.get("CUDA_HOME", "/usr/local/cuda")
-KERNELS = [("prelude", "xs_prelude.cuh"), ("resident", "xs_resident.cuh"), ("stream", "xs_stream.cuh")]
+KERNELS = [("prelude", "xs_prelude.cuh"), ("noise", "xs_noise.cuh"), ("resident", "xs_resident.cuh"),
+           ("stream", "xs_stream.cuh")]
 SOURCES = ["xs_capi.cpp", "xs_expr.cpp", "xs_aot.cu"]
 
 

@@ -218,13 +218,15 @@ __device__ __forceinline__ void xs_boxmuller(u32 x0, u32 x1, real& z0, real& z1)
   z0 = r * c;
   z1 = r * s;
 #else
+  // FP32 fields: hardware approximations (__logf, __sincosf).  The angle is
+  // taken in (-pi, pi): cos(2 pi u) = -cos(2 pi (u - 1/2)), likewise sin.
   const float u0 = ((float)x0 + 0.5f) * 2.3283064365386963e-10f;
-  const float u1 = ((float)x1 + 0.5f) * 2.3283064365386963e-10f;
-  const float r = sqrtf(-2.0f * logf(u0));
+  const float hu = (float)((int)(x1 ^ 0x80000000u)) * 2.3283064365386963e-10f + 1.16415321826934814e-10f;
+  const float r = sqrtf(-2.0f * __logf(u0));
   float s, c;
-  sincospif(2.0f * u1, &s, &c);
-  z0 = r * c;
-  z1 = r * s;
+  __sincosf(6.28318530717958648f * hu, &s, &c);
+  z0 = -r * c;
+  z1 = -r * s;
 #endif
 }
 

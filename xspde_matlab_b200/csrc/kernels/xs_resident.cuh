@@ -207,7 +207,7 @@ __device__ __forceinline__ void xs_noise(real* W, real* Wp, int mode, int draw, 
     const u32 blk = (u32)(P.block0 + e / P.ens1);
     const u32 el = (u32)(e % P.ens1);
     real z[XS_NW];
-    xs_normals<XS_NW>(z, (u32)s, el, (u32)draw, (u32)P.seq, P.seed, blk);
+    xs_normals_site<XS_NW>(z, (u32)s, el, (u32)draw, (u32)P.seq, P.seed, blk);
 #pragma unroll
     for (int c = 0; c < XS_NW; ++c) {
       const int j = (g * XS_NWS + c) * XS_NS + s;
@@ -338,7 +338,7 @@ extern "C" __global__ void __launch_bounds__(XS_THREADS) xs_resident(const XsPat
       xs_site(s, i1, i2, i3, x, y, z);
       real v[XS_NV > 0 ? XS_NV : 1];
 #if XS_NV > 0
-      xs_normals<XS_NV>(v, (u32)s, (u32)(e % P.ens1), 0u, (u32)P.seq, P.seed, (u32)(P.block0 + e / P.ens1));
+      xs_normals_site<XS_NV>(v, (u32)s, (u32)(e % P.ens1), 0u, (u32)P.seq, P.seed, (u32)(P.block0 + e / P.ens1));
 #pragma unroll
       for (int c = 0; c < XS_NV; ++c) v[c] *= (real)P.vscale;
 #endif

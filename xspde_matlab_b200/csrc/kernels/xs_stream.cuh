@@ -59,11 +59,22 @@ template <int R> __device__ __forceinline__ void xs_dftR(cx (&v)[R]);
 
 __device__ __forceinline__ cx xs_cj(cx a) { return mkcx(a.re, -a.im); }
 
-// W_N^(t*k) for the four-step split, N = R*R: tw[t*R + k] = exp(-2 pi i t k / N)
+// True when this launch's dynamic shared memory holds `need` bytes; otherwise
+// the CTA records status bit 1 and must return without touching shared memory.
+__device__ __forceinline__ bool xs_smem_ok(size_t need, int* status) {
+  u32 dyn;
+  asm volatile("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn));
+  if ((size_t)dyn >= need) return true;
+  if (threadIdx.x == 0) atomicOr(status, 2);
+  return false;
+}
+
+// W_N^(t*k) for the four-step split, N = R*R: tw[k*R + t] = exp(-2 pi i t k / N)
+// (t fastest, so the threads of a line read consecutive words).
 template <int R>
 __device__ __forceinline__ void xs_fill_twiddles(cx* tw) {
   for (int i = threadIdx.x; i < R * R; i += blockDim.x) {
-    const int t = i / R, k = i % R;
+    const int k = i / R, t = i % R;
     double s, c;
     sincospi(-2.0 * (double)(t * k) / (double)(R * R), &s, &c);
     tw[i] = mkcx((real)c, (real)s);
@@ -71,28 +82,30 @@ __device__ __forceinline__ void xs_fill_twiddles(cx* tw) {
 }
 
 // Forward DFT of N = R*R points held four-step style: thread t holds v[j] =
-// x[t + R*j].  `buf` is this line's (R x (R+1)) shared-memory scratch; `sync`
+// x[t + R*j].  `buf` is the line's shared-memory scratch: element (k, t) of
+// the R x R transpose lives at buf[(k*R + t)*LS] + padding chosen by the
+// caller through LS (line stride between interleaved lines) and PAD; `sync`
 // is the barrier that covers the threads of the line.  On return v[k2] =
 // X[t + R*k2].
-template <int R, class Sync>
+template <int R, int LS, int PAD, class Sync>
 __device__ __forceinline__ void xs_fft4(cx (&v)[R], int t, const cx* __restrict__ tw, cx* buf, Sync sync) {
   xs_dftR<R>(v);  // v[k1] = sum_j x[t + R j] W_R^(j k1)
 #pragma unroll
-  for (int k = 1; k < R; ++k) v[k] = v[k] * tw[t * R + k];
+  for (int k = 1; k < R; ++k) v[k] = v[k] * tw[k * R + t];
 #pragma unroll
-  for (int k = 0; k < R; ++k) buf[k * (R + 1) + t] = v[k];
+  for (int k = 0; k < R; ++k) buf[(k * (R + PAD) + t) * LS] = v[k];
   sync();
 #pragma unroll
-  for (int n = 0; n < R; ++n) v[n] = buf[t * (R + 1) + n];
+  for (int n = 0; n < R; ++n) v[n] = buf[(t * (R + PAD) + n) * LS];
   sync();
   xs_dftR<R>(v);
 }
 
-template <int R, class Sync>
+template <int R, int LS, int PAD, class Sync>
 __device__ __forceinline__ void xs_ifft4(cx (&v)[R], int t, const cx* __restrict__ tw, cx* buf, Sync sync) {
 #pragma unroll
   for (int k = 0; k < R; ++k) v[k] = xs_cj(v[k]);
-  xs_fft4<R>(v, t, tw, buf, sync);
+  xs_fft4<R, LS, PAD>(v, t, tw, buf, sync);
   const real sc = (real)(1.0 / (double)(R * R));
 #pragma unroll
   for (int k = 0; k < R; ++k) v[k] = mkcx(v[k].re * sc, -v[k].im * sc);
@@ -107,7 +120,8 @@ struct XsBlockSync {
 
 // ---- row passes -------------------------------------------------------------
 // Shared memory: twiddles (RX*RX) + per-row transpose scratch (RX*(RX+1)).
-#define XS_XSMEM (XS_RX * XS_RX + XS_XROWS * XS_RX * (XS_RX + 1))
+#define XS_XLINE (XS_F * XS_RX * XS_RX > XS_RX * (XS_RX + 1) ? XS_F * XS_RX * XS_RX : XS_RX * (XS_RX + 1))
+#define XS_XSMEM (XS_RX * XS_RX + XS_XROWS * XS_XLINE)
 
 __device__ __forceinline__ void xs_row_coords(int y, int t, int j, real& x, real& yy) {
   x = (real)(XS_O1 + XS_DX1 * (double)(t + XS_RX * j));
@@ -124,12 +138,13 @@ __device__ __forceinline__ void xs_xpass_body(const XsStreamArgs& A) {
     if (threadIdx.x == 0) atomicOr(A.status, 2);
     return;
   }
+  if (!xs_smem_ok(XS_XSMEM * sizeof(cx), A.status)) return;
   cx* smem = (cx*)xs_dsmem;
   cx* tw = smem;
   xs_fill_twiddles<XS_RX>(tw);
   __syncthreads();
   const int r = threadIdx.x / XS_RX, t = threadIdx.x % XS_RX;
-  cx* buf = tw + XS_RX * XS_RX + r * XS_RX * (XS_RX + 1);
+  cx* buf = tw + XS_RX * XS_RX + r * XS_XLINE;
   const size_t row = (size_t)blockIdx.x * XS_XROWS + r;  // over ntraj * NY
   const int e = (int)(row / XS_NY), y = (int)(row % XS_NY);
   const u32 blk = (u32)(A.block0 + e / A.ens1), el = (u32)(e % A.ens1);
@@ -152,7 +167,7 @@ __device__ __forceinline__ void xs_xpass_body(const XsStreamArgs& A) {
       } else {
         real vv[XS_NV > 0 ? XS_NV : 1];
 #if XS_NV > 0
-        xs_normals<XS_NV>(vv, (u32)s, el, 0u, (u32)A.seq, A.seed, blk);
+        xs_normals_site<XS_NV>(vv, (u32)s, el, 0u, (u32)A.seq, A.seed, blk);
 #pragma unroll
         for (int c = 0; c < XS_NV; ++c) vv[c] *= (real)A.vscale;
 #endif
@@ -167,33 +182,28 @@ __device__ __forceinline__ void xs_xpass_body(const XsStreamArgs& A) {
 #pragma unroll
       for (int j = 0; j < XS_RX; ++j) v[f][j] = base[(size_t)f * XS_NS + XS_RX * j];
 #pragma unroll
-    for (int f = 0; f < XS_F; ++f) xs_ifft4<XS_RX>(v[f], t, tw, buf, ws);
+    for (int f = 0; f < XS_F; ++f) xs_ifft4<XS_RX, 1, 1>(v[f], t, tw, buf, ws);
   }
   if (MODE == 1) {
-    // MP midpoint iterations (Applications/SDE/MP.m:13-23) at t + dtr/2.
+    // MP midpoint iterations (Applications/SDE/MP.m:13-23) at t + dtr/2.  The
+    // row is staged in this row's shared scratch so that the per-element loop
+    // stays rolled (one copy of the drift/noise code): each thread touches
+    // only its own elements, stage[(f*RX + j)*RX + t].
     const real h = (real)(A.dtr * 0.5);
     const real tm = (real)(A.t + A.dtr * 0.5);
+    cx* stage = buf;
 #pragma unroll
-    for (int j = 0; j < XS_RX; ++j) {
+    for (int f = 0; f < XS_F; ++f)
+#pragma unroll
+      for (int j = 0; j < XS_RX; ++j) stage[(f * XS_RX + j) * XS_RX + t] = v[f][j];
+    // One element: noise w (already scaled and, on a coarse pass, averaged),
+    // midpoint iterations, 2a - a0.
+    auto nl_element = [&](int j, const real* w) {
       real x, yy;
       xs_row_coords(y, t, j, x, yy);
-      const u32 s = (u32)(y * XS_NX + t + XS_RX * j);
-      real w[XS_NW > 0 ? XS_NW : 1];
-#if XS_NW > 0
-      xs_normals<XS_NW>(w, s, el, (u32)A.draw0, (u32)A.seq, A.seed, blk);
-      if (A.draw1 >= 0) {
-        real w2[XS_NW];
-        xs_normals<XS_NW>(w2, s, el, (u32)A.draw1, (u32)A.seq, A.seed, blk);
-#pragma unroll
-        for (int c = 0; c < XS_NW; ++c) w[c] = (w[c] * (real)A.wscale + w2[c] * (real)A.wscale) * (real)0.5;
-      } else {
-#pragma unroll
-        for (int c = 0; c < XS_NW; ++c) w[c] = w[c] * (real)A.wscale;
-      }
-#endif
       cx a0[XS_F], a[XS_F], d[XS_F];
 #pragma unroll
-      for (int f = 0; f < XS_F; ++f) a0[f] = a[f] = v[f][j];
+      for (int f = 0; f < XS_F; ++f) a0[f] = a[f] = stage[(f * XS_RX + j) * XS_RX + t];
 #pragma unroll
       for (int it = 0; it < XS_ITER; ++it) {
         xs_deriv(a, w, x, yy, (real)0, tm, d);
@@ -201,8 +211,59 @@ __device__ __forceinline__ void xs_xpass_body(const XsStreamArgs& A) {
         for (int f = 0; f < XS_F; ++f) a[f] = a0[f] + h * d[f];
       }
 #pragma unroll
-      for (int f = 0; f < XS_F; ++f) v[f][j] = (real)2 * a[f] - a0[f];
+      for (int f = 0; f < XS_F; ++f) stage[(f * XS_RX + j) * XS_RX + t] = (real)2 * a[f] - a0[f];
+    };
+    const real ws = (real)A.wscale;
+#if XS_NW > 0 && XS_PAIRED(XS_NW)
+    // one Philox call per pair of sites (x, x + NX/2) = elements (j, j + RX/2)
+#pragma unroll 1
+    for (int j = 0; j < XS_RX / 2; ++j) {
+      const u32 pidx = (u32)(t + XS_RX * j) + (u32)(XS_NX / 2) * (u32)y;
+      real wl[XS_NW], wh[XS_NW];
+      xs_normals_pair<XS_NW>(wl, wh, pidx, el, (u32)A.draw0, (u32)A.seq, A.seed, blk);
+      if (A.draw1 >= 0) {
+        real wl2[XS_NW], wh2[XS_NW];
+        xs_normals_pair<XS_NW>(wl2, wh2, pidx, el, (u32)A.draw1, (u32)A.seq, A.seed, blk);
+#pragma unroll
+        for (int c = 0; c < XS_NW; ++c) {
+          wl[c] = (wl[c] * ws + wl2[c] * ws) * (real)0.5;
+          wh[c] = (wh[c] * ws + wh2[c] * ws) * (real)0.5;
+        }
+      } else {
+#pragma unroll
+        for (int c = 0; c < XS_NW; ++c) {
+          wl[c] *= ws;
+          wh[c] *= ws;
+        }
+      }
+      nl_element(j, wl);
+      nl_element(j + XS_RX / 2, wh);
     }
+#else
+#pragma unroll 1
+    for (int j = 0; j < XS_RX; ++j) {
+      const u32 s = (u32)(y * XS_NX + t + XS_RX * j);
+      real w[XS_NW > 0 ? XS_NW : 1];
+#if XS_NW > 0
+      xs_normals_site<XS_NW>(w, s, el, (u32)A.draw0, (u32)A.seq, A.seed, blk);
+      if (A.draw1 >= 0) {
+        real w2[XS_NW];
+        xs_normals_site<XS_NW>(w2, s, el, (u32)A.draw1, (u32)A.seq, A.seed, blk);
+#pragma unroll
+        for (int c = 0; c < XS_NW; ++c) w[c] = (w[c] * ws + w2[c] * ws) * (real)0.5;
+      } else {
+#pragma unroll
+        for (int c = 0; c < XS_NW; ++c) w[c] = w[c] * ws;
+      }
+#endif
+      nl_element(j, w);
+    }
+#endif
+#pragma unroll
+    for (int f = 0; f < XS_F; ++f)
+#pragma unroll
+      for (int j = 0; j < XS_RX; ++j) v[f][j] = stage[(f * XS_RX + j) * XS_RX + t];
+    __syncwarp();  // the FFT below reuses the scratch other threads may still read
   }
   if (MODE == 3) {
     bool bad = false;
@@ -220,7 +281,7 @@ __device__ __forceinline__ void xs_xpass_body(const XsStreamArgs& A) {
     return;
   }
 #pragma unroll
-  for (int f = 0; f < XS_F; ++f) xs_fft4<XS_RX>(v[f], t, tw, buf, ws);
+  for (int f = 0; f < XS_F; ++f) xs_fft4<XS_RX, 1, 1>(v[f], t, tw, buf, ws);
 #pragma unroll
   for (int f = 0; f < XS_F; ++f)
 #pragma unroll
@@ -234,18 +295,19 @@ extern "C" __global__ void __launch_bounds__(256) xs_x_final(const XsStreamArgs 
 // ---- column pass ------------------------------------------------------------
 // CTA = TX consecutive kx columns of one (trajectory, component); thread
 // (c = tid % TX, t = tid / TX) holds y = t + RY*j of column c.
-#define XS_SSMEM (XS_RY * XS_RY + XS_TX * XS_RY * (XS_RY + 1))
+#define XS_SSMEM (XS_RY * XS_RY + XS_TX * XS_RY * XS_RY)
 
 extern "C" __global__ void __launch_bounds__(256) xs_s_pass(const XsStreamArgs A) {
   if ((size_t)blockIdx.x >= (size_t)A.ntraj * XS_F * (XS_NX / XS_TX)) {
     if (threadIdx.x == 0) atomicOr(A.status, 2);
     return;
   }
+  if (!xs_smem_ok(XS_SSMEM * sizeof(cx), A.status)) return;
   cx* smem = (cx*)xs_dsmem;
   cx* tw = smem;
   xs_fill_twiddles<XS_RY>(tw);
   const int c = threadIdx.x % XS_TX, t = threadIdx.x / XS_TX;
-  cx* buf = tw + XS_RY * XS_RY + c * XS_RY * (XS_RY + 1);
+  cx* buf = tw + XS_RY * XS_RY + c;  // element (k, t) of column c at ((k*RY + t)*TX + c)
   constexpr int TILES = XS_NX / XS_TX;
   const size_t tile = blockIdx.x;  // over ntraj * F * TILES
   const int x0 = (int)(tile % TILES) * XS_TX;
@@ -257,15 +319,15 @@ extern "C" __global__ void __launch_bounds__(256) xs_s_pass(const XsStreamArgs A
   for (int j = 0; j < XS_RY; ++j) v[j] = base[(size_t)(t + XS_RY * j) * XS_NX];
   __syncthreads();  // twiddles ready
   XsBlockSync bs;
-  xs_fft4<XS_RY>(v, t, tw, buf, bs);
+  xs_fft4<XS_RY, XS_TX, 0>(v, t, tw, buf, bs);
   const double2* P = (A.m == 2 ? A.prop2 : A.prop1) + (XS_PROP_COMPS > 1 ? (size_t)f * XS_NS : 0);
 #pragma unroll
   for (int k = 0; k < XS_RY; ++k) {
-    const double2 pr = P[(size_t)(t + XS_RY * k) * XS_NX + x0 + c];
+    const double2 pr = __ldg(&P[(size_t)(t + XS_RY * k) * XS_NX + x0 + c]);
     const double vr = (double)v[k].re, vi = (double)v[k].im;
     v[k] = mkcx((real)(vr * pr.x - vi * pr.y), (real)(vr * pr.y + vi * pr.x));
   }
-  xs_ifft4<XS_RY>(v, t, tw, buf, bs);
+  xs_ifft4<XS_RY, XS_TX, 0>(v, t, tw, buf, bs);
 #pragma unroll
   for (int j = 0; j < XS_RY; ++j) base[(size_t)(t + XS_RY * j) * XS_NX] = v[j];
 }
@@ -309,7 +371,7 @@ extern "C" __global__ void __launch_bounds__(XS_OROWS * XS_RX) xs_x_obs(const Xs
 #pragma unroll
       for (int j = 0; j < XS_RX; ++j) v[f][j] = base[(size_t)f * XS_NS + XS_RX * j];
 #pragma unroll
-    for (int f = 0; f < XS_F; ++f) xs_ifft4<XS_RX>(v[f], t, tw, buf, ws);
+    for (int f = 0; f < XS_F; ++f) xs_ifft4<XS_RX, 1, 1>(v[f], t, tw, buf, ws);
 #if XS_NRED > 0
     double acc[2 * XS_NRED];
 #pragma unroll

@@ -26,6 +26,7 @@
 #include "xs_expr.hpp"
 
 extern const char* xs_kernel_source_prelude;
+extern const char* xs_kernel_source_noise;
 extern const char* xs_kernel_source_resident;
 extern const char* xs_kernel_source_stream;
 
@@ -629,8 +630,23 @@ struct xs_handle {
   cudaStream_t stream = nullptr;
   DevBuf d_prop[2], d_prop2[2], d_tmat, d_obs, d_av, d_ain, d_aout, d_status, d_w, d_field, d_redpart;
   double prop_dtr[2] = {-1, -1}, prop2_dtr[2] = {-1, -1};
+  // launch accounting (xs_kernel_stats)
+  bool timing = false;
+  long long launches[XS_KERNEL_KINDS] = {};
+  double kms[XS_KERNEL_KINDS] = {};
+  struct Pending {
+    int kind;
+    cudaEvent_t a, b;
+  };
+  std::vector<Pending> pending;
+  std::vector<cudaEvent_t> event_pool;
   std::vector<int> tmat_off;
   ~xs_handle() {
+    for (auto& p : pending) {
+      cudaEventDestroy(p.a);
+      cudaEventDestroy(p.b);
+    }
+    for (auto e : event_pool) cudaEventDestroy(e);
     if (mod && driver().unload) driver().unload(mod);
     if (stream) cudaStreamDestroy(stream);
   }
@@ -749,8 +765,9 @@ void plan_stream(xs_handle& h) {
   sp.TX = 256 / sp.RY;
   sp.OROWS = std::max(1, 64 / sp.RX);
   size_t cxs = h.fp64 ? 16 : 8;
-  sp.xsmem = (size_t)(sp.RX * sp.RX + sp.XROWS * sp.RX * (sp.RX + 1)) * cxs;
-  sp.ssmem = (size_t)(sp.RY * sp.RY + sp.TX * sp.RY * (sp.RY + 1)) * cxs;
+  const size_t xline = std::max<size_t>((size_t)P.F * sp.RX * sp.RX, (size_t)sp.RX * (sp.RX + 1));
+  sp.xsmem = (sp.RX * sp.RX + sp.XROWS * xline) * cxs;
+  sp.ssmem = (size_t)(sp.RY * sp.RY + sp.TX * sp.RY * sp.RY) * cxs;
   sp.osmem = (size_t)(sp.RX * sp.RX + sp.OROWS * sp.RX * (sp.RX + 1)) * cxs;
   if (P.N[1] % sp.XROWS || P.N[1] % sp.OROWS || P.N[0] % sp.TX)
     raise(XS_ERR_SHAPE, "internal: streaming tile sizes do not divide the lattice");
@@ -774,6 +791,7 @@ void emit_common_header(const xs_handle& h, std::ostringstream& os) {
   os << "#define XS_METHOD " << P.p.method << "\n#define XS_ITER " << P.p.iterations << "\n";
   os << "#define XS_HAS_PROP " << ((P.has_linear && P.D > 0) ? 1 : 0) << "\n#define XS_PROP_COMPS " << P.Lc << "\n";
   os << "#define XS_SETBOUND " << (P.setbound ? 1 : 0) << "\n";
+  os << xs_kernel_source_noise << "\n";
 }
 
 void build_source(xs_handle& h) {
@@ -830,6 +848,8 @@ void load_module(xs_handle& h) {
       cu_check(d.getfn(f.f, h.mod, f.name), f.name);
       if (f.smem > 48 * 1024)
         cu_check(d.setattr(*f.f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, (int)f.smem), f.name);
+      // these kernels stage through shared memory and use little L1: prefer shared
+      cu_check(d.setattr(*f.f, CU_FUNC_ATTRIBUTE_PREFERRED_SHARED_MEMORY_CARVEOUT, 100), f.name);
     }
     CUDA_CHECK(cudaStreamCreateWithFlags(&h.stream, cudaStreamNonBlocking));
     h.d_status.ensure(sizeof(int));
@@ -920,6 +940,33 @@ size_t av_doubles_per_block(const Problem& P) {
   return n;
 }
 
+cudaEvent_t take_event(xs_handle& h) {
+  if (!h.event_pool.empty()) {
+    cudaEvent_t e = h.event_pool.back();
+    h.event_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  CUDA_CHECK(cudaEventCreate(&e));
+  return e;
+}
+
+void xs_launch(xs_handle& h, int kind, CUfunction f, unsigned gx, unsigned gy, unsigned gz, unsigned bx,
+               unsigned smem, cudaStream_t st, void** params, const char* what) {
+  cudaEvent_t a = nullptr, b = nullptr;
+  if (h.timing) {
+    a = take_event(h);
+    b = take_event(h);
+    CUDA_CHECK(cudaEventRecord(a, st));
+  }
+  cu_check(driver().launch(f, gx, gy, gz, bx, 1, 1, smem, (CUstream)st, params, nullptr), what);
+  h.launches[kind]++;
+  if (h.timing) {
+    CUDA_CHECK(cudaEventRecord(b, st));
+    h.pending.push_back({kind, a, b});
+  }
+}
+
 // Launch the resident path; av_dev receives [nblocks][npoints][stride] complex.
 void launch_resident(xs_handle& h, int first_block, int nblocks, int nc, const void* a_in_dev, void* av_dev,
                      void* a_out_dev, cudaStream_t st) {
@@ -952,9 +999,8 @@ void launch_resident(xs_handle& h, int first_block, int nblocks, int nc, const v
   a.obs = h.d_obs.p;
   a.status = (int*)h.d_status.p;
   void* params[] = {&a};
-  cu_check(driver().launch(h.f_resident, nctas, 1, 1, h.rp.threads, 1, 1, (unsigned)h.rp.smem, (CUstream)st, params,
-                           nullptr),
-           "launch xs_resident");
+  xs_launch(h, XS_KERNEL_RESIDENT, h.f_resident, nctas, 1, 1, h.rp.threads, (unsigned)h.rp.smem, st, params,
+            "launch xs_resident");
   if (stride > 0) {
     const void* part = h.d_obs.p;
     int ctas_per_block = P.E1 / G;
@@ -962,9 +1008,8 @@ void launch_resident(xs_handle& h, int first_block, int nblocks, int nc, const v
     double inv = 1.0 / P.E1;
     void* rparams[] = {&part, &av_dev, (void*)&npts, (void*)&nctas, &ctas_per_block, &strd, &inv};
     unsigned gx = (unsigned)((stride + 127) / 128);
-    cu_check(driver().launch(h.f_reduce, gx, (unsigned)npts, (unsigned)nblocks, 128, 1, 1, 0, (CUstream)st, rparams,
-                             nullptr),
-             "launch xs_obs_reduce");
+    xs_launch(h, XS_KERNEL_OBS_REDUCE, h.f_reduce, gx, (unsigned)npts, (unsigned)nblocks, 128, 0, st, rparams,
+              "launch xs_obs_reduce");
   }
 }
 
@@ -1031,28 +1076,24 @@ void launch_stream(xs_handle& h, int first_block, int nblocks, int nc, const voi
   a.av = av_dev;
   a.redpart = h.d_redpart.p;
   a.status = (int*)h.d_status.p;
-  Driver& d = driver();
   void* params[] = {&a};
   const unsigned xgrid = (unsigned)((size_t)total * P.N[1] / sp.XROWS);
   const unsigned sgrid = (unsigned)((size_t)total * P.F * (P.N[0] / sp.TX));
-  auto row = [&](CUfunction f) {
-    cu_check(d.launch(f, xgrid, 1, 1, 256, 1, 1, (unsigned)sp.xsmem, (CUstream)st, params, nullptr), "row pass");
+  auto row = [&](int kind, CUfunction f) {
+    xs_launch(h, kind, f, xgrid, 1, 1, 256, (unsigned)sp.xsmem, st, params, "row pass");
   };
   auto col = [&](int m) {
     a.m = m;
-    cu_check(d.launch(h.f_spass, sgrid, 1, 1, 256, 1, 1, (unsigned)sp.ssmem, (CUstream)st, params, nullptr),
-             "column pass");
+    xs_launch(h, XS_KERNEL_Y_PASS, h.f_spass, sgrid, 1, 1, 256, (unsigned)sp.ssmem, st, params, "column pass");
   };
   auto observe = [&](int n) {
     a.n = n;
-    cu_check(d.launch(h.f_xobs, (unsigned)nrg, (unsigned)nblocks, 1, (unsigned)(sp.OROWS * sp.RX), 1, 1,
-                      (unsigned)sp.osmem, (CUstream)st, params, nullptr),
-             "observation pass");
+    xs_launch(h, XS_KERNEL_X_OBS, h.f_xobs, (unsigned)nrg, (unsigned)nblocks, 1, (unsigned)(sp.OROWS * sp.RX),
+              (unsigned)sp.osmem, st, params, "observation pass");
     if (P.nout_scalar)
-      cu_check(d.launch(h.f_scalar, (unsigned)nblocks, 1, 1, 256, 1, 1, 0, (CUstream)st, params, nullptr),
-               "scalar observables");
+      xs_launch(h, XS_KERNEL_SCALAR, h.f_scalar, (unsigned)nblocks, 1, 1, 256, 0, st, params, "scalar observables");
   };
-  row(h.f_xinit);
+  row(XS_KERNEL_X_INIT, h.f_xinit);
   int pending = 0, draw = 0, prev_draw = -1;
   const int npts = P.p.points[0], S = P.p.steps, checks = P.p.checks;
   for (int n = 0; n < npts; ++n) {
@@ -1067,7 +1108,7 @@ void launch_stream(xs_handle& h, int first_block, int nblocks, int nc, const voi
           col(pending + 1);
           a.draw0 = draw;
           a.draw1 = (nc == 2 && checks) ? prev_draw : -1;
-          row(h.f_xnl);
+          row(XS_KERNEL_X_STEP, h.f_xnl);
           a.t += a.dtr;
           pending = 1;
         }
@@ -1081,7 +1122,7 @@ void launch_stream(xs_handle& h, int first_block, int nblocks, int nc, const voi
   }
   if (a_out_dev) {
     if (pending) col(pending);
-    row(h.f_xfinal);
+    row(XS_KERNEL_X_FINAL, h.f_xfinal);
   }
 }
 
@@ -1283,6 +1324,42 @@ XS_API xs_status xs_sync(xs_handle* h) {
     CUDA_CHECK(cudaMemcpy(&status, h->d_status.p, sizeof(int), cudaMemcpyDeviceToHost));
     if (status & 2) raise(XS_ERR_SHAPE, "kernel refused a launch whose shared-memory layout or grid did not match");
     if (status & 1) raise(XS_ERR_NAN, "a trajectory became non-finite (NaN/Inf) during the path");
+    return XS_OK;
+  });
+}
+
+XS_API xs_status xs_set_kernel_timing(xs_handle* h, int on) {
+  if (!h) {
+    g_err = "null handle";
+    return XS_ERR_ARG;
+  }
+  h->timing = on != 0;
+  return XS_OK;
+}
+
+XS_API xs_status xs_kernel_stats(xs_handle* h, int reset, double* ms_out, long long* launches_out) {
+  return guard([&]() -> xs_status {
+    if (!h) raise(XS_ERR_ARG, "null handle");
+    if (!h->pending.empty()) {
+      CUDA_CHECK(cudaStreamSynchronize(h->stream));
+      CUDA_CHECK(cudaDeviceSynchronize());
+      for (auto& p : h->pending) {
+        float ms = 0;
+        CUDA_CHECK(cudaEventElapsedTime(&ms, p.a, p.b));
+        h->kms[p.kind] += ms;
+        h->event_pool.push_back(p.a);
+        h->event_pool.push_back(p.b);
+      }
+      h->pending.clear();
+    }
+    for (int k = 0; k < XS_KERNEL_KINDS; ++k) {
+      if (ms_out) ms_out[k] = h->kms[k];
+      if (launches_out) launches_out[k] = h->launches[k];
+      if (reset) {
+        h->kms[k] = 0;
+        h->launches[k] = 0;
+      }
+    }
     return XS_OK;
   });
 }

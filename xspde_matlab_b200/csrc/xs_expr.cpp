@@ -756,6 +756,19 @@ struct Gen {
       }
       case NK::Un: return un(n->name, gen(n->kids[0]));
       case NK::Bin: {
+        // abs(x).^2 and abs(x)^2 -> |x|^2 without the square root
+        if ((n->name == ".^" || n->name == "^") && n->kids[0]->kind == NK::Index && n->kids[0]->kids.size() == 2 &&
+            n->kids[0]->kids[0]->kind == NK::Var && n->kids[0]->kids[0]->name == "abs") {
+          Vec e;
+          if (try_const(n->kids[1], e) && e.size() == 1 && e[0] == C(2.0)) {
+            Val v = gen(n->kids[0]->kids[1]);
+            Val r;
+            r.len = v.len;
+            r.spatial = v.spatial;
+            for (auto& c2 : v.c) r.c.push_back(tmp(false, "xs_abs2(" + c2 + ")"));
+            return r;
+          }
+        }
         // conj(x).*x and x.*conj(x) -> |x|^2 (real)
         if (n->name == ".*" || n->name == "*") {
           if (is_conj_of(n->kids[0], n->kids[1]) || is_conj_of(n->kids[1], n->kids[0])) {
