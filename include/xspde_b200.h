@@ -141,6 +141,27 @@ XS_API xs_status xs_run_path(xs_handle* h, int first_block, int nblocks, int nc,
 XS_API xs_status xs_run_path_device(xs_handle* h, int first_block, int nblocks, int nc, const double* a_in_dev,
                                     double* av_dev, double* a_out_dev, void* stream);
 
+/* xs_run_path_device for callers that cannot allocate device memory: no
+ * counterpart in the reference.  A MATLAB MEX function that must leave device
+ * memory to MATLAB's own gpuArray allocator, code recorded into a CUDA graph,
+ * or a service whose memory budget is fixed after start-up may not call
+ * cudaMalloc; this entry point calls no cudaMalloc, cudaFree or allocating
+ * library routine.  It runs the resident path (problems whose per-trajectory
+ * field fits in shared memory) with the observable partial sums in a fixed
+ * 16 MiB device array inside the library (1,048,576 complex FP64 values);
+ * launches that need more -- points(1) x (trajectories / trajectories per
+ * CTA) x row length -- are rejected with XS_ERR_SHAPE, and a streaming-path
+ * handle with XS_ERR_UNSUPPORTED.  The handle must already hold its tables
+ * for check pass nc: call xs_run_path or xs_run_path_device once with the
+ * same nc first (those calls allocate).  The first call on each device looks
+ * up the array's device address (cudaGetSymbolAddress) and should come before
+ * any stream capture.  Every call shares the one array per device, so calls
+ * that overlap on the GPU race; nothing in it needs to start at zero, since
+ * each call writes every element it later reads.  The initial field comes
+ * from p.initial on the device; av_dev is as for xs_run_path_device. */
+XS_API xs_status xs_run_path_device_noalloc(xs_handle* h, int first_block, int nblocks, int nc, double* av_dev,
+                                            void* stream);
+
 /* Wait for the handle's work and report device-side status (XS_ERR_NAN when a
  * trajectory became non-finite in the last run). */
 XS_API xs_status xs_sync(xs_handle* h);

@@ -16,7 +16,7 @@ MAXDIM = 4
 # Every symbol include/xspde_b200.h declares.
 EXPORTS = ["xs_create", "xs_destroy", "xs_last_error", "xs_version", "xs_observe_info", "xs_av_doubles_per_block",
            "xs_run_path", "xs_run_path_device", "xs_sync", "xs_noise", "xs_random", "xs_step", "xs_compile_check",
-           "xs_set_kernel_timing", "xs_kernel_stats"]
+           "xs_set_kernel_timing", "xs_kernel_stats", "xs_run_path_device_noalloc"]
 KERNEL_KINDS = ["resident", "obs_reduce", "x_init", "x_step", "x_final", "y_pass", "x_obs", "scalar"]
 
 
@@ -99,6 +99,9 @@ def lib():
         L.xs_set_kernel_timing.restype = ctypes.c_int
         L.xs_kernel_stats.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
         L.xs_kernel_stats.restype = ctypes.c_int
+        L.xs_run_path_device_noalloc.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                 ctypes.c_void_p, ctypes.c_void_p]
+        L.xs_run_path_device_noalloc.restype = ctypes.c_int
         _ = dp
         _lib = L
     return _lib

@@ -24,6 +24,7 @@
 #include <vector>
 
 #include "xs_expr.hpp"
+#include "xs_noalloc.hpp"
 
 extern const char* xs_kernel_source_prelude;
 extern const char* xs_kernel_source_noise;
@@ -1324,6 +1325,81 @@ XS_API xs_status xs_sync(xs_handle* h) {
     CUDA_CHECK(cudaMemcpy(&status, h->d_status.p, sizeof(int), cudaMemcpyDeviceToHost));
     if (status & 2) raise(XS_ERR_SHAPE, "kernel refused a launch whose shared-memory layout or grid did not match");
     if (status & 1) raise(XS_ERR_NAN, "a trajectory became non-finite (NaN/Inf) during the path");
+    return XS_OK;
+  });
+}
+
+// Resident path with its observable partial sums in the library's fixed
+// device scratch (xs_noalloc.cu) instead of handle-owned memory.  Uses only
+// tables the handle already holds; allocates nothing.
+XS_API xs_status xs_run_path_device_noalloc(xs_handle* h, int first_block, int nblocks, int nc, double* av_dev,
+                                            void* stream) {
+  return guard([&]() -> xs_status {
+    if (!h || nblocks < 1 || first_block < 0 || (nc != 1 && nc != 2) || !av_dev)
+      raise(XS_ERR_ARG, "bad arguments to xs_run_path_device_noalloc");
+    const Problem& P = h->P;
+    if (h->kind != 1)
+      raise(XS_ERR_UNSUPPORTED, "xs_run_path_device_noalloc covers problems on the resident path only");
+    if (nc == 2 && !P.p.checks) raise(XS_ERR_ARG, "coarse pass requested without checks");
+    const int slot = nc == 2 ? 1 : 0;
+    if (!h->loaded || !h->d_prop[slot].p || (P.has_linear && h->prop_dtr[slot] != pass_dtr(P, nc)))
+      raise(XS_ERR_ARG,
+            "handle not prepared for this check pass: call xs_run_path or xs_run_path_device once with the same "
+            "nc first (that call allocates the handle's tables)");
+    const int total = nblocks * P.E1;
+    const int G = h->rp.G;
+    const int nctas = total / G;
+    const size_t stride = av_stride(P);
+    const int npts = P.p.points[0];
+    const size_t need = (size_t)npts * nctas * stride;
+    if (need > XS_NOALLOC_SCRATCH_DOUBLE2)
+      raise(XS_ERR_SHAPE, "xs_run_path_device_noalloc needs " + std::to_string(need) +
+                              " complex FP64 scratch values for this launch; the fixed scratch holds " +
+                              std::to_string((size_t)XS_NOALLOC_SCRATCH_DOUBLE2) + " (16 MiB): use fewer blocks per call");
+    void* scratch = nullptr;
+    cudaError_t e = xs_noalloc_scratch_address(&scratch);
+    if (e != cudaSuccess) raise(XS_ERR_CUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
+    cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
+    CUDA_CHECK(cudaMemsetAsync(h->d_status.p, 0, sizeof(int), st));
+    PathArgsHost a{};
+    a.ntraj = total;
+    a.ens1 = P.E1;
+    a.block0 = first_block;
+    a.nc = nc;
+    a.checks = P.p.checks;
+    a.npoints = npts;
+    a.steps = P.p.steps;
+    a.seq = 0;
+    a.seed = (unsigned)(P.p.seed & 0xffffffffu);
+    a.wscale = std::sqrt(P.nscale * P.noisefactor);
+    a.vscale = std::sqrt(P.noisefactor);
+    a.dtr = pass_dtr(P, nc);
+    a.t0 = P.p.origins[0];
+    a.prop = h->d_prop[slot].p;
+    a.tmat = h->d_tmat.p;
+    for (int i = 0; i < 4; ++i) a.tmat_off[i] = h->tmat_off[i];
+    a.a_in = nullptr;
+    a.a_out = nullptr;
+    a.obs = scratch;
+    a.status = (int*)h->d_status.p;
+    void* params[] = {&a};
+    cu_check(driver().launch(h->f_resident, nctas, 1, 1, h->rp.threads, 1, 1, (unsigned)h->rp.smem, (CUstream)st,
+                             params, nullptr),
+             "launch xs_resident (no-alloc)");
+    h->launches[XS_KERNEL_RESIDENT]++;
+    if (stride > 0) {
+      const void* part = scratch;
+      void* av = av_dev;
+      int ctas_per_block = P.E1 / G;
+      int strd = (int)stride;
+      double inv = 1.0 / P.E1;
+      int np = npts, nct = nctas;
+      void* rparams[] = {&part, &av, &np, &nct, &ctas_per_block, &strd, &inv};
+      cu_check(driver().launch(h->f_reduce, (unsigned)((stride + 127) / 128), (unsigned)npts, (unsigned)nblocks, 128,
+                               1, 1, 0, (CUstream)st, rparams, nullptr),
+               "launch xs_obs_reduce (no-alloc)");
+      h->launches[XS_KERNEL_OBS_REDUCE]++;
+    }
     return XS_OK;
   });
 }
