@@ -38,3 +38,31 @@ __device__ __forceinline__ void xs_normals_pair(real* zlo, real* zhi, u32 p, u32
   zhi[0] = b0;
   if (NC > 1) zhi[NC > 1 ? 1 : 0] = b1;
 }
+
+// p.noisegen / p.randomgen export (Simulator/xnoise.m:29-32, xrandom.m:20-23):
+// out[c + NC (s + NS e)] = z_c(s, e) * scale for one block and draw, in the
+// MATLAB layout [components, space, ens1].
+template <int NC>
+__device__ __forceinline__ void xs_export_normals(double* __restrict__ out, int ens1, u32 block, u32 draw, u32 seq,
+                                                  u32 seed, double scale) {
+  const size_t total = (size_t)XS_NS * (size_t)ens1;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+    const u32 s = (u32)(i % XS_NS), e = (u32)(i / XS_NS);
+    real z[NC > 0 ? NC : 1];
+    xs_normals_site<NC>(z, s, e, draw, seq, seed, block);
+#pragma unroll
+    for (int c = 0; c < NC; ++c) out[(size_t)c + (size_t)NC * i] = (double)z[c] * scale;
+  }
+}
+extern "C" __global__ void xs_export_noise(double* out, int ens1, u32 block, u32 draw, u32 seq, u32 seed,
+                                           double scale) {
+#if XS_NW > 0
+  xs_export_normals<XS_NW>(out, ens1, block, draw, seq, seed, scale);
+#endif
+}
+extern "C" __global__ void xs_export_random(double* out, int ens1, u32 block, u32 draw, u32 seq, u32 seed,
+                                            double scale) {
+#if XS_NV > 0
+  xs_export_normals<XS_NV>(out, ens1, block, draw, seq, seed, scale);
+#endif
+}

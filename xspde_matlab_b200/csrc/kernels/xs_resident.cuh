@@ -31,6 +31,9 @@ struct XsPathArgs {
   double2* a_out;       // optional [ntraj][F][NS] final field (FP64)
   double2* obs;         // [npoints][nctas][XS_OBS_STRIDE] observable partial sums
   int* status;          // bit 0: non-finite field
+  int single_step;      // 1: one method step from t0 with the noise w_in (p.method)
+  int pad1;
+  const double* w_in;   // [NW, space, ens1] pre-scaled noise for single_step (null: zero)
 };
 
 #define XS_STRIDE1 1
@@ -349,6 +352,18 @@ extern "C" __global__ void __launch_bounds__(XS_THREADS) xs_resident(const XsPat
   }
   __syncthreads();
 
+  if (P.single_step) {
+    // p.method(a, w, p) on the given noise (Simulator/xpath.m:150)
+    for (int i = threadIdx.x; i < XS_G * XS_NS; i += blockDim.x) {
+      const int g = i / XS_NS, s = i % XS_NS;
+      const size_t e = (size_t)(g0 + g);
+#pragma unroll
+      for (int c = 0; c < XS_NW; ++c)
+        W[(g * XS_NWS + c) * XS_NS + s] = P.w_in ? (real)P.w_in[c + (size_t)XS_NW * (s + (size_t)XS_NS * e)] : (real)0;
+    }
+    __syncthreads();
+    xs_method(A, B1, B2, B3, T, W, P, P.t0);
+  } else {
   double t = P.t0;
   int draw = 0;
   for (int n = 0; n < P.npoints; ++n) {
@@ -371,6 +386,7 @@ extern "C" __global__ void __launch_bounds__(XS_THREADS) xs_resident(const XsPat
         xs_observe(A, RED, n, t, P, wsum);
       }
     }
+  }
   }
   __syncthreads();
   // final field and non-finite check

@@ -623,13 +623,14 @@ struct xs_handle {
   // device state
   bool loaded = false;
   CUmodule mod = nullptr;
-  CUfunction f_resident = nullptr, f_reduce = nullptr, f_noise = nullptr;
+  CUfunction f_resident = nullptr, f_reduce = nullptr, f_noise = nullptr, f_random = nullptr;
   CUfunction f_xinit = nullptr, f_xnl = nullptr, f_xfinal = nullptr, f_spass = nullptr, f_xobs = nullptr,
              f_scalar = nullptr;
   StreamPlan sp;
   int path_kind = 0;
   cudaStream_t stream = nullptr;
-  DevBuf d_prop[2], d_prop2[2], d_tmat, d_obs, d_av, d_ain, d_aout, d_status, d_w, d_field, d_redpart;
+  DevBuf d_prop[2], d_prop2[2], d_tmat, d_obs, d_av, d_ain, d_aout, d_status, d_w, d_field, d_redpart, d_pstep;
+  double pstep_dtr = -1;
   double prop_dtr[2] = {-1, -1}, prop2_dtr[2] = {-1, -1};
   // launch accounting (xs_kernel_stats)
   bool timing = false;
@@ -845,6 +846,8 @@ void load_module(xs_handle& h) {
     } fns[] = {{&h.f_xinit, "xs_x_init", h.sp.xsmem}, {&h.f_xnl, "xs_x_nl", h.sp.xsmem},
                {&h.f_xfinal, "xs_x_final", h.sp.xsmem}, {&h.f_spass, "xs_s_pass", h.sp.ssmem},
                {&h.f_xobs, "xs_x_obs", h.sp.osmem}, {&h.f_scalar, "xs_stream_scalar", 0}};
+    cu_check(d.getfn(&h.f_noise, h.mod, "xs_export_noise"), "xs_export_noise");
+    cu_check(d.getfn(&h.f_random, h.mod, "xs_export_random"), "xs_export_random");
     for (auto& f : fns) {
       cu_check(d.getfn(f.f, h.mod, f.name), f.name);
       if (f.smem > 48 * 1024)
@@ -862,6 +865,8 @@ void load_module(xs_handle& h) {
   cu_check(d.load(&h.mod, cubin.data()), "cuModuleLoadData");
   cu_check(d.getfn(&h.f_resident, h.mod, "xs_resident"), "cuModuleGetFunction(xs_resident)");
   cu_check(d.getfn(&h.f_reduce, h.mod, "xs_obs_reduce"), "cuModuleGetFunction(xs_obs_reduce)");
+  cu_check(d.getfn(&h.f_noise, h.mod, "xs_export_noise"), "cuModuleGetFunction(xs_export_noise)");
+  cu_check(d.getfn(&h.f_random, h.mod, "xs_export_random"), "cuModuleGetFunction(xs_export_random)");
   if (h.rp.smem > 48 * 1024)
     cu_check(d.setattr(h.f_resident, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, (int)h.rp.smem),
              "cuFuncSetAttribute(max dynamic smem)");
@@ -931,6 +936,9 @@ struct PathArgsHost {
   void* a_out;
   void* obs;
   int* status;
+  int single_step;
+  int pad1;
+  const double* w_in;
 };
 
 size_t av_stride(const Problem& P) { return (size_t)P.nout_site * P.NS + P.nout_scalar; }
@@ -1440,20 +1448,117 @@ XS_API xs_status xs_kernel_stats(xs_handle* h, int reset, double* ms_out, long l
   });
 }
 
+namespace {
+xs_status export_normals(xs_handle* h, bool random, int block, int draw, double scale, double* out) {
+  return guard([&]() -> xs_status {
+    if (!h || block < 0 || draw < 0 || !out) raise(XS_ERR_ARG, "bad arguments");
+    load_module(*h);
+    const Problem& P = h->P;
+    const int nc = random ? P.NV : P.NW;
+    const size_t n = (size_t)nc * P.NS * P.E1;
+    if (n == 0) return XS_OK;
+    h->d_w.ensure(n * 8);
+    unsigned blk = (unsigned)block, dr = (unsigned)draw, seq = 0, seed = (unsigned)(P.p.seed & 0xffffffffu);
+    int ens1 = P.E1;
+    void* dp = h->d_w.p;
+    void* params[] = {&dp, &ens1, &blk, &dr, &seq, &seed, &scale};
+    unsigned grid = (unsigned)std::min<size_t>((n / nc + 255) / 256, 148 * 16);
+    xs_launch(*h, XS_KERNEL_RESIDENT, random ? h->f_random : h->f_noise, grid, 1, 1, 256, 0, h->stream, params,
+              "noise export");
+    h->launches[XS_KERNEL_RESIDENT]--;  // not a path launch
+    CUDA_CHECK(cudaMemcpyAsync(out, h->d_w.p, n * 8, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_CHECK(cudaStreamSynchronize(h->stream));
+    return XS_OK;
+  });
+}
+}  // namespace
+
 XS_API xs_status xs_noise(xs_handle* h, int block, int draw, double scale, double* w_out) {
-  (void)h; (void)block; (void)draw; (void)scale; (void)w_out;
-  g_err = "xs_noise: not available yet";
-  return XS_ERR_UNSUPPORTED;
+  if (!h) {
+    g_err = "null handle";
+    return XS_ERR_ARG;
+  }
+  return export_normals(h, false, block, draw, std::sqrt(scale * h->P.noisefactor), w_out);  // xnoise.m:32
 }
 
 XS_API xs_status xs_random(xs_handle* h, int block, double* v_out) {
-  (void)h; (void)block; (void)v_out;
-  g_err = "xs_random: not available yet";
-  return XS_ERR_UNSUPPORTED;
+  if (!h) {
+    g_err = "null handle";
+    return XS_ERR_ARG;
+  }
+  return export_normals(h, true, block, 0, std::sqrt(h->P.noisefactor), v_out);  // xrandom.m:23
 }
 
 XS_API xs_status xs_step(xs_handle* h, double* a_inout, const double* w, double t, double dtr) {
-  (void)h; (void)a_inout; (void)w; (void)t; (void)dtr;
-  g_err = "xs_step: not available yet";
-  return XS_ERR_UNSUPPORTED;
+  return guard([&]() -> xs_status {
+    if (!h || !a_inout || !(dtr > 0)) raise(XS_ERR_ARG, "bad arguments to xs_step");
+    if (h->kind != 1) raise(XS_ERR_UNSUPPORTED, "xs_step covers problems on the resident path only");
+    load_module(*h);
+    const Problem& P = h->P;
+    const size_t ntraj = (size_t)P.E1;
+    const size_t fbytes = ntraj * P.F * P.NS * 16;
+    // exp(L dtr/ipsteps) for this step (xpropfactor.m:28-39)
+    if (P.has_linear && h->pstep_dtr != dtr) {
+      std::vector<cd> pr(P.L.size());
+      for (size_t i = 0; i < P.L.size(); ++i) pr[i] = std::exp(P.L[i] * (dtr / P.p.ipsteps));
+      h->d_pstep.ensure(pr.size() * 16);
+      CUDA_CHECK(cudaMemcpy(h->d_pstep.p, pr.data(), pr.size() * 16, cudaMemcpyHostToDevice));
+      h->pstep_dtr = dtr;
+    } else if (!P.has_linear) {
+      h->d_pstep.ensure(16);
+    }
+    std::vector<double> tmp(ntraj * P.F * P.NS * 2);
+    for (size_t e = 0; e < ntraj; ++e)
+      for (int f = 0; f < P.F; ++f)
+        for (int s = 0; s < P.NS; ++s) {
+          size_t src = (f + (size_t)P.F * (s + (size_t)P.NS * e)) * 2, dst = ((e * P.F + f) * P.NS + s) * 2;
+          tmp[dst] = a_inout[src];
+          tmp[dst + 1] = a_inout[src + 1];
+        }
+    h->d_ain.ensure(fbytes);
+    h->d_aout.ensure(fbytes);
+    CUDA_CHECK(cudaMemcpyAsync(h->d_ain.p, tmp.data(), fbytes, cudaMemcpyHostToDevice, h->stream));
+    const size_t wn = (size_t)P.NW * P.NS * ntraj;
+    if (w && wn) {
+      h->d_w.ensure(wn * 8);
+      CUDA_CHECK(cudaMemcpyAsync(h->d_w.p, w, wn * 8, cudaMemcpyHostToDevice, h->stream));
+    }
+    h->d_obs.ensure(16);
+    CUDA_CHECK(cudaMemsetAsync(h->d_status.p, 0, sizeof(int), h->stream));
+    PathArgsHost a{};
+    a.ntraj = (int)ntraj;
+    a.ens1 = P.E1;
+    a.nc = 1;
+    a.npoints = 0;
+    a.steps = 1;
+    a.seed = (unsigned)(P.p.seed & 0xffffffffu);
+    a.dtr = dtr;
+    a.t0 = t;
+    a.prop = h->d_pstep.p;
+    a.tmat = h->d_tmat.p;
+    for (int i = 0; i < 4; ++i) a.tmat_off[i] = h->tmat_off[i];
+    a.a_in = h->d_ain.p;
+    a.a_out = h->d_aout.p;
+    a.obs = h->d_obs.p;
+    a.status = (int*)h->d_status.p;
+    a.single_step = 1;
+    a.w_in = (w && wn) ? (const double*)h->d_w.p : nullptr;
+    void* params[] = {&a};
+    xs_launch(*h, XS_KERNEL_RESIDENT, h->f_resident, (unsigned)(ntraj / h->rp.G), 1, 1, h->rp.threads,
+              (unsigned)h->rp.smem, h->stream, params, "launch xs_resident (step)");
+    int status = 0;
+    CUDA_CHECK(cudaMemcpyAsync(tmp.data(), h->d_aout.p, fbytes, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_CHECK(cudaMemcpyAsync(&status, h->d_status.p, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_CHECK(cudaStreamSynchronize(h->stream));
+    for (size_t e = 0; e < ntraj; ++e)
+      for (int f = 0; f < P.F; ++f)
+        for (int s = 0; s < P.NS; ++s) {
+          size_t dst = (f + (size_t)P.F * (s + (size_t)P.NS * e)) * 2, src = ((e * P.F + f) * P.NS + s) * 2;
+          a_inout[dst] = tmp[src];
+          a_inout[dst + 1] = tmp[src + 1];
+        }
+    if (status & 2) raise(XS_ERR_SHAPE, "kernel refused a launch whose shared-memory layout or grid did not match");
+    if (status & 1) raise(XS_ERR_NAN, "a trajectory became non-finite (NaN/Inf) during the step");
+    return XS_OK;
+  });
 }

@@ -258,6 +258,42 @@ class GpuPath:
         return av, aout
 
 
+def _hook_methods():
+    """p.noisegen / p.randomgen / p.method replacements on a GpuPath."""
+
+    def noise(self, block, draw, scale):
+        """One p.noisegen draw (Simulator/xnoise.m:29-32) before any coarse
+        averaging: [noises, space..., ens1] real."""
+        P = self.p
+        out = np.empty([P.noises] + list(P.space) + [P.ensembles[0]], dtype=np.float64, order="F")
+        _lib.check(_lib.lib().xs_noise(self.h, block, draw, float(scale), out.ctypes.data))
+        return out
+
+    def random(self, block):
+        """p.randomgen (Simulator/xrandom.m:20-23): [inrandoms, space..., ens1] real."""
+        P = self.p
+        out = np.empty([P.inrandoms] + list(P.space) + [P.ensembles[0]], dtype=np.float64, order="F")
+        _lib.check(_lib.lib().xs_random(self.h, block, out.ctypes.data))
+        return out
+
+    def step(self, a, w, t, dtr):
+        """p.method(a, w, p) for one block of trajectories: returns the new field."""
+        a = np.array(a, dtype=np.complex128, order="F", copy=True)
+        wp = None
+        if w is not None:
+            wp = np.asfortranarray(np.asarray(w, dtype=np.float64))
+        _lib.check(_lib.lib().xs_step(self.h, a.ctypes.data, wp.ctypes.data if wp is not None else None,
+                                      float(t), float(dtr)))
+        return a
+
+    GpuPath.noise = noise
+    GpuPath.random = random
+    GpuPath.step = step
+
+
+_hook_methods()
+
+
 def _xcompress(n, data, p, xk):
     """Axis reduction of an output array (Applications/SPDE/xcompress.m:142-194)."""
     axes = list(p.axes[n])
