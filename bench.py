@@ -36,6 +36,7 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+METRIC = "traj-steps/s (2D 256x256 stochastic GPE, MP, 4096 trajectories)"
 HBM_FALLBACK_GBS = 6650.0
 # DRAM bytes per launch of the dominant kernels from one ncu capture of a
 # 512-trajectory case of the same problem, scaled to 4096 trajectories (traffic
@@ -109,6 +110,13 @@ class Clocks:
                 "samples": len(sm)}
 
 
+def _config(ntraj, world):
+    return {"workload": "gpe_2d: 256x256 periodic, %d trajectories per GPU (%d blocks x 256), 51 points x 10 steps"
+                        " = 509 MP steps, observable <|a|^2>(x,y,t)" % (ntraj, ntraj // 256),
+            "global_batch": world * ntraj, "l2": "field 2.1 GB per pass > 126 MB L2 (no flush needed)",
+            "parallelism": "dp%d (blocks per rank)" % world}
+
+
 def _problem(ntraj=4096):
     from xspde_matlab_b200.problems import GPE_2D
     p = dict(GPE_2D)
@@ -180,11 +188,10 @@ def run_reference(args, rank, world):
     value = statistics.mean(r for r, _ in per_step)
     ms = 1000 * statistics.mean(d for _, d in per_step)
     line = {
-        "impl": "reference", "metric": "traj-steps/s (2D 256x256 stochastic GPE, MP)", "value": value,
+        "impl": "reference", "metric": METRIC, "value": value,
         "unit": "traj-steps/s", "n_gpus": 0, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
-        "config": {"workload": "gpe_2d 256x256, 4096 traj, 509 MP steps (bounded CPU sample per step)",
-                   "parallelism": "host processes"},
+        "config": dict(_config(4096, 1), parallelism="host processes (bounded sample per step)"),
         "cpu_baseline": {"value": value, "unit": "traj-steps/s", "cores": cores, "kind": "port",
                          "sample": "per core: 2 trajectories x ~4 s of MP steps of the 256x256 problem; MATLAB "
                                    "reference unavailable on this box (no MATLAB/Octave)"},
@@ -296,14 +303,11 @@ def run_ours(args, rank, world, local_rank):
     gpu_launches = sum(int(kl[i]) for i in range(8))
     cpu_val, cpu_desc = _cpu_sample()
     line = {
-        "metric": "traj-steps/s (2D 256x256 stochastic GPE, MP, FP32 fields + FP64 tables/moments)",
+        "metric": METRIC,
         "value": value, "unit": "traj-steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64",
         "data": "synthetic (Philox initial field and noise, seed 0)",
-        "config": {"workload": "gpe_2d: 256x256 periodic, 4096 trajectories (16 blocks x 256), 51 points x 10 "
-                               "steps = 509 MP steps, observable <|a|^2>(x,y,t)",
-                   "global_batch": world * ntraj, "l2": "field 2.1 GB per pass > 126 MB L2",
-                   "parallelism": "dp%d (blocks per rank)" % world},
+        "config": _config(ntraj, world),
         "e2e": {"value": e2e_value, "unit": "traj-steps/s",
                 "h2d_bytes_per_step": int(a_in.numel() * 8), "d2h_bytes_per_step": int(av_host.numel() * 8)},
         "gpu_launches": gpu_launches * world // max(1, world),

@@ -334,9 +334,12 @@ def _grid(xk):
     return q
 
 
-def _ensembles(inp, paths):
+def _ensembles(inp, paths, rank=0, size=1, reduce=None):
     """Block loop, check passes and moments (Simulator/xensemble.m:12-108) with
-    all blocks of a pass integrated by one device call."""
+    all blocks of a pass integrated by one device call.  With size > 1 this
+    rank integrates its own contiguous share of the blocks and `reduce` sums
+    the moment accumulators over the ranks (Simulator/xsim.m:99-106)."""
+    from .dist import shard
     p1 = inp[0]
     nb = p1.ensembles[1] * p1.ensembles[2]
     m = p1.nchk
@@ -346,9 +349,10 @@ def _ensembles(inp, paths):
     for s, p in enumerate(inp):
         data.append([None] * len(p.output))
     D = {}
+    lo, hi = shard(nb, rank, size)
     chunk = max(1, min(nb, int(2 ** 27 // max(1, paths[0].per_block * 8))))
-    for b0 in range(0, nb, chunk):
-        nbk = min(chunk, nb - b0)
+    for b0 in range(lo, hi, chunk):
+        nbk = min(chunk, hi - b0)
         prev = None
         for nc in range(1, p1.nchk + 1):
             prev = None
@@ -372,6 +376,18 @@ def _ensembles(inp, paths):
                         data[s][o][:, n1 - 1] += D[(s, b, n1, o)] * inv
                     data[s][o][:, m1 - 1] += D[(s, b, 1, o)] ** 2 * inv
         D.clear()
+    if size > 1:
+        for s, p in enumerate(inp):
+            for o in range(len(p.output)):
+                if data[s][o] is None:  # a rank without blocks: sizes from the output shapes
+                    data[s][o] = np.zeros((int(np.prod(p.gpoints[o][:-1])), m1))
+        flat = [x for row in data for x in row]
+        flat = reduce(flat)
+        pos = 0
+        for s in range(len(data)):
+            for o in range(len(data[s])):
+                data[s][o] = flat[pos]
+                pos += 1
     return data
 
 
@@ -395,7 +411,15 @@ def xsim(*inputs, path_kind=0):
             g = _fsize(p.output[o](O, p))
             p.gpoints.append(g + [max(3, 1 + p.nchk)])
         p.xk = [[p.xc[0]] + [p.xc[d] for d in range(1, len(p.points))] for _ in p.output]
-    data = _ensembles(inp, paths)
+    from .dist import allreduce_sum, world
+    rank, size, group = world()
+    dev = None
+    if size > 1:
+        import torch.distributed as tdist
+        if tdist.get_backend(group) == "nccl":
+            import torch
+            dev = torch.device("cuda", torch.cuda.current_device())
+    data = _ensembles(inp, paths, rank, size, reduce=lambda arrs: allreduce_sum(arrs, group, dev))
     p = inp[0]
     ne = p.ensembles[1] * p.ensembles[2]
     sx = max(3, 1 + p.nchk)
