@@ -38,10 +38,12 @@ sys.path.insert(0, ROOT)
 
 METRIC = "traj-steps/s (2D 256x256 stochastic GPE, MP, 4096 trajectories)"
 HBM_FALLBACK_GBS = 6650.0
-# DRAM bytes per launch of the dominant kernels from one ncu capture of a
-# 512-trajectory case of the same problem, scaled to 4096 trajectories (traffic
-# grows with the trajectory count); profiles/ holds the capture summary.
-NCU_TRAFFIC_PER_TRAJ = {"x_step": None, "y_pass": None}
+# DRAM bytes (read + write) per launch and per trajectory of the two streaming
+# kernels, from one ncu --set full capture of the 512-trajectory case of this
+# problem (profiles/xs_stream_gpe_256x256.md); a launch's traffic grows in
+# proportion to the trajectories it processes, so bench lines scale these by
+# the trajectory count.
+NCU_TRAFFIC_PER_TRAJ = {"x_step": (268470784 + 209269504) / 512.0, "y_pass": (269653248 + 212555520) / 512.0}
 
 
 def _peaks():

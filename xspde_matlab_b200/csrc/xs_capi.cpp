@@ -852,8 +852,6 @@ void load_module(xs_handle& h) {
       cu_check(d.getfn(f.f, h.mod, f.name), f.name);
       if (f.smem > 48 * 1024)
         cu_check(d.setattr(*f.f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, (int)f.smem), f.name);
-      // these kernels stage through shared memory and use little L1: prefer shared
-      cu_check(d.setattr(*f.f, CU_FUNC_ATTRIBUTE_PREFERRED_SHARED_MEMORY_CARVEOUT, 100), f.name);
     }
     CUDA_CHECK(cudaStreamCreateWithFlags(&h.stream, cudaStreamNonBlocking));
     h.d_status.ensure(sizeof(int));
