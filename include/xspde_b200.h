@@ -181,6 +181,35 @@ XS_API xs_status xs_random(xs_handle* h, int block, double* v_out);
  * the pre-scaled noise w [noises, space, ens1] (NULL: zero noise). */
 XS_API xs_status xs_step(xs_handle* h, double* a_inout, const double* w, double t, double dtr);
 
+/* Inputs of the learned control variate (no counterpart in the reference):
+ * coarse space-time projections of the Wiener increments that p.noisegen
+ * feeds the trajectories of blocks first_block .. first_block+nblocks-1
+ * (fine pass).  region = {i1lo, i2lo, bw, bh, nbx, nby}: nbx x nby lattice
+ * blocks of bw x bh sites starting at x index i1lo, y index i2lo (<= 16 x 16
+ * blocks); windows of draws_per_window consecutive draws starting at
+ * first_draw (>= 1).  out_dev[traj][comp][window][by][bx] (FP32, device):
+ * the sum of the standard normals over the block and window divided by
+ * sqrt(draws * sites), so each feature is N(0,1) and independent of the
+ * others.  Asynchronous on `stream` (NULL: the handle's stream). */
+XS_API xs_status xs_noise_features(xs_handle* h, int first_block, int nblocks, const int* region, int first_draw,
+                                   int draws_per_window, int windows, float* out_dev, void* stream);
+
+/* Learned control variate network (no counterpart in the reference): MLP
+ * in -> hidden -> hidden -> hidden -> 1 with GELU, BF16 tensor-core operands
+ * and FP32 accumulation.  All pointers are device pointers (FP32); work is
+ * the activation workspace.  xs_mlp_sizes returns the workspace floats for a
+ * batch and the parameter count (W1[h][in], b1, W2[h][h], b2, W3[h][h], b3,
+ * w4[h], b4).  xs_mlp_train_grad runs the forward pass, the MSE loss against
+ * target (*loss_dev, FP64) and the backward pass into grad.  xs_mlp_adam
+ * applies one Adam step (step >= 1). */
+XS_API size_t xs_mlp_sizes(int in, int hidden, int batch, size_t* nparams);
+XS_API xs_status xs_mlp_forward(int batch, int in, int hidden, const float* x, const float* params, float* work,
+                                float* y, void* stream);
+XS_API xs_status xs_mlp_train_grad(int batch, int in, int hidden, const float* x, const float* params, float* work,
+                                   const float* target, float* grad, double* loss_dev, void* stream);
+XS_API xs_status xs_mlp_adam(size_t n, float* params, const float* grad, float* m, float* v, float lr, float beta1,
+                             float beta2, float eps, int step, void* stream);
+
 /* Kernel kinds counted by xs_kernel_stats. */
 enum {
   XS_KERNEL_RESIDENT = 0, /* whole path with fields in shared memory */

@@ -16,7 +16,8 @@ MAXDIM = 4
 # Every symbol include/xspde_b200.h declares.
 EXPORTS = ["xs_create", "xs_destroy", "xs_last_error", "xs_version", "xs_observe_info", "xs_av_doubles_per_block",
            "xs_run_path", "xs_run_path_device", "xs_sync", "xs_noise", "xs_random", "xs_step", "xs_compile_check",
-           "xs_set_kernel_timing", "xs_kernel_stats", "xs_run_path_device_noalloc"]
+           "xs_set_kernel_timing", "xs_kernel_stats", "xs_run_path_device_noalloc", "xs_noise_features",
+           "xs_mlp_sizes", "xs_mlp_forward", "xs_mlp_train_grad", "xs_mlp_adam"]
 KERNEL_KINDS = ["resident", "obs_reduce", "x_init", "x_step", "x_final", "y_pass", "x_obs", "scalar"]
 
 
@@ -102,6 +103,19 @@ def lib():
         L.xs_run_path_device_noalloc.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                  ctypes.c_void_p, ctypes.c_void_p]
         L.xs_run_path_device_noalloc.restype = ctypes.c_int
+        L.xs_noise_features.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
+                                        ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+        L.xs_noise_features.restype = ctypes.c_int
+        vp, ci = ctypes.c_void_p, ctypes.c_int
+        L.xs_mlp_sizes.argtypes = [ci, ci, ci, P(ctypes.c_size_t)]
+        L.xs_mlp_sizes.restype = ctypes.c_size_t
+        L.xs_mlp_forward.argtypes = [ci, ci, ci, vp, vp, vp, vp, vp]
+        L.xs_mlp_forward.restype = ci
+        L.xs_mlp_train_grad.argtypes = [ci, ci, ci, vp, vp, vp, vp, vp, vp, vp]
+        L.xs_mlp_train_grad.restype = ci
+        L.xs_mlp_adam.argtypes = [ctypes.c_size_t, vp, vp, vp, vp, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                                  ctypes.c_float, ci, vp]
+        L.xs_mlp_adam.restype = ci
         _ = dp
         _lib = L
     return _lib

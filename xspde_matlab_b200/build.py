@@ -15,7 +15,7 @@ LIB = os.path.join(HERE, "libxspde_b200.so")
 CUDA = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 KERNELS = [("prelude", "xs_prelude.cuh"), ("noise", "xs_noise.cuh"), ("resident", "xs_resident.cuh"),
            ("stream", "xs_stream.cuh")]
-SOURCES = ["xs_capi.cpp", "xs_expr.cpp", "xs_aot.cu", "xs_noalloc.cu"]
+SOURCES = ["xs_capi.cpp", "xs_expr.cpp", "xs_aot.cu", "xs_noalloc.cu", "xs_mlp.cu"]
 
 
 def _embed():
@@ -40,6 +40,7 @@ def _stale():
     t = os.path.getmtime(LIB)
     deps = [os.path.join(CSRC, s) for s in SOURCES] + [os.path.join(CSRC, "xs_expr.hpp"),
                                                       os.path.join(CSRC, "xs_noalloc.hpp"),
+                                                      os.path.join(CSRC, "xs_mlp.hpp"),
                                                       os.path.join(HERE, "build.py"),
                                                       os.path.join(os.path.dirname(HERE), "include", "xspde_b200.h")]
     deps += [os.path.join(CSRC, "kernels", k) for _, k in KERNELS]

@@ -25,6 +25,7 @@
 
 #include "xs_expr.hpp"
 #include "xs_noalloc.hpp"
+#include "xs_mlp.hpp"
 
 extern const char* xs_kernel_source_prelude;
 extern const char* xs_kernel_source_noise;
@@ -623,7 +624,7 @@ struct xs_handle {
   // device state
   bool loaded = false;
   CUmodule mod = nullptr;
-  CUfunction f_resident = nullptr, f_reduce = nullptr, f_noise = nullptr, f_random = nullptr;
+  CUfunction f_resident = nullptr, f_reduce = nullptr, f_noise = nullptr, f_random = nullptr, f_feat = nullptr;
   CUfunction f_xinit = nullptr, f_xnl = nullptr, f_xfinal = nullptr, f_spass = nullptr, f_xobs = nullptr,
              f_scalar = nullptr;
   StreamPlan sp;
@@ -848,6 +849,7 @@ void load_module(xs_handle& h) {
                {&h.f_xobs, "xs_x_obs", h.sp.osmem}, {&h.f_scalar, "xs_stream_scalar", 0}};
     cu_check(d.getfn(&h.f_noise, h.mod, "xs_export_noise"), "xs_export_noise");
     cu_check(d.getfn(&h.f_random, h.mod, "xs_export_random"), "xs_export_random");
+    cu_check(d.getfn(&h.f_feat, h.mod, "xs_noise_features"), "xs_noise_features");
     for (auto& f : fns) {
       cu_check(d.getfn(f.f, h.mod, f.name), f.name);
       if (f.smem > 48 * 1024)
@@ -865,6 +867,7 @@ void load_module(xs_handle& h) {
   cu_check(d.getfn(&h.f_reduce, h.mod, "xs_obs_reduce"), "cuModuleGetFunction(xs_obs_reduce)");
   cu_check(d.getfn(&h.f_noise, h.mod, "xs_export_noise"), "cuModuleGetFunction(xs_export_noise)");
   cu_check(d.getfn(&h.f_random, h.mod, "xs_export_random"), "cuModuleGetFunction(xs_export_random)");
+  cu_check(d.getfn(&h.f_feat, h.mod, "xs_noise_features"), "cuModuleGetFunction(xs_noise_features)");
   if (h.rp.smem > 48 * 1024)
     cu_check(d.setattr(h.f_resident, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, (int)h.rp.smem),
              "cuFuncSetAttribute(max dynamic smem)");
@@ -1408,6 +1411,100 @@ XS_API xs_status xs_run_path_device_noalloc(xs_handle* h, int first_block, int n
     }
     return XS_OK;
   });
+}
+
+XS_API xs_status xs_noise_features(xs_handle* h, int first_block, int nblocks, const int* region, int first_draw,
+                                   int draws_per_window, int windows, float* out_dev, void* stream) {
+  return guard([&]() -> xs_status {
+    if (!h || nblocks < 1 || first_block < 0 || !region || !out_dev || draws_per_window < 1 || windows < 1 ||
+        first_draw < 1)
+      raise(XS_ERR_ARG, "bad arguments to xs_noise_features");
+    const Problem& P = h->P;
+    if (P.D < 2 || P.NW < 1) raise(XS_ERR_UNSUPPORTED, "noise features need two space dimensions and noises");
+    const int i1lo = region[0], i2lo = region[1], bw = region[2], bh = region[3], nbx = region[4], nby = region[5];
+    if (bw < 1 || bh < 1 || nbx < 1 || nby < 1 || nbx > 16 || nby > 16 || i1lo < 0 || i2lo < 0 ||
+        i1lo + nbx * bw > P.N[0] || i2lo + nby * bh > P.N[1])
+      raise(XS_ERR_ARG, "feature region outside the lattice or more than 16x16 blocks");
+    load_module(*h);
+    struct {
+      int ntraj, ens1, block0, seq;
+      unsigned seed;
+      int i1lo, i2lo, bw, bh, nbx, nby;
+      int d0, dw, nt;
+      float* out;
+      int* status;
+    } a{};
+    a.ntraj = nblocks * P.E1;
+    a.ens1 = P.E1;
+    a.block0 = first_block;
+    a.seed = (unsigned)(P.p.seed & 0xffffffffu);
+    a.i1lo = i1lo;
+    a.i2lo = i2lo;
+    a.bw = bw;
+    a.bh = bh;
+    a.nbx = nbx;
+    a.nby = nby;
+    a.d0 = first_draw;
+    a.dw = draws_per_window;
+    a.nt = windows;
+    a.out = out_dev;
+    a.status = (int*)h->d_status.p;
+    void* params[] = {&a};
+    cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
+    cu_check(driver().launch(h->f_feat, (unsigned)(a.ntraj * windows), 1, 1, 256, 1, 1, 0, (CUstream)st, params,
+                             nullptr),
+             "launch xs_noise_features");
+    return XS_OK;
+  });
+}
+
+// ---- learned control variate network (device pointers, caller's stream) ----
+XS_API size_t xs_mlp_sizes(int in, int hidden, int batch, size_t* nparams) {
+  if (in < 1 || hidden < 1 || batch < 1) return 0;
+  return xs_mlp_layout(in, hidden, batch, nparams);
+}
+
+XS_API xs_status xs_mlp_forward(int batch, int in, int hidden, const float* x, const float* params, float* work,
+                                float* y, void* stream) {
+  if (batch < 1 || in < 1 || hidden < 1 || !x || !params || !work) {
+    g_err = "bad arguments to xs_mlp_forward";
+    return XS_ERR_ARG;
+  }
+  int e = xs_mlp_forward_impl(batch, in, hidden, x, params, work, y, (cudaStream_t)stream);
+  if (e) {
+    g_err = std::string("xs_mlp_forward: ") + cudaGetErrorString((cudaError_t)e);
+    return XS_ERR_CUDA;
+  }
+  return XS_OK;
+}
+
+XS_API xs_status xs_mlp_train_grad(int batch, int in, int hidden, const float* x, const float* params, float* work,
+                                   const float* target, float* grad, double* loss_dev, void* stream) {
+  if (batch < 1 || in < 1 || hidden < 1 || !x || !params || !work || !target || !grad || !loss_dev) {
+    g_err = "bad arguments to xs_mlp_train_grad";
+    return XS_ERR_ARG;
+  }
+  int e = xs_mlp_forward_impl(batch, in, hidden, x, params, work, nullptr, (cudaStream_t)stream);
+  if (!e) e = xs_mlp_backward_impl(batch, in, hidden, x, params, work, target, grad, loss_dev, (cudaStream_t)stream);
+  if (e) {
+    g_err = std::string("xs_mlp_train_grad: ") + cudaGetErrorString((cudaError_t)e);
+    return XS_ERR_CUDA;
+  }
+  return XS_OK;
+}
+
+XS_API xs_status xs_mlp_adam(size_t n, float* params, const float* grad, float* m, float* v, float lr, float beta1,
+                             float beta2, float eps, int step, void* stream) {
+  if (!n || !params || !grad || !m || !v || step < 1) {
+    g_err = "bad arguments to xs_mlp_adam";
+    return XS_ERR_ARG;
+  }
+  int e = xs_mlp_adam_impl(n, params, grad, m, v, lr, beta1, beta2, eps, step, (cudaStream_t)stream);
+  if (e) {
+    g_err = std::string("xs_mlp_adam: ") + cudaGetErrorString((cudaError_t)e);
+    return XS_ERR_CUDA;
+  }
+  return XS_OK;
 }
 
 XS_API xs_status xs_set_kernel_timing(xs_handle* h, int on) {
