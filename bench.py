@@ -324,6 +324,143 @@ def run_ours(args, rank, world, local_rank):
     print(json.dumps(line))
 
 
+# ---- second headline: time to 1e-3 relative sampling error on <|a|^2> ----------
+CV_OBSERVE = "@(a,p) Int(abs(a).^2, p.dx, [0 0; -1.2 1.25; -1.2 1.25], p)"  # central 32x32 sites at t = 5
+# Control-variate inputs: (region {i1lo, i2lo, bw, bh, nbx, nby}, steps per window,
+# windows, steps between the window end and the observed step).  The 64x64
+# sites around the centre: 8x8 blocks over the last 30 steps, then 4x4 blocks
+# over four windows of 30 steps before that; 2 noise components each.
+CV_SETS = (((96, 96, 8, 8, 8, 8), 30, 1, 0), ((96, 96, 16, 16, 4, 4), 30, 4, 30))
+CV_FEATURES = sum(2 * nt * r[4] * r[5] for r, dw, nt, gap in CV_SETS)
+
+
+def _cv_path(prec, nb):
+    from xspde_matlab_b200 import GpuPath, xpreferences
+    from xspde_matlab_b200.problems import GPE_2D
+    p = dict(GPE_2D, precision=prec, ensembles=[1, nb, 1], observe=[CV_OBSERVE])
+    return GpuPath(xpreferences([p])[0])
+
+
+def _cv_solve(path, first, nb, feats=False):
+    """Per-trajectory observable at the last output time (blocks of one
+    trajectory) and, optionally, the noise features of the same trajectories."""
+    import torch
+    from xspde_matlab_b200 import _lib
+    L = _lib.lib()
+    st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    av = torch.zeros((nb, path.p.points[0], 1, 2), dtype=torch.float64, device="cuda")
+    _lib.check(L.xs_run_path_device(path.h, first, nb, 1, None, ctypes.c_void_p(av.data_ptr()), None, st))
+    X = None
+    if feats:
+        X = torch.empty((nb, CV_FEATURES), dtype=torch.float32, device="cuda")
+        last = (path.p.points[0] - 1) * path.p.steps[0]  # draw of the step observed at the last output
+        col = 0
+        for reg, dw, nt, gap in CV_SETS:
+            nf = 2 * nt * reg[4] * reg[5]
+            part = torch.empty((nb, nf), dtype=torch.float32, device="cuda")
+            r = (ctypes.c_int * 6)(*reg)
+            _lib.check(L.xs_noise_features(path.h, first, nb, r, last - gap - dw * nt + 1, dw, nt, 0.0,
+                                           ctypes.c_void_p(part.data_ptr()), st))
+            X[:, col:col + nf] = part
+            col += nf
+    _lib.check(L.xs_sync(path.h))  # surfaces device-side status (non-finite values, refused launches)
+    return av[:, -1, 0, 0], X
+
+
+def run_cv(args):
+    import numpy as np
+    import torch
+    from xspde_matlab_b200.cv import ControlVariateNet, block_sampling_error, two_level
+    target = 1e-3
+    nblk = 16
+    ntrain, nval, chunk = 1 << 16, 8192, 8192
+    p32 = _cv_path("fp32", chunk)
+    # training pairs generated by the solver itself (global blocks 0 .. 65535)
+    t0 = time.perf_counter()
+    fs, Xs = [], []
+    for b0 in range(0, ntrain + nval, chunk):
+        f, X = _cv_solve(p32, b0, chunk, feats=True)
+        fs.append(f)
+        Xs.append(X)
+    torch.cuda.synchronize()
+    t_data = time.perf_counter() - t0
+    f_all, X_all = torch.cat(fs), torch.cat(Xs)
+    f_tr, X_tr, f_va, X_va = f_all[:ntrain], X_all[:ntrain], f_all[ntrain:], X_all[ntrain:]
+    # control variate g = linear least squares + MLP on the residual
+    t0 = time.perf_counter()
+    A = torch.cat([X_tr.double(), torch.ones(ntrain, 1, dtype=torch.float64, device="cuda")], 1)
+    coef = torch.linalg.solve(A.T @ A, A.T @ f_tr.double().unsqueeze(1))[:, 0]
+
+    def g_lin(X):
+        return X.double() @ coef[:-1] + coef[-1]
+    net = ControlVariateNet(CV_FEATURES, 256, seed=0)
+    r_tr = (f_tr.double() - g_lin(X_tr)).float()
+    r_va = f_va.double() - g_lin(X_va)
+    best = (float(r_va.var()), None)  # the linear fit alone
+    for ep in range(20):
+        net.fit(X_tr, r_tr, epochs=1, batch=1024, lr=3e-4 if ep > 9 else 1e-3, seed=ep, weight_decay=1e-2)
+        v = float((r_va - net.predict(X_va)).var())
+        if v < best[0]:
+            best = (v, net.params.clone(), net.mean, net.scale)
+    use_mlp = best[1] is not None
+    if use_mlp:
+        net.params.copy_(best[1])
+        net.mean, net.scale = best[2], best[3]
+    torch.cuda.synchronize()
+    t_fit = time.perf_counter() - t0
+
+    def g(X):
+        return g_lin(X) + (net.predict(X) if use_mlp else 0.0)
+    var_plain = float(f_va.double().var())
+    var_cv = float((f_va.double() - g(X_va)).var())
+    mu = float(f_va.double().mean())
+    print("cv pilot: mean %.6g var_plain %.4g var_cv %.4g mlp %s" % (mu, var_plain, var_cv, use_mlp), file=sys.stderr)
+    # plain FP64 estimator at the N that reaches the target (pilot variance)
+    n_plain = nblk * max(2, math.ceil(var_plain / (target * mu) ** 2 / nblk))
+    p64 = _cv_path("fp64", n_plain)
+    _cv_solve(p64, 1 << 20, nblk)  # compile and warm the FP64 kernels
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    f64, _ = _cv_solve(p64, 1 << 20, n_plain)
+    est_plain, err_plain = block_sampling_error(f64.cpu().numpy(), nblk)
+    t_plain = time.perf_counter() - t0
+    # FP32 + learned control variate at its own N, fresh trajectories and fresh network inputs
+    n_cv = nblk * max(2, math.ceil(var_cv / (target * mu) ** 2 / nblk))
+    m_fresh = 1 << 20
+    pcv = _cv_path("fp32", n_cv)
+    _cv_solve(pcv, 1 << 21, nblk, feats=True)
+    gen = torch.Generator(device="cuda").manual_seed(12345)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    f32, Xc = _cv_solve(pcv, 1 << 21, n_cv, feats=True)
+    gx = g(Xc)
+    Xf = torch.randn((m_fresh, CV_FEATURES), device="cuda", generator=gen)
+    gf = g(Xf)
+    est_cv, err_cv = two_level(f32.cpu().numpy(), gx.cpu().numpy(), gf.cpu().numpy(), nblk)
+    t_cv = time.perf_counter() - t0
+    # FP32 trajectories against FP64 ones on identical noise (the FP64-oracle error of the FP32 path)
+    ncmp = min(256, n_cv)
+    p64b = _cv_path("fp64", ncmp)
+    f64b, _ = _cv_solve(p64b, 1 << 21, ncmp)
+    d32 = float(((f32[:ncmp].double() - f64b) / f64b).abs().max())
+    line = {
+        "metric": "time to 1e-3 relative sampling error on <|a|^2> (central region, t=5)", "value": t_cv,
+        "unit": "s", "higher_is_better": False, "n_gpus": 1,
+        "plain_fp64": {"seconds": t_plain, "trajectories": n_plain, "estimate": est_plain,
+                       "rel_sampling_error": err_plain / est_plain},
+        "fp32_cv": {"seconds": t_cv, "trajectories": n_cv, "fresh_network_inputs": m_fresh, "estimate": est_cv,
+                    "rel_sampling_error": err_cv / est_cv, "mlp_used": use_mlp},
+        "speedup_vs_plain_fp64": t_plain / t_cv,
+        "variance_ratio": {"linear+mlp": var_plain / var_cv, "plain_var": var_plain, "cv_var": var_cv},
+        "estimates_agree_sigma": abs(est_cv - est_plain) / math.sqrt(err_cv ** 2 + err_plain ** 2),
+        "fp32_vs_fp64_traj_max_rel": d32,
+        "training": {"pairs": ntrain, "data_seconds": t_data, "fit_seconds": t_fit,
+                     "features": "%d coarse space-time noise projections: %s" % (CV_FEATURES, CV_SETS)},
+        "config": {"workload": "gpe_2d 256x256, 509 MP steps; sampling error from %d blocks (xsim.m:144)" % nblk},
+    }
+    print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -332,12 +469,19 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--ntraj", type=int, default=4096, help="trajectories per GPU (multiple of 256)")
     ap.add_argument("--quick", action="store_true", help="device timing only (no e2e, no CPU sample)")
+    ap.add_argument("--cv", action="store_true", help="second headline: time to 1e-3 sampling error, "
+                                                      "plain FP64 vs FP32 + learned control variate")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.cv:
+        import torch
+        torch.cuda.set_device(local_rank)
+        run_cv(args)
         return
     if world > 1:
         import datetime

@@ -132,8 +132,8 @@ XS_API xs_status xs_run_path(xs_handle* h, int first_block, int nblocks, int nc,
                              double* av_out, double* a_out);
 
 /* Same as xs_run_path with device pointers and a caller stream (cudaStream_t
- * passed as void*); nothing is copied to or from the host and the call
- * returns without synchronising.  a_in_dev/a_out_dev use the device layout
+ * passed as void*; NULL is the default stream, as in CUDA); nothing is copied
+ * to or from the host and the call returns without synchronising.  a_in_dev/a_out_dev use the device layout
  * [ens][fields][space] (identical to the host layout when fields == 1) and
  * may be NULL.  av_dev receives, per block and output time, one row of
  * complex FP64 values: site observables' lines k at k*nspace + s (s the
@@ -187,12 +187,13 @@ XS_API xs_status xs_step(xs_handle* h, double* a_inout, const double* w, double 
  * (fine pass).  region = {i1lo, i2lo, bw, bh, nbx, nby}: nbx x nby lattice
  * blocks of bw x bh sites starting at x index i1lo, y index i2lo (<= 16 x 16
  * blocks); windows of draws_per_window consecutive draws starting at
- * first_draw (>= 1).  out_dev[traj][comp][window][by][bx] (FP32, device):
- * the sum of the standard normals over the block and window divided by
- * sqrt(draws * sites), so each feature is N(0,1) and independent of the
- * others.  Asynchronous on `stream` (NULL: the handle's stream). */
+ * first_draw (>= 1); within a window the draws are weighted by
+ * exp(-decay * (last draw of the window - draw)).  out_dev[traj][comp][window]
+ * [by][bx] (FP32, device): the weighted sum of the standard normals over the
+ * block and window divided by sqrt(sum of squared weights * sites), so each
+ * feature is N(0,1) and independent of the others.  Asynchronous on `stream` (a cudaStream_t; NULL is the default stream). */
 XS_API xs_status xs_noise_features(xs_handle* h, int first_block, int nblocks, const int* region, int first_draw,
-                                   int draws_per_window, int windows, float* out_dev, void* stream);
+                                   int draws_per_window, int windows, double decay, float* out_dev, void* stream);
 
 /* Learned control variate network (no counterpart in the reference): MLP
  * in -> hidden -> hidden -> hidden -> 1 with GELU, BF16 tensor-core operands
@@ -201,14 +202,14 @@ XS_API xs_status xs_noise_features(xs_handle* h, int first_block, int nblocks, c
  * batch and the parameter count (W1[h][in], b1, W2[h][h], b2, W3[h][h], b3,
  * w4[h], b4).  xs_mlp_train_grad runs the forward pass, the MSE loss against
  * target (*loss_dev, FP64) and the backward pass into grad.  xs_mlp_adam
- * applies one Adam step (step >= 1). */
+ * applies one Adam step (step >= 1) with decoupled weight decay. */
 XS_API size_t xs_mlp_sizes(int in, int hidden, int batch, size_t* nparams);
 XS_API xs_status xs_mlp_forward(int batch, int in, int hidden, const float* x, const float* params, float* work,
                                 float* y, void* stream);
 XS_API xs_status xs_mlp_train_grad(int batch, int in, int hidden, const float* x, const float* params, float* work,
                                    const float* target, float* grad, double* loss_dev, void* stream);
 XS_API xs_status xs_mlp_adam(size_t n, float* params, const float* grad, float* m, float* v, float lr, float beta1,
-                             float beta2, float eps, int step, void* stream);
+                             float beta2, float eps, int step, float weight_decay, void* stream);
 
 /* Kernel kinds counted by xs_kernel_stats. */
 enum {

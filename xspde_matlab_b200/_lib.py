@@ -104,7 +104,7 @@ def lib():
                                                  ctypes.c_void_p, ctypes.c_void_p]
         L.xs_run_path_device_noalloc.restype = ctypes.c_int
         L.xs_noise_features.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
-                                        ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+                                        ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p]
         L.xs_noise_features.restype = ctypes.c_int
         vp, ci = ctypes.c_void_p, ctypes.c_int
         L.xs_mlp_sizes.argtypes = [ci, ci, ci, P(ctypes.c_size_t)]
@@ -114,7 +114,7 @@ def lib():
         L.xs_mlp_train_grad.argtypes = [ci, ci, ci, vp, vp, vp, vp, vp, vp, vp]
         L.xs_mlp_train_grad.restype = ci
         L.xs_mlp_adam.argtypes = [ctypes.c_size_t, vp, vp, vp, vp, ctypes.c_float, ctypes.c_float, ctypes.c_float,
-                                  ctypes.c_float, ci, vp]
+                                  ctypes.c_float, ci, ctypes.c_float, vp]
         L.xs_mlp_adam.restype = ci
         _ = dp
         _lib = L

@@ -71,9 +71,10 @@ extern "C" __global__ void xs_export_random(double* out, int ens1, u32 block, u3
 // learned control variate: for trajectory e and window tw,
 //   out[e][((c*NT + tw)*NBY + by)*NBX + bx] =
 //     sum over draws d0 + tw*DW .. d0 + (tw+1)*DW - 1 and over the sites of
-//     lattice block (bx, by) of the standard normal z_c(site, e, draw),
-//   divided by sqrt(DW * BW * BH) so that every feature is N(0, 1) and the
-//   features of one trajectory are independent.  The lattice block (bx, by)
+//     lattice block (bx, by) of the standard normal z_c(site, e, draw)
+//     weighted by exp(-decay (last draw of the window - draw)),
+//   divided by sqrt(sum of squared weights * BW * BH) so that every feature
+//   is N(0, 1) and the features of one trajectory are independent.  The lattice block (bx, by)
 //   covers x indices i1lo + bx*BW .. + BW - 1 and y indices i2lo + by*BH ...
 //   One CTA per (trajectory, window).
 struct XsFeatArgs {
@@ -81,6 +82,7 @@ struct XsFeatArgs {
   u32 seed;
   int i1lo, i2lo, bw, bh, nbx, nby;
   int d0, dw, nt;
+  float decay;  // draws weighted by exp(-decay * (last draw of the window - draw))
   float* out;
   int* status;
 };
@@ -98,8 +100,11 @@ extern "C" __global__ void __launch_bounds__(256) xs_noise_features(const XsFeat
   __syncthreads();
   const int W = F.nbx * F.bw, H = F.nby * F.bh;
   const u32 blk = (u32)(F.block0 + e / F.ens1), el = (u32)(e % F.ens1);
+  float wsum2 = 0.f;
   for (int q = 0; q < F.dw; ++q) {
     const u32 draw = (u32)(F.d0 + tw * F.dw + q);
+    const float wq = __expf(-F.decay * (float)(F.dw - 1 - q));
+    wsum2 += wq * wq;
     for (int i = threadIdx.x; i < W * H; i += blockDim.x) {
       const int lx = i % W, ly = i / W;
       const int i1 = F.i1lo + lx, i2 = F.i2lo + ly;
@@ -108,11 +113,11 @@ extern "C" __global__ void __launch_bounds__(256) xs_noise_features(const XsFeat
       xs_normals_site<XS_NW>(z, s, el, draw, (u32)F.seq, F.seed, blk);
       const int b = (ly / F.bh) * F.nbx + (lx / F.bw);
 #pragma unroll
-      for (int c = 0; c < XS_NW; ++c) atomicAdd(&acc[c * nb + b], (float)z[c]);
+      for (int c = 0; c < XS_NW; ++c) atomicAdd(&acc[c * nb + b], wq * (float)z[c]);
     }
   }
   __syncthreads();
-  const float sc = rsqrtf((float)(F.dw * F.bw * F.bh));
+  const float sc = rsqrtf(wsum2 * (float)(F.bw * F.bh));
   for (int i = threadIdx.x; i < XS_NW * nb; i += blockDim.x) {
     const int c = i / nb, b = i % nb;
     F.out[(size_t)e * (XS_NW * F.nt * nb) + ((size_t)c * F.nt + tw) * nb + b] = acc[i] * sc;

@@ -1318,7 +1318,7 @@ XS_API xs_status xs_run_path_device(xs_handle* h, int first_block, int nblocks, 
     if (!h || nblocks < 1 || first_block < 0 || (nc != 1 && nc != 2) || !av_dev)
       raise(XS_ERR_ARG, "bad arguments to xs_run_path_device");
     load_module(*h);
-    cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
+    cudaStream_t st = (cudaStream_t)stream;  // the caller's stream; NULL is the default stream
     CUDA_CHECK(cudaMemsetAsync(h->d_status.p, 0, sizeof(int), st));
     if (h->kind == 2) launch_stream(*h, first_block, nblocks, nc, a_in_dev, av_dev, a_out_dev, st);
     else launch_resident(*h, first_block, nblocks, nc, a_in_dev, av_dev, a_out_dev, st);
@@ -1368,7 +1368,7 @@ XS_API xs_status xs_run_path_device_noalloc(xs_handle* h, int first_block, int n
     void* scratch = nullptr;
     cudaError_t e = xs_noalloc_scratch_address(&scratch);
     if (e != cudaSuccess) raise(XS_ERR_CUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
-    cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
+    cudaStream_t st = (cudaStream_t)stream;  // the caller's stream; NULL is the default stream
     CUDA_CHECK(cudaMemsetAsync(h->d_status.p, 0, sizeof(int), st));
     PathArgsHost a{};
     a.ntraj = total;
@@ -1414,7 +1414,7 @@ XS_API xs_status xs_run_path_device_noalloc(xs_handle* h, int first_block, int n
 }
 
 XS_API xs_status xs_noise_features(xs_handle* h, int first_block, int nblocks, const int* region, int first_draw,
-                                   int draws_per_window, int windows, float* out_dev, void* stream) {
+                                   int draws_per_window, int windows, double decay, float* out_dev, void* stream) {
   return guard([&]() -> xs_status {
     if (!h || nblocks < 1 || first_block < 0 || !region || !out_dev || draws_per_window < 1 || windows < 1 ||
         first_draw < 1)
@@ -1431,6 +1431,7 @@ XS_API xs_status xs_noise_features(xs_handle* h, int first_block, int nblocks, c
       unsigned seed;
       int i1lo, i2lo, bw, bh, nbx, nby;
       int d0, dw, nt;
+      float decay;
       float* out;
       int* status;
     } a{};
@@ -1447,10 +1448,11 @@ XS_API xs_status xs_noise_features(xs_handle* h, int first_block, int nblocks, c
     a.d0 = first_draw;
     a.dw = draws_per_window;
     a.nt = windows;
+    a.decay = (float)decay;
     a.out = out_dev;
     a.status = (int*)h->d_status.p;
     void* params[] = {&a};
-    cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
+    cudaStream_t st = (cudaStream_t)stream;  // the caller's stream; NULL is the default stream
     cu_check(driver().launch(h->f_feat, (unsigned)(a.ntraj * windows), 1, 1, 256, 1, 1, 0, (CUstream)st, params,
                              nullptr),
              "launch xs_noise_features");
@@ -1494,12 +1496,12 @@ XS_API xs_status xs_mlp_train_grad(int batch, int in, int hidden, const float* x
 }
 
 XS_API xs_status xs_mlp_adam(size_t n, float* params, const float* grad, float* m, float* v, float lr, float beta1,
-                             float beta2, float eps, int step, void* stream) {
+                             float beta2, float eps, int step, float weight_decay, void* stream) {
   if (!n || !params || !grad || !m || !v || step < 1) {
     g_err = "bad arguments to xs_mlp_adam";
     return XS_ERR_ARG;
   }
-  int e = xs_mlp_adam_impl(n, params, grad, m, v, lr, beta1, beta2, eps, step, (cudaStream_t)stream);
+  int e = xs_mlp_adam_impl(n, params, grad, m, v, lr, beta1, beta2, eps, step, weight_decay, (cudaStream_t)stream);
   if (e) {
     g_err = std::string("xs_mlp_adam: ") + cudaGetErrorString((cudaError_t)e);
     return XS_ERR_CUDA;

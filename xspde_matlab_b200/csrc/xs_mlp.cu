@@ -164,15 +164,16 @@ __global__ void gelu_backward(const float* __restrict__ dA, const float* __restr
     dZ[i] = dA[i] * gelu_d(Z[i]);
 }
 
+// Adam (Kingma & Ba, 2015) with decoupled weight decay wd (Loshchilov & Hutter, 2019).
 __global__ void adam(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m, float* __restrict__ v,
-                     size_t n, float lr, float b1, float b2, float eps, float c1, float c2) {
+                     size_t n, float lr, float b1, float b2, float eps, float c1, float c2, float wd) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
     const float gi = g[i];
     const float mi = b1 * m[i] + (1.f - b1) * gi;
     const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
     m[i] = mi;
     v[i] = vi;
-    p[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+    p[i] -= lr * ((mi / c1) / (sqrtf(vi / c2) + eps) + wd * p[i]);
   }
 }
 
@@ -265,8 +266,8 @@ int xs_mlp_backward_impl(int B, int in, int H, const float* x, const float* P, f
 }
 
 int xs_mlp_adam_impl(size_t n, float* P, const float* g, float* m, float* v, float lr, float b1, float b2, float eps,
-                     int step, cudaStream_t st) {
+                     int step, float wd, cudaStream_t st) {
   float c1 = 1.f - powf(b1, (float)step), c2 = 1.f - powf(b2, (float)step);
-  adam<<<grid1(n), 256, 0, st>>>(P, g, m, v, n, lr, b1, b2, eps, c1, c2);
+  adam<<<grid1(n), 256, 0, st>>>(P, g, m, v, n, lr, b1, b2, eps, c1, c2, wd);
   return (int)cudaGetLastError();
 }

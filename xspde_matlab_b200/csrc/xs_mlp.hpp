@@ -8,4 +8,4 @@ int xs_mlp_forward_impl(int B, int in, int H, const float* x, const float* P, fl
 int xs_mlp_backward_impl(int B, int in, int H, const float* x, const float* P, float* work, const float* target,
                          float* grad, double* loss, cudaStream_t st);
 int xs_mlp_adam_impl(size_t n, float* P, const float* g, float* m, float* v, float lr, float b1, float b2, float eps,
-                     int step, cudaStream_t st);
+                     int step, float wd, cudaStream_t st);

@@ -59,7 +59,7 @@ class ControlVariateNet:
             self._work = {B: torch.empty(n, dtype=torch.float32, device=self.device)}
         return self._work[B]
 
-    def fit(self, X, f, epochs=30, batch=1024, lr=1e-3, seed=0, stream=None):
+    def fit(self, X, f, epochs=30, batch=1024, lr=1e-3, seed=0, stream=None, weight_decay=0.0):
         """Fit g to (f - mean)/scale on device tensors X [n, n_in] (FP32), f [n]."""
         import torch
         L = _lib.lib()
@@ -84,7 +84,7 @@ class ControlVariateNet:
                                                _ptr(work), _ptr(tb), _ptr(self.grad), _ptr(loss), st))
                 self.step += 1
                 _lib.check(L.xs_mlp_adam(self.nparams, _ptr(self.params), _ptr(self.grad), _ptr(self.m),
-                                         _ptr(self.v), lr, 0.9, 0.999, 1e-8, self.step, st))
+                                         _ptr(self.v), lr, 0.9, 0.999, 1e-8, self.step, weight_decay, st))
                 tot += float(loss.item()) if b0 == 0 else 0.0
             hist.append(tot)
         return hist
