@@ -91,6 +91,9 @@ typedef struct xs_problem {
   const char* const* param_names;
   const double* param_values;
   int path_kind;               /* 0 = automatic, 1 = resident, 2 = streaming */
+  int runtime_params;          /* 1: named scalars are read at run time (per batch item; param_values are
+                                  the defaults), so one compiled kernel serves many parameter values.
+                                  p.linear always uses param_values. */
 } xs_problem;
 
 /* Create a handle: parse, generate and compile the kernels (NVRTC, cached).

@@ -48,6 +48,7 @@ class XsProblem(ctypes.Structure):
         ("param_names", ctypes.POINTER(ctypes.c_char_p)),
         ("param_values", ctypes.POINTER(ctypes.c_double)),
         ("path_kind", ctypes.c_int),
+        ("runtime_params", ctypes.c_int),
     ]
 
 

@@ -34,6 +34,7 @@ struct XsPathArgs {
   int single_step;      // 1: one method step from t0 with the noise w_in (p.method)
   int pad1;
   const double* w_in;   // [NW, space, ens1] pre-scaled noise for single_step (null: zero)
+  const double* params; // runtime named scalars p.<name> (prm[k])
 };
 
 #define XS_STRIDE1 1
@@ -78,6 +79,83 @@ __device__ __forceinline__ void xs_transform_dim(cx* X, cx* T, const XsPathArgs&
   __syncthreads();
 }
 
+// ---- shared-memory FFT for periodic power-of-two dimensions -----------------
+// Stockham autosort FFT (Govindaraju et al., "High performance discrete Fourier
+// transforms on graphics processors", SC 2008): stage with radix R after
+// earlier stages of total radix NSP maps butterfly j (k = j mod NSP) as
+//   v[r] = in[j + r N/R] * exp(-2 pi i k r / (NSP R)),  v = DFT_R(v),
+//   out[(j / NSP) NSP R + k + r NSP] = v[r],
+// ping-ponging between X and T; the output is in natural (MATLAB fft) order.
+// The inverse is conj(FFT(conj(x))) / N, folded into the first load and the
+// last store.  Twiddles exp(-2 pi i m / N) come from an FP64-built table.
+template <int R> __device__ __forceinline__ void xs_dft_r(cx (&v)[R]);
+template <> __device__ __forceinline__ void xs_dft_r<2>(cx (&v)[2]) {
+  const cx a = v[0];
+  v[0] = a + v[1];
+  v[1] = a - v[1];
+}
+template <> __device__ __forceinline__ void xs_dft_r<4>(cx (&v)[4]) {
+  const cx s02 = v[0] + v[2], d02 = v[0] - v[2], s13 = v[1] + v[3], d13 = v[1] - v[3];
+  v[0] = s02 + s13;
+  v[2] = s02 - s13;
+  v[1] = mkcx(d02.re + d13.im, d02.im - d13.re);  // d02 - i d13
+  v[3] = mkcx(d02.re - d13.im, d02.im + d13.re);  // d02 + i d13
+}
+template <> __device__ __forceinline__ void xs_dft_r<8>(cx (&v)[8]) {
+  cx e[4] = {v[0], v[2], v[4], v[6]}, o[4] = {v[1], v[3], v[5], v[7]};
+  xs_dft_r<4>(e);
+  xs_dft_r<4>(o);
+  const real c = (real)0.70710678118654752440;
+  const cx t1 = mkcx(c * (o[1].re + o[1].im), c * (o[1].im - o[1].re));   // o1 exp(-i pi/4)
+  const cx t2 = mkcx(o[2].im, -o[2].re);                                  // o2 (-i)
+  const cx t3 = mkcx(c * (o[3].im - o[3].re), -c * (o[3].re + o[3].im));  // o3 exp(-3i pi/4)
+  v[0] = e[0] + o[0];
+  v[4] = e[0] - o[0];
+  v[1] = e[1] + t1;
+  v[5] = e[1] - t1;
+  v[2] = e[2] + t2;
+  v[6] = e[2] - t2;
+  v[3] = e[3] + t3;
+  v[7] = e[3] - t3;
+}
+
+// One stage along a dimension of length ND and site stride SD, over every
+// line of every (trajectory, component) of the CTA.
+template <int ND, int SD, int R, int NSP, bool FIRST, bool LAST>
+__device__ __forceinline__ void xs_fft_stage(const cx* __restrict__ in, cx* __restrict__ out, const cx* __restrict__ tw,
+                                             int inv) {
+  constexpr int NB = ND / R;
+  constexpr int NHI = XS_G * XS_F * XS_NS / (SD * ND);
+  const real sc = (LAST ? (real)(1.0 / ND) : (real)1);
+  for (int b = threadIdx.x; b < NHI * NB * SD; b += blockDim.x) {
+    const int lo = b % SD, rem = b / SD;
+    const int j = rem % NB, hi = rem / NB;
+    const int base = lo + SD * ND * hi;
+    const int k = j % NSP;
+    cx v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      cx a = in[base + SD * (j + r * NB)];
+      if (FIRST && inv) a.im = -a.im;
+      if (NSP > 1 && r > 0) a = a * tw[k * r * (ND / (NSP * R))];
+      v[r] = a;
+    }
+    xs_dft_r<R>(v);
+    const int o0 = base + SD * ((j / NSP) * NSP * R + k);
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      cx a = v[r];
+      if (LAST && inv) a = mkcx(a.re * sc, -a.im * sc);
+      out[o0 + SD * r * NSP] = a;
+    }
+  }
+}
+
+// Per-dimension stage sequences generated for the problem's lattice
+// (specialisations of xs_fft_d for the dimensions flagged XS_FFTD<D>).
+template <int D> __device__ __forceinline__ void xs_fft_d(cx*, cx*, const cx*, int) {}
+XS_FFT_STAGES
+
 __device__ __forceinline__ void xs_setbound(cx* X) {
 #if XS_SETBOUND
   for (int i = threadIdx.x; i < XS_G * XS_NS; i += blockDim.x) {
@@ -93,12 +171,26 @@ __device__ __forceinline__ void xs_setbound(cx* X) {
 #endif
 }
 
+// Transform along dimension D: generated Stockham stages (xs_fft_d<D>, defined
+// by the problem header when XS_FFTD<D> is set) or the dense matrix.
+template <int D>
+__device__ __forceinline__ void xs_tr(cx* X, cx* T, const XsPathArgs& P, int dir) {
+  constexpr bool fft = D == 1 ? XS_FFTD1 : (D == 2 ? XS_FFTD2 : XS_FFTD3);
+  if constexpr (fft) {
+    __syncthreads();
+    xs_fft_d<D>(X, T, P.tmat + P.tmat_off[D], dir);
+    __syncthreads();
+  } else {
+    xs_transform_dim<D>(X, T, P, dir);
+  }
+}
+
 // xprop (Applications/SPDE/xprop.m:76-104): transform, multiply by exp(L dt), inverse.
 __device__ __forceinline__ void xs_prop(cx* X, cx* T, const XsPathArgs& P) {
 #if XS_HAS_PROP
-  xs_transform_dim<1>(X, T, P, 0);
-  xs_transform_dim<2>(X, T, P, 0);
-  xs_transform_dim<3>(X, T, P, 0);
+  xs_tr<1>(X, T, P, 0);
+  xs_tr<2>(X, T, P, 0);
+  xs_tr<3>(X, T, P, 0);
   for (int i = threadIdx.x; i < XS_G * XS_F * XS_NS; i += blockDim.x) {
     const int s = i % XS_NS;
     const int f = (i / XS_NS) % XS_F;
@@ -107,9 +199,9 @@ __device__ __forceinline__ void xs_prop(cx* X, cx* T, const XsPathArgs& P) {
     const double vr = (double)v.re, vi = (double)v.im;
     X[i] = mkcx((real)(vr * pr.x - vi * pr.y), (real)(vr * pr.y + vi * pr.x));
   }
-  xs_transform_dim<1>(X, T, P, 1);
-  xs_transform_dim<2>(X, T, P, 1);
-  xs_transform_dim<3>(X, T, P, 1);
+  xs_tr<1>(X, T, P, 1);
+  xs_tr<2>(X, T, P, 1);
+  xs_tr<3>(X, T, P, 1);
 #endif
   __syncthreads();
   xs_setbound(X);
@@ -117,7 +209,8 @@ __device__ __forceinline__ void xs_prop(cx* X, cx* T, const XsPathArgs& P) {
 }
 
 // dst = base + h * deriv(src, w, t), pointwise over sites (all components at once).
-__device__ __forceinline__ void xs_deriv_update(cx* dst, const cx* base, const cx* src, const real* W, real h, double t) {
+__device__ __forceinline__ void xs_deriv_update(cx* dst, const cx* base, const cx* src, const real* W, real h, double t,
+                                                const double* prm) {
   for (int i = threadIdx.x; i < XS_G * XS_NS; i += blockDim.x) {
     const int g = i / XS_NS, s = i % XS_NS;
     int i1, i2, i3;
@@ -129,7 +222,7 @@ __device__ __forceinline__ void xs_deriv_update(cx* dst, const cx* base, const c
     for (int f = 0; f < XS_F; ++f) a[f] = src[(g * XS_F + f) * XS_NS + s];
 #pragma unroll
     for (int c = 0; c < XS_NW; ++c) w[c] = W[(g * XS_NWS + c) * XS_NS + s];
-    xs_deriv(a, w, x, y, z, (real)t, d);
+    xs_deriv(a, w, x, y, z, (real)t, prm, d);
 #pragma unroll
     for (int f = 0; f < XS_F; ++f) {
       const int j = (g * XS_F + f) * XS_NS + s;
@@ -158,7 +251,7 @@ __device__ void xs_method(cx* A, cx* B1, cx* B2, cx* B3, cx* T, const real* W, c
   xs_prop(A, T, P);
   xs_copy(B1, A);
   for (int it = 0; it < XS_ITER; ++it) {
-    xs_deriv_update(A, B1, A, W, h, t + dtr * 0.5);
+    xs_deriv_update(A, B1, A, W, h, t + dtr * 0.5, P.params);
     xs_setbound(A);
   }
   xs_axpby(A, (real)2, A, (real)-1, B1);
@@ -167,35 +260,35 @@ __device__ void xs_method(cx* A, cx* B1, cx* B2, cx* B3, cx* T, const real* W, c
   // RK4 (Applications/SDE/RK4.m:35-70)
   const real h = (real)(dtr * 0.5);
   xs_setbound(A);
-  xs_deriv_update(B1, A, A, W, h, t);
+  xs_deriv_update(B1, A, A, W, h, t, P.params);
   xs_prop(B1, T, P);
   xs_prop(A, T, P);
-  xs_deriv_update(B2, A, B1, W, h, t + dtr * 0.5);
+  xs_deriv_update(B2, A, B1, W, h, t + dtr * 0.5, P.params);
   xs_setbound(B2);
-  xs_deriv_update(B3, A, B2, W, (real)(2 * (dtr * 0.5)), t + dtr * 0.5);
+  xs_deriv_update(B3, A, B2, W, (real)(2 * (dtr * 0.5)), t + dtr * 0.5, P.params);
   xs_setbound(B3);
   for (int i = threadIdx.x; i < XS_G * XS_F * XS_NS; i += blockDim.x)
     A[i] = (B1[i] + (real)2 * B2[i] + B3[i] - A[i]) / (real)3;
   __syncthreads();
   xs_prop(A, T, P);
   xs_prop(B3, T, P);
-  xs_deriv_update(A, A, B3, W, (real)(dtr * 0.5 / 3.0), t + dtr);
+  xs_deriv_update(A, A, B3, W, (real)(dtr * 0.5 / 3.0), t + dtr, P.params);
   xs_setbound(A);
 #elif XS_METHOD == 2
   // Euler (Applications/SDE/Euler.m:77-81)
-  xs_deriv_update(A, A, A, W, (real)dtr, t);
+  xs_deriv_update(A, A, A, W, (real)dtr, t, P.params);
   xs_prop(A, T, P);
 #elif XS_METHOD == 3
   // RK2 (Applications/SDE/RK2.m:89-107): B1 holds the predictor a.
-  xs_deriv_update(B1, A, A, W, (real)dtr, t);
+  xs_deriv_update(B1, A, A, W, (real)dtr, t, P.params);
   xs_prop(A, T, P);
   xs_prop(B1, T, P);
-  xs_deriv_update(A, A, B1, W, (real)dtr, t + dtr);
+  xs_deriv_update(A, A, B1, W, (real)dtr, t + dtr, P.params);
   xs_axpby(A, (real)0.5, B1, (real)0.5, A);
 #elif XS_METHOD == 4
   // Implicit (Applications/SDE/Implicit.m:116-125)
   xs_copy(B1, A);
-  for (int it = 0; it < XS_ITER; ++it) xs_deriv_update(A, B1, A, W, (real)dtr, t + dtr);
+  for (int it = 0; it < XS_ITER; ++it) xs_deriv_update(A, B1, A, W, (real)dtr, t + dtr, P.params);
   xs_prop(A, T, P);
 #endif
   __syncthreads();
@@ -242,7 +335,7 @@ __device__ void xs_observe(const cx* A, cx* RED, int n, double t, const XsPathAr
       cx a[XS_F], r[XS_NRED];
 #pragma unroll
       for (int f = 0; f < XS_F; ++f) a[f] = A[(g * XS_F + f) * XS_NS + s];
-      xs_integrands(a, i1, i2, i3, x, y, z, (real)t, r);
+      xs_integrands(a, i1, i2, i3, x, y, z, (real)t, P.params, r);
 #pragma unroll
       for (int k = 0; k < XS_NRED; ++k) { acc[2 * k] += (double)r[k].re; acc[2 * k + 1] += (double)r[k].im; }
     }
@@ -274,7 +367,7 @@ __device__ void xs_observe(const cx* A, cx* RED, int n, double t, const XsPathAr
       cx a[XS_F], o[XS_NOUT_SITE];
 #pragma unroll
       for (int f = 0; f < XS_F; ++f) a[f] = A[(g * XS_F + f) * XS_NS + s];
-      xs_obs_site(a, RED + g * (XS_NRED > 0 ? XS_NRED : 1), x, y, z, (real)t, o);
+      xs_obs_site(a, RED + g * (XS_NRED > 0 ? XS_NRED : 1), x, y, z, (real)t, P.params, o);
 #pragma unroll
       for (int k = 0; k < XS_NOUT_SITE; ++k) { sr[k] += (double)o[k].re; si[k] += (double)o[k].im; }
     }
@@ -288,7 +381,7 @@ __device__ void xs_observe(const cx* A, cx* RED, int n, double t, const XsPathAr
     for (int k = 0; k < XS_NOUT_SCALAR; ++k) sr[k] = si[k] = 0;
     for (int g = 0; g < XS_G; ++g) {
       cx o[XS_NOUT_SCALAR];
-      xs_obs_scalar(RED + g * (XS_NRED > 0 ? XS_NRED : 1), (real)t, o);
+      xs_obs_scalar(RED + g * (XS_NRED > 0 ? XS_NRED : 1), (real)t, P.params, o);
       for (int k = 0; k < XS_NOUT_SCALAR; ++k) { sr[k] += (double)o[k].re; si[k] += (double)o[k].im; }
     }
     for (int k = 0; k < XS_NOUT_SCALAR; ++k)
@@ -345,7 +438,7 @@ extern "C" __global__ void __launch_bounds__(XS_THREADS) xs_resident(const XsPat
 #pragma unroll
       for (int c = 0; c < XS_NV; ++c) v[c] *= (real)P.vscale;
 #endif
-      xs_initial(v, x, y, z, a);
+      xs_initial(v, x, y, z, P.params, a);
     }
 #pragma unroll
     for (int f = 0; f < XS_F; ++f) A[(g * XS_F + f) * XS_NS + s] = a[f];

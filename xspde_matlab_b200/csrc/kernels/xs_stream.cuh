@@ -43,6 +43,7 @@ struct XsStreamArgs {
   double2* av;               // [nblocks][npoints][XS_OBS_STRIDE]
   double2* redpart;          // [ntraj][XS_NRG][XS_NRED] integrand sums per row group
   int* status;
+  const double* params;      // runtime values of the named scalars p.<name>
 };
 
 #define XS_RX XS_FFT_RX
@@ -171,7 +172,7 @@ __device__ __forceinline__ void xs_xpass_body(const XsStreamArgs& A) {
 #pragma unroll
         for (int c = 0; c < XS_NV; ++c) vv[c] *= (real)A.vscale;
 #endif
-        xs_initial(vv, x, yy, (real)0, a);
+        xs_initial(vv, x, yy, (real)0, A.params, a);
       }
 #pragma unroll
       for (int f = 0; f < XS_F; ++f) v[f][j] = a[f];
@@ -206,7 +207,7 @@ __device__ __forceinline__ void xs_xpass_body(const XsStreamArgs& A) {
       for (int f = 0; f < XS_F; ++f) a0[f] = a[f] = stage[(f * XS_RX + j) * XS_RX + t];
 #pragma unroll
       for (int it = 0; it < XS_ITER; ++it) {
-        xs_deriv(a, w, x, yy, (real)0, tm, d);
+        xs_deriv(a, w, x, yy, (real)0, tm, A.params, d);
 #pragma unroll
         for (int f = 0; f < XS_F; ++f) a[f] = a0[f] + h * d[f];
       }
@@ -386,13 +387,13 @@ extern "C" __global__ void __launch_bounds__(XS_OROWS * XS_RX) xs_x_obs(const Xs
       for (int f = 0; f < XS_F; ++f) a[f] = v[f][j];
 #if XS_NRED > 0
       cx rr[XS_NRED];
-      xs_integrands(a, t + XS_RX * j, y, 0, x, yy, (real)0, tt, rr);
+      xs_integrands(a, t + XS_RX * j, y, 0, x, yy, (real)0, tt, A.params, rr);
 #pragma unroll
       for (int k = 0; k < XS_NRED; ++k) { acc[2 * k] += (double)rr[k].re; acc[2 * k + 1] += (double)rr[k].im; }
 #endif
 #if XS_NOUT_SITE > 0
       cx o[XS_NOUT_SITE];
-      xs_obs_site(a, (const cx*)nullptr, x, yy, (real)0, tt, o);
+      xs_obs_site(a, (const cx*)nullptr, x, yy, (real)0, tt, A.params, o);
 #pragma unroll
       for (int k = 0; k < XS_NOUT_SITE; ++k) { sr[k][j] += (double)o[k].re; si[k][j] += (double)o[k].im; }
 #endif
@@ -454,7 +455,7 @@ extern "C" __global__ void __launch_bounds__(256) xs_stream_scalar(const XsStrea
       red[k] = mkcx((real)re, (real)im);
     }
     cx o[XS_NOUT_SCALAR];
-    xs_obs_scalar(red, (real)A.t, o);
+    xs_obs_scalar(red, (real)A.t, A.params, o);
 #pragma unroll
     for (int k = 0; k < XS_NOUT_SCALAR; ++k) { acc[2 * k] += (double)o[k].re; acc[2 * k + 1] += (double)o[k].im; }
   }

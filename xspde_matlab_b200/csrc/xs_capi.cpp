@@ -212,6 +212,8 @@ struct Problem {
   std::string deriv, initial, linear;
   std::vector<std::string> observe;
   xs::Scalars scalars;
+  std::vector<std::string> runtime_names;  // named scalars read at run time (prm[k])
+  std::vector<double> runtime_defaults;
   std::vector<int> bnd;  // [D][F][2]
   int D = 0, F = 1, NW = 0, NV = 0, NS = 1, E1 = 1;
   int N[3] = {1, 1, 1};
@@ -272,7 +274,18 @@ void setup_problem(const xs_problem* in, Problem& P) {
   P.linear = (p.linear && *p.linear) ? p.linear : "";
   for (int i = 0; i < p.nobserve; ++i) P.observe.push_back(p.observe && p.observe[i] ? p.observe[i] : "@(a,p) a");
   if (P.observe.empty()) P.observe.push_back("@(a,p) a");
-  for (int i = 0; i < p.nparams; ++i) P.scalars.values[p.param_names[i]] = p.param_values[i];
+  for (int i = 0; i < p.nparams; ++i) {
+    if (p.runtime_params) {
+      P.runtime_names.push_back(p.param_names[i]);
+      P.runtime_defaults.push_back(p.param_values[i]);
+    } else {
+      P.scalars.values[p.param_names[i]] = p.param_values[i];
+    }
+  }
+  if (p.runtime_params && !P.linear.empty()) {
+    // p.linear is evaluated on the host once: it reads the default values
+    for (int i = 0; i < p.nparams; ++i) P.scalars.values[p.param_names[i]] = p.param_values[i];
+  }
   P.p.deriv = P.p.initial = P.p.linear = nullptr;
   P.p.observe = nullptr;
   P.p.param_names = nullptr;
@@ -449,6 +462,7 @@ xs::GenCtx make_ctx(const Problem& P, std::vector<xs::Role> roles, bool reduce) 
   c.ndim = P.D;
   c.allow_reduce = reduce;
   c.scalars = &P.scalars;
+  c.runtime = P.runtime_names.empty() ? nullptr : &P.runtime_names;
   for (int d = 0; d < P.p.dimensions; ++d) {
     c.dx.push_back(P.dx[d]);
     c.dk.push_back(P.dk[d]);
@@ -467,8 +481,8 @@ void generate_functions(Problem& P, std::ostringstream& os) {
     auto g = xs::generate(fn, make_ctx(P, {Role::Field, Role::Noise, Role::Params}, false));
     if (g.len != P.F && g.len != 1)
       raise(XS_ERR_SHAPE, "p.deriv returns " + std::to_string(g.len) + " components, fields = " + std::to_string(P.F));
-    os << "__device__ __forceinline__ void xs_deriv(const cx* __restrict__ a, const real* __restrict__ w, real x, real y, real z, real t, cx* __restrict__ out) {\n";
-    os << "  (void)a; (void)w; (void)x; (void)y; (void)z; (void)t;\n";
+    os << "__device__ __forceinline__ void xs_deriv(const cx* __restrict__ a, const real* __restrict__ w, real x, real y, real z, real t, const double* __restrict__ prm, cx* __restrict__ out) {\n";
+    os << "  (void)a; (void)w; (void)x; (void)y; (void)z; (void)t; (void)prm;\n";
     if (g.len == 1 && P.F > 1) {
       os << "  cx o1[1];\n  { cx* out = o1;\n" << g.code << "  }\n";
       os << "  for (int f = 0; f < " << P.F << "; ++f) out[f] = o1[0];\n";
@@ -483,8 +497,8 @@ void generate_functions(Problem& P, std::ostringstream& os) {
     auto g = xs::generate(fn, make_ctx(P, {Role::Random, Role::Params}, false));
     if (g.len != P.F && g.len != 1)
       raise(XS_ERR_SHAPE, "p.initial returns " + std::to_string(g.len) + " components, fields = " + std::to_string(P.F));
-    os << "__device__ __forceinline__ void xs_initial(const real* __restrict__ v, real x, real y, real z, cx* __restrict__ out) {\n";
-    os << "  (void)v; (void)x; (void)y; (void)z; const real t = (real)" << fmt(P.p.origins[0]) << "; (void)t;\n";
+    os << "__device__ __forceinline__ void xs_initial(const real* __restrict__ v, real x, real y, real z, const double* __restrict__ prm, cx* __restrict__ out) {\n";
+    os << "  (void)v; (void)x; (void)y; (void)z; (void)prm; const real t = (real)" << fmt(P.p.origins[0]) << "; (void)t;\n";
     if (g.len == 1 && P.F > 1) {
       os << "  cx o1[1];\n  { cx* out = o1;\n" << g.code << "  }\n";
       os << "  for (int f = 0; f < " << P.F << "; ++f) out[f] = o1[0];\n";
@@ -520,8 +534,8 @@ void generate_functions(Problem& P, std::ostringstream& os) {
   os << "#define XS_NRED " << P.nred << "\n#define XS_NOUT_SITE " << P.nout_site << "\n#define XS_NOUT_SCALAR "
      << P.nout_scalar << "\n#define XS_OBS_STRIDE (XS_NOUT_SITE * XS_NS + XS_NOUT_SCALAR)\n";
   // integrands with bounds masks and weights
-  os << "__device__ __forceinline__ void xs_integrands(const cx* __restrict__ a, int i1, int i2, int i3, real x, real y, real z, real t, cx* __restrict__ rr) {\n";
-  os << "  (void)a; (void)i1; (void)i2; (void)i3; (void)x; (void)y; (void)z; (void)t; (void)rr;\n";
+  os << "__device__ __forceinline__ void xs_integrands(const cx* __restrict__ a, int i1, int i2, int i3, real x, real y, real z, real t, const double* __restrict__ prm, cx* __restrict__ rr) {\n";
+  os << "  (void)a; (void)i1; (void)i2; (void)i3; (void)x; (void)y; (void)z; (void)t; (void)rr; (void)prm;\n";
   int off = 0;
   for (auto& o : P.obs) {
     for (auto& r : o.gen.reductions) {
@@ -551,15 +565,15 @@ void generate_functions(Problem& P, std::ostringstream& os) {
     }
   }
   os << "}\n";
-  os << "__device__ __forceinline__ void xs_obs_site(const cx* __restrict__ a, const cx* __restrict__ redall, real x, real y, real z, real t, cx* __restrict__ outall) {\n";
-  os << "  (void)a; (void)redall; (void)x; (void)y; (void)z; (void)t; (void)outall;\n";
+  os << "__device__ __forceinline__ void xs_obs_site(const cx* __restrict__ a, const cx* __restrict__ redall, real x, real y, real z, real t, const double* __restrict__ prm, cx* __restrict__ outall) {\n";
+  os << "  (void)a; (void)redall; (void)x; (void)y; (void)z; (void)t; (void)outall; (void)prm;\n";
   for (auto& o : P.obs)
     if (o.spatial)
       os << "  {\n    const cx* red = redall + " << o.red_off << "; (void)red;\n    cx* out = outall + " << o.out_off
          << ";\n" << o.gen.code << "  }\n";
   os << "}\n";
-  os << "__device__ __forceinline__ void xs_obs_scalar(const cx* __restrict__ redall, real t, cx* __restrict__ outall) {\n";
-  os << "  (void)redall; (void)t; (void)outall; const cx* a = nullptr; const real x = 0, y = 0, z = 0; (void)a; (void)x; (void)y; (void)z;\n";
+  os << "__device__ __forceinline__ void xs_obs_scalar(const cx* __restrict__ redall, real t, const double* __restrict__ prm, cx* __restrict__ outall) {\n";
+  os << "  (void)redall; (void)t; (void)outall; (void)prm; const cx* a = nullptr; const real x = 0, y = 0, z = 0; (void)a; (void)x; (void)y; (void)z;\n";
   for (auto& o : P.obs)
     if (!o.spatial)
       os << "  {\n    const cx* red = redall + " << o.red_off << "; (void)red;\n    cx* out = outall + " << o.out_off
@@ -630,7 +644,8 @@ struct xs_handle {
   StreamPlan sp;
   int path_kind = 0;
   cudaStream_t stream = nullptr;
-  DevBuf d_prop[2], d_prop2[2], d_tmat, d_obs, d_av, d_ain, d_aout, d_status, d_w, d_field, d_redpart, d_pstep;
+  DevBuf d_prop[2], d_prop2[2], d_tmat, d_obs, d_av, d_ain, d_aout, d_status, d_w, d_field, d_redpart, d_pstep,
+      d_params;
   double pstep_dtr = -1;
   double prop_dtr[2] = {-1, -1}, prop2_dtr[2] = {-1, -1};
   // launch accounting (xs_kernel_stats)
@@ -695,6 +710,43 @@ void plan_resident(xs_handle& h, int total_traj) {
   rp.threads = std::min(256, std::max(32, (items + 31) / 32 * 32));
   rp.smem = resident_smem(h, rp.G, rp.narr);
   h.rp = rp;
+}
+
+// A space dimension (0-based d) is transformed by the shared-memory Stockham
+// FFT when it is periodic for every field and its length is a power of two.
+bool fft_dim(const Problem& P, int d) {
+  if (d >= P.D) return false;
+  const int n = P.N[d];
+  if (n < 2 || (n & (n - 1)) || n > 4096) return false;
+  for (int f = 0; f < P.F; ++f)
+    if (P.type(d, f) != 0) return false;
+  return true;
+}
+
+// Stockham stage sequence of one dimension (length n, site stride sd): an even
+// number of stages (so the result lands back in X) of radix 2, 4 or 8 with
+// the larger radices first; a lone radix-2 stage is followed by a copy.
+std::string gen_fft_stages(int D, int n, int sd) {
+  int k = 0;
+  while ((1 << k) < n) ++k;
+  int S = (k + 2) / 3;
+  if (S % 2 == 1 && k >= S + 1) ++S;
+  std::vector<int> bits(S, k / S);
+  for (int i = 0; i < k % S; ++i) ++bits[i];
+  std::ostringstream os;
+  os << "template <> __device__ __forceinline__ void xs_fft_d<" << D
+     << ">(cx* X, cx* T, const cx* __restrict__ tw, int inv) { ";
+  int nsp = 1;
+  for (int i = 0; i < S; ++i) {
+    const int R = 1 << bits[i];
+    os << "xs_fft_stage<" << n << ", " << sd << ", " << R << ", " << nsp << ", " << (i == 0 ? "true" : "false") << ", "
+       << (i == S - 1 ? "true" : "false") << ">(" << (i % 2 ? "T, X" : "X, T") << ", tw, inv); __syncthreads(); ";
+    nsp *= R;
+  }
+  if (S % 2)
+    os << "for (int i = threadIdx.x; i < XS_G * XS_F * XS_NS; i += blockDim.x) X[i] = T[i]; __syncthreads(); ";
+  os << "} ";
+  return os.str();
 }
 
 int isqrt_pow2(int n) {
@@ -828,14 +880,34 @@ void build_source(xs_handle& h) {
   emit_common_header(h, os);
   os << "#define XS_G " << h.rp.G << "\n#define XS_THREADS " << h.rp.threads << "\n#define XS_NARR " << h.rp.narr << "\n";
   os << "#define XS_SMEM_BYTES " << h.rp.smem << "\n";
+  {
+    std::string stages;
+    int sd = 1;
+    for (int d = 0; d < 3; ++d) {
+      const bool f = fft_dim(P, d);
+      os << "#define XS_FFTD" << d + 1 << " " << (f ? 1 : 0) << "\n";
+      if (f) stages += gen_fft_stages(d + 1, P.N[d], sd);
+      if (d < P.D) sd *= P.N[d];
+    }
+    os << "#define XS_FFT_STAGES " << stages << "\n";
+  }
   os << fns.str();
   os << xs_kernel_source_resident << "\n";
   h.source = os.str();
 }
 
+void upload_params(xs_handle& h) {
+  const Problem& P = h.P;
+  if (P.runtime_defaults.empty()) return;
+  h.d_params.ensure(P.runtime_defaults.size() * 8);
+  CUDA_CHECK(cudaMemcpy(h.d_params.p, P.runtime_defaults.data(), P.runtime_defaults.size() * 8,
+                        cudaMemcpyHostToDevice));
+}
+
 void load_module(xs_handle& h) {
   if (h.loaded) return;
   ensure_device();
+  upload_params(h);
   if (h.kind == 2) {
     std::string cubin = nvrtc_compile(h.source, "xs_stream", nullptr);
     Driver& d = driver();
@@ -880,6 +952,10 @@ void load_module(xs_handle& h) {
     h.tmat_off[d + 1] = (int)all.size();
     int n = P.N[d];
     if (n <= 1) continue;
+    if (h.kind == 1 && fft_dim(P, d)) {  // Stockham twiddles exp(-2 pi i m / n)
+      for (int m = 0; m < n; ++m) all.push_back(std::polar(1.0, -2 * M_PI * (double)m / n));
+      continue;
+    }
     for (int f = 0; f < P.F; ++f)
       for (int dir = 0; dir < 2; ++dir) {
         auto M = transform_matrix(P.type(d, f), dir == 1, n);
@@ -940,6 +1016,7 @@ struct PathArgsHost {
   int single_step;
   int pad1;
   const double* w_in;
+  const double* params;
 };
 
 size_t av_stride(const Problem& P) { return (size_t)P.nout_site * P.NS + P.nout_scalar; }
@@ -1008,6 +1085,7 @@ void launch_resident(xs_handle& h, int first_block, int nblocks, int nc, const v
   a.a_out = a_out_dev;
   a.obs = h.d_obs.p;
   a.status = (int*)h.d_status.p;
+  a.params = (const double*)h.d_params.p;
   void* params[] = {&a};
   xs_launch(h, XS_KERNEL_RESIDENT, h.f_resident, nctas, 1, 1, h.rp.threads, (unsigned)h.rp.smem, st, params,
             "launch xs_resident");
@@ -1051,6 +1129,7 @@ struct StreamArgsHost {
   void* av;
   void* redpart;
   int* status;
+  const double* params;
 };
 
 // Streaming schedule of one xpath call (Simulator/xpath.m:137-194) for MP:
@@ -1086,6 +1165,7 @@ void launch_stream(xs_handle& h, int first_block, int nblocks, int nc, const voi
   a.av = av_dev;
   a.redpart = h.d_redpart.p;
   a.status = (int*)h.d_status.p;
+  a.params = (const double*)h.d_params.p;
   void* params[] = {&a};
   const unsigned xgrid = (unsigned)((size_t)total * P.N[1] / sp.XROWS);
   const unsigned sgrid = (unsigned)((size_t)total * P.F * (P.N[0] / sp.TX));
@@ -1391,6 +1471,7 @@ XS_API xs_status xs_run_path_device_noalloc(xs_handle* h, int first_block, int n
     a.a_out = nullptr;
     a.obs = scratch;
     a.status = (int*)h->d_status.p;
+    a.params = (const double*)h->d_params.p;
     void* params[] = {&a};
     cu_check(driver().launch(h->f_resident, nctas, 1, 1, h->rp.threads, 1, 1, (unsigned)h->rp.smem, (CUstream)st,
                              params, nullptr),
@@ -1640,6 +1721,7 @@ XS_API xs_status xs_step(xs_handle* h, double* a_inout, const double* w, double 
     a.status = (int*)h->d_status.p;
     a.single_step = 1;
     a.w_in = (w && wn) ? (const double*)h->d_w.p : nullptr;
+    a.params = (const double*)h->d_params.p;
     void* params[] = {&a};
     xs_launch(*h, XS_KERNEL_RESIDENT, h->f_resident, (unsigned)(ntraj / h->rp.G), 1, 1, h->rp.threads,
               (unsigned)h->rp.smem, h->stream, params, "launch xs_resident (step)");

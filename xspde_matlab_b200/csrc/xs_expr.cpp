@@ -590,6 +590,9 @@ struct Gen {
       if (f == "origins") return vec(c->origins);
       if (f == "ranges") return vec(c->ranges);
       if (f == "dt") { out = {C(c->dt)}; return true; }
+      if (c->runtime)
+        for (auto& r : *c->runtime)
+          if (r == f) return false;  // a per-instance value: not a compile-time constant
       if (c->scalars) {
         auto it = c->scalars->values.find(f);
         if (it != c->scalars->values.end()) { out = {C(it->second)}; return true; }
@@ -651,6 +654,13 @@ struct Gen {
     if (f == "z") return coord(3);
     if (f == "Dx" || f == "Dy" || f == "Dz" || f == "kx" || f == "ky" || f == "kz" || f == "D" || f == "k")
       throw GrammarError("k-space grid 'p." + f + "' is only available in p.linear");
+    if (ctx.runtime)
+      for (size_t k = 0; k < ctx.runtime->size(); ++k)
+        if ((*ctx.runtime)[k] == f) {
+          Val r;
+          r.c = {"((real)prm[" + std::to_string(k) + "])"};
+          return r;
+        }
     Vec v;
     auto e = const_env();
     if (e.field(f, v)) return constant(v);

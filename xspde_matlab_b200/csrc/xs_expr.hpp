@@ -57,6 +57,7 @@ struct GenCtx {
   int ndim = 0;              // space dimensions
   bool allow_reduce = false; // Int/Ave allowed (observe)
   const Scalars* scalars = nullptr;
+  const std::vector<std::string>* runtime = nullptr;  // p.<name> read at run time as prm[k]
   std::vector<double> dx, dk, origins, ranges;  // index 0 = time
   double dt = 0;
 };
