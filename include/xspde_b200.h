@@ -235,6 +235,34 @@ enum {
 XS_API xs_status xs_set_kernel_timing(xs_handle* h, int on);
 XS_API xs_status xs_kernel_stats(xs_handle* h, int reset, double* ms_out, long long* launches_out);
 
+/* Uneven batch (no counterpart in the reference): many independent problems,
+ * each one ensemble block (ensembles(2) = ensembles(3) = 1, checks = 0),
+ * integrated by ONE CUDA-graph launch.  Items whose generated kernels agree
+ * (same lattice, fields, expressions, method, precision; set runtime_params
+ * so that named scalars differ per item) share a persistent kernel that pulls
+ * (item, trajectory tile) units from a longest-first queue; items too large
+ * for shared memory run their streaming launches inside the same graph.
+ *   xs_batch_create  groups the items (host only; copies everything it needs)
+ *   xs_batch_tune    picks each variant's tile: mode 0 heuristic, mode 1 times
+ *                    the candidates on the device (cached per source and GPU)
+ *   xs_batch_run     captures the graph on first use, then launches it on
+ *                    `stream` (NULL: the batch's own stream); asynchronous
+ *   xs_batch_sync    waits for the device and reports kernel status
+ *   xs_batch_results item means in the layout of xs_run_path's av_out
+ *                    (xs_batch_av_doubles doubles)
+ *   xs_batch_info    item >= 0: {variant, path (1 resident, 2 streaming), G,
+ *                    threads, CTAs, units}; item < 0: {items, variants,
+ *                    streaming items, kernel launches per run} */
+typedef struct xs_batch xs_batch;
+XS_API xs_status xs_batch_create(const xs_problem* items, int nitems, xs_batch** out);
+XS_API void xs_batch_destroy(xs_batch* b);
+XS_API xs_status xs_batch_tune(xs_batch* b, int mode);
+XS_API xs_status xs_batch_run(xs_batch* b, void* stream);
+XS_API xs_status xs_batch_sync(xs_batch* b);
+XS_API size_t xs_batch_av_doubles(const xs_batch* b, int item);
+XS_API xs_status xs_batch_results(xs_batch* b, int item, double* av_out);
+XS_API xs_status xs_batch_info(const xs_batch* b, int item, int* info, int ninfo);
+
 /* Compile-only check (no device needed): parse and NVRTC-compile the kernels
  * of a problem for sm_100a.  Writes the compile log (truncated to n). */
 XS_API xs_status xs_compile_check(const xs_problem* prob, char* log, size_t n);

@@ -17,7 +17,9 @@ MAXDIM = 4
 EXPORTS = ["xs_create", "xs_destroy", "xs_last_error", "xs_version", "xs_observe_info", "xs_av_doubles_per_block",
            "xs_run_path", "xs_run_path_device", "xs_sync", "xs_noise", "xs_random", "xs_step", "xs_compile_check",
            "xs_set_kernel_timing", "xs_kernel_stats", "xs_run_path_device_noalloc", "xs_noise_features",
-           "xs_mlp_sizes", "xs_mlp_forward", "xs_mlp_train_grad", "xs_mlp_adam"]
+           "xs_mlp_sizes", "xs_mlp_forward", "xs_mlp_train_grad", "xs_mlp_adam", "xs_batch_create",
+           "xs_batch_destroy", "xs_batch_tune", "xs_batch_run", "xs_batch_sync", "xs_batch_av_doubles",
+           "xs_batch_results", "xs_batch_info"]
 KERNEL_KINDS = ["resident", "obs_reduce", "x_init", "x_step", "x_final", "y_pass", "x_obs", "scalar"]
 
 
@@ -117,6 +119,22 @@ def lib():
         L.xs_mlp_adam.argtypes = [ctypes.c_size_t, vp, vp, vp, vp, ctypes.c_float, ctypes.c_float, ctypes.c_float,
                                   ctypes.c_float, ci, ctypes.c_float, vp]
         L.xs_mlp_adam.restype = ci
+        L.xs_batch_create.argtypes = [vp, ci, P(vp)]
+        L.xs_batch_create.restype = ci
+        L.xs_batch_destroy.argtypes = [vp]
+        L.xs_batch_destroy.restype = None
+        L.xs_batch_tune.argtypes = [vp, ci]
+        L.xs_batch_tune.restype = ci
+        L.xs_batch_run.argtypes = [vp, vp]
+        L.xs_batch_run.restype = ci
+        L.xs_batch_sync.argtypes = [vp]
+        L.xs_batch_sync.restype = ci
+        L.xs_batch_av_doubles.argtypes = [vp, ci]
+        L.xs_batch_av_doubles.restype = ctypes.c_size_t
+        L.xs_batch_results.argtypes = [vp, ci, vp]
+        L.xs_batch_results.restype = ci
+        L.xs_batch_info.argtypes = [vp, ci, P(ci), ci]
+        L.xs_batch_info.restype = ci
         _ = dp
         _lib = L
     return _lib

@@ -318,9 +318,8 @@ __device__ __forceinline__ void xs_noise(real* W, real* Wp, int mode, int draw, 
 }
 
 // Observables at one output time: per-CTA sums over its trajectories.
-__device__ void xs_observe(const cx* A, cx* RED, int n, double t, const XsPathArgs& P, double* wsum) {
-  const int cta = blockIdx.x;
-  const int nctas = gridDim.x;
+__device__ void xs_observe(const cx* A, cx* RED, int n, double t, const XsPathArgs& P, double* wsum, int cta,
+                           int nctas) {
   double2* out = P.obs + ((size_t)n * nctas + cta) * XS_OBS_STRIDE;
 #if XS_NRED > 0
   // full-space reductions (Int/Ave) per trajectory
@@ -391,8 +390,28 @@ __device__ void xs_observe(const cx* A, cx* RED, int n, double t, const XsPathAr
   __syncthreads();
 }
 
-extern "C" __global__ void __launch_bounds__(XS_THREADS) xs_resident(const XsPathArgs P) {
-  extern __shared__ __align__(16) unsigned char xs_smem[];
+extern __shared__ __align__(16) unsigned char xs_smem[];
+
+// Shared-memory layout of one CTA (XS_SMEM_BYTES in total).  False, with
+// status bit 1 set, when this launch's dynamic shared memory or block size do
+// not match the layout; the CTA must then return without touching it.
+__device__ __forceinline__ bool xs_layout_ok(int* status) {
+  constexpr size_t GF = (size_t)XS_G * XS_F * XS_NS;
+  constexpr size_t need = XS_NARR * GF * sizeof(cx) + (size_t)XS_G * (XS_NRED > 0 ? XS_NRED : 1) * sizeof(cx) +
+                          32 * 2 * (XS_NRED > 0 ? XS_NRED : 1) * sizeof(double) +
+                          2 * (size_t)XS_G * XS_NWS * XS_NS * sizeof(real);
+  u32 dyn;
+  asm volatile("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn));
+  if (need > (size_t)dyn || need != (size_t)XS_SMEM_BYTES || (int)blockDim.x != XS_THREADS) {
+    if (threadIdx.x == 0) atomicOr(status, 2);
+    return false;
+  }
+  return true;
+}
+
+// One CTA's share of an xpath call: trajectories cta*G .. cta*G+G-1 of P,
+// observable partial sums in row `cta` of `nctas`.
+__device__ void xs_resident_run(const XsPathArgs& P, int cta, int nctas) {
   constexpr int GF = XS_G * XS_F * XS_NS;
   cx* A = (cx*)xs_smem;
   cx* B1 = A + GF;
@@ -403,18 +422,10 @@ extern "C" __global__ void __launch_bounds__(XS_THREADS) xs_resident(const XsPat
   double* wsum = (double*)(RED + XS_G * (XS_NRED > 0 ? XS_NRED : 1));  // [32][2*NRED]
   real* W = (real*)(wsum + 32 * 2 * (XS_NRED > 0 ? XS_NRED : 1));
   real* Wp = W + XS_G * XS_NWS * XS_NS;
-  const int g0 = blockIdx.x * XS_G;
-  {
-    // The layout above must fit the dynamic shared memory of this launch;
-    // refuse to run (status bit 1) rather than touch memory outside it.
-    u32 dyn;
-    asm volatile("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn));
-    const size_t need = (size_t)((unsigned char*)(Wp + XS_G * XS_NWS * XS_NS) - xs_smem);
-    if (need > (size_t)dyn || need != (size_t)XS_SMEM_BYTES || (int)blockDim.x != XS_THREADS ||
-        (blockIdx.x + 1) * XS_G > (unsigned)P.ntraj) {
-      if (threadIdx.x == 0) atomicOr(P.status, 2);
-      return;
-    }
+  const int g0 = cta * XS_G;
+  if ((cta + 1) * XS_G > P.ntraj || cta >= nctas) {
+    if (threadIdx.x == 0) atomicOr(P.status, 2);
+    return;
   }
 
   // initial field: p.initial(v,p) with v = p.randomgen(p) (xensemble.m:53-64)
@@ -476,7 +487,7 @@ extern "C" __global__ void __launch_bounds__(XS_THREADS) xs_resident(const XsPat
       }
       if (step == 0) {
         __syncthreads();
-        xs_observe(A, RED, n, t, P, wsum);
+        xs_observe(A, RED, n, t, P, wsum, cta, nctas);
       }
     }
   }
@@ -493,6 +504,107 @@ extern "C" __global__ void __launch_bounds__(XS_THREADS) xs_resident(const XsPat
     }
   }
   if (bad) atomicOr(P.status, 1);
+  __syncthreads();
+}
+
+extern "C" __global__ void __launch_bounds__(XS_THREADS) xs_resident(const XsPathArgs P) {
+  if (!xs_layout_ok(P.status)) return;
+  xs_resident_run(P, blockIdx.x, gridDim.x);
+}
+
+// ---- uneven batch -------------------------------------------------------------
+// Many independent problems of one compiled variant (same lattice, fields,
+// expressions and tile) differing in trajectories, steps, time step, seed and
+// the runtime scalars.  The persistent kernel pulls units (item, group of G
+// trajectories) from a longest-first queue with one atomic per unit; the last
+// unit of an item to finish reduces the item's partial sums in a fixed order,
+// so the result does not depend on the schedule.
+struct XsBatchItem {
+  int ntraj, steps, npoints, seq;
+  u32 seed;
+  int block0;
+  int nunits;
+  int pad;
+  double wscale, vscale, dtr, t0;
+  const double2* prop;   // [XS_PROP_COMPS][XS_NS] exp(L dtr / ipsteps) of this item
+  double2* part;         // [npoints][nunits][XS_OBS_STRIDE] partial sums
+  double2* av;           // [npoints][XS_OBS_STRIDE] means over the item's trajectories
+  const double* params;  // runtime scalars of this item
+  int* done;             // units finished
+  int pad2[2];
+};
+
+struct XsBatchArgs {
+  const XsBatchItem* items;
+  const int2* units;     // (item, unit within item), longest first
+  int nunits;
+  int pad;
+  int* next;             // queue head (zeroed before the launch)
+  int* status;
+  const cx* tmat;
+  int tmat_off[4];
+};
+
+extern "C" __global__ void __launch_bounds__(XS_THREADS) xs_batch(const XsBatchArgs B) {
+  if (!xs_layout_ok(B.status)) return;
+  __shared__ int s_unit, s_last;
+  for (;;) {
+    if (threadIdx.x == 0) s_unit = atomicAdd(B.next, 1);
+    __syncthreads();
+    const int u = s_unit;
+    __syncthreads();
+    if (u >= B.nunits) break;
+    const int2 un = B.units[u];
+    const XsBatchItem& it = B.items[un.x];
+    XsPathArgs P;
+    P.ntraj = it.ntraj;
+    P.ens1 = it.ntraj;
+    P.block0 = it.block0;
+    P.nc = 1;
+    P.checks = 0;
+    P.npoints = it.npoints;
+    P.steps = it.steps;
+    P.seq = it.seq;
+    P.seed = it.seed;
+    P.pad0 = 0;
+    P.wscale = it.wscale;
+    P.vscale = it.vscale;
+    P.dtr = it.dtr;
+    P.t0 = it.t0;
+    P.prop = it.prop;
+    P.tmat = B.tmat;
+#pragma unroll
+    for (int d = 0; d < 4; ++d) P.tmat_off[d] = B.tmat_off[d];
+    P.a_in = nullptr;
+    P.a_out = nullptr;
+    P.obs = it.part;
+    P.status = B.status;
+    P.single_step = 0;
+    P.pad1 = 0;
+    P.w_in = nullptr;
+    P.params = it.params;
+    xs_resident_run(P, un.y, it.nunits);
+    // publish this unit's partial sums, then count it (threadFenceReduction pattern)
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) s_last = atomicAdd(it.done, 1) == it.nunits - 1;
+    __syncthreads();
+    if (s_last && XS_OBS_STRIDE > 0) {
+      __threadfence();
+      const double inv = 1.0 / (double)it.ntraj;
+      for (int k = threadIdx.x; k < it.npoints * XS_OBS_STRIDE; k += blockDim.x) {
+        const int n = k / XS_OBS_STRIDE, q = k % XS_OBS_STRIDE;
+        double re = 0, im = 0;
+        for (int c = 0; c < it.nunits; ++c) {
+          const double2 v = __ldcg(it.part + ((size_t)n * it.nunits + c) * XS_OBS_STRIDE + q);
+          re += v.x;
+          im += v.y;
+        }
+        it.av[k] = make_double2(re * inv, im * inv);
+      }
+    }
+    __syncthreads();
+  }
 }
 
 // Block means over trajectories (xdata.m:84): av[b][n][k] = sum over the CTAs

@@ -5,6 +5,10 @@
 
 #include <cuda.h>
 #include <cuda_runtime.h>
+#include <atomic>
+#include <functional>
+#include <numeric>
+#include <thread>
 #include <nvrtc.h>
 
 #include <algorithm>
@@ -61,6 +65,7 @@ typedef CUresult (*PFN_FuncSetAttribute)(CUfunction, CUfunction_attribute, int);
 typedef CUresult (*PFN_LaunchKernel)(CUfunction, unsigned, unsigned, unsigned, unsigned, unsigned, unsigned,
                                      unsigned, CUstream, void**, void**);
 typedef CUresult (*PFN_GetErrorString)(CUresult, const char**);
+typedef CUresult (*PFN_Occupancy)(int*, CUfunction, int, size_t);
 
 struct Driver {
   PFN_ModuleLoadData load = nullptr;
@@ -69,6 +74,7 @@ struct Driver {
   PFN_FuncSetAttribute setattr = nullptr;
   PFN_LaunchKernel launch = nullptr;
   PFN_GetErrorString errstr = nullptr;
+  PFN_Occupancy occupancy = nullptr;
 };
 
 template <class T>
@@ -93,6 +99,7 @@ Driver& driver() {
       resolve("cuFuncSetAttribute", d.setattr);
       resolve("cuLaunchKernel", d.launch);
       resolve("cuGetErrorString", d.errstr);
+      resolve("cuOccupancyMaxActiveBlocksPerMultiprocessor", d.occupancy);
     } catch (const XsError& e) {
       err = e.msg;
     }
@@ -187,7 +194,8 @@ std::string nvrtc_compile(const std::string& src, const std::string& name, std::
   nvrtcGetCUBIN(prog, &cubin[0]);
   nvrtcDestroyProgram(&prog);
   mkdirs(dir);
-  std::string tmp = path + ".tmp" + std::to_string((long)getpid());
+  std::string tmp = path + ".tmp" + std::to_string((long)getpid()) + "_" +
+                    std::to_string(std::hash<std::thread::id>{}(std::this_thread::get_id()));
   {
     std::ofstream f(tmp, std::ios::binary);
     f.write(cubin.data(), (std::streamsize)cubin.size());
@@ -643,6 +651,8 @@ struct xs_handle {
              f_scalar = nullptr;
   StreamPlan sp;
   int path_kind = 0;
+  int force_G = 0, force_threads = 0;  // resident tile fixed by the caller (uneven batch)
+  CUfunction f_batch = nullptr;
   cudaStream_t stream = nullptr;
   DevBuf d_prop[2], d_prop2[2], d_tmat, d_obs, d_av, d_ain, d_aout, d_status, d_w, d_field, d_redpart, d_pstep,
       d_params;
@@ -697,6 +707,17 @@ void plan_resident(xs_handle& h, int total_traj) {
   const size_t limit = 200 * 1024;
   if (resident_smem(h, 1, rp.narr) > limit)
     raise(XS_ERR_UNSUPPORTED, "field of one trajectory does not fit in shared memory for the resident path");
+  if (h.force_G > 0) {
+    if (resident_smem(h, h.force_G, rp.narr) > limit) raise(XS_ERR_UNSUPPORTED, "tile does not fit in shared memory");
+    if (h.force_threads % 32 || h.force_threads < 0 || h.force_threads > 1024)
+      raise(XS_ERR_ARG, "threads per CTA must be a multiple of 32, at most 1024");
+    rp.G = h.force_G;
+    const int items = rp.G * P.NS * P.F;
+    rp.threads = h.force_threads ? h.force_threads : std::min(256, std::max(32, (items + 31) / 32 * 32));
+    rp.smem = resident_smem(h, rp.G, rp.narr);
+    h.rp = rp;
+    return;
+  }
   int best = 1;
   for (int G = 1; G <= P.E1 && G <= 1024; ++G) {
     if (P.E1 % G) continue;
@@ -936,13 +957,17 @@ void load_module(xs_handle& h) {
   Driver& d = driver();
   cu_check(d.load(&h.mod, cubin.data()), "cuModuleLoadData");
   cu_check(d.getfn(&h.f_resident, h.mod, "xs_resident"), "cuModuleGetFunction(xs_resident)");
+  cu_check(d.getfn(&h.f_batch, h.mod, "xs_batch"), "cuModuleGetFunction(xs_batch)");
   cu_check(d.getfn(&h.f_reduce, h.mod, "xs_obs_reduce"), "cuModuleGetFunction(xs_obs_reduce)");
   cu_check(d.getfn(&h.f_noise, h.mod, "xs_export_noise"), "cuModuleGetFunction(xs_export_noise)");
   cu_check(d.getfn(&h.f_random, h.mod, "xs_export_random"), "cuModuleGetFunction(xs_export_random)");
   cu_check(d.getfn(&h.f_feat, h.mod, "xs_noise_features"), "cuModuleGetFunction(xs_noise_features)");
-  if (h.rp.smem > 48 * 1024)
+  if (h.rp.smem > 48 * 1024) {
     cu_check(d.setattr(h.f_resident, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, (int)h.rp.smem),
              "cuFuncSetAttribute(max dynamic smem)");
+    cu_check(d.setattr(h.f_batch, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, (int)h.rp.smem),
+             "cuFuncSetAttribute(max dynamic smem)");
+  }
   CUDA_CHECK(cudaStreamCreateWithFlags(&h.stream, cudaStreamNonBlocking));
   // dense transform matrices (per space dim, per component, fwd/inv)
   const Problem& P = h.P;
@@ -1738,6 +1763,660 @@ XS_API xs_status xs_step(xs_handle* h, double* a_inout, const double* w, double 
         }
     if (status & 2) raise(XS_ERR_SHAPE, "kernel refused a launch whose shared-memory layout or grid did not match");
     if (status & 1) raise(XS_ERR_NAN, "a trajectory became non-finite (NaN/Inf) during the step");
+    return XS_OK;
+  });
+}
+
+// ---------------------------------------------------------------------------
+// Uneven batch: many independent problems in one CUDA-graph launch
+// ---------------------------------------------------------------------------
+namespace {
+
+struct BatchItemHost {  // mirrors XsBatchItem
+  int ntraj, steps, npoints, seq;
+  unsigned seed;
+  int block0, nunits, pad;
+  double wscale, vscale, dtr, t0;
+  const void* prop;
+  void* part;
+  void* av;
+  const double* params;
+  int* done;
+  int pad2[2];
+};
+static_assert(sizeof(BatchItemHost) == 112, "XsBatchItem layout");
+
+struct BatchArgsHost {  // mirrors XsBatchArgs
+  const void* items;
+  const void* units;
+  int nunits, pad;
+  int* next;
+  int* status;
+  const void* tmat;
+  int tmat_off[4];
+};
+static_assert(sizeof(BatchArgsHost) == 64, "XsBatchArgs layout");
+
+struct BatchVariant {
+  std::string key;                 // generated source at a unit tile
+  std::vector<int> items;
+  std::unique_ptr<xs_handle> h;    // compiled at the chosen tile
+  int G = 0, threads = 0, grid = 0, nunits = 0, gcd_traj = 0;
+  bool tuned = false;
+  double probe_us = 0;             // autotuner: probe microseconds per trajectory-step
+  double work = 0;
+  DevBuf d_items, d_units, d_next;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t join = nullptr;
+  ~BatchVariant() {
+    if (join) cudaEventDestroy(join);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+struct BatchEntry {
+  std::unique_ptr<xs_handle> h;    // the item's problem; streaming items also run through it
+  int variant = -1;                // resident variant, -1 = streaming path
+  size_t av_off = 0, part_off = 0, prop_off = 0, param_off = 0;  // element offsets
+  int nunits = 0;
+  double work = 0;                 // trajectory-steps x sites
+};
+
+int ntraj_of(const Problem& P) { return P.p.ensembles[0]; }
+
+double item_dtr(const Problem& P) { return P.dt / P.p.steps; }  // fine pass (xensemble.m:41-45)
+
+std::vector<cd> prop_table(const Problem& P, double dtr) {
+  std::vector<cd> pr(P.L.size());
+  const double dt = dtr / P.p.ipsteps;  // xpropfactor.m:28
+  for (size_t i = 0; i < P.L.size(); ++i) pr[i] = std::exp(P.L[i] * dt);
+  return pr;
+}
+
+// Tile chosen by the autotuner, cached per variant source and device.
+std::string tile_cache_path() { return cache_dir() + "/batch_tiles.txt"; }
+
+std::string tile_key(const std::string& src) {
+  cudaDeviceProp prop{};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  cudaGetDeviceProperties(&prop, dev);
+  char b[64];
+  snprintf(b, sizeof b, "%016llx_%d", (unsigned long long)fnv1a(src + prop.name), prop.multiProcessorCount);
+  return b;
+}
+
+bool tile_lookup(const std::string& key, int& G, int& threads) {
+  std::ifstream f(tile_cache_path());
+  std::string k;
+  int g, t;
+  while (f >> k >> g >> t)
+    if (k == key) {
+      G = g;
+      threads = t;
+      return true;
+    }
+  return false;
+}
+
+void tile_store(const std::string& key, int G, int threads) {
+  mkdirs(cache_dir());
+  std::ofstream f(tile_cache_path(), std::ios::app);
+  f << key << " " << G << " " << threads << "\n";
+}
+
+}  // namespace
+
+struct xs_batch {
+  std::vector<std::unique_ptr<BatchVariant>> variants;
+  std::vector<std::unique_ptr<BatchEntry>> items;
+  DevBuf d_av, d_part, d_prop, d_params, d_done, d_status;
+  size_t av_total = 0;
+  cudaStream_t stream = nullptr;
+  std::vector<cudaStream_t> side;
+  std::vector<cudaEvent_t> side_join;
+  cudaEvent_t fork = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  bool prepared = false;
+  int launches_per_run = 0;
+  ~xs_batch() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    for (auto e : side_join) cudaEventDestroy(e);
+    for (auto s : side) cudaStreamDestroy(s);
+    if (fork) cudaEventDestroy(fork);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+namespace {
+
+void batch_drop_graph(xs_batch& b) {
+  if (b.exec) cudaGraphExecDestroy(b.exec);
+  if (b.graph) cudaGraphDestroy(b.graph);
+  b.exec = nullptr;
+  b.graph = nullptr;
+  b.prepared = false;
+}
+
+// Candidate tiles of a variant: G trajectories per CTA (a power of two that
+// divides every item's trajectory count and fits shared memory), threads.
+std::vector<std::pair<int, int>> tile_candidates(const BatchVariant& v, const xs_handle& proto) {
+  const Problem& P = proto.P;
+  const int narr = method_arrays(P.p.method);
+  std::vector<int> Gs;
+  for (int G = 1; G <= 1024 && v.gcd_traj % G == 0; G *= 2) {
+    if (resident_smem(proto, G, narr) > 200 * 1024) break;
+    if ((size_t)G * P.NS > 16384 && G > 1) break;
+    Gs.push_back(G);
+  }
+  if (Gs.empty()) raise(XS_ERR_UNSUPPORTED, "no trajectory tile of this variant fits shared memory");
+  std::vector<std::pair<int, int>> out;
+  const int nG = (int)Gs.size();
+  for (int i = std::max(0, nG - 3); i < nG; ++i) {
+    const int G = Gs[i];
+    const int items = G * P.NS * P.F;
+    for (int t : {128, 256, 512})
+      if (t <= std::max(128, (items + 31) / 32 * 32)) out.push_back({G, t});
+  }
+  return out;
+}
+
+std::unique_ptr<xs_handle> variant_handle(const xs_problem& raw, const Problem& P, bool fp64, int G, int threads) {
+  auto h = std::make_unique<xs_handle>();
+  h->P = P;  // grid, expressions and L already set up
+  h->fp64 = fp64;
+  h->path_kind = 1;
+  h->force_G = G;
+  h->force_threads = threads;
+  (void)raw;
+  build_source(*h);
+  return h;
+}
+
+// Items table and longest-first unit queue of a variant at its tile.
+void variant_tables(xs_batch& b, BatchVariant& v, int steps_cap, int points_cap, DevBuf& d_items, DevBuf& d_units,
+                    void* part_base) {
+  std::vector<BatchItemHost> its;
+  std::vector<std::pair<double, std::pair<int, int>>> units;
+  size_t part = 0;
+  for (size_t k = 0; k < v.items.size(); ++k) {
+    BatchEntry& e = *b.items[v.items[k]];
+    const Problem& P = e.h->P;
+    BatchItemHost it{};
+    it.ntraj = ntraj_of(P);
+    it.steps = steps_cap > 0 ? std::min(P.p.steps, steps_cap) : P.p.steps;
+    it.npoints = points_cap > 0 ? std::min(P.p.points[0], points_cap) : P.p.points[0];
+    it.seq = 0;
+    it.seed = (unsigned)(P.p.seed & 0xffffffffu);
+    it.block0 = 0;
+    it.nunits = it.ntraj / v.G;
+    it.wscale = std::sqrt(P.nscale * P.noisefactor);  // xnoise.m:32
+    it.vscale = std::sqrt(P.noisefactor);              // xrandom.m:23
+    it.dtr = item_dtr(P);
+    it.t0 = P.p.origins[0];
+    it.prop = (const char*)b.d_prop.p + e.prop_off * 16;
+    const size_t stride = av_stride(P);
+    if (part_base) {
+      it.part = (char*)part_base + part * 16;
+      part += (size_t)it.npoints * it.nunits * stride;
+    } else {
+      it.part = (char*)b.d_part.p + e.part_off * 16;
+    }
+    it.av = (char*)b.d_av.p + e.av_off * 16;
+    it.params = P.runtime_defaults.empty() ? (const double*)b.d_params.p
+                                           : (const double*)((const char*)b.d_params.p + e.param_off * 8);
+    it.done = (int*)b.d_done.p + v.items[k];
+    its.push_back(it);
+    const double cost = (double)it.steps * it.npoints;
+    for (int u = 0; u < it.nunits; ++u) units.push_back({cost, {(int)k, u}});
+  }
+  std::stable_sort(units.begin(), units.end(), [](const auto& a, const auto& c) { return a.first > c.first; });
+  std::vector<int> flat;
+  for (auto& u : units) {
+    flat.push_back(u.second.first);
+    flat.push_back(u.second.second);
+  }
+  d_items.ensure(its.size() * sizeof(BatchItemHost));
+  CUDA_CHECK(cudaMemcpy(d_items.p, its.data(), its.size() * sizeof(BatchItemHost), cudaMemcpyHostToDevice));
+  d_units.ensure(std::max<size_t>(flat.size(), 2) * sizeof(int));
+  CUDA_CHECK(cudaMemcpy(d_units.p, flat.data(), flat.size() * sizeof(int), cudaMemcpyHostToDevice));
+  v.nunits = (int)units.size();
+}
+
+void variant_launch(xs_batch& b, BatchVariant& v, const DevBuf& d_items, const DevBuf& d_units, cudaStream_t st) {
+  xs_handle& h = *v.h;
+  BatchArgsHost a{};
+  a.items = d_items.p;
+  a.units = d_units.p;
+  a.nunits = v.nunits;
+  a.next = (int*)v.d_next.p;
+  a.status = (int*)b.d_status.p;
+  a.tmat = h.d_tmat.p;
+  for (int i = 0; i < 4; ++i) a.tmat_off[i] = h.tmat_off[i];
+  void* params[] = {&a};
+  cu_check(driver().launch(h.f_batch, (unsigned)v.grid, 1, 1, (unsigned)h.rp.threads, 1, 1, (unsigned)h.rp.smem,
+                           (CUstream)st, params, nullptr),
+           "launch xs_batch");
+}
+
+int variant_grid(const BatchVariant& v) {
+  int dev = 0, sms = 0, occ = 0;
+  CUDA_CHECK(cudaGetDevice(&dev));
+  CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  cu_check(driver().occupancy(&occ, v.h->f_batch, v.h->rp.threads, v.h->rp.smem), "occupancy");
+  if (occ < 1) raise(XS_ERR_UNSUPPORTED, "batch tile cannot be resident on an SM");
+  return std::max(1, std::min(v.nunits, sms * occ));
+}
+
+// Device buffers shared by all items: propagators, runtime scalars, means,
+// partial sums, unit counters.
+void batch_buffers(xs_batch& b) {
+  size_t prop = 0, par = 0, av = 0, part = 0;
+  for (auto& ep : b.items) {
+    BatchEntry& e = *ep;
+    const Problem& P = e.h->P;
+    const size_t stride = av_stride(P);
+    e.av_off = av;
+    av += (size_t)P.p.points[0] * stride;
+    if (e.variant < 0) continue;
+    const BatchVariant& v = *b.variants[e.variant];
+    e.nunits = ntraj_of(P) / std::max(v.G, 1);
+    e.prop_off = prop;
+    prop += P.has_linear ? P.L.size() : 1;
+    e.param_off = par;
+    par += P.runtime_defaults.size();
+    e.part_off = part;
+    part += (size_t)P.p.points[0] * e.nunits * stride;
+  }
+  b.av_total = av;
+  b.d_av.ensure(std::max<size_t>(av, 1) * 16);
+  b.d_part.ensure(std::max<size_t>(part, 1) * 16);
+  b.d_prop.ensure(std::max<size_t>(prop, 1) * 16);
+  b.d_params.ensure(std::max<size_t>(par, 1) * 8);
+  b.d_done.ensure(std::max<size_t>(b.items.size(), 1) * sizeof(int));
+  b.d_status.ensure(sizeof(int));
+  std::vector<cd> hp(std::max<size_t>(prop, 1));
+  std::vector<double> hpar(std::max<size_t>(par, 1));
+  for (auto& ep : b.items) {
+    BatchEntry& e = *ep;
+    if (e.variant < 0) continue;
+    const Problem& P = e.h->P;
+    if (P.has_linear) {
+      auto pr = prop_table(P, item_dtr(P));
+      std::copy(pr.begin(), pr.end(), hp.begin() + e.prop_off);
+    }
+    std::copy(P.runtime_defaults.begin(), P.runtime_defaults.end(), hpar.begin() + e.param_off);
+  }
+  CUDA_CHECK(cudaMemcpy(b.d_prop.p, hp.data(), hp.size() * 16, cudaMemcpyHostToDevice));
+  CUDA_CHECK(cudaMemcpy(b.d_params.p, hpar.data(), hpar.size() * 8, cudaMemcpyHostToDevice));
+  CUDA_CHECK(cudaMemset(b.d_done.p, 0, b.items.size() * sizeof(int)));
+  CUDA_CHECK(cudaMemset(b.d_status.p, 0, sizeof(int)));
+}
+
+void compile_all(std::vector<xs_handle*>& hs) {
+  std::vector<std::string> errs(hs.size());
+  std::vector<std::thread> th;
+  const unsigned ncpu = std::max(1u, std::thread::hardware_concurrency());
+  std::atomic<size_t> next{0};
+  for (unsigned t = 0; t < std::min<unsigned>(ncpu, (unsigned)hs.size()); ++t)
+    th.emplace_back([&]() {
+      for (size_t i = next++; i < hs.size(); i = next++) {
+        try {
+          nvrtc_compile(hs[i]->source, "xs_resident", nullptr);
+        } catch (const XsError& e) {
+          errs[i] = e.msg;
+        } catch (const std::exception& e) {
+          errs[i] = e.what();
+        }
+      }
+    });
+  for (auto& t : th) t.join();
+  for (auto& e : errs)
+    if (!e.empty()) raise(XS_ERR_NVRTC, e);
+}
+
+// Choose each resident variant's tile.  mode 0: the largest tile that still
+// gives every SM work; mode 1: time every candidate on a short probe (the
+// variant's own items with steps and output points capped) and keep the
+// fastest per trajectory-step; the choice is cached per source and device.
+void batch_tune(xs_batch& b, int mode) {
+  ensure_device();
+  batch_drop_graph(b);
+  int dev = 0, sms = 0;
+  CUDA_CHECK(cudaGetDevice(&dev));
+  CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  if (!b.stream) CUDA_CHECK(cudaStreamCreateWithFlags(&b.stream, cudaStreamNonBlocking));
+  for (auto& vp : b.variants) {
+    BatchVariant& v = *vp;
+    const BatchEntry& proto = *b.items[v.items[0]];
+    auto cands = tile_candidates(v, *proto.h);
+    const std::string tkey = tile_key(v.key);
+    int G = 0, T = 0;
+    bool cached = mode == 1 && tile_lookup(tkey, G, T);
+    if (cached) {
+      bool ok = false;
+      for (auto& c : cands) ok = ok || (c.first == G && c.second == T);
+      cached = ok;
+    }
+    if (!cached && mode == 0) {
+      // largest G whose unit count still covers the SMs, 256 threads
+      long long total = 0;
+      for (int i : v.items) total += ntraj_of(b.items[i]->h->P);
+      G = cands.front().first;
+      for (auto& c : cands)
+        if (total / c.first >= sms) G = std::max(G, c.first);
+      T = 0;
+      for (auto& c : cands)
+        if (c.first == G && (T == 0 || std::abs(c.second - 256) < std::abs(T - 256))) T = c.second;
+    }
+    if (!cached && mode == 1) {
+      std::vector<std::unique_ptr<xs_handle>> hs;
+      std::vector<xs_handle*> raw;
+      for (auto& c : cands) {
+        hs.push_back(variant_handle(proto.h->P.p, proto.h->P, proto.h->fp64, c.first, c.second));
+        raw.push_back(hs.back().get());
+      }
+      compile_all(raw);
+      double best = 1e300;
+      for (size_t ci = 0; ci < cands.size(); ++ci) {
+        v.G = cands[ci].first;
+        v.h = std::move(hs[ci]);
+        load_module(*v.h);
+        batch_buffers(b);
+        DevBuf d_items, d_units, d_part;
+        size_t part = 0;
+        double ts = 0;
+        for (int i : v.items) {
+          const Problem& P = b.items[i]->h->P;
+          part += (size_t)std::min(P.p.points[0], 1) * (ntraj_of(P) / v.G) * av_stride(P);
+          ts += (double)ntraj_of(P) * std::min(P.p.steps, 8);
+        }
+        d_part.ensure(std::max<size_t>(part, 1) * 16);
+        variant_tables(b, v, 8, 1, d_items, d_units, d_part.p);
+        v.d_next.ensure(sizeof(int));
+        v.grid = variant_grid(v);
+        cudaEvent_t e0, e1;
+        CUDA_CHECK(cudaEventCreate(&e0));
+        CUDA_CHECK(cudaEventCreate(&e1));
+        float ms = 1e30f;
+        for (int rep = 0; rep < 2; ++rep) {
+          CUDA_CHECK(cudaMemsetAsync(v.d_next.p, 0, sizeof(int), b.stream));
+          CUDA_CHECK(cudaMemsetAsync(b.d_done.p, 0, b.items.size() * sizeof(int), b.stream));
+          CUDA_CHECK(cudaEventRecord(e0, b.stream));
+          variant_launch(b, v, d_items, d_units, b.stream);
+          CUDA_CHECK(cudaEventRecord(e1, b.stream));
+          CUDA_CHECK(cudaEventSynchronize(e1));
+          float m = 0;
+          CUDA_CHECK(cudaEventElapsedTime(&m, e0, e1));
+          ms = std::min(ms, m);
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        int st = 0;
+        CUDA_CHECK(cudaMemcpy(&st, b.d_status.p, sizeof(int), cudaMemcpyDeviceToHost));
+        if (st & 2) raise(XS_ERR_SHAPE, "batch probe refused its launch layout");
+        const double us = 1e3 * ms / ts;
+        if (us < best) {
+          best = us;
+          G = cands[ci].first;
+          T = cands[ci].second;
+        }
+        hs[ci] = std::move(v.h);
+      }
+      v.probe_us = best;
+      tile_store(tkey, G, T);
+    }
+    v.G = G;
+    v.threads = T;
+    v.h = variant_handle(proto.h->P.p, proto.h->P, proto.h->fp64, G, T);
+    v.tuned = true;
+  }
+}
+
+void batch_prepare(xs_batch& b) {
+  if (b.prepared) return;
+  for (auto& vp : b.variants)
+    if (!vp->tuned) {
+      batch_tune(b, 0);
+      break;
+    }
+  ensure_device();
+  if (!b.stream) CUDA_CHECK(cudaStreamCreateWithFlags(&b.stream, cudaStreamNonBlocking));
+  std::vector<xs_handle*> raw;
+  for (auto& vp : b.variants) raw.push_back(vp->h.get());
+  for (auto& ep : b.items)
+    if (ep->variant < 0) raw.push_back(ep->h.get());
+  {
+    std::vector<xs_handle*> res, str;
+    for (auto* h : raw) (h->kind == 2 ? str : res).push_back(h);
+    compile_all(res);
+    std::vector<std::string> errs(str.size());
+    std::vector<std::thread> th;
+    for (size_t i = 0; i < str.size(); ++i)
+      th.emplace_back([&, i]() {
+        try {
+          nvrtc_compile(str[i]->source, "xs_stream", nullptr);
+        } catch (const XsError& e) {
+          errs[i] = e.msg;
+        }
+      });
+    for (auto& t : th) t.join();
+    for (auto& e : errs)
+      if (!e.empty()) raise(XS_ERR_NVRTC, e);
+  }
+  for (auto* h : raw) load_module(*h);
+  batch_buffers(b);
+  for (auto& vp : b.variants) {
+    BatchVariant& v = *vp;
+    variant_tables(b, v, 0, 0, v.d_items, v.d_units, nullptr);
+    v.d_next.ensure(sizeof(int));
+    v.grid = variant_grid(v);
+    if (!v.stream) CUDA_CHECK(cudaStreamCreateWithFlags(&v.stream, cudaStreamNonBlocking));
+    if (!v.join) CUDA_CHECK(cudaEventCreateWithFlags(&v.join, cudaEventDisableTiming));
+  }
+  // streaming items: buffers and propagators before capture (no uploads inside it)
+  std::vector<int> sitems;
+  for (size_t i = 0; i < b.items.size(); ++i)
+    if (b.items[i]->variant < 0) {
+      xs_handle& h = *b.items[i]->h;
+      const Problem& P = h.P;
+      h.d_field.ensure((size_t)P.E1 * P.F * P.NS * (h.fp64 ? 16 : 8));
+      if (P.nred) h.d_redpart.ensure((size_t)P.E1 * (P.N[1] / h.sp.OROWS) * P.nred * 16);
+      ensure_prop(h, 1);
+      ensure_prop2(h, 1);
+      sitems.push_back((int)i);
+    }
+  std::sort(sitems.begin(), sitems.end(), [&](int x, int y) { return b.items[x]->work > b.items[y]->work; });
+  const int nside = (int)std::min<size_t>(sitems.size(), 4);
+  while ((int)b.side.size() < nside) {
+    cudaStream_t s;
+    cudaEvent_t e;
+    CUDA_CHECK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    CUDA_CHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    b.side.push_back(s);
+    b.side_join.push_back(e);
+  }
+  if (!b.fork) CUDA_CHECK(cudaEventCreateWithFlags(&b.fork, cudaEventDisableTiming));
+  CUDA_CHECK(cudaDeviceSynchronize());
+  // capture: counters reset, then every variant and streaming chain forked from one event
+  std::vector<size_t> order(b.variants.size());
+  std::iota(order.begin(), order.end(), 0);
+  for (auto& vp : b.variants) {
+    vp->work = 0;
+    for (int i : vp->items) vp->work += b.items[i]->work;
+  }
+  std::sort(order.begin(), order.end(), [&](size_t x, size_t y) { return b.variants[x]->work > b.variants[y]->work; });
+  int launches = 0;
+  CUDA_CHECK(cudaStreamBeginCapture(b.stream, cudaStreamCaptureModeRelaxed));
+  try {
+    CUDA_CHECK(cudaMemsetAsync(b.d_done.p, 0, b.items.size() * sizeof(int), b.stream));
+    CUDA_CHECK(cudaMemsetAsync(b.d_status.p, 0, sizeof(int), b.stream));
+    for (auto& vp : b.variants) CUDA_CHECK(cudaMemsetAsync(vp->d_next.p, 0, sizeof(int), b.stream));
+    for (int i : sitems) CUDA_CHECK(cudaMemsetAsync(b.items[i]->h->d_status.p, 0, sizeof(int), b.stream));
+    CUDA_CHECK(cudaEventRecord(b.fork, b.stream));
+    for (size_t k : order) {
+      BatchVariant& v = *b.variants[k];
+      CUDA_CHECK(cudaStreamWaitEvent(v.stream, b.fork, 0));
+      variant_launch(b, v, v.d_items, v.d_units, v.stream);
+      ++launches;
+      CUDA_CHECK(cudaEventRecord(v.join, v.stream));
+    }
+    for (int s = 0; s < nside; ++s) CUDA_CHECK(cudaStreamWaitEvent(b.side[s], b.fork, 0));
+    for (size_t q = 0; q < sitems.size(); ++q) {
+      BatchEntry& e = *b.items[sitems[q]];
+      xs_handle& h = *e.h;
+      const long long before = std::accumulate(std::begin(h.launches), std::end(h.launches), 0LL);
+      launch_stream(h, 0, 1, 1, nullptr, (char*)b.d_av.p + e.av_off * 16, nullptr, b.side[q % nside]);
+      launches += (int)(std::accumulate(std::begin(h.launches), std::end(h.launches), 0LL) - before);
+    }
+    for (int s = 0; s < nside; ++s) {
+      CUDA_CHECK(cudaEventRecord(b.side_join[s], b.side[s]));
+      CUDA_CHECK(cudaStreamWaitEvent(b.stream, b.side_join[s], 0));
+    }
+    for (auto& vp : b.variants) CUDA_CHECK(cudaStreamWaitEvent(b.stream, vp->join, 0));
+  } catch (...) {
+    cudaGraph_t g = nullptr;
+    cudaStreamEndCapture(b.stream, &g);
+    if (g) cudaGraphDestroy(g);
+    throw;
+  }
+  CUDA_CHECK(cudaStreamEndCapture(b.stream, &b.graph));
+  CUDA_CHECK(cudaGraphInstantiate(&b.exec, b.graph, 0));
+  b.launches_per_run = launches;
+  b.prepared = true;
+}
+
+}  // namespace
+
+XS_API xs_status xs_batch_create(const xs_problem* items, int nitems, xs_batch** out) {
+  if (!out) return XS_ERR_ARG;
+  *out = nullptr;
+  return guard([&]() -> xs_status {
+    if (!items || nitems < 1) raise(XS_ERR_ARG, "empty batch");
+    auto b = std::make_unique<xs_batch>();
+    std::map<std::string, int> vmap;
+    for (int i = 0; i < nitems; ++i) {
+      auto e = std::make_unique<BatchEntry>();
+      e->h = std::make_unique<xs_handle>();
+      xs_handle& h = *e->h;
+      try {
+        setup_problem(&items[i], h.P);
+        h.fp64 = items[i].precision != XS_PREC_FP32;
+        if (items[i].path_kind < 0 || items[i].path_kind > 2) raise(XS_ERR_ARG, "path_kind must be 0, 1 or 2");
+        h.path_kind = items[i].path_kind;
+        if (items[i].checks) raise(XS_ERR_UNSUPPORTED, "batch items run the fine pass only (checks = 0)");
+        if (items[i].ensembles[1] != 1 || items[i].ensembles[2] != 1)
+          raise(XS_ERR_UNSUPPORTED, "a batch item is one ensemble block (ensembles(2) = ensembles(3) = 1)");
+        h.force_G = 1;
+        build_source(h);
+      } catch (XsError& err) {
+        err.msg = "batch item " + std::to_string(i) + ": " + err.msg;
+        throw;
+      }
+      const Problem& P = h.P;
+      e->work = (double)ntraj_of(P) * P.p.steps * std::max(1, P.p.points[0] - 1) * P.NS;
+      if (h.kind == 1) {
+        auto it = vmap.find(h.source);
+        if (it == vmap.end()) {
+          auto v = std::make_unique<BatchVariant>();
+          v->key = h.source;
+          it = vmap.emplace(h.source, (int)b->variants.size()).first;
+          b->variants.push_back(std::move(v));
+        }
+        BatchVariant& v = *b->variants[it->second];
+        e->variant = it->second;
+        v.items.push_back(i);
+        v.gcd_traj = std::gcd(v.gcd_traj, ntraj_of(P));
+      } else {
+        h.force_G = 0;
+      }
+      b->items.push_back(std::move(e));
+    }
+    *out = b.release();
+    return XS_OK;
+  });
+}
+
+XS_API void xs_batch_destroy(xs_batch* b) { delete b; }
+
+XS_API xs_status xs_batch_tune(xs_batch* b, int mode) {
+  return guard([&]() -> xs_status {
+    if (!b || mode < 0 || mode > 1) raise(XS_ERR_ARG, "bad arguments to xs_batch_tune");
+    batch_tune(*b, mode);
+    return XS_OK;
+  });
+}
+
+XS_API xs_status xs_batch_run(xs_batch* b, void* stream) {
+  return guard([&]() -> xs_status {
+    if (!b) raise(XS_ERR_ARG, "null batch");
+    batch_prepare(*b);
+    CUDA_CHECK(cudaGraphLaunch(b->exec, stream ? (cudaStream_t)stream : b->stream));
+    return XS_OK;
+  });
+}
+
+XS_API xs_status xs_batch_sync(xs_batch* b) {
+  return guard([&]() -> xs_status {
+    if (!b) raise(XS_ERR_ARG, "null batch");
+    CUDA_CHECK(cudaDeviceSynchronize());
+    int st = 0;
+    if (b->d_status.p) CUDA_CHECK(cudaMemcpy(&st, b->d_status.p, sizeof(int), cudaMemcpyDeviceToHost));
+    for (auto& ep : b->items)
+      if (ep->variant < 0 && ep->h->d_status.p) {
+        int s2 = 0;
+        CUDA_CHECK(cudaMemcpy(&s2, ep->h->d_status.p, sizeof(int), cudaMemcpyDeviceToHost));
+        st |= s2;
+      }
+    if (st & 2) raise(XS_ERR_SHAPE, "kernel refused a launch whose shared-memory layout or grid did not match");
+    if (st & 1) raise(XS_ERR_NAN, "a trajectory became non-finite (NaN/Inf)");
+    return XS_OK;
+  });
+}
+
+XS_API size_t xs_batch_av_doubles(const xs_batch* b, int item) {
+  if (!b || item < 0 || item >= (int)b->items.size()) return 0;
+  return av_doubles_per_block(b->items[item]->h->P);
+}
+
+XS_API xs_status xs_batch_results(xs_batch* b, int item, double* av_out) {
+  return guard([&]() -> xs_status {
+    if (!b || item < 0 || item >= (int)b->items.size() || !av_out) raise(XS_ERR_ARG, "bad arguments to xs_batch_results");
+    if (!b->prepared) raise(XS_ERR_ARG, "xs_batch_run has not been called");
+    const BatchEntry& e = *b->items[item];
+    const Problem& P = e.h->P;
+    const size_t n = (size_t)P.p.points[0] * av_stride(P) * 2;
+    std::vector<double> dev(std::max<size_t>(n, 1));
+    CUDA_CHECK(cudaStreamSynchronize(b->stream));
+    if (n) CUDA_CHECK(cudaMemcpy(dev.data(), (const char*)b->d_av.p + e.av_off * 16, n * 8, cudaMemcpyDeviceToHost));
+    scatter_av(P, dev, 1, av_out);
+    return XS_OK;
+  });
+}
+
+XS_API xs_status xs_batch_info(const xs_batch* b, int item, int* info, int ninfo) {
+  return guard([&]() -> xs_status {
+    if (!b || !info || ninfo < 1) raise(XS_ERR_ARG, "bad arguments to xs_batch_info");
+    if (item < 0) {  // batch summary: items, variants, streaming items, launches per run
+      int nst = 0;
+      for (auto& ep : b->items) nst += ep->variant < 0;
+      const int v[4] = {(int)b->items.size(), (int)b->variants.size(), nst, b->launches_per_run};
+      for (int k = 0; k < ninfo && k < 4; ++k) info[k] = v[k];
+      return XS_OK;
+    }
+    if (item >= (int)b->items.size()) raise(XS_ERR_ARG, "item index out of range");
+    const BatchEntry& e = *b->items[item];
+    int v[6] = {e.variant, e.variant < 0 ? 2 : 1, 0, 0, 0, 0};
+    if (e.variant >= 0) {
+      const BatchVariant& bv = *b->variants[e.variant];
+      v[2] = bv.G;
+      v[3] = bv.threads;
+      v[4] = bv.grid;
+      v[5] = e.nunits;
+    }
+    for (int k = 0; k < ninfo && k < 6; ++k) info[k] = v[k];
     return XS_OK;
   });
 }

@@ -162,51 +162,61 @@ def xpreferences(inputs):
     return out
 
 
+def make_problem(p, path_kind=0, runtime_params=False):
+    """The C-ABI problem struct (xs_problem) of one preference-filled input;
+    returns it with the ctypes arrays it points into (keep them alive).
+    With runtime_params the named scalars p.<name> are read by the kernels
+    at run time instead of being compiled in."""
+    pr = _lib.XsProblem()
+    pr.dimensions = p.dimensions
+    pr.fields = p.fields
+    pr.noises = p.noises
+    pr.inrandoms = p.inrandoms
+    for d in range(len(p.points)):
+        pr.points[d] = p.points[d]
+        pr.ranges[d] = p.ranges[d]
+        pr.origins[d] = p.origins[d]
+    pr.steps = p.steps[0]
+    pr.checks = p.checks[0]
+    for i in range(3):
+        pr.ensembles[i] = p.ensembles[i]
+    pr.method = _lib.METHODS[p.method]
+    pr.iterations = p.iterations
+    pr.ipsteps = p.ipsteps
+    pr.precision = 1 if p.precision in ("fp32", "single", "float32") else 0
+    pr.seed = p.seed & 0xFFFFFFFFFFFFFFFF
+    keep = []
+    if p.boundaries is not None:
+        flat = np.concatenate([np.asarray(b, np.int32).reshape(-1) for b in p.boundaries]).astype(np.int32)
+        arr = (ctypes.c_int * flat.size)(*flat.tolist())
+        keep.append(arr)
+        pr.boundaries = arr
+    pr.deriv = (p.get("deriv") or "@(a,w,p) 0*a").encode()
+    pr.initial = (p.get("initial") or "@(v,p) 0").encode()
+    pr.linear = (p.get("linear") or "").encode()
+    obs = (ctypes.c_char_p * len(p.observe))(*[o.encode() for o in p.observe])
+    keep.append(obs)
+    pr.nobserve = len(p.observe)
+    pr.observe = obs
+    names = list(p.params.keys())
+    if names:
+        nm = (ctypes.c_char_p * len(names))(*[n.encode() for n in names])
+        vals = (ctypes.c_double * len(names))(*[float(p.params[n]) for n in names])
+        keep += [nm, vals]
+        pr.nparams = len(names)
+        pr.param_names = nm
+        pr.param_values = vals
+    pr.path_kind = path_kind
+    pr.runtime_params = 1 if runtime_params else 0
+    return pr, keep
+
+
 class GpuPath:
     """One compiled device problem: the p.path/p.method replacements of one input."""
 
-    def __init__(self, p, path_kind=0):
+    def __init__(self, p, path_kind=0, runtime_params=False):
         L = _lib.lib()
-        pr = _lib.XsProblem()
-        pr.dimensions = p.dimensions
-        pr.fields = p.fields
-        pr.noises = p.noises
-        pr.inrandoms = p.inrandoms
-        for d in range(len(p.points)):
-            pr.points[d] = p.points[d]
-            pr.ranges[d] = p.ranges[d]
-            pr.origins[d] = p.origins[d]
-        pr.steps = p.steps[0]
-        pr.checks = p.checks[0]
-        for i in range(3):
-            pr.ensembles[i] = p.ensembles[i]
-        pr.method = _lib.METHODS[p.method]
-        pr.iterations = p.iterations
-        pr.ipsteps = p.ipsteps
-        pr.precision = 1 if p.precision in ("fp32", "single", "float32") else 0
-        pr.seed = p.seed & 0xFFFFFFFFFFFFFFFF
-        keep = []
-        if p.boundaries is not None:
-            flat = np.concatenate([np.asarray(b, np.int32).reshape(-1) for b in p.boundaries]).astype(np.int32)
-            arr = (ctypes.c_int * flat.size)(*flat.tolist())
-            keep.append(arr)
-            pr.boundaries = arr
-        pr.deriv = (p.get("deriv") or "@(a,w,p) 0*a").encode()
-        pr.initial = (p.get("initial") or "@(v,p) 0").encode()
-        pr.linear = (p.get("linear") or "").encode()
-        obs = (ctypes.c_char_p * len(p.observe))(*[o.encode() for o in p.observe])
-        keep.append(obs)
-        pr.nobserve = len(p.observe)
-        pr.observe = obs
-        names = list(p.params.keys())
-        if names:
-            nm = (ctypes.c_char_p * len(names))(*[n.encode() for n in names])
-            vals = (ctypes.c_double * len(names))(*[float(p.params[n]) for n in names])
-            keep += [nm, vals]
-            pr.nparams = len(names)
-            pr.param_names = nm
-            pr.param_values = vals
-        pr.path_kind = path_kind
+        pr, keep = make_problem(p, path_kind, runtime_params)
         h = ctypes.c_void_p()
         _lib.check(L.xs_create(ctypes.byref(pr), ctypes.byref(h)))
         self._keep = keep
