@@ -294,6 +294,68 @@ __device__ void xs_method(cx* A, cx* B1, cx* B2, cx* B3, cx* T, const real* W, c
   __syncthreads();
 }
 
+#if XS_LEAN
+// MP step with the midpoint iterations fused per site (Applications/SDE/MP.m:
+// 13-23): the iterations are pointwise, so a0, the iterate and the noise live
+// in registers and only the field and the transform scratch stay in shared
+// memory.  mode 0: fine draw `draw`; 2: coarse pass, mean of draws `prev` and
+// `draw` (Simulator/xnoise.m:33-35); 3: the caller's noise P.w_in (p.method).
+// The arithmetic is that of the unfused step, operation for operation.
+__device__ void xs_mp_lean(cx* A, cx* T, const XsPathArgs& P, double t, int g0, int mode, int draw, int prev) {
+  const double dtr = P.dtr;
+  const real h = (real)(dtr * 0.5);
+  const real tm = (real)(t + dtr * 0.5);
+  xs_prop(A, T, P);
+  for (int i = threadIdx.x; i < XS_G * XS_NS; i += blockDim.x) {
+    const int g = i / XS_NS, s = i % XS_NS;
+    const int e = g0 + g;
+    int i1, i2, i3;
+    real x, y, z;
+    xs_site(s, i1, i2, i3, x, y, z);
+    real w[XS_NWS];
+#if XS_NW > 0
+    if (mode == 3) {
+#pragma unroll
+      for (int c = 0; c < XS_NW; ++c)
+        w[c] = P.w_in ? (real)P.w_in[c + (size_t)XS_NW * (s + (size_t)XS_NS * e)] : (real)0;
+    } else {
+      const u32 blk = (u32)(P.block0 + e / P.ens1);
+      const u32 el = (u32)(e % P.ens1);
+      real zz[XS_NW];
+      xs_normals_site<XS_NW>(zz, (u32)s, el, (u32)draw, (u32)P.seq, P.seed, blk);
+#pragma unroll
+      for (int c = 0; c < XS_NW; ++c) w[c] = zz[c] * (real)P.wscale;
+      if (mode == 2) {
+        xs_normals_site<XS_NW>(zz, (u32)s, el, (u32)prev, (u32)P.seq, P.seed, blk);
+#pragma unroll
+        for (int c = 0; c < XS_NW; ++c) w[c] = (w[c] + zz[c] * (real)P.wscale) * (real)0.5;
+      }
+    }
+#else
+    w[0] = (real)0;
+#endif
+    cx a0[XS_F], a[XS_F], d[XS_F];
+#pragma unroll
+    for (int f = 0; f < XS_F; ++f) a0[f] = a[f] = A[(g * XS_F + f) * XS_NS + s];
+    for (int it = 0; it < XS_ITER; ++it) {
+      xs_deriv(a, w, x, y, z, tm, P.params, d);
+#pragma unroll
+      for (int f = 0; f < XS_F; ++f) {
+        a[f] = a0[f] + h * d[f];
+#if XS_SETBOUND
+        if (xs_dirichlet(f, i1, i2, i3)) a[f] = mkcx((real)0, (real)0);
+#endif
+      }
+    }
+#pragma unroll
+    for (int f = 0; f < XS_F; ++f) A[(g * XS_F + f) * XS_NS + s] = (real)2 * a[f] - a0[f];
+  }
+  __syncthreads();
+  xs_prop(A, T, P);
+  __syncthreads();
+}
+#endif
+
 // Noise of one p.noisegen call into W (coarse pass: averaged with Wp, xnoise.m:33-35).
 __device__ __forceinline__ void xs_noise(real* W, real* Wp, int mode, int draw, int g0, const XsPathArgs& P) {
 #if XS_NW > 0
@@ -399,7 +461,7 @@ __device__ __forceinline__ bool xs_layout_ok(int* status) {
   constexpr size_t GF = (size_t)XS_G * XS_F * XS_NS;
   constexpr size_t need = XS_NARR * GF * sizeof(cx) + (size_t)XS_G * (XS_NRED > 0 ? XS_NRED : 1) * sizeof(cx) +
                           32 * 2 * (XS_NRED > 0 ? XS_NRED : 1) * sizeof(double) +
-                          2 * (size_t)XS_G * XS_NWS * XS_NS * sizeof(real);
+                          XS_WARR * (size_t)XS_G * XS_NWS * XS_NS * sizeof(real);
   u32 dyn;
   asm volatile("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn));
   if (need > (size_t)dyn || need != (size_t)XS_SMEM_BYTES || (int)blockDim.x != XS_THREADS) {
@@ -458,6 +520,7 @@ __device__ void xs_resident_run(const XsPathArgs& P, int cta, int nctas) {
 
   if (P.single_step) {
     // p.method(a, w, p) on the given noise (Simulator/xpath.m:150)
+#if !XS_LEAN
     for (int i = threadIdx.x; i < XS_G * XS_NS; i += blockDim.x) {
       const int g = i / XS_NS, s = i % XS_NS;
       const size_t e = (size_t)(g0 + g);
@@ -465,8 +528,13 @@ __device__ void xs_resident_run(const XsPathArgs& P, int cta, int nctas) {
       for (int c = 0; c < XS_NW; ++c)
         W[(g * XS_NWS + c) * XS_NS + s] = P.w_in ? (real)P.w_in[c + (size_t)XS_NW * (s + (size_t)XS_NS * e)] : (real)0;
     }
+#endif
     __syncthreads();
+#if XS_LEAN
+    xs_mp_lean(A, T, P, P.t0, g0, 3, 0, 0);
+#else
     xs_method(A, B1, B2, B3, T, W, P, P.t0);
+#endif
   } else {
   double t = P.t0;
   int draw = 0;
@@ -477,12 +545,20 @@ __device__ void xs_resident_run(const XsPathArgs& P, int cta, int nctas) {
           ++draw;
           int mode = 0;
           if (P.nc == 2 && P.checks) mode = chk == 0 ? 1 : 2;
+#if XS_LEAN
+          if (P.nc == 1 || chk == 1) {
+            __syncthreads();
+            xs_mp_lean(A, T, P, t, g0, mode, draw, draw - 1);
+            t += P.dtr;
+          }
+#else
           xs_noise(W, Wp, mode, draw, g0, P);
           if (P.nc == 1 || chk == 1) {
             __syncthreads();
             xs_method(A, B1, B2, B3, T, W, P, t);
             t += P.dtr;
           }
+#endif
         }
       }
       if (step == 0) {

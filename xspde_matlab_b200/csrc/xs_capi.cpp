@@ -687,12 +687,14 @@ size_t resident_smem(const xs_handle& h, int G, int narr) {
   size_t cxs = h.fp64 ? 16 : 8, rs = h.fp64 ? 8 : 4;
   size_t nred = std::max(P.nred, 1);
   size_t nws = std::max(P.NW, 1);
-  return (size_t)narr * G * P.F * P.NS * cxs + (size_t)G * nred * cxs + 32 * 2 * nred * 8 + 2 * (size_t)G * nws * P.NS * rs;
+  const size_t warr = P.p.method == XS_METHOD_MP ? 0 : 2;  // MP keeps its noise in registers
+  return (size_t)narr * G * P.F * P.NS * cxs + (size_t)G * nred * cxs + 32 * 2 * nred * 8 +
+         warr * (size_t)G * nws * P.NS * rs;
 }
 
 int method_arrays(int m) {
   switch (m) {
-    case XS_METHOD_MP: return 3;
+    case XS_METHOD_MP: return 2;  // field + transform scratch (fused midpoint iterations)
     case XS_METHOD_RK4: return 5;
     case XS_METHOD_EULER: return 2;
     case XS_METHOD_RK2: return 3;
@@ -900,6 +902,8 @@ void build_source(xs_handle& h) {
   std::ostringstream os;
   emit_common_header(h, os);
   os << "#define XS_G " << h.rp.G << "\n#define XS_THREADS " << h.rp.threads << "\n#define XS_NARR " << h.rp.narr << "\n";
+  os << "#define XS_LEAN " << (P.p.method == XS_METHOD_MP ? 1 : 0) << "\n#define XS_WARR "
+     << (P.p.method == XS_METHOD_MP ? 0 : 2) << "\n";
   os << "#define XS_SMEM_BYTES " << h.rp.smem << "\n";
   {
     std::string stages;
