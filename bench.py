@@ -520,6 +520,91 @@ def run_batch(args):
     print(json.dumps(line))
 
 
+def _dpo_cpu_sample(seconds=10.0, ntraj=4096):
+    """Oracle (FP64 NumPy, one core) on the DPO: `ntraj` trajectories for as
+    many MP steps as fit in about `seconds`."""
+    import numpy as np
+    from oracle import xspde_ref as X
+    from xspde_matlab_b200.problems import DPO_0D
+    gam, eps, chi = 1.0, 1.25, 1e-3
+
+    def deriv(a, w, q):
+        a1, a2 = a[0:1], a[1:2]
+        return np.concatenate([
+            -gam * a1 + eps * a2 - chi * a1 ** 2 * a2 + 0.5 * chi * a1 + np.sqrt(-chi * a1 ** 2 + 0j) * w[0:1],
+            -gam * a2 + eps * a1 - chi * a2 ** 2 * a1 + 0.5 * chi * a2 + np.sqrt(-chi * a2 ** 2 + 0j) * w[1:2]])
+    o = {k: v for k, v in DPO_0D.items() if k not in ("deriv", "initial", "observe", "params")}
+    o.update(ensembles=[ntraj, 1, 1], deriv=deriv, initial=lambda v, q: np.array([[1.0 + 0j], [1.0 + 0j]]),
+             observe=[lambda a, q: np.real(a[0:1] * a[1:2])])
+    q = X.xpreferences([o])[0].copy()
+    q.block, q.seq = 0, 0
+    q.dtr = q.dt / q.steps[0]
+    q.propagator, q.da = q.propfactor(q)
+    q.t = q.origins[0]
+    a = X.fit(np.asarray(q.initial(0, q), dtype=complex), q.ca)
+    method = X.METHODS["MP"]
+    q.draw = 0
+    t0 = time.perf_counter()
+    steps = 0
+    while time.perf_counter() - t0 < seconds:
+        q.draw += 1
+        a = method(a, q.noisegen(None, 1, q.nscale, q), q)
+        q.t += q.dtr
+        steps += 1
+    el = time.perf_counter() - t0
+    return steps * ntraj / el, "%d DPO trajectories x %d MP steps (FP64 NumPy oracle, 1 core)" % (ntraj, steps)
+
+
+def run_dpo(args):
+    """Positive-P DPO (0-D, two complex fields): 8 blocks x 125000 trajectories,
+    each block its own pump eps ~ U[0.5, 2], 2000 MP steps, as one batch (one
+    graph launch); FP64 and FP32 fields, FP32 observables compared with FP64."""
+    import numpy as np
+    import torch
+    from xspde_matlab_b200 import batch as B
+    out = {}
+    res = {}
+    for prec in ("fp64", "fp32"):
+        inst = B.dpo_instances(precision=prec)
+        b = B.Batch(inst)
+        b.tune(1)
+        st = torch.cuda.Stream()
+        for _ in range(max(1, args.warmup)):
+            b.run(st)
+        st.synchronize()
+        b.sync()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with Clocks(torch.cuda.current_device()) as clk:
+            e0.record(st)
+            for _ in range(args.steps):
+                b.run(st)
+            e1.record(st)
+            e1.synchronize()
+        b.sync()
+        ms = e0.elapsed_time(e1) / args.steps
+        ts = sum(B.trajectory_steps(i) for i in inst)
+        res[prec] = [b.results(i) for i in range(len(inst))]
+        out[prec] = {"traj_steps_per_s": ts / (ms * 1e-3), "ms_per_run": ms, "tile": b.info(0),
+                     "clocks": clk.summary()}
+    d = 0.0
+    for r64, r32 in zip(res["fp64"], res["fp32"]):
+        for o64, o32 in zip(r64, r32):
+            d = max(d, float(np.max(np.abs(o32 - o64)) / max(np.max(np.abs(o64)), 1e-300)))
+    inst = B.dpo_instances()
+    n_final = [float(np.real(r[0][0, -1])) for r in res["fp64"]]
+    cpu, sample = _dpo_cpu_sample()
+    line = {"metric": "traj-steps/s, positive-P DPO 10^6 trajectories x 2000 steps (one graph launch)",
+            "value": out["fp64"]["traj_steps_per_s"], "unit": "traj-steps/s", "dtype": "f64", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "data": "synthetic",
+            "fp64": out["fp64"], "fp32": out["fp32"], "fp32_vs_fp64_observables_max_rel": d,
+            "eps": [i["params"]["eps"] for i in inst], "final_mean_photon_number": n_final,
+            "cpu_baseline": {"value": cpu, "unit": "traj-steps/s", "cores": 1, "kind": "port", "sample": sample},
+            "config": {"workload": "dpo_0d: gam=1, chi=1e-3, eps~U[0.5,2] per block (Philox seed 1), 8 blocks x "
+                                   "125000 trajectories, 2000 MP steps to t=10, observables <Re(alpha beta)>, "
+                                   "<Re alpha> at 11 times"}}
+    print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -532,12 +617,18 @@ def main():
                                                       "plain FP64 vs FP32 + learned control variate")
     ap.add_argument("--batch", action="store_true", help="uneven batch of independent problems, one graph launch")
     ap.add_argument("--batch-items", type=int, default=512)
+    ap.add_argument("--dpo", action="store_true", help="positive-P DPO, 10^6 trajectories x 2000 steps")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.dpo:
+        import torch
+        torch.cuda.set_device(local_rank)
+        run_dpo(args)
         return
     if args.batch:
         import torch

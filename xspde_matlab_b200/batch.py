@@ -62,6 +62,21 @@ def uneven_instances(n=512, seed=1, output_points=5):
     return out
 
 
+def dpo_instances(blocks=8, ntraj=125000, seed=1, precision="fp64"):
+    """Positive-P DPO sweep: `blocks` items of `ntraj` trajectories, each with
+    its own pump eps ~ U[0.5, 2] (numpy Philox generator of the given seed) and
+    Philox noise seed; 2000 MP steps to t = 10 (problems.DPO_0D)."""
+    from .problems import DPO_0D
+    rng = np.random.Generator(np.random.Philox(seed))
+    out = []
+    for b in range(blocks):
+        eps = float(rng.uniform(0.5, 2.0))
+        d = dict(DPO_0D, ensembles=[ntraj, 1, 1], seed=b + 1, precision=precision, name="dpo_0d",
+                 params=dict(DPO_0D["params"], eps=eps))
+        out.append(d)
+    return out
+
+
 def trajectory_steps(inp):
     """Trajectory-steps of one input: ntraj x steps x (points(1) - 1)."""
     return inp["ensembles"][0] * inp["steps"] * max(1, inp["points"][0] - 1)

@@ -1909,8 +1909,9 @@ void batch_drop_graph(xs_batch& b) {
 std::vector<std::pair<int, int>> tile_candidates(const BatchVariant& v, const xs_handle& proto) {
   const Problem& P = proto.P;
   const int narr = method_arrays(P.p.method);
-  std::vector<int> Gs;
-  for (int G = 1; G <= 1024 && v.gcd_traj % G == 0; G *= 2) {
+  std::vector<int> Gs;  // divisors of every item's trajectory count, ascending
+  for (int G = 1; G <= 4096 && G <= v.gcd_traj; ++G) {
+    if (v.gcd_traj % G) continue;
     if (resident_smem(proto, G, narr) > 200 * 1024) break;
     if ((size_t)G * P.NS > 16384 && G > 1) break;
     Gs.push_back(G);

@@ -7,12 +7,18 @@ gpe_2d: 2D stochastic Gross-Pitaevskii / complex Ginzburg-Landau on 256x256
   periodic over [-10,10]^2, da/dt = (i+0.1) lap a + (1-|a|^2) a - 0.5i |a|^2 a
   + 0.05 xi, a0 = 1 + 0.1 complex Gaussian, 4096 trajectories in 16 blocks,
   500 steps to t = 5 (51 output points).
+dpo_0d: positive-P degenerate parametric oscillator, two complex fields
+  (alpha, beta), d alpha = (-gam alpha + eps beta - chi alpha^2 beta) dt +
+  sqrt(-chi alpha^2) dW1 and the partner equation, gam = 1, chi = 1e-3, eps a
+  runtime scalar; MP integrates in the Stratonovich sense, so the drift carries
+  the correction -1/2 B dB/dalpha = +chi alpha / 2 (the Ito form is the one
+  Euler takes).  alpha = beta = 1 at t = 0; 2000 steps to t = 10.
 xi is complex white noise (w1 + i w2)/sqrt(2).
 """
 import ctypes
 
 from . import _lib
-from .xsim import GpuPath, xpreferences
+from .xsim import make_problem, xpreferences
 
 SNLS_1D = dict(
     dimensions=2, points=[51, 64], ranges=[1.0, 10.0], steps=4, ensembles=[128, 8, 1], noises=2, method="RK4",
@@ -28,36 +34,24 @@ GPE_2D = dict(
     initial="@(v,p) 1 + 0.1*(v(1,:)+1i*v(2,:))/sqrt(2)", linear="@(p) (1i+0.1)*(p.Dx.^2+p.Dy.^2)",
     observe=["@(a,p) abs(a).^2"])
 
-PROBLEMS = {"snls_1d": SNLS_1D, "gpe_2d": GPE_2D}
+DPO_0D = dict(
+    dimensions=1, fields=2, noises=2, inrandoms=0, points=[11], ranges=[10.0], steps=200, ensembles=[125000, 8, 1],
+    method="MP", checks=0, params={"gam": 1.0, "eps": 1.5, "chi": 1e-3},
+    deriv="@(a,w,p) [-p.gam*a(1,:)+p.eps*a(2,:)-p.chi*a(1,:).^2.*a(2,:)+0.5*p.chi*a(1,:)"
+          "+sqrt(-p.chi*a(1,:).^2).*w(1,:); -p.gam*a(2,:)+p.eps*a(1,:)-p.chi*a(2,:).^2.*a(1,:)"
+          "+0.5*p.chi*a(2,:)+sqrt(-p.chi*a(2,:).^2).*w(2,:)]",
+    initial="@(v,p) [1; 1]",
+    observe=["@(a,p) real(a(1,:).*a(2,:))", "@(a,p) real(a(1,:))"])
+
+PROBLEMS = {"snls_1d": SNLS_1D, "gpe_2d": GPE_2D, "dpo_0d": DPO_0D}
 
 
 def compile_check(name, **over):
     """NVRTC-compile the kernels of a named problem for sm_100a (no GPU needed)."""
     p = dict(PROBLEMS[name], **over)
     q = xpreferences([p])[0]
-    g = GpuPath.__new__(GpuPath)
-    pr, keep = _struct(q)
+    pr, keep = make_problem(q)
     log = ctypes.create_string_buffer(1 << 16)
     _lib.check(_lib.lib().xs_compile_check(ctypes.byref(pr), log, len(log)))
-    del g, keep
+    del keep
     return log.value.decode(errors="replace")
-
-
-def _struct(q):
-    pr = _lib.XsProblem()
-    keep = []
-    pr.dimensions, pr.fields, pr.noises, pr.inrandoms = q.dimensions, q.fields, q.noises, q.inrandoms
-    for d in range(len(q.points)):
-        pr.points[d], pr.ranges[d], pr.origins[d] = q.points[d], q.ranges[d], q.origins[d]
-    pr.steps, pr.checks = q.steps[0], q.checks[0]
-    for i in range(3):
-        pr.ensembles[i] = q.ensembles[i]
-    pr.method, pr.iterations, pr.ipsteps = _lib.METHODS[q.method], q.iterations, q.ipsteps
-    pr.precision = 1 if q.precision == "fp32" else 0
-    pr.seed = q.seed
-    pr.deriv, pr.initial = q.deriv.encode(), q.initial.encode()
-    pr.linear = (q.get("linear") or "").encode()
-    obs = (ctypes.c_char_p * len(q.observe))(*[o.encode() for o in q.observe])
-    keep.append(obs)
-    pr.nobserve, pr.observe = len(q.observe), obs
-    return pr, keep
