@@ -164,6 +164,47 @@ def _cpu_sample(seconds=12.0, ntraj=2):
         ntraj, steps)
 
 
+def _precision_report(ntraj_fp64):
+    """The problem as plain FP64 and as FP32 bulk (FP64 tables and moments):
+    FP64 throughput on the full workload (device timing, one step after one
+    warm-up), and the FP32 observable's error against FP64 on one block of 256
+    trajectories over all 51 output times (the FP64 device path agrees with the
+    FP64 oracle to 1e-10 in the parity tests, so it stands in for it here)."""
+    import numpy as np
+    import torch
+    from xspde_matlab_b200 import GpuPath, _lib, xpreferences
+    L = _lib.lib()
+    p64 = xpreferences([dict(_problem(ntraj_fp64), precision="fp64")])[0]
+    g64 = GpuPath(p64)
+    nb = p64.ensembles[1]
+    av = torch.zeros((nb, p64.points[0], p64.nspace, 2), dtype=torch.float64, device="cuda")
+    st = torch.cuda.current_stream()
+
+    def run():
+        _lib.check(L.xs_run_path_device(g64.h, 0, nb, 1, None, ctypes.c_void_p(av.data_ptr()), None,
+                                        ctypes.c_void_p(st.cuda_stream)))
+    run()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    run()
+    e1.record(st)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    steps = p64.points[0] * p64.steps[0] - 1
+    del g64, av
+    torch.cuda.empty_cache()
+    one = dict(_problem(256), ensembles=[256, 1, 1])
+    a64, _ = GpuPath(xpreferences([dict(one, precision="fp64")])[0]).run_path(0, 1, 1)
+    a32, _ = GpuPath(xpreferences([one])[0]).run_path(0, 1, 1)
+    x64, x32 = a64[0][0][0], a32[0][0][0]
+    err = np.abs(x32 - x64)
+    return ({"value": nb * p64.ensembles[0] * steps / (ms * 1e-3), "unit": "traj-steps/s", "ms_per_step": ms},
+            {"observable": "<|a|^2>(x,y,t), 256 trajectories, 51 times", "max_rel": float(err.max() / np.abs(x64).max()),
+             "rms_rel": float(np.sqrt(np.mean(err ** 2)) / np.sqrt(np.mean(np.abs(x64) ** 2))),
+             "reference": "FP64 device path (pinned to the FP64 oracle at 1e-10)"})
+
+
 def _reference_worker(args):
     seconds, ntraj = args
     os.environ.setdefault("OMP_NUM_THREADS", "1")
@@ -303,6 +344,7 @@ def run_ours(args, rank, world, local_rank):
     peak, kind = _peaks()
     tr = NCU_TRAFFIC_PER_TRAJ.get(dom)
     gpu_launches = sum(int(kl[i]) for i in range(8))
+    fp64_line, fp32_err = _precision_report(ntraj)
     cpu_val, cpu_desc = _cpu_sample()
     line = {
         "metric": METRIC,
@@ -320,6 +362,7 @@ def run_ours(args, rank, world, local_rank):
                      "algorithmic_bytes_per_launch": alg_bytes},
         "cpu_baseline": {"value": cpu_val, "unit": "traj-steps/s", "cores": 1, "kind": "port", "sample": cpu_desc},
         "clocks": clocks,
+        "fp64": fp64_line, "fp32_vs_fp64": fp32_err,
     }
     print(json.dumps(line))
 

@@ -28,7 +28,7 @@ def _items():
     return [item("nls", 1, 32, 0.05, 10, 64, 1), item("nls", 1, 32, 0.01, 7, 128, 2),
             item("allen_cahn", 1, 256, 0.1, 5, 64, 3), item("nls", 2, 32, 0.03, 4, 64, 4),
             item("allen_cahn", 2, 64, 0.08, 3, 64, 5), item("nls", 2, 256, 0.02, 3, 64, 6),
-            item("nls", 1, 1024, 0.005, 6, 192, 7)]
+            item("nls", 1, 1024, 0.005, 6, 192, 7), item("allen_cahn", 2, 128, 0.05, 3, 64, 8)]
 
 
 def _single(inp):
@@ -44,7 +44,7 @@ def test_batch_items_match_single_problem_path():
     items = _items()
     b = Batch(items)
     s = b.summary()
-    assert s["items"] == len(items) and s["streaming"] == 1 and s["variants"] == 5, s
+    assert s["items"] == len(items) and s["streaming"] == 1 and s["variants"] == 6, s
     b.run()
     b.sync()
     for i, inp in enumerate(items):
@@ -84,7 +84,7 @@ def test_batch_autotune_and_relaunch_deterministic():
     b = Batch(items)
     b.tune(1)
     tiles = [b.info(i) for i in range(len(items))]
-    assert all(t["path"] == 2 or (t["G"] >= 1 and t["threads"] in (128, 256, 512)) for t in tiles), tiles
+    assert all(t["path"] == 2 or (t["G"] >= 1 and t["threads"] in (128, 256, 512, 1024)) for t in tiles), tiles
     b.run()
     b.sync()
     first = [b.results(i) for i in range(len(items))]

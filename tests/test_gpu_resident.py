@@ -136,3 +136,32 @@ def test_a_in_a_out_roundtrip():
     av_g, a_g = _gpu(g, [1], 1, a_in=a0, a_out=True)
     assert rel_err(a_g, b_o) < FP64_TOL
     assert rel_err(av_g[0][0], av_o[0]) < FP64_TOL
+
+
+def test_field_in_device_memory_2d_periodic_fp64():
+    """128 x 128 FP64 (256 KB per array) exceeds shared memory: the resident
+    kernel keeps field and scratch in per-CTA device-memory slices."""
+    base = dict(dimensions=3, points=[3, 128, 128], ranges=[0.2, 20.0, 20.0], steps=3, ensembles=[2, 2, 1],
+                noises=2, method="MP", checks=1)
+    g = dict(base, deriv="@(a,w,p) 1i*abs(a).^2.*a + 0.02*(w(1,:)+1i*w(2,:))",
+             initial="@(v,p) exp(-(p.x.^2+p.y.^2)/8) + 0.1*v(1,:)", linear="@(p) 0.5i*(p.Dx.^2+p.Dy.^2)",
+             observe=["@(a,p) abs(a).^2", "@(a,p) Int(abs(a).^2, p)"])
+    o = dict(base, deriv=lambda a, w, p: 1j * abs(a) ** 2 * a + 0.02 * (w[0:1] + 1j * w[1:2]),
+             initial=lambda v, p: np.exp(-(p.x ** 2 + p.y ** 2) / 8) + 0.1 * v[0:1],
+             linear=lambda p: 0.5j * (p.Dx ** 2 + p.Dy ** 2),
+             observe=[lambda a, p: abs(a) ** 2, lambda a, p: X.Int(abs(a) ** 2, p)])
+    _compare(g, o, [0, 1], [1, 2], FP64_TOL)
+
+
+def test_field_in_device_memory_3d_dst_dct_fp64():
+    """3D lattice with Dirichlet (DST-I), Neumann (DCT-I) and mixed (DST-III/II)
+    boundaries, too large for shared memory; Allen-Cahn drift with noise."""
+    base = dict(dimensions=4, points=[3, 24, 20, 16], ranges=[0.1, 6.0, 5.0, 4.0], steps=2, ensembles=[2, 2, 1],
+                noises=1, inrandoms=1, method="MP", checks=1, boundaries=[None, [[-1, -1]], [[1, 1]], [[-1, 1]]])
+    g = dict(base, deriv="@(a,w,p) a - a.^3 + 0.1*w(1,:)", initial="@(v,p) 0.3*v(1,:) + 0.5",
+             linear="@(p) 0.05*(p.Dx.^2+p.Dy.^2+p.Dz.^2)",
+             observe=["@(a,p) abs(a).^2", "@(a,p) Int(real(a).^2, p)"])
+    o = dict(base, deriv=lambda a, w, p: a - a ** 3 + 0.1 * w[0:1], initial=lambda v, p: 0.3 * v[0:1] + 0.5,
+             linear=lambda p: 0.05 * (p.Dx ** 2 + p.Dy ** 2 + p.Dz ** 2),
+             observe=[lambda a, p: abs(a) ** 2, lambda a, p: X.Int(np.real(a) ** 2, p)])
+    _compare(g, o, [0, 1], [1, 2], FP64_TOL)

@@ -35,7 +35,15 @@ struct XsPathArgs {
   int pad1;
   const double* w_in;   // [NW, space, ens1] pre-scaled noise for single_step (null: zero)
   const double* params; // runtime named scalars p.<name> (prm[k])
+  cx* gfield;           // XS_GFIELD: per-CTA field + scratch slices [grid][XS_NARR][G*F*NS]
 };
+
+// XS_GFIELD: the lattice is too large for shared memory, so each CTA keeps its
+// field and transform scratch in its own slice of device memory (sized by the
+// host so that the slices of all resident CTAs stay in L2 where possible) and
+// only the reduction scratch in shared memory.  The code is the same; only the
+// arrays' home differs (__syncthreads orders global accesses within a CTA).
+#define XS_FARR (XS_GFIELD ? 0 : XS_NARR)
 
 #define XS_STRIDE1 1
 #define XS_STRIDE2 (XS_N1)
@@ -459,7 +467,7 @@ extern __shared__ __align__(16) unsigned char xs_smem[];
 // not match the layout; the CTA must then return without touching it.
 __device__ __forceinline__ bool xs_layout_ok(int* status) {
   constexpr size_t GF = (size_t)XS_G * XS_F * XS_NS;
-  constexpr size_t need = XS_NARR * GF * sizeof(cx) + (size_t)XS_G * (XS_NRED > 0 ? XS_NRED : 1) * sizeof(cx) +
+  constexpr size_t need = XS_FARR * GF * sizeof(cx) + (size_t)XS_G * (XS_NRED > 0 ? XS_NRED : 1) * sizeof(cx) +
                           32 * 2 * (XS_NRED > 0 ? XS_NRED : 1) * sizeof(double) +
                           XS_WARR * (size_t)XS_G * XS_NWS * XS_NS * sizeof(real);
   u32 dyn;
@@ -475,12 +483,17 @@ __device__ __forceinline__ bool xs_layout_ok(int* status) {
 // observable partial sums in row `cta` of `nctas`.
 __device__ void xs_resident_run(const XsPathArgs& P, int cta, int nctas) {
   constexpr int GF = XS_G * XS_F * XS_NS;
+#if XS_GFIELD
+  cx* A = P.gfield + (size_t)blockIdx.x * XS_NARR * GF;
+  cx* RED = (cx*)xs_smem;             // [G][NRED]
+#else
   cx* A = (cx*)xs_smem;
+  cx* RED = A + XS_NARR * GF;         // [G][NRED]
+#endif
   cx* B1 = A + GF;
   cx* B2 = B1 + (XS_NARR >= 3 ? GF : 0);
   cx* B3 = B2 + (XS_NARR >= 4 ? GF : 0);
   cx* T = A + (XS_NARR - 1) * GF;     // transform scratch is the last array
-  cx* RED = A + XS_NARR * GF;         // [G][NRED]
   double* wsum = (double*)(RED + XS_G * (XS_NRED > 0 ? XS_NRED : 1));  // [32][2*NRED]
   real* W = (real*)(wsum + 32 * 2 * (XS_NRED > 0 ? XS_NRED : 1));
   real* Wp = W + XS_G * XS_NWS * XS_NS;
@@ -585,7 +598,13 @@ __device__ void xs_resident_run(const XsPathArgs& P, int cta, int nctas) {
 
 extern "C" __global__ void __launch_bounds__(XS_THREADS) xs_resident(const XsPathArgs P) {
   if (!xs_layout_ok(P.status)) return;
+#if XS_GFIELD
+  // one slice per CTA of the grid; CTAs loop over the trajectory tiles
+  const int nctas = P.ntraj / XS_G;
+  for (int c = blockIdx.x; c < nctas; c += gridDim.x) xs_resident_run(P, c, nctas);
+#else
   xs_resident_run(P, blockIdx.x, gridDim.x);
+#endif
 }
 
 // ---- uneven batch -------------------------------------------------------------
@@ -619,6 +638,7 @@ struct XsBatchArgs {
   int* status;
   const cx* tmat;
   int tmat_off[4];
+  cx* gfield;            // XS_GFIELD slices, one per CTA of the grid
 };
 
 extern "C" __global__ void __launch_bounds__(XS_THREADS) xs_batch(const XsBatchArgs B) {
@@ -659,6 +679,7 @@ extern "C" __global__ void __launch_bounds__(XS_THREADS) xs_batch(const XsBatchA
     P.pad1 = 0;
     P.w_in = nullptr;
     P.params = it.params;
+    P.gfield = B.gfield;
     xs_resident_run(P, un.y, it.nunits);
     // publish this unit's partial sums, then count it (threadFenceReduction pattern)
     __threadfence();

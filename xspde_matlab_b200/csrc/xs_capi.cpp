@@ -626,6 +626,7 @@ struct DevBuf {
 struct ResidentPlan {
   int G = 1, threads = 32, narr = 2;
   size_t smem = 0;
+  bool gfield = false;  // field + scratch in per-CTA device-memory slices (lattice beyond shared memory)
 };
 
 // Streaming plan: 2D lattice with NX = RX^2, NY = RY^2 (RX, RY in {8, 16, 32}).
@@ -655,7 +656,7 @@ struct xs_handle {
   CUfunction f_batch = nullptr;
   cudaStream_t stream = nullptr;
   DevBuf d_prop[2], d_prop2[2], d_tmat, d_obs, d_av, d_ain, d_aout, d_status, d_w, d_field, d_redpart, d_pstep,
-      d_params;
+      d_params, d_gfield;
   double pstep_dtr = -1;
   double prop_dtr[2] = {-1, -1}, prop2_dtr[2] = {-1, -1};
   // launch accounting (xs_kernel_stats)
@@ -707,8 +708,20 @@ void plan_resident(xs_handle& h, int total_traj) {
   ResidentPlan rp;
   rp.narr = method_arrays(P.p.method);
   const size_t limit = 200 * 1024;
-  if (resident_smem(h, 1, rp.narr) > limit)
-    raise(XS_ERR_UNSUPPORTED, "field of one trajectory does not fit in shared memory for the resident path");
+  if (resident_smem(h, 1, rp.narr) > limit) {
+    // lattice beyond shared memory: one trajectory per CTA, field and scratch in device memory (MP only,
+    // whose noise lives in registers)
+    if (P.p.method != XS_METHOD_MP)
+      raise(XS_ERR_UNSUPPORTED, "field of one trajectory does not fit in shared memory (only MP runs such lattices "
+                                "with the field in device memory)");
+    if (h.force_G > 1) raise(XS_ERR_UNSUPPORTED, "lattices beyond shared memory take one trajectory per CTA");
+    rp.gfield = true;
+    rp.G = 1;
+    rp.threads = h.force_threads ? h.force_threads : 512;
+    rp.smem = resident_smem(h, 1, 0);
+    h.rp = rp;
+    return;
+  }
   if (h.force_G > 0) {
     if (resident_smem(h, h.force_G, rp.narr) > limit) raise(XS_ERR_UNSUPPORTED, "tile does not fit in shared memory");
     if (h.force_threads % 32 || h.force_threads < 0 || h.force_threads > 1024)
@@ -878,7 +891,9 @@ void build_source(xs_handle& h) {
   generate_functions(P, fns);  // fixes P.nred / nout_* before the launch plan
   const bool fits = resident_smem(h, 1, method_arrays(P.p.method)) <= 200 * 1024;
   const std::string why = stream_blocker(P);
-  if (h.path_kind == 2 || (h.path_kind == 0 && !fits)) {
+  // too large for shared memory: the streaming path when it covers the problem, else the resident
+  // path with the field in device memory (MP)
+  if (h.path_kind == 2 || (h.path_kind == 0 && !fits && (why.empty() || P.p.method != XS_METHOD_MP))) {
     if (!why.empty()) {
       if (!fits) raise(XS_ERR_UNSUPPORTED, "field too large for the resident path, and " + why);
       raise(XS_ERR_UNSUPPORTED, why);
@@ -903,7 +918,7 @@ void build_source(xs_handle& h) {
   emit_common_header(h, os);
   os << "#define XS_G " << h.rp.G << "\n#define XS_THREADS " << h.rp.threads << "\n#define XS_NARR " << h.rp.narr << "\n";
   os << "#define XS_LEAN " << (P.p.method == XS_METHOD_MP ? 1 : 0) << "\n#define XS_WARR "
-     << (P.p.method == XS_METHOD_MP ? 0 : 2) << "\n";
+     << (P.p.method == XS_METHOD_MP ? 0 : 2) << "\n#define XS_GFIELD " << (h.rp.gfield ? 1 : 0) << "\n";
   os << "#define XS_SMEM_BYTES " << h.rp.smem << "\n";
   {
     std::string stages;
@@ -1046,6 +1061,7 @@ struct PathArgsHost {
   int pad1;
   const double* w_in;
   const double* params;
+  void* gfield;
 };
 
 size_t av_stride(const Problem& P) { return (size_t)P.nout_site * P.NS + P.nout_scalar; }
@@ -1083,6 +1099,23 @@ void xs_launch(xs_handle& h, int kind, CUfunction f, unsigned gx, unsigned gy, u
   }
 }
 
+// Grid of a resident launch over nctas trajectory tiles.  With the field in
+// device memory the grid is persistent: one slice per CTA, as many CTAs as
+// are resident at once but no more slices than ~96 MB (L2-sized) unless that
+// would leave SMs idle.
+int resident_grid(xs_handle& h, CUfunction f, int nctas) {
+  if (!h.rp.gfield) return nctas;
+  int dev = 0, sms = 0, occ = 0;
+  CUDA_CHECK(cudaGetDevice(&dev));
+  CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  cu_check(driver().occupancy(&occ, f, h.rp.threads, h.rp.smem), "occupancy");
+  const size_t slice = (size_t)h.rp.narr * h.rp.G * h.P.F * h.P.NS * (h.fp64 ? 16 : 8);
+  const int l2 = (int)std::max<size_t>(1, (96u << 20) / slice);
+  const int grid = std::max(1, std::min({nctas, sms * std::max(occ, 1), std::max(sms, l2)}));
+  h.d_gfield.ensure((size_t)grid * slice);
+  return grid;
+}
+
 // Launch the resident path; av_dev receives [nblocks][npoints][stride] complex.
 void launch_resident(xs_handle& h, int first_block, int nblocks, int nc, const void* a_in_dev, void* av_dev,
                      void* a_out_dev, cudaStream_t st) {
@@ -1115,8 +1148,10 @@ void launch_resident(xs_handle& h, int first_block, int nblocks, int nc, const v
   a.obs = h.d_obs.p;
   a.status = (int*)h.d_status.p;
   a.params = (const double*)h.d_params.p;
+  const int grid = resident_grid(h, h.f_resident, nctas);
+  a.gfield = h.d_gfield.p;
   void* params[] = {&a};
-  xs_launch(h, XS_KERNEL_RESIDENT, h.f_resident, nctas, 1, 1, h.rp.threads, (unsigned)h.rp.smem, st, params,
+  xs_launch(h, XS_KERNEL_RESIDENT, h.f_resident, grid, 1, 1, h.rp.threads, (unsigned)h.rp.smem, st, params,
             "launch xs_resident");
   if (stride > 0) {
     const void* part = h.d_obs.p;
@@ -1458,6 +1493,8 @@ XS_API xs_status xs_run_path_device_noalloc(xs_handle* h, int first_block, int n
     const Problem& P = h->P;
     if (h->kind != 1)
       raise(XS_ERR_UNSUPPORTED, "xs_run_path_device_noalloc covers problems on the resident path only");
+    if (h->rp.gfield)
+      raise(XS_ERR_UNSUPPORTED, "xs_run_path_device_noalloc needs the field in shared memory (it would allocate slices)");
     if (nc == 2 && !P.p.checks) raise(XS_ERR_ARG, "coarse pass requested without checks");
     const int slot = nc == 2 ? 1 : 0;
     if (!h->loaded || !h->d_prop[slot].p || (P.has_linear && h->prop_dtr[slot] != pass_dtr(P, nc)))
@@ -1752,7 +1789,9 @@ XS_API xs_status xs_step(xs_handle* h, double* a_inout, const double* w, double 
     a.w_in = (w && wn) ? (const double*)h->d_w.p : nullptr;
     a.params = (const double*)h->d_params.p;
     void* params[] = {&a};
-    xs_launch(*h, XS_KERNEL_RESIDENT, h->f_resident, (unsigned)(ntraj / h->rp.G), 1, 1, h->rp.threads,
+    const int grid = resident_grid(*h, h->f_resident, (int)(ntraj / h->rp.G));
+    a.gfield = h->d_gfield.p;
+    xs_launch(*h, XS_KERNEL_RESIDENT, h->f_resident, (unsigned)grid, 1, 1, h->rp.threads,
               (unsigned)h->rp.smem, h->stream, params, "launch xs_resident (step)");
     int status = 0;
     CUDA_CHECK(cudaMemcpyAsync(tmp.data(), h->d_aout.p, fbytes, cudaMemcpyDeviceToHost, h->stream));
@@ -1798,8 +1837,9 @@ struct BatchArgsHost {  // mirrors XsBatchArgs
   int* status;
   const void* tmat;
   int tmat_off[4];
+  void* gfield;
 };
-static_assert(sizeof(BatchArgsHost) == 64, "XsBatchArgs layout");
+static_assert(sizeof(BatchArgsHost) == 72, "XsBatchArgs layout");
 
 struct BatchVariant {
   std::string key;                 // generated source at a unit tile
@@ -1909,6 +1949,8 @@ void batch_drop_graph(xs_batch& b) {
 std::vector<std::pair<int, int>> tile_candidates(const BatchVariant& v, const xs_handle& proto) {
   const Problem& P = proto.P;
   const int narr = method_arrays(P.p.method);
+  if (resident_smem(proto, 1, narr) > 200 * 1024)  // field in device memory: one trajectory per CTA
+    return {{1, 256}, {1, 512}, {1, 1024}};
   std::vector<int> Gs;  // divisors of every item's trajectory count, ascending
   for (int G = 1; G <= 4096 && G <= v.gcd_traj; ++G) {
     if (v.gcd_traj % G) continue;
@@ -2000,13 +2042,15 @@ void variant_launch(xs_batch& b, BatchVariant& v, const DevBuf& d_items, const D
   a.status = (int*)b.d_status.p;
   a.tmat = h.d_tmat.p;
   for (int i = 0; i < 4; ++i) a.tmat_off[i] = h.tmat_off[i];
+  a.gfield = h.d_gfield.p;
   void* params[] = {&a};
   cu_check(driver().launch(h.f_batch, (unsigned)v.grid, 1, 1, (unsigned)h.rp.threads, 1, 1, (unsigned)h.rp.smem,
                            (CUstream)st, params, nullptr),
            "launch xs_batch");
 }
 
-int variant_grid(const BatchVariant& v) {
+int variant_grid(BatchVariant& v) {
+  if (v.h->rp.gfield) return resident_grid(*v.h, v.h->f_batch, v.nunits);
   int dev = 0, sms = 0, occ = 0;
   CUDA_CHECK(cudaGetDevice(&dev));
   CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));

@@ -13,6 +13,10 @@ dpo_0d: positive-P degenerate parametric oscillator, two complex fields
   runtime scalar; MP integrates in the Stratonovich sense, so the drift carries
   the correction -1/2 B dB/dalpha = +chi alpha / 2 (the Ito form is the one
   Euler takes).  alpha = beta = 1 at t = 0; 2000 steps to t = 10.
+ac_3d: 3D stochastic Allen-Cahn on 64^3 over [-10,10]^3, da/dt = 0.05 lap a +
+  a - a^3 + 0.1 w, Dirichlet (DST-I) boundaries in x, Neumann (DCT-I) in y,
+  Dirichlet-Neumann (DST-III/II) in z, a0 = 0.1 v, FP32 fields, 256
+  trajectories in 8 blocks, 100 MP steps to t = 1 (6 output points).
 xi is complex white noise (w1 + i w2)/sqrt(2).
 """
 import ctypes
@@ -43,7 +47,15 @@ DPO_0D = dict(
     initial="@(v,p) [1; 1]",
     observe=["@(a,p) real(a(1,:).*a(2,:))", "@(a,p) real(a(1,:))"])
 
-PROBLEMS = {"snls_1d": SNLS_1D, "gpe_2d": GPE_2D, "dpo_0d": DPO_0D}
+AC_3D = dict(
+    dimensions=4, points=[6, 64, 64, 64], ranges=[1.0, 20.0, 20.0, 20.0], steps=20, ensembles=[32, 8, 1],
+    noises=1, inrandoms=1, method="MP", checks=0, precision="fp32",
+    boundaries=[None, [[-1, -1]], [[1, 1]], [[-1, 1]]],
+    deriv="@(a,w,p) a - a.^3 + 0.1*w(1,:)", initial="@(v,p) 0.1*v(1,:)",
+    linear="@(p) 0.05*(p.Dx.^2+p.Dy.^2+p.Dz.^2)",
+    observe=["@(a,p) abs(a).^2", "@(a,p) Int(real(a).^2, p)"])
+
+PROBLEMS = {"snls_1d": SNLS_1D, "gpe_2d": GPE_2D, "dpo_0d": DPO_0D, "ac_3d": AC_3D}
 
 
 def compile_check(name, **over):
