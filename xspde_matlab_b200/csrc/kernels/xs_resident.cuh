@@ -36,6 +36,7 @@ struct XsPathArgs {
   const double* w_in;   // [NW, space, ens1] pre-scaled noise for single_step (null: zero)
   const double* params; // runtime named scalars p.<name> (prm[k])
   cx* gfield;           // XS_GFIELD: per-CTA field + scratch slices [grid][XS_NARR][G*F*NS]
+  const double2* prop2; // exp(2 L dtr / ipsteps): two consecutive half-step propagators of MP
 };
 
 // XS_GFIELD: the lattice is too large for shared memory, so each CTA keeps its
@@ -44,6 +45,8 @@ struct XsPathArgs {
 // only the reduction scratch in shared memory.  The code is the same; only the
 // arrays' home differs (__syncthreads orders global accesses within a CTA).
 #define XS_FARR (XS_GFIELD ? 0 : XS_NARR)
+
+extern __shared__ __align__(16) unsigned char xs_smem[];
 
 #define XS_STRIDE1 1
 #define XS_STRIDE2 (XS_N1)
@@ -179,11 +182,113 @@ __device__ __forceinline__ void xs_setbound(cx* X) {
 #endif
 }
 
+// ---- tiled line transforms (field in device memory) --------------------------
+// A tile of TL lines along dimension D is loaded once into shared memory as
+// S[n][l] (element n of line l, row stride LSP = padded TL), transformed there
+// (Stockham stages ping-ponging S and S2, or the dense matrix into S2), and
+// stored once: one read and one write of the field per transformed dimension.
+template <int ND, int R, int NSP, bool FIRST, bool LAST, int TL, int LSP>
+__device__ __forceinline__ void xs_fft_tstage(const cx* __restrict__ in, cx* __restrict__ out,
+                                              const cx* __restrict__ tw, int inv) {
+  constexpr int NB = ND / R;
+  const real sc = (LAST ? (real)(1.0 / ND) : (real)1);
+  for (int b = threadIdx.x; b < NB * TL; b += blockDim.x) {
+    const int l = b % TL, j = b / TL;
+    const int k = j % NSP;
+    cx v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      cx a = in[(j + r * NB) * LSP + l];
+      if (FIRST && inv) a.im = -a.im;
+      if (NSP > 1 && r > 0) a = a * tw[k * r * (ND / (NSP * R))];
+      v[r] = a;
+    }
+    xs_dft_r<R>(v);
+    const int o0 = (j / NSP) * NSP * R + k;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      cx a = v[r];
+      if (LAST && inv) a = mkcx(a.re * sc, -a.im * sc);
+      out[(o0 + r * NSP) * LSP + l] = a;
+    }
+  }
+}
+
+// Generated per-dimension tile stage lists (return the buffer with the result).
+template <int D> __device__ __forceinline__ cx* xs_fft_tile_d(cx* S, cx*, const cx*, int) { return S; }
+XS_FFT_TILE_STAGES
+
+#if XS_GFIELD
+template <int D>
+__device__ void xs_tr_tiled(cx* X, const XsPathArgs& P, int dir) {
+  constexpr int ND = D == 1 ? XS_N1 : (D == 2 ? XS_N2 : XS_N3);
+  constexpr int SD = D == 1 ? XS_STRIDE1 : (D == 2 ? XS_STRIDE2 : XS_STRIDE3);
+  constexpr int TL = D == 1 ? XS_TL1 : (D == 2 ? XS_TL2 : XS_TL3);
+  constexpr int LSP = D == 1 ? XS_LSP1 : (D == 2 ? XS_LSP2 : XS_LSP3);
+  constexpr bool fft = D == 1 ? XS_FFTD1 : (D == 2 ? XS_FFTD2 : XS_FFTD3);
+  if constexpr (ND > 1) {
+    constexpr int NHI = XS_G * XS_F * XS_NS / (SD * ND);  // line groups (g, f, slower dims)
+    constexpr int NPER = XS_NS / (SD * ND);               // line groups per (g, f)
+    constexpr int NT = SD == 1 ? NHI / TL : NHI * (SD / (SD == 1 ? 1 : TL));
+    cx* S = (cx*)xs_smem;
+    cx* S2 = S + XS_TILE_ELEMS;
+    for (int tile = 0; tile < NT; ++tile) {
+      int hi0, lo0;
+      if constexpr (SD == 1) { hi0 = tile * TL; lo0 = 0; }
+      else { hi0 = tile / (SD / TL); lo0 = (tile % (SD / TL)) * TL; }
+      for (int i = threadIdx.x; i < TL * ND; i += blockDim.x) {
+        int n, l;
+        size_t gi;
+        if constexpr (SD == 1) { l = i / ND; n = i % ND; gi = (size_t)(hi0 + l) * ND + n; }
+        else { n = i / TL; l = i % TL; gi = (size_t)lo0 + l + (size_t)SD * (n + (size_t)ND * hi0); }
+        S[n * LSP + l] = X[gi];
+      }
+      __syncthreads();
+      cx* Rb;
+      if constexpr (fft) {
+        Rb = xs_fft_tile_d<D>(S, S2, P.tmat + P.tmat_off[D], dir);
+      } else {
+        const int f = (hi0 / NPER) % XS_F;
+        const cx* M = P.tmat + P.tmat_off[D] + (size_t)(f * 2 + dir) * ND * ND;
+        for (int i = threadIdx.x; i < TL * ND; i += blockDim.x) {
+          const int l = i % TL, k = i / TL;
+          real ar = 0, ai = 0;
+#pragma unroll 8
+          for (int n = 0; n < ND; ++n) {
+            const cx m = M[n * ND + k];
+            const cx v = S[n * LSP + l];
+            ar += m.re * v.re - m.im * v.im;
+            ai += m.re * v.im + m.im * v.re;
+          }
+          S2[k * LSP + l] = mkcx(ar, ai);
+        }
+        __syncthreads();
+        Rb = S2;
+      }
+      for (int i = threadIdx.x; i < TL * ND; i += blockDim.x) {
+        int n, l;
+        size_t gi;
+        if constexpr (SD == 1) { l = i / ND; n = i % ND; gi = (size_t)(hi0 + l) * ND + n; }
+        else { n = i / TL; l = i % TL; gi = (size_t)lo0 + l + (size_t)SD * (n + (size_t)ND * hi0); }
+        X[gi] = Rb[n * LSP + l];
+      }
+      __syncthreads();
+    }
+  }
+}
+#endif
+
 // Transform along dimension D: generated Stockham stages (xs_fft_d<D>, defined
 // by the problem header when XS_FFTD<D> is set) or the dense matrix.
 template <int D>
 __device__ __forceinline__ void xs_tr(cx* X, cx* T, const XsPathArgs& P, int dir) {
   constexpr bool fft = D == 1 ? XS_FFTD1 : (D == 2 ? XS_FFTD2 : XS_FFTD3);
+#if XS_GFIELD
+  if (true) {
+    __syncthreads();
+    xs_tr_tiled<D>(X, P, dir);
+  } else
+#endif
   if constexpr (fft) {
     __syncthreads();
     xs_fft_d<D>(X, T, P.tmat + P.tmat_off[D], dir);
@@ -194,7 +299,7 @@ __device__ __forceinline__ void xs_tr(cx* X, cx* T, const XsPathArgs& P, int dir
 }
 
 // xprop (Applications/SPDE/xprop.m:76-104): transform, multiply by exp(L dt), inverse.
-__device__ __forceinline__ void xs_prop(cx* X, cx* T, const XsPathArgs& P) {
+__device__ __forceinline__ void xs_prop_tab(cx* X, cx* T, const XsPathArgs& P, const double2* __restrict__ tab) {
 #if XS_HAS_PROP
   xs_tr<1>(X, T, P, 0);
   xs_tr<2>(X, T, P, 0);
@@ -202,7 +307,7 @@ __device__ __forceinline__ void xs_prop(cx* X, cx* T, const XsPathArgs& P) {
   for (int i = threadIdx.x; i < XS_G * XS_F * XS_NS; i += blockDim.x) {
     const int s = i % XS_NS;
     const int f = (i / XS_NS) % XS_F;
-    const double2 pr = P.prop[(XS_PROP_COMPS > 1 ? f : 0) * XS_NS + s];
+    const double2 pr = tab[(XS_PROP_COMPS > 1 ? f : 0) * XS_NS + s];
     const cx v = X[i];
     const double vr = (double)v.re, vi = (double)v.im;
     X[i] = mkcx((real)(vr * pr.x - vi * pr.y), (real)(vr * pr.y + vi * pr.x));
@@ -215,6 +320,7 @@ __device__ __forceinline__ void xs_prop(cx* X, cx* T, const XsPathArgs& P) {
   xs_setbound(X);
   __syncthreads();
 }
+__device__ __forceinline__ void xs_prop(cx* X, cx* T, const XsPathArgs& P) { xs_prop_tab(X, T, P, P.prop); }
 
 // dst = base + h * deriv(src, w, t), pointwise over sites (all components at once).
 __device__ __forceinline__ void xs_deriv_update(cx* dst, const cx* base, const cx* src, const real* W, real h, double t,
@@ -309,11 +415,16 @@ __device__ void xs_method(cx* A, cx* B1, cx* B2, cx* B3, cx* T, const real* W, c
 // memory.  mode 0: fine draw `draw`; 2: coarse pass, mean of draws `prev` and
 // `draw` (Simulator/xnoise.m:33-35); 3: the caller's noise P.w_in (p.method).
 // The arithmetic is that of the unfused step, operation for operation.
-__device__ void xs_mp_lean(cx* A, cx* T, const XsPathArgs& P, double t, int g0, int mode, int draw, int prev) {
+// Consecutive half-step propagators of neighbouring steps are merged, as in
+// the streaming path: `merged` = the previous step's second half is still
+// pending, so the first half applies exp(2 L dt/2) (P.prop2); with `last` the
+// step ends with its own second half, otherwise that half is left pending.
+__device__ void xs_mp_lean(cx* A, cx* T, const XsPathArgs& P, double t, int g0, int mode, int draw, int prev,
+                           bool merged, bool last) {
   const double dtr = P.dtr;
   const real h = (real)(dtr * 0.5);
   const real tm = (real)(t + dtr * 0.5);
-  xs_prop(A, T, P);
+  xs_prop_tab(A, T, P, merged ? P.prop2 : P.prop);
   for (int i = threadIdx.x; i < XS_G * XS_NS; i += blockDim.x) {
     const int g = i / XS_NS, s = i % XS_NS;
     const int e = g0 + g;
@@ -359,7 +470,7 @@ __device__ void xs_mp_lean(cx* A, cx* T, const XsPathArgs& P, double t, int g0, 
     for (int f = 0; f < XS_F; ++f) A[(g * XS_F + f) * XS_NS + s] = (real)2 * a[f] - a0[f];
   }
   __syncthreads();
-  xs_prop(A, T, P);
+  if (last) xs_prop(A, T, P);
   __syncthreads();
 }
 #endif
@@ -460,14 +571,12 @@ __device__ void xs_observe(const cx* A, cx* RED, int n, double t, const XsPathAr
   __syncthreads();
 }
 
-extern __shared__ __align__(16) unsigned char xs_smem[];
-
 // Shared-memory layout of one CTA (XS_SMEM_BYTES in total).  False, with
 // status bit 1 set, when this launch's dynamic shared memory or block size do
 // not match the layout; the CTA must then return without touching it.
 __device__ __forceinline__ bool xs_layout_ok(int* status) {
   constexpr size_t GF = (size_t)XS_G * XS_F * XS_NS;
-  constexpr size_t need = XS_FARR * GF * sizeof(cx) + (size_t)XS_G * (XS_NRED > 0 ? XS_NRED : 1) * sizeof(cx) +
+  constexpr size_t need = (XS_FARR * GF + 2 * (size_t)XS_TILE_ELEMS) * sizeof(cx) + (size_t)XS_G * (XS_NRED > 0 ? XS_NRED : 1) * sizeof(cx) +
                           32 * 2 * (XS_NRED > 0 ? XS_NRED : 1) * sizeof(double) +
                           XS_WARR * (size_t)XS_G * XS_NWS * XS_NS * sizeof(real);
   u32 dyn;
@@ -485,7 +594,7 @@ __device__ void xs_resident_run(const XsPathArgs& P, int cta, int nctas) {
   constexpr int GF = XS_G * XS_F * XS_NS;
 #if XS_GFIELD
   cx* A = P.gfield + (size_t)blockIdx.x * XS_NARR * GF;
-  cx* RED = (cx*)xs_smem;             // [G][NRED]
+  cx* RED = (cx*)xs_smem + 2 * XS_TILE_ELEMS;  // after the two transform tiles; [G][NRED]
 #else
   cx* A = (cx*)xs_smem;
   cx* RED = A + XS_NARR * GF;         // [G][NRED]
@@ -544,13 +653,14 @@ __device__ void xs_resident_run(const XsPathArgs& P, int cta, int nctas) {
 #endif
     __syncthreads();
 #if XS_LEAN
-    xs_mp_lean(A, T, P, P.t0, g0, 3, 0, 0);
+    xs_mp_lean(A, T, P, P.t0, g0, 3, 0, 0, false, true);
 #else
     xs_method(A, B1, B2, B3, T, W, P, P.t0);
 #endif
   } else {
   double t = P.t0;
   int draw = 0;
+  bool pending = false;  // lean MP: second half-step propagator not yet applied
   for (int n = 0; n < P.npoints; ++n) {
     for (int step = 0; step < P.steps; ++step) {
       if (n > 0 || step > 0 || P.npoints == 1) {
@@ -561,7 +671,8 @@ __device__ void xs_resident_run(const XsPathArgs& P, int cta, int nctas) {
 #if XS_LEAN
           if (P.nc == 1 || chk == 1) {
             __syncthreads();
-            xs_mp_lean(A, T, P, t, g0, mode, draw, draw - 1);
+            xs_mp_lean(A, T, P, t, g0, mode, draw, draw - 1, pending, false);
+            pending = true;
             t += P.dtr;
           }
 #else
@@ -576,10 +687,17 @@ __device__ void xs_resident_run(const XsPathArgs& P, int cta, int nctas) {
       }
       if (step == 0) {
         __syncthreads();
+#if XS_LEAN
+        if (pending) xs_prop(A, T, P);
+        pending = false;
+#endif
         xs_observe(A, RED, n, t, P, wsum, cta, nctas);
       }
     }
   }
+#if XS_LEAN
+  if (pending) xs_prop(A, T, P);
+#endif
   }
   __syncthreads();
   // final field and non-finite check
@@ -626,7 +744,7 @@ struct XsBatchItem {
   double2* av;           // [npoints][XS_OBS_STRIDE] means over the item's trajectories
   const double* params;  // runtime scalars of this item
   int* done;             // units finished
-  int pad2[2];
+  const double2* prop2;  // exp(2 L dtr / ipsteps) of this item
 };
 
 struct XsBatchArgs {
@@ -680,6 +798,7 @@ extern "C" __global__ void __launch_bounds__(XS_THREADS) xs_batch(const XsBatchA
     P.w_in = nullptr;
     P.params = it.params;
     P.gfield = B.gfield;
+    P.prop2 = it.prop2;
     xs_resident_run(P, un.y, it.nunits);
     // publish this unit's partial sums, then count it (threadFenceReduction pattern)
     __threadfence();

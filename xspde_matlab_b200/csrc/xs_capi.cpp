@@ -683,13 +683,46 @@ struct xs_handle {
 
 namespace {
 
+// Tiles of the line transforms when the field lives in device memory: lines
+// per tile TL (a divisor of the line count that keeps both tile buffers within
+// ~96 KB) and padded row stride LSP, per space dimension; elems = the larger
+// tile buffer in complex elements.
+void tile_plan(const Problem& P, bool fp64, int tl[3], int lsp[3], size_t& elems) {
+  const size_t cxs = fp64 ? 16 : 8, cap = 96 * 1024;
+  elems = 0;
+  int sd = 1;
+  for (int d = 0; d < 3; ++d) {
+    tl[d] = lsp[d] = 1;
+    const int nd = d < P.D ? P.N[d] : 1;
+    if (nd > 1) {
+      const int lines = sd == 1 ? P.NS / nd : sd;  // lines per (g, f) group (d = 0) or per line group
+      int best = 1;
+      for (int t = 1; t <= (sd == 1 ? lines : std::min(lines, 32)); ++t) {
+        if (lines % t) continue;
+        const int lp = t % 2 ? t : t + 1;
+        if (2 * (size_t)nd * lp * cxs > cap) break;
+        best = t;
+      }
+      tl[d] = best;
+      lsp[d] = best % 2 ? best : best + 1;
+      elems = std::max(elems, (size_t)nd * lsp[d]);
+    }
+    if (d < P.D) sd *= P.N[d];
+  }
+}
+
 size_t resident_smem(const xs_handle& h, int G, int narr) {
   const Problem& P = h.P;
   size_t cxs = h.fp64 ? 16 : 8, rs = h.fp64 ? 8 : 4;
   size_t nred = std::max(P.nred, 1);
   size_t nws = std::max(P.NW, 1);
   const size_t warr = P.p.method == XS_METHOD_MP ? 0 : 2;  // MP keeps its noise in registers
-  return (size_t)narr * G * P.F * P.NS * cxs + (size_t)G * nred * cxs + 32 * 2 * nred * 8 +
+  size_t tiles = 0;
+  if (narr == 0) {  // field in device memory: two transform tiles in shared memory
+    int tl[3], lsp[3];
+    tile_plan(P, h.fp64, tl, lsp, tiles);
+  }
+  return (size_t)narr * G * P.F * P.NS * cxs + 2 * tiles * cxs + (size_t)G * nred * cxs + 32 * 2 * nred * 8 +
          warr * (size_t)G * nws * P.NS * rs;
 }
 
@@ -757,6 +790,29 @@ bool fft_dim(const Problem& P, int d) {
   for (int f = 0; f < P.F; ++f)
     if (P.type(d, f) != 0) return false;
   return true;
+}
+
+// Stage list of a shared-memory tile (TL lines of length n, row stride lsp);
+// returns the buffer that holds the result.
+std::string gen_fft_tile_stages(int D, int n, int tl, int lsp) {
+  int k = 0;
+  while ((1 << k) < n) ++k;
+  const int S = (k + 2) / 3;
+  std::vector<int> bits(S, k / S);
+  for (int i = 0; i < k % S; ++i) ++bits[i];
+  std::ostringstream os;
+  os << "template <> __device__ __forceinline__ cx* xs_fft_tile_d<" << D
+     << ">(cx* S, cx* S2, const cx* __restrict__ tw, int inv) { ";
+  int nsp = 1;
+  for (int i = 0; i < S; ++i) {
+    const int R = 1 << bits[i];
+    os << "xs_fft_tstage<" << n << ", " << R << ", " << nsp << ", " << (i == 0 ? "true" : "false") << ", "
+       << (i == S - 1 ? "true" : "false") << ", " << tl << ", " << lsp << ">(" << (i % 2 ? "S2, S" : "S, S2")
+       << ", tw, inv); __syncthreads(); ";
+    nsp *= R;
+  }
+  os << "return " << (S % 2 ? "S2" : "S") << "; } ";
+  return os.str();
 }
 
 // Stockham stage sequence of one dimension (length n, site stride sd): an even
@@ -930,6 +986,16 @@ void build_source(xs_handle& h) {
       if (d < P.D) sd *= P.N[d];
     }
     os << "#define XS_FFT_STAGES " << stages << "\n";
+    int tl[3] = {1, 1, 1}, lsp[3] = {1, 1, 1};
+    size_t elems = 0;
+    std::string tstages;
+    if (h.rp.gfield) {
+      tile_plan(P, h.fp64, tl, lsp, elems);
+      for (int d = 0; d < 3; ++d)
+        if (fft_dim(P, d)) tstages += gen_fft_tile_stages(d + 1, P.N[d], tl[d], lsp[d]);
+    }
+    for (int d = 0; d < 3; ++d) os << "#define XS_TL" << d + 1 << " " << tl[d] << "\n#define XS_LSP" << d + 1 << " " << lsp[d] << "\n";
+    os << "#define XS_TILE_ELEMS " << elems << "\n#define XS_FFT_TILE_STAGES " << tstages << "\n";
   }
   os << fns.str();
   os << xs_kernel_source_resident << "\n";
@@ -1062,6 +1128,7 @@ struct PathArgsHost {
   const double* w_in;
   const double* params;
   void* gfield;
+  const void* prop2;
 };
 
 size_t av_stride(const Problem& P) { return (size_t)P.nout_site * P.NS + P.nout_scalar; }
@@ -1098,6 +1165,8 @@ void xs_launch(xs_handle& h, int kind, CUfunction f, unsigned gx, unsigned gy, u
     h.pending.push_back({kind, a, b});
   }
 }
+
+const void* ensure_prop2(xs_handle& h, int nc);
 
 // Grid of a resident launch over nctas trajectory tiles.  With the field in
 // device memory the grid is persistent: one slice per CTA, as many CTAs as
@@ -1141,6 +1210,7 @@ void launch_resident(xs_handle& h, int first_block, int nblocks, int nc, const v
   a.dtr = pass_dtr(P, nc);
   a.t0 = P.p.origins[0];
   a.prop = ensure_prop(h, nc);
+  a.prop2 = ensure_prop2(h, nc);
   a.tmat = h.d_tmat.p;
   for (int i = 0; i < 4; ++i) a.tmat_off[i] = h.tmat_off[i];
   a.a_in = a_in_dev;
@@ -1531,6 +1601,7 @@ XS_API xs_status xs_run_path_device_noalloc(xs_handle* h, int first_block, int n
     a.dtr = pass_dtr(P, nc);
     a.t0 = P.p.origins[0];
     a.prop = h->d_prop[slot].p;
+    a.prop2 = h->d_prop2[slot].p;
     a.tmat = h->d_tmat.p;
     for (int i = 0; i < 4; ++i) a.tmat_off[i] = h->tmat_off[i];
     a.a_in = nullptr;
@@ -1779,6 +1850,7 @@ XS_API xs_status xs_step(xs_handle* h, double* a_inout, const double* w, double 
     a.dtr = dtr;
     a.t0 = t;
     a.prop = h->d_pstep.p;
+    a.prop2 = h->d_pstep.p;  // one whole step: no merged half steps
     a.tmat = h->d_tmat.p;
     for (int i = 0; i < 4; ++i) a.tmat_off[i] = h->tmat_off[i];
     a.a_in = h->d_ain.p;
@@ -1825,7 +1897,7 @@ struct BatchItemHost {  // mirrors XsBatchItem
   void* av;
   const double* params;
   int* done;
-  int pad2[2];
+  const void* prop2;
 };
 static_assert(sizeof(BatchItemHost) == 112, "XsBatchItem layout");
 
@@ -2004,6 +2076,7 @@ void variant_tables(xs_batch& b, BatchVariant& v, int steps_cap, int points_cap,
     it.dtr = item_dtr(P);
     it.t0 = P.p.origins[0];
     it.prop = (const char*)b.d_prop.p + e.prop_off * 16;
+    it.prop2 = (const char*)b.d_prop.p + (e.prop_off + (P.has_linear ? P.L.size() : 1)) * 16;
     const size_t stride = av_stride(P);
     if (part_base) {
       it.part = (char*)part_base + part * 16;
@@ -2072,8 +2145,8 @@ void batch_buffers(xs_batch& b) {
     if (e.variant < 0) continue;
     const BatchVariant& v = *b.variants[e.variant];
     e.nunits = ntraj_of(P) / std::max(v.G, 1);
-    e.prop_off = prop;
-    prop += P.has_linear ? P.L.size() : 1;
+    e.prop_off = prop;  // exp(L dtr/ipsteps), then exp(2 L dtr/ipsteps)
+    prop += 2 * (P.has_linear ? P.L.size() : 1);
     e.param_off = par;
     par += P.runtime_defaults.size();
     e.part_off = part;
@@ -2095,6 +2168,8 @@ void batch_buffers(xs_batch& b) {
     if (P.has_linear) {
       auto pr = prop_table(P, item_dtr(P));
       std::copy(pr.begin(), pr.end(), hp.begin() + e.prop_off);
+      auto pr2 = prop_table(P, 2 * item_dtr(P));
+      std::copy(pr2.begin(), pr2.end(), hp.begin() + e.prop_off + pr.size());
     }
     std::copy(P.runtime_defaults.begin(), P.runtime_defaults.end(), hpar.begin() + e.param_off);
   }
