@@ -606,7 +606,8 @@ def run_ac3d(args):
     from xspde_matlab_b200 import GpuPath, _lib, xpreferences
     from xspde_matlab_b200.problems import AC_3D
     L = _lib.lib()
-    p = xpreferences([dict(AC_3D)])[0]
+    blocks = max(1, args.ac3d_traj // AC_3D["ensembles"][0])
+    p = xpreferences([dict(AC_3D, ensembles=[AC_3D["ensembles"][0], blocks, 1])])[0]
     g = GpuPath(p)
     nb = p.ensembles[1]
     av = torch.zeros((nb * g.per_block,), dtype=torch.float64, device="cuda")
@@ -655,7 +656,7 @@ def run_ac3d(args):
                              "sample": "1 trajectory x %d MP steps (FP64 NumPy oracle)" % n},
             "clocks": clk.summary(),
             "config": {"workload": "ac_3d: 64^3, x Dirichlet (DST-I), y Neumann (DCT-I), z Dirichlet-Neumann, "
-                                   "256 trajectories (8 blocks), 6 points x 20 steps = 99 MP steps"}}
+                                   "%d trajectories (%d blocks), 6 points x 20 steps = 99 MP steps" % (ntraj, nb)}}
     print(json.dumps(line))
 
 
@@ -723,6 +724,7 @@ def main():
     ap.add_argument("--batch-items", type=int, default=512)
     ap.add_argument("--dpo", action="store_true", help="positive-P DPO, 10^6 trajectories x 2000 steps")
     ap.add_argument("--ac3d", action="store_true", help="3D stochastic Allen-Cahn 64^3 with DST/DCT boundaries")
+    ap.add_argument("--ac3d-traj", type=int, default=256, help="trajectories of --ac3d (multiple of 32)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -249,18 +249,41 @@ __device__ void xs_tr_tiled(cx* X, const XsPathArgs& P, int dir) {
         Rb = xs_fft_tile_d<D>(S, S2, P.tmat + P.tmat_off[D], dir);
       } else {
         const int f = (hi0 / NPER) % XS_F;
-        const cx* M = P.tmat + P.tmat_off[D] + (size_t)(f * 2 + dir) * ND * ND;
-        for (int i = threadIdx.x; i < TL * ND; i += blockDim.x) {
-          const int l = i % TL, k = i / TL;
-          real ar = 0, ai = 0;
-#pragma unroll 8
+        const cx* __restrict__ M = P.tmat + P.tmat_off[D] + (size_t)(f * 2 + dir) * ND * ND;
+        // register block: KB outputs k x LB lines per thread; real matrices
+        // (every DST/DCT type) skip the imaginary part of M
+        constexpr int KB = ND % 4 == 0 ? 4 : 1, LB = TL % 2 == 0 ? 2 : 1;
+        constexpr bool RM = D == 1 ? XS_REALM1 : (D == 2 ? XS_REALM2 : XS_REALM3);
+        for (int i = threadIdx.x; i < (ND / KB) * (TL / LB); i += blockDim.x) {
+          const int l0 = (i % (TL / LB)) * LB, k0 = (i / (TL / LB)) * KB;
+          real ar[KB][LB], ai[KB][LB];
+#pragma unroll
+          for (int q = 0; q < KB; ++q)
+#pragma unroll
+            for (int j = 0; j < LB; ++j) ar[q][j] = ai[q][j] = 0;
+#pragma unroll 4
           for (int n = 0; n < ND; ++n) {
-            const cx m = M[n * ND + k];
-            const cx v = S[n * LSP + l];
-            ar += m.re * v.re - m.im * v.im;
-            ai += m.re * v.im + m.im * v.re;
+            cx v[LB], m[KB];
+#pragma unroll
+            for (int j = 0; j < LB; ++j) v[j] = S[n * LSP + l0 + j];
+#pragma unroll
+            for (int q = 0; q < KB; ++q) m[q] = M[n * ND + k0 + q];
+#pragma unroll
+            for (int q = 0; q < KB; ++q)
+#pragma unroll
+              for (int j = 0; j < LB; ++j) {
+                ar[q][j] += m[q].re * v[j].re;
+                ai[q][j] += m[q].re * v[j].im;
+                if (!RM) {
+                  ar[q][j] -= m[q].im * v[j].im;
+                  ai[q][j] += m[q].im * v[j].re;
+                }
+              }
           }
-          S2[k * LSP + l] = mkcx(ar, ai);
+#pragma unroll
+          for (int q = 0; q < KB; ++q)
+#pragma unroll
+            for (int j = 0; j < LB; ++j) S2[(k0 + q) * LSP + l0 + j] = mkcx(ar[q][j], ai[q][j]);
         }
         __syncthreads();
         Rb = S2;

@@ -996,6 +996,11 @@ void build_source(xs_handle& h) {
     }
     for (int d = 0; d < 3; ++d) os << "#define XS_TL" << d + 1 << " " << tl[d] << "\n#define XS_LSP" << d + 1 << " " << lsp[d] << "\n";
     os << "#define XS_TILE_ELEMS " << elems << "\n#define XS_FFT_TILE_STAGES " << tstages << "\n";
+    for (int d = 0; d < 3; ++d) {  // real transform matrices: every field non-periodic along d
+      bool real_m = d < P.D;
+      for (int f = 0; f < P.F && real_m; ++f) real_m = P.type(d, f) != 0;
+      os << "#define XS_REALM" << d + 1 << " " << (real_m ? 1 : 0) << "\n";
+    }
   }
   os << fns.str();
   os << xs_kernel_source_resident << "\n";
@@ -1170,8 +1175,8 @@ const void* ensure_prop2(xs_handle& h, int nc);
 
 // Grid of a resident launch over nctas trajectory tiles.  With the field in
 // device memory the grid is persistent: one slice per CTA, as many CTAs as
-// are resident at once but no more slices than ~96 MB (L2-sized) unless that
-// would leave SMs idle.
+// are resident at once, but no more slices than ~96 MB (L2-sized) when at
+// least one slice per SM fits that budget.
 int resident_grid(xs_handle& h, CUfunction f, int nctas) {
   if (!h.rp.gfield) return nctas;
   int dev = 0, sms = 0, occ = 0;
@@ -1180,7 +1185,10 @@ int resident_grid(xs_handle& h, CUfunction f, int nctas) {
   cu_check(driver().occupancy(&occ, f, h.rp.threads, h.rp.smem), "occupancy");
   const size_t slice = (size_t)h.rp.narr * h.rp.G * h.P.F * h.P.NS * (h.fp64 ? 16 : 8);
   const int l2 = (int)std::max<size_t>(1, (96u << 20) / slice);
-  const int grid = std::max(1, std::min({nctas, sms * std::max(occ, 1), std::max(sms, l2)}));
+  // slices that fit L2 for a full wave: cap the grid there; larger slices stream from HBM anyway,
+  // so take every CTA the SMs can hold (latency hiding)
+  const int cap = l2 >= sms ? l2 : sms * std::max(occ, 1);
+  const int grid = std::max(1, std::min({nctas, sms * std::max(occ, 1), cap}));
   h.d_gfield.ensure((size_t)grid * slice);
   return grid;
 }
