@@ -339,7 +339,10 @@ def run_ours(args, rank, world, local_rank):
     stats = {kinds[i]: {"launches": int(kl[i]), "ms": float(kms[i])} for i in range(8) if kl[i]}
     dom = max(("x_step", "y_pass"), key=lambda k: stats.get(k, {"ms": 0})["ms"])
     per_launch_ms = stats[dom]["ms"] / stats[dom]["launches"]
-    alg_bytes = 2.0 * ntraj * p.fields * p.nspace * 8  # read + write of the FP32 complex field
+    # the blocks may run as two staggered groups (two launches per pass, each on half the trajectories)
+    groups = max(1, round(stats["x_step"]["launches"] / float(args.steps * steps_per_traj)))
+    traj_per_launch = ntraj / groups
+    alg_bytes = 2.0 * traj_per_launch * p.fields * p.nspace * 8  # read + write of the FP32 complex field
     achieved = alg_bytes / (per_launch_ms / 1000.0) / 1e9
     peak, kind = _peaks()
     tr = NCU_TRAFFIC_PER_TRAJ.get(dom)
@@ -358,8 +361,13 @@ def run_ours(args, rank, world, local_rank):
         "kernels": stats,
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": kind,
-                     "traffic": (tr * ntraj if tr else None),
-                     "algorithmic_bytes_per_launch": alg_bytes},
+                     "traffic": (tr * traj_per_launch if tr else None),
+                     "algorithmic_bytes_per_launch": alg_bytes, "trajectories_per_launch": traj_per_launch},
+        "step_roofline": {"bound": "hbm", "unit": "GB/s", "peak": peak,
+                          "achieved": value / world * 4.0 * p.fields * p.nspace * 8 / 1e9,
+                          "frac": value / world * 4.0 * p.fields * p.nspace * 8 / 1e9 / peak,
+                          "bytes_per_traj_step": 4.0 * p.fields * p.nspace * 8,
+                          "note": "whole MP step: two passes, each one read and one write of the field"},
         "cpu_baseline": {"value": cpu_val, "unit": "traj-steps/s", "cores": 1, "kind": "port", "sample": cpu_desc},
         "clocks": clocks,
         "fp64": fp64_line, "fp32_vs_fp64": fp32_err,

@@ -67,3 +67,35 @@ def test_stream_final_field_and_rectangular_lattice():
     av_g, a_g = _run(g, [0], 1, a_out=True)
     assert rel_err(a_g, b_o) < 1e-10
     assert rel_err(av_g[0][0], av_o[0]) < 1e-10
+
+
+@pytest.mark.parametrize("checks", [0, 1])
+def test_stream_512_trajectories_final_field_match_oracle(checks):
+    """512 trajectories in 2 blocks of 256 (the benchmark's block size) with
+    the final field requested: FP64 observables and fields agree with the
+    oracle for both blocks and both check passes."""
+    g, o = _case(checks, points=(3, 64, 64), ens=(256, 2, 1))
+    for nc in ([1, 2] if checks else [1]):
+        av_g, a_g = _run(g, [0, 1], nc, a_out=True)
+        for i, b in enumerate([0, 1]):
+            av_o, a_o = oracle_block_av(o, b, nc)
+            for k in range(len(av_o)):
+                e = rel_err(av_g[i][k].reshape(-1, order="F"), av_o[k].reshape(-1, order="F"))
+                assert e < 1e-10, (nc, b, k, e)
+            e = rel_err(a_g[..., 256 * i:256 * (i + 1)], a_o)
+            assert e < 1e-10, (nc, b, "field", e)
+
+
+def test_stream_nonseparable_linear_fp64():
+    """A linear operator with a kx^2 ky^2 cross term is not separable, so the
+    column pass reads the full [ky][kx] propagator table (the separable GPE
+    operator above uses two 1D tables); both agree with the oracle."""
+    g, o = _case(0, obs_int=False)
+    g = dict(g, linear="@(p) (1i+0.1)*(p.Dx.^2+p.Dy.^2) + 0.02i*p.Dx.^2.*p.Dy.^2")
+    o = dict(o, linear=lambda p: (1j + 0.1) * (p.Dx ** 2 + p.Dy ** 2) + 0.02j * p.Dx ** 2 * p.Dy ** 2)
+    av_g, _ = _run(g, [0, 1], 1)
+    for i, b in enumerate([0, 1]):
+        av_o, _ = oracle_block_av(o, b, 1)
+        for k in range(len(av_o)):
+            e = rel_err(av_g[i][k].reshape(-1, order="F"), av_o[k].reshape(-1, order="F"))
+            assert e < 1e-10, (b, k, e)

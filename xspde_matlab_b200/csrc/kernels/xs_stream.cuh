@@ -298,7 +298,7 @@ extern "C" __global__ void __launch_bounds__(256) xs_x_final(const XsStreamArgs 
 // (c = tid % TX, t = tid / TX) holds y = t + RY*j of column c.
 #define XS_SSMEM (XS_RY * XS_RY + XS_TX * XS_RY * XS_RY)
 
-extern "C" __global__ void __launch_bounds__(256) xs_s_pass(const XsStreamArgs A) {
+extern "C" __global__ void __launch_bounds__(256, 4) xs_s_pass(const XsStreamArgs A) {
   if ((size_t)blockIdx.x >= (size_t)A.ntraj * XS_F * (XS_NX / XS_TX)) {
     if (threadIdx.x == 0) atomicOr(A.status, 2);
     return;
@@ -321,10 +321,23 @@ extern "C" __global__ void __launch_bounds__(256) xs_s_pass(const XsStreamArgs A
   __syncthreads();  // twiddles ready
   XsBlockSync bs;
   xs_fft4<XS_RY, XS_TX, 0>(v, t, tw, buf, bs);
+#if XS_SEP
+  // separable L(kx, ky) = Lx(kx) + Ly(ky): exp(L dt) = ex[kx] * ey[ky] from two
+  // 1D FP64 tables [NX] + [NY] (L1-resident) instead of the [NY][NX] table
+  const double2* Pt = A.m == 2 ? A.prop2 : A.prop1;
+  const double2 ex = __ldg(&Pt[x0 + c]);
+  (void)f;
+#else
   const double2* P = (A.m == 2 ? A.prop2 : A.prop1) + (XS_PROP_COMPS > 1 ? (size_t)f * XS_NS : 0);
+#endif
 #pragma unroll
   for (int k = 0; k < XS_RY; ++k) {
+#if XS_SEP
+    const double2 ey = __ldg(&Pt[XS_NX + t + XS_RY * k]);
+    const double2 pr = make_double2(ey.x * ex.x - ey.y * ex.y, ey.x * ex.y + ey.y * ex.x);
+#else
     const double2 pr = __ldg(&P[(size_t)(t + XS_RY * k) * XS_NX + x0 + c]);
+#endif
     const double vr = (double)v[k].re, vi = (double)v[k].im;
     v[k] = mkcx((real)(vr * pr.x - vi * pr.y), (real)(vr * pr.y + vi * pr.x));
   }

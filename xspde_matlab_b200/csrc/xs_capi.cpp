@@ -653,6 +653,7 @@ struct xs_handle {
   StreamPlan sp;
   int path_kind = 0;
   int force_G = 0, force_threads = 0;  // resident tile fixed by the caller (uneven batch)
+  bool sep = false;                    // streaming: L(kx, ky) = Lx(kx) + Ly(ky), 1D propagator tables
   CUfunction f_batch = nullptr;
   cudaStream_t stream = nullptr;
   DevBuf d_prop[2], d_prop2[2], d_tmat, d_obs, d_av, d_ain, d_aout, d_status, d_w, d_field, d_redpart, d_pstep,
@@ -841,6 +842,21 @@ std::string gen_fft_stages(int D, int n, int sd) {
   return os.str();
 }
 
+// True when the 2D linear operator is additively separable, L(kx, ky) =
+// Lx(kx) + Ly(ky), to FP64 rounding (then exp(L dt) factors into 1D tables).
+bool separable(const Problem& P) {
+  if (P.D != 2 || P.Lc != 1 || !P.has_linear) return false;
+  const int N1 = P.N[0], N2 = P.N[1];
+  double mx = 0;
+  for (auto& v : P.L) mx = std::max(mx, std::abs(v));
+  for (int i2 = 0; i2 < N2; ++i2)
+    for (int i1 = 0; i1 < N1; ++i1) {
+      const cd d = P.L[(size_t)i2 * N1 + i1] - (P.L[i1] + P.L[(size_t)i2 * N1] - P.L[0]);
+      if (std::abs(d) > 1e-13 * mx + 1e-300) return false;
+    }
+  return true;
+}
+
 int isqrt_pow2(int n) {
   for (int r : {8, 16, 32})
     if (r * r == n) return r;
@@ -956,8 +972,10 @@ void build_source(xs_handle& h) {
     }
     h.kind = 2;
     plan_stream(h);
+    h.sep = separable(P);
     std::ostringstream os;
     emit_common_header(h, os);
+    os << "#define XS_SEP " << (h.sep ? 1 : 0) << "\n";
     os << "#define XS_FFT_RX " << h.sp.RX << "\n#define XS_FFT_RY " << h.sp.RY << "\n#define XS_OBS_ROWS " << h.sp.OROWS
        << "\n";
     os << fns.str();
@@ -1098,6 +1116,23 @@ double pass_dtr(const Problem& P, int nc) {
   return (P.p.checks && nc != 2) ? P.dt / (2.0 * P.p.steps) : P.dt / P.p.steps;  // xensemble.m:41-45
 }
 
+// exp(L dt) in the layout the kernels read: [Lc][NS] (xpropfactor.m:39), or,
+// for a separable streaming problem, ex[kx] = exp(L(kx, 0) dt) followed by
+// ey[ky] = exp((L(0, ky) - L(0, 0)) dt).
+std::vector<cd> prop_values(const xs_handle& h, double dt) {
+  const Problem& P = h.P;
+  if (h.kind == 2 && h.sep) {
+    const int N1 = P.N[0], N2 = P.N[1];
+    std::vector<cd> pr((size_t)N1 + N2);
+    for (int i1 = 0; i1 < N1; ++i1) pr[i1] = std::exp(P.L[i1] * dt);
+    for (int i2 = 0; i2 < N2; ++i2) pr[(size_t)N1 + i2] = std::exp((P.L[(size_t)i2 * N1] - P.L[0]) * dt);
+    return pr;
+  }
+  std::vector<cd> pr(P.L.size());
+  for (size_t i = 0; i < P.L.size(); ++i) pr[i] = std::exp(P.L[i] * dt);
+  return pr;
+}
+
 const void* ensure_prop(xs_handle& h, int nc) {
   const Problem& P = h.P;
   int slot = nc == 2 ? 1 : 0;
@@ -1108,8 +1143,7 @@ const void* ensure_prop(xs_handle& h, int nc) {
   }
   if (h.prop_dtr[slot] == dtr) return h.d_prop[slot].p;
   double dt = dtr / P.p.ipsteps;  // xpropfactor.m:28
-  std::vector<cd> pr(P.L.size());
-  for (size_t i = 0; i < P.L.size(); ++i) pr[i] = std::exp(P.L[i] * dt);  // xpropfactor.m:39
+  std::vector<cd> pr = prop_values(h, dt);
   h.d_prop[slot].ensure(pr.size() * 16);
   CUDA_CHECK(cudaMemcpy(h.d_prop[slot].p, pr.data(), pr.size() * 16, cudaMemcpyHostToDevice));
   h.prop_dtr[slot] = dtr;
@@ -1250,8 +1284,7 @@ const void* ensure_prop2(xs_handle& h, int nc) {
   ensure_prop(h, nc);
   double dt = 2.0 * pass_dtr(P, nc) / P.p.ipsteps;
   if (h.prop2_dtr[slot] == dt) return h.d_prop2[slot].p;
-  std::vector<cd> pr(P.L.size());
-  for (size_t i = 0; i < P.L.size(); ++i) pr[i] = std::exp(P.L[i] * dt);
+  std::vector<cd> pr = prop_values(h, dt);
   h.d_prop2[slot].ensure(std::max<size_t>(pr.size(), 1) * 16);
   CUDA_CHECK(cudaMemcpy(h.d_prop2[slot].p, pr.data(), pr.size() * 16, cudaMemcpyHostToDevice));
   h.prop2_dtr[slot] = dt;
