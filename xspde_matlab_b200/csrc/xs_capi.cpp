@@ -166,6 +166,12 @@ std::string nvrtc_compile(const std::string& src, const std::string& name, std::
   snprintf(hb, sizeof hb, "%016llx", (unsigned long long)fnv1a(key));
   std::string dir = cache_dir();
   std::string path = dir + "/" + name + "_" + hb + ".cubin";
+  if (const char* dd = getenv("XSPDE_B200_DUMP"))  // generated CUDA C++ source, for inspection
+    if (*dd) {
+      mkdirs(dd);
+      std::ofstream f(std::string(dd) + "/" + name + "_" + hb + ".cu");
+      f << src;
+    }
   {
     std::ifstream f(path, std::ios::binary);
     if (f) {

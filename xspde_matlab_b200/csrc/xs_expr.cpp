@@ -531,6 +531,7 @@ Vec eval(const NodeP& n, const EvalEnv& env) {
 struct Val {
   int len = 1;
   bool cplx = false;
+  bool imag = false;                    // purely imaginary: c[] are real expressions of the imaginary part
   bool spatial = false;                 // depends on the site (a, w, v, x, y, z)
   std::vector<std::string> c;           // per-component C expression (temp names / literals)
 };
@@ -565,12 +566,22 @@ struct Gen {
     return name;
   }
 
-  Val constant(const Vec& v) {
+  Val constant(const Vec& v, bool allow_imag = false) {
     Val r;
     r.len = (int)v.size();
     r.cplx = false;
     for (auto& z : v)
       if (z.imag() != 0) r.cplx = true;
+    if (allow_imag && r.cplx) {
+      bool pure = true;
+      for (auto& z : v) pure = pure && z.real() == 0;
+      if (pure) {  // e.g. 0.5i: kept as its imaginary part
+        r.cplx = false;
+        r.imag = true;
+        for (auto& z : v) r.c.push_back(lit(z.imag()));
+        return r;
+      }
+    }
     for (auto& z : v) r.c.push_back(r.cplx ? "mkcx(" + lit(z.real()) + "," + lit(z.imag()) + ")" : lit(z.real()));
     return r;
   }
@@ -682,9 +693,75 @@ struct Gen {
     return r;
   }
 
-  Val bin(const std::string& op, const Val& a, const Val& b, const NodeP& rnode) {
-    if (a.len != b.len && a.len != 1 && b.len != 1)
-      throw GrammarError("component count mismatch (" + std::to_string(a.len) + " vs " + std::to_string(b.len) + ") in '" + op + "'");
+  // A purely imaginary value as an ordinary complex one.
+  Val mat(const Val& v) {
+    if (!v.imag) return v;
+    Val r = v;
+    r.imag = false;
+    r.cplx = true;
+    for (auto& c : r.c) c = tmp(true, "mkcx((real)0, " + c + ")");
+    return r;
+  }
+
+  // + - * / with a purely imaginary operand (i b): the forms below are what the
+  // full complex arithmetic (prelude operators, Smith's division) computes for
+  // finite operands, without the products and sums with the zero real part.
+  bool imag_bin(const std::string& op, const Val& a, const Val& b, Val& r) {
+    const bool mul = op == "*" || op == ".*", dv = op == "/" || op == "./", add = op == "+", sub = op == "-";
+    if (!(mul || dv || add || sub)) return false;
+    if (mul && op == "*" && a.len > 1 && b.len > 1) return false;
+    auto kind = [](const Val& v) { return v.imag ? 'i' : (v.cplx ? 'c' : 'r'); };
+    const char ka = kind(a), kb = kind(b);
+    r.len = std::max(a.len, b.len);
+    r.spatial = a.spatial || b.spatial;
+    r.c.clear();
+    for (int i = 0; i < r.len; ++i) {
+      const std::string x = "(" + a.c[a.len == 1 ? 0 : i] + ")", y = "(" + b.c[b.len == 1 ? 0 : i] + ")";
+      char out;
+      std::string e;
+      if (ka == 'i' && kb == 'r') {
+        if (mul) { out = 'i'; e = x + " * " + y; }
+        else if (dv) { out = 'i'; e = x + " / " + y; }
+        else { out = 'c'; e = "mkcx(" + std::string(add ? "" : "-") + y + ", " + x + ")"; }
+      } else if (ka == 'r' && kb == 'i') {
+        if (mul) { out = 'i'; e = x + " * " + y; }
+        else if (dv) { out = 'i'; e = "-(" + x + " / " + y + ")"; }
+        else { out = 'c'; e = "mkcx(" + x + ", " + (add ? "" : "-") + y + ")"; }
+      } else if (ka == 'i' && kb == 'i') {
+        if (mul) { out = 'r'; e = "-(" + x + " * " + y + ")"; }
+        else if (dv) { out = 'r'; e = x + " / " + y; }
+        else { out = 'i'; e = x + (add ? " + " : " - ") + y; }
+      } else if (ka == 'i' && kb == 'c') {
+        if (mul) { out = 'c'; e = "mkcx(-(" + x + " * " + y + ".im), " + x + " * " + y + ".re)"; }
+        else if (dv) return false;
+        else if (add) { out = 'c'; e = "mkcx(" + y + ".re, " + x + " + " + y + ".im)"; }
+        else { out = 'c'; e = "mkcx(-" + y + ".re, " + x + " - " + y + ".im)"; }
+      } else if (ka == 'c' && kb == 'i') {
+        if (mul) { out = 'c'; e = "mkcx(-(" + x + ".im * " + y + "), " + x + ".re * " + y + ")"; }
+        else if (dv) { out = 'c'; e = "mkcx(" + x + ".im / " + y + ", -(" + x + ".re / " + y + "))"; }
+        else { out = 'c'; e = "mkcx(" + x + ".re, " + x + ".im " + (add ? "+ " : "- ") + y + ")"; }
+      } else {
+        return false;
+      }
+      if (i == 0) {
+        r.imag = out == 'i';
+        r.cplx = out == 'c';
+      } else if ((out == 'i') != r.imag || (out == 'c') != r.cplx) {
+        return false;
+      }
+      r.c.push_back(tmp(out == 'c', e));
+    }
+    return true;
+  }
+
+  Val bin(const std::string& op, const Val& a0, const Val& b0, const NodeP& rnode) {
+    if (a0.len != b0.len && a0.len != 1 && b0.len != 1)
+      throw GrammarError("component count mismatch (" + std::to_string(a0.len) + " vs " + std::to_string(b0.len) + ") in '" + op + "'");
+    if (a0.imag || b0.imag) {
+      Val ri;
+      if (imag_bin(op, a0, b0, ri)) return ri;
+    }
+    const Val a = mat(a0), b = mat(b0);
     if ((op == "*" || op == "/") && a.len > 1 && b.len > 1)
       throw GrammarError("matrix '" + op + "' between vectors; use '." + op + "'");
     Val r;
@@ -745,9 +822,12 @@ struct Gen {
     return true;
   }
 
-  Val gen(const NodeP& n) {
+  Val gen(const NodeP& n) { return mat(gen_raw(n)); }
+
+  // gen() that may return a purely imaginary value (consumed only by bin()).
+  Val gen_raw(const NodeP& n) {
     Vec cv;
-    if (n->kind != NK::Colon && try_const(n, cv)) return constant(cv);
+    if (n->kind != NK::Colon && try_const(n, cv)) return constant(cv, true);
     switch (n->kind) {
       case NK::Num: case NK::Imag: return constant(eval(n, EvalEnv{}));
       case NK::Var: return var(n->name);
@@ -791,7 +871,7 @@ struct Gen {
             return r;
           }
         }
-        return bin(n->name, gen(n->kids[0]), gen(n->kids[1]), n->kids[1]);
+        return bin(n->name, gen_raw(n->kids[0]), gen_raw(n->kids[1]), n->kids[1]);
       }
       case NK::Concat: {
         Val r;
