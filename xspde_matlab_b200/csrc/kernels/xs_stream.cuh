@@ -44,6 +44,8 @@ struct XsStreamArgs {
   double2* redpart;          // [ntraj][XS_NRG][XS_NRED] integrand sums per row group
   int* status;
   const double* params;      // runtime values of the named scalars p.<name>
+  const cx* tw_x;            // [RX*RX] four-step twiddles of the rows, built in FP64 on the host
+  const cx* tw_y;            // [RY*RY] four-step twiddles of the columns
 };
 
 #define XS_RX XS_FFT_RX
@@ -71,15 +73,11 @@ __device__ __forceinline__ bool xs_smem_ok(size_t need, int* status) {
 }
 
 // W_N^(t*k) for the four-step split, N = R*R: tw[k*R + t] = exp(-2 pi i t k / N)
-// (t fastest, so the threads of a line read consecutive words).
+// (t fastest, so the threads of a line read consecutive words), copied from
+// the host-built table (L2-resident) into the CTA's shared memory.
 template <int R>
-__device__ __forceinline__ void xs_fill_twiddles(cx* tw) {
-  for (int i = threadIdx.x; i < R * R; i += blockDim.x) {
-    const int k = i / R, t = i % R;
-    double s, c;
-    sincospi(-2.0 * (double)(t * k) / (double)(R * R), &s, &c);
-    tw[i] = mkcx((real)c, (real)s);
-  }
+__device__ __forceinline__ void xs_fill_twiddles(cx* tw, const cx* __restrict__ src) {
+  for (int i = threadIdx.x; i < R * R; i += blockDim.x) tw[i] = src[i];
 }
 
 // Forward DFT of N = R*R points held four-step style: thread t holds v[j] =
@@ -142,7 +140,7 @@ __device__ __forceinline__ void xs_xpass_body(const XsStreamArgs& A) {
   if (!xs_smem_ok(XS_XSMEM * sizeof(cx), A.status)) return;
   cx* smem = (cx*)xs_dsmem;
   cx* tw = smem;
-  xs_fill_twiddles<XS_RX>(tw);
+  xs_fill_twiddles<XS_RX>(tw, A.tw_x);
   __syncthreads();
   const int r = threadIdx.x / XS_RX, t = threadIdx.x % XS_RX;
   cx* buf = tw + XS_RX * XS_RX + r * XS_XLINE;
@@ -306,7 +304,7 @@ extern "C" __global__ void __launch_bounds__(256, 4) xs_s_pass(const XsStreamArg
   if (!xs_smem_ok(XS_SSMEM * sizeof(cx), A.status)) return;
   cx* smem = (cx*)xs_dsmem;
   cx* tw = smem;
-  xs_fill_twiddles<XS_RY>(tw);
+  xs_fill_twiddles<XS_RY>(tw, A.tw_y);
   const int c = threadIdx.x % XS_TX, t = threadIdx.x / XS_TX;
   cx* buf = tw + XS_RY * XS_RY + c;  // element (k, t) of column c at ((k*RY + t)*TX + c)
   constexpr int TILES = XS_NX / XS_TX;
@@ -360,7 +358,7 @@ extern "C" __global__ void __launch_bounds__(XS_OROWS * XS_RX) xs_x_obs(const Xs
   cx* smem = (cx*)xs_dsmem;
   __shared__ double wred[(XS_OROWS * XS_RX + 31) / 32][2 * (XS_NRED > 0 ? XS_NRED : 1)];
   cx* tw = smem;
-  xs_fill_twiddles<XS_RX>(tw);
+  xs_fill_twiddles<XS_RX>(tw, A.tw_x);
   __syncthreads();
   const int r = threadIdx.x / XS_RX, t = threadIdx.x % XS_RX;
   cx* buf = tw + XS_RX * XS_RX + r * XS_RX * (XS_RX + 1);

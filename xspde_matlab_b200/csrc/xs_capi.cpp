@@ -663,7 +663,7 @@ struct xs_handle {
   CUfunction f_batch = nullptr;
   cudaStream_t stream = nullptr;
   DevBuf d_prop[2], d_prop2[2], d_tmat, d_obs, d_av, d_ain, d_aout, d_status, d_w, d_field, d_redpart, d_pstep,
-      d_params, d_gfield;
+      d_params, d_gfield, d_twiddle;
   double pstep_dtr = -1;
   double prop_dtr[2] = {-1, -1}, prop2_dtr[2] = {-1, -1};
   // launch accounting (xs_kernel_stats)
@@ -1063,6 +1063,24 @@ void load_module(xs_handle& h) {
         cu_check(d.setattr(*f.f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, (int)f.smem), f.name);
     }
     CUDA_CHECK(cudaStreamCreateWithFlags(&h.stream, cudaStreamNonBlocking));
+    {  // four-step twiddles exp(-2 pi i t k / R^2), [k][t], rows then columns
+      std::vector<double> tw;
+      for (int R : {h.sp.RX, h.sp.RY})
+        for (int k = 0; k < R; ++k)
+          for (int t = 0; t < R; ++t) {
+            const double ang = -2.0 * M_PI * (double)(t * k) / (double)(R * R);
+            tw.push_back(std::cos(ang));
+            tw.push_back(std::sin(ang));
+          }
+      if (h.fp64) {
+        h.d_twiddle.ensure(tw.size() * 8);
+        CUDA_CHECK(cudaMemcpy(h.d_twiddle.p, tw.data(), tw.size() * 8, cudaMemcpyHostToDevice));
+      } else {
+        std::vector<float> tf(tw.begin(), tw.end());
+        h.d_twiddle.ensure(tf.size() * 4);
+        CUDA_CHECK(cudaMemcpy(h.d_twiddle.p, tf.data(), tf.size() * 4, cudaMemcpyHostToDevice));
+      }
+    }
     h.d_status.ensure(sizeof(int));
     h.loaded = true;
     return;
@@ -1311,6 +1329,8 @@ struct StreamArgsHost {
   void* redpart;
   int* status;
   const double* params;
+  const void* tw_x;
+  const void* tw_y;
 };
 
 // Streaming schedule of one xpath call (Simulator/xpath.m:137-194) for MP:
@@ -1347,6 +1367,8 @@ void launch_stream(xs_handle& h, int first_block, int nblocks, int nc, const voi
   a.redpart = h.d_redpart.p;
   a.status = (int*)h.d_status.p;
   a.params = (const double*)h.d_params.p;
+  a.tw_x = h.d_twiddle.p;
+  a.tw_y = (const char*)h.d_twiddle.p + (size_t)sp.RX * sp.RX * cxs;
   void* params[] = {&a};
   const unsigned xgrid = (unsigned)((size_t)total * P.N[1] / sp.XROWS);
   const unsigned sgrid = (unsigned)((size_t)total * P.F * (P.N[0] / sp.TX));
