@@ -421,6 +421,10 @@ def _cv_solve(path, first, nb, feats=False):
 def run_cv(args):
     import numpy as np
     import torch
+    global CV_SETS, CV_FEATURES
+    if args.cv_sets:
+        CV_SETS = tuple((tuple(r), dw, nt, gap) for r, dw, nt, gap in json.loads(args.cv_sets))
+        CV_FEATURES = sum(2 * nt * r[4] * r[5] for r, dw, nt, gap in CV_SETS)
     from xspde_matlab_b200.cv import ControlVariateNet, block_sampling_error, two_level
     target = 1e-3
     nblk = 16
@@ -442,12 +446,15 @@ def run_cv(args):
     A = torch.cat([X_tr.double(), torch.ones(ntrain, 1, dtype=torch.float64, device="cuda")], 1)
     coef = torch.linalg.solve(A.T @ A, A.T @ f_tr.double().unsqueeze(1))[:, 0]
 
-    def g_lin(X):
-        return X.double() @ coef[:-1] + coef[-1]
+    w32, b0 = coef[:-1].float(), float(coef[-1])
+
+    def g_lin(X):  # the same function for the solver's inputs and the fresh ones (FP32 dot, FP64 sum)
+        return (X @ w32).double() + b0
     net = ControlVariateNet(CV_FEATURES, 256, seed=0)
     r_tr = (f_tr.double() - g_lin(X_tr)).float()
     r_va = f_va.double() - g_lin(X_va)
-    best = (float(r_va.var()), None)  # the linear fit alone
+    var_lin = float(r_va.var())
+    best = (var_lin, None)  # the linear fit alone
     for ep in range(20):
         net.fit(X_tr, r_tr, epochs=1, batch=1024, lr=3e-4 if ep > 9 else 1e-3, seed=ep, weight_decay=1e-2)
         v = float((r_va - net.predict(X_va)).var())
@@ -469,26 +476,40 @@ def run_cv(args):
     # plain FP64 estimator at the N that reaches the target (pilot variance)
     n_plain = nblk * max(2, math.ceil(var_plain / (target * mu) ** 2 / nblk))
     p64 = _cv_path("fp64", n_plain)
-    _cv_solve(p64, 1 << 20, nblk)  # compile and warm the FP64 kernels
+    _cv_solve(p64, 1 << 19, n_plain)  # compile and warm the FP64 kernels and buffers at the timed size
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     f64, _ = _cv_solve(p64, 1 << 20, n_plain)
     est_plain, err_plain = block_sampling_error(f64.cpu().numpy(), nblk)
     t_plain = time.perf_counter() - t0
     # FP32 + learned control variate at its own N, fresh trajectories and fresh network inputs
+    from xspde_matlab_b200.cv import fresh_moments
     n_cv = nblk * max(2, math.ceil(var_cv / (target * mu) ** 2 / nblk))
     m_fresh = 1 << 20
     pcv = _cv_path("fp32", n_cv)
-    _cv_solve(pcv, 1 << 21, nblk, feats=True)
+    _, Xw = _cv_solve(pcv, 1 << 22, n_cv, feats=True)  # warm at the timed size
+    g(Xw)
+    gen = torch.Generator(device="cuda").manual_seed(777)
+    fresh_moments(g(torch.randn((m_fresh, CV_FEATURES), device="cuda", generator=gen)))
     gen = torch.Generator(device="cuda").manual_seed(12345)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     f32, Xc = _cv_solve(pcv, 1 << 21, n_cv, feats=True)
+    t1 = time.perf_counter()
     gx = g(Xc)
     Xf = torch.randn((m_fresh, CV_FEATURES), device="cuda", generator=gen)
-    gf = g(Xf)
-    est_cv, err_cv = two_level(f32.cpu().numpy(), gx.cpu().numpy(), gf.cpu().numpy(), nblk)
+    mom = fresh_moments(g(Xf))
+    t2 = time.perf_counter()
+    est_cv, err_cv = two_level(f32.cpu().numpy(), gx.cpu().numpy(), mom, nblk)
     t_cv = time.perf_counter() - t0
+    t_parts = {"solve_and_features": t1 - t0, "fresh_network_inputs": t2 - t1, "estimate": t_cv - (t2 - t0)}
+    # cost of the network on the 2^20 fresh inputs (BF16 tensor-core forward), whether or not it is used
+    net.predict(Xf)
+    torch.cuda.synchronize()
+    tm0 = time.perf_counter()
+    net.predict(Xf)
+    torch.cuda.synchronize()
+    t_mlp = time.perf_counter() - tm0
     # FP32 trajectories against FP64 ones on identical noise (the FP64-oracle error of the FP32 path)
     ncmp = min(256, n_cv)
     p64b = _cv_path("fp64", ncmp)
@@ -500,9 +521,11 @@ def run_cv(args):
         "plain_fp64": {"seconds": t_plain, "trajectories": n_plain, "estimate": est_plain,
                        "rel_sampling_error": err_plain / est_plain},
         "fp32_cv": {"seconds": t_cv, "trajectories": n_cv, "fresh_network_inputs": m_fresh, "estimate": est_cv,
-                    "rel_sampling_error": err_cv / est_cv, "mlp_used": use_mlp},
+                    "rel_sampling_error": err_cv / est_cv, "mlp_used": use_mlp, "seconds_by_phase": t_parts,
+                    "mlp_forward_2p20_seconds": t_mlp},
         "speedup_vs_plain_fp64": t_plain / t_cv,
-        "variance_ratio": {"linear+mlp": var_plain / var_cv, "plain_var": var_plain, "cv_var": var_cv},
+        "variance_ratio": {"used": var_plain / var_cv, "linear_only": var_plain / var_lin,
+                           "linear_plus_mlp_best": var_plain / best[0], "plain_var": var_plain, "cv_var": var_cv},
         "estimates_agree_sigma": abs(est_cv - est_plain) / math.sqrt(err_cv ** 2 + err_plain ** 2),
         "fp32_vs_fp64_traj_max_rel": d32,
         "training": {"pairs": ntrain, "data_seconds": t_data, "fit_seconds": t_fit,
@@ -728,6 +751,7 @@ def main():
     ap.add_argument("--quick", action="store_true", help="device timing only (no e2e, no CPU sample)")
     ap.add_argument("--cv", action="store_true", help="second headline: time to 1e-3 sampling error, "
                                                       "plain FP64 vs FP32 + learned control variate")
+    ap.add_argument("--cv-sets", default="", help="JSON list of noise-feature sets [[region6], steps, windows, gap]")
     ap.add_argument("--batch", action="store_true", help="uneven batch of independent problems, one graph launch")
     ap.add_argument("--batch-items", type=int, default=512)
     ap.add_argument("--dpo", action="store_true", help="positive-P DPO, 10^6 trajectories x 2000 steps")

@@ -117,10 +117,21 @@ def block_sampling_error(values, nblocks):
 
 def two_level(f, g_x, g_fresh, nblocks):
     """Two-level estimate mean(f - g(x)) + mean(g(x')) and its sampling error
-    (block estimate of the first term combined with the error of the second)."""
+    (block estimate of the first term combined with the error of the second).
+    g_fresh is the array g(x') or its moments (mean, standard deviation, count)."""
     d = np.asarray(f, dtype=np.float64) - np.asarray(g_x, dtype=np.float64)
     m1, e1 = block_sampling_error(d, nblocks)
-    gf = np.asarray(g_fresh, dtype=np.float64)
-    m2 = float(gf.mean())
-    e2 = float(gf.std(ddof=1) / math.sqrt(gf.size))
+    if isinstance(g_fresh, tuple):
+        m2, sd, n = g_fresh
+        e2 = sd / math.sqrt(n)
+    else:
+        gf = np.asarray(g_fresh, dtype=np.float64)
+        m2 = float(gf.mean())
+        e2 = float(gf.std(ddof=1) / math.sqrt(gf.size))
     return m1 + m2, math.sqrt(e1 ** 2 + e2 ** 2)
+
+
+def fresh_moments(g_fresh):
+    """(mean, standard deviation, count) of a device tensor g(x'), reduced on the device."""
+    gd = g_fresh.double()
+    return float(gd.mean()), float(gd.std()), int(gd.numel())
