@@ -686,7 +686,7 @@ def run_ac3d(args):
             "cpu_baseline": {"value": cpu, "unit": "traj-steps/s", "cores": 1, "kind": "port",
                              "sample": "1 trajectory x %d MP steps (FP64 NumPy oracle)" % n},
             "clocks": clk.summary(),
-            "config": {"workload": "ac_3d: 64^3, x Dirichlet (DST-I), y Neumann (DCT-I), z Dirichlet-Neumann, "
+            "config": {"workload": "ac_3d: 64^3, x Neumann (DCT-I), y Dirichlet (DST-I), z Neumann-Dirichlet (DCT-III/II), "
                                    "%d trajectories (%d blocks), 6 points x 20 steps = 99 MP steps" % (ntraj, nb)}}
     print(json.dumps(line))
 

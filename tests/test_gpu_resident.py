@@ -154,8 +154,9 @@ def test_field_in_device_memory_2d_periodic_fp64():
 
 
 def test_field_in_device_memory_3d_dst_dct_fp64():
-    """3D lattice with Dirichlet (DST-I), Neumann (DCT-I) and mixed (DST-III/II)
-    boundaries, too large for shared memory; Allen-Cahn drift with noise."""
+    """3D lattice with Neumann (DCT-I), Dirichlet (DST-I) and mixed
+    Neumann-Dirichlet (DCT-III/II) boundaries, too large for shared memory;
+    Allen-Cahn drift with noise."""
     base = dict(dimensions=4, points=[3, 24, 20, 16], ranges=[0.1, 6.0, 5.0, 4.0], steps=2, ensembles=[2, 2, 1],
                 noises=1, inrandoms=1, method="MP", checks=1, boundaries=[None, [[-1, -1]], [[1, 1]], [[-1, 1]]])
     g = dict(base, deriv="@(a,w,p) a - a.^3 + 0.1*w(1,:)", initial="@(v,p) 0.3*v(1,:) + 0.5",

@@ -14,8 +14,9 @@ dpo_0d: positive-P degenerate parametric oscillator, two complex fields
   the correction -1/2 B dB/dalpha = +chi alpha / 2 (the Ito form is the one
   Euler takes).  alpha = beta = 1 at t = 0; 2000 steps to t = 10.
 ac_3d: 3D stochastic Allen-Cahn on 64^3 over [-10,10]^3, da/dt = 0.05 lap a +
-  a - a^3 + 0.1 w, Dirichlet (DST-I) boundaries in x, Neumann (DCT-I) in y,
-  Dirichlet-Neumann (DST-III/II) in z, a0 = 0.1 v, FP32 fields, 256
+  a - a^3 + 0.1 w, Neumann (DCT-I) boundaries in x, Dirichlet (DST-I) in y,
+  Neumann at z_min / Dirichlet at z_max (DCT-III/II) in z (xSPDE's flags: 1
+  Dirichlet, -1 Neumann), a0 = 0.1 v, FP32 fields, 256
   trajectories in 8 blocks, 100 MP steps to t = 1 (6 output points).
 xi is complex white noise (w1 + i w2)/sqrt(2).
 """
