@@ -99,3 +99,20 @@ def test_stream_nonseparable_linear_fp64():
         for k in range(len(av_o)):
             e = rel_err(av_g[i][k].reshape(-1, order="F"), av_o[k].reshape(-1, order="F"))
             assert e < 1e-10, (b, k, e)
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp64"])
+def test_stream_tma_column_pass_bit_identical(precision, monkeypatch):
+    """The column pass fed by TMA bulk tensor copies (XSPDE_B200_TMA=1, NY <= 256)
+    and the plain one (default) do the same arithmetic: identical bits."""
+    from xspde_matlab_b200 import GpuPath, xpreferences
+    g, _ = _case(0, precision=precision, ens=(32, 2, 1))
+    p = xpreferences([g])[0]
+    monkeypatch.delenv("XSPDE_B200_TMA", raising=False)
+    av_plain, a_plain = GpuPath(p, path_kind=2).run_path(0, 2, 1, a_out=True)
+    monkeypatch.setenv("XSPDE_B200_TMA", "1")
+    av_tma, a_tma = GpuPath(p, path_kind=2).run_path(0, 2, 1, a_out=True)
+    assert np.array_equal(a_plain, a_tma)
+    for b in range(2):
+        for k in range(len(av_plain[b])):
+            assert np.array_equal(av_plain[b][k], av_tma[b][k]), (b, k)

@@ -296,27 +296,9 @@ extern "C" __global__ void __launch_bounds__(256) xs_x_final(const XsStreamArgs 
 // (c = tid % TX, t = tid / TX) holds y = t + RY*j of column c.
 #define XS_SSMEM (XS_RY * XS_RY + XS_TX * XS_RY * XS_RY)
 
-extern "C" __global__ void __launch_bounds__(256, 4) xs_s_pass(const XsStreamArgs A) {
-  if ((size_t)blockIdx.x >= (size_t)A.ntraj * XS_F * (XS_NX / XS_TX)) {
-    if (threadIdx.x == 0) atomicOr(A.status, 2);
-    return;
-  }
-  if (!xs_smem_ok(XS_SSMEM * sizeof(cx), A.status)) return;
-  cx* smem = (cx*)xs_dsmem;
-  cx* tw = smem;
-  xs_fill_twiddles<XS_RY>(tw, A.tw_y);
-  const int c = threadIdx.x % XS_TX, t = threadIdx.x / XS_TX;
-  cx* buf = tw + XS_RY * XS_RY + c;  // element (k, t) of column c at ((k*RY + t)*TX + c)
-  constexpr int TILES = XS_NX / XS_TX;
-  const size_t tile = blockIdx.x;  // over ntraj * F * TILES
-  const int x0 = (int)(tile % TILES) * XS_TX;
-  const size_t ef = tile / TILES;  // e * F + f
-  const int f = (int)(ef % XS_F);
-  cx* base = A.field + ef * XS_NS + x0 + c;
-  cx v[XS_RY];
-#pragma unroll
-  for (int j = 0; j < XS_RY; ++j) v[j] = base[(size_t)(t + XS_RY * j) * XS_NX];
-  __syncthreads();  // twiddles ready
+// FFT_y, x exp(L dt)^m, IFFT_y of one tile column held four-step style in v.
+__device__ __forceinline__ void xs_col_tile(cx (&v)[XS_RY], int t, int c, int x0, int f, const cx* tw, cx* buf,
+                                            const XsStreamArgs& A) {
   XsBlockSync bs;
   xs_fft4<XS_RY, XS_TX, 0>(v, t, tw, buf, bs);
 #if XS_SEP
@@ -340,8 +322,128 @@ extern "C" __global__ void __launch_bounds__(256, 4) xs_s_pass(const XsStreamArg
     v[k] = mkcx((real)(vr * pr.x - vi * pr.y), (real)(vr * pr.y + vi * pr.x));
   }
   xs_ifft4<XS_RY, XS_TX, 0>(v, t, tw, buf, bs);
+}
+
+extern "C" __global__ void __launch_bounds__(256, 4) xs_s_pass(const XsStreamArgs A) {
+  if ((size_t)blockIdx.x >= (size_t)A.ntraj * XS_F * (XS_NX / XS_TX)) {
+    if (threadIdx.x == 0) atomicOr(A.status, 2);
+    return;
+  }
+  if (!xs_smem_ok(XS_SSMEM * sizeof(cx), A.status)) return;
+  cx* smem = (cx*)xs_dsmem;
+  cx* tw = smem;
+  xs_fill_twiddles<XS_RY>(tw, A.tw_y);
+  const int c = threadIdx.x % XS_TX, t = threadIdx.x / XS_TX;
+  cx* buf = tw + XS_RY * XS_RY + c;  // element (k, t) of column c at ((k*RY + t)*TX + c)
+  constexpr int TILES = XS_NX / XS_TX;
+  const size_t tile = blockIdx.x;  // over ntraj * F * TILES
+  const int x0 = (int)(tile % TILES) * XS_TX;
+  const size_t ef = tile / TILES;  // e * F + f
+  cx* base = A.field + ef * XS_NS + x0 + c;
+  cx v[XS_RY];
+#pragma unroll
+  for (int j = 0; j < XS_RY; ++j) v[j] = base[(size_t)(t + XS_RY * j) * XS_NX];
+  __syncthreads();  // twiddles ready
+  xs_col_tile(v, t, c, x0, (int)(ef % XS_F), tw, buf, A);
 #pragma unroll
   for (int j = 0; j < XS_RY; ++j) base[(size_t)(t + XS_RY * j) * XS_NX] = v[j];
+}
+
+// ---- column pass fed by the Tensor Memory Accelerator ---------------------------
+// Persistent CTAs walk the tiles (TX columns x NY rows of one trajectory and
+// component) with stride gridDim.x.  Thread 0 issues one 2D bulk tensor copy
+// per tile (cp.async.bulk.tensor, box 2*TX reals x NY rows of the field viewed
+// as [rows][2*NX] reals) into one of two shared-memory stages, completing on
+// that stage's mbarrier; the tile after next is requested as soon as a stage
+// has been read into registers, so HBM reads overlap the FFTs.  Results are
+// stored straight from registers (128-byte row segments).  Arithmetic is that
+// of xs_s_pass.  Every wait is bounded: on a timeout the CTA sets status bit 3,
+// waits (bounded) for its copies in flight and returns.
+struct __align__(64) XsTmap {
+  unsigned long long w[16];
+};
+
+__device__ __forceinline__ u32 xs_smem_u32(const void* p) { return (u32)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ bool xs_mbar_wait(u32 bar, u32 parity) {
+  for (int it = 0; it < (1 << 22); ++it) {
+    u32 ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void xs_tma_load_2d(const XsTmap* tm, u32 dst, u32 bar, int x, int y, u32 bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+          dst),
+      "l"((unsigned long long)tm), "r"(x), "r"(y), "r"(bar)
+      : "memory");
+}
+
+#define XS_STAGE_ELEMS (XS_NY * XS_TX)
+#define XS_TSMEM_BYTES (2 * XS_STAGE_ELEMS * sizeof(cx) + XS_RY * XS_RY * sizeof(cx) + 16 + 128)
+
+extern "C" __global__ void __launch_bounds__(256) xs_s_pass_tma(const XsStreamArgs A, const __grid_constant__ XsTmap tmap) {
+  constexpr int TILES = XS_NX / XS_TX;
+  const int ntiles = A.ntraj * XS_F * TILES;
+  if (!xs_smem_ok(XS_TSMEM_BYTES, A.status)) return;
+  unsigned char* base = (unsigned char*)(((size_t)xs_dsmem + 127) & ~(size_t)127);
+  cx* stage = (cx*)base;                 // [2][NY][TX] (row-major tiles as the copies deliver them)
+  cx* tw = stage + 2 * XS_STAGE_ELEMS;   // [RY*RY] twiddles
+  const int c = threadIdx.x % XS_TX, t = threadIdx.x / XS_TX;
+  unsigned long long* bars = (unsigned long long*)(tw + XS_RY * XS_RY);
+  const u32 bar0 = xs_smem_u32(&bars[0]);  // stage s completes on bar0 + 8 s
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar0) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar0 + 8u) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  xs_fill_twiddles<XS_RY>(tw, A.tw_y);
+  __syncthreads();
+  const u32 bytes = (u32)(XS_STAGE_ELEMS * sizeof(cx));
+  auto issue = [&](int tile, int sidx) {
+    const int x0 = (tile % TILES) * XS_TX, ef = tile / TILES;
+    xs_tma_load_2d(&tmap, xs_smem_u32(stage + sidx * XS_STAGE_ELEMS), bar0 + 8u * sidx, 2 * x0, ef * XS_NY, bytes);
+  };
+  if (threadIdx.x == 0) {
+    if ((int)blockIdx.x < ntiles) issue(blockIdx.x, 0);
+    if ((int)(blockIdx.x + gridDim.x) < ntiles) issue(blockIdx.x + gridDim.x, 1);
+  }
+  int i = 0;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++i) {
+    const int sidx = i & 1;
+    const bool ok = xs_mbar_wait(bar0 + 8u * sidx, (u32)((i >> 1) & 1));
+    if (__syncthreads_or(!ok)) {
+      if (threadIdx.x == 0) {
+        atomicOr(A.status, 8);
+        xs_mbar_wait(bar0 + 8u * sidx, (u32)((i >> 1) & 1));
+        if (tile + (int)gridDim.x < ntiles) xs_mbar_wait(bar0 + 8u * (sidx ^ 1), (u32)(((i + 1) >> 1) & 1));
+      }
+      return;
+    }
+    cx v[XS_RY];
+    cx* st = stage + sidx * XS_STAGE_ELEMS;
+#pragma unroll
+    for (int j = 0; j < XS_RY; ++j) v[j] = st[(t + XS_RY * j) * XS_TX + c];
+    __syncthreads();  // stage sidx fully read: it becomes this tile's transpose scratch
+    const int x0 = (tile % TILES) * XS_TX, ef = tile / TILES;
+    xs_col_tile(v, t, c, x0, ef % XS_F, tw, st + c, A);
+    cx* gb = A.field + (size_t)ef * XS_NS + x0 + c;
+#pragma unroll
+    for (int j = 0; j < XS_RY; ++j) gb[(size_t)(t + XS_RY * j) * XS_NX] = v[j];
+    // the FFTs end with a barrier, so the scratch is free: refill it with the tile after next
+    if (threadIdx.x == 0 && tile + 2 * (int)gridDim.x < ntiles) {
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      issue(tile + 2 * gridDim.x, sidx);
+    }
+  }
 }
 
 // ---- observation pass ---------------------------------------------------------
