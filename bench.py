@@ -581,8 +581,7 @@ def run_batch(args):
         "unit": "traj-steps/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "dtype": "f32 fields, f64 tables and moments", "data": "synthetic",
         "site_steps_per_s": sites / (ms * 1e-3), "items": summ["items"], "skipped_items": len(b.skipped),
-        "skipped_reason": "2D 128x128 lattices: no device path yet (neither shared memory nor the 64/256/1024 "
-                          "streaming FFT covers them)",
+        "skipped_reason": "the library rejected these inputs (xs_batch_create)" if b.skipped else None,
         "variants": summ["variants"], "streaming_items": summ["streaming"], "launches_per_step": summ["launches"],
         "stream_traj_step_share": ts_stream / ts, "tiles": tiles,
         "host_seconds": {"create": t_create, "tune": t_tune, "first_run_with_compile_and_capture": t_first},

@@ -166,3 +166,29 @@ def test_field_in_device_memory_3d_dst_dct_fp64():
              linear=lambda p: 0.05 * (p.Dx ** 2 + p.Dy ** 2 + p.Dz ** 2),
              observe=[lambda a, p: abs(a) ** 2, lambda a, p: X.Int(np.real(a) ** 2, p)])
     _compare(g, o, [0, 1], [1, 2], FP64_TOL)
+
+
+def test_two_fields_a_in_a_out_fp64():
+    """Two-component field through the host layout a(fields, ens): initial field
+    in, final field and block means out (device-side reordering both ways)."""
+    base = dict(dimensions=1, fields=2, noises=2, points=[4], ranges=[0.5], steps=5, ensembles=[16, 1, 1],
+                method="MP", checks=0)
+    g = dict(base, params={"gam": 1.0, "eps": 1.2, "chi": 1e-3},
+             deriv="@(a,w,p) [-p.gam*a(1,:)+p.eps*a(2,:)-p.chi*a(1,:).^2.*a(2,:)+sqrt(-p.chi*a(1,:).^2).*w(1,:);"
+                   " -p.gam*a(2,:)+p.eps*a(1,:)-p.chi*a(2,:).^2.*a(1,:)+sqrt(-p.chi*a(2,:).^2).*w(2,:)]",
+             initial="@(v,p) [1+0*v(1,:); 1+0*v(2,:)]", observe=["@(a,p) real(a(1,:).*a(2,:))", "@(a,p) a"])
+    gam, eps, chi = 1.0, 1.2, 1e-3
+
+    def deriv(a, w, p):
+        a1, a2 = a[0:1], a[1:2]
+        return np.concatenate([-gam * a1 + eps * a2 - chi * a1 ** 2 * a2 + np.sqrt(-chi * a1 ** 2 + 0j) * w[0:1],
+                               -gam * a2 + eps * a1 - chi * a2 ** 2 * a1 + np.sqrt(-chi * a2 ** 2 + 0j) * w[1:2]])
+    rng = np.random.default_rng(3)
+    a0 = np.asfortranarray(rng.normal(size=(2, 16)) + 1j * rng.normal(size=(2, 16)))
+    o = dict(base, deriv=deriv, initial=lambda v, p: a0, observe=[lambda a, p: np.real(a[0:1] * a[1:2]),
+                                                                   lambda a, p: a])
+    av_o, b_o = oracle_block_av(o, 0, 1)
+    av_g, a_g = _gpu(g, [0], 1, a_in=a0, a_out=True)
+    assert rel_err(a_g, b_o) < FP64_TOL
+    for k in range(2):
+        assert rel_err(av_g[0][k].reshape(-1, order="F"), av_o[k].reshape(-1, order="F")) < FP64_TOL

@@ -3,6 +3,8 @@
 // device layout.  Problem kernels are generated and compiled by NVRTC.
 #include <cuda_runtime.h>
 
+#include "xs_aot.hpp"
+
 // [F, NS, E] (MATLAB, field fastest) <-> [E][F][NS] (device), complex FP64.
 extern "C" __global__ void xs_aot_reorder(const double2* __restrict__ src, double2* __restrict__ dst, int F, int NS,
                                           long long E, int to_device) {
@@ -24,5 +26,35 @@ extern "C" int xs_aot_reorder_launch(const void* src, void* dst, int F, int NS, 
   if (blocks > 148 * 32) blocks = 148 * 32;
   if (blocks < 1) blocks = 1;
   xs_aot_reorder<<<blocks, 256, 0, st>>>((const double2*)src, (double2*)dst, F, NS, E, to_device);
+  return (int)cudaGetLastError();
+}
+
+// Block means into MATLAB's av{o}(lines, time, space) order, one block after
+// another: output element (b, o, l, n, s) <- device [b][n][k], k the line's
+// site row (site observables) or its scalar slot.  Writes are contiguous.
+extern "C" __global__ void xs_aot_av_matlab(const double2* __restrict__ src, double2* __restrict__ dst, const XsAvMap m,
+                                            int nblocks) {
+  const long long total = (long long)nblocks * m.per_block;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
+    const long long b = i / m.per_block, r = i % m.per_block;
+    int o = 0;
+    while (o + 1 < m.nobs && r >= m.o_off[o + 1]) ++o;
+    const long long idx = r - m.o_off[o];
+    const int l = (int)(idx % m.lines[o]);
+    const long long q = idx / m.lines[o];
+    const int n = (int)(q % m.npts);
+    const long long s = q / m.npts;
+    const long long k = m.spatial[o] ? (long long)(m.out_off[o] + l) * m.NS + s
+                                     : (long long)m.nout_site * m.NS + m.out_off[o] + l;
+    dst[i] = src[(b * m.npts + n) * m.stride + k];
+  }
+}
+
+extern "C" int xs_aot_av_matlab_launch(const void* src, void* dst, const XsAvMap* m, int nblocks, cudaStream_t st) {
+  const long long total = (long long)nblocks * m->per_block;
+  long long blocks = (total + 255) / 256;
+  if (blocks > 148 * 32) blocks = 148 * 32;
+  if (blocks < 1) blocks = 1;
+  xs_aot_av_matlab<<<(unsigned)blocks, 256, 0, st>>>((const double2*)src, (double2*)dst, *m, nblocks);
   return (int)cudaGetLastError();
 }

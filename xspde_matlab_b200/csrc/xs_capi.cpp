@@ -30,6 +30,7 @@
 #include "xs_expr.hpp"
 #include "xs_noalloc.hpp"
 #include "xs_mlp.hpp"
+#include "xs_aot.hpp"
 
 extern const char* xs_kernel_source_prelude;
 extern const char* xs_kernel_source_noise;
@@ -675,7 +676,7 @@ struct xs_handle {
   CUfunction f_batch = nullptr;
   cudaStream_t stream = nullptr;
   DevBuf d_prop[2], d_prop2[2], d_tmat, d_obs, d_av, d_ain, d_aout, d_status, d_w, d_field, d_redpart, d_pstep,
-      d_params, d_gfield, d_twiddle;
+      d_params, d_gfield, d_twiddle, d_tmp, d_avm;
   double pstep_dtr = -1;
   double prop_dtr[2] = {-1, -1}, prop2_dtr[2] = {-1, -1};
   // launch accounting (xs_kernel_stats)
@@ -1597,16 +1598,11 @@ XS_API xs_status xs_run_path(xs_handle* h, int first_block, int nblocks, int nc,
       h->d_ain.ensure(fbytes);
       if (P.F == 1) {
         CUDA_CHECK(cudaMemcpyAsync(h->d_ain.p, a_in, fbytes, cudaMemcpyHostToDevice, h->stream));
-      } else {
-        std::vector<double> tmp(ntraj * P.F * P.NS * 2);
-        for (size_t e = 0; e < ntraj; ++e)
-          for (int f = 0; f < P.F; ++f)
-            for (int s = 0; s < P.NS; ++s) {
-              size_t src = (f + (size_t)P.F * (s + (size_t)P.NS * e)) * 2, dst = ((e * P.F + f) * P.NS + s) * 2;
-              tmp[dst] = a_in[src];
-              tmp[dst + 1] = a_in[src + 1];
-            }
-        CUDA_CHECK(cudaMemcpy(h->d_ain.p, tmp.data(), fbytes, cudaMemcpyHostToDevice));
+      } else {  // reorder on the device
+        h->d_tmp.ensure(fbytes);
+        CUDA_CHECK(cudaMemcpyAsync(h->d_tmp.p, a_in, fbytes, cudaMemcpyHostToDevice, h->stream));
+        CUDA_CHECK((cudaError_t)xs_aot_reorder_launch(h->d_tmp.p, h->d_ain.p, P.F, P.NS, (long long)ntraj, 1,
+                                                      h->stream));
       }
       din = h->d_ain.p;
     }
@@ -1620,29 +1616,49 @@ XS_API xs_status xs_run_path(xs_handle* h, int first_block, int nblocks, int nc,
     CUDA_CHECK(cudaMemsetAsync(h->d_status.p, 0, sizeof(int), h->stream));
     if (h->kind == 2) launch_stream(*h, first_block, nblocks, nc, din, h->d_av.p, dout, h->stream);
     else launch_resident(*h, first_block, nblocks, nc, din, h->d_av.p, dout, h->stream);
-    std::vector<double> av(avd);
-    if (avd) CUDA_CHECK(cudaMemcpyAsync(av.data(), h->d_av.p, avd * 8, cudaMemcpyDeviceToHost, h->stream));
+    // block means into MATLAB's layout on the device, then one copy into the caller's buffer
+    const size_t per_block = av_doubles_per_block(P);
+    const bool dev_perm = P.obs.size() <= 32;
+    std::vector<double> av(dev_perm ? 0 : avd);
+    if (av_out && per_block) {
+      if (dev_perm) {
+        XsAvMap m{};
+        m.nobs = (int)P.obs.size();
+        m.npts = P.p.points[0];
+        m.NS = P.NS;
+        m.nout_site = P.nout_site;
+        m.stride = (int)stride;
+        m.per_block = (long long)(per_block / 2);
+        long long off = 0;
+        for (int o = 0; o < m.nobs; ++o) {
+          m.lines[o] = P.obs[o].lines;
+          m.spatial[o] = P.obs[o].spatial ? 1 : 0;
+          m.out_off[o] = P.obs[o].out_off;
+          m.o_off[o] = off;
+          off += (long long)P.obs[o].lines * m.npts * (P.obs[o].spatial ? P.NS : 1);
+        }
+        h->d_avm.ensure((size_t)nblocks * per_block * 8);
+        CUDA_CHECK((cudaError_t)xs_aot_av_matlab_launch(h->d_av.p, h->d_avm.p, &m, nblocks, h->stream));
+        CUDA_CHECK(cudaMemcpyAsync(av_out, h->d_avm.p, (size_t)nblocks * per_block * 8, cudaMemcpyDeviceToHost,
+                                   h->stream));
+      } else if (avd) {
+        CUDA_CHECK(cudaMemcpyAsync(av.data(), h->d_av.p, avd * 8, cudaMemcpyDeviceToHost, h->stream));
+      }
+    }
     int status = 0;
     CUDA_CHECK(cudaMemcpyAsync(&status, h->d_status.p, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
     if (a_out) {
       if (P.F == 1) {
         CUDA_CHECK(cudaMemcpyAsync(a_out, dout, fbytes, cudaMemcpyDeviceToHost, h->stream));
         CUDA_CHECK(cudaStreamSynchronize(h->stream));
-      } else {
-        std::vector<double> tmp(ntraj * P.F * P.NS * 2);
-        CUDA_CHECK(cudaMemcpyAsync(tmp.data(), dout, fbytes, cudaMemcpyDeviceToHost, h->stream));
-        CUDA_CHECK(cudaStreamSynchronize(h->stream));
-        for (size_t e = 0; e < ntraj; ++e)
-          for (int f = 0; f < P.F; ++f)
-            for (int s = 0; s < P.NS; ++s) {
-              size_t dst = (f + (size_t)P.F * (s + (size_t)P.NS * e)) * 2, src = ((e * P.F + f) * P.NS + s) * 2;
-              a_out[dst] = tmp[src];
-              a_out[dst + 1] = tmp[src + 1];
-            }
+      } else {  // reorder on the device
+        h->d_tmp.ensure(fbytes);
+        CUDA_CHECK((cudaError_t)xs_aot_reorder_launch(dout, h->d_tmp.p, P.F, P.NS, (long long)ntraj, 0, h->stream));
+        CUDA_CHECK(cudaMemcpyAsync(a_out, h->d_tmp.p, fbytes, cudaMemcpyDeviceToHost, h->stream));
       }
     }
     CUDA_CHECK(cudaStreamSynchronize(h->stream));
-    if (av_out) scatter_av(P, av, nblocks, av_out);
+    if (av_out && !dev_perm) scatter_av(P, av, nblocks, av_out);
     if (status & 2) raise(XS_ERR_SHAPE, "kernel refused a launch whose shared-memory layout or grid did not match");
     if (status & 1) raise(XS_ERR_NAN, "a trajectory became non-finite (NaN/Inf) during the path");
     return XS_OK;
