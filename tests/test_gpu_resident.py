@@ -138,11 +138,13 @@ def test_a_in_a_out_roundtrip():
     assert rel_err(av_g[0][0], av_o[0]) < FP64_TOL
 
 
-def test_field_in_device_memory_2d_periodic_fp64():
+@pytest.mark.parametrize("method", ["MP", "RK4"])
+def test_field_in_device_memory_2d_periodic_fp64(method):
     """128 x 128 FP64 (256 KB per array) exceeds shared memory: the resident
-    kernel keeps field and scratch in per-CTA device-memory slices."""
+    kernel keeps field, scratch and (RK4) noise arrays in per-CTA device-memory
+    slices."""
     base = dict(dimensions=3, points=[3, 128, 128], ranges=[0.2, 20.0, 20.0], steps=3, ensembles=[2, 2, 1],
-                noises=2, method="MP", checks=1)
+                noises=2, method=method, checks=1)
     g = dict(base, deriv="@(a,w,p) 1i*abs(a).^2.*a + 0.02*(w(1,:)+1i*w(2,:))",
              initial="@(v,p) exp(-(p.x.^2+p.y.^2)/8) + 0.1*v(1,:)", linear="@(p) 0.5i*(p.Dx.^2+p.Dy.^2)",
              observe=["@(a,p) abs(a).^2", "@(a,p) Int(abs(a).^2, p)"])

@@ -30,6 +30,11 @@ GOLDEN = {
                       initial="@(v,p) sech(p.x)", deriv="@(a,~,~) 1i*a.*(conj(a).*a)",
                       linear="@(p) 0.5*1i*(p.Dx.^2-1.0)",
                       compare=[lambda p: np.pi / 10 + 0 * p.t, lambda p: np.pi + 0 * p.t]),
+    # Examples/SPDE_nD/Gaussian3D.m: 35^3 FP64 lattice, beyond shared memory (field in device memory)
+    "Gaussian3D": dict(noises=0, dimensions=4, initial="@(w,p) exp(-(p.x.^2+p.y.^2+p.z.^2)/2)",
+                       observe=["@(a,p) a.*conj(a)"], linear="@(p) -0.5 + 1i*0.05*(p.Dx.^2+p.Dy.^2+p.Dz.^2)",
+                       compare=[lambda p: (1 + (p.t / 10) ** 2) ** -1.5
+                                * np.exp(-p.t - (p.x ** 2 + p.y ** 2 + p.z ** 2) / (1 + (p.t / 10) ** 2))]),
 }
 
 

@@ -45,6 +45,9 @@ struct XsPathArgs {
 // only the reduction scratch in shared memory.  The code is the same; only the
 // arrays' home differs (__syncthreads orders global accesses within a CTA).
 #define XS_FARR (XS_GFIELD ? 0 : XS_NARR)
+// complex elements of one CTA's slice: the field arrays, then (methods other
+// than MP) the two noise arrays of reals
+#define XS_GSLICE ((size_t)XS_NARR * XS_G * XS_F * XS_NS + (size_t)XS_WARR * XS_G * XS_NWS * XS_NS * sizeof(real) / sizeof(cx))
 
 extern __shared__ __align__(16) unsigned char xs_smem[];
 
@@ -601,7 +604,7 @@ __device__ __forceinline__ bool xs_layout_ok(int* status) {
   constexpr size_t GF = (size_t)XS_G * XS_F * XS_NS;
   constexpr size_t need = (XS_FARR * GF + 2 * (size_t)XS_TILE_ELEMS) * sizeof(cx) + (size_t)XS_G * (XS_NRED > 0 ? XS_NRED : 1) * sizeof(cx) +
                           32 * 2 * (XS_NRED > 0 ? XS_NRED : 1) * sizeof(double) +
-                          XS_WARR * (size_t)XS_G * XS_NWS * XS_NS * sizeof(real);
+                          (XS_GFIELD ? 0 : XS_WARR) * (size_t)XS_G * XS_NWS * XS_NS * sizeof(real);
   u32 dyn;
   asm volatile("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn));
   if (need > (size_t)dyn || need != (size_t)XS_SMEM_BYTES || (int)blockDim.x != XS_THREADS) {
@@ -616,7 +619,7 @@ __device__ __forceinline__ bool xs_layout_ok(int* status) {
 __device__ void xs_resident_run(const XsPathArgs& P, int cta, int nctas) {
   constexpr int GF = XS_G * XS_F * XS_NS;
 #if XS_GFIELD
-  cx* A = P.gfield + (size_t)blockIdx.x * XS_NARR * GF;
+  cx* A = P.gfield + (size_t)blockIdx.x * XS_GSLICE;
   cx* RED = (cx*)xs_smem + 2 * XS_TILE_ELEMS;  // after the two transform tiles; [G][NRED]
 #else
   cx* A = (cx*)xs_smem;
@@ -627,7 +630,11 @@ __device__ void xs_resident_run(const XsPathArgs& P, int cta, int nctas) {
   cx* B3 = B2 + (XS_NARR >= 4 ? GF : 0);
   cx* T = A + (XS_NARR - 1) * GF;     // transform scratch is the last array
   double* wsum = (double*)(RED + XS_G * (XS_NRED > 0 ? XS_NRED : 1));  // [32][2*NRED]
+#if XS_GFIELD
+  real* W = (real*)(A + XS_NARR * GF);  // noise arrays follow the field arrays in the CTA's slice
+#else
   real* W = (real*)(wsum + 32 * 2 * (XS_NRED > 0 ? XS_NRED : 1));
+#endif
   real* Wp = W + XS_G * XS_NWS * XS_NS;
   const int g0 = cta * XS_G;
   if ((cta + 1) * XS_G > P.ntraj || cta >= nctas) {

@@ -736,8 +736,9 @@ size_t resident_smem(const xs_handle& h, int G, int narr) {
   size_t cxs = h.fp64 ? 16 : 8, rs = h.fp64 ? 8 : 4;
   size_t nred = std::max(P.nred, 1);
   size_t nws = std::max(P.NW, 1);
-  const size_t warr = P.p.method == XS_METHOD_MP ? 0 : 2;  // MP keeps its noise in registers
+  size_t warr = P.p.method == XS_METHOD_MP ? 0 : 2;  // MP keeps its noise in registers
   size_t tiles = 0;
+  if (narr == 0) warr = 0;  // field in device memory: the noise arrays live in the CTA's slice too
   if (narr == 0) {  // field in device memory: two transform tiles in shared memory
     int tl[3], lsp[3];
     tile_plan(P, h.fp64, tl, lsp, tiles);
@@ -762,11 +763,7 @@ void plan_resident(xs_handle& h, int total_traj) {
   rp.narr = method_arrays(P.p.method);
   const size_t limit = 200 * 1024;
   if (resident_smem(h, 1, rp.narr) > limit) {
-    // lattice beyond shared memory: one trajectory per CTA, field and scratch in device memory (MP only,
-    // whose noise lives in registers)
-    if (P.p.method != XS_METHOD_MP)
-      raise(XS_ERR_UNSUPPORTED, "field of one trajectory does not fit in shared memory (only MP runs such lattices "
-                                "with the field in device memory)");
+    // lattice beyond shared memory: one trajectory per CTA, field, scratch and noise arrays in device memory
     if (h.force_G > 1) raise(XS_ERR_UNSUPPORTED, "lattices beyond shared memory take one trajectory per CTA");
     rp.gfield = true;
     rp.G = 1;
@@ -987,7 +984,7 @@ void build_source(xs_handle& h) {
   const std::string why = stream_blocker(P);
   // too large for shared memory: the streaming path when it covers the problem, else the resident
   // path with the field in device memory (MP)
-  if (h.path_kind == 2 || (h.path_kind == 0 && !fits && (why.empty() || P.p.method != XS_METHOD_MP))) {
+  if (h.path_kind == 2 || (h.path_kind == 0 && !fits && why.empty())) {
     if (!why.empty()) {
       if (!fits) raise(XS_ERR_UNSUPPORTED, "field too large for the resident path, and " + why);
       raise(XS_ERR_UNSUPPORTED, why);
@@ -1275,7 +1272,9 @@ int resident_grid(xs_handle& h, CUfunction f, int nctas) {
   CUDA_CHECK(cudaGetDevice(&dev));
   CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   cu_check(driver().occupancy(&occ, f, h.rp.threads, h.rp.smem), "occupancy");
-  const size_t slice = (size_t)h.rp.narr * h.rp.G * h.P.F * h.P.NS * (h.fp64 ? 16 : 8);
+  const size_t warr = h.P.p.method == XS_METHOD_MP ? 0 : 2;
+  const size_t slice = (size_t)h.rp.narr * h.rp.G * h.P.F * h.P.NS * (h.fp64 ? 16 : 8) +
+                       warr * h.rp.G * std::max(h.P.NW, 1) * h.P.NS * (h.fp64 ? 8 : 4);
   const int l2 = (int)std::max<size_t>(1, (96u << 20) / slice);
   // slices that fit L2 for a full wave: cap the grid there; larger slices stream from HBM anyway,
   // so take every CTA the SMs can hold (latency hiding)
