@@ -94,6 +94,10 @@ typedef struct xs_problem {
   int runtime_params;          /* 1: named scalars are read at run time (per batch item; param_values are
                                   the defaults), so one compiled kernel serves many parameter values.
                                   p.linear always uses param_values. */
+  const int* transforms;       /* NULL: every observable in x space; else [nobserve][4] flags of
+                                  p.transforms{n} (time, x, y, z): 1 = the observable sees the field
+                                  Fourier-transformed along that space dimension (xnft.m, periodic
+                                  dimensions only; time spectra are not supported) */
 } xs_problem;
 
 /* Create a handle: parse, generate and compile the kernels (NVRTC, cached).

@@ -30,6 +30,26 @@ GOLDEN = {
                       initial="@(v,p) sech(p.x)", deriv="@(a,~,~) 1i*a.*(conj(a).*a)",
                       linear="@(p) 0.5*1i*(p.Dx.^2-1.0)",
                       compare=[lambda p: np.pi / 10 + 0 * p.t, lambda p: np.pi + 0 * p.t]),
+    # Examples/SPDE_2D/GaussianAv2D.m: k-space observable (p.transforms)
+    "GaussianAv2D": dict(dimensions=3, initial="@(v,p) exp(-0.5*(p.x.^2+p.y.^2))", deriv="@(a,w,p) 0*a",
+                         observe=["@(a,p) a.*conj(a)", "@(a,p) Ave(a.*conj(a), p.dx, p)",
+                                  "@(a,p) Int(a.*conj(a), p.dx, p)", "@(a,p) a.*conj(a)"],
+                         linear="@(p) 1i*0.05*(p.Dx.^2+p.Dy.^2)", transforms=[0, 0, 0, [0, 1, 1]],
+                         compare=[lambda p: (1 + (p.t / 10) ** 2) ** -1
+                                  * np.exp(-(p.x ** 2 + p.y ** 2) / (1 + (p.t / 10) ** 2)), None, None,
+                                  lambda r: 1], axes=[None, None, None, [0, -1, -1]]),
+    # Examples/SPDE_2D/GaussianKinetic.m: k-space observables with p.kx, p.ky and p.dk integrals
+    "GaussianKinetic": dict(dimensions=3, fields=1, ranges=[5, 200, 6], points=[49, 70, 34],
+                            initial="@(v,p) sqrt(exp(-p.x.^2/3.3^2 - p.y.^2/0.235^2)/(pi*3.3*0.235))",
+                            linear="@(p) 1i*(p.Dx.^2)",
+                            observe=["@(a,p) abs(a).^2", "@(a,p) abs(a).^2",
+                                     "@(a,p) Int(abs(a).^2.*(p.kx.^2+p.ky.^2), p.dk, p)",
+                                     "@(a,p) sqrt(Int(p.y.^2.*abs(a).^2, p.dx, p)./Int(abs(a).^2, p.dx, p))",
+                                     "@(a,p) sqrt(Int(p.x.^2.*abs(a).^2, p.dx, p)./Int(abs(a).^2, p.dx, p))",
+                                     "@(a,p) sqrt(Int(p.ky.^2.*abs(a).^2, p.dk, p)./Int(abs(a).^2, p.dk, p))"],
+                            transforms=[0, [0, 1, 1], [0, 1, 1], 0, 0, [0, 1, 1]],
+                            compare=[None, None, lambda p: 1 / (2 * 3.3 ** 2) + 1 / (2 * 0.235 ** 2),
+                                     lambda p: 0.235 / np.sqrt(2), None, lambda p: 1 / (np.sqrt(2) * 0.235)]),
     # Examples/SPDE_nD/Gaussian3D.m: 35^3 FP64 lattice, beyond shared memory (field in device memory)
     "Gaussian3D": dict(noises=0, dimensions=4, initial="@(w,p) exp(-(p.x.^2+p.y.^2+p.z.^2)/2)",
                        observe=["@(a,p) a.*conj(a)"], linear="@(p) -0.5 + 1i*0.05*(p.Dx.^2+p.Dy.^2+p.Dz.^2)",

@@ -51,6 +51,7 @@ class XsProblem(ctypes.Structure):
         ("param_values", ctypes.POINTER(ctypes.c_double)),
         ("path_kind", ctypes.c_int),
         ("runtime_params", ctypes.c_int),
+        ("transforms", ctypes.POINTER(ctypes.c_int)),
     ]
 
 

@@ -47,7 +47,7 @@ struct XsPathArgs {
 #define XS_FARR (XS_GFIELD ? 0 : XS_NARR)
 // complex elements of one CTA's slice: the field arrays, then (methods other
 // than MP) the two noise arrays of reals
-#define XS_GSLICE ((size_t)XS_NARR * XS_G * XS_F * XS_NS + (size_t)XS_WARR * XS_G * XS_NWS * XS_NS * sizeof(real) / sizeof(cx))
+#define XS_GSLICE ((size_t)(XS_NARR + XS_KARR) * XS_G * XS_F * XS_NS + (size_t)XS_WARR * XS_G * XS_NWS * XS_NS * sizeof(real) / sizeof(cx))
 
 extern __shared__ __align__(16) unsigned char xs_smem[];
 
@@ -525,9 +525,27 @@ __device__ __forceinline__ void xs_noise(real* W, real* Wp, int mode, int draw, 
 }
 
 // Observables at one output time: per-CTA sums over its trajectories.
+// K (XS_KOBS): the field Fourier-transformed along the flagged dimensions for
+// the observables with p.transforms (xnft.m: fft along each, times dx/sqrt(2 pi));
+// T is the transform scratch, free at output times.
 __device__ void xs_observe(const cx* A, cx* RED, int n, double t, const XsPathArgs& P, double* wsum, int cta,
-                           int nctas) {
+                           int nctas, cx* K, cx* T) {
   double2* out = P.obs + ((size_t)n * nctas + cta) * XS_OBS_STRIDE;
+#if XS_KOBS
+  for (int i = threadIdx.x; i < XS_G * XS_F * XS_NS; i += blockDim.x) K[i] = A[i];
+  __syncthreads();
+  if (XS_KTR1) xs_tr<1>(K, T, P, 0);
+  if (XS_KTR2) xs_tr<2>(K, T, P, 0);
+  if (XS_KTR3) xs_tr<3>(K, T, P, 0);
+  __syncthreads();
+#define XS_LOAD_AK(g, s)                                                          \
+  _Pragma("unroll") for (int f = 0; f < XS_F; ++f) ak[f] = K[((g) * XS_F + f) * XS_NS + (s)] * (real)XS_KFACT;
+#else
+  (void)K;
+  (void)T;
+#define XS_LOAD_AK(g, s)                                                          \
+  _Pragma("unroll") for (int f = 0; f < XS_F; ++f) ak[f] = a[f];
+#endif
 #if XS_NRED > 0
   // full-space reductions (Int/Ave) per trajectory
   for (int g = 0; g < XS_G; ++g) {
@@ -538,10 +556,11 @@ __device__ void xs_observe(const cx* A, cx* RED, int n, double t, const XsPathAr
       int i1, i2, i3;
       real x, y, z;
       xs_site(s, i1, i2, i3, x, y, z);
-      cx a[XS_F], r[XS_NRED];
+      cx a[XS_F], ak[XS_F], r[XS_NRED];
 #pragma unroll
       for (int f = 0; f < XS_F; ++f) a[f] = A[(g * XS_F + f) * XS_NS + s];
-      xs_integrands(a, i1, i2, i3, x, y, z, (real)t, P.params, r);
+      XS_LOAD_AK(g, s)
+      xs_integrands(a, ak, i1, i2, i3, x, y, z, (real)t, P.params, r);
 #pragma unroll
       for (int k = 0; k < XS_NRED; ++k) { acc[2 * k] += (double)r[k].re; acc[2 * k + 1] += (double)r[k].im; }
     }
@@ -570,10 +589,11 @@ __device__ void xs_observe(const cx* A, cx* RED, int n, double t, const XsPathAr
 #pragma unroll
     for (int k = 0; k < XS_NOUT_SITE; ++k) sr[k] = si[k] = 0;
     for (int g = 0; g < XS_G; ++g) {
-      cx a[XS_F], o[XS_NOUT_SITE];
+      cx a[XS_F], ak[XS_F], o[XS_NOUT_SITE];
 #pragma unroll
       for (int f = 0; f < XS_F; ++f) a[f] = A[(g * XS_F + f) * XS_NS + s];
-      xs_obs_site(a, RED + g * (XS_NRED > 0 ? XS_NRED : 1), x, y, z, (real)t, P.params, o);
+      XS_LOAD_AK(g, s)
+      xs_obs_site(a, ak, RED + g * (XS_NRED > 0 ? XS_NRED : 1), x, y, z, i1, i2, i3, (real)t, P.params, o);
 #pragma unroll
       for (int k = 0; k < XS_NOUT_SITE; ++k) { sr[k] += (double)o[k].re; si[k] += (double)o[k].im; }
     }
@@ -594,6 +614,7 @@ __device__ void xs_observe(const cx* A, cx* RED, int n, double t, const XsPathAr
       out[(size_t)XS_NOUT_SITE * XS_NS + k] = make_double2(sr[k], si[k]);
   }
 #endif
+#undef XS_LOAD_AK
   __syncthreads();
 }
 
@@ -602,7 +623,7 @@ __device__ void xs_observe(const cx* A, cx* RED, int n, double t, const XsPathAr
 // not match the layout; the CTA must then return without touching it.
 __device__ __forceinline__ bool xs_layout_ok(int* status) {
   constexpr size_t GF = (size_t)XS_G * XS_F * XS_NS;
-  constexpr size_t need = (XS_FARR * GF + 2 * (size_t)XS_TILE_ELEMS) * sizeof(cx) + (size_t)XS_G * (XS_NRED > 0 ? XS_NRED : 1) * sizeof(cx) +
+  constexpr size_t need = ((XS_GFIELD ? 0 : XS_NARR + XS_KARR) * GF + 2 * (size_t)XS_TILE_ELEMS) * sizeof(cx) + (size_t)XS_G * (XS_NRED > 0 ? XS_NRED : 1) * sizeof(cx) +
                           32 * 2 * (XS_NRED > 0 ? XS_NRED : 1) * sizeof(double) +
                           (XS_GFIELD ? 0 : XS_WARR) * (size_t)XS_G * XS_NWS * XS_NS * sizeof(real);
   u32 dyn;
@@ -623,15 +644,16 @@ __device__ void xs_resident_run(const XsPathArgs& P, int cta, int nctas) {
   cx* RED = (cx*)xs_smem + 2 * XS_TILE_ELEMS;  // after the two transform tiles; [G][NRED]
 #else
   cx* A = (cx*)xs_smem;
-  cx* RED = A + XS_NARR * GF;         // [G][NRED]
+  cx* RED = A + (XS_NARR + XS_KARR) * GF;  // [G][NRED]
 #endif
+  cx* K = A + XS_NARR * GF;  // k-space copy of the field (XS_KARR)
   cx* B1 = A + GF;
   cx* B2 = B1 + (XS_NARR >= 3 ? GF : 0);
   cx* B3 = B2 + (XS_NARR >= 4 ? GF : 0);
   cx* T = A + (XS_NARR - 1) * GF;     // transform scratch is the last array
   double* wsum = (double*)(RED + XS_G * (XS_NRED > 0 ? XS_NRED : 1));  // [32][2*NRED]
 #if XS_GFIELD
-  real* W = (real*)(A + XS_NARR * GF);  // noise arrays follow the field arrays in the CTA's slice
+  real* W = (real*)(A + (XS_NARR + XS_KARR) * GF);  // noise arrays follow the field arrays in the CTA's slice
 #else
   real* W = (real*)(wsum + 32 * 2 * (XS_NRED > 0 ? XS_NRED : 1));
 #endif
@@ -721,7 +743,7 @@ __device__ void xs_resident_run(const XsPathArgs& P, int cta, int nctas) {
         if (pending) xs_prop(A, T, P);
         pending = false;
 #endif
-        xs_observe(A, RED, n, t, P, wsum, cta, nctas);
+        xs_observe(A, RED, n, t, P, wsum, cta, nctas, K, T);
       }
     }
   }

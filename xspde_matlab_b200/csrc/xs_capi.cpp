@@ -225,6 +225,7 @@ struct ObsInfo {
   bool spatial = true;
   int red_off = 0;      // offset of its reductions in the combined red[] array
   int out_off = 0;      // offset in the site (spatial) or scalar output lists
+  bool kspace = false;  // evaluated on the Fourier-transformed field (p.transforms{n})
   xs::Generated gen;
 };
 
@@ -234,6 +235,9 @@ struct Problem {
   std::vector<std::string> observe;
   xs::Scalars scalars;
   std::vector<std::string> runtime_names;  // named scalars read at run time (prm[k])
+  std::vector<std::vector<int>> obs_tr;    // per observable: p.transforms{n} flags (time, x, y, z)
+  int ktr[3] = {0, 0, 0};                  // space dimensions the k-space observables transform
+  bool kobs = false;                       // some observable is evaluated in Fourier space
   std::vector<double> runtime_defaults;
   std::vector<int> bnd;  // [D][F][2]
   int D = 0, F = 1, NW = 0, NV = 0, NS = 1, E1 = 1;
@@ -307,6 +311,13 @@ void setup_problem(const xs_problem* in, Problem& P) {
     // p.linear is evaluated on the host once: it reads the default values
     for (int i = 0; i < p.nparams; ++i) P.scalars.values[p.param_names[i]] = p.param_values[i];
   }
+  for (int i = 0; i < p.nobserve || (i == 0 && p.nobserve == 0); ++i) {
+    std::vector<int> tr(4, 0);
+    if (p.transforms && i < p.nobserve)
+      for (int d = 0; d < 4; ++d) tr[d] = p.transforms[i * 4 + d] ? 1 : 0;
+    P.obs_tr.push_back(tr);
+  }
+  P.p.transforms = nullptr;
   P.p.deriv = P.p.initial = P.p.linear = nullptr;
   P.p.observe = nullptr;
   P.p.param_names = nullptr;
@@ -324,6 +335,28 @@ void setup_problem(const xs_problem* in, Problem& P) {
       }
   }
   P.p.boundaries = nullptr;
+  // k-space observables (xdata.m, xnft.m): one common set of periodic space dimensions
+  for (auto& tr : P.obs_tr) {
+    if (tr[0]) raise(XS_ERR_UNSUPPORTED, "time-spectrum observables (p.transforms{n}(1)) are not supported on the device");
+    int k[3] = {0, 0, 0};
+    bool any = false;
+    for (int d = 0; d < P.D; ++d)
+      if (tr[d + 1] && P.N[d] > 1) {
+        for (int f = 0; f < P.F; ++f)
+          if (P.type(d, f) != 0)
+            raise(XS_ERR_UNSUPPORTED, "k-space observables are supported along periodic dimensions only");
+        k[d] = 1;
+        any = true;
+      }
+    if (!any) {
+      tr.assign(4, 0);
+      continue;
+    }
+    if (P.kobs && (k[0] != P.ktr[0] || k[1] != P.ktr[1] || k[2] != P.ktr[2]))
+      raise(XS_ERR_UNSUPPORTED, "k-space observables must all transform the same dimensions");
+    for (int d = 0; d < 3; ++d) P.ktr[d] = k[d];
+    P.kobs = true;
+  }
   // grid constants (Simulator/xpreferences.m:133-175, spdpreferences.m:190-244)
   for (int d = 0; d < p.dimensions; ++d) {
     int n = p.points[d];
@@ -482,6 +515,7 @@ xs::GenCtx make_ctx(const Problem& P, std::vector<xs::Role> roles, bool reduce) 
   c.nrand = P.NV;
   c.ndim = P.D;
   c.allow_reduce = reduce;
+  c.kgrid = reduce;  // observe functions may read p.kx/ky/kz
   c.scalars = &P.scalars;
   c.runtime = P.runtime_names.empty() ? nullptr : &P.runtime_names;
   for (int d = 0; d < P.p.dimensions; ++d) {
@@ -531,8 +565,10 @@ void generate_functions(Problem& P, std::ostringstream& os) {
   // observe{n}(a, p) (xdata.m:339)
   P.obs.clear();
   P.nred = P.nout_site = P.nout_scalar = 0;
-  for (auto& txt : P.observe) {
+  for (size_t oi = 0; oi < P.observe.size(); ++oi) {
+    const std::string& txt = P.observe[oi];
     ObsInfo o;
+    o.kspace = oi < P.obs_tr.size() && (P.obs_tr[oi][1] || P.obs_tr[oi][2] || P.obs_tr[oi][3]);
     auto fn = xs::parse_anon(txt);
     o.gen = xs::generate(fn, make_ctx(P, {Role::Field, Role::Params}, true));
     o.lines = o.gen.len;
@@ -554,9 +590,26 @@ void generate_functions(Problem& P, std::ostringstream& os) {
   }
   os << "#define XS_NRED " << P.nred << "\n#define XS_NOUT_SITE " << P.nout_site << "\n#define XS_NOUT_SCALAR "
      << P.nout_scalar << "\n#define XS_OBS_STRIDE (XS_NOUT_SITE * XS_NS + XS_NOUT_SCALAR)\n";
+  // k-space observables: transformed dimensions, normalisation prod kfact = prod dx/sqrt(2 pi) (xnft.m),
+  // k grids of the observe functions (p.kx ... in propagation order)
+  {
+    double kf = 1;
+    for (int d = 0; d < 3; ++d)
+      if (P.ktr[d]) kf *= P.dx[d + 1] / std::sqrt(2 * M_PI);
+    os << "#define XS_KOBS " << (P.kobs ? 1 : 0) << "\n#define XS_KTR1 " << P.ktr[0] << "\n#define XS_KTR2 "
+       << P.ktr[1] << "\n#define XS_KTR3 " << P.ktr[2] << "\n#define XS_KFACT " << fmt(kf) << "\n";
+    for (int d = 0; d < 3; ++d) {
+      os << "__device__ const double xs_kt" << d + 1 << "[] = {";
+      if (d < P.D && !P.kprop.empty())
+        for (size_t i = 0; i < P.kprop[0][d].size(); ++i) os << (i ? "," : "") << fmt(P.kprop[0][d][i]);
+      else
+        os << "0";
+      os << "};\n";
+    }
+  }
   // integrands with bounds masks and weights
-  os << "__device__ __forceinline__ void xs_integrands(const cx* __restrict__ a, int i1, int i2, int i3, real x, real y, real z, real t, const double* __restrict__ prm, cx* __restrict__ rr) {\n";
-  os << "  (void)a; (void)i1; (void)i2; (void)i3; (void)x; (void)y; (void)z; (void)t; (void)rr; (void)prm;\n";
+  os << "__device__ __forceinline__ void xs_integrands(const cx* __restrict__ a, const cx* __restrict__ ak, int i1, int i2, int i3, real x, real y, real z, real t, const double* __restrict__ prm, cx* __restrict__ rr) {\n";
+  os << "  (void)a; (void)ak; (void)i1; (void)i2; (void)i3; (void)x; (void)y; (void)z; (void)t; (void)rr; (void)prm;\n";
   int off = 0;
   for (auto& o : P.obs) {
     for (auto& r : o.gen.reductions) {
@@ -579,22 +632,24 @@ void generate_functions(Problem& P, std::ostringstream& os) {
           mask += std::string(" && ") + iv + " >= " + std::to_string(j0) + " && " + iv + " < " + std::to_string(j);
         }
       }
-      os << "  {\n    cx* r = rr + " << off << ";\n" << r.integrand_code;
+      os << "  {\n    cx* r = rr + " << off << ";\n" << (o.kspace ? "    const cx* a = ak; (void)a;\n" : "")
+         << r.integrand_code;
       os << "    const real wgt = (" << mask << ") ? (real)" << fmt(w) << " : (real)0;\n";
       os << "    for (int k = 0; k < " << r.lines << "; ++k) r[k] = r[k] * wgt;\n  }\n";
       off += r.lines;
     }
   }
   os << "}\n";
-  os << "__device__ __forceinline__ void xs_obs_site(const cx* __restrict__ a, const cx* __restrict__ redall, real x, real y, real z, real t, const double* __restrict__ prm, cx* __restrict__ outall) {\n";
-  os << "  (void)a; (void)redall; (void)x; (void)y; (void)z; (void)t; (void)outall; (void)prm;\n";
+  os << "__device__ __forceinline__ void xs_obs_site(const cx* __restrict__ a, const cx* __restrict__ ak, const cx* __restrict__ redall, real x, real y, real z, int i1, int i2, int i3, real t, const double* __restrict__ prm, cx* __restrict__ outall) {\n";
+  os << "  (void)a; (void)ak; (void)redall; (void)x; (void)y; (void)z; (void)i1; (void)i2; (void)i3; (void)t; (void)outall; (void)prm;\n";
   for (auto& o : P.obs)
     if (o.spatial)
       os << "  {\n    const cx* red = redall + " << o.red_off << "; (void)red;\n    cx* out = outall + " << o.out_off
-         << ";\n" << o.gen.code << "  }\n";
+         << ";\n" << (o.kspace ? "    const cx* a = ak; (void)a;\n" : "") << o.gen.code << "  }\n";
   os << "}\n";
   os << "__device__ __forceinline__ void xs_obs_scalar(const cx* __restrict__ redall, real t, const double* __restrict__ prm, cx* __restrict__ outall) {\n";
   os << "  (void)redall; (void)t; (void)outall; (void)prm; const cx* a = nullptr; const real x = 0, y = 0, z = 0; (void)a; (void)x; (void)y; (void)z;\n";
+  os << "  const int i1 = 0, i2 = 0, i3 = 0; (void)i1; (void)i2; (void)i3;\n";
   for (auto& o : P.obs)
     if (!o.spatial)
       os << "  {\n    const cx* red = redall + " << o.red_off << "; (void)red;\n    cx* out = outall + " << o.out_off
@@ -739,6 +794,7 @@ size_t resident_smem(const xs_handle& h, int G, int narr) {
   size_t warr = P.p.method == XS_METHOD_MP ? 0 : 2;  // MP keeps its noise in registers
   size_t tiles = 0;
   if (narr == 0) warr = 0;  // field in device memory: the noise arrays live in the CTA's slice too
+  if (narr > 0 && P.kobs) narr += 1;  // the k-space copy of the field for transformed observables
   if (narr == 0) {  // field in device memory: two transform tiles in shared memory
     int tl[3], lsp[3];
     tile_plan(P, h.fp64, tl, lsp, tiles);
@@ -889,6 +945,7 @@ std::string stream_blocker(const Problem& P) {
   if (!P.has_linear) return "the streaming path needs p.linear";
   for (auto& o : P.obs)
     if (o.spatial && !o.gen.reductions.empty()) return "site observables that use Int/Ave are not streamed";
+  if (P.kobs) return "k-space observables (p.transforms) are not streamed";
   return "";
 }
 
@@ -1010,6 +1067,7 @@ void build_source(xs_handle& h) {
   std::ostringstream os;
   emit_common_header(h, os);
   os << "#define XS_G " << h.rp.G << "\n#define XS_THREADS " << h.rp.threads << "\n#define XS_NARR " << h.rp.narr << "\n";
+  os << "#define XS_KARR " << (P.kobs ? 1 : 0) << "\n";
   os << "#define XS_LEAN " << (P.p.method == XS_METHOD_MP ? 1 : 0) << "\n#define XS_WARR "
      << (P.p.method == XS_METHOD_MP ? 0 : 2) << "\n#define XS_GFIELD " << (h.rp.gfield ? 1 : 0) << "\n";
   os << "#define XS_SMEM_BYTES " << h.rp.smem << "\n";
@@ -1273,7 +1331,7 @@ int resident_grid(xs_handle& h, CUfunction f, int nctas) {
   CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   cu_check(driver().occupancy(&occ, f, h.rp.threads, h.rp.smem), "occupancy");
   const size_t warr = h.P.p.method == XS_METHOD_MP ? 0 : 2;
-  const size_t slice = (size_t)h.rp.narr * h.rp.G * h.P.F * h.P.NS * (h.fp64 ? 16 : 8) +
+  const size_t slice = (size_t)(h.rp.narr + (h.P.kobs ? 1 : 0)) * h.rp.G * h.P.F * h.P.NS * (h.fp64 ? 16 : 8) +
                        warr * h.rp.G * std::max(h.P.NW, 1) * h.P.NS * (h.fp64 ? 8 : 4);
   const int l2 = (int)std::max<size_t>(1, (96u << 20) / slice);
   // slices that fit L2 for a full wave: cap the grid there; larger slices stream from HBM anyway,

@@ -663,8 +663,17 @@ struct Gen {
     if (f == "x") return coord(1);
     if (f == "y") return coord(2);
     if (f == "z") return coord(3);
+    if (ctx.kgrid && (f == "kx" || f == "ky" || f == "kz")) {
+      const int d = f == "kx" ? 1 : (f == "ky" ? 2 : 3);
+      if (d > ctx.ndim) throw GrammarError("space dimension of 'p." + f + "' is not present");
+      static const char* ix[] = {"", "i1", "i2", "i3"};
+      Val r;
+      r.spatial = true;
+      r.c = {"((real)xs_kt" + std::to_string(d) + "[" + ix[d] + "])"};
+      return r;
+    }
     if (f == "Dx" || f == "Dy" || f == "Dz" || f == "kx" || f == "ky" || f == "kz" || f == "D" || f == "k")
-      throw GrammarError("k-space grid 'p." + f + "' is only available in p.linear");
+      throw GrammarError("k-space grid 'p." + f + "' is only available in p.linear and observe");
     if (ctx.runtime)
       for (size_t k = 0; k < ctx.runtime->size(); ++k)
         if ((*ctx.runtime)[k] == f) {

@@ -56,6 +56,7 @@ struct GenCtx {
   int nrand = 0;             // components of v
   int ndim = 0;              // space dimensions
   bool allow_reduce = false; // Int/Ave allowed (observe)
+  bool kgrid = false;        // p.kx/ky/kz available as site values (observe): xs_kt<d>[i<d>]
   const Scalars* scalars = nullptr;
   const std::vector<std::string>* runtime = nullptr;  // p.<name> read at run time as prm[k]
   std::vector<double> dx, dk, origins, ranges;  // index 0 = time

@@ -137,6 +137,18 @@ def xpreferences(inputs):
         ax = list(p.get("axes", None) or [])
         ax += [None] * (len(p.output) - len(ax))
         p.axes = [list(a) + [0] * (nd + 10 - len(a)) if a is not None else [0] * (nd + 10) for a in ax]
+        # p.transforms{n}: Fourier-space observables (xpreferences.m, xnft.m)
+        tr = p.get("transforms", None)
+        if tr is None:
+            tr = [[0] * (nd + 1)] * len(p.observe)
+        elif not isinstance(tr, (list, tuple)) or not isinstance(tr[0], (list, tuple, np.ndarray)):
+            tr = [tr] if not isinstance(tr, (list, tuple)) else list(tr)
+        tr = [[int(v) for v in np.atleast_1d(x)] + [0] * (nd + 1) for x in tr]
+        tr += [[0] * (nd + 1)] * (len(p.observe) - len(tr))
+        p.transforms = [x[: nd + 1] for x in tr]
+        ftr = p.get("ftransforms", None)
+        p.ftransforms = [list(x) for x in (ftr if ftr is not None else p.transforms)]
+        p.ftransforms += [[0] * (nd + 1)] * (len(p.output) - len(p.ftransforms))
         p.params = dict(p.get("params", {}))
         bnd = p.get("boundaries", None)
         if bnd is not None:
@@ -208,6 +220,13 @@ def make_problem(p, path_kind=0, runtime_params=False):
         pr.param_values = vals
     pr.path_kind = path_kind
     pr.runtime_params = 1 if runtime_params else 0
+    if any(any(t[1:]) or t[0] for t in p.transforms):
+        flags = []
+        for t in p.transforms:
+            flags += [int(t[j]) if j < len(t) else 0 for j in range(4)]
+        arr = (ctypes.c_int * len(flags))(*flags)
+        keep.append(arr)
+        pr.transforms = arr
     return pr, keep
 
 
@@ -315,6 +334,8 @@ def _xcompress(n, data, p, xk):
     for ax in range(d):
         ind = axes[ax]
         if np.size(x[ax]) > 1:
+            if ax + 1 <= p.dimensions and ax < len(p.ftransforms[n]) and p.ftransforms[n][ax]:
+                x[ax] = p.kc[ax]  # k axis (xcompress.m:151-153)
             if np.size(ind) == 1:
                 ind = int(np.atleast_1d(ind)[0])
                 ind = (list(range(1, shp[ax + 1] + 1)) if ind == 0 else [mid[ax + 1]] if ind == -1
@@ -341,6 +362,8 @@ def _grid(xk):
     r += [None] * (4 - len(r))
     q.r = r
     q.t, q.x, q.y, q.z = r[0], r[1], r[2], r[3]
+    q.w, q.kx, q.ky, q.kz = r[0], r[1], r[2], r[3]
+    q.rr = r
     return q
 
 
@@ -437,6 +460,9 @@ def xsim(*inputs, path_kind=0):
     for s, p in enumerate(inp):
         for n in range(len(p.output)):
             d = np.reshape(np.real(data[s][n]), p.gpoints[n], order="F")
+            for ax in range(1, min(p.dimensions, len(p.gpoints[n]) - 2)):
+                if p.ftransforms[n][ax]:  # k-space axes in centred order (xsim.m:117-121)
+                    d = np.fft.fftshift(d, axes=ax + 1)
             d, xkn = _xcompress(n, d, p, p.xk[n])
             gp = list(d.shape[:-1])
             nd_ = int(np.prod(gp))
