@@ -194,3 +194,21 @@ def test_two_fields_a_in_a_out_fp64():
     assert rel_err(a_g, b_o) < FP64_TOL
     for k in range(2):
         assert rel_err(av_g[0][k].reshape(-1, order="F"), av_o[k].reshape(-1, order="F")) < FP64_TOL
+
+
+def test_finite_difference_observables_fp64():
+    """D1/D2 (Applications/SPDE/D1.m, D2.m) in observables: three components with
+    periodic, Neumann and Dirichlet boundaries, site values and an integral."""
+    bnd = [[0, 0], [-1, -1], [1, 1]]
+    base = dict(dimensions=2, fields=3, noises=3, points=[3, 24], ranges=[0.1, 6.0], steps=2, ensembles=[4, 2, 1],
+                method="MP", checks=1, boundaries=[None, bnd])
+    g = dict(base, deriv="@(a,w,p) -0.2*a + 0.1*w", initial="@(v,p) [sin(p.x); cos(p.x); sin(p.x/2)] + 0.2*v",
+             linear="@(p) 0.3*p.Dx.^2",
+             observe=["@(a,p) D1(a,2,p)", "@(a,p) D2(a,p)", "@(a,p) Int(abs(D1(a(2,:),2,p)).^2, p)"])
+
+    def init(v, p):
+        return np.concatenate([np.sin(p.x), np.cos(p.x), np.sin(p.x / 2)], axis=0) + 0.2 * v
+    o = dict(base, deriv=lambda a, w, p: -0.2 * a + 0.1 * w, initial=init, linear=lambda p: 0.3 * p.Dx ** 2,
+             observe=[lambda a, p: X.D1(a, 1, p), lambda a, p: X.D2(a, 1, p),
+                      lambda a, p: X.Int(abs(X.D1(a, 1, p)[1:2]) ** 2, p)])
+    _compare(g, o, [0, 1], [1, 2], FP64_TOL)

@@ -50,6 +50,12 @@ GOLDEN = {
                             transforms=[0, [0, 1, 1], [0, 1, 1], 0, 0, [0, 1, 1]],
                             compare=[None, None, lambda p: 1 / (2 * 3.3 ** 2) + 1 / (2 * 0.235 ** 2),
                                      lambda p: 0.235 / np.sqrt(2), None, lambda p: 1 / (np.sqrt(2) * 0.235)]),
+    # Examples/SPDE_2D/SolitonDerivN.m: RK4, Neumann (DCT-I) boundaries, D1 finite differences in an observable
+    "SolitonDerivN": dict(dimensions=2, points=[101, 101], method="RK4", order=4, ranges=[10, 15],
+                          initial="@(v,p) sech(p.x)",
+                          observe=["@(a,p) a.*conj(a)", "@(a,p) Int(abs(D1(a,2,p)).^2,p)"],
+                          boundaries=[None, [-1, -1]], deriv="@(a,w,p) 1i*a.*(conj(a).*a)",
+                          linear="@(p) 0.5i*(p.Dx.^2-1)"),
     # Examples/SPDE_nD/Gaussian3D.m: 35^3 FP64 lattice, beyond shared memory (field in device memory)
     "Gaussian3D": dict(noises=0, dimensions=4, initial="@(w,p) exp(-(p.x.^2+p.y.^2+p.z.^2)/2)",
                        observe=["@(a,p) a.*conj(a)"], linear="@(p) -0.5 + 1i*0.05*(p.Dx.^2+p.Dy.^2+p.Dz.^2)",

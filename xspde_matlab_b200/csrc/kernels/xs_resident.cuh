@@ -560,7 +560,7 @@ __device__ void xs_observe(const cx* A, cx* RED, int n, double t, const XsPathAr
 #pragma unroll
       for (int f = 0; f < XS_F; ++f) a[f] = A[(g * XS_F + f) * XS_NS + s];
       XS_LOAD_AK(g, s)
-      xs_integrands(a, ak, i1, i2, i3, x, y, z, (real)t, P.params, r);
+      xs_integrands(a, ak, A, g, s, i1, i2, i3, x, y, z, (real)t, P.params, r);
 #pragma unroll
       for (int k = 0; k < XS_NRED; ++k) { acc[2 * k] += (double)r[k].re; acc[2 * k + 1] += (double)r[k].im; }
     }
@@ -593,7 +593,7 @@ __device__ void xs_observe(const cx* A, cx* RED, int n, double t, const XsPathAr
 #pragma unroll
       for (int f = 0; f < XS_F; ++f) a[f] = A[(g * XS_F + f) * XS_NS + s];
       XS_LOAD_AK(g, s)
-      xs_obs_site(a, ak, RED + g * (XS_NRED > 0 ? XS_NRED : 1), x, y, z, i1, i2, i3, (real)t, P.params, o);
+      xs_obs_site(a, ak, A, g, s, RED + g * (XS_NRED > 0 ? XS_NRED : 1), x, y, z, i1, i2, i3, (real)t, P.params, o);
 #pragma unroll
       for (int k = 0; k < XS_NOUT_SITE; ++k) { sr[k] += (double)o[k].re; si[k] += (double)o[k].im; }
     }

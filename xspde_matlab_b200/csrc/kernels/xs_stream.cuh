@@ -500,13 +500,13 @@ extern "C" __global__ void __launch_bounds__(XS_OROWS * XS_RX) xs_x_obs(const Xs
       for (int f = 0; f < XS_F; ++f) a[f] = v[f][j];
 #if XS_NRED > 0
       cx rr[XS_NRED];
-      xs_integrands(a, a, t + XS_RX * j, y, 0, x, yy, (real)0, tt, A.params, rr);
+      xs_integrands(a, a, (const cx*)nullptr, 0, 0, t + XS_RX * j, y, 0, x, yy, (real)0, tt, A.params, rr);
 #pragma unroll
       for (int k = 0; k < XS_NRED; ++k) { acc[2 * k] += (double)rr[k].re; acc[2 * k + 1] += (double)rr[k].im; }
 #endif
 #if XS_NOUT_SITE > 0
       cx o[XS_NOUT_SITE];
-      xs_obs_site(a, a, (const cx*)nullptr, x, yy, (real)0, t + XS_RX * j, y, 0, tt, A.params, o);
+      xs_obs_site(a, a, (const cx*)nullptr, 0, 0, (const cx*)nullptr, x, yy, (real)0, t + XS_RX * j, y, 0, tt, A.params, o);
 #pragma unroll
       for (int k = 0; k < XS_NOUT_SITE; ++k) { sr[k][j] += (double)o[k].re; si[k][j] += (double)o[k].im; }
 #endif

@@ -238,6 +238,7 @@ struct Problem {
   std::vector<std::vector<int>> obs_tr;    // per observable: p.transforms{n} flags (time, x, y, z)
   int ktr[3] = {0, 0, 0};                  // space dimensions the k-space observables transform
   bool kobs = false;                       // some observable is evaluated in Fourier space
+  bool stencil = false;                    // some observable uses D1/D2 (neighbouring sites)
   std::vector<double> runtime_defaults;
   std::vector<int> bnd;  // [D][F][2]
   int D = 0, F = 1, NW = 0, NV = 0, NS = 1, E1 = 1;
@@ -573,6 +574,7 @@ void generate_functions(Problem& P, std::ostringstream& os) {
     o.gen = xs::generate(fn, make_ctx(P, {Role::Field, Role::Params}, true));
     o.lines = o.gen.len;
     o.spatial = o.gen.spatial;  // depends on the field or the site (0-D: one site)
+    if (o.gen.stencil) P.stencil = true;
     o.red_off = P.nred;
     for (auto& r : o.gen.reductions) {
       if ((int)r.dims.size() != P.D)
@@ -607,9 +609,52 @@ void generate_functions(Problem& P, std::ostringstream& os) {
       os << "};\n";
     }
   }
+  // D1/D2 of the field at site s of trajectory g (Applications/SPDE/D1.m:60-110, D2.m:214-271):
+  // central differences with periodic wrap; at a Neumann end D1 is the boundary value and D2 the
+  // one-sided form, at a Dirichlet end D2 repeats its neighbour (boundary values zero)
+  os << "__device__ const int xs_btab[3][" << P.F << "][2] = {";
+  for (int d = 0; d < 3; ++d) {
+    os << (d ? "," : "") << "{";
+    for (int f = 0; f < P.F; ++f) {
+      const int lo = (d < P.D && !P.bnd.empty()) ? P.bnd[(d * P.F + f) * 2] : 0;
+      const int hi = (d < P.D && !P.bnd.empty()) ? P.bnd[(d * P.F + f) * 2 + 1] : 0;
+      os << (f ? "," : "") << "{" << lo << "," << hi << "}";
+    }
+    os << "}";
+  }
+  os << "};\n";
+  os << R"(__device__ __forceinline__ void xs_fd_geom(int s, int d, int& n, int& sd, int& id, real& dx) {
+  if (d == 1) { n = XS_N1; sd = 1; id = s % XS_N1; dx = (real)XS_DX1; }
+  else if (d == 2) { n = XS_N2; sd = XS_N1; id = (s / XS_N1) % XS_N2; dx = (real)XS_DX2; }
+  else { n = XS_N3; sd = XS_N1 * XS_N2; id = s / (XS_N1 * XS_N2); dx = (real)XS_DX3; }
+}
+__device__ __forceinline__ cx xs_fd1(const cx* __restrict__ fld, int g, int s, int f, int d) {
+  int n, sd, id; real dx;
+  xs_fd_geom(s, d, n, sd, id, dx);
+  const cx* b = fld + (size_t)(g * XS_F + f) * XS_NS;
+  const int sp = s + ((id + 1) % n - id) * sd, sm = s + ((id + n - 1) % n - id) * sd;
+  cx o = (b[sp] - b[sm]) / ((real)2 * dx);
+  if (id == 0 && xs_btab[d - 1][f][0] == -1) o = mkcx((real)0, (real)0);
+  if (id == n - 1 && xs_btab[d - 1][f][1] == -1) o = mkcx((real)0, (real)0);
+  return o;
+}
+__device__ __forceinline__ cx xs_fd2(const cx* __restrict__ fld, int g, int s, int f, int d) {
+  int n, sd, id; real dx;
+  xs_fd_geom(s, d, n, sd, id, dx);
+  const cx* b = fld + (size_t)(g * XS_F + f) * XS_NS;
+  const int sp = s + ((id + 1) % n - id) * sd, sm = s + ((id + n - 1) % n - id) * sd;
+  cx o = (b[sp] + b[sm] - (real)2 * b[s]) / (dx * dx);
+  const int lo = xs_btab[d - 1][f][0], hi = xs_btab[d - 1][f][1];
+  if (lo != 0 && n > 2) {
+    if (id == 0) o = lo == -1 ? (real)2 * ((b[s + sd] - b[s]) / dx) / dx : (b[s + 2 * sd] + b[s] - (real)2 * b[s + sd]) / (dx * dx);
+    if (id == n - 1) o = hi == -1 ? (real)2 * ((b[s - sd] - b[s]) / dx) / dx : (b[s] + b[s - 2 * sd] - (real)2 * b[s - sd]) / (dx * dx);
+  }
+  return o;
+}
+)";
   // integrands with bounds masks and weights
-  os << "__device__ __forceinline__ void xs_integrands(const cx* __restrict__ a, const cx* __restrict__ ak, int i1, int i2, int i3, real x, real y, real z, real t, const double* __restrict__ prm, cx* __restrict__ rr) {\n";
-  os << "  (void)a; (void)ak; (void)i1; (void)i2; (void)i3; (void)x; (void)y; (void)z; (void)t; (void)rr; (void)prm;\n";
+  os << "__device__ __forceinline__ void xs_integrands(const cx* __restrict__ a, const cx* __restrict__ ak, const cx* __restrict__ fld, int g, int s, int i1, int i2, int i3, real x, real y, real z, real t, const double* __restrict__ prm, cx* __restrict__ rr) {\n";
+  os << "  (void)a; (void)ak; (void)fld; (void)g; (void)s; (void)i1; (void)i2; (void)i3; (void)x; (void)y; (void)z; (void)t; (void)rr; (void)prm;\n";
   int off = 0;
   for (auto& o : P.obs) {
     for (auto& r : o.gen.reductions) {
@@ -640,8 +685,8 @@ void generate_functions(Problem& P, std::ostringstream& os) {
     }
   }
   os << "}\n";
-  os << "__device__ __forceinline__ void xs_obs_site(const cx* __restrict__ a, const cx* __restrict__ ak, const cx* __restrict__ redall, real x, real y, real z, int i1, int i2, int i3, real t, const double* __restrict__ prm, cx* __restrict__ outall) {\n";
-  os << "  (void)a; (void)ak; (void)redall; (void)x; (void)y; (void)z; (void)i1; (void)i2; (void)i3; (void)t; (void)outall; (void)prm;\n";
+  os << "__device__ __forceinline__ void xs_obs_site(const cx* __restrict__ a, const cx* __restrict__ ak, const cx* __restrict__ fld, int g, int s, const cx* __restrict__ redall, real x, real y, real z, int i1, int i2, int i3, real t, const double* __restrict__ prm, cx* __restrict__ outall) {\n";
+  os << "  (void)a; (void)ak; (void)fld; (void)g; (void)s; (void)redall; (void)x; (void)y; (void)z; (void)i1; (void)i2; (void)i3; (void)t; (void)outall; (void)prm;\n";
   for (auto& o : P.obs)
     if (o.spatial)
       os << "  {\n    const cx* red = redall + " << o.red_off << "; (void)red;\n    cx* out = outall + " << o.out_off
@@ -650,6 +695,7 @@ void generate_functions(Problem& P, std::ostringstream& os) {
   os << "__device__ __forceinline__ void xs_obs_scalar(const cx* __restrict__ redall, real t, const double* __restrict__ prm, cx* __restrict__ outall) {\n";
   os << "  (void)redall; (void)t; (void)outall; (void)prm; const cx* a = nullptr; const real x = 0, y = 0, z = 0; (void)a; (void)x; (void)y; (void)z;\n";
   os << "  const int i1 = 0, i2 = 0, i3 = 0; (void)i1; (void)i2; (void)i3;\n";
+  os << "  const cx* fld = nullptr; const int g = 0, s = 0; (void)fld; (void)g; (void)s;\n";
   for (auto& o : P.obs)
     if (!o.spatial)
       os << "  {\n    const cx* red = redall + " << o.red_off << "; (void)red;\n    cx* out = outall + " << o.out_off
@@ -946,6 +992,7 @@ std::string stream_blocker(const Problem& P) {
   for (auto& o : P.obs)
     if (o.spatial && !o.gen.reductions.empty()) return "site observables that use Int/Ave are not streamed";
   if (P.kobs) return "k-space observables (p.transforms) are not streamed";
+  if (P.stencil) return "observables with D1/D2 finite differences are not streamed";
   return "";
 }
 

@@ -553,6 +553,7 @@ struct Gen {
   std::string pname = "p", aname, wname, vname;
   std::vector<std::string> aux_names;
   bool in_integrand = false;
+  bool stencil = false;  // D1/D2 used: the code reads neighbours through xs_fd1/xs_fd2
 
   explicit Gen(const GenCtx& c) : ctx(c) {}
 
@@ -1021,6 +1022,46 @@ struct Gen {
           r.c = {e};
           return r;
         }
+        if (f == "D1" || f == "D2") {
+          // D1/D2(a[, d], p) (Applications/SPDE/D1.m, D2.m): central differences of the field along
+          // dimension d (2 = x), with the boundary rules of the field's boundary types
+          if (!ctx.allow_reduce)
+            throw GrammarError(f + " (finite differences) is supported in observe functions only on the device");
+          const size_t na = n->kids.size() - 1;
+          if (na != 2 && na != 3) throw GrammarError(f + " on the device takes (a, p) or (a, d, p)");
+          int dd = 2;
+          if (na == 3) {
+            Vec dv;
+            if (!try_const(n->kids[2], dv) || dv.size() != 1) throw GrammarError(f + ": the direction must be a constant");
+            dd = (int)dv[0].real();
+          }
+          if (dd < 2 || dd - 1 > ctx.ndim) throw GrammarError(f + ": the direction must be a space dimension (2 = x)");
+          const NodeP& arg = n->kids[1];
+          std::vector<int> comps;
+          if (arg->kind == NK::Var && arg->name == aname) {
+            for (int k = 0; k < ctx.nfield; ++k) comps.push_back(k);
+          } else if (arg->kind == NK::Index && arg->kids[0]->kind == NK::Var && arg->kids[0]->name == aname &&
+                     arg->kids.size() >= 2) {
+            Vec kv;
+            if (!try_const(arg->kids[1], kv)) throw GrammarError(f + ": a(k,:) needs a constant k");
+            for (auto& z : kv) {
+              const int k = (int)z.real() - 1;
+              if (k < 0 || k >= ctx.nfield) throw GrammarError(f + ": field component out of range");
+              comps.push_back(k);
+            }
+          } else {
+            throw GrammarError(f + " on the device takes the field a (or a(k,:)) as its first argument");
+          }
+          stencil = true;
+          Val r;
+          r.len = (int)comps.size();
+          r.cplx = true;
+          r.spatial = true;
+          for (int k : comps)
+            r.c.push_back(tmp(true, "xs_fd" + std::string(1, f[1]) + "(fld, g, s, " + std::to_string(k) + ", " +
+                                        std::to_string(dd - 1) + ")"));
+          return r;
+        }
         if (unary_funcs().count(f)) {
           if (n->kids.size() != 2) throw GrammarError(f + " takes one argument");
           Val a = gen(n->kids[1]);
@@ -1099,6 +1140,7 @@ Generated generate(const AnonFn& fn, const GenCtx& ctx) {
   out.code = code.str();
   out.reductions = reds;
   out.uses_k = false;
+  out.stencil = g.stencil;
   out.spatial = v.spatial;
   return out;
 }
@@ -1111,6 +1153,9 @@ std::vector<std::complex<double>> eval_linear(const AnonFn& fn, const GridInfo& 
   std::vector<int> idx(g.ndim);
   std::vector<std::vector<C>> per_site;
   int ncomp = 1;
+  std::vector<bool> uniform_k(g.ndim, true);
+  for (int d = 0; d < g.ndim; ++d)
+    for (int f = 1; f < g.nfield; ++f) uniform_k[d] = uniform_k[d] && g.k[f][d] == g.k[0][d];
   for (size_t s = 0; s < ns; ++s) {
     size_t r = s;
     for (int d = 0; d < g.ndim; ++d) {
@@ -1120,11 +1165,10 @@ std::vector<std::complex<double>> eval_linear(const AnonFn& fn, const GridInfo& 
     EvalEnv env;
     env.pname = pname;
     auto kvec = [&](int d) {
+      // one component when every field has the same k grid along d (all sites), else one per field
       Vec out;
       for (int f = 0; f < g.nfield; ++f) out.push_back(C(g.k[f][d][idx[d]]));
-      bool same = true;
-      for (int f = 1; f < g.nfield; ++f) same = same && out[f] == out[0];
-      if (same) out.resize(1);
+      if (uniform_k[d]) out.resize(1);
       return out;
     };
     env.field = [&](const std::string& f, Vec& out) -> bool {

@@ -79,6 +79,7 @@ struct Generated {
   std::string code;                  // device statements; result in out[0..len)
   std::vector<Reduction> reductions; // observe only
   bool uses_k = false;               // needs k-space field (not supported: error)
+  bool stencil = false;              // D1/D2 finite differences: reads neighbouring sites of the field
   bool spatial = true;               // result depends on the lattice site
 };
 
