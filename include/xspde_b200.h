@@ -98,6 +98,10 @@ typedef struct xs_problem {
                                   p.transforms{n} (time, x, y, z): 1 = the observable sees the field
                                   Fourier-transformed along that space dimension (xnft.m, periodic
                                   dimensions only; time spectra are not supported) */
+  int sequence;                /* index of this input in a sequence (xensemble.m:36-62): part of the
+                                  Philox counter, so every sequence draws its own noise */
+  int boundary_values;         /* 1: p.boundfun gives boundary values (MP only); the caller supplies
+                                  them per check pass with xs_set_boundary_values before each path */
 } xs_problem;
 
 /* Create a handle: parse, generate and compile the kernels (NVRTC, cached).
@@ -266,6 +270,13 @@ XS_API xs_status xs_batch_sync(xs_batch* b);
 XS_API size_t xs_batch_av_doubles(const xs_batch* b, int item);
 XS_API xs_status xs_batch_results(xs_batch* b, int item, double* av_out);
 XS_API xs_status xs_batch_info(const xs_batch* b, int item, int* info, int ninfo);
+
+/* Boundary values of p.boundfun for one check pass nc (xpatch.m, xsetbound.m;
+ * problems created with boundary_values = 1): values = complex FP64
+ * [ntimes][space dims][fields][2] (lower, upper end) at t = origins(1) +
+ * k dtr/2, k = 0..ntimes-1, dtr the pass's step; the host evaluates the user's
+ * p.boundfun there (it may be any function of t and the parameters). */
+XS_API xs_status xs_set_boundary_values(xs_handle* h, int nc, int ntimes, const double* values);
 
 /* Compile-only check (no device needed): parse and NVRTC-compile the kernels
  * of a problem for sm_100a.  Writes the compile log (truncated to n). */

@@ -44,7 +44,7 @@ def test_compile_check_cfg1(tmp_path, monkeypatch):
 
 
 @pytest.mark.parametrize("deriv,frag", [
-    ("@(a,w,p) D2(a,2,p)", "D2 (finite differences) is supported in observe functions only"),
+    ("@(a,w,p) D2(b,2,p)", "D2 on the device takes the field a"),
     ("@(a,w,p) a.*q", "unknown identifier 'q'"),
     ("@(a,w,p) a + p.gamma", "unknown parameter 'p.gamma'"),
     ("@(a,w,p) a(3,:)", "out of range"),

@@ -212,3 +212,23 @@ def test_finite_difference_observables_fp64():
              observe=[lambda a, p: X.D1(a, 1, p), lambda a, p: X.D2(a, 1, p),
                       lambda a, p: X.Int(abs(X.D1(a, 1, p)[1:2]) ** 2, p)])
     _compare(g, o, [0, 1], [1, 2], FP64_TOL)
+
+
+def _bfun(a, c, d, p):
+    s, k = np.sin(2 * p.t), np.cos(p.t)
+    return [[1 + 0.5 * s, 2 - k], [0.3 * k, -0.2 * s], [0.7 + s, 0.1 * k], [0.2 * s, 1 + 0.3 * k]]
+
+
+def test_boundary_values_all_types_stochastic_fp64():
+    """Time-dependent boundary values (p.boundfun, xpatch.m + xsetbound.m) for
+    Dirichlet-Dirichlet, Neumann-Neumann, Dirichlet-Neumann and Neumann-Dirichlet
+    components, with noise, merged-step-free MP and both check passes."""
+    bnd = [[1, 1], [-1, -1], [1, -1], [-1, 1]]
+    base = dict(dimensions=2, fields=4, noises=4, points=[4, 25], ranges=[0.3, 4.0], origins=[0.2, -1.0], steps=3,
+                ensembles=[4, 2, 1], method="MP", checks=1, boundaries=[None, bnd], boundfun=_bfun)
+    g = dict(base, deriv="@(a,w,p) -0.3*a.*conj(a).*a + 0.05*w", initial="@(v,p) 1 + 0.2*cos(p.x) + 0.1*v",
+             linear="@(p) (0.4+0.2i)*p.Dx.^2", observe=["@(a,p) a", "@(a,p) Int(abs(a).^2, p)"])
+    o = dict(base, deriv=lambda a, w, p: -0.3 * a * np.conj(a) * a + 0.05 * w,
+             initial=lambda v, p: 1 + 0.2 * np.cos(p.x) + 0.1 * v, linear=lambda p: (0.4 + 0.2j) * p.Dx ** 2,
+             observe=[lambda a, p: a, lambda a, p: X.Int(abs(a) ** 2, p)])
+    _compare(g, o, [0, 1], [1, 2], FP64_TOL)

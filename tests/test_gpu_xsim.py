@@ -16,6 +16,37 @@ def sech(x):
     return 1 / np.cosh(x)
 
 
+def _per(x, t):
+    P = np.exp(1j * t) * (4 * (1 + 2j * t) / (1 + 4 * (t ** 2 + x ** 2)) - 1)
+    dP = -8 * x * np.exp(1j * t) * (4 * (1 + 2j * t) / (1 + 4 * (t ** 2 + x ** 2)) ** 2)
+    return P, dP
+
+
+def _peregrine_bv(a, c, d, p):
+    P, dP = _per(p.origins[1], p.t)
+    return [[P, P], [dP, -dP], [P, -dP], [dP, P]]
+
+
+def _heat_in(p):
+    x = p.x
+    return np.concatenate([4 * np.sin(x) + np.sin(2 * x), 5 + 4 * np.cos(x) + np.cos(2 * x),
+                           4 * np.sin(x / 2) + np.sin(3 * x / 2), 4 * np.cos(x / 2) + np.cos(3 * x / 2),
+                           2 + np.cos(2 * x / 1.02) + np.sin(4 * x / 1.02)], axis=0)
+
+
+_E = np.exp
+_B2 = dict(dimensions=2, points=[51, 51], method="MP", order=0, fields=5, ranges=[4, np.pi], origins=[0, 0],
+           initial="@(v,p) [4*sin(p.x)+sin(2*p.x); 5+4*cos(p.x)+cos(2*p.x); 4*sin(p.x/2)+sin(3*p.x/2);"
+                   " 4*cos(p.x/2)+cos(3*p.x/2); 2+cos(2*p.x/1.02)+sin(4*p.x/1.02)]",
+           observe=["@(a,p) a(%d,:)" % i for i in range(1, 6)],
+           compare=[lambda p: 4 * np.sin(p.x) * _E(-p.t) + np.sin(2 * p.x) * _E(-4 * p.t),
+                    lambda p: 5 + 4 * np.cos(p.x) * _E(-p.t) + np.cos(2 * p.x) * _E(-4 * p.t),
+                    lambda p: 4 * np.sin(p.x / 2) * _E(-p.t / 4) + np.sin(3 * p.x / 2) * _E(-9 * p.t / 4),
+                    lambda p: 4 * np.cos(p.x / 2) * _E(-p.t / 4) + np.cos(3 * p.x / 2) * _E(-9 * p.t / 4),
+                    lambda p: 2 + np.cos(2 * p.x / 1.02) * _E(-4 * p.t / 1.02 ** 2)
+                    + np.sin(4 * p.x / 1.02) * _E(-16 * p.t / 1.02 ** 2)],
+           boundaries=[None, [[1, 1], [-1, -1], [1, -1], [-1, 1], [0, 0]]])
+
 GOLDEN = {
     # Examples/SPDE_2D/Soliton.m
     "Soliton": dict(dimensions=2, checks=0, order=2, initial="@(v,p) sech(p.x)",
@@ -56,6 +87,20 @@ GOLDEN = {
                           observe=["@(a,p) a.*conj(a)", "@(a,p) Int(abs(D1(a,2,p)).^2,p)"],
                           boundaries=[None, [-1, -1]], deriv="@(a,w,p) 1i*a.*(conj(a).*a)",
                           linear="@(p) 0.5i*(p.Dx.^2-1)"),
+    # Examples/SPDE_2D/Boundaries2.m: five components with every boundary type, then a second
+    # sequence with a D2 finite-difference drift started by a transfer function
+    "Boundaries2": [
+        dict(_B2, linear="@(p) p.Dx.^2"),
+        dict(_B2, deriv="@(a,w,p) D2(a,2,p)", steps=80, transfer=lambda b, v, p: _heat_in(p))],
+    # Examples/SPDE_2D/Peregrine.m: time-dependent boundary values of four boundary types (p.boundfun,
+    # evaluated on the host, tabulated per half step) through xpatch/xsetbound on the device
+    "Peregrine": dict(dimensions=2, noises=1, fields=4, order=2, ranges=[10, 10], origins=[-5, -5], points=[51, 161],
+                      method="MP", boundaries=[None, [[1, 1], [-1, -1], [1, -1], [-1, 1]]], boundfun=_peregrine_bv,
+                      initial="@(v,p) exp(1i*p.origins(1)).*(4*(1+2i*p.origins(1))./(1+4*(p.origins(1).^2+p.x.^2))-1)",
+                      compare=[lambda p: abs(_per(p.x, p.t)[0] ** 2)] * 4,
+                      observe=["@(a,p) a(%d,:)" % i for i in range(1, 5)],
+                      output=[(lambda i: (lambda o, p: abs(o[i]) ** 2))(i) for i in range(4)], steps=20,
+                      deriv="@(a,w,p) 1i*a.*(conj(a).*a)", linear="@(p) 0.5i*p.Dx.^2"),
     # Examples/SPDE_nD/Gaussian3D.m: 35^3 FP64 lattice, beyond shared memory (field in device memory)
     "Gaussian3D": dict(noises=0, dimensions=4, initial="@(w,p) exp(-(p.x.^2+p.y.^2+p.z.^2)/2)",
                        observe=["@(a,p) a.*conj(a)"], linear="@(p) -0.5 + 1i*0.05*(p.Dx.^2+p.Dy.^2+p.Dz.^2)",
@@ -92,3 +137,28 @@ def test_gpu_xsim_stochastic_matches_oracle():
     assert np.allclose(eg[keep], eo[keep], rtol=1e-9, atol=1e-14), (eg, eo)
     for a, b in zip(dg[0], do[0]):
         assert np.allclose(a, b, rtol=1e-9, atol=1e-13)
+
+
+def test_gpu_xsim_two_sequences_stochastic_matches_oracle():
+    """Two sequences (xensemble.m:36-62): the second continues from the first's
+    fields through a transfer function and draws its own noise (the sequence
+    index is part of the Philox counter); error and data columns match the oracle."""
+    from xspde_matlab_b200 import xsim
+    base = dict(dimensions=2, points=[5, 16], ranges=[0.5, 8.0], steps=2, ensembles=[8, 2, 1], noises=2,
+                method="MP", checks=1, order=1)
+    g1 = dict(base, deriv="@(a,w,p) 1i*a.*conj(a).*a + 0.05*(w(1,:)+1i*w(2,:))",
+              initial="@(v,p) exp(-p.x.^2) + 0.01*v(1,:)", linear="@(p) 1i*p.Dx.^2", observe=["@(a,p) a.*conj(a)"])
+    g2 = dict(g1, transfer=lambda b, v, p: 0.5 * b)
+    o1 = dict(base, deriv=lambda a, w, p: 1j * a * np.conj(a) * a + 0.05 * (w[0:1] + 1j * w[1:2]),
+              initial=lambda v, p: np.exp(-p.x ** 2) + 0.01 * v[0:1], linear=lambda p: 1j * p.Dx ** 2,
+              observe=[lambda a, p: a * np.conj(a)])
+    o2 = dict(o1, transfer=lambda b, v, p: 0.5 * b)
+    eg, dg, _ = xsim([g1, g2])
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore", RuntimeWarning)
+        eo, do, _ = X.xsim([o1, o2])
+    keep = [i for i in range(len(eo)) if i != 5]  # error(sx+2) with sx = 3 is the run time
+    assert np.allclose(np.asarray(eg)[keep], np.asarray(eo)[keep], rtol=1e-8, atol=1e-14)
+    for s in range(2):
+        for a, b in zip(dg[s], do[s]):
+            assert np.allclose(np.asarray(a), np.asarray(b), rtol=1e-9, atol=1e-12)

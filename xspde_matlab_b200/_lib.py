@@ -19,7 +19,7 @@ EXPORTS = ["xs_create", "xs_destroy", "xs_last_error", "xs_version", "xs_observe
            "xs_set_kernel_timing", "xs_kernel_stats", "xs_run_path_device_noalloc", "xs_noise_features",
            "xs_mlp_sizes", "xs_mlp_forward", "xs_mlp_train_grad", "xs_mlp_adam", "xs_batch_create",
            "xs_batch_destroy", "xs_batch_tune", "xs_batch_run", "xs_batch_sync", "xs_batch_av_doubles",
-           "xs_batch_results", "xs_batch_info"]
+           "xs_batch_results", "xs_batch_info", "xs_set_boundary_values"]
 KERNEL_KINDS = ["resident", "obs_reduce", "x_init", "x_step", "x_final", "y_pass", "x_obs", "scalar"]
 
 
@@ -52,6 +52,8 @@ class XsProblem(ctypes.Structure):
         ("path_kind", ctypes.c_int),
         ("runtime_params", ctypes.c_int),
         ("transforms", ctypes.POINTER(ctypes.c_int)),
+        ("sequence", ctypes.c_int),
+        ("boundary_values", ctypes.c_int),
     ]
 
 
@@ -136,6 +138,8 @@ def lib():
         L.xs_batch_results.restype = ci
         L.xs_batch_info.argtypes = [vp, ci, P(ci), ci]
         L.xs_batch_info.restype = ci
+        L.xs_set_boundary_values.argtypes = [vp, ci, ci, vp]
+        L.xs_set_boundary_values.restype = ci
         _ = dp
         _lib = L
     return _lib

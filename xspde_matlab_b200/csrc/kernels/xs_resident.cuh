@@ -37,6 +37,10 @@ struct XsPathArgs {
   const double* params; // runtime named scalars p.<name> (prm[k])
   cx* gfield;           // XS_GFIELD: per-CTA field + scratch slices [grid][XS_NARR][G*F*NS]
   const double2* prop2; // exp(2 L dtr / ipsteps): two consecutive half-step propagators of MP
+  const double2* bval;  // XS_BVAL: p.boundfun values [bval_n][ND][F][2] at t0 + k dtr/2
+  const double2* bda;   // XS_BVAL: [ND][F] the da term of the Neumann patch (xpropfactor.m:45-50)
+  int bval_n;
+  int pad3;
 };
 
 // XS_GFIELD: the lattice is too large for shared memory, so each CTA keeps its
@@ -170,16 +174,40 @@ __device__ __forceinline__ void xs_fft_stage(const cx* __restrict__ in, cx* __re
 template <int D> __device__ __forceinline__ void xs_fft_d(cx*, cx*, const cx*, int) {}
 XS_FFT_STAGES
 
-__device__ __forceinline__ void xs_setbound(cx* X) {
+#if XS_BVAL
+// Boundary values of p.boundfun at time tb (host table at half steps t0 + k dtr/2).
+__device__ __forceinline__ const double2* xs_bv(const XsPathArgs& P, double tb) {
+  int k = (int)llrint((tb - P.t0) / (0.5 * P.dtr));
+  k = k < 0 ? 0 : (k >= P.bval_n ? P.bval_n - 1 : k);
+  return P.bval + (size_t)k * (XS_ND * XS_F * 2);
+}
+#endif
+
+// xsetbound (Applications/SPDE/xsetbound.m:30-63): Dirichlet ends take the
+// boundary values at time tb (zero without p.boundfun values).
+__device__ __forceinline__ void xs_setbound(cx* X, const XsPathArgs* P = nullptr, double tb = 0) {
 #if XS_SETBOUND
+#if XS_BVAL
+  if (!P) return;
+  const double2* bv = xs_bv(*P, tb);
+#else
+  (void)P;
+  (void)tb;
+#endif
   for (int i = threadIdx.x; i < XS_G * XS_NS; i += blockDim.x) {
     const int g = i / XS_NS, s = i % XS_NS;
     int i1, i2, i3;
     real x, y, z;
     xs_site(s, i1, i2, i3, x, y, z);
 #pragma unroll
-    for (int f = 0; f < XS_F; ++f)
+    for (int f = 0; f < XS_F; ++f) {
+#if XS_BVAL
+      cx v;
+      if (xs_dirichlet_val(f, i1, i2, i3, bv, v)) X[(g * XS_F + f) * XS_NS + s] = v;
+#else
       if (xs_dirichlet(f, i1, i2, i3)) X[(g * XS_F + f) * XS_NS + s] = mkcx((real)0, (real)0);
+#endif
+    }
   }
   __syncthreads();
 #endif
@@ -324,9 +352,26 @@ __device__ __forceinline__ void xs_tr(cx* X, cx* T, const XsPathArgs& P, int dir
   }
 }
 
-// xprop (Applications/SPDE/xprop.m:76-104): transform, multiply by exp(L dt), inverse.
-__device__ __forceinline__ void xs_prop_tab(cx* X, cx* T, const XsPathArgs& P, const double2* __restrict__ tab) {
+// xprop (Applications/SPDE/xprop.m:76-104): transform, multiply by exp(L dt),
+// inverse; with boundary values (XS_BVAL) the xpatch.m patch at time tb is
+// taken off before and put back (with its Neumann term) after.
+__device__ __forceinline__ void xs_prop_tab(cx* X, cx* T, const XsPathArgs& P, const double2* __restrict__ tab,
+                                            double tb = 0) {
 #if XS_HAS_PROP
+#if XS_BVAL
+  const double2* bv = xs_bv(P, tb);
+  for (int i = threadIdx.x; i < XS_G * XS_F * XS_NS; i += blockDim.x) {
+    const int s = i % XS_NS, f = (i / XS_NS) % XS_F;
+    int i1, i2, i3;
+    real x, y, z;
+    xs_site(s, i1, i2, i3, x, y, z);
+    cx lp;
+    X[i] = X[i] - xs_bpatch(f, i1, i2, i3, bv, P.bda, lp);
+  }
+  __syncthreads();
+#else
+  (void)tb;
+#endif
   xs_tr<1>(X, T, P, 0);
   xs_tr<2>(X, T, P, 0);
   xs_tr<3>(X, T, P, 0);
@@ -341,16 +386,34 @@ __device__ __forceinline__ void xs_prop_tab(cx* X, cx* T, const XsPathArgs& P, c
   xs_tr<1>(X, T, P, 1);
   xs_tr<2>(X, T, P, 1);
   xs_tr<3>(X, T, P, 1);
+#if XS_BVAL
+  __syncthreads();
+  for (int i = threadIdx.x; i < XS_G * XS_F * XS_NS; i += blockDim.x) {
+    const int s = i % XS_NS, f = (i / XS_NS) % XS_F;
+    int i1, i2, i3;
+    real x, y, z;
+    xs_site(s, i1, i2, i3, x, y, z);
+    cx lp;
+    const cx pa = xs_bpatch(f, i1, i2, i3, bv, P.bda, lp);
+    X[i] = X[i] + (pa + lp);
+  }
+#endif
 #endif
   __syncthreads();
-  xs_setbound(X);
+  xs_setbound(X, &P, tb);
   __syncthreads();
 }
-__device__ __forceinline__ void xs_prop(cx* X, cx* T, const XsPathArgs& P) { xs_prop_tab(X, T, P, P.prop); }
+__device__ __forceinline__ void xs_prop(cx* X, cx* T, const XsPathArgs& P, double tb = 0) {
+  xs_prop_tab(X, T, P, P.prop, tb);
+}
 
 // dst = base + h * deriv(src, w, t), pointwise over sites (all components at once).
+// dst = base + h * deriv(src, w, t).  A drift with finite differences
+// (XS_STENCIL) reads neighbours of src, so an in-place update (dst == src)
+// writes through the transform scratch T first.
 __device__ __forceinline__ void xs_deriv_update(cx* dst, const cx* base, const cx* src, const real* W, real h, double t,
-                                                const double* prm) {
+                                                const double* prm, cx* T) {
+  cx* out = (XS_STENCIL && dst == src) ? T : dst;
   for (int i = threadIdx.x; i < XS_G * XS_NS; i += blockDim.x) {
     const int g = i / XS_NS, s = i % XS_NS;
     int i1, i2, i3;
@@ -362,14 +425,18 @@ __device__ __forceinline__ void xs_deriv_update(cx* dst, const cx* base, const c
     for (int f = 0; f < XS_F; ++f) a[f] = src[(g * XS_F + f) * XS_NS + s];
 #pragma unroll
     for (int c = 0; c < XS_NW; ++c) w[c] = W[(g * XS_NWS + c) * XS_NS + s];
-    xs_deriv(a, w, x, y, z, (real)t, prm, d);
+    xs_deriv(a, w, x, y, z, (real)t, prm, src, g, s, d);
 #pragma unroll
     for (int f = 0; f < XS_F; ++f) {
       const int j = (g * XS_F + f) * XS_NS + s;
-      dst[j] = base[j] + h * d[f];
+      out[j] = base[j] + h * d[f];
     }
   }
   __syncthreads();
+  if (out != dst) {
+    for (int i = threadIdx.x; i < XS_G * XS_F * XS_NS; i += blockDim.x) dst[i] = out[i];
+    __syncthreads();
+  }
 }
 
 __device__ __forceinline__ void xs_axpby(cx* dst, real ca, const cx* A, real cb, const cx* B) {
@@ -388,47 +455,47 @@ __device__ void xs_method(cx* A, cx* B1, cx* B2, cx* B3, cx* T, const real* W, c
 #if XS_METHOD == 0
   // MP (Applications/SDE/MP.m:10-27)
   const real h = (real)(dtr * 0.5);
-  xs_prop(A, T, P);
+  xs_prop(A, T, P, t);
   xs_copy(B1, A);
   for (int it = 0; it < XS_ITER; ++it) {
-    xs_deriv_update(A, B1, A, W, h, t + dtr * 0.5, P.params);
-    xs_setbound(A);
+    xs_deriv_update(A, B1, A, W, h, t + dtr * 0.5, P.params, T);
+    xs_setbound(A, &P, t + dtr * 0.5);
   }
   xs_axpby(A, (real)2, A, (real)-1, B1);
-  xs_prop(A, T, P);
+  xs_prop(A, T, P, t + dtr);
 #elif XS_METHOD == 1
   // RK4 (Applications/SDE/RK4.m:35-70)
   const real h = (real)(dtr * 0.5);
   xs_setbound(A);
-  xs_deriv_update(B1, A, A, W, h, t, P.params);
+  xs_deriv_update(B1, A, A, W, h, t, P.params, T);
   xs_prop(B1, T, P);
   xs_prop(A, T, P);
-  xs_deriv_update(B2, A, B1, W, h, t + dtr * 0.5, P.params);
+  xs_deriv_update(B2, A, B1, W, h, t + dtr * 0.5, P.params, T);
   xs_setbound(B2);
-  xs_deriv_update(B3, A, B2, W, (real)(2 * (dtr * 0.5)), t + dtr * 0.5, P.params);
+  xs_deriv_update(B3, A, B2, W, (real)(2 * (dtr * 0.5)), t + dtr * 0.5, P.params, T);
   xs_setbound(B3);
   for (int i = threadIdx.x; i < XS_G * XS_F * XS_NS; i += blockDim.x)
     A[i] = (B1[i] + (real)2 * B2[i] + B3[i] - A[i]) / (real)3;
   __syncthreads();
   xs_prop(A, T, P);
   xs_prop(B3, T, P);
-  xs_deriv_update(A, A, B3, W, (real)(dtr * 0.5 / 3.0), t + dtr, P.params);
+  xs_deriv_update(A, A, B3, W, (real)(dtr * 0.5 / 3.0), t + dtr, P.params, T);
   xs_setbound(A);
 #elif XS_METHOD == 2
   // Euler (Applications/SDE/Euler.m:77-81)
-  xs_deriv_update(A, A, A, W, (real)dtr, t, P.params);
+  xs_deriv_update(A, A, A, W, (real)dtr, t, P.params, T);
   xs_prop(A, T, P);
 #elif XS_METHOD == 3
   // RK2 (Applications/SDE/RK2.m:89-107): B1 holds the predictor a.
-  xs_deriv_update(B1, A, A, W, (real)dtr, t, P.params);
+  xs_deriv_update(B1, A, A, W, (real)dtr, t, P.params, T);
   xs_prop(A, T, P);
   xs_prop(B1, T, P);
-  xs_deriv_update(A, A, B1, W, (real)dtr, t + dtr, P.params);
+  xs_deriv_update(A, A, B1, W, (real)dtr, t + dtr, P.params, T);
   xs_axpby(A, (real)0.5, B1, (real)0.5, A);
 #elif XS_METHOD == 4
   // Implicit (Applications/SDE/Implicit.m:116-125)
   xs_copy(B1, A);
-  for (int it = 0; it < XS_ITER; ++it) xs_deriv_update(A, B1, A, W, (real)dtr, t + dtr, P.params);
+  for (int it = 0; it < XS_ITER; ++it) xs_deriv_update(A, B1, A, W, (real)dtr, t + dtr, P.params, T);
   xs_prop(A, T, P);
 #endif
   __syncthreads();
@@ -450,7 +517,10 @@ __device__ void xs_mp_lean(cx* A, cx* T, const XsPathArgs& P, double t, int g0, 
   const double dtr = P.dtr;
   const real h = (real)(dtr * 0.5);
   const real tm = (real)(t + dtr * 0.5);
-  xs_prop_tab(A, T, P, merged ? P.prop2 : P.prop);
+  xs_prop_tab(A, T, P, merged ? P.prop2 : P.prop, t);
+#if XS_BVAL
+  const double2* bvm = xs_bv(P, t + dtr * 0.5);  // Dirichlet values during the midpoint iterations
+#endif
   for (int i = threadIdx.x; i < XS_G * XS_NS; i += blockDim.x) {
     const int g = i / XS_NS, s = i % XS_NS;
     const int e = g0 + g;
@@ -483,12 +553,19 @@ __device__ void xs_mp_lean(cx* A, cx* T, const XsPathArgs& P, double t, int g0, 
 #pragma unroll
     for (int f = 0; f < XS_F; ++f) a0[f] = a[f] = A[(g * XS_F + f) * XS_NS + s];
     for (int it = 0; it < XS_ITER; ++it) {
-      xs_deriv(a, w, x, y, z, tm, P.params, d);
+      xs_deriv(a, w, x, y, z, tm, P.params, A, g, s, d);
 #pragma unroll
       for (int f = 0; f < XS_F; ++f) {
         a[f] = a0[f] + h * d[f];
 #if XS_SETBOUND
+#if XS_BVAL
+        {
+          cx bvv;
+          if (xs_dirichlet_val(f, i1, i2, i3, bvm, bvv)) a[f] = bvv;
+        }
+#else
         if (xs_dirichlet(f, i1, i2, i3)) a[f] = mkcx((real)0, (real)0);
+#endif
 #endif
       }
     }
@@ -496,7 +573,7 @@ __device__ void xs_mp_lean(cx* A, cx* T, const XsPathArgs& P, double t, int g0, 
     for (int f = 0; f < XS_F; ++f) A[(g * XS_F + f) * XS_NS + s] = (real)2 * a[f] - a0[f];
   }
   __syncthreads();
-  if (last) xs_prop(A, T, P);
+  if (last) xs_prop(A, T, P, t + dtr);
   __syncthreads();
 }
 #endif
@@ -723,8 +800,9 @@ __device__ void xs_resident_run(const XsPathArgs& P, int cta, int nctas) {
 #if XS_LEAN
           if (P.nc == 1 || chk == 1) {
             __syncthreads();
-            xs_mp_lean(A, T, P, t, g0, mode, draw, draw - 1, pending, false);
-            pending = true;
+            // time-dependent boundary patches (XS_BVAL) forbid merging half steps
+            xs_mp_lean(A, T, P, t, g0, mode, draw, draw - 1, pending && !XS_BVAL, XS_BVAL != 0);
+            pending = !XS_BVAL;
             t += P.dtr;
           }
 #else

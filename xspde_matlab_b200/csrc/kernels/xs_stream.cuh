@@ -205,7 +205,7 @@ __device__ __forceinline__ void xs_xpass_body(const XsStreamArgs& A) {
       for (int f = 0; f < XS_F; ++f) a0[f] = a[f] = stage[(f * XS_RX + j) * XS_RX + t];
 #pragma unroll
       for (int it = 0; it < XS_ITER; ++it) {
-        xs_deriv(a, w, x, yy, (real)0, tm, A.params, d);
+        xs_deriv(a, w, x, yy, (real)0, tm, A.params, (const cx*)nullptr, 0, 0, d);
 #pragma unroll
         for (int f = 0; f < XS_F; ++f) a[f] = a0[f] + h * d[f];
       }

@@ -239,6 +239,8 @@ struct Problem {
   int ktr[3] = {0, 0, 0};                  // space dimensions the k-space observables transform
   bool kobs = false;                       // some observable is evaluated in Fourier space
   bool stencil = false;                    // some observable uses D1/D2 (neighbouring sites)
+  bool dstencil = false;                   // the drift uses D1/D2: no fused MP iterations
+  bool bvals = false;                      // boundary values of p.boundfun supplied per pass
   std::vector<double> runtime_defaults;
   std::vector<int> bnd;  // [D][F][2]
   int D = 0, F = 1, NW = 0, NV = 0, NS = 1, E1 = 1;
@@ -279,6 +281,7 @@ void setup_problem(const xs_problem* in, Problem& P) {
   if (p.noises < 0 || p.noises > 32 || p.inrandoms < 0 || p.inrandoms > 32) raise(XS_ERR_SHAPE, "noises/inrandoms must be 0..32");
   if (p.steps < 1 || p.points[0] < 1) raise(XS_ERR_SHAPE, "points(1) and steps must be positive");
   if (p.checks < 0 || p.checks > 1) raise(XS_ERR_SHAPE, "checks(1) must be 0 or 1");
+  if (p.sequence < 0 || p.sequence > 32767) raise(XS_ERR_ARG, "sequence index must be 0..32767");
   if (p.method < 0 || p.method > 4) raise(XS_ERR_ARG, "unknown method");
   if (p.iterations < 1) raise(XS_ERR_ARG, "iterations must be >= 1");
   if (p.ipsteps < 1) raise(XS_ERR_ARG, "ipsteps must be >= 1");
@@ -336,6 +339,11 @@ void setup_problem(const xs_problem* in, Problem& P) {
       }
   }
   P.p.boundaries = nullptr;
+  if (p.boundary_values) {
+    if (P.bnd.empty()) raise(XS_ERR_ARG, "boundary values given but every boundary is periodic");
+    if (p.method != XS_METHOD_MP) raise(XS_ERR_UNSUPPORTED, "boundary values (p.boundfun) are supported with MP");
+    P.bvals = true;
+  }
   // k-space observables (xdata.m, xnft.m): one common set of periodic space dimensions
   for (auto& tr : P.obs_tr) {
     if (tr[0]) raise(XS_ERR_UNSUPPORTED, "time-spectrum observables (p.transforms{n}(1)) are not supported on the device");
@@ -537,8 +545,12 @@ void generate_functions(Problem& P, std::ostringstream& os) {
     auto g = xs::generate(fn, make_ctx(P, {Role::Field, Role::Noise, Role::Params}, false));
     if (g.len != P.F && g.len != 1)
       raise(XS_ERR_SHAPE, "p.deriv returns " + std::to_string(g.len) + " components, fields = " + std::to_string(P.F));
-    os << "__device__ __forceinline__ void xs_deriv(const cx* __restrict__ a, const real* __restrict__ w, real x, real y, real z, real t, const double* __restrict__ prm, cx* __restrict__ out) {\n";
-    os << "  (void)a; (void)w; (void)x; (void)y; (void)z; (void)t; (void)prm;\n";
+    P.dstencil = g.stencil;
+    os << "#define XS_STENCIL " << (g.stencil ? 1 : 0) << "\n";
+    os << "__device__ __forceinline__ cx xs_fd1(const cx* __restrict__ fld, int g, int s, int f, int d);\n";
+    os << "__device__ __forceinline__ cx xs_fd2(const cx* __restrict__ fld, int g, int s, int f, int d);\n";
+    os << "__device__ __forceinline__ void xs_deriv(const cx* __restrict__ a, const real* __restrict__ w, real x, real y, real z, real t, const double* __restrict__ prm, const cx* __restrict__ fld, int g, int s, cx* __restrict__ out) {\n";
+    os << "  (void)a; (void)w; (void)x; (void)y; (void)z; (void)t; (void)prm; (void)fld; (void)g; (void)s;\n";
     if (g.len == 1 && P.F > 1) {
       os << "  cx o1[1];\n  { cx* out = o1;\n" << g.code << "  }\n";
       os << "  for (int f = 0; f < " << P.F << "; ++f) out[f] = o1[0];\n";
@@ -716,6 +728,57 @@ __device__ __forceinline__ cx xs_fd2(const cx* __restrict__ fld, int g, int s, i
     }
   }
   os << "  return false;\n}\n";
+  // boundary values: Dirichlet ends (xsetbound.m, later dimensions last) and the xpatch.m patch of
+  // the last non-periodic dimension (xpatch.m recomputes it per dimension), in FP64
+  os << "#define XS_BVAL " << (P.bvals ? 1 : 0) << "\n";
+  os << "__device__ __forceinline__ bool xs_dirichlet_val(int f, int i1, int i2, int i3, const double2* __restrict__ bv, cx& v) {\n"
+        "  (void)f; (void)i1; (void)i2; (void)i3; (void)bv; (void)v; bool hit = false;\n";
+  if (P.bvals)
+    for (int d = 0; d < P.D; ++d) {
+      if (P.N[d] <= 1) continue;
+      const char* iv = d == 0 ? "i1" : d == 1 ? "i2" : "i3";
+      for (int f = 0; f < P.F; ++f)
+        for (int e = 0; e < 2; ++e)
+          if (P.bnd[(d * P.F + f) * 2 + e] == 1)
+            os << "  if (f == " << f << " && " << iv << " == " << (e ? P.N[d] - 1 : 0) << ") { const double2 q = bv["
+               << (d * P.F + f) * 2 + e << "]; v = mkcx((real)q.x, (real)q.y); hit = true; }\n";
+    }
+  os << "  return hit;\n}\n";
+  os << "__device__ __forceinline__ cx xs_bpatch(int f, int i1, int i2, int i3, const double2* __restrict__ bv, const double2* __restrict__ da, cx& lp) {\n"
+        "  (void)f; (void)i1; (void)i2; (void)i3; (void)bv; (void)da; lp = mkcx((real)0, (real)0);\n";
+  {
+    int dl = -1;
+    for (int d = 0; d < P.D; ++d) {
+      bool any = false;
+      for (int f = 0; f < P.F; ++f) any = any || P.type(d, f) != 0;
+      if (any && P.N[d] > 1) dl = d;
+    }
+    if (P.bvals && dl >= 0) {
+      const char* iv = dl == 0 ? "i1" : dl == 1 ? "i2" : "i3";
+      os << "  const double x = (double)" << iv << " * " << fmt(P.dx[dl + 1]) << ", R = " << fmt(P.p.ranges[dl + 1])
+         << ";\n";
+      for (int f = 0; f < P.F; ++f) {
+        const int t = P.type(dl, f);
+        const int o = (dl * P.F + f) * 2;
+        os << "  if (f == " << f << ") {\n    const double2 b0 = bv[" << o << "], b1 = bv[" << o + 1 << "];\n"
+           << "    (void)b0; (void)b1;\n";
+        if (t == -3)  // Neumann both ends: b0 x + x^2 db / 2, and db * da
+          os << "    const double2 db = make_double2((b1.x - b0.x) / R, (b1.y - b0.y) / R);\n"
+                "    const double2 q = da[" << dl * P.F + f << "];\n"
+                "    lp = mkcx((real)(db.x * q.x - db.y * q.y), (real)(db.x * q.y + db.y * q.x));\n"
+                "    return mkcx((real)(b0.x * x + 0.5 * x * x * db.x), (real)(b0.y * x + 0.5 * x * x * db.y));\n";
+        else if (t == -1)  // Dirichlet lower, Neumann upper: b0 + x b1
+          os << "    return mkcx((real)(b0.x + x * b1.x), (real)(b0.y + x * b1.y));\n";
+        else if (t == 1)  // Neumann lower, Dirichlet upper: b1 + (x - R) b0
+          os << "    return mkcx((real)(b1.x + (x - R) * b0.x), (real)(b1.y + (x - R) * b0.y));\n";
+        else if (t == 3)  // Dirichlet both ends: linear interpolation
+          os << "    return mkcx((real)(b0.x + x * (b1.x - b0.x) / R), (real)(b0.y + x * (b1.y - b0.y) / R));\n";
+        os << "  }\n";
+      }
+      os << "  (void)x; (void)R;\n";
+    }
+  }
+  os << "  return mkcx((real)0, (real)0);\n}\n";
 }
 
 // ---------------------------------------------------------------------------
@@ -777,7 +840,8 @@ struct xs_handle {
   CUfunction f_batch = nullptr;
   cudaStream_t stream = nullptr;
   DevBuf d_prop[2], d_prop2[2], d_tmat, d_obs, d_av, d_ain, d_aout, d_status, d_w, d_field, d_redpart, d_pstep,
-      d_params, d_gfield, d_twiddle, d_tmp, d_avm;
+      d_params, d_gfield, d_twiddle, d_tmp, d_avm, d_bval[2], d_bda[2];
+  int bval_n[2] = {0, 0};
   double pstep_dtr = -1;
   double prop_dtr[2] = {-1, -1}, prop2_dtr[2] = {-1, -1};
   // launch accounting (xs_kernel_stats)
@@ -832,12 +896,16 @@ void tile_plan(const Problem& P, bool fp64, int tl[3], int lsp[3], size_t& elems
   }
 }
 
+// MP with its midpoint iterations fused per site (noise in registers); not
+// possible when the drift reads neighbouring sites.
+bool lean_mp(const Problem& P) { return P.p.method == XS_METHOD_MP && !P.dstencil; }
+
 size_t resident_smem(const xs_handle& h, int G, int narr) {
   const Problem& P = h.P;
   size_t cxs = h.fp64 ? 16 : 8, rs = h.fp64 ? 8 : 4;
   size_t nred = std::max(P.nred, 1);
   size_t nws = std::max(P.NW, 1);
-  size_t warr = P.p.method == XS_METHOD_MP ? 0 : 2;  // MP keeps its noise in registers
+  size_t warr = lean_mp(P) ? 0 : 2;  // fused MP keeps its noise in registers
   size_t tiles = 0;
   if (narr == 0) warr = 0;  // field in device memory: the noise arrays live in the CTA's slice too
   if (narr > 0 && P.kobs) narr += 1;  // the k-space copy of the field for transformed observables
@@ -849,9 +917,9 @@ size_t resident_smem(const xs_handle& h, int G, int narr) {
          warr * (size_t)G * nws * P.NS * rs;
 }
 
-int method_arrays(int m) {
-  switch (m) {
-    case XS_METHOD_MP: return 2;  // field + transform scratch (fused midpoint iterations)
+int method_arrays(const Problem& P) {
+  switch (P.p.method) {
+    case XS_METHOD_MP: return lean_mp(P) ? 2 : 3;  // field + scratch (fused), or + a0 copy
     case XS_METHOD_RK4: return 5;
     case XS_METHOD_EULER: return 2;
     case XS_METHOD_RK2: return 3;
@@ -862,7 +930,7 @@ int method_arrays(int m) {
 void plan_resident(xs_handle& h, int total_traj) {
   const Problem& P = h.P;
   ResidentPlan rp;
-  rp.narr = method_arrays(P.p.method);
+  rp.narr = method_arrays(P);
   const size_t limit = 200 * 1024;
   if (resident_smem(h, 1, rp.narr) > limit) {
     // lattice beyond shared memory: one trajectory per CTA, field, scratch and noise arrays in device memory
@@ -993,6 +1061,7 @@ std::string stream_blocker(const Problem& P) {
     if (o.spatial && !o.gen.reductions.empty()) return "site observables that use Int/Ave are not streamed";
   if (P.kobs) return "k-space observables (p.transforms) are not streamed";
   if (P.stencil) return "observables with D1/D2 finite differences are not streamed";
+  if (P.dstencil) return "drifts with D1/D2 finite differences are not streamed";
   return "";
 }
 
@@ -1084,7 +1153,9 @@ void build_source(xs_handle& h) {
   Problem& P = h.P;
   std::ostringstream fns;
   generate_functions(P, fns);  // fixes P.nred / nout_* before the launch plan
-  const bool fits = resident_smem(h, 1, method_arrays(P.p.method)) <= 200 * 1024;
+  if (P.bvals && (P.stencil || P.dstencil))
+    raise(XS_ERR_UNSUPPORTED, "D1/D2 use zero boundary values on the device: not combined with p.boundfun values");
+  const bool fits = resident_smem(h, 1, method_arrays(P)) <= 200 * 1024;
   const std::string why = stream_blocker(P);
   // too large for shared memory: the streaming path when it covers the problem, else the resident
   // path with the field in device memory (MP)
@@ -1115,8 +1186,8 @@ void build_source(xs_handle& h) {
   emit_common_header(h, os);
   os << "#define XS_G " << h.rp.G << "\n#define XS_THREADS " << h.rp.threads << "\n#define XS_NARR " << h.rp.narr << "\n";
   os << "#define XS_KARR " << (P.kobs ? 1 : 0) << "\n";
-  os << "#define XS_LEAN " << (P.p.method == XS_METHOD_MP ? 1 : 0) << "\n#define XS_WARR "
-     << (P.p.method == XS_METHOD_MP ? 0 : 2) << "\n#define XS_GFIELD " << (h.rp.gfield ? 1 : 0) << "\n";
+  os << "#define XS_LEAN " << (lean_mp(P) ? 1 : 0) << "\n#define XS_WARR " << (lean_mp(P) ? 0 : 2)
+     << "\n#define XS_GFIELD " << (h.rp.gfield ? 1 : 0) << "\n";
   os << "#define XS_SMEM_BYTES " << h.rp.smem << "\n";
   {
     std::string stages;
@@ -1328,6 +1399,10 @@ struct PathArgsHost {
   const double* params;
   void* gfield;
   const void* prop2;
+  const void* bval;
+  const void* bda;
+  int bval_n;
+  int pad3;
 };
 
 size_t av_stride(const Problem& P) { return (size_t)P.nout_site * P.NS + P.nout_scalar; }
@@ -1377,7 +1452,7 @@ int resident_grid(xs_handle& h, CUfunction f, int nctas) {
   CUDA_CHECK(cudaGetDevice(&dev));
   CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   cu_check(driver().occupancy(&occ, f, h.rp.threads, h.rp.smem), "occupancy");
-  const size_t warr = h.P.p.method == XS_METHOD_MP ? 0 : 2;
+  const size_t warr = lean_mp(h.P) ? 0 : 2;
   const size_t slice = (size_t)(h.rp.narr + (h.P.kobs ? 1 : 0)) * h.rp.G * h.P.F * h.P.NS * (h.fp64 ? 16 : 8) +
                        warr * h.rp.G * std::max(h.P.NW, 1) * h.P.NS * (h.fp64 ? 8 : 4);
   const int l2 = (int)std::max<size_t>(1, (96u << 20) / slice);
@@ -1407,7 +1482,7 @@ void launch_resident(xs_handle& h, int first_block, int nblocks, int nc, const v
   a.checks = P.p.checks;
   a.npoints = npts;
   a.steps = P.p.steps;
-  a.seq = 0;
+  a.seq = P.p.sequence;
   a.seed = (unsigned)(P.p.seed & 0xffffffffu);
   a.wscale = std::sqrt(P.nscale * P.noisefactor);  // xnoise.m:32
   a.vscale = std::sqrt(P.noisefactor);              // xrandom.m:23
@@ -1415,6 +1490,13 @@ void launch_resident(xs_handle& h, int first_block, int nblocks, int nc, const v
   a.t0 = P.p.origins[0];
   a.prop = ensure_prop(h, nc);
   a.prop2 = ensure_prop2(h, nc);
+  if (P.bvals) {
+    const int slot = nc == 2 ? 1 : 0;
+    if (!h.bval_n[slot]) raise(XS_ERR_ARG, "boundary values of this check pass were not set (xs_set_boundary_values)");
+    a.bval = h.d_bval[slot].p;
+    a.bda = h.d_bda[slot].p;
+    a.bval_n = h.bval_n[slot];
+  }
   a.tmat = h.d_tmat.p;
   for (int i = 0; i < 4; ++i) a.tmat_off[i] = h.tmat_off[i];
   a.a_in = a_in_dev;
@@ -1487,7 +1569,7 @@ void launch_stream(xs_handle& h, int first_block, int nblocks, int nc, const voi
   a.ntraj = total;
   a.ens1 = P.E1;
   a.block0 = first_block;
-  a.seq = 0;
+  a.seq = P.p.sequence;
   a.seed = (unsigned)(P.p.seed & 0xffffffffu);
   a.draw0 = 0;
   a.draw1 = -1;
@@ -1798,6 +1880,40 @@ XS_API xs_status xs_sync(xs_handle* h) {
 // Resident path with its observable partial sums in the library's fixed
 // device scratch (xs_noalloc.cu) instead of handle-owned memory.  Uses only
 // tables the handle already holds; allocates nothing.
+XS_API xs_status xs_set_boundary_values(xs_handle* h, int nc, int ntimes, const double* values) {
+  return guard([&]() -> xs_status {
+    if (!h || (nc != 1 && nc != 2) || ntimes < 1 || !values) raise(XS_ERR_ARG, "bad arguments to xs_set_boundary_values");
+    const Problem& P = h->P;
+    if (!P.bvals) raise(XS_ERR_ARG, "the problem was created without boundary_values");
+    load_module(*h);
+    const int slot = nc == 2 ? 1 : 0;
+    const size_t n = (size_t)ntimes * P.D * P.F * 2;
+    h->d_bval[slot].ensure(n * 16);
+    CUDA_CHECK(cudaMemcpy(h->d_bval[slot].p, values, n * 16, cudaMemcpyHostToDevice));
+    // da of the Neumann patch (xpropfactor.m:45-50): -(L(k1) - L(k0)) dt / pi^2 R^2 along each dimension
+    std::vector<cd> da((size_t)std::max(P.D, 1) * P.F, cd(0, 0));
+    if (P.has_linear) {
+      const double dt = pass_dtr(P, nc) / P.p.ipsteps;
+      const double fda = dt / (M_PI * M_PI);
+      int sd = 1;
+      for (int d = 0; d < P.D; ++d) {
+        for (int f = 0; f < P.F; ++f) {
+          const int c = P.Lc > 1 ? f : 0;
+          if (P.N[d] > 1) {
+            const cd L1 = P.L[(size_t)c * P.NS], L2 = P.L[(size_t)c * P.NS + sd];
+            da[(size_t)d * P.F + f] = -(L2 - L1) * fda * P.p.ranges[d + 1] * P.p.ranges[d + 1];
+          }
+        }
+        sd *= P.N[d];
+      }
+    }
+    h->d_bda[slot].ensure(da.size() * 16);
+    CUDA_CHECK(cudaMemcpy(h->d_bda[slot].p, da.data(), da.size() * 16, cudaMemcpyHostToDevice));
+    h->bval_n[slot] = ntimes;
+    return XS_OK;
+  });
+}
+
 XS_API xs_status xs_run_path_device_noalloc(xs_handle* h, int first_block, int nblocks, int nc, double* av_dev,
                                             void* stream) {
   return guard([&]() -> xs_status {
@@ -1808,6 +1924,7 @@ XS_API xs_status xs_run_path_device_noalloc(xs_handle* h, int first_block, int n
       raise(XS_ERR_UNSUPPORTED, "xs_run_path_device_noalloc covers problems on the resident path only");
     if (h->rp.gfield)
       raise(XS_ERR_UNSUPPORTED, "xs_run_path_device_noalloc needs the field in shared memory (it would allocate slices)");
+    if (h->P.bvals) raise(XS_ERR_UNSUPPORTED, "xs_run_path_device_noalloc does not take boundary values");
     if (nc == 2 && !P.p.checks) raise(XS_ERR_ARG, "coarse pass requested without checks");
     const int slot = nc == 2 ? 1 : 0;
     if (!h->loaded || !h->d_prop[slot].p || (P.has_linear && h->prop_dtr[slot] != pass_dtr(P, nc)))
@@ -1837,7 +1954,7 @@ XS_API xs_status xs_run_path_device_noalloc(xs_handle* h, int first_block, int n
     a.checks = P.p.checks;
     a.npoints = npts;
     a.steps = P.p.steps;
-    a.seq = 0;
+    a.seq = P.p.sequence;
     a.seed = (unsigned)(P.p.seed & 0xffffffffu);
     a.wscale = std::sqrt(P.nscale * P.noisefactor);
     a.vscale = std::sqrt(P.noisefactor);
@@ -2016,7 +2133,8 @@ xs_status export_normals(xs_handle* h, bool random, int block, int draw, double 
     const size_t n = (size_t)nc * P.NS * P.E1;
     if (n == 0) return XS_OK;
     h->d_w.ensure(n * 8);
-    unsigned blk = (unsigned)block, dr = (unsigned)draw, seq = 0, seed = (unsigned)(P.p.seed & 0xffffffffu);
+    unsigned blk = (unsigned)block, dr = (unsigned)draw, seq = (unsigned)P.p.sequence,
+             seed = (unsigned)(P.p.seed & 0xffffffffu);
     int ens1 = P.E1;
     void* dp = h->d_w.p;
     void* params[] = {&dp, &ens1, &blk, &dr, &seq, &seed, &scale};
@@ -2051,6 +2169,7 @@ XS_API xs_status xs_step(xs_handle* h, double* a_inout, const double* w, double 
   return guard([&]() -> xs_status {
     if (!h || !a_inout || !(dtr > 0)) raise(XS_ERR_ARG, "bad arguments to xs_step");
     if (h->kind != 1) raise(XS_ERR_UNSUPPORTED, "xs_step covers problems on the resident path only");
+    if (h->P.bvals) raise(XS_ERR_UNSUPPORTED, "xs_step does not take boundary values");
     load_module(*h);
     const Problem& P = h->P;
     const size_t ntraj = (size_t)P.E1;
@@ -2263,7 +2382,7 @@ void batch_drop_graph(xs_batch& b) {
 // divides every item's trajectory count and fits shared memory), threads.
 std::vector<std::pair<int, int>> tile_candidates(const BatchVariant& v, const xs_handle& proto) {
   const Problem& P = proto.P;
-  const int narr = method_arrays(P.p.method);
+  const int narr = method_arrays(P);
   if (resident_smem(proto, 1, narr) > 200 * 1024)  // field in device memory: one trajectory per CTA
     return {{1, 256}, {1, 512}, {1, 1024}};
   std::vector<int> Gs;  // divisors of every item's trajectory count, ascending
@@ -2310,7 +2429,7 @@ void variant_tables(xs_batch& b, BatchVariant& v, int steps_cap, int points_cap,
     it.ntraj = ntraj_of(P);
     it.steps = steps_cap > 0 ? std::min(P.p.steps, steps_cap) : P.p.steps;
     it.npoints = points_cap > 0 ? std::min(P.p.points[0], points_cap) : P.p.points[0];
-    it.seq = 0;
+    it.seq = P.p.sequence;
     it.seed = (unsigned)(P.p.seed & 0xffffffffu);
     it.block0 = 0;
     it.nunits = it.ntraj / v.G;
@@ -2674,6 +2793,7 @@ XS_API xs_status xs_batch_create(const xs_problem* items, int nitems, xs_batch**
         if (items[i].path_kind < 0 || items[i].path_kind > 2) raise(XS_ERR_ARG, "path_kind must be 0, 1 or 2");
         h.path_kind = items[i].path_kind;
         if (items[i].checks) raise(XS_ERR_UNSUPPORTED, "batch items run the fine pass only (checks = 0)");
+        if (items[i].boundary_values) raise(XS_ERR_UNSUPPORTED, "batch items take no boundary values");
         if (items[i].ensembles[1] != 1 || items[i].ensembles[2] != 1)
           raise(XS_ERR_UNSUPPORTED, "a batch item is one ensemble block (ensembles(2) = ensembles(3) = 1)");
         h.force_G = 1;

@@ -1025,8 +1025,6 @@ struct Gen {
         if (f == "D1" || f == "D2") {
           // D1/D2(a[, d], p) (Applications/SPDE/D1.m, D2.m): central differences of the field along
           // dimension d (2 = x), with the boundary rules of the field's boundary types
-          if (!ctx.allow_reduce)
-            throw GrammarError(f + " (finite differences) is supported in observe functions only on the device");
           const size_t na = n->kids.size() - 1;
           if (na != 2 && na != 3) throw GrammarError(f + " on the device takes (a, p) or (a, d, p)");
           int dd = 2;

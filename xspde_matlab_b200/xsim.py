@@ -169,6 +169,16 @@ def xpreferences(inputs):
         p.xc = [p.origins[d] + np.arange(p.points[d]) * p.dx[d] for d in range(nd)]
         p.kc = [(np.arange(p.points[d]) - p.points[d] // 2) * p.dk[d] for d in range(nd)]
         p.kc[0] = (np.arange(p.points[0]) - p.points[0] // 2) * (2 * math.pi / (p.ranges[0] + p.dt))
+        # lattice coordinates for host-side functions (transfer): p.r{d}, p.x, p.y, p.z shaped
+        # [1, ..., N_d, ..., 1] like a field array (xgrid.m)
+        p.r = [None] * max(4, nd)
+        for d in range(1, nd):
+            sh = [1] * (nd + 1)
+            sh[d] = p.points[d]
+            p.r[d] = p.xc[d].reshape(sh)
+        p.x, p.y, p.z = p.r[1], p.r[2], p.r[3]
+        p.sequence = s
+        p.transfer = p.get("transfer", None)
         out.append(p)
         origin = p.origins[0] + p.ranges[0]
     return out
@@ -220,6 +230,8 @@ def make_problem(p, path_kind=0, runtime_params=False):
         pr.param_values = vals
     pr.path_kind = path_kind
     pr.runtime_params = 1 if runtime_params else 0
+    pr.sequence = int(p.get("sequence", 0) or 0)
+    pr.boundary_values = 1 if callable(p.get("boundfun", None)) else 0
     if any(any(t[1:]) or t[0] for t in p.transforms):
         flags = []
         for t in p.transforms:
@@ -261,10 +273,37 @@ class GpuPath:
         P = self.p
         return [(ln, P.points[0]) + (tuple(P.space) if sp else ()) for ln, sp in self.obs]
 
+    def _boundary_values(self, nc):
+        """p.boundfun(a, c, d, p) tabulated at every half step t0 + k dtr/2 of check
+        pass nc (the times xprop/xsetbound query in MP, Applications/SDE/MP.m:11-26),
+        as complex [times][space dims][fields][2]; handed to the device once per pass."""
+        cache = self.__dict__.setdefault("_bv_done", set())
+        if nc in cache:
+            return
+        P = self.p
+        fine = P.checks[0] and nc != 2
+        dtr = P.dt / (2 * P.steps[0]) if fine else P.dt / P.steps[0]
+        nsteps = (P.points[0] * P.steps[0] - 1) * (2 if fine else 1)
+        ntimes = 2 * nsteps + 3
+        nd = P.dimensions - 1
+        tab = np.zeros((ntimes, nd, P.fields, 2), dtype=np.complex128)
+        q = P.copy()
+        for k in range(ntimes):
+            q.t = P.origins[0] + k * dtr / 2
+            for d in range(nd):
+                if P.boundaries is not None and np.any(np.asarray(P.boundaries[d]) != 0):
+                    b = np.asarray(P.boundfun(None, 0, d + 1, q), dtype=np.complex128)
+                    tab[k, d] = np.broadcast_to(b.reshape(-1, 2) if b.size >= 2 else b, (P.fields, 2))
+        tab = np.ascontiguousarray(tab)
+        _lib.check(_lib.lib().xs_set_boundary_values(self.h, nc, ntimes, tab.ctypes.data))
+        cache.add(nc)
+
     def run_path(self, first_block, nblocks, nc, a_in=None, a_out=False):
         """p.path for blocks [first_block, first_block+nblocks): returns
         (av, a) with av[b][o] complex arrays of shape av_shapes()[o]."""
         P = self.p
+        if callable(P.get("boundfun", None)):
+            self._boundary_values(nc)
         buf = np.empty(nblocks * self.per_block, dtype=np.float64)
         ain = None
         if a_in is not None:
@@ -391,6 +430,16 @@ def _ensembles(inp, paths, rank=0, size=1, reduce=None):
             prev = None
             for s, p in enumerate(inp):
                 a_in = prev if s > 0 else None
+                if s > 0 and p.transfer is not None:
+                    # p.transfer(b, v, p) on the host between the two device paths (xensemble.m:62)
+                    if p.inrandoms > 0:
+                        v = np.concatenate([paths[s].random(b0 + b) for b in range(nbk)], axis=-1)
+                    else:
+                        v = np.zeros([0] + list(p.space) + [p.ensembles[0] * nbk])
+                    shape = [p.fields] + list(p.space) + [p.ensembles[0] * nbk]
+                    r = np.asarray(p.transfer(prev, v, p), dtype=complex)
+                    r = r.reshape(r.shape + (1,) * (len(shape) - r.ndim))
+                    a_in = np.asfortranarray(np.broadcast_to(r, shape))
                 av, prev = paths[s].run_path(b0, nbk, nc, a_in=a_in, a_out=(s + 1 < len(inp)))
                 for b in range(nbk):
                     for o in range(len(p.output)):
@@ -435,8 +484,6 @@ def xsim(*inputs, path_kind=0):
     inp = xpreferences(list(inputs))
     paths = [GpuPath(p, path_kind) for p in inp]
     for s, p in enumerate(inp):
-        if s > 0 and "transfer" in p and p.transfer is not None:
-            raise _lib.XsError(-9, "p.transfer functions are not supported on the device path")
         shapes = paths[s].av_shapes()
         O = [np.zeros(x) for x in shapes]
         p.gpoints = []
