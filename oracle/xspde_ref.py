@@ -876,22 +876,43 @@ def xpath(a, nc, p):
     method = METHODS[p.method]
     w = None
     p.draw = 0
+    spectrum = any(tr[0] for tr in p.transforms)                         # xpreferences.m:246
+    aft = np.zeros((P1 * S,) + np.shape(a), dtype=complex) if spectrum else None
+    n1 = -1
     for n in range(P1):                                                  # :137
         for step in range(S):                                            # :138
+            n1 += 1                                                      # :27
             if n > 0 or step > 0 or P1 == 1:                             # :140
                 for checks in range(p.checks[0] + 1):                    # :141
                     p.draw += 1
                     w = p.noisegen(w, nc, p.nscale, p)                   # :142
                     if nc == 1 or checks == 1:                           # :143
                         a = method(a, w, p)                              # :150
+                        if spectrum:                                     # :46-54
+                            if checks == 1 and nc == 1:
+                                aft[n1] = (a + aft[n1]) / 2
+                            else:
+                                aft[n1] = a
                         w = None                                         # :164
                         p.t = p.t + p.dtr                                # :165
+            elif spectrum:                                               # :64-68
+                aft[n1] = a
             if step == 0:                                                # :181
                 for o in p.averages:
                     if not p.transforms[o][0]:
                         r = xdata(a, o, p)
                         L = p.d_av[o][0]
                         av[o][:, n] = freshape(r, [L] + list(p.d_av[o][2:]))
+    if spectrum:                                                         # :90-106
+        nt = P1 * S
+        f = np.fft.fftshift(np.fft.ifft(aft, axis=0) * p.fsc, axes=0)   # ifft(aft, P1 S, 2) * fsc, fftshift
+        sel = np.arange(P1) - P1 // 2 + nt // 2                          # specpts = plotpts + floor(S P1/2) + 1
+        for n in range(P1):
+            for o in p.averages:
+                if p.transforms[o][0]:
+                    r = xdata(f[sel[n]], o, p)
+                    L = p.d_av[o][0]
+                    av[o][:, n] = freshape(r, [L] + list(p.d_av[o][2:]))
     return a, av
 
 

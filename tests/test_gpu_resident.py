@@ -232,3 +232,59 @@ def test_boundary_values_all_types_stochastic_fp64():
              initial=lambda v, p: 1 + 0.2 * np.cos(p.x) + 0.1 * v, linear=lambda p: (0.4 + 0.2j) * p.Dx ** 2,
              observe=[lambda a, p: a, lambda a, p: X.Int(abs(a) ** 2, p)])
     _compare(g, o, [0, 1], [1, 2], FP64_TOL)
+
+
+@pytest.mark.parametrize("method", ["MP", "RK4"])
+def test_time_spectrum_sde_fp64(method):
+    """Observables on the time spectrum of the field (p.transforms{n}(1),
+    Simulator/xpath.m:46-106) beside a time-domain one; both check passes (the fine
+    pass records the mean of its two half steps)."""
+    base = dict(dimensions=1, points=[24], ranges=[6.0], steps=3, ensembles=[32, 2, 1], noises=2, method=method,
+                checks=1, transforms=[[0], [1], [1]])
+    g = dict(base, initial="@(w,p) (w(1,:)+1i*w(2,:))/sqrt(2)", deriv="@(a,w,p) (0.5i-1)*a + w(1,:)+1i*w(2,:)",
+             observe=["@(a,p) a.*conj(a)", "@(a,p) a.*conj(a)", "@(a,p) a"])
+    o = dict(base, initial=lambda w, p: (w[0:1] + 1j * w[1:2]) / np.sqrt(2),
+             deriv=lambda a, w, p: (0.5j - 1) * a + w[0:1] + 1j * w[1:2],
+             observe=[lambda a, p: a * np.conj(a), lambda a, p: a * np.conj(a), lambda a, p: a])
+    _compare(g, o, [0, 1], [1, 2], FP64_TOL)
+
+
+def test_time_spectrum_sde_fp32_bound():
+    base = dict(dimensions=1, points=[24], ranges=[6.0], steps=3, ensembles=[32, 2, 1], noises=2, method="MP",
+                checks=1, transforms=[[0], [1]])
+    g = dict(base, precision="fp32", initial="@(w,p) (w(1,:)+1i*w(2,:))/sqrt(2)",
+             deriv="@(a,w,p) -a + w(1,:)+1i*w(2,:)", observe=["@(a,p) a.*conj(a)", "@(a,p) a.*conj(a)"])
+    o = dict(base, initial=lambda w, p: (w[0:1] + 1j * w[1:2]) / np.sqrt(2),
+             deriv=lambda a, w, p: -a + w[0:1] + 1j * w[1:2],
+             observe=[lambda a, p: a * np.conj(a), lambda a, p: a * np.conj(a)])
+    _compare(g, o, [0, 1], [1, 2], FP32_TOL)
+
+
+def test_time_spectrum_pde_kspace_integral_fp64():
+    """Time spectrum of a 1D stochastic NLS field: the (w, x) spectrum, the (w, k)
+    spectrum (time and space transforms together) and the integral of the (w, x)
+    spectrum."""
+    base = dict(dimensions=2, points=[10, 32], ranges=[2.0, 10.0], steps=3, ensembles=[4, 2, 1], noises=2,
+                method="MP", checks=1, transforms=[[0, 0], [1, 0], [1, 1], [1, 0]])
+    g = dict(base, deriv="@(a,w,p) 1i*a.*conj(a).*a + 0.1*(w(1,:)+1i*w(2,:))", initial="@(v,p) exp(-p.x.^2)",
+             linear="@(p) 1i*p.Dx.^2",
+             observe=["@(a,p) a.*conj(a)", "@(a,p) a.*conj(a)", "@(a,p) a.*conj(a)", "@(a,p) Int(a.*conj(a),p)"])
+    o = dict(base, deriv=lambda a, w, p: 1j * a * np.conj(a) * a + 0.1 * (w[0:1] + 1j * w[1:2]),
+             initial=lambda v, p: np.exp(-p.x ** 2), linear=lambda p: 1j * p.Dx ** 2,
+             observe=[lambda a, p: a * np.conj(a)] * 3 + [lambda a, p: X.Int(a * np.conj(a), p)])
+    _compare(g, o, [0, 1], [1, 2], FP64_TOL)
+
+
+def test_time_spectrum_field_in_device_memory_fp64():
+    """128 x 128 FP64 lattice (field in per-CTA device-memory slices) with a
+    time-spectrum observable."""
+    base = dict(dimensions=3, points=[4, 128, 128], ranges=[0.3, 20.0, 20.0], steps=2, ensembles=[2, 1, 1],
+                noises=2, method="MP", checks=1, transforms=[[0, 0, 0], [1, 0, 0]])
+    g = dict(base, deriv="@(a,w,p) 1i*abs(a).^2.*a + 0.02*(w(1,:)+1i*w(2,:))",
+             initial="@(v,p) exp(-(p.x.^2+p.y.^2)/8)", linear="@(p) 0.5i*(p.Dx.^2+p.Dy.^2)",
+             observe=["@(a,p) abs(a).^2", "@(a,p) abs(a).^2"])
+    o = dict(base, deriv=lambda a, w, p: 1j * abs(a) ** 2 * a + 0.02 * (w[0:1] + 1j * w[1:2]),
+             initial=lambda v, p: np.exp(-(p.x ** 2 + p.y ** 2) / 8),
+             linear=lambda p: 0.5j * (p.Dx ** 2 + p.Dy ** 2),
+             observe=[lambda a, p: abs(a) ** 2, lambda a, p: abs(a) ** 2])
+    _compare(g, o, [0], [1, 2], FP64_TOL)

@@ -162,3 +162,30 @@ def test_gpu_xsim_two_sequences_stochastic_matches_oracle():
     for s in range(2):
         for a, b in zip(dg[s], do[s]):
             assert np.allclose(np.asarray(a), np.asarray(b), rtol=1e-9, atol=1e-12)
+
+
+def test_gpu_xsim_equilibrium_spectrum():
+    """Examples/SDE_1D/Equilibrium.m through xsim: the time-domain and spectral
+    observables, errors and frequency axis match the oracle's xsim, and the
+    spectrum meets the example's comparison T / (pi (1 + w^2))."""
+    from xspde_matlab_b200 import xsim
+    base = dict(points=[200], steps=2, ranges=[25.0], seed=241, noises=2, ensembles=[50, 1, 12],
+                transforms=[[0], [1]])
+    g = dict(base, initial="@(w,p) (w(1,:)+1i*w(2,:))/sqrt(2)", deriv="@(a,w,p) -a + w(1,:)+1i*w(2,:)",
+             observe=["@(a,p) a.*conj(a)", "@(a,p) a.*conj(a)"])
+    o = dict(base, initial=lambda w, p: (w[0] + 1j * w[1]) / np.sqrt(2), deriv=lambda a, w, p: -a + w[0] + 1j * w[1],
+             observe=[lambda a, p: a * np.conj(a), lambda a, p: a * np.conj(a)])
+    eg, dg, ig = xsim(g)
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore", RuntimeWarning)
+        eo, do, io = X.xsim(o)
+    keep = [i for i in range(len(eo)) if i != 5]
+    assert np.allclose(np.asarray(eg)[keep], np.asarray(eo)[keep], rtol=1e-9, atol=1e-14)
+    for a, b in zip(dg[0], do[0]):
+        assert np.allclose(np.asarray(a), np.asarray(b), rtol=1e-9, atol=1e-12)
+    w = io[0].kc[0]
+    assert np.allclose(ig[0].kc[0], w)
+    spec, err = np.real(dg[0][1][:, 0]), np.real(dg[0][1][:, 2])
+    exact = 25.0 / (np.pi * (1 + w ** 2))
+    sel = np.abs(w) < 4
+    assert np.all(np.abs(spec[sel] - exact[sel]) < 5 * err[sel] + 0.02 * exact[sel])

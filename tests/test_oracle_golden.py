@@ -40,3 +40,50 @@ def test_philox_normals_moments():
     assert abs(z.mean()) < 0.01
     assert abs(z.var() - 1) < 0.01
     assert abs(np.mean(z ** 4) - 3) < 0.05
+
+
+def test_time_spectrum_exact_geometric_series():
+    """p.transforms{n}(1) (Simulator/xpath.m:90-106): a linear ODE stepped by RK4 is
+    a_j = r^j with r the RK4 amplification 1 + z + z^2/2 + z^3/6 + z^4/24, z = lambda dtr,
+    so the recorded spectrum fsc/Nt sum_j r^j exp(2 pi i m j / Nt) at m = n - floor(P1/2)
+    has the closed form fsc/Nt (1 - (r q)^Nt) / (1 - r q), q = exp(2 pi i m / Nt)."""
+    lam = 2j - 0.3
+    o = dict(dimensions=1, points=[33], ranges=[20.0], steps=4, ensembles=[2, 1, 1], noises=1, method="RK4",
+             checks=0, deriv=lambda a, w, p: lam * a, initial=lambda v, p: 1 + 0 * v,
+             observe=[lambda a, p: a, lambda a, p: a], transforms=[[1], [0]])
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore", RuntimeWarning)
+        e, data, inp = X.xsim(o)
+    p = inp[0]
+    P1, S = 33, 4
+    nt = P1 * S
+    dt = 20.0 / (P1 - 1)
+    z = lam * dt / S
+    r = 1 + z + z ** 2 / 2 + z ** 3 / 6 + z ** 4 / 24
+    dw = 2 * np.pi / (20.0 + dt)
+    fsc = np.sqrt(2 * np.pi) / dw
+    m = np.arange(P1) - P1 // 2
+    q = np.exp(2j * np.pi * m / nt)
+    want = fsc / nt * (1 - (r * q) ** nt) / (1 - r * q)
+    got = data[0][0][:, 0]
+    assert np.max(np.abs(got - np.real(want))) < 1e-11 * np.max(np.abs(want))
+    assert np.allclose(p.kc[0], m * dw)
+    assert np.allclose(data[0][1][:, 0], np.real(r ** (S * np.arange(P1))), atol=1e-12)
+
+
+def test_time_spectrum_equilibrium_known_answer():
+    """Examples/SDE_1D/Equilibrium.m: the Ornstein-Uhlenbeck spectrum |a(w)|^2 equals
+    its comparison T / (pi (1 + w^2)) within the sampling error, and |a(t)|^2 = 1."""
+    o = dict(points=[200], steps=2, ranges=[25.0], seed=241, noises=2, ensembles=[50, 1, 12],
+             initial=lambda w, p: (w[0] + 1j * w[1]) / np.sqrt(2), deriv=lambda a, w, p: -a + w[0] + 1j * w[1],
+             observe=[lambda a, p: a * np.conj(a), lambda a, p: a * np.conj(a)], transforms=[[0], [1]])
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore", RuntimeWarning)
+        e, data, inp = X.xsim(o)
+    w = inp[0].kc[0]
+    spec, err = np.real(data[0][1][:, 0]), np.real(data[0][1][:, 2])
+    exact = 25.0 / (np.pi * (1 + w ** 2))
+    sel = np.abs(w) < 4
+    assert np.all(np.abs(spec[sel] - exact[sel]) < 5 * err[sel] + 0.02 * exact[sel])
+    tdom = np.real(data[0][0][:, 0])
+    assert np.all(np.abs(tdom - 1) < 5 * np.real(data[0][0][:, 2]) + 0.02)

@@ -41,6 +41,12 @@ struct XsPathArgs {
   const double2* bda;   // XS_BVAL: [ND][F] the da term of the Neumann patch (xpropfactor.m:45-50)
   int bval_n;
   int pad3;
+  cx* aft;              // XS_SPEC: per trajectory tile [nt + npoints][G*F*NS]: the field at every
+                        // step count, then its spectrum at the output frequencies
+  const double2* twt;   // XS_SPEC: exp(2 pi i k / nt), k < nt
+  int nt;               // XS_SPEC: points(1) x steps(1)
+  int pad4;
+  double fscn;          // XS_SPEC: p.fsc / nt
 };
 
 // XS_GFIELD: the lattice is too large for shared memory, so each CTA keeps its
@@ -49,6 +55,7 @@ struct XsPathArgs {
 // only the reduction scratch in shared memory.  The code is the same; only the
 // arrays' home differs (__syncthreads orders global accesses within a CTA).
 #define XS_FARR (XS_GFIELD ? 0 : XS_NARR)
+#define XS_NOMERGE (XS_BVAL || XS_SPEC)
 // complex elements of one CTA's slice: the field arrays, then (methods other
 // than MP) the two noise arrays of reals
 #define XS_GSLICE ((size_t)(XS_NARR + XS_KARR) * XS_G * XS_F * XS_NS + (size_t)XS_WARR * XS_G * XS_NWS * XS_NS * sizeof(real) / sizeof(cx))
@@ -605,8 +612,10 @@ __device__ __forceinline__ void xs_noise(real* W, real* Wp, int mode, int draw, 
 // K (XS_KOBS): the field Fourier-transformed along the flagged dimensions for
 // the observables with p.transforms (xnft.m: fft along each, times dx/sqrt(2 pi));
 // T is the transform scratch, free at output times.
+// phase 0 writes the slots of observables on the field at the output time, phase 1
+// (XS_SPEC) those on its time spectrum; A is then the spectral field of output n.
 __device__ void xs_observe(const cx* A, cx* RED, int n, double t, const XsPathArgs& P, double* wsum, int cta,
-                           int nctas, cx* K, cx* T) {
+                           int nctas, cx* K, cx* T, int phase) {
   double2* out = P.obs + ((size_t)n * nctas + cta) * XS_OBS_STRIDE;
 #if XS_KOBS
   for (int i = threadIdx.x; i < XS_G * XS_F * XS_NS; i += blockDim.x) K[i] = A[i];
@@ -675,7 +684,8 @@ __device__ void xs_observe(const cx* A, cx* RED, int n, double t, const XsPathAr
       for (int k = 0; k < XS_NOUT_SITE; ++k) { sr[k] += (double)o[k].re; si[k] += (double)o[k].im; }
     }
 #pragma unroll
-    for (int k = 0; k < XS_NOUT_SITE; ++k) out[(size_t)k * XS_NS + s] = make_double2(sr[k], si[k]);
+    for (int k = 0; k < XS_NOUT_SITE; ++k)
+      if (xs_ospec_site[k] == phase) out[(size_t)k * XS_NS + s] = make_double2(sr[k], si[k]);
   }
 #endif
 #if XS_NOUT_SCALAR > 0
@@ -688,12 +698,65 @@ __device__ void xs_observe(const cx* A, cx* RED, int n, double t, const XsPathAr
       for (int k = 0; k < XS_NOUT_SCALAR; ++k) { sr[k] += (double)o[k].re; si[k] += (double)o[k].im; }
     }
     for (int k = 0; k < XS_NOUT_SCALAR; ++k)
-      out[(size_t)XS_NOUT_SITE * XS_NS + k] = make_double2(sr[k], si[k]);
+      if (xs_ospec_scalar[k] == phase) out[(size_t)XS_NOUT_SITE * XS_NS + k] = make_double2(sr[k], si[k]);
   }
 #endif
 #undef XS_LOAD_AK
   __syncthreads();
 }
+
+#if XS_SPEC
+// Time spectrum (Simulator/xpath.m:46-68, 90-106).  Row n1 of the tile's record holds
+// the field after step count n1 (the initial field at n1 = 0); the fine pass of a
+// checked run stores the mean of its two half steps.
+__device__ void xs_spec_store(const cx* A, const XsPathArgs& P, int cta, int n1, bool avg) {
+  constexpr int GF = XS_G * XS_F * XS_NS;
+  cx* S = P.aft + ((size_t)cta * (P.nt + P.npoints) + n1) * GF;
+  __syncthreads();
+  for (int i = threadIdx.x; i < GF; i += blockDim.x) S[i] = avg ? (A[i] + S[i]) * (real)0.5 : A[i];
+  __syncthreads();
+}
+
+// Spectral field of output n: fsc/nt sum_j a_j exp(2 pi i m j / nt), m = n - floor(P1/2)
+// (ifft along time, fftshift, p.specpts), in FP64 from the FP64 table; each thread owns
+// one site of one trajectory and forms XS_SPEC_NB frequencies per pass over the record.
+#define XS_SPEC_NB 4
+__device__ void xs_spectrum(const XsPathArgs& P, int cta) {
+  constexpr int GF = XS_G * XS_F * XS_NS;
+  const int nt = P.nt, np = P.npoints;
+  cx* S = P.aft + (size_t)cta * (nt + np) * GF;
+  __syncthreads();
+  for (int i = threadIdx.x; i < GF; i += blockDim.x) {
+    for (int n0 = 0; n0 < np; n0 += XS_SPEC_NB) {
+      double re[XS_SPEC_NB], im[XS_SPEC_NB];
+      int ph[XS_SPEC_NB], dm[XS_SPEC_NB];
+#pragma unroll
+      for (int b = 0; b < XS_SPEC_NB; ++b) {
+        const int m = n0 + b - np / 2;
+        dm[b] = ((m % nt) + nt) % nt;
+        ph[b] = 0;
+        re[b] = im[b] = 0;
+      }
+      for (int j = 0; j < nt; ++j) {
+        const cx x = S[(size_t)j * GF + i];
+        const double xr = (double)x.re, xi = (double)x.im;
+#pragma unroll
+        for (int b = 0; b < XS_SPEC_NB; ++b) {
+          const double2 w = P.twt[ph[b]];
+          re[b] += xr * w.x - xi * w.y;
+          im[b] += xr * w.y + xi * w.x;
+          ph[b] += dm[b];
+          if (ph[b] >= nt) ph[b] -= nt;
+        }
+      }
+#pragma unroll
+      for (int b = 0; b < XS_SPEC_NB; ++b)
+        if (n0 + b < np) S[(size_t)(nt + n0 + b) * GF + i] = mkcx((real)(re[b] * P.fscn), (real)(im[b] * P.fscn));
+    }
+  }
+  __syncthreads();
+}
+#endif
 
 // Shared-memory layout of one CTA (XS_SMEM_BYTES in total).  False, with
 // status bit 1 set, when this launch's dynamic shared memory or block size do
@@ -769,6 +832,7 @@ __device__ void xs_resident_run(const XsPathArgs& P, int cta, int nctas) {
   }
   __syncthreads();
 
+  double t = P.t0;
   if (P.single_step) {
     // p.method(a, w, p) on the given noise (Simulator/xpath.m:150)
 #if !XS_LEAN
@@ -787,7 +851,6 @@ __device__ void xs_resident_run(const XsPathArgs& P, int cta, int nctas) {
     xs_method(A, B1, B2, B3, T, W, P, P.t0);
 #endif
   } else {
-  double t = P.t0;
   int draw = 0;
   bool pending = false;  // lean MP: second half-step propagator not yet applied
   for (int n = 0; n < P.npoints; ++n) {
@@ -800,10 +863,14 @@ __device__ void xs_resident_run(const XsPathArgs& P, int cta, int nctas) {
 #if XS_LEAN
           if (P.nc == 1 || chk == 1) {
             __syncthreads();
-            // time-dependent boundary patches (XS_BVAL) forbid merging half steps
-            xs_mp_lean(A, T, P, t, g0, mode, draw, draw - 1, pending && !XS_BVAL, XS_BVAL != 0);
-            pending = !XS_BVAL;
+            // time-dependent boundary patches (XS_BVAL) and the spectrum record (XS_SPEC)
+            // forbid merging half steps
+            xs_mp_lean(A, T, P, t, g0, mode, draw, draw - 1, pending && !XS_NOMERGE, XS_NOMERGE != 0);
+            pending = !XS_NOMERGE;
             t += P.dtr;
+#if XS_SPEC
+            xs_spec_store(A, P, cta, n * P.steps + step, P.nc == 1 && chk == 1);
+#endif
           }
 #else
           xs_noise(W, Wp, mode, draw, g0, P);
@@ -811,17 +878,25 @@ __device__ void xs_resident_run(const XsPathArgs& P, int cta, int nctas) {
             __syncthreads();
             xs_method(A, B1, B2, B3, T, W, P, t);
             t += P.dtr;
+#if XS_SPEC
+            xs_spec_store(A, P, cta, n * P.steps + step, P.nc == 1 && chk == 1);
+#endif
           }
 #endif
         }
       }
+#if XS_SPEC
+      else {
+        xs_spec_store(A, P, cta, 0, false);
+      }
+#endif
       if (step == 0) {
         __syncthreads();
 #if XS_LEAN
         if (pending) xs_prop(A, T, P);
         pending = false;
 #endif
-        xs_observe(A, RED, n, t, P, wsum, cta, nctas, K, T);
+        xs_observe(A, RED, n, t, P, wsum, cta, nctas, K, T, 0);
       }
     }
   }
@@ -842,6 +917,13 @@ __device__ void xs_resident_run(const XsPathArgs& P, int cta, int nctas) {
   }
   if (bad) atomicOr(P.status, 1);
   __syncthreads();
+#if XS_SPEC
+  if (!P.single_step) {
+    xs_spectrum(P, cta);
+    for (int n = 0; n < P.npoints; ++n)
+      xs_observe(P.aft + ((size_t)cta * (P.nt + P.npoints) + P.nt + n) * GF, RED, n, t, P, wsum, cta, nctas, K, T, 1);
+  }
+#endif
 }
 
 extern "C" __global__ void __launch_bounds__(XS_THREADS) xs_resident(const XsPathArgs P) {
@@ -929,6 +1011,13 @@ extern "C" __global__ void __launch_bounds__(XS_THREADS) xs_batch(const XsBatchA
     P.params = it.params;
     P.gfield = B.gfield;
     P.prop2 = it.prop2;
+    P.bval = nullptr;
+    P.bda = nullptr;
+    P.bval_n = 0;
+    P.aft = nullptr;
+    P.twt = nullptr;
+    P.nt = 0;
+    P.fscn = 0;
     xs_resident_run(P, un.y, it.nunits);
     // publish this unit's partial sums, then count it (threadFenceReduction pattern)
     __threadfence();

@@ -226,6 +226,7 @@ struct ObsInfo {
   int red_off = 0;      // offset of its reductions in the combined red[] array
   int out_off = 0;      // offset in the site (spatial) or scalar output lists
   bool kspace = false;  // evaluated on the Fourier-transformed field (p.transforms{n})
+  bool tspec = false;   // evaluated on the time spectrum of the field (p.transforms{n}(1))
   xs::Generated gen;
 };
 
@@ -241,6 +242,7 @@ struct Problem {
   bool stencil = false;                    // some observable uses D1/D2 (neighbouring sites)
   bool dstencil = false;                   // the drift uses D1/D2: no fused MP iterations
   bool bvals = false;                      // boundary values of p.boundfun supplied per pass
+  bool spec = false;                       // some observable is evaluated on the time spectrum
   std::vector<double> runtime_defaults;
   std::vector<int> bnd;  // [D][F][2]
   int D = 0, F = 1, NW = 0, NV = 0, NS = 1, E1 = 1;
@@ -346,7 +348,7 @@ void setup_problem(const xs_problem* in, Problem& P) {
   }
   // k-space observables (xdata.m, xnft.m): one common set of periodic space dimensions
   for (auto& tr : P.obs_tr) {
-    if (tr[0]) raise(XS_ERR_UNSUPPORTED, "time-spectrum observables (p.transforms{n}(1)) are not supported on the device");
+    if (tr[0]) P.spec = true;  // time spectrum (xpath.m:46-106)
     int k[3] = {0, 0, 0};
     bool any = false;
     for (int d = 0; d < P.D; ++d)
@@ -358,7 +360,7 @@ void setup_problem(const xs_problem* in, Problem& P) {
         any = true;
       }
     if (!any) {
-      tr.assign(4, 0);
+      for (int d = 1; d < 4; ++d) tr[d] = 0;
       continue;
     }
     if (P.kobs && (k[0] != P.ktr[0] || k[1] != P.ktr[1] || k[2] != P.ktr[2]))
@@ -582,6 +584,7 @@ void generate_functions(Problem& P, std::ostringstream& os) {
     const std::string& txt = P.observe[oi];
     ObsInfo o;
     o.kspace = oi < P.obs_tr.size() && (P.obs_tr[oi][1] || P.obs_tr[oi][2] || P.obs_tr[oi][3]);
+    o.tspec = oi < P.obs_tr.size() && P.obs_tr[oi][0];
     auto fn = xs::parse_anon(txt);
     o.gen = xs::generate(fn, make_ctx(P, {Role::Field, Role::Params}, true));
     o.lines = o.gen.len;
@@ -604,6 +607,17 @@ void generate_functions(Problem& P, std::ostringstream& os) {
   }
   os << "#define XS_NRED " << P.nred << "\n#define XS_NOUT_SITE " << P.nout_site << "\n#define XS_NOUT_SCALAR "
      << P.nout_scalar << "\n#define XS_OBS_STRIDE (XS_NOUT_SITE * XS_NS + XS_NOUT_SCALAR)\n";
+  // output slots evaluated on the time spectrum (1) or on the field at the output time (0)
+  {
+    std::vector<int> site(std::max(P.nout_site, 1), 0), scal(std::max(P.nout_scalar, 1), 0);
+    for (auto& o : P.obs)
+      for (int l = 0; l < o.lines; ++l) (o.spatial ? site : scal)[o.out_off + l] = o.tspec ? 1 : 0;
+    os << "#define XS_SPEC " << (P.spec ? 1 : 0) << "\n__device__ const signed char xs_ospec_site[] = {";
+    for (size_t i = 0; i < site.size(); ++i) os << (i ? "," : "") << site[i];
+    os << "};\n__device__ const signed char xs_ospec_scalar[] = {";
+    for (size_t i = 0; i < scal.size(); ++i) os << (i ? "," : "") << scal[i];
+    os << "};\n";
+  }
   // k-space observables: transformed dimensions, normalisation prod kfact = prod dx/sqrt(2 pi) (xnft.m),
   // k grids of the observe functions (p.kx ... in propagation order)
   {
@@ -840,8 +854,9 @@ struct xs_handle {
   CUfunction f_batch = nullptr;
   cudaStream_t stream = nullptr;
   DevBuf d_prop[2], d_prop2[2], d_tmat, d_obs, d_av, d_ain, d_aout, d_status, d_w, d_field, d_redpart, d_pstep,
-      d_params, d_gfield, d_twiddle, d_tmp, d_avm, d_bval[2], d_bda[2];
+      d_params, d_gfield, d_twiddle, d_tmp, d_avm, d_bval[2], d_bda[2], d_aft, d_twt;
   int bval_n[2] = {0, 0};
+  int twt_n = 0;
   double pstep_dtr = -1;
   double prop_dtr[2] = {-1, -1}, prop2_dtr[2] = {-1, -1};
   // launch accounting (xs_kernel_stats)
@@ -1060,6 +1075,7 @@ std::string stream_blocker(const Problem& P) {
   for (auto& o : P.obs)
     if (o.spatial && !o.gen.reductions.empty()) return "site observables that use Int/Ave are not streamed";
   if (P.kobs) return "k-space observables (p.transforms) are not streamed";
+  if (P.spec) return "time-spectrum observables (p.transforms{n}(1)) are not streamed";
   if (P.stencil) return "observables with D1/D2 finite differences are not streamed";
   if (P.dstencil) return "drifts with D1/D2 finite differences are not streamed";
   return "";
@@ -1403,6 +1419,11 @@ struct PathArgsHost {
   const void* bda;
   int bval_n;
   int pad3;
+  void* aft;
+  const void* twt;
+  int nt;
+  int pad4;
+  double fscn;
 };
 
 size_t av_stride(const Problem& P) { return (size_t)P.nout_site * P.NS + P.nout_scalar; }
@@ -1464,6 +1485,41 @@ int resident_grid(xs_handle& h, CUfunction f, int nctas) {
   return grid;
 }
 
+// Time spectrum (Simulator/xpath.m:26-106): the field at every step count, Nt = points(1) x steps
+// rows per trajectory tile, then points(1) rows of its inverse DFT at the frequencies
+// (0..P1-1) - floor(P1/2) (ifft, fftshift and p.specpts), scaled by p.fsc / Nt with
+// p.fsc = sqrt(2 pi) / p.dw, p.dw = 2 pi / (ranges(1) + dt) (xpreferences.m:246-249).
+// exp(2 pi i k / Nt) in FP64 for the DFT sums.
+void spectrum_buffers(xs_handle& h, int nctas, PathArgsHost& a) {
+  const Problem& P = h.P;
+  const int P1 = P.p.points[0];
+  const int nt = P1 * P.p.steps;
+  const size_t rows = (size_t)nt + P1;
+  const size_t bytes = (size_t)nctas * rows * h.rp.G * P.F * P.NS * (h.fp64 ? 16 : 8);
+  size_t free_b = 0, total_b = 0;
+  CUDA_CHECK(cudaMemGetInfo(&free_b, &total_b));
+  if (bytes > free_b + h.d_aft.bytes)
+    raise(XS_ERR_SHAPE, "the time-spectrum record (" + std::to_string(bytes >> 20) +
+                            " MiB) exceeds free device memory: run fewer ensemble blocks per call");
+  h.d_aft.ensure(bytes);
+  if (h.twt_n != nt) {
+    std::vector<double> w(2 * (size_t)nt);
+    for (int k = 0; k < nt; ++k) {
+      const double ph = 2 * M_PI * (double)k / nt;
+      w[2 * k] = std::cos(ph);
+      w[2 * k + 1] = std::sin(ph);
+    }
+    h.d_twt.ensure(w.size() * 8);
+    CUDA_CHECK(cudaMemcpy(h.d_twt.p, w.data(), w.size() * 8, cudaMemcpyHostToDevice));
+    h.twt_n = nt;
+  }
+  const double dw = 2 * M_PI / (P.p.ranges[0] + P.dt);
+  a.aft = h.d_aft.p;
+  a.twt = h.d_twt.p;
+  a.nt = nt;
+  a.fscn = std::sqrt(2 * M_PI) / dw / nt;
+}
+
 // Launch the resident path; av_dev receives [nblocks][npoints][stride] complex.
 void launch_resident(xs_handle& h, int first_block, int nblocks, int nc, const void* a_in_dev, void* av_dev,
                      void* a_out_dev, cudaStream_t st) {
@@ -1504,6 +1560,7 @@ void launch_resident(xs_handle& h, int first_block, int nblocks, int nc, const v
   a.obs = h.d_obs.p;
   a.status = (int*)h.d_status.p;
   a.params = (const double*)h.d_params.p;
+  if (P.spec) spectrum_buffers(h, nctas, a);
   const int grid = resident_grid(h, h.f_resident, nctas);
   a.gfield = h.d_gfield.p;
   void* params[] = {&a};
@@ -1925,6 +1982,7 @@ XS_API xs_status xs_run_path_device_noalloc(xs_handle* h, int first_block, int n
     if (h->rp.gfield)
       raise(XS_ERR_UNSUPPORTED, "xs_run_path_device_noalloc needs the field in shared memory (it would allocate slices)");
     if (h->P.bvals) raise(XS_ERR_UNSUPPORTED, "xs_run_path_device_noalloc does not take boundary values");
+    if (h->P.spec) raise(XS_ERR_UNSUPPORTED, "xs_run_path_device_noalloc does not record time spectra");
     if (nc == 2 && !P.p.checks) raise(XS_ERR_ARG, "coarse pass requested without checks");
     const int slot = nc == 2 ? 1 : 0;
     if (!h->loaded || !h->d_prop[slot].p || (P.has_linear && h->prop_dtr[slot] != pass_dtr(P, nc)))
@@ -2794,6 +2852,7 @@ XS_API xs_status xs_batch_create(const xs_problem* items, int nitems, xs_batch**
         h.path_kind = items[i].path_kind;
         if (items[i].checks) raise(XS_ERR_UNSUPPORTED, "batch items run the fine pass only (checks = 0)");
         if (items[i].boundary_values) raise(XS_ERR_UNSUPPORTED, "batch items take no boundary values");
+        if (h.P.spec) raise(XS_ERR_UNSUPPORTED, "batch items take no time-spectrum observables");
         if (items[i].ensembles[1] != 1 || items[i].ensembles[2] != 1)
           raise(XS_ERR_UNSUPPORTED, "a batch item is one ensemble block (ensembles(2) = ensembles(3) = 1)");
         h.force_G = 1;
