@@ -142,6 +142,16 @@ XS_API size_t xs_av_doubles_per_block(const xs_handle* h);
 XS_API xs_status xs_run_path(xs_handle* h, int first_block, int nblocks, int nc, const double* a_in,
                              double* av_out, double* a_out);
 
+/* xs_run_path that also returns p.path's third output `raw` when p.rawdata is
+ * set (Simulator/xpath.m:72-77, stored at xensemble.m:79 and returned by
+ * xsim.m:1): raw_out is the field at every output time, [fields, points(1),
+ * space, ens1*nblocks] complex FP64 (raw{l} of Simulator/xpreferences.m:148 for
+ * consecutive blocks).  Resident path only (XS_ERR_UNSUPPORTED on the
+ * streaming path); XS_ERR_SHAPE when the record exceeds free device memory.
+ * raw_out NULL is xs_run_path. */
+XS_API xs_status xs_run_path_raw(xs_handle* h, int first_block, int nblocks, int nc, const double* a_in,
+                                 double* av_out, double* a_out, double* raw_out);
+
 /* Same as xs_run_path with device pointers and a caller stream (cudaStream_t
  * passed as void*; NULL is the default stream, as in CUDA); nothing is copied
  * to or from the host and the call returns without synchronising.  a_in_dev/a_out_dev use the device layout

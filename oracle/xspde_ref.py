@@ -118,6 +118,7 @@ def xpreferences(inputs):
         if s > 0:
             p.checks = out[0].checks                                     # :32
         p.iterations = int(p.get("iterations", 4))                       # :59
+        p.rawdata = int(p.get("rawdata", 0))                             # :85
         if "deriv" not in p:
             p.deriv = lambda a, w, p: 0 * a                              # :64
         nz = p.get("noises", None)
@@ -878,6 +879,8 @@ def xpath(a, nc, p):
     p.draw = 0
     spectrum = any(tr[0] for tr in p.transforms)                         # xpreferences.m:246
     aft = np.zeros((P1 * S,) + np.shape(a), dtype=complex) if spectrum else None
+    # raw{l}: [fields, points(1), space, ens] (xpreferences.m:148)
+    raw = np.zeros((np.shape(a)[0], P1) + np.shape(a)[1:], dtype=complex) if p.rawdata else None
     n1 = -1
     for n in range(P1):                                                  # :137
         for step in range(S):                                            # :138
@@ -898,6 +901,8 @@ def xpath(a, nc, p):
             elif spectrum:                                               # :64-68
                 aft[n1] = a
             if step == 0:                                                # :181
+                if p.rawdata:                                            # :72-77
+                    raw[:, n] = a
                 for o in p.averages:
                     if not p.transforms[o][0]:
                         r = xdata(a, o, p)
@@ -913,7 +918,7 @@ def xpath(a, nc, p):
                     r = xdata(f[sel[n]], o, p)
                     L = p.d_av[o][0]
                     av[o][:, n] = freshape(r, [L] + list(p.d_av[o][2:]))
-    return a, av
+    return a, av, raw
 
 
 def xensemble(npar, inputs):
@@ -927,6 +932,7 @@ def xensemble(npar, inputs):
     m = p1.fbsw + p1.nchk                                                # :18
     m1 = max(3, m + 1)                                                   # :19
     data = [[np.zeros((inputs[s].d_data[o], m1)) for o in inputs[s].outputs] for s in range(seq)]
+    raws = [[[None] * p1.ensembles[1] for _ in range(p1.nchk)] for _ in range(seq)]  # :15
     D = [dict() for _ in range(seq)]
     for j in range(p1.ensembles[1]):                                     # :25
         block = (npar - 1) + j * p1.ensembles[2]                         # :26
@@ -953,7 +959,8 @@ def xensemble(npar, inputs):
                     for d in range(1, p.dimensions):
                         p.boundval[d] = p.boundfun(a, 0, d, p)
                 p.t = p.origins[0]
-                b, av = p.path(a, nc, p)                                 # :79
+                b, av, r = p.path(a, nc, p)                              # :79
+                raws[s][nc - 1][j] = r
                 for o in p.outputs:                                      # :84
                     if p.d_data[o] > 0:
                         nes = 1 + ne
@@ -967,7 +974,7 @@ def xensemble(npar, inputs):
                             for n1 in range(1, m + 1):                   # :98-100
                                 data[s][o][:, n1 - 1] += D[s][(n1, o)] * nes
                             data[s][o][:, m1 - 1] += D[s][(1, o)] ** 2 * nes  # :101
-    return data
+    return data, raws
 
 
 # ---------------------------------------------------------------------------
@@ -1018,7 +1025,10 @@ def xcompress(n, data, p, xk):
 def xsim(*inputs):
     """Run ensembles and compute error columns (xsim.m:77-263).
 
-    Returns (error, data, input) like the reference (raw omitted)."""
+    Returns (error, data, input) like the reference, and raw as a fourth value
+    when an input sets p.rawdata: raw[s][nc][k] is the [fields, points(1), space,
+    ens(1)] field array of sequence s, check pass nc and ensemble k = j + ens(2) npar
+    (xsim.m:42-57)."""
     t0 = time.perf_counter()
     if len(inputs) == 1 and isinstance(inputs[0], (list, tuple)):
         inputs = inputs[0]
@@ -1031,9 +1041,14 @@ def xsim(*inputs):
     sx = max(3, 1 + nc1)                                                 # :89
     err = np.zeros(6)
     data = None
+    raw = [[[None] * (p.ensembles[1] * p.ensembles[2]) for _ in range(p.nchk)] for _ in range(seq)]  # :42
     for npar in range(1, p.ensembles[2] + 1):                            # :99-109
-        dp = xensemble(npar, inp)
+        dp, rp = xensemble(npar, inp)
         data = dp if data is None else [[x + y for x, y in zip(a, b)] for a, b in zip(data, dp)]
+        for s in range(seq):                                             # :54, :57 raw(:,:,:,npar)
+            for nc in range(p.nchk):
+                for j in range(p.ensembles[1]):
+                    raw[s][nc][j + p.ensembles[1] * (npar - 1)] = rp[s][nc][j]
     totout = sum(len(q.outputs) for q in inp)
     er = np.zeros((totout, max(6, nc1 + 4)))
     em = np.zeros_like(er)
@@ -1107,4 +1122,6 @@ def xsim(*inputs):
     error[sx + 1:sx + 3] = np.sum(er[:, sx + 1:sx + 3], axis=0)
     error[sx + 1] = error[sx + 1] / (1e-20 + error[sx + 2])
     error[sx + 2] = time.perf_counter() - t0
+    if any(q.rawdata for q in inp):
+        return error, data, inp, raw                                     # xsim.m:1 [error,data,input,raw]
     return error, data, inp

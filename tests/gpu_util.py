@@ -21,7 +21,9 @@ def oracle_block_av(pdict, block, nc):
         v = p.randomgen(p)
         p.t = p.origins[0]
         a = X.fit(np.asarray(p.initial(v, p), dtype=complex), p.ca)
-        b, av = p.path(a, nc, p)
+        b, av, raw = p.path(a, nc, p)
+    if p.rawdata:
+        return av, b, raw
     return av, b
 
 

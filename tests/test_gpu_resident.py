@@ -288,3 +288,27 @@ def test_time_spectrum_field_in_device_memory_fp64():
              linear=lambda p: 0.5j * (p.Dx ** 2 + p.Dy ** 2),
              observe=[lambda a, p: abs(a) ** 2, lambda a, p: abs(a) ** 2])
     _compare(g, o, [0], [1, 2], FP64_TOL)
+
+
+@pytest.mark.parametrize("nc", [1, 2])
+def test_raw_trajectories_two_fields_fp64(nc):
+    """p.rawdata (Simulator/xpath.m:72-77): the field of every trajectory at every
+    output time, [fields, points(1), space, ens], for two blocks in one call."""
+    from xspde_matlab_b200 import GpuPath, xpreferences
+    base = dict(dimensions=2, fields=2, noises=2, points=[6, 16], ranges=[0.6, 6.0], steps=2, ensembles=[4, 2, 1],
+                method="MP", checks=1, rawdata=1)
+    g = dict(base, deriv="@(a,w,p) [1i*a(2,:) + 0.1*w(1,:); 1i*a(1,:) - 0.2*a(2,:) + 0.1*w(2,:)]",
+             initial="@(v,p) [exp(-p.x.^2); 0.5 + 0.1*v(1,:)]", linear="@(p) 0.2i*p.Dx.^2",
+             observe=["@(a,p) a(1,:).*conj(a(2,:))"])
+    o = dict(base, deriv=lambda a, w, p: np.concatenate([1j * a[1:2] + 0.1 * w[0:1],
+                                                         1j * a[0:1] - 0.2 * a[1:2] + 0.1 * w[1:2]]),
+             initial=lambda v, p: np.concatenate([np.exp(-p.x ** 2) + 0 * v[0:1], 0.5 + 0.1 * v[0:1]]),
+             linear=lambda p: 0.2j * p.Dx ** 2, observe=[lambda a, p: a[0:1] * np.conj(a[1:2])])
+    path = GpuPath(xpreferences([g])[0])
+    av, _, raw = path.run_path(0, 2, nc, raw=True)
+    assert raw.shape == (2, 6, 16, 8)
+    for b in range(2):
+        av_o, b_o, raw_o = oracle_block_av(o, b, nc)
+        assert rel_err(raw[..., 4 * b:4 * b + 4], raw_o) < FP64_TOL
+        assert rel_err(av[b][0].reshape(-1, order="F"), av_o[0].reshape(-1, order="F")) < FP64_TOL
+        assert rel_err(raw[:, -1, :, 4 * b:4 * b + 4], b_o) < FP64_TOL

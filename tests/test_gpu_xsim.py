@@ -189,3 +189,24 @@ def test_gpu_xsim_equilibrium_spectrum():
     exact = 25.0 / (np.pi * (1 + w ** 2))
     sel = np.abs(w) < 4
     assert np.all(np.abs(spec[sel] - exact[sel]) < 5 * err[sel] + 0.02 * exact[sel])
+
+
+def test_gpu_xsim_raw_matches_oracle():
+    """xsim's fourth output raw{s, nc, k} (Simulator/xsim.m:42-57) with two serial and
+    two parallel ensembles: same trajectories, same ordering as the oracle."""
+    from xspde_matlab_b200 import xsim
+    base = dict(dimensions=2, points=[5, 16], ranges=[0.5, 6.0], steps=2, ensembles=[4, 2, 2], noises=2,
+                method="MP", checks=1, rawdata=1)
+    g = dict(base, deriv="@(a,w,p) 1i*a.*conj(a).*a + 0.05*(w(1,:)+1i*w(2,:))",
+             initial="@(v,p) exp(-p.x.^2) + 0.01*v(1,:)", linear="@(p) 1i*p.Dx.^2", observe=["@(a,p) a.*conj(a)"])
+    o = dict(base, deriv=lambda a, w, p: 1j * a * np.conj(a) * a + 0.05 * (w[0:1] + 1j * w[1:2]),
+             initial=lambda v, p: np.exp(-p.x ** 2) + 0.01 * v[0:1], linear=lambda p: 1j * p.Dx ** 2,
+             observe=[lambda a, p: a * np.conj(a)])
+    eg, dg, _, rg = xsim(g)
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore", RuntimeWarning)
+        eo, do, _, ro = X.xsim(o)
+    for nc in range(2):
+        for k in range(4):
+            assert rg[0][nc][k].shape == (1, 5, 16, 4)
+            assert np.allclose(rg[0][nc][k], ro[0][nc][k], rtol=1e-10, atol=1e-12), (nc, k)

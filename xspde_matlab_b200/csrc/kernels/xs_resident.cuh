@@ -47,6 +47,8 @@ struct XsPathArgs {
   int nt;               // XS_SPEC: points(1) x steps(1)
   int pad4;
   double fscn;          // XS_SPEC: p.fsc / nt
+  double2* raw;         // optional raw trajectories (p.rawdata, xpath.m:72-77): the field at every
+                        // output time in MATLAB's layout [F][npoints][NS][ntraj], fastest first
 };
 
 // XS_GFIELD: the lattice is too large for shared memory, so each CTA keeps its
@@ -896,6 +898,15 @@ __device__ void xs_resident_run(const XsPathArgs& P, int cta, int nctas) {
         if (pending) xs_prop(A, T, P);
         pending = false;
 #endif
+        if (P.raw) {
+          __syncthreads();
+          for (int i = threadIdx.x; i < GF; i += blockDim.x) {
+            const int g = i / (XS_F * XS_NS), f = (i / XS_NS) % XS_F, s = i % XS_NS;
+            const cx v = A[i];
+            P.raw[f + (size_t)XS_F * (n + (size_t)P.npoints * (s + (size_t)XS_NS * (g0 + g)))] =
+                make_double2((double)v.re, (double)v.im);
+          }
+        }
         xs_observe(A, RED, n, t, P, wsum, cta, nctas, K, T, 0);
       }
     }
@@ -1018,6 +1029,7 @@ extern "C" __global__ void __launch_bounds__(XS_THREADS) xs_batch(const XsBatchA
     P.twt = nullptr;
     P.nt = 0;
     P.fscn = 0;
+    P.raw = nullptr;
     xs_resident_run(P, un.y, it.nunits);
     // publish this unit's partial sums, then count it (threadFenceReduction pattern)
     __threadfence();

@@ -854,9 +854,10 @@ struct xs_handle {
   CUfunction f_batch = nullptr;
   cudaStream_t stream = nullptr;
   DevBuf d_prop[2], d_prop2[2], d_tmat, d_obs, d_av, d_ain, d_aout, d_status, d_w, d_field, d_redpart, d_pstep,
-      d_params, d_gfield, d_twiddle, d_tmp, d_avm, d_bval[2], d_bda[2], d_aft, d_twt;
+      d_params, d_gfield, d_twiddle, d_tmp, d_avm, d_bval[2], d_bda[2], d_aft, d_twt, d_raw;
   int bval_n[2] = {0, 0};
   int twt_n = 0;
+  void* raw_dev = nullptr;  // raw trajectories of the current resident launch (xs_run_path_raw)
   double pstep_dtr = -1;
   double prop_dtr[2] = {-1, -1}, prop2_dtr[2] = {-1, -1};
   // launch accounting (xs_kernel_stats)
@@ -1424,6 +1425,7 @@ struct PathArgsHost {
   int nt;
   int pad4;
   double fscn;
+  void* raw;
 };
 
 size_t av_stride(const Problem& P) { return (size_t)P.nout_site * P.NS + P.nout_scalar; }
@@ -1561,6 +1563,7 @@ void launch_resident(xs_handle& h, int first_block, int nblocks, int nc, const v
   a.status = (int*)h.d_status.p;
   a.params = (const double*)h.d_params.p;
   if (P.spec) spectrum_buffers(h, nctas, a);
+  a.raw = h.raw_dev;
   const int grid = resident_grid(h, h.f_resident, nctas);
   a.gfield = h.d_gfield.p;
   void* params[] = {&a};
@@ -1825,13 +1828,32 @@ XS_API xs_status xs_observe_info(const xs_handle* h, int o, int* lines, int* spa
 
 XS_API size_t xs_av_doubles_per_block(const xs_handle* h) { return h ? av_doubles_per_block(h->P) : 0; }
 
-XS_API xs_status xs_run_path(xs_handle* h, int first_block, int nblocks, int nc, const double* a_in, double* av_out,
-                             double* a_out) {
+namespace {
+struct RawScope {  // the raw-trajectory pointer belongs to one xs_run_path_raw call
+  xs_handle* h;
+  ~RawScope() { h->raw_dev = nullptr; }
+};
+
+xs_status run_path_impl(xs_handle* h, int first_block, int nblocks, int nc, const double* a_in, double* av_out,
+                        double* a_out, double* raw_out) {
   return guard([&]() -> xs_status {
     if (!h || nblocks < 1 || first_block < 0 || (nc != 1 && nc != 2)) raise(XS_ERR_ARG, "bad arguments to xs_run_path");
     if (nc == 2 && !h->P.p.checks) raise(XS_ERR_ARG, "coarse pass requested without checks");
     load_module(*h);
     const Problem& P = h->P;
+    RawScope raw_scope{h};
+    size_t rbytes = 0;
+    if (raw_out) {
+      if (h->kind != 1) raise(XS_ERR_UNSUPPORTED, "raw trajectories are recorded by the resident path only");
+      rbytes = (size_t)nblocks * P.E1 * P.p.points[0] * P.F * P.NS * 16;
+      size_t free_b = 0, total_b = 0;
+      CUDA_CHECK(cudaMemGetInfo(&free_b, &total_b));
+      if (rbytes > free_b + h->d_raw.bytes)
+        raise(XS_ERR_SHAPE, "raw trajectories (" + std::to_string(rbytes >> 20) +
+                                " MiB) exceed free device memory: run fewer ensemble blocks per call");
+      h->d_raw.ensure(rbytes);
+      h->raw_dev = h->d_raw.p;
+    }
     const size_t ntraj = (size_t)nblocks * P.E1;
     const size_t fbytes = ntraj * P.F * P.NS * 16;
     const void* din = nullptr;
@@ -1890,6 +1912,7 @@ XS_API xs_status xs_run_path(xs_handle* h, int first_block, int nblocks, int nc,
     }
     int status = 0;
     CUDA_CHECK(cudaMemcpyAsync(&status, h->d_status.p, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    if (raw_out) CUDA_CHECK(cudaMemcpyAsync(raw_out, h->d_raw.p, rbytes, cudaMemcpyDeviceToHost, h->stream));
     if (a_out) {
       if (P.F == 1) {
         CUDA_CHECK(cudaMemcpyAsync(a_out, dout, fbytes, cudaMemcpyDeviceToHost, h->stream));
@@ -1906,6 +1929,17 @@ XS_API xs_status xs_run_path(xs_handle* h, int first_block, int nblocks, int nc,
     if (status & 1) raise(XS_ERR_NAN, "a trajectory became non-finite (NaN/Inf) during the path");
     return XS_OK;
   });
+}
+}  // namespace
+
+XS_API xs_status xs_run_path(xs_handle* h, int first_block, int nblocks, int nc, const double* a_in, double* av_out,
+                             double* a_out) {
+  return run_path_impl(h, first_block, nblocks, nc, a_in, av_out, a_out, nullptr);
+}
+
+XS_API xs_status xs_run_path_raw(xs_handle* h, int first_block, int nblocks, int nc, const double* a_in,
+                                 double* av_out, double* a_out, double* raw_out) {
+  return run_path_impl(h, first_block, nblocks, nc, a_in, av_out, a_out, raw_out);
 }
 
 XS_API xs_status xs_run_path_device(xs_handle* h, int first_block, int nblocks, int nc, const double* a_in_dev,

@@ -86,6 +86,7 @@ def xpreferences(inputs):
         if any(p.checks[1:]):
             raise _lib.XsError(-9, "space-step checks (checks(2:end)) are not supported")
         p.iterations = int(p.get("iterations", 4))
+        p.rawdata = int(p.get("rawdata", 0))  # xpreferences.m:85
         nz = p.get("noises", None)
         p.noises = int(np.atleast_1d(nz)[0]) if nz is not None else p.fields
         rz = p.get("inrandoms", None)
@@ -298,9 +299,11 @@ class GpuPath:
         _lib.check(_lib.lib().xs_set_boundary_values(self.h, nc, ntimes, tab.ctypes.data))
         cache.add(nc)
 
-    def run_path(self, first_block, nblocks, nc, a_in=None, a_out=False):
+    def run_path(self, first_block, nblocks, nc, a_in=None, a_out=False, raw=False):
         """p.path for blocks [first_block, first_block+nblocks): returns
-        (av, a) with av[b][o] complex arrays of shape av_shapes()[o]."""
+        (av, a) with av[b][o] complex arrays of shape av_shapes()[o]; with
+        raw=True (p.rawdata, Simulator/xpath.m:72-77) also the field at every
+        output time, [fields, points(1), space..., ens1*nblocks]: (av, a, raw)."""
         P = self.p
         if callable(P.get("boundfun", None)):
             self._boundary_values(nc)
@@ -311,9 +314,14 @@ class GpuPath:
         aout = None
         if a_out:
             aout = np.empty([P.fields] + list(P.space) + [P.ensembles[0] * nblocks], dtype=np.complex128, order="F")
-        _lib.check(_lib.lib().xs_run_path(self.h, first_block, nblocks, nc,
-                                          ain.ctypes.data if ain is not None else None,
-                                          buf.ctypes.data, aout.ctypes.data if aout is not None else None))
+        rout = None
+        if raw:
+            rout = np.empty([P.fields, P.points[0]] + list(P.space) + [P.ensembles[0] * nblocks],
+                            dtype=np.complex128, order="F")
+        _lib.check(_lib.lib().xs_run_path_raw(self.h, first_block, nblocks, nc,
+                                              ain.ctypes.data if ain is not None else None,
+                                              buf.ctypes.data, aout.ctypes.data if aout is not None else None,
+                                              rout.ctypes.data if rout is not None else None))
         cbuf = buf.view(np.complex128)
         av, pos = [], 0
         for b in range(nblocks):
@@ -323,6 +331,8 @@ class GpuPath:
                 row.append(np.reshape(cbuf[pos:pos + n], shp, order="F"))
                 pos += n
             av.append(row)
+        if raw:
+            return av, aout, rout
         return av, aout
 
 
@@ -406,11 +416,14 @@ def _grid(xk):
     return q
 
 
-def _ensembles(inp, paths, rank=0, size=1, reduce=None):
+def _ensembles(inp, paths, rank=0, size=1, reduce=None, raw=None):
     """Block loop, check passes and moments (Simulator/xensemble.m:12-108) with
     all blocks of a pass integrated by one device call.  With size > 1 this
     rank integrates its own contiguous share of the blocks and `reduce` sums
-    the moment accumulators over the ranks (Simulator/xsim.m:99-106)."""
+    the moment accumulators over the ranks (Simulator/xsim.m:99-106).  With
+    `raw` (nested lists [s][nc-1][k]) the blocks' raw trajectories of inputs
+    with p.rawdata are stored at k = j + ens(2) (npar-1) for global block
+    (npar-1) + j ens(3) (xensemble.m:26,79; xsim.m:42-57)."""
     from .dist import shard
     p1 = inp[0]
     nb = p1.ensembles[1] * p1.ensembles[2]
@@ -440,7 +453,15 @@ def _ensembles(inp, paths, rank=0, size=1, reduce=None):
                     r = np.asarray(p.transfer(prev, v, p), dtype=complex)
                     r = r.reshape(r.shape + (1,) * (len(shape) - r.ndim))
                     a_in = np.asfortranarray(np.broadcast_to(r, shape))
-                av, prev = paths[s].run_path(b0, nbk, nc, a_in=a_in, a_out=(s + 1 < len(inp)))
+                if raw is not None and p.rawdata:
+                    av, prev, r = paths[s].run_path(b0, nbk, nc, a_in=a_in, a_out=(s + 1 < len(inp)), raw=True)
+                    e1 = p.ensembles[0]
+                    for b in range(nbk):
+                        g = b0 + b
+                        k = g // p.ensembles[2] + p.ensembles[1] * (g % p.ensembles[2])
+                        raw[s][nc - 1][k] = r[..., b * e1:(b + 1) * e1]
+                else:
+                    av, prev = paths[s].run_path(b0, nbk, nc, a_in=a_in, a_out=(s + 1 < len(inp)))
                 for b in range(nbk):
                     for o in range(len(p.output)):
                         Dv = np.real(np.asarray(p.output[o](av[b], p)))
@@ -474,7 +495,10 @@ def _ensembles(inp, paths, rank=0, size=1, reduce=None):
 
 
 def xsim(*inputs, path_kind=0):
-    """Simulate and return (error, data, input) (Simulator/xsim.m:77-263).
+    """Simulate and return (error, data, input) (Simulator/xsim.m:77-263), and
+    raw as a fourth value when an input sets p.rawdata: raw[s][nc][k] is the
+    [fields, points(1), space..., ens(1)] field array of sequence s, check pass nc
+    and ensemble k (xsim.m:42-57; under several ranks each rank holds its own blocks).
 
     error: [total RMS, step errors..., sampling, difference, chi^2/k, time]
     data[s][o]: columns mean, step error, sampling error, comparison."""
@@ -499,7 +523,10 @@ def xsim(*inputs, path_kind=0):
         if tdist.get_backend(group) == "nccl":
             import torch
             dev = torch.device("cuda", torch.cuda.current_device())
-    data = _ensembles(inp, paths, rank, size, reduce=lambda arrs: allreduce_sum(arrs, group, dev))
+    want_raw = any(q.rawdata for q in inp)
+    nb = inp[0].ensembles[1] * inp[0].ensembles[2]
+    raw = [[[None] * nb for _ in range(inp[0].nchk)] for _ in inp] if want_raw else None
+    data = _ensembles(inp, paths, rank, size, reduce=lambda arrs: allreduce_sum(arrs, group, dev), raw=raw)
     p = inp[0]
     ne = p.ensembles[1] * p.ensembles[2]
     sx = max(3, 1 + p.nchk)
@@ -555,6 +582,8 @@ def xsim(*inputs, path_kind=0):
     error[sx + 1:sx + 3] = np.sum(er[:, sx + 1:sx + 3], axis=0)
     error[sx + 1] /= 1e-20 + error[sx + 2]
     error[sx + 2] = time.perf_counter() - t0
+    if want_raw:
+        return error, data, inp, raw
     return error, data, inp
 
 
