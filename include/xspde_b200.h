@@ -97,11 +97,21 @@ typedef struct xs_problem {
   const int* transforms;       /* NULL: every observable in x space; else [nobserve][4] flags of
                                   p.transforms{n} (time, x, y, z): 1 = the observable sees the field
                                   Fourier-transformed along that space dimension (xnft.m, periodic
-                                  dimensions only; time spectra are not supported) */
+                                  dimensions only); the time flag evaluates the observable on the time
+                                  spectrum of the field (Simulator/xpath.m:90-106) */
   int sequence;                /* index of this input in a sequence (xensemble.m:36-62): part of the
                                   Philox counter, so every sequence draws its own noise */
   int boundary_values;         /* 1: p.boundfun gives boundary values (MP only); the caller supplies
                                   them per check pass with xs_set_boundary_values before each path */
+  int knoises;                 /* p.knoises: k-filtered noise components (Simulator/xnoise.m:39-50), the
+                                  drift's next noise argument after w: @(a,w,z,p), or @(a,z,p) when
+                                  noises = 0; every space dimension periodic */
+  int krandoms;                /* p.krandoms: k-filtered initial randoms (Simulator/xrandom.m:24-29), the
+                                  initial function's next argument after v */
+  const double* nfilter;       /* NULL (p.nfilter = identity) or [knoises][space] complex FP64: the factor
+                                  p.nfilter multiplies each k-space noise value by, the k lattice in FFT
+                                  order (p.kx ... in propagation order, Simulator/xgrid.m) */
+  const double* rfilter;       /* the same for p.rfilter and krandoms */
 } xs_problem;
 
 /* Create a handle: parse, generate and compile the kernels (NVRTC, cached).

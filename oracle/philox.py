@@ -26,6 +26,11 @@ Box-Muller pair (Box and Muller, 1958) with uniforms u = (x + 1/2) 2^-32:
 Component c of the call uses pair (c % 4) // 2 and the cos (even c) or sin
 (odd c) branch.
 
+k-space noises and randoms (knoises, krandoms: Simulator/xnoise.m:39-50,
+xrandom.m:24-29) come from their own stream: the fourth counter word carries
+bit 15 as well, (component // 4) | 0x8000 | seq << 16, with no site pairing;
+the site index is the column-major index of the k-space lattice in FFT order.
+
 Site pairing: when there are at most two components and the first space
 dimension has an even number of points N1, one call serves two sites that
 are N1/2 apart along x.  Site s with x index i1 uses the call whose site
@@ -77,12 +82,14 @@ def _boxmuller(w0, w1):
     return r * np.cos(th), r * np.sin(th)
 
 
-def normals(ncomp, nspace, nens, draw, block, seed, seq=0, n1=1):
+def normals(ncomp, nspace, nens, draw, block, seed, seq=0, n1=1, kstream=False):
     """Standard normals z[c, s, e] for one draw, shape (ncomp, nspace, nens).
-    n1 is the number of points along the first space dimension (1 for SDEs)."""
+    n1 is the number of points along the first space dimension (1 for SDEs);
+    kstream selects the k-space stream."""
     out = np.empty((ncomp, nspace, nens), dtype=np.float64)
     e = np.arange(nens, dtype=np.uint64)[None, :]
-    if ncomp <= 2 and n1 > 1 and n1 % 2 == 0 and nspace % n1 == 0:
+    kbit = 0x8000 if kstream else 0
+    if not kstream and ncomp <= 2 and n1 > 1 and n1 % 2 == 0 and nspace % n1 == 0:
         h = n1 // 2
         s = np.arange(nspace)
         i1 = s % n1
@@ -96,7 +103,7 @@ def normals(ncomp, nspace, nens, draw, block, seed, seq=0, n1=1):
         return out
     s = np.arange(nspace, dtype=np.uint64)[:, None]
     for g in range((ncomp + 3) // 4):
-        w = philox4x32_10(s, e, draw, g | (seq << 16), seed, block)
+        w = philox4x32_10(s, e, draw, g | kbit | (seq << 16), seed, block)
         for pair in range(2):
             c_even = 4 * g + 2 * pair
             if c_even >= ncomp:

@@ -122,9 +122,17 @@ def xpreferences(inputs):
         if "deriv" not in p:
             p.deriv = lambda a, w, p: 0 * a                              # :64
         nz = p.get("noises", None)
-        p.noises = int(np.atleast_1d(nz)[0]) if nz is not None else p.fields  # :65-70
+        kz = p.get("knoises", None)
+        p.knoises = int(np.atleast_1d(kz)[0]) if kz is not None else 0     # :67
+        p.noises = (int(np.atleast_1d(nz)[0]) if nz is not None
+                    else (0 if kz is not None else p.fields))            # :65-70
+        krz = p.get("krandoms", None)
+        p.krandoms = int(np.atleast_1d(krz)[0]) if krz is not None else 0  # :73
+        p.nfilter = p.get("nfilter", lambda w, p: w)                     # :122, :419-421
+        p.rfilter = p.get("rfilter", lambda w, p: w)                     # :123, :423-425
         rz = p.get("inrandoms", None)
-        p.inrandoms = int(np.atleast_1d(rz)[0]) if rz is not None else p.noises  # :71-76
+        p.inrandoms = (int(np.atleast_1d(rz)[0]) if rz is not None
+                       else (0 if krz is not None else p.noises))        # :71-76
         p.ranges = [float(x) for x in _pad(p.get("ranges", [10.0] * nd), nd, 10.0)]  # :81
         st = list(np.atleast_1d(p.get("steps", [1])))
         p.steps = [int(x) for x in st] + [1] * (nd - len(st))            # :82
@@ -626,8 +634,20 @@ def xprop(a, p):
 # Steppers: Applications/SDE/MP.m, RK4.m, Euler.m, RK2.m, Implicit.m
 # ---------------------------------------------------------------------------
 
+class Cells(list):
+    """Several noise or random cells (Gaussian, then k-filtered), passed to the
+    user's functions as separate arguments: p.deriv{c}(a{:}, xi{:}, p) (MP.m:16),
+    p.initial(v{:}, p) (xensemble.m:60)."""
+
+
+def call_cells(fn, first, cells, p):
+    if isinstance(cells, Cells):
+        return fn(*([] if first is None else [first]), *cells, p)
+    return fn(*([] if first is None else [first]), cells, p)
+
+
 def _deriv(a, w, p):
-    return fit(p.deriv(a, w, p), p.ca)
+    return fit(call_cells(p.deriv, a, w, p), p.ca)
 
 
 def MP(a, xi, p):
@@ -716,10 +736,33 @@ METHODS = {"MP": MP, "RK4": RK4, "Euler": Euler, "RK2": RK2, "Implicit": Implici
 # Noise hooks: Simulator/xnoise.m, Simulator/xrandom.m (Philox stream)
 # ---------------------------------------------------------------------------
 
+def _kcells(nk, draw, filt, scale, p):
+    """k-filtered cell (xnoise.m:40-46, xrandom.m:24-29): real normals on the
+    k-space lattice from the k stream, the filter, xift (ifft along each space
+    dimension, Applications/SPDE/xift.m), times the scale."""
+    z = philox.normals(nk, p.nspace, p.ensembles[0], draw, p.block, p.seed, p.get("seq", 0), kstream=True)
+    zk = freshape(z, [nk] + p.space + [p.ensembles[0]]).astype(complex)
+    zk = np.asarray(filt(zk, p), dtype=complex)                          # :42
+    for d in range(1, p.dimensions):                                     # xift.m:8-10
+        zk = np.fft.ifft(zk, axis=d)
+    return zk * scale                                                    # :43
+
+
 def philox_noisegen(w1, nc, s, p):
     """p.noisegen replacement: Gaussian noise * sqrt(s*noisefactor), coarse
     pass averages two fine draws (xnoise.m:29-38).  The draw index comes
-    from ``p.draw`` which xpath advances once per call."""
+    from ``p.draw`` which xpath advances once per call.  With knoises the
+    cells [Gaussian (if noises > 0), k-filtered] come as ``Cells``."""
+    if p.knoises > 0:
+        cells = Cells()
+        if p.noises > 0:
+            z = philox.normals(p.noises, p.nspace, p.ensembles[0], p.draw, p.block, p.seed, p.get("seq", 0),
+                               p.space[0] if p.space else 1)
+            cells.append(freshape(z, [p.noises] + p.space + [p.ensembles[0]]) * math.sqrt(s * p.noisefactor))
+        cells.append(_kcells(p.knoises, p.draw, p.nfilter, math.sqrt(s * p.knoisefactor), p))
+        if w1 is not None and p.checks[0] and nc == 2:                   # :33-35, :45-47
+            cells = Cells((x + y) / 2 for x, y in zip(cells, w1))
+        return cells
     if p.noises <= 0:
         return 0
     z = philox.normals(p.noises, p.nspace, p.ensembles[0], p.draw, p.block, p.seed, p.get("seq", 0),
@@ -733,7 +776,16 @@ def philox_noisegen(w1, nc, s, p):
 
 def philox_randomgen(p):
     """p.randomgen replacement: initial Gaussian randoms * sqrt(noisefactor)
-    (xrandom.m:20-23), Philox draw 0."""
+    (xrandom.m:20-23), Philox draw 0; with krandoms the cells [Gaussian (if
+    inrandoms > 0), k-filtered * sqrt(knoisefactor)] (xrandom.m:24-29)."""
+    if p.krandoms > 0:
+        cells = Cells()
+        if p.inrandoms > 0:
+            z = philox.normals(p.inrandoms, p.nspace, p.ensembles[0], 0, p.block, p.seed, p.get("seq", 0),
+                               p.space[0] if p.space else 1)
+            cells.append(freshape(z, [p.inrandoms] + p.space + [p.ensembles[0]]) * math.sqrt(p.noisefactor))
+        cells.append(_kcells(p.krandoms, 0, p.rfilter, math.sqrt(p.knoisefactor), p))
+        return cells
     if p.inrandoms <= 0:
         return 0
     z = philox.normals(p.inrandoms, p.nspace, p.ensembles[0], 0, p.block, p.seed, p.get("seq", 0),
@@ -950,7 +1002,7 @@ def xensemble(npar, inputs):
                 v = p.randomgen(p)                                       # :53
                 p.t = p.origins[0]
                 if s == 0:
-                    a = p.initial(v, p)                                  # :60
+                    a = call_cells(p.initial, None, v, p)                # :60
                 else:
                     a = p.transfer(b, v, p)                              # :62
                 a = fit(np.asarray(a, dtype=complex), p.ca)              # :64

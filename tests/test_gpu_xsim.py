@@ -210,3 +210,39 @@ def test_gpu_xsim_raw_matches_oracle():
         for k in range(4):
             assert rg[0][nc][k].shape == (1, 5, 16, 4)
             assert np.allclose(rg[0][nc][k], ro[0][nc][k], rtol=1e-10, atol=1e-12), (nc, k)
+
+
+def test_gpu_xsim_planar_knoise_known_answer():
+    """Examples/SPDE_3D/Planar.m (smaller lattice) through xsim: x-space and
+    k-filtered noise integrals follow the example's comparison (1 + t) nspace, and
+    errors and data match the oracle's xsim."""
+    from xspde_matlab_b200 import xsim
+
+    def init(u, v, p):
+        return np.concatenate([(u[0:1] + 1j * u[1:2]) / np.sqrt(2), (v[0:1] + 1j * v[1:2]) / np.sqrt(2)], axis=0)
+
+    def deriv(a, w, z, p):
+        return np.concatenate([(w[0:1] + 1j * w[1:2]) / np.sqrt(2), (z[0:1] + 1j * z[1:2]) / np.sqrt(2)], axis=0)
+    base = dict(dimensions=3, fields=2, ranges=[1, 5, 5], points=[11, 16, 12], steps=2, noises=2, knoises=2,
+                inrandoms=2, krandoms=2, ensembles=[10, 2, 6], transforms=[[0, 0, 0], [0, 1, 1], [0, 0, 0]],
+                compare=[lambda p: (1 + p.t) * 192, lambda p: (1 + p.t) * 192, lambda p: (1 + p.t) * 192])
+    g = dict(base, initial="@(u,v,p) [(u(1,:)+1i*u(2,:))/sqrt(2); (v(1,:)+1i*v(2,:))/sqrt(2)]",
+             deriv="@(a,w,z,p) [(w(1,:)+1i*w(2,:))/sqrt(2); (z(1,:)+1i*z(2,:))/sqrt(2)]",
+             linear="@(p) 0.5i*(p.Dx.^2+p.Dy.^2)",
+             observe=["@(a,p) Int(a(1,:).*conj(a(1,:)),p)", "@(a,p) Int(a(2,:).*conj(a(2,:)),p)",
+                      "@(a,p) Int(a(2,:).*conj(a(2,:)),p)"])
+    o = dict(base, initial=init, deriv=deriv, linear=lambda p: 0.5j * (p.Dx ** 2 + p.Dy ** 2),
+             observe=[lambda a, p: X.Int(a[0:1] * np.conj(a[0:1]), p), lambda a, p: X.Int(a[1:2] * np.conj(a[1:2]), p),
+                      lambda a, p: X.Int(a[1:2] * np.conj(a[1:2]), p)])
+    eg, dg, ig = xsim(g)
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore", RuntimeWarning)
+        eo, do, io = X.xsim(o)
+    keep = [i for i in range(len(eo)) if i != 5]
+    assert np.allclose(np.asarray(eg)[keep], np.asarray(eo)[keep], rtol=1e-8, atol=1e-14)
+    for a, b in zip(dg[0], do[0]):
+        assert np.allclose(np.asarray(a), np.asarray(b), rtol=1e-9, atol=1e-10)
+    t = io[0].xc[0]
+    for k in range(3):
+        mean, err = np.real(dg[0][k][:, 0]), np.real(dg[0][k][:, 2])
+        assert np.all(np.abs(mean - (1 + t) * 192) < 5 * err), k

@@ -87,3 +87,35 @@ def test_time_spectrum_equilibrium_known_answer():
     assert np.all(np.abs(spec[sel] - exact[sel]) < 5 * err[sel] + 0.02 * exact[sel])
     tdom = np.real(data[0][0][:, 0])
     assert np.all(np.abs(tdom - 1) < 5 * np.real(data[0][0][:, 2]) + 0.02)
+
+
+def _planar_init(u, v, p):
+    return np.concatenate([(u[0:1] + 1j * u[1:2]) / np.sqrt(2), (v[0:1] + 1j * v[1:2]) / np.sqrt(2)], axis=0)
+
+
+def _planar_deriv(a, w, z, p):
+    return np.concatenate([(w[0:1] + 1j * w[1:2]) / np.sqrt(2), (z[0:1] + 1j * z[1:2]) / np.sqrt(2)], axis=0)
+
+
+def test_knoise_planar_known_answer():
+    """Examples/SPDE_3D/Planar.m on a smaller lattice: x-space noise drives a_1 and
+    k-filtered noise (knoises, krandoms; Simulator/xnoise.m:39-50, xrandom.m:24-29)
+    drives a_2; both integrals grow as the example's comparison (1 + t) nspace, and
+    the k-space integral of |a_2(k)|^2 dk equals the x-space one (Parseval)."""
+    o = dict(dimensions=3, fields=2, ranges=[1, 5, 5], points=[11, 16, 12], steps=2, noises=2, knoises=2,
+             inrandoms=2, krandoms=2, ensembles=[10, 2, 6], initial=_planar_init, deriv=_planar_deriv,
+             linear=lambda p: 0.5j * (p.Dx ** 2 + p.Dy ** 2),
+             observe=[lambda a, p: X.Int(a[0:1] * np.conj(a[0:1]), p),
+                      lambda a, p: X.Int(a[1:2] * np.conj(a[1:2]), p.dk, p),
+                      lambda a, p: X.Int(a[1:2] * np.conj(a[1:2]), p)],
+             transforms=[[0, 0, 0], [0, 1, 1], [0, 0, 0]])
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore", RuntimeWarning)
+        e, data, inp = X.xsim(o)
+    p = inp[0]
+    t = p.xc[0]
+    exact = (1 + t) * p.nspace
+    for k in range(3):
+        mean, err = np.real(data[0][k][:, 0]), np.real(data[0][k][:, 2])
+        assert np.all(np.abs(mean - exact) < 5 * err + 1e-9 * exact), k
+    assert np.allclose(data[0][1][:, 0], data[0][2][:, 0], rtol=1e-10)

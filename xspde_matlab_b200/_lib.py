@@ -54,6 +54,10 @@ class XsProblem(ctypes.Structure):
         ("transforms", ctypes.POINTER(ctypes.c_int)),
         ("sequence", ctypes.c_int),
         ("boundary_values", ctypes.c_int),
+        ("knoises", ctypes.c_int),
+        ("krandoms", ctypes.c_int),
+        ("nfilter", ctypes.POINTER(ctypes.c_double)),
+        ("rfilter", ctypes.POINTER(ctypes.c_double)),
     ]
 
 

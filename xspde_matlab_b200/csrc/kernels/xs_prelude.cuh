@@ -248,6 +248,16 @@ __device__ __forceinline__ void xs_normals(real* z, u32 s, u32 e, u32 q, u32 seq
   }
 }
 
+// One standard normal of component k from the k-space stream (k-filtered
+// noises and randoms): the fourth counter word carries bit 15, no site pairing.
+__device__ __forceinline__ real xs_knormal(int k, u32 s, u32 e, u32 q, u32 seq, u32 seed, u32 block) {
+  const uint4 w = xs_philox(make_uint4(s, e, q, (u32)(k >> 2) | 0x8000u | (seq << 16)), seed, block);
+  real z0, z1;
+  if (k & 2) xs_boxmuller(w.z, w.w, z0, z1);
+  else xs_boxmuller(w.x, w.y, z0, z1);
+  return (k & 1) ? z1 : z0;
+}
+
 // ---- block reductions --------------------------------------------------------
 __device__ __forceinline__ double xs_warp_sum(double v) {
 #pragma unroll

@@ -49,6 +49,10 @@ struct XsPathArgs {
   double fscn;          // XS_SPEC: p.fsc / nt
   double2* raw;         // optional raw trajectories (p.rawdata, xpath.m:72-77): the field at every
                         // output time in MATLAB's layout [F][npoints][NS][ntraj], fastest first
+  const double2* kfilt; // XS_NK: [NK][NS] factors of p.nfilter on the FFT-ordered k lattice (null: 1)
+  const double2* rfilt; // XS_NKV: the same for p.rfilter
+  double kwscale;       // sqrt(nscale * knoisefactor), knoisefactor = prod(space points) / dv
+  double kvscale;       // sqrt(knoisefactor)
 };
 
 // XS_GFIELD: the lattice is too large for shared memory, so each CTA keeps its
@@ -60,9 +64,24 @@ struct XsPathArgs {
 #define XS_NOMERGE (XS_BVAL || XS_SPEC)
 // complex elements of one CTA's slice: the field arrays, then (methods other
 // than MP) the two noise arrays of reals
-#define XS_GSLICE ((size_t)(XS_NARR + XS_KARR) * XS_G * XS_F * XS_NS + (size_t)XS_WARR * XS_G * XS_NWS * XS_NS * sizeof(real) / sizeof(cx))
+#define XS_GSLICE ((size_t)(XS_NARR + XS_KARR + XS_KNARR) * XS_G * XS_F * XS_NS + (size_t)XS_WARR * XS_G * XS_NWS * XS_NS * sizeof(real) / sizeof(cx))
 
 extern __shared__ __align__(16) unsigned char xs_smem[];
+
+// k-filtered noise arrays (XS_KNARR field-sized complex arrays after the field
+// arrays): ceil(NK/F) chunks of the current draw, as many of the first coarse
+// draw, then ceil(NKV/F) chunks of the k-filtered randoms.  Component k of
+// trajectory g at site s is element (k / F) G F NS + (g F + k % F) NS + s.
+__device__ __forceinline__ cx* xs_zbuf(const XsPathArgs& P) {
+  constexpr size_t GF = (size_t)XS_G * XS_F * XS_NS;
+#if XS_GFIELD
+  return P.gfield + (size_t)blockIdx.x * XS_GSLICE + (XS_NARR + XS_KARR) * GF;
+#else
+  (void)P;
+  return (cx*)xs_smem + (XS_NARR + XS_KARR) * GF;
+#endif
+}
+#define XS_ZIDX(k, g, s) ((size_t)((k) / XS_F) * (XS_G * XS_F * XS_NS) + ((g) * XS_F + (k) % XS_F) * XS_NS + (s))
 
 #define XS_STRIDE1 1
 #define XS_STRIDE2 (XS_N1)
@@ -416,12 +435,66 @@ __device__ __forceinline__ void xs_prop(cx* X, cx* T, const XsPathArgs& P, doubl
   xs_prop_tab(X, T, P, P.prop, tb);
 }
 
+#if XS_NK > 0 || XS_NKV > 0
+// k-filtered Gaussian cell (Simulator/xnoise.m:40-46, xrandom.m:24-29): real
+// standard normals on the FFT-ordered k lattice from the k stream, times the
+// FP64 filter factor and the scale, then the inverse DFT along every space
+// dimension (Applications/SPDE/xift.m) with the field's own transforms, one
+// field-sized chunk at a time.
+template <int NC>
+__device__ void xs_kgen(cx* X, cx* T, const XsPathArgs& P, const double2* filt, int g0, int draw, double scale) {
+  constexpr int GF = XS_G * XS_F * XS_NS;
+  constexpr int NCH = (NC + XS_F - 1) / XS_F;
+  __syncthreads();
+  for (int i = threadIdx.x; i < NCH * GF; i += blockDim.x) {
+    const int ch = i / GF, r = i - ch * GF;
+    const int s = r % XS_NS, gf = r / XS_NS;
+    const int f = gf % XS_F, g = gf / XS_F;
+    const int k = ch * XS_F + f;
+    cx v = mkcx((real)0, (real)0);
+    if (k < NC) {
+      const int e = g0 + g;
+      const double zr = (double)xs_knormal(k, (u32)s, (u32)(e % P.ens1), (u32)draw, (u32)P.seq, P.seed,
+                                           (u32)(P.block0 + e / P.ens1));
+      const double2 fv = filt ? filt[(size_t)k * XS_NS + s] : make_double2(1.0, 0.0);
+      v = mkcx((real)(zr * fv.x * scale), (real)(zr * fv.y * scale));
+    }
+    X[i] = v;
+  }
+  __syncthreads();
+  for (int ch = 0; ch < NCH; ++ch) {
+    cx* C = X + (size_t)ch * GF;
+    xs_tr<1>(C, T, P, 1);
+    xs_tr<2>(C, T, P, 1);
+    xs_tr<3>(C, T, P, 1);
+  }
+  __syncthreads();
+}
+#endif
+
+// k-filtered noise of one p.noisegen call (xnoise.m:39-50): mode 0 fine draw,
+// 1 first coarse draw (kept), 2 second coarse draw averaged with the first.
+__device__ __forceinline__ void xs_knoise(const XsPathArgs& P, cx* T, int mode, int draw, int g0) {
+#if XS_NK > 0
+  constexpr size_t GF = (size_t)XS_G * XS_F * XS_NS;
+  cx* Z = xs_zbuf(P);
+  cx* Zp = Z + XS_NKC * GF;
+  xs_kgen<XS_NK>(mode == 1 ? Zp : Z, T, P, P.kfilt, g0, draw, P.kwscale);
+  if (mode == 2) {
+    for (size_t i = threadIdx.x; i < XS_NKC * GF; i += blockDim.x) Z[i] = (Z[i] + Zp[i]) * (real)0.5;
+    __syncthreads();
+  }
+#else
+  (void)P; (void)T; (void)mode; (void)draw; (void)g0;
+#endif
+}
+
 // dst = base + h * deriv(src, w, t), pointwise over sites (all components at once).
 // dst = base + h * deriv(src, w, t).  A drift with finite differences
 // (XS_STENCIL) reads neighbours of src, so an in-place update (dst == src)
 // writes through the transform scratch T first.
-__device__ __forceinline__ void xs_deriv_update(cx* dst, const cx* base, const cx* src, const real* W, real h, double t,
-                                                const double* prm, cx* T) {
+__device__ __forceinline__ void xs_deriv_update(cx* dst, const cx* base, const cx* src, const real* W, const cx* Z,
+                                                real h, double t, const double* prm, cx* T) {
   cx* out = (XS_STENCIL && dst == src) ? T : dst;
   for (int i = threadIdx.x; i < XS_G * XS_NS; i += blockDim.x) {
     const int g = i / XS_NS, s = i % XS_NS;
@@ -434,7 +507,11 @@ __device__ __forceinline__ void xs_deriv_update(cx* dst, const cx* base, const c
     for (int f = 0; f < XS_F; ++f) a[f] = src[(g * XS_F + f) * XS_NS + s];
 #pragma unroll
     for (int c = 0; c < XS_NW; ++c) w[c] = W[(g * XS_NWS + c) * XS_NS + s];
-    xs_deriv(a, w, x, y, z, (real)t, prm, src, g, s, d);
+    cx zk[XS_NK > 0 ? XS_NK : 1];
+#pragma unroll
+    for (int k = 0; k < XS_NK; ++k) zk[k] = Z[XS_ZIDX(k, g, s)];
+    (void)Z;
+    xs_deriv(a, w, zk, x, y, z, (real)t, prm, src, g, s, d);
 #pragma unroll
     for (int f = 0; f < XS_F; ++f) {
       const int j = (g * XS_F + f) * XS_NS + s;
@@ -461,13 +538,15 @@ __device__ __forceinline__ void xs_copy(cx* dst, const cx* src) {
 // start of the step (xpath's p.t).
 __device__ void xs_method(cx* A, cx* B1, cx* B2, cx* B3, cx* T, const real* W, const XsPathArgs& P, double t) {
   const double dtr = P.dtr;
+  const cx* Z = xs_zbuf(P);
+  (void)Z;
 #if XS_METHOD == 0
   // MP (Applications/SDE/MP.m:10-27)
   const real h = (real)(dtr * 0.5);
   xs_prop(A, T, P, t);
   xs_copy(B1, A);
   for (int it = 0; it < XS_ITER; ++it) {
-    xs_deriv_update(A, B1, A, W, h, t + dtr * 0.5, P.params, T);
+    xs_deriv_update(A, B1, A, W, Z, h, t + dtr * 0.5, P.params, T);
     xs_setbound(A, &P, t + dtr * 0.5);
   }
   xs_axpby(A, (real)2, A, (real)-1, B1);
@@ -476,35 +555,35 @@ __device__ void xs_method(cx* A, cx* B1, cx* B2, cx* B3, cx* T, const real* W, c
   // RK4 (Applications/SDE/RK4.m:35-70)
   const real h = (real)(dtr * 0.5);
   xs_setbound(A);
-  xs_deriv_update(B1, A, A, W, h, t, P.params, T);
+  xs_deriv_update(B1, A, A, W, Z, h, t, P.params, T);
   xs_prop(B1, T, P);
   xs_prop(A, T, P);
-  xs_deriv_update(B2, A, B1, W, h, t + dtr * 0.5, P.params, T);
+  xs_deriv_update(B2, A, B1, W, Z, h, t + dtr * 0.5, P.params, T);
   xs_setbound(B2);
-  xs_deriv_update(B3, A, B2, W, (real)(2 * (dtr * 0.5)), t + dtr * 0.5, P.params, T);
+  xs_deriv_update(B3, A, B2, W, Z, (real)(2 * (dtr * 0.5)), t + dtr * 0.5, P.params, T);
   xs_setbound(B3);
   for (int i = threadIdx.x; i < XS_G * XS_F * XS_NS; i += blockDim.x)
     A[i] = (B1[i] + (real)2 * B2[i] + B3[i] - A[i]) / (real)3;
   __syncthreads();
   xs_prop(A, T, P);
   xs_prop(B3, T, P);
-  xs_deriv_update(A, A, B3, W, (real)(dtr * 0.5 / 3.0), t + dtr, P.params, T);
+  xs_deriv_update(A, A, B3, W, Z, (real)(dtr * 0.5 / 3.0), t + dtr, P.params, T);
   xs_setbound(A);
 #elif XS_METHOD == 2
   // Euler (Applications/SDE/Euler.m:77-81)
-  xs_deriv_update(A, A, A, W, (real)dtr, t, P.params, T);
+  xs_deriv_update(A, A, A, W, Z, (real)dtr, t, P.params, T);
   xs_prop(A, T, P);
 #elif XS_METHOD == 3
   // RK2 (Applications/SDE/RK2.m:89-107): B1 holds the predictor a.
-  xs_deriv_update(B1, A, A, W, (real)dtr, t, P.params, T);
+  xs_deriv_update(B1, A, A, W, Z, (real)dtr, t, P.params, T);
   xs_prop(A, T, P);
   xs_prop(B1, T, P);
-  xs_deriv_update(A, A, B1, W, (real)dtr, t + dtr, P.params, T);
+  xs_deriv_update(A, A, B1, W, Z, (real)dtr, t + dtr, P.params, T);
   xs_axpby(A, (real)0.5, B1, (real)0.5, A);
 #elif XS_METHOD == 4
   // Implicit (Applications/SDE/Implicit.m:116-125)
   xs_copy(B1, A);
-  for (int it = 0; it < XS_ITER; ++it) xs_deriv_update(A, B1, A, W, (real)dtr, t + dtr, P.params, T);
+  for (int it = 0; it < XS_ITER; ++it) xs_deriv_update(A, B1, A, W, Z, (real)dtr, t + dtr, P.params, T);
   xs_prop(A, T, P);
 #endif
   __syncthreads();
@@ -558,11 +637,19 @@ __device__ void xs_mp_lean(cx* A, cx* T, const XsPathArgs& P, double t, int g0, 
 #else
     w[0] = (real)0;
 #endif
+    cx zk[XS_NK > 0 ? XS_NK : 1];
+#if XS_NK > 0
+    {
+      const cx* Z = xs_zbuf(P);
+#pragma unroll
+      for (int k = 0; k < XS_NK; ++k) zk[k] = Z[XS_ZIDX(k, g, s)];
+    }
+#endif
     cx a0[XS_F], a[XS_F], d[XS_F];
 #pragma unroll
     for (int f = 0; f < XS_F; ++f) a0[f] = a[f] = A[(g * XS_F + f) * XS_NS + s];
     for (int it = 0; it < XS_ITER; ++it) {
-      xs_deriv(a, w, x, y, z, tm, P.params, A, g, s, d);
+      xs_deriv(a, w, zk, x, y, z, tm, P.params, A, g, s, d);
 #pragma unroll
       for (int f = 0; f < XS_F; ++f) {
         a[f] = a0[f] + h * d[f];
@@ -765,7 +852,7 @@ __device__ void xs_spectrum(const XsPathArgs& P, int cta) {
 // not match the layout; the CTA must then return without touching it.
 __device__ __forceinline__ bool xs_layout_ok(int* status) {
   constexpr size_t GF = (size_t)XS_G * XS_F * XS_NS;
-  constexpr size_t need = ((XS_GFIELD ? 0 : XS_NARR + XS_KARR) * GF + 2 * (size_t)XS_TILE_ELEMS) * sizeof(cx) + (size_t)XS_G * (XS_NRED > 0 ? XS_NRED : 1) * sizeof(cx) +
+  constexpr size_t need = ((XS_GFIELD ? 0 : XS_NARR + XS_KARR + XS_KNARR) * GF + 2 * (size_t)XS_TILE_ELEMS) * sizeof(cx) + (size_t)XS_G * (XS_NRED > 0 ? XS_NRED : 1) * sizeof(cx) +
                           32 * 2 * (XS_NRED > 0 ? XS_NRED : 1) * sizeof(double) +
                           (XS_GFIELD ? 0 : XS_WARR) * (size_t)XS_G * XS_NWS * XS_NS * sizeof(real);
   u32 dyn;
@@ -786,7 +873,7 @@ __device__ void xs_resident_run(const XsPathArgs& P, int cta, int nctas) {
   cx* RED = (cx*)xs_smem + 2 * XS_TILE_ELEMS;  // after the two transform tiles; [G][NRED]
 #else
   cx* A = (cx*)xs_smem;
-  cx* RED = A + (XS_NARR + XS_KARR) * GF;  // [G][NRED]
+  cx* RED = A + (XS_NARR + XS_KARR + XS_KNARR) * GF;  // [G][NRED]
 #endif
   cx* K = A + XS_NARR * GF;  // k-space copy of the field (XS_KARR)
   cx* B1 = A + GF;
@@ -795,7 +882,7 @@ __device__ void xs_resident_run(const XsPathArgs& P, int cta, int nctas) {
   cx* T = A + (XS_NARR - 1) * GF;     // transform scratch is the last array
   double* wsum = (double*)(RED + XS_G * (XS_NRED > 0 ? XS_NRED : 1));  // [32][2*NRED]
 #if XS_GFIELD
-  real* W = (real*)(A + (XS_NARR + XS_KARR) * GF);  // noise arrays follow the field arrays in the CTA's slice
+  real* W = (real*)(A + (XS_NARR + XS_KARR + XS_KNARR) * GF);  // noise arrays follow the field arrays in the CTA's slice
 #else
   real* W = (real*)(wsum + 32 * 2 * (XS_NRED > 0 ? XS_NRED : 1));
 #endif
@@ -807,6 +894,10 @@ __device__ void xs_resident_run(const XsPathArgs& P, int cta, int nctas) {
   }
 
   // initial field: p.initial(v,p) with v = p.randomgen(p) (xensemble.m:53-64)
+#if XS_NKV > 0
+  cx* VK = xs_zbuf(P) + 2 * XS_NKC * GF;  // k-filtered randoms (xrandom.m:24-29), draw 0 of the k stream
+  if (!P.a_in) xs_kgen<XS_NKV>(VK, T, P, P.rfilt, g0, 0, P.kvscale);
+#endif
   for (int i = threadIdx.x; i < XS_G * XS_NS; i += blockDim.x) {
     const int g = i / XS_NS, s = i % XS_NS;
     const int e = g0 + g;
@@ -827,7 +918,12 @@ __device__ void xs_resident_run(const XsPathArgs& P, int cta, int nctas) {
 #pragma unroll
       for (int c = 0; c < XS_NV; ++c) v[c] *= (real)P.vscale;
 #endif
-      xs_initial(v, x, y, z, P.params, a);
+      cx vk[XS_NKV > 0 ? XS_NKV : 1];
+#if XS_NKV > 0
+#pragma unroll
+      for (int k = 0; k < XS_NKV; ++k) vk[k] = VK[XS_ZIDX(k, g, s)];
+#endif
+      xs_initial(v, vk, x, y, z, P.params, a);
     }
 #pragma unroll
     for (int f = 0; f < XS_F; ++f) A[(g * XS_F + f) * XS_NS + s] = a[f];
@@ -862,6 +958,7 @@ __device__ void xs_resident_run(const XsPathArgs& P, int cta, int nctas) {
           ++draw;
           int mode = 0;
           if (P.nc == 2 && P.checks) mode = chk == 0 ? 1 : 2;
+          if (XS_NK > 0) xs_knoise(P, T, mode, draw, g0);
 #if XS_LEAN
           if (P.nc == 1 || chk == 1) {
             __syncthreads();
@@ -1030,6 +1127,10 @@ extern "C" __global__ void __launch_bounds__(XS_THREADS) xs_batch(const XsBatchA
     P.nt = 0;
     P.fscn = 0;
     P.raw = nullptr;
+    P.kfilt = nullptr;
+    P.rfilt = nullptr;
+    P.kwscale = 0;
+    P.kvscale = 0;
     xs_resident_run(P, un.y, it.nunits);
     // publish this unit's partial sums, then count it (threadFenceReduction pattern)
     __threadfence();

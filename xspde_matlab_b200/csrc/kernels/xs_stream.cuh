@@ -170,7 +170,7 @@ __device__ __forceinline__ void xs_xpass_body(const XsStreamArgs& A) {
 #pragma unroll
         for (int c = 0; c < XS_NV; ++c) vv[c] *= (real)A.vscale;
 #endif
-        xs_initial(vv, x, yy, (real)0, A.params, a);
+        xs_initial(vv, (const cx*)nullptr, x, yy, (real)0, A.params, a);
       }
 #pragma unroll
       for (int f = 0; f < XS_F; ++f) v[f][j] = a[f];
@@ -205,7 +205,7 @@ __device__ __forceinline__ void xs_xpass_body(const XsStreamArgs& A) {
       for (int f = 0; f < XS_F; ++f) a0[f] = a[f] = stage[(f * XS_RX + j) * XS_RX + t];
 #pragma unroll
       for (int it = 0; it < XS_ITER; ++it) {
-        xs_deriv(a, w, x, yy, (real)0, tm, A.params, (const cx*)nullptr, 0, 0, d);
+        xs_deriv(a, w, (const cx*)nullptr, x, yy, (real)0, tm, A.params, (const cx*)nullptr, 0, 0, d);
 #pragma unroll
         for (int f = 0; f < XS_F; ++f) a[f] = a0[f] + h * d[f];
       }

@@ -243,6 +243,8 @@ struct Problem {
   bool dstencil = false;                   // the drift uses D1/D2: no fused MP iterations
   bool bvals = false;                      // boundary values of p.boundfun supplied per pass
   bool spec = false;                       // some observable is evaluated on the time spectrum
+  int NK = 0, NKV = 0;                     // k-filtered noises / initial randoms (xnoise.m:39-50, xrandom.m:24-29)
+  std::vector<double> kfilt, rfilt;        // [NK][NS] / [NKV][NS] complex filter factors (empty: identity)
   std::vector<double> runtime_defaults;
   std::vector<int> bnd;  // [D][F][2]
   int D = 0, F = 1, NW = 0, NV = 0, NS = 1, E1 = 1;
@@ -341,6 +343,20 @@ void setup_problem(const xs_problem* in, Problem& P) {
       }
   }
   P.p.boundaries = nullptr;
+  if (p.knoises < 0 || p.knoises > 32 || p.krandoms < 0 || p.krandoms > 32)
+    raise(XS_ERR_SHAPE, "knoises/krandoms must be 0..32");
+  P.NK = p.knoises;
+  P.NKV = p.krandoms;
+  if (P.NK || P.NKV) {
+    if (P.D == 0) raise(XS_ERR_UNSUPPORTED, "k-filtered noises need at least one space dimension");
+    for (int d = 0; d < P.D; ++d)
+      for (int f = 0; f < P.F; ++f)
+        if (P.type(d, f) != 0)
+          raise(XS_ERR_UNSUPPORTED, "k-filtered noises need periodic space dimensions (xift.m: inverse DFT)");
+    if (p.nfilter && P.NK) P.kfilt.assign(p.nfilter, p.nfilter + (size_t)2 * P.NK * P.NS);
+    if (p.rfilter && P.NKV) P.rfilt.assign(p.rfilter, p.rfilter + (size_t)2 * P.NKV * P.NS);
+  }
+  P.p.nfilter = P.p.rfilter = nullptr;
   if (p.boundary_values) {
     if (P.bnd.empty()) raise(XS_ERR_ARG, "boundary values given but every boundary is periodic");
     if (p.method != XS_METHOD_MP) raise(XS_ERR_UNSUPPORTED, "boundary values (p.boundfun) are supported with MP");
@@ -524,6 +540,8 @@ xs::GenCtx make_ctx(const Problem& P, std::vector<xs::Role> roles, bool reduce) 
   c.nfield = P.F;
   c.nnoise = P.NW;
   c.nrand = P.NV;
+  c.nknoise = P.NK;
+  c.nkrand = P.NKV;
   c.ndim = P.D;
   c.allow_reduce = reduce;
   c.kgrid = reduce;  // observe functions may read p.kx/ky/kz
@@ -544,15 +562,20 @@ void generate_functions(Problem& P, std::ostringstream& os) {
   // deriv(a, w, p): xSPDE calls p.deriv{c}(a{:}, xi{:}, p) (MP.m:16)
   {
     auto fn = xs::parse_anon(P.deriv);
-    auto g = xs::generate(fn, make_ctx(P, {Role::Field, Role::Noise, Role::Params}, false));
+    // noise cells in xnoise.m order: Gaussian (absent when noises = 0 and knoises > 0), k-filtered
+    std::vector<Role> roles = {Role::Field};
+    if (P.NW > 0 || P.NK == 0) roles.push_back(Role::Noise);
+    if (P.NK > 0) roles.push_back(Role::KNoise);
+    roles.push_back(Role::Params);
+    auto g = xs::generate(fn, make_ctx(P, roles, false));
     if (g.len != P.F && g.len != 1)
       raise(XS_ERR_SHAPE, "p.deriv returns " + std::to_string(g.len) + " components, fields = " + std::to_string(P.F));
     P.dstencil = g.stencil;
     os << "#define XS_STENCIL " << (g.stencil ? 1 : 0) << "\n";
     os << "__device__ __forceinline__ cx xs_fd1(const cx* __restrict__ fld, int g, int s, int f, int d);\n";
     os << "__device__ __forceinline__ cx xs_fd2(const cx* __restrict__ fld, int g, int s, int f, int d);\n";
-    os << "__device__ __forceinline__ void xs_deriv(const cx* __restrict__ a, const real* __restrict__ w, real x, real y, real z, real t, const double* __restrict__ prm, const cx* __restrict__ fld, int g, int s, cx* __restrict__ out) {\n";
-    os << "  (void)a; (void)w; (void)x; (void)y; (void)z; (void)t; (void)prm; (void)fld; (void)g; (void)s;\n";
+    os << "__device__ __forceinline__ void xs_deriv(const cx* __restrict__ a, const real* __restrict__ w, const cx* __restrict__ zk, real x, real y, real z, real t, const double* __restrict__ prm, const cx* __restrict__ fld, int g, int s, cx* __restrict__ out) {\n";
+    os << "  (void)a; (void)w; (void)zk; (void)x; (void)y; (void)z; (void)t; (void)prm; (void)fld; (void)g; (void)s;\n";
     if (g.len == 1 && P.F > 1) {
       os << "  cx o1[1];\n  { cx* out = o1;\n" << g.code << "  }\n";
       os << "  for (int f = 0; f < " << P.F << "; ++f) out[f] = o1[0];\n";
@@ -564,11 +587,15 @@ void generate_functions(Problem& P, std::ostringstream& os) {
   // initial(v, p) (xensemble.m:60)
   {
     auto fn = xs::parse_anon(P.initial);
-    auto g = xs::generate(fn, make_ctx(P, {Role::Random, Role::Params}, false));
+    std::vector<Role> roles;  // random cells in xrandom.m order: Gaussian, k-filtered
+    if (P.NV > 0 || P.NKV == 0) roles.push_back(Role::Random);
+    if (P.NKV > 0) roles.push_back(Role::KRandom);
+    roles.push_back(Role::Params);
+    auto g = xs::generate(fn, make_ctx(P, roles, false));
     if (g.len != P.F && g.len != 1)
       raise(XS_ERR_SHAPE, "p.initial returns " + std::to_string(g.len) + " components, fields = " + std::to_string(P.F));
-    os << "__device__ __forceinline__ void xs_initial(const real* __restrict__ v, real x, real y, real z, const double* __restrict__ prm, cx* __restrict__ out) {\n";
-    os << "  (void)v; (void)x; (void)y; (void)z; (void)prm; const real t = (real)" << fmt(P.p.origins[0]) << "; (void)t;\n";
+    os << "__device__ __forceinline__ void xs_initial(const real* __restrict__ v, const cx* __restrict__ vk, real x, real y, real z, const double* __restrict__ prm, cx* __restrict__ out) {\n";
+    os << "  (void)v; (void)vk; (void)x; (void)y; (void)z; (void)prm; const real t = (real)" << fmt(P.p.origins[0]) << "; (void)t;\n";
     if (g.len == 1 && P.F > 1) {
       os << "  cx o1[1];\n  { cx* out = o1;\n" << g.code << "  }\n";
       os << "  for (int f = 0; f < " << P.F << "; ++f) out[f] = o1[0];\n";
@@ -854,10 +881,11 @@ struct xs_handle {
   CUfunction f_batch = nullptr;
   cudaStream_t stream = nullptr;
   DevBuf d_prop[2], d_prop2[2], d_tmat, d_obs, d_av, d_ain, d_aout, d_status, d_w, d_field, d_redpart, d_pstep,
-      d_params, d_gfield, d_twiddle, d_tmp, d_avm, d_bval[2], d_bda[2], d_aft, d_twt, d_raw;
+      d_params, d_gfield, d_twiddle, d_tmp, d_avm, d_bval[2], d_bda[2], d_aft, d_twt, d_raw, d_kfilt, d_rfilt;
   int bval_n[2] = {0, 0};
   int twt_n = 0;
   void* raw_dev = nullptr;  // raw trajectories of the current resident launch (xs_run_path_raw)
+  bool kfilt_up = false;    // k-noise filter tables uploaded
   double pstep_dtr = -1;
   double prop_dtr[2] = {-1, -1}, prop2_dtr[2] = {-1, -1};
   // launch accounting (xs_kernel_stats)
@@ -912,6 +940,10 @@ void tile_plan(const Problem& P, bool fp64, int tl[3], int lsp[3], size_t& elems
   }
 }
 
+// Field-sized complex arrays of the k-filtered noise: the current and the
+// first coarse draw (ceil(NK/F) chunks each), then the k-filtered randoms.
+int knarr(const Problem& P) { return 2 * ((P.NK + P.F - 1) / P.F) + (P.NKV + P.F - 1) / P.F; }
+
 // MP with its midpoint iterations fused per site (noise in registers); not
 // possible when the drift reads neighbouring sites.
 bool lean_mp(const Problem& P) { return P.p.method == XS_METHOD_MP && !P.dstencil; }
@@ -925,6 +957,7 @@ size_t resident_smem(const xs_handle& h, int G, int narr) {
   size_t tiles = 0;
   if (narr == 0) warr = 0;  // field in device memory: the noise arrays live in the CTA's slice too
   if (narr > 0 && P.kobs) narr += 1;  // the k-space copy of the field for transformed observables
+  if (narr > 0) narr += knarr(P);      // k-filtered noise arrays (in the slice when the field is in device memory)
   if (narr == 0) {  // field in device memory: two transform tiles in shared memory
     int tl[3], lsp[3];
     tile_plan(P, h.fp64, tl, lsp, tiles);
@@ -1077,6 +1110,7 @@ std::string stream_blocker(const Problem& P) {
     if (o.spatial && !o.gen.reductions.empty()) return "site observables that use Int/Ave are not streamed";
   if (P.kobs) return "k-space observables (p.transforms) are not streamed";
   if (P.spec) return "time-spectrum observables (p.transforms{n}(1)) are not streamed";
+  if (P.NK || P.NKV) return "k-filtered noises are not streamed";
   if (P.stencil) return "observables with D1/D2 finite differences are not streamed";
   if (P.dstencil) return "drifts with D1/D2 finite differences are not streamed";
   return "";
@@ -1163,6 +1197,8 @@ void emit_common_header(const xs_handle& h, std::ostringstream& os) {
   os << "#define XS_METHOD " << P.p.method << "\n#define XS_ITER " << P.p.iterations << "\n";
   os << "#define XS_HAS_PROP " << ((P.has_linear && P.D > 0) ? 1 : 0) << "\n#define XS_PROP_COMPS " << P.Lc << "\n";
   os << "#define XS_SETBOUND " << (P.setbound ? 1 : 0) << "\n";
+  os << "#define XS_NK " << P.NK << "\n#define XS_NKV " << P.NKV << "\n#define XS_NKC " << (P.NK + P.F - 1) / P.F
+     << "\n#define XS_NKVC " << (P.NKV + P.F - 1) / P.F << "\n#define XS_KNARR " << knarr(P) << "\n";
   os << xs_kernel_source_noise << "\n";
 }
 
@@ -1426,6 +1462,10 @@ struct PathArgsHost {
   int pad4;
   double fscn;
   void* raw;
+  const void* kfilt;
+  const void* rfilt;
+  double kwscale;
+  double kvscale;
 };
 
 size_t av_stride(const Problem& P) { return (size_t)P.nout_site * P.NS + P.nout_scalar; }
@@ -1476,7 +1516,7 @@ int resident_grid(xs_handle& h, CUfunction f, int nctas) {
   CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   cu_check(driver().occupancy(&occ, f, h.rp.threads, h.rp.smem), "occupancy");
   const size_t warr = lean_mp(h.P) ? 0 : 2;
-  const size_t slice = (size_t)(h.rp.narr + (h.P.kobs ? 1 : 0)) * h.rp.G * h.P.F * h.P.NS * (h.fp64 ? 16 : 8) +
+  const size_t slice = (size_t)(h.rp.narr + (h.P.kobs ? 1 : 0) + knarr(h.P)) * h.rp.G * h.P.F * h.P.NS * (h.fp64 ? 16 : 8) +
                        warr * h.rp.G * std::max(h.P.NW, 1) * h.P.NS * (h.fp64 ? 8 : 4);
   const int l2 = (int)std::max<size_t>(1, (96u << 20) / slice);
   // slices that fit L2 for a full wave: cap the grid there; larger slices stream from HBM anyway,
@@ -1564,6 +1604,25 @@ void launch_resident(xs_handle& h, int first_block, int nblocks, int nc, const v
   a.params = (const double*)h.d_params.p;
   if (P.spec) spectrum_buffers(h, nctas, a);
   a.raw = h.raw_dev;
+  if (P.NK || P.NKV) {
+    // k-filtered noise (xnoise.m:43) and randoms (xrandom.m:27): knoisefactor = prod(space points) / dv
+    if (!h.kfilt_up) {
+      if (!P.kfilt.empty()) {
+        h.d_kfilt.ensure(P.kfilt.size() * 8);
+        CUDA_CHECK(cudaMemcpy(h.d_kfilt.p, P.kfilt.data(), P.kfilt.size() * 8, cudaMemcpyHostToDevice));
+      }
+      if (!P.rfilt.empty()) {
+        h.d_rfilt.ensure(P.rfilt.size() * 8);
+        CUDA_CHECK(cudaMemcpy(h.d_rfilt.p, P.rfilt.data(), P.rfilt.size() * 8, cudaMemcpyHostToDevice));
+      }
+      h.kfilt_up = true;
+    }
+    const double kf = (double)P.NS / P.dv;
+    a.kfilt = P.kfilt.empty() ? nullptr : h.d_kfilt.p;
+    a.rfilt = P.rfilt.empty() ? nullptr : h.d_rfilt.p;
+    a.kwscale = std::sqrt(P.nscale * kf);
+    a.kvscale = std::sqrt(kf);
+  }
   const int grid = resident_grid(h, h.f_resident, nctas);
   a.gfield = h.d_gfield.p;
   void* params[] = {&a};
@@ -2017,6 +2076,7 @@ XS_API xs_status xs_run_path_device_noalloc(xs_handle* h, int first_block, int n
       raise(XS_ERR_UNSUPPORTED, "xs_run_path_device_noalloc needs the field in shared memory (it would allocate slices)");
     if (h->P.bvals) raise(XS_ERR_UNSUPPORTED, "xs_run_path_device_noalloc does not take boundary values");
     if (h->P.spec) raise(XS_ERR_UNSUPPORTED, "xs_run_path_device_noalloc does not record time spectra");
+    if (h->P.NK || h->P.NKV) raise(XS_ERR_UNSUPPORTED, "xs_run_path_device_noalloc does not take k-filtered noises");
     if (nc == 2 && !P.p.checks) raise(XS_ERR_ARG, "coarse pass requested without checks");
     const int slot = nc == 2 ? 1 : 0;
     if (!h->loaded || !h->d_prop[slot].p || (P.has_linear && h->prop_dtr[slot] != pass_dtr(P, nc)))
@@ -2262,6 +2322,7 @@ XS_API xs_status xs_step(xs_handle* h, double* a_inout, const double* w, double 
     if (!h || !a_inout || !(dtr > 0)) raise(XS_ERR_ARG, "bad arguments to xs_step");
     if (h->kind != 1) raise(XS_ERR_UNSUPPORTED, "xs_step covers problems on the resident path only");
     if (h->P.bvals) raise(XS_ERR_UNSUPPORTED, "xs_step does not take boundary values");
+    if (h->P.NK || h->P.NKV) raise(XS_ERR_UNSUPPORTED, "xs_step does not take k-filtered noises");
     load_module(*h);
     const Problem& P = h->P;
     const size_t ntraj = (size_t)P.E1;
@@ -2887,6 +2948,7 @@ XS_API xs_status xs_batch_create(const xs_problem* items, int nitems, xs_batch**
         if (items[i].checks) raise(XS_ERR_UNSUPPORTED, "batch items run the fine pass only (checks = 0)");
         if (items[i].boundary_values) raise(XS_ERR_UNSUPPORTED, "batch items take no boundary values");
         if (h.P.spec) raise(XS_ERR_UNSUPPORTED, "batch items take no time-spectrum observables");
+        if (h.P.NK || h.P.NKV) raise(XS_ERR_UNSUPPORTED, "batch items take no k-filtered noises");
         if (items[i].ensembles[1] != 1 || items[i].ensembles[2] != 1)
           raise(XS_ERR_UNSUPPORTED, "a batch item is one ensemble block (ensembles(2) = ensembles(3) = 1)");
         h.force_G = 1;

@@ -550,7 +550,7 @@ struct Gen {
   int ntmp = 0;
   std::map<std::string, std::string> memo;  // expression text -> temp
   std::vector<Reduction>* reds = nullptr;
-  std::string pname = "p", aname, wname, vname;
+  std::string pname = "p", aname, wname, vname, kname, kvname;
   std::vector<std::string> aux_names;
   bool in_integrand = false;
   bool stencil = false;  // D1/D2 used: the code reads neighbours through xs_fd1/xs_fd2
@@ -637,6 +637,20 @@ struct Gen {
       r.len = ctx.nnoise;
       r.spatial = true;
       for (int i = 0; i < ctx.nnoise; ++i) r.c.push_back("w[" + std::to_string(i) + "]");
+      return r;
+    }
+    if (name == kname && !kname.empty()) {  // k-filtered noise cell (xnoise.m:39-50): complex
+      r.len = ctx.nknoise;
+      r.cplx = true;
+      r.spatial = true;
+      for (int i = 0; i < ctx.nknoise; ++i) r.c.push_back("zk[" + std::to_string(i) + "]");
+      return r;
+    }
+    if (name == kvname && !kvname.empty()) {  // k-filtered randoms (xrandom.m:24-29): complex
+      r.len = ctx.nkrand;
+      r.cplx = true;
+      r.spatial = true;
+      for (int i = 0; i < ctx.nkrand; ++i) r.c.push_back("vk[" + std::to_string(i) + "]");
       return r;
     }
     if (name == vname && !vname.empty()) {
@@ -967,6 +981,7 @@ struct Gen {
     // integrand code in its own generator scope
     Gen sub(ctx);
     sub.aname = aname; sub.wname = wname; sub.vname = vname; sub.pname = pname;
+    sub.kname = kname; sub.kvname = kvname;
     sub.in_integrand = true;
     Val iv = sub.gen(integrand);
     R.lines = iv.len;
@@ -992,7 +1007,8 @@ struct Gen {
     auto base = n->kids[0];
     if (base->kind == NK::Var) {
       const std::string& f = base->name;
-      bool is_arg = f == aname || f == wname || f == vname;
+      bool is_arg = f == aname || f == wname || f == vname || (!kname.empty() && f == kname) ||
+                    (!kvname.empty() && f == kvname);
       if (!is_arg) {
         if (f == "Int") return reduction(n, false);
         if (f == "Ave") return reduction(n, true);
@@ -1122,6 +1138,8 @@ Generated generate(const AnonFn& fn, const GenCtx& ctx) {
       case Role::Field: g.aname = nm; break;
       case Role::Noise: g.wname = nm; break;
       case Role::Random: g.vname = nm; break;
+      case Role::KNoise: g.kname = nm; break;
+      case Role::KRandom: g.kvname = nm; break;
       case Role::Params: g.pname = nm; break;
       default: break;
     }

@@ -42,7 +42,7 @@ struct AnonFn {
 AnonFn parse_anon(const std::string& text);
 
 // Roles of the anonymous function's arguments.
-enum class Role { Field, Noise, Random, Params, Ignored, Aux };
+enum class Role { Field, Noise, Random, Params, Ignored, Aux, KNoise, KRandom };
 
 struct Scalars {
   std::map<std::string, double> values;  // p.<name> constants
@@ -54,6 +54,8 @@ struct GenCtx {
   int nfield = 1;            // components of the field a
   int nnoise = 0;            // components of w
   int nrand = 0;             // components of v
+  int nknoise = 0;           // components of the k-filtered noise (complex, zk[])
+  int nkrand = 0;            // components of the k-filtered randoms (complex, vk[])
   int ndim = 0;              // space dimensions
   bool allow_reduce = false; // Int/Ave allowed (observe)
   bool kgrid = false;        // p.kx/ky/kz available as site values (observe): xs_kt<d>[i<d>]

@@ -87,10 +87,13 @@ def xpreferences(inputs):
             raise _lib.XsError(-9, "space-step checks (checks(2:end)) are not supported")
         p.iterations = int(p.get("iterations", 4))
         p.rawdata = int(p.get("rawdata", 0))  # xpreferences.m:85
-        nz = p.get("noises", None)
-        p.noises = int(np.atleast_1d(nz)[0]) if nz is not None else p.fields
-        rz = p.get("inrandoms", None)
-        p.inrandoms = int(np.atleast_1d(rz)[0]) if rz is not None else p.noises
+        # noise and random cells (xpreferences.m:65-76): Gaussian x-space, then k-filtered
+        nz, kz = p.get("noises", None), p.get("knoises", None)
+        p.knoises = int(np.atleast_1d(kz)[0]) if kz is not None else 0
+        p.noises = int(np.atleast_1d(nz)[0]) if nz is not None else (0 if kz is not None else p.fields)
+        rz, krz = p.get("inrandoms", None), p.get("krandoms", None)
+        p.krandoms = int(np.atleast_1d(krz)[0]) if krz is not None else 0
+        p.inrandoms = int(np.atleast_1d(rz)[0]) if rz is not None else (0 if krz is not None else p.noises)
         p.ranges = [float(x) for x in _vec(p.get("ranges", [10.0] * nd), nd, 10.0)]
         st = [int(x) for x in np.atleast_1d(p.get("steps", [1]))]
         p.steps = st + [1] * (nd - len(st))
@@ -178,11 +181,30 @@ def xpreferences(inputs):
             sh[d] = p.points[d]
             p.r[d] = p.xc[d].reshape(sh)
         p.x, p.y, p.z = p.r[1], p.r[2], p.r[3]
+        # k grids in propagation (FFT) order, shaped like p.x (xgrid.m), for p.nfilter / p.rfilter
+        p.k = [None] * max(4, nd)
+        for d in range(1, nd):
+            p.k[d] = np.fft.ifftshift(p.kc[d]).reshape(p.r[d].shape)
+        p.kx, p.ky, p.kz = p.k[1], p.k[2], p.k[3]
         p.sequence = s
         p.transfer = p.get("transfer", None)
         out.append(p)
         origin = p.origins[0] + p.ranges[0]
     return out
+
+
+def _filter_table(fn, nc, p):
+    """Factors of a k-space filter (p.nfilter / p.rfilter, Simulator/xnoise.m:42,
+    xrandom.m:26) on the FFT-ordered k lattice: fn(ones, p) as [nc][space] complex
+    FP64 (interleaved re, im; site index column-major).  The device applies
+    filters of the form w .* f(p.kx, ...): a random probe checks that fn is one."""
+    shape = [nc] + list(p.space) + [1]
+    f = np.broadcast_to(np.asarray(fn(np.ones(shape, complex), p), dtype=complex), shape)
+    v = np.random.default_rng(7).normal(size=shape).astype(complex)
+    if not np.allclose(np.asarray(fn(v, p), dtype=complex), v * f, rtol=1e-12, atol=1e-300):
+        raise ValueError("p.nfilter / p.rfilter must multiply each k-space value by a function of k")
+    f = np.reshape(f[..., 0], (nc, -1), order="F")
+    return np.ascontiguousarray(f).view(np.float64).reshape(-1)
 
 
 def make_problem(p, path_kind=0, runtime_params=False):
@@ -195,6 +217,8 @@ def make_problem(p, path_kind=0, runtime_params=False):
     pr.fields = p.fields
     pr.noises = p.noises
     pr.inrandoms = p.inrandoms
+    pr.knoises = p.knoises
+    pr.krandoms = p.krandoms
     for d in range(len(p.points)):
         pr.points[d] = p.points[d]
         pr.ranges[d] = p.ranges[d]
@@ -233,6 +257,13 @@ def make_problem(p, path_kind=0, runtime_params=False):
     pr.runtime_params = 1 if runtime_params else 0
     pr.sequence = int(p.get("sequence", 0) or 0)
     pr.boundary_values = 1 if callable(p.get("boundfun", None)) else 0
+    for nc, key in ((p.knoises, "nfilter"), (p.krandoms, "rfilter")):
+        fn = p.get(key, None)
+        if nc > 0 and fn is not None:
+            tab = _filter_table(fn, nc, p)
+            arr = (ctypes.c_double * tab.size)(*tab.tolist())
+            keep.append(arr)
+            setattr(pr, key, arr)
     if any(any(t[1:]) or t[0] for t in p.transforms):
         flags = []
         for t in p.transforms:
