@@ -229,10 +229,11 @@ def test_gpu_xsim_planar_knoise_known_answer():
     g = dict(base, initial="@(u,v,p) [(u(1,:)+1i*u(2,:))/sqrt(2); (v(1,:)+1i*v(2,:))/sqrt(2)]",
              deriv="@(a,w,z,p) [(w(1,:)+1i*w(2,:))/sqrt(2); (z(1,:)+1i*z(2,:))/sqrt(2)]",
              linear="@(p) 0.5i*(p.Dx.^2+p.Dy.^2)",
-             observe=["@(a,p) Int(a(1,:).*conj(a(1,:)),p)", "@(a,p) Int(a(2,:).*conj(a(2,:)),p)",
+             observe=["@(a,p) Int(a(1,:).*conj(a(1,:)),p)", "@(a,p) Int(a(2,:).*conj(a(2,:)),p.dk,p)",
                       "@(a,p) Int(a(2,:).*conj(a(2,:)),p)"])
     o = dict(base, initial=init, deriv=deriv, linear=lambda p: 0.5j * (p.Dx ** 2 + p.Dy ** 2),
-             observe=[lambda a, p: X.Int(a[0:1] * np.conj(a[0:1]), p), lambda a, p: X.Int(a[1:2] * np.conj(a[1:2]), p),
+             observe=[lambda a, p: X.Int(a[0:1] * np.conj(a[0:1]), p),
+                      lambda a, p: X.Int(a[1:2] * np.conj(a[1:2]), p.dk, p),
                       lambda a, p: X.Int(a[1:2] * np.conj(a[1:2]), p)])
     eg, dg, ig = xsim(g)
     with warnings.catch_warnings():
