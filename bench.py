@@ -292,8 +292,9 @@ def run_ours(args, rank, world, local_rank):
     if dist is not None:
         dist.barrier()
     ms = ev0.elapsed_time(ev1) / args.steps
-    kms = (ctypes.c_double * 8)()
-    kl = (ctypes.c_longlong * 8)()
+    nk = len(_lib.KERNEL_KINDS)
+    kms = (ctypes.c_double * nk)()
+    kl = (ctypes.c_longlong * nk)()
     _lib.check(L.xs_kernel_stats(path.h, 1, kms, kl))
     L.xs_set_kernel_timing(path.h, 0)
     clocks = clk.summary()
@@ -307,7 +308,7 @@ def run_ours(args, rank, world, local_rank):
         if rank == 0:
             print(json.dumps({"quick": True, "value": value, "ms_per_step": ms_max,
                               "kernels": {_lib.KERNEL_KINDS[i]: {"launches": int(kl[i]), "ms": float(kms[i])}
-                                          for i in range(8) if kl[i]}}))
+                                          for i in range(nk) if kl[i]}}))
         return
     # end to end through the host C ABI (pinned host buffers, copies inside the timed region)
     a_in = torch.empty((ntraj * p.nspace * 2,), dtype=torch.float64, pin_memory=True)
@@ -336,17 +337,23 @@ def run_ours(args, rank, world, local_rank):
     if rank != 0:
         return
     kinds = _lib.KERNEL_KINDS
-    stats = {kinds[i]: {"launches": int(kl[i]), "ms": float(kms[i])} for i in range(8) if kl[i]}
-    dom = max(("x_step", "y_pass"), key=lambda k: stats.get(k, {"ms": 0})["ms"])
+    stats = {kinds[i]: {"launches": int(kl[i]), "ms": float(kms[i])} for i in range(nk) if kl[i]}
+    dom = max(("x_step", "y_pass", "rc_pass"), key=lambda k: stats.get(k, {"ms": 0})["ms"])
     per_launch_ms = stats[dom]["ms"] / stats[dom]["launches"]
-    # the blocks may run as two staggered groups (two launches per pass, each on half the trajectories)
-    groups = max(1, round(stats["x_step"]["launches"] / float(args.steps * steps_per_traj)))
-    traj_per_launch = ntraj / groups
-    alg_bytes = 2.0 * traj_per_launch * p.fields * p.nspace * 8  # read + write of the FP32 complex field
+    if dom == "rc_pass":
+        # one fused launch: the row pass of one half of the trajectories and the column pass of the
+        # other half, each one read and one write of its half's field
+        traj_per_launch = ntraj / 2.0
+        alg_bytes = 2.0 * 2.0 * traj_per_launch * p.fields * p.nspace * 8
+    else:
+        # one pass over every trajectory (both halves when the schedule is not fused)
+        launches_per_pass = max(1, round(stats[dom]["launches"] / float(args.steps * steps_per_traj)))
+        traj_per_launch = ntraj / launches_per_pass
+        alg_bytes = 2.0 * traj_per_launch * p.fields * p.nspace * 8  # read + write of the FP32 complex field
     achieved = alg_bytes / (per_launch_ms / 1000.0) / 1e9
     peak, kind = _peaks()
     tr = NCU_TRAFFIC_PER_TRAJ.get(dom)
-    gpu_launches = sum(int(kl[i]) for i in range(8))
+    gpu_launches = sum(int(kl[i]) for i in range(nk))
     fp64_line, fp32_err = _precision_report(ntraj)
     cpu_val, cpu_desc = _cpu_sample()
     line = {

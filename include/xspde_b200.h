@@ -252,6 +252,8 @@ enum {
   XS_KERNEL_Y_PASS,       /* streaming: column pass (FFT_y, exp(L dt), IFFT_y) */
   XS_KERNEL_X_OBS,        /* streaming: observables */
   XS_KERNEL_SCALAR,       /* streaming: Int/Ave scalar observables */
+  XS_KERNEL_RC_PASS,      /* streaming: row pass of one half of the trajectories fused with the
+                             column pass of the other half */
   XS_KERNEL_KINDS
 };
 

@@ -116,3 +116,32 @@ def test_stream_tma_column_pass_bit_identical(precision, monkeypatch):
     for b in range(2):
         for k in range(len(av_plain[b])):
             assert np.array_equal(av_plain[b][k], av_tma[b][k]), (b, k)
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp64"])
+def test_stream_fused_halves_bit_identical(precision, monkeypatch):
+    """With an even number of blocks the two halves of the trajectories run one
+    pass apart and each row pass shares an xs_rc_pass launch with the other
+    half's column pass; per trajectory the arithmetic is unchanged, so fields,
+    site observables and Int reductions equal the one-pass-at-a-time schedule
+    (the default) bit for bit, for both check passes (XSPDE_B200_FUSE=1 selects it)."""
+    import ctypes
+    from xspde_matlab_b200 import GpuPath, _lib, xpreferences
+    g, _ = _case(1, precision=precision, ens=(8, 4, 1))
+    p = xpreferences([g])[0]
+    L = _lib.lib()
+    n = len(_lib.KERNEL_KINDS)
+    for nc in (1, 2):
+        monkeypatch.delenv("XSPDE_B200_FUSE", raising=False)
+        av_a, a_a = GpuPath(p, path_kind=2).run_path(0, 4, nc, a_out=True)
+        monkeypatch.setenv("XSPDE_B200_FUSE", "1")
+        path = GpuPath(p, path_kind=2)
+        _lib.check(L.xs_set_kernel_timing(path.h, 1))
+        av_b, a_b = path.run_path(0, 4, nc, a_out=True)
+        kms, kl = (ctypes.c_double * n)(), (ctypes.c_longlong * n)()
+        _lib.check(L.xs_kernel_stats(path.h, 1, kms, kl))
+        assert kl[_lib.KERNEL_KINDS.index("rc_pass")] > 0
+        assert np.array_equal(a_a, a_b), nc
+        for b in range(4):
+            for k in range(len(av_a[b])):
+                assert np.array_equal(av_a[b][k], av_b[b][k]), (nc, b, k)

@@ -20,7 +20,7 @@ EXPORTS = ["xs_create", "xs_destroy", "xs_last_error", "xs_version", "xs_observe
            "xs_mlp_sizes", "xs_mlp_forward", "xs_mlp_train_grad", "xs_mlp_adam", "xs_batch_create",
            "xs_batch_destroy", "xs_batch_tune", "xs_batch_run", "xs_batch_sync", "xs_batch_av_doubles",
            "xs_batch_results", "xs_batch_info", "xs_set_boundary_values", "xs_run_path_raw"]
-KERNEL_KINDS = ["resident", "obs_reduce", "x_init", "x_step", "x_final", "y_pass", "x_obs", "scalar"]
+KERNEL_KINDS = ["resident", "obs_reduce", "x_init", "x_step", "x_final", "y_pass", "x_obs", "scalar", "rc_pass"]
 
 
 class XsProblem(ctypes.Structure):

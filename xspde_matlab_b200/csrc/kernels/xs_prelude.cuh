@@ -200,9 +200,10 @@ __device__ __forceinline__ uint4 xs_philox(uint4 c, u32 k0, u32 k1) {
       k0 += 0x9E3779B9u;
       k1 += 0xBB67AE85u;
     }
-    const u32 hi0 = __umulhi(0xD2511F53u, c.x), lo0 = 0xD2511F53u * c.x;
-    const u32 hi1 = __umulhi(0xCD9E8D57u, c.z), lo1 = 0xCD9E8D57u * c.z;
-    c = make_uint4(hi1 ^ c.y ^ k0, lo1, hi0 ^ c.w ^ k1, lo0);
+    // one widening 32 x 32 -> 64-bit multiply gives both halves of each product
+    const unsigned long long p0 = (unsigned long long)c.x * 0xD2511F53u;
+    const unsigned long long p1 = (unsigned long long)c.z * 0xCD9E8D57u;
+    c = make_uint4((u32)(p1 >> 32) ^ c.y ^ k0, (u32)p1, (u32)(p0 >> 32) ^ c.w ^ k1, (u32)p0);
   }
   return c;
 }
@@ -222,7 +223,8 @@ __device__ __forceinline__ void xs_boxmuller(u32 x0, u32 x1, real& z0, real& z1)
   // taken in (-pi, pi): cos(2 pi u) = -cos(2 pi (u - 1/2)), likewise sin.
   const float u0 = ((float)x0 + 0.5f) * 2.3283064365386963e-10f;
   const float hu = (float)((int)(x1 ^ 0x80000000u)) * 2.3283064365386963e-10f + 1.16415321826934814e-10f;
-  const float r = sqrtf(-2.0f * __logf(u0));
+  const float q = -2.0f * __logf(u0);  // > 0: u0 < 1
+  const float r = q * rsqrtf(q);
   float s, c;
   __sincosf(6.28318530717958648f * hu, &s, &c);
   z0 = -r * c;

@@ -76,8 +76,12 @@ __device__ __forceinline__ bool xs_smem_ok(size_t need, int* status) {
 // (t fastest, so the threads of a line read consecutive words), copied from
 // the host-built table (L2-resident) into the CTA's shared memory.
 template <int R>
-__device__ __forceinline__ void xs_fill_twiddles(cx* tw, const cx* __restrict__ src) {
-  for (int i = threadIdx.x; i < R * R; i += blockDim.x) tw[i] = src[i];
+__device__ __forceinline__ void xs_fill_twiddles(cx* tw, const cx* __restrict__ src, int tid = -1, int nthr = 0) {
+  if (tid < 0) {
+    tid = threadIdx.x;
+    nthr = blockDim.x;
+  }
+  for (int i = tid; i < R * R; i += nthr) tw[i] = src[i];
 }
 
 // Forward DFT of N = R*R points held four-step style: thread t holds v[j] =
@@ -117,6 +121,7 @@ struct XsBlockSync {
   __device__ __forceinline__ void operator()() const { __syncthreads(); }
 };
 
+
 // ---- row passes -------------------------------------------------------------
 // Shared memory: twiddles (RX*RX) + per-row transpose scratch (RX*(RX+1)).
 #define XS_XLINE (XS_F * XS_RX * XS_RX > XS_RX * (XS_RX + 1) ? XS_F * XS_RX * XS_RX : XS_RX * (XS_RX + 1))
@@ -130,21 +135,16 @@ __device__ __forceinline__ void xs_row_coords(int y, int t, int j, real& x, real
 // MODE 0: initial field (expression or a_in) -> K state
 // MODE 1: one MP step in x space (K state in, K state out)
 // MODE 3: K state -> x-space a_out (FP64)
-template <int MODE>
-__device__ __forceinline__ void xs_xpass_body(const XsStreamArgs& A) {
-  // The grid covers ntraj*NY rows exactly; a CTA outside it leaves as a whole.
-  if ((size_t)(blockIdx.x + 1) * XS_XROWS > (size_t)A.ntraj * XS_NY) {
-    if (threadIdx.x == 0) atomicOr(A.status, 2);
-    return;
-  }
-  if (!xs_smem_ok(XS_XSMEM * sizeof(cx), A.status)) return;
-  cx* smem = (cx*)xs_dsmem;
+// Row block `cta` (XS_XROWS rows) by 256 threads tid = 0..255 with the shared
+// memory `smem` (XS_XSMEM elements) and the barrier `bsync` of those threads.
+template <int MODE, class Sync>
+__device__ __forceinline__ void xs_xpass_core(const XsStreamArgs& A, int tid, size_t cta, cx* smem, Sync bsync) {
   cx* tw = smem;
-  xs_fill_twiddles<XS_RX>(tw, A.tw_x);
-  __syncthreads();
-  const int r = threadIdx.x / XS_RX, t = threadIdx.x % XS_RX;
+  xs_fill_twiddles<XS_RX>(tw, A.tw_x, tid, 256);
+  bsync();
+  const int r = tid / XS_RX, t = tid % XS_RX;
   cx* buf = tw + XS_RX * XS_RX + r * XS_XLINE;
-  const size_t row = (size_t)blockIdx.x * XS_XROWS + r;  // over ntraj * NY
+  const size_t row = cta * XS_XROWS + r;  // over ntraj * NY
   const int e = (int)(row / XS_NY), y = (int)(row % XS_NY);
   const u32 blk = (u32)(A.block0 + e / A.ens1), el = (u32)(e % A.ens1);
   cx v[XS_F][XS_RX];
@@ -287,6 +287,17 @@ __device__ __forceinline__ void xs_xpass_body(const XsStreamArgs& A) {
     for (int j = 0; j < XS_RX; ++j) base[(size_t)f * XS_NS + XS_RX * j] = v[f][j];
 }
 
+template <int MODE>
+__device__ __forceinline__ void xs_xpass_body(const XsStreamArgs& A) {
+  // The grid covers ntraj*NY rows exactly; a CTA outside it leaves as a whole.
+  if ((size_t)(blockIdx.x + 1) * XS_XROWS > (size_t)A.ntraj * XS_NY) {
+    if (threadIdx.x == 0) atomicOr(A.status, 2);
+    return;
+  }
+  if (!xs_smem_ok(XS_XSMEM * sizeof(cx), A.status)) return;
+  xs_xpass_core<MODE>(A, threadIdx.x, blockIdx.x, (cx*)xs_dsmem, XsBlockSync());
+}
+
 extern "C" __global__ void __launch_bounds__(256) xs_x_init(const XsStreamArgs A) { xs_xpass_body<0>(A); }
 extern "C" __global__ void __launch_bounds__(256) xs_x_nl(const XsStreamArgs A) { xs_xpass_body<1>(A); }
 extern "C" __global__ void __launch_bounds__(256) xs_x_final(const XsStreamArgs A) { xs_xpass_body<3>(A); }
@@ -297,9 +308,9 @@ extern "C" __global__ void __launch_bounds__(256) xs_x_final(const XsStreamArgs 
 #define XS_SSMEM (XS_RY * XS_RY + XS_TX * XS_RY * XS_RY)
 
 // FFT_y, x exp(L dt)^m, IFFT_y of one tile column held four-step style in v.
+template <class Sync = XsBlockSync>
 __device__ __forceinline__ void xs_col_tile(cx (&v)[XS_RY], int t, int c, int x0, int f, const cx* tw, cx* buf,
-                                            const XsStreamArgs& A) {
-  XsBlockSync bs;
+                                            const XsStreamArgs& A, Sync bs = Sync()) {
   xs_fft4<XS_RY, XS_TX, 0>(v, t, tw, buf, bs);
 #if XS_SEP
   // separable L(kx, ky) = Lx(kx) + Ly(ky): exp(L dt) = ex[kx] * ey[ky] from two
@@ -324,29 +335,64 @@ __device__ __forceinline__ void xs_col_tile(cx (&v)[XS_RY], int t, int c, int x0
   xs_ifft4<XS_RY, XS_TX, 0>(v, t, tw, buf, bs);
 }
 
-extern "C" __global__ void __launch_bounds__(256, 4) xs_s_pass(const XsStreamArgs A) {
-  if ((size_t)blockIdx.x >= (size_t)A.ntraj * XS_F * (XS_NX / XS_TX)) {
-    if (threadIdx.x == 0) atomicOr(A.status, 2);
-    return;
-  }
-  if (!xs_smem_ok(XS_SSMEM * sizeof(cx), A.status)) return;
-  cx* smem = (cx*)xs_dsmem;
+// Column tile `tile` (over ntraj * F * NX/TX) by 256 threads tid = 0..255 with
+// the shared memory `smem` (XS_SSMEM elements) and their barrier `bs`.
+template <class Sync>
+__device__ __forceinline__ void xs_col_core(const XsStreamArgs& A, int tid, size_t tile, cx* smem, Sync bs) {
   cx* tw = smem;
-  xs_fill_twiddles<XS_RY>(tw, A.tw_y);
-  const int c = threadIdx.x % XS_TX, t = threadIdx.x / XS_TX;
+  xs_fill_twiddles<XS_RY>(tw, A.tw_y, tid, 256);
+  const int c = tid % XS_TX, t = tid / XS_TX;
   cx* buf = tw + XS_RY * XS_RY + c;  // element (k, t) of column c at ((k*RY + t)*TX + c)
   constexpr int TILES = XS_NX / XS_TX;
-  const size_t tile = blockIdx.x;  // over ntraj * F * TILES
   const int x0 = (int)(tile % TILES) * XS_TX;
   const size_t ef = tile / TILES;  // e * F + f
   cx* base = A.field + ef * XS_NS + x0 + c;
   cx v[XS_RY];
 #pragma unroll
   for (int j = 0; j < XS_RY; ++j) v[j] = base[(size_t)(t + XS_RY * j) * XS_NX];
-  __syncthreads();  // twiddles ready
-  xs_col_tile(v, t, c, x0, (int)(ef % XS_F), tw, buf, A);
+  bs();  // twiddles ready
+  xs_col_tile(v, t, c, x0, (int)(ef % XS_F), tw, buf, A, bs);
 #pragma unroll
   for (int j = 0; j < XS_RY; ++j) base[(size_t)(t + XS_RY * j) * XS_NX] = v[j];
+}
+
+extern "C" __global__ void __launch_bounds__(256, 4) xs_s_pass(const XsStreamArgs A) {
+  if ((size_t)blockIdx.x >= (size_t)A.ntraj * XS_F * (XS_NX / XS_TX)) {
+    if (threadIdx.x == 0) atomicOr(A.status, 2);
+    return;
+  }
+  if (!xs_smem_ok(XS_SSMEM * sizeof(cx), A.status)) return;
+  xs_col_core(A, threadIdx.x, blockIdx.x, (cx*)xs_dsmem, XsBlockSync());
+}
+
+// ---- fused row + column pass ------------------------------------------------------
+// Two independent halves of the trajectories one pass apart: one grid holds the
+// row blocks of R (xs_x_nl) and the column tiles of C (xs_s_pass), interleaved
+// by block index (row, column, row, ...), each CTA one role with the usual
+// 256 threads.  As short column CTAs finish, the block scheduler refills their
+// slots, so every SM keeps a mix of issue-bound row CTAs and HBM-bound column
+// CTAs.
+extern "C" __global__ void __launch_bounds__(256, 4) xs_rc_pass(const XsStreamArgs R, const XsStreamArgs C) {
+  const size_t nr = (size_t)R.ntraj * XS_NY / XS_XROWS, ncol = (size_t)C.ntraj * XS_F * (XS_NX / XS_TX);
+  const size_t m = nr < ncol ? nr : ncol;
+  const size_t i = blockIdx.x;
+  const bool row = i < 2 * m ? (i & 1) == 0 : nr > ncol;
+  const size_t idx = i < 2 * m ? i >> 1 : m + (i - 2 * m);
+  if (row) {
+    if (idx >= nr) {
+      if (threadIdx.x == 0) atomicOr(R.status, 2);
+      return;
+    }
+    if (!xs_smem_ok(XS_XSMEM * sizeof(cx), R.status)) return;
+    xs_xpass_core<1>(R, threadIdx.x, idx, (cx*)xs_dsmem, XsBlockSync());
+  } else {
+    if (idx >= ncol) {
+      if (threadIdx.x == 0) atomicOr(C.status, 2);
+      return;
+    }
+    if (!xs_smem_ok(XS_SSMEM * sizeof(cx), C.status)) return;
+    xs_col_core(C, threadIdx.x, idx, (cx*)xs_dsmem, XsBlockSync());
+  }
 }
 
 // ---- column pass fed by the Tensor Memory Accelerator ---------------------------

@@ -872,6 +872,8 @@ struct xs_handle {
   int path_kind = 0;
   int force_G = 0, force_threads = 0;  // resident tile fixed by the caller (uneven batch)
   CUfunction f_spass_tma = nullptr;    // column pass fed by TMA (NY <= 256)
+  CUfunction f_rc = nullptr;           // fused row pass (one half) + column pass (other half)
+  bool fuse = false;                   // run the two halves of the trajectories one pass apart, fused
   bool tma = false;
   CUtensorMap tmap{};                  // field as [rows][2*NX] reals, box [NY][2*TX]
   const void* tmap_ptr = nullptr;
@@ -1317,6 +1319,16 @@ void load_module(xs_handle& h) {
       }
     }
     cu_check(d.getfn(&h.f_feat, h.mod, "xs_noise_features"), "xs_noise_features");
+    {
+      // opt-in (measured: 1.39 ms per fused launch against 1.41 ms per row + column pass pair at
+      // 4096 trajectories of the 256x256 GPE, within run-to-run spread)
+      const char* e = getenv("XSPDE_B200_FUSE");
+      h.fuse = e && *e == '1';
+      cu_check(d.getfn(&h.f_rc, h.mod, "xs_rc_pass"), "xs_rc_pass");
+      const size_t rsm = std::max(h.sp.xsmem, h.sp.ssmem);
+      if (rsm > 48 * 1024)
+        cu_check(d.setattr(h.f_rc, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, (int)rsm), "xs_rc_pass smem");
+    }
     for (auto& f : fns) {
       cu_check(d.getfn(f.f, h.mod, f.name), f.name);
       if (f.smem > 48 * 1024)
@@ -1672,6 +1684,127 @@ struct StreamArgsHost {
   const void* tw_y;
 };
 
+// The pass sequence of one streaming p.path call (Simulator/xpath.m:137-194 with merged MP
+// half steps): initial field, then per step a column pass (exp(L dt)^m, m = 2 when the previous
+// step's second half is merged in) and a row pass (drift and noise), and at output times the
+// pending half step and the observables.
+struct StreamOp {
+  enum Kind { INIT, COL, ROW, OBS, FINAL } kind;
+  int m, draw0, draw1, n;
+  double t;
+};
+
+std::vector<StreamOp> stream_ops(const Problem& P, int nc, bool final_field) {
+  std::vector<StreamOp> ops;
+  double t = P.p.origins[0];
+  const double dtr = pass_dtr(P, nc);
+  ops.push_back({StreamOp::INIT, 0, 0, -1, 0, t});
+  int pending = 0, draw = 0, prev_draw = -1;
+  const int npts = P.p.points[0], S = P.p.steps, checks = P.p.checks;
+  for (int n = 0; n < npts; ++n)
+    for (int step = 0; step < S; ++step) {
+      if (n > 0 || step > 0 || npts == 1)
+        for (int chk = 0; chk <= checks; ++chk) {
+          ++draw;
+          if (nc == 2 && checks && chk == 0) {
+            prev_draw = draw;
+            continue;
+          }
+          ops.push_back({StreamOp::COL, pending + 1, 0, -1, 0, t});
+          ops.push_back({StreamOp::ROW, 0, draw, (nc == 2 && checks) ? prev_draw : -1, 0, t});
+          t += dtr;
+          pending = 1;
+        }
+      if (step == 0) {
+        if (pending) ops.push_back({StreamOp::COL, pending, 0, -1, 0, t});
+        pending = 0;
+        ops.push_back({StreamOp::OBS, 0, 0, -1, n, t});
+      }
+    }
+  if (final_field) {
+    if (pending) ops.push_back({StreamOp::COL, pending, 0, -1, 0, t});
+    ops.push_back({StreamOp::FINAL, 0, 0, -1, 0, t});
+  }
+  return ops;
+}
+
+// The two halves of the blocks (independent trajectories) run the same pass sequence one pass
+// apart, so that wherever one half's row pass meets the other half's column pass the two go into
+// one xs_rc_pass launch: the issue-bound row pass and the HBM-bound column pass share the SMs.
+void launch_stream_halves(xs_handle& h, const StreamArgsHost& a, int nblocks, int nc, void* av_dev, cudaStream_t st) {
+  const Problem& P = h.P;
+  const StreamPlan& sp = h.sp;
+  const size_t cxs = h.fp64 ? 16 : 8;
+  const int nb = nblocks / 2, th = nb * P.E1;
+  const int nrg = P.N[1] / sp.OROWS;
+  const size_t stride = av_stride(P);
+  StreamArgsHost half[2] = {a, a};
+  for (int hf = 0; hf < 2; ++hf) {
+    StreamArgsHost& b = half[hf];
+    const size_t e0 = (size_t)hf * th;
+    b.ntraj = th;
+    b.block0 = a.block0 + hf * nb;
+    b.field = (char*)a.field + e0 * P.F * P.NS * cxs;
+    if (a.a_in) b.a_in = (const char*)a.a_in + e0 * P.F * P.NS * 16;
+    if (a.a_out) b.a_out = (char*)a.a_out + e0 * P.F * P.NS * 16;
+    b.av = (char*)av_dev + (size_t)hf * nb * P.p.points[0] * stride * 16;
+    if (a.redpart) b.redpart = (char*)a.redpart + e0 * nrg * std::max(P.nred, 1) * 16;
+  }
+  const unsigned xgrid = (unsigned)((size_t)th * P.N[1] / sp.XROWS);
+  const unsigned sgrid = (unsigned)((size_t)th * P.F * (P.N[0] / sp.TX));
+  auto set = [](StreamArgsHost& b, const StreamOp& o) {
+    b.m = o.m;
+    b.draw0 = o.draw0;
+    b.draw1 = o.draw1;
+    b.n = o.n;
+    b.t = o.t;
+  };
+  auto run = [&](const StreamOp& o, StreamArgsHost& b) {
+    set(b, o);
+    void* prm[] = {&b};
+    switch (o.kind) {
+      case StreamOp::INIT:
+        xs_launch(h, XS_KERNEL_X_INIT, h.f_xinit, xgrid, 1, 1, 256, (unsigned)sp.xsmem, st, prm, "row pass");
+        break;
+      case StreamOp::ROW:
+        xs_launch(h, XS_KERNEL_X_STEP, h.f_xnl, xgrid, 1, 1, 256, (unsigned)sp.xsmem, st, prm, "row pass");
+        break;
+      case StreamOp::FINAL:
+        xs_launch(h, XS_KERNEL_X_FINAL, h.f_xfinal, xgrid, 1, 1, 256, (unsigned)sp.xsmem, st, prm, "row pass");
+        break;
+      case StreamOp::COL:
+        xs_launch(h, XS_KERNEL_Y_PASS, h.f_spass, sgrid, 1, 1, 256, (unsigned)sp.ssmem, st, prm, "column pass");
+        break;
+      case StreamOp::OBS:
+        xs_launch(h, XS_KERNEL_X_OBS, h.f_xobs, (unsigned)nrg, (unsigned)nb, 1, (unsigned)(sp.OROWS * sp.RX),
+                  (unsigned)sp.osmem, st, prm, "observation pass");
+        if (P.nout_scalar)
+          xs_launch(h, XS_KERNEL_SCALAR, h.f_scalar, (unsigned)nb, 1, 1, 256, 0, st, prm, "scalar observables");
+        break;
+    }
+  };
+  const std::vector<StreamOp> ops = stream_ops(P, nc, a.a_out != nullptr);
+  const size_t L = ops.size();
+  for (size_t i = 0; i <= L; ++i) {
+    const StreamOp* o0 = i < L ? &ops[i] : nullptr;      // first half: op i
+    const StreamOp* o1 = i >= 1 ? &ops[i - 1] : nullptr;  // second half: op i - 1
+    if (o0 && o1 && ((o0->kind == StreamOp::ROW && o1->kind == StreamOp::COL) ||
+                     (o0->kind == StreamOp::COL && o1->kind == StreamOp::ROW))) {
+      const int hr = o0->kind == StreamOp::ROW ? 0 : 1;
+      StreamArgsHost& R = half[hr];
+      StreamArgsHost& C = half[1 - hr];
+      set(R, hr == 0 ? *o0 : *o1);
+      set(C, hr == 0 ? *o1 : *o0);
+      void* prm[] = {&R, &C};
+      xs_launch(h, XS_KERNEL_RC_PASS, h.f_rc, xgrid + sgrid, 1, 1, 256, (unsigned)std::max(sp.xsmem, sp.ssmem), st,
+                prm, "fused row/column pass");
+      continue;
+    }
+    if (o0) run(*o0, half[0]);
+    if (o1) run(*o1, half[1]);
+  }
+}
+
 // Streaming schedule of one xpath call (Simulator/xpath.m:137-194) for MP:
 // column passes apply the pending half-step propagators, row passes do the
 // midpoint step; observations need all half steps applied first.
@@ -1746,6 +1879,10 @@ void launch_stream(xs_handle& h, int first_block, int nblocks, int nc, const voi
     if (P.nout_scalar)
       xs_launch(h, XS_KERNEL_SCALAR, h.f_scalar, (unsigned)nblocks, 1, 1, 256, 0, st, params, "scalar observables");
   };
+  if (h.fuse && h.f_rc && !h.tma && nblocks >= 2 && nblocks % 2 == 0) {
+    launch_stream_halves(h, a, nblocks, nc, av_dev, st);
+    return;
+  }
   row(XS_KERNEL_X_INIT, h.f_xinit);
   int pending = 0, draw = 0, prev_draw = -1;
   const int npts = P.p.points[0], S = P.p.steps, checks = P.p.checks;

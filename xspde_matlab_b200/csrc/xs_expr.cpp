@@ -809,13 +809,25 @@ struct Gen {
     }
     if (cmp) cplx = false;
     r.cplx = cplx;
+    // division by a real literal constant: multiply by its reciprocal (within one rounding of the
+    // quotient; the divide is several instructions, the multiply one)
+    std::string recip;
+    if ((op == "/" || op == "./") && !b.cplx) {
+      Vec cv;
+      if (try_const(rnode, cv) && cv.size() == 1 && cv[0].imag() == 0 && cv[0].real() != 0 &&
+          std::isfinite(cv[0].real()) && std::isfinite(1.0 / cv[0].real())) {
+        char buf[64];
+        snprintf(buf, sizeof buf, "(real)(%.17g)", 1.0 / cv[0].real());
+        recip = buf;
+      }
+    }
     for (int i = 0; i < r.len; ++i) {
       const std::string& x = a.c[a.len == 1 ? 0 : i];
       const std::string& y = b.c[b.len == 1 ? 0 : i];
       std::string e;
       if (op == "+" || op == "-") e = x + " " + op + " " + y;
       else if (op == "*" || op == ".*") e = x + " * " + y;
-      else if (op == "/" || op == "./") e = x + " / " + y;
+      else if (op == "/" || op == "./") e = recip.empty() ? x + " / " + y : x + " * " + recip;
       else if (op == "\\" || op == ".\\") e = y + " / " + x;
       else if (op == "^" || op == ".^") {
         if (ipow) e = "xs_powi<" + std::to_string(ie) + ">(" + x + ")";
