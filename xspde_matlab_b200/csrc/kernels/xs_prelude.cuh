@@ -223,8 +223,9 @@ __device__ __forceinline__ void xs_boxmuller(u32 x0, u32 x1, real& z0, real& z1)
   // taken in (-pi, pi): cos(2 pi u) = -cos(2 pi (u - 1/2)), likewise sin.
   const float u0 = ((float)x0 + 0.5f) * 2.3283064365386963e-10f;
   const float hu = (float)((int)(x1 ^ 0x80000000u)) * 2.3283064365386963e-10f + 1.16415321826934814e-10f;
-  const float q = -2.0f * __logf(u0);  // > 0: u0 < 1
-  const float r = q * rsqrtf(q);
+  // u0 rounds to 1 in FP32 for the largest words (q = 0): r = 0 there, as sqrtf gives
+  const float q = -2.0f * __logf(u0);
+  const float r = q > 0.0f ? q * rsqrtf(q) : 0.0f;
   float s, c;
   __sincosf(6.28318530717958648f * hu, &s, &c);
   z0 = -r * c;

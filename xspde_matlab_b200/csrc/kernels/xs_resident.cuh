@@ -61,6 +61,9 @@ struct XsPathArgs {
 // only the reduction scratch in shared memory.  The code is the same; only the
 // arrays' home differs (__syncthreads orders global accesses within a CTA).
 #define XS_FARR (XS_GFIELD ? 0 : XS_NARR)
+// XS_GFIELD: shared-memory copy of a real transform matrix (XS_MSM reals, 16-byte padded) ahead
+// of the two tiles
+#define XS_MS_CX ((((size_t)XS_MSM * sizeof(real) + 15) / 16) * 16 / sizeof(cx))
 #define XS_NOMERGE (XS_BVAL || XS_SPEC)
 // complex elements of one CTA's slice: the field arrays, then (methods other
 // than MP) the two noise arrays of reals
@@ -289,7 +292,10 @@ __device__ void xs_tr_tiled(cx* X, const XsPathArgs& P, int dir) {
     constexpr int NHI = XS_G * XS_F * XS_NS / (SD * ND);  // line groups (g, f, slower dims)
     constexpr int NPER = XS_NS / (SD * ND);               // line groups per (g, f)
     constexpr int NT = SD == 1 ? NHI / TL : NHI * (SD / (SD == 1 ? 1 : TL));
-    cx* S = (cx*)xs_smem;
+    constexpr bool RM = D == 1 ? XS_REALM1 : (D == 2 ? XS_REALM2 : XS_REALM3);
+    real* Ms = (real*)xs_smem;  // real matrix of the current component (RM)
+    int ms_f = -1;
+    cx* S = (cx*)xs_smem + XS_MS_CX;
     cx* S2 = S + XS_TILE_ELEMS;
     for (int tile = 0; tile < NT; ++tile) {
       int hi0, lo0;
@@ -310,9 +316,17 @@ __device__ void xs_tr_tiled(cx* X, const XsPathArgs& P, int dir) {
         const int f = (hi0 / NPER) % XS_F;
         const cx* __restrict__ M = P.tmat + P.tmat_off[D] + (size_t)(f * 2 + dir) * ND * ND;
         // register block: KB outputs k x LB lines per thread; real matrices
-        // (every DST/DCT type) skip the imaginary part of M
+        // (every DST/DCT type) skip the imaginary part of M and are read from
+        // a shared-memory copy, KB entries per vector load
         constexpr int KB = ND % 4 == 0 ? 4 : 1, LB = TL % 2 == 0 ? 2 : 1;
-        constexpr bool RM = D == 1 ? XS_REALM1 : (D == 2 ? XS_REALM2 : XS_REALM3);
+        constexpr bool MSH = RM && (size_t)ND * ND <= (size_t)XS_MSM;
+        if constexpr (MSH) {
+          if (f != ms_f) {  // tiles of one component share its matrix (uniform branch)
+            for (int i = threadIdx.x; i < ND * ND; i += blockDim.x) Ms[i] = M[i].re;
+            ms_f = f;
+            __syncthreads();
+          }
+        }
         for (int i = threadIdx.x; i < (ND / KB) * (TL / LB); i += blockDim.x) {
           const int l0 = (i % (TL / LB)) * LB, k0 = (i / (TL / LB)) * KB;
           real ar[KB][LB], ai[KB][LB];
@@ -325,8 +339,19 @@ __device__ void xs_tr_tiled(cx* X, const XsPathArgs& P, int dir) {
             cx v[LB], m[KB];
 #pragma unroll
             for (int j = 0; j < LB; ++j) v[j] = S[n * LSP + l0 + j];
+            if constexpr (MSH && KB == 4 && sizeof(real) == 4) {
+              const float4 q4 = *reinterpret_cast<const float4*>(Ms + n * ND + k0);
+              m[0] = mkcx((real)q4.x, (real)0);
+              m[1] = mkcx((real)q4.y, (real)0);
+              m[2] = mkcx((real)q4.z, (real)0);
+              m[3] = mkcx((real)q4.w, (real)0);
+            } else if constexpr (MSH) {
 #pragma unroll
-            for (int q = 0; q < KB; ++q) m[q] = M[n * ND + k0 + q];
+              for (int q = 0; q < KB; ++q) m[q] = mkcx(Ms[n * ND + k0 + q], (real)0);
+            } else {
+#pragma unroll
+              for (int q = 0; q < KB; ++q) m[q] = M[n * ND + k0 + q];
+            }
 #pragma unroll
             for (int q = 0; q < KB; ++q)
 #pragma unroll
@@ -852,7 +877,7 @@ __device__ void xs_spectrum(const XsPathArgs& P, int cta) {
 // not match the layout; the CTA must then return without touching it.
 __device__ __forceinline__ bool xs_layout_ok(int* status) {
   constexpr size_t GF = (size_t)XS_G * XS_F * XS_NS;
-  constexpr size_t need = ((XS_GFIELD ? 0 : XS_NARR + XS_KARR + XS_KNARR) * GF + 2 * (size_t)XS_TILE_ELEMS) * sizeof(cx) + (size_t)XS_G * (XS_NRED > 0 ? XS_NRED : 1) * sizeof(cx) +
+  constexpr size_t need = ((XS_GFIELD ? 0 : XS_NARR + XS_KARR + XS_KNARR) * GF + 2 * (size_t)XS_TILE_ELEMS + (XS_GFIELD ? XS_MS_CX : 0)) * sizeof(cx) + (size_t)XS_G * (XS_NRED > 0 ? XS_NRED : 1) * sizeof(cx) +
                           32 * 2 * (XS_NRED > 0 ? XS_NRED : 1) * sizeof(double) +
                           (XS_GFIELD ? 0 : XS_WARR) * (size_t)XS_G * XS_NWS * XS_NS * sizeof(real);
   u32 dyn;
@@ -870,7 +895,7 @@ __device__ void xs_resident_run(const XsPathArgs& P, int cta, int nctas) {
   constexpr int GF = XS_G * XS_F * XS_NS;
 #if XS_GFIELD
   cx* A = P.gfield + (size_t)blockIdx.x * XS_GSLICE;
-  cx* RED = (cx*)xs_smem + 2 * XS_TILE_ELEMS;  // after the two transform tiles; [G][NRED]
+  cx* RED = (cx*)xs_smem + XS_MS_CX + 2 * XS_TILE_ELEMS;  // after the matrix copy and the two tiles; [G][NRED]
 #else
   cx* A = (cx*)xs_smem;
   cx* RED = A + (XS_NARR + XS_KARR + XS_KNARR) * GF;  // [G][NRED]

@@ -946,6 +946,21 @@ void tile_plan(const Problem& P, bool fp64, int tl[3], int lsp[3], size_t& elems
 // first coarse draw (ceil(NK/F) chunks each), then the k-filtered randoms.
 int knarr(const Problem& P) { return 2 * ((P.NK + P.F - 1) / P.F) + (P.NKV + P.F - 1) / P.F; }
 
+bool fft_dim(const Problem& P, int d);
+
+// Reals of the shared-memory copy of a real (DST/DCT) transform matrix used by the tiled
+// transforms when the field lives in device memory: the largest N_d^2 over such dimensions.
+size_t msm_reals(const Problem& P) {
+  size_t m = 0;
+  for (int d = 0; d < P.D; ++d) {
+    if (P.N[d] < 2 || fft_dim(P, d)) continue;
+    bool real_m = true;
+    for (int f = 0; f < P.F && real_m; ++f) real_m = P.type(d, f) != 0;
+    if (real_m) m = std::max(m, (size_t)P.N[d] * P.N[d]);
+  }
+  return m;
+}
+
 // MP with its midpoint iterations fused per site (noise in registers); not
 // possible when the drift reads neighbouring sites.
 bool lean_mp(const Problem& P) { return P.p.method == XS_METHOD_MP && !P.dstencil; }
@@ -960,11 +975,13 @@ size_t resident_smem(const xs_handle& h, int G, int narr) {
   if (narr == 0) warr = 0;  // field in device memory: the noise arrays live in the CTA's slice too
   if (narr > 0 && P.kobs) narr += 1;  // the k-space copy of the field for transformed observables
   if (narr > 0) narr += knarr(P);      // k-filtered noise arrays (in the slice when the field is in device memory)
-  if (narr == 0) {  // field in device memory: two transform tiles in shared memory
+  size_t ms_bytes = 0;
+  if (narr == 0) {  // field in device memory: two transform tiles (and a real matrix) in shared memory
     int tl[3], lsp[3];
     tile_plan(P, h.fp64, tl, lsp, tiles);
+    ms_bytes = (msm_reals(P) * rs + 15) / 16 * 16;
   }
-  return (size_t)narr * G * P.F * P.NS * cxs + 2 * tiles * cxs + (size_t)G * nred * cxs + 32 * 2 * nred * 8 +
+  return (size_t)narr * G * P.F * P.NS * cxs + 2 * tiles * cxs + ms_bytes + (size_t)G * nred * cxs + 32 * 2 * nred * 8 +
          warr * (size_t)G * nws * P.NS * rs;
 }
 
@@ -1264,6 +1281,7 @@ void build_source(xs_handle& h) {
     }
     for (int d = 0; d < 3; ++d) os << "#define XS_TL" << d + 1 << " " << tl[d] << "\n#define XS_LSP" << d + 1 << " " << lsp[d] << "\n";
     os << "#define XS_TILE_ELEMS " << elems << "\n#define XS_FFT_TILE_STAGES " << tstages << "\n";
+    os << "#define XS_MSM " << (h.rp.gfield ? msm_reals(P) : 0) << "\n";
     for (int d = 0; d < 3; ++d) {  // real transform matrices: every field non-periodic along d
       bool real_m = d < P.D;
       for (int f = 0; f < P.F && real_m; ++f) real_m = P.type(d, f) != 0;
