@@ -43,7 +43,7 @@ HBM_FALLBACK_GBS = 6650.0
 # problem (profiles/xs_stream_gpe_256x256.md); a launch's traffic grows in
 # proportion to the trajectories it processes, so bench lines scale these by
 # the trajectory count.
-NCU_TRAFFIC_PER_TRAJ = {"x_step": (268468480 + 211565056) / 512.0, "y_pass": (268484608 + 214534400) / 512.0}
+NCU_TRAFFIC_PER_TRAJ = {"x_step": (268465408 + 209754880) / 512.0, "y_pass": (268470528 + 213135104) / 512.0}
 
 
 def _peaks():
