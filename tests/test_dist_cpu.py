@@ -89,3 +89,18 @@ def test_two_ranks_match_single_process():
         pr.join(timeout=120)
         assert pr.exitcode == 0
     assert np.allclose(got, ref, rtol=0, atol=1e-12)
+
+
+def test_compensated_moment_sums():
+    """The moment accumulation over blocks keeps terms that a plain FP64 sum loses."""
+    import numpy as np
+    from xspde_matlab_b200.xsim import _kadd
+    s = np.zeros(3)
+    c = np.zeros(3)
+    for x in (1e16, 1.0, -1e16, 1.0, 3.0, -3.0):
+        _kadd(s, c, np.full(3, x))
+    assert np.all(s + c == 2.0)
+    plain = 0.0
+    for x in (1e16, 1.0, -1e16, 1.0, 3.0, -3.0):
+        plain += x
+    assert plain != 2.0

@@ -373,3 +373,15 @@ def test_knoise_field_in_device_memory_rk4_fp64():
              deriv=lambda a, w, p: -1j * a * np.conj(a) * a + 0.1 * (w[0:1] + 1j * w[1:2]),
              linear=lambda p: 0.5j * (p.Dx ** 2 + p.Dy ** 2), observe=[lambda a, p: a * np.conj(a)])
     _compare(g, o, [0], [1, 2], FP64_TOL)
+
+
+def test_block_means_are_compensated_sums_fp64():
+    """Block means sum the trajectories with Neumaier compensation: the values
+    [1e16, 1, -1e16, 1] average to exactly 0.5 (a plain left-to-right FP64 sum
+    loses both ones against 1e16 and gives 0.25)."""
+    base = dict(dimensions=1, points=[2], ranges=[0.1], steps=1, ensembles=[4, 1, 1], noises=1, method="MP",
+                checks=0)
+    g = dict(base, deriv="@(a,w,p) 0*a", initial="@(v,p) 0", observe=["@(a,p) real(a)"])
+    a0 = np.array([[1e16, 1.0, -1e16, 1.0]], dtype=complex)
+    av, _ = _gpu(g, [0], 1, a_in=a0)
+    assert np.all(np.real(av[0][0]) == 0.5), av[0][0]

@@ -261,6 +261,15 @@ __device__ __forceinline__ real xs_knormal(int k, u32 s, u32 e, u32 q, u32 seq, 
   return (k & 1) ? z1 : z0;
 }
 
+// Neumaier's compensated summation (A. Neumaier, ZAMM 54 (1974) 39-51) for the FP64
+// moment sums: the running sum s and the correction c together hold the total to about
+// one rounding of the exact sum, whatever the number of terms; the result is s + c.
+__device__ __forceinline__ void xs_kadd(double& s, double& c, double x) {
+  const double t = s + x;
+  c += fabs(s) >= fabs(x) ? (s - t) + x : (x - t) + s;
+  s = t;
+}
+
 // ---- block reductions --------------------------------------------------------
 __device__ __forceinline__ double xs_warp_sum(double v) {
 #pragma unroll

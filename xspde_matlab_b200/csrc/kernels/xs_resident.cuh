@@ -785,9 +785,9 @@ __device__ void xs_observe(const cx* A, cx* RED, int n, double t, const XsPathAr
     int i1, i2, i3;
     real x, y, z;
     xs_site(s, i1, i2, i3, x, y, z);
-    double sr[XS_NOUT_SITE], si[XS_NOUT_SITE];
+    double sr[XS_NOUT_SITE], si[XS_NOUT_SITE], cr[XS_NOUT_SITE], ci[XS_NOUT_SITE];  // compensated sums
 #pragma unroll
-    for (int k = 0; k < XS_NOUT_SITE; ++k) sr[k] = si[k] = 0;
+    for (int k = 0; k < XS_NOUT_SITE; ++k) sr[k] = si[k] = cr[k] = ci[k] = 0;
     for (int g = 0; g < XS_G; ++g) {
       cx a[XS_F], ak[XS_F], o[XS_NOUT_SITE];
 #pragma unroll
@@ -795,24 +795,31 @@ __device__ void xs_observe(const cx* A, cx* RED, int n, double t, const XsPathAr
       XS_LOAD_AK(g, s)
       xs_obs_site(a, ak, A, g, s, RED + g * (XS_NRED > 0 ? XS_NRED : 1), x, y, z, i1, i2, i3, (real)t, P.params, o);
 #pragma unroll
-      for (int k = 0; k < XS_NOUT_SITE; ++k) { sr[k] += (double)o[k].re; si[k] += (double)o[k].im; }
+      for (int k = 0; k < XS_NOUT_SITE; ++k) {
+        xs_kadd(sr[k], cr[k], (double)o[k].re);
+        if (xs_ocplx_site(k)) xs_kadd(si[k], ci[k], (double)o[k].im);
+      }
     }
 #pragma unroll
     for (int k = 0; k < XS_NOUT_SITE; ++k)
-      if (xs_ospec_site[k] == phase) out[(size_t)k * XS_NS + s] = make_double2(sr[k], si[k]);
+      if (xs_ospec_site(k) == phase) out[(size_t)k * XS_NS + s] = make_double2(sr[k] + cr[k], si[k] + ci[k]);
   }
 #endif
 #if XS_NOUT_SCALAR > 0
   if (threadIdx.x == 0) {
-    double sr[XS_NOUT_SCALAR], si[XS_NOUT_SCALAR];
-    for (int k = 0; k < XS_NOUT_SCALAR; ++k) sr[k] = si[k] = 0;
+    double sr[XS_NOUT_SCALAR], si[XS_NOUT_SCALAR], cr[XS_NOUT_SCALAR], ci[XS_NOUT_SCALAR];
+    for (int k = 0; k < XS_NOUT_SCALAR; ++k) sr[k] = si[k] = cr[k] = ci[k] = 0;
     for (int g = 0; g < XS_G; ++g) {
       cx o[XS_NOUT_SCALAR];
       xs_obs_scalar(RED + g * (XS_NRED > 0 ? XS_NRED : 1), (real)t, P.params, o);
-      for (int k = 0; k < XS_NOUT_SCALAR; ++k) { sr[k] += (double)o[k].re; si[k] += (double)o[k].im; }
+      for (int k = 0; k < XS_NOUT_SCALAR; ++k) {
+        xs_kadd(sr[k], cr[k], (double)o[k].re);
+        xs_kadd(si[k], ci[k], (double)o[k].im);
+      }
     }
     for (int k = 0; k < XS_NOUT_SCALAR; ++k)
-      if (xs_ospec_scalar[k] == phase) out[(size_t)XS_NOUT_SITE * XS_NS + k] = make_double2(sr[k], si[k]);
+      if (xs_ospec_scalar(k) == phase)
+        out[(size_t)XS_NOUT_SITE * XS_NS + k] = make_double2(sr[k] + cr[k], si[k] + ci[k]);
   }
 #endif
 #undef XS_LOAD_AK
@@ -1167,13 +1174,13 @@ extern "C" __global__ void __launch_bounds__(XS_THREADS) xs_batch(const XsBatchA
       const double inv = 1.0 / (double)it.ntraj;
       for (int k = threadIdx.x; k < it.npoints * XS_OBS_STRIDE; k += blockDim.x) {
         const int n = k / XS_OBS_STRIDE, q = k % XS_OBS_STRIDE;
-        double re = 0, im = 0;
+        double re = 0, im = 0, cre = 0, cim = 0;
         for (int c = 0; c < it.nunits; ++c) {
           const double2 v = __ldcg(it.part + ((size_t)n * it.nunits + c) * XS_OBS_STRIDE + q);
-          re += v.x;
-          im += v.y;
+          xs_kadd(re, cre, v.x);
+          xs_kadd(im, cim, v.y);
         }
-        it.av[k] = make_double2(re * inv, im * inv);
+        it.av[k] = make_double2((re + cre) * inv, (im + cim) * inv);
       }
     }
     __syncthreads();
@@ -1188,11 +1195,11 @@ extern "C" __global__ void xs_obs_reduce(const double2* __restrict__ partial, do
   const int n = blockIdx.y;
   const int b = blockIdx.z;
   if (k >= stride) return;
-  double sr = 0, si = 0;
+  double sr = 0, si = 0, cr = 0, ci = 0;
   for (int c = 0; c < ctas_per_block; ++c) {
     const double2 v = partial[((size_t)n * nctas + (size_t)b * ctas_per_block + c) * stride + k];
-    sr += v.x;
-    si += v.y;
+    xs_kadd(sr, cr, v.x);
+    xs_kadd(si, ci, v.y);
   }
-  av[((size_t)b * npoints + n) * stride + k] = make_double2(sr * inv_ens, si * inv_ens);
+  av[((size_t)b * npoints + n) * stride + k] = make_double2((sr + cr) * inv_ens, (si + ci) * inv_ens);
 }

@@ -46,6 +46,7 @@ struct XsStreamArgs {
   const double* params;      // runtime values of the named scalars p.<name>
   const cx* tw_x;            // [RX*RX] four-step twiddles of the rows, built in FP64 on the host
   const cx* tw_y;            // [RY*RY] four-step twiddles of the columns
+  double2* opart;            // [gridDim.z][nblocks][XS_NOUT_SITE * NS] per-split sums of xs_x_obs
 };
 
 #define XS_RX XS_FFT_RX
@@ -516,13 +517,16 @@ extern "C" __global__ void __launch_bounds__(XS_OROWS * XS_RX) xs_x_obs(const Xs
   const real tt = (real)A.t;
   XsWarpSync ws;
 #if XS_NOUT_SITE > 0
-  double sr[XS_NOUT_SITE][XS_RX], si[XS_NOUT_SITE][XS_RX];
+  // compensated sums over the block's trajectories (xs_kadd)
+  double sr[XS_NOUT_SITE][XS_RX], si[XS_NOUT_SITE][XS_RX], cr[XS_NOUT_SITE][XS_RX], ci[XS_NOUT_SITE][XS_RX];
 #pragma unroll
   for (int k = 0; k < XS_NOUT_SITE; ++k)
 #pragma unroll
-    for (int j = 0; j < XS_RX; ++j) sr[k][j] = si[k][j] = 0;
+    for (int j = 0; j < XS_RX; ++j) sr[k][j] = si[k][j] = cr[k][j] = ci[k][j] = 0;
 #endif
-  for (int el = 0; el < A.ens1; ++el) {
+  // the block's trajectories el = z, z + Z, ... (Z = gridDim.z splits of each block, for
+  // latency hiding; xs_x_obs_combine adds the splits)
+  for (int el = blockIdx.z; el < A.ens1; el += gridDim.z) {
     const int e = b * A.ens1 + el;
     cx v[XS_F][XS_RX];
     const cx* base = A.field + ((size_t)e * XS_F) * XS_NS + (size_t)y * XS_NX + t;
@@ -554,7 +558,10 @@ extern "C" __global__ void __launch_bounds__(XS_OROWS * XS_RX) xs_x_obs(const Xs
       cx o[XS_NOUT_SITE];
       xs_obs_site(a, a, (const cx*)nullptr, 0, 0, (const cx*)nullptr, x, yy, (real)0, t + XS_RX * j, y, 0, tt, A.params, o);
 #pragma unroll
-      for (int k = 0; k < XS_NOUT_SITE; ++k) { sr[k][j] += (double)o[k].re; si[k][j] += (double)o[k].im; }
+      for (int k = 0; k < XS_NOUT_SITE; ++k) {
+        xs_kadd(sr[k][j], cr[k][j], (double)o[k].re);
+        if (xs_ocplx_site(k)) xs_kadd(si[k][j], ci[k][j], (double)o[k].im);
+      }
 #endif
     }
 #if XS_NRED > 0
@@ -577,13 +584,43 @@ extern "C" __global__ void __launch_bounds__(XS_OROWS * XS_RX) xs_x_obs(const Xs
 #endif
   }
 #if XS_NOUT_SITE > 0
+  if (gridDim.z == 1) {
+    const double inv = 1.0 / (double)A.ens1;
+    double2* out = A.av + ((size_t)b * A.npoints + A.n) * XS_OBS_STRIDE;
+#pragma unroll
+    for (int k = 0; k < XS_NOUT_SITE; ++k)
+#pragma unroll
+      for (int j = 0; j < XS_RX; ++j)
+        out[(size_t)k * XS_NS + (size_t)y * XS_NX + t + XS_RX * j] =
+            make_double2((sr[k][j] + cr[k][j]) * inv, (si[k][j] + ci[k][j]) * inv);
+  } else {
+    double2* out = A.opart + ((size_t)blockIdx.z * gridDim.y + b) * ((size_t)XS_NOUT_SITE * XS_NS);
+#pragma unroll
+    for (int k = 0; k < XS_NOUT_SITE; ++k)
+#pragma unroll
+      for (int j = 0; j < XS_RX; ++j)
+        out[(size_t)k * XS_NS + (size_t)y * XS_NX + t + XS_RX * j] =
+            make_double2(sr[k][j] + cr[k][j], si[k][j] + ci[k][j]);
+  }
+#endif
+}
+
+// Block means of the site observables from the nsplit partial sums of xs_x_obs
+// (compensated, fixed order): grid (ceil(NOUT_SITE * NS / 256), nblocks).
+extern "C" __global__ void __launch_bounds__(256) xs_x_obs_combine(const XsStreamArgs A, int nsplit) {
+#if XS_NOUT_SITE > 0
+  constexpr size_t M = (size_t)XS_NOUT_SITE * XS_NS;
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int b = blockIdx.y;
+  if (i >= M) return;
+  double re = 0, im = 0, cre = 0, cim = 0;
+  for (int z = 0; z < nsplit; ++z) {
+    const double2 q = A.opart[((size_t)z * gridDim.y + b) * M + i];
+    xs_kadd(re, cre, q.x);
+    xs_kadd(im, cim, q.y);
+  }
   const double inv = 1.0 / (double)A.ens1;
-  double2* out = A.av + ((size_t)b * A.npoints + A.n) * XS_OBS_STRIDE;
-#pragma unroll
-  for (int k = 0; k < XS_NOUT_SITE; ++k)
-#pragma unroll
-    for (int j = 0; j < XS_RX; ++j)
-      out[(size_t)k * XS_NS + (size_t)y * XS_NX + t + XS_RX * j] = make_double2(sr[k][j] * inv, si[k][j] * inv);
+  A.av[((size_t)b * A.npoints + A.n) * XS_OBS_STRIDE + i] = make_double2((re + cre) * inv, (im + cim) * inv);
 #endif
 }
 
@@ -597,9 +634,9 @@ extern "C" __global__ void __launch_bounds__(256) xs_stream_scalar(const XsStrea
     if (threadIdx.x == 0) atomicOr(A.status, 2);
     return;
   }
-  double acc[2 * XS_NOUT_SCALAR];
+  double acc[2 * XS_NOUT_SCALAR], cmp[2 * XS_NOUT_SCALAR];  // compensated per-thread sums
 #pragma unroll
-  for (int k = 0; k < 2 * XS_NOUT_SCALAR; ++k) acc[k] = 0;
+  for (int k = 0; k < 2 * XS_NOUT_SCALAR; ++k) acc[k] = cmp[k] = 0;
   for (int el = threadIdx.x; el < A.ens1; el += blockDim.x) {
     const int e = b * A.ens1 + el;
     cx red[XS_NRED > 0 ? XS_NRED : 1];
@@ -616,12 +653,15 @@ extern "C" __global__ void __launch_bounds__(256) xs_stream_scalar(const XsStrea
     cx o[XS_NOUT_SCALAR];
     xs_obs_scalar(red, (real)A.t, A.params, o);
 #pragma unroll
-    for (int k = 0; k < XS_NOUT_SCALAR; ++k) { acc[2 * k] += (double)o[k].re; acc[2 * k + 1] += (double)o[k].im; }
+    for (int k = 0; k < XS_NOUT_SCALAR; ++k) {
+      xs_kadd(acc[2 * k], cmp[2 * k], (double)o[k].re);
+      xs_kadd(acc[2 * k + 1], cmp[2 * k + 1], (double)o[k].im);
+    }
   }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
   for (int k = 0; k < 2 * XS_NOUT_SCALAR; ++k) {
-    const double s = xs_warp_sum(acc[k]);
+    const double s = xs_warp_sum(acc[k] + cmp[k]);
     if (lane == 0) part[warp][k] = s;
   }
   __syncthreads();

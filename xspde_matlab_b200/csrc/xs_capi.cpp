@@ -634,16 +634,27 @@ void generate_functions(Problem& P, std::ostringstream& os) {
   }
   os << "#define XS_NRED " << P.nred << "\n#define XS_NOUT_SITE " << P.nout_site << "\n#define XS_NOUT_SCALAR "
      << P.nout_scalar << "\n#define XS_OBS_STRIDE (XS_NOUT_SITE * XS_NS + XS_NOUT_SCALAR)\n";
-  // output slots evaluated on the time spectrum (1) or on the field at the output time (0)
+  // output slots evaluated on the time spectrum (1) or on the field at the output time (0), and
+  // slots whose values can have an imaginary part (real ones skip the imaginary moment sums)
   {
     std::vector<int> site(std::max(P.nout_site, 1), 0), scal(std::max(P.nout_scalar, 1), 0);
+    std::vector<int> csite(std::max(P.nout_site, 1), 0), cscal(std::max(P.nout_scalar, 1), 0);
     for (auto& o : P.obs)
-      for (int l = 0; l < o.lines; ++l) (o.spatial ? site : scal)[o.out_off + l] = o.tspec ? 1 : 0;
-    os << "#define XS_SPEC " << (P.spec ? 1 : 0) << "\n__device__ const signed char xs_ospec_site[] = {";
-    for (size_t i = 0; i < site.size(); ++i) os << (i ? "," : "") << site[i];
-    os << "};\n__device__ const signed char xs_ospec_scalar[] = {";
-    for (size_t i = 0; i < scal.size(); ++i) os << (i ? "," : "") << scal[i];
-    os << "};\n";
+      for (int l = 0; l < o.lines; ++l) {
+        (o.spatial ? site : scal)[o.out_off + l] = o.tspec ? 1 : 0;
+        (o.spatial ? csite : cscal)[o.out_off + l] = o.gen.is_complex ? 1 : 0;
+      }
+    // inline switch functions: with the slot index a constant (unrolled loops) they fold away
+    auto table = [&](const char* name, const std::vector<int>& v) {
+      os << "__device__ __forceinline__ int " << name << "(int k) {\n  switch (k) {\n";
+      for (size_t i = 0; i < v.size(); ++i) os << "    case " << i << ": return " << v[i] << ";\n";
+      os << "    default: return 0;\n  }\n}\n";
+    };
+    os << "#define XS_SPEC " << (P.spec ? 1 : 0) << "\n";
+    table("xs_ospec_site", site);
+    table("xs_ospec_scalar", scal);
+    table("xs_ocplx_site", csite);
+    table("xs_ocplx_scalar", cscal);
   }
   // k-space observables: transformed dimensions, normalisation prod kfact = prod dx/sqrt(2 pi) (xnft.m),
   // k grids of the observe functions (p.kx ... in propagation order)
@@ -866,6 +877,7 @@ struct xs_handle {
   bool loaded = false;
   CUmodule mod = nullptr;
   CUfunction f_resident = nullptr, f_reduce = nullptr, f_noise = nullptr, f_random = nullptr, f_feat = nullptr;
+  CUfunction f_xcomb = nullptr;  // adds the trajectory splits of xs_x_obs
   CUfunction f_xinit = nullptr, f_xnl = nullptr, f_xfinal = nullptr, f_spass = nullptr, f_xobs = nullptr,
              f_scalar = nullptr;
   StreamPlan sp;
@@ -883,7 +895,8 @@ struct xs_handle {
   CUfunction f_batch = nullptr;
   cudaStream_t stream = nullptr;
   DevBuf d_prop[2], d_prop2[2], d_tmat, d_obs, d_av, d_ain, d_aout, d_status, d_w, d_field, d_redpart, d_pstep,
-      d_params, d_gfield, d_twiddle, d_tmp, d_avm, d_bval[2], d_bda[2], d_aft, d_twt, d_raw, d_kfilt, d_rfilt;
+      d_params, d_gfield, d_twiddle, d_tmp, d_avm, d_bval[2], d_bda[2], d_aft, d_twt, d_raw, d_kfilt, d_rfilt,
+      d_opart;
   int bval_n[2] = {0, 0};
   int twt_n = 0;
   void* raw_dev = nullptr;  // raw trajectories of the current resident launch (xs_run_path_raw)
@@ -1315,7 +1328,8 @@ void load_module(xs_handle& h) {
       size_t smem;
     } fns[] = {{&h.f_xinit, "xs_x_init", h.sp.xsmem}, {&h.f_xnl, "xs_x_nl", h.sp.xsmem},
                {&h.f_xfinal, "xs_x_final", h.sp.xsmem}, {&h.f_spass, "xs_s_pass", h.sp.ssmem},
-               {&h.f_xobs, "xs_x_obs", h.sp.osmem}, {&h.f_scalar, "xs_stream_scalar", 0}};
+               {&h.f_xobs, "xs_x_obs", h.sp.osmem}, {&h.f_scalar, "xs_stream_scalar", 0},
+               {&h.f_xcomb, "xs_x_obs_combine", 0}};
     cu_check(d.getfn(&h.f_noise, h.mod, "xs_export_noise"), "xs_export_noise");
     cu_check(d.getfn(&h.f_random, h.mod, "xs_export_random"), "xs_export_random");
     {
@@ -1700,7 +1714,23 @@ struct StreamArgsHost {
   const double* params;
   const void* tw_x;
   const void* tw_y;
+  void* opart;
 };
+
+// Observation pass: each block's trajectories split over kObsSplit CTAs (grid z) for latency
+// hiding, then xs_x_obs_combine adds the splits into the block means.
+constexpr int kObsSplit = 4;
+void launch_observe(xs_handle& h, void** prm, int nrg, int nb, cudaStream_t st) {
+  const StreamPlan& sp = h.sp;
+  xs_launch(h, XS_KERNEL_X_OBS, h.f_xobs, (unsigned)nrg, (unsigned)nb, kObsSplit, (unsigned)(sp.OROWS * sp.RX),
+            (unsigned)sp.osmem, st, prm, "observation pass");
+  if (h.P.nout_site) {
+    int nsplit = kObsSplit;
+    void* cprm[] = {prm[0], &nsplit};
+    const unsigned gx = (unsigned)(((size_t)h.P.nout_site * h.P.NS + 255) / 256);
+    xs_launch(h, XS_KERNEL_X_OBS, h.f_xcomb, gx, (unsigned)nb, 1, 256, 0, st, cprm, "observation combine");
+  }
+}
 
 // The pass sequence of one streaming p.path call (Simulator/xpath.m:137-194 with merged MP
 // half steps): initial field, then per step a column pass (exp(L dt)^m, m = 2 when the previous
@@ -1794,8 +1824,7 @@ void launch_stream_halves(xs_handle& h, const StreamArgsHost& a, int nblocks, in
         xs_launch(h, XS_KERNEL_Y_PASS, h.f_spass, sgrid, 1, 1, 256, (unsigned)sp.ssmem, st, prm, "column pass");
         break;
       case StreamOp::OBS:
-        xs_launch(h, XS_KERNEL_X_OBS, h.f_xobs, (unsigned)nrg, (unsigned)nb, 1, (unsigned)(sp.OROWS * sp.RX),
-                  (unsigned)sp.osmem, st, prm, "observation pass");
+        launch_observe(h, prm, nrg, nb, st);
         if (P.nout_scalar)
           xs_launch(h, XS_KERNEL_SCALAR, h.f_scalar, (unsigned)nb, 1, 1, 256, 0, st, prm, "scalar observables");
         break;
@@ -1859,6 +1888,10 @@ void launch_stream(xs_handle& h, int first_block, int nblocks, int nc, const voi
   a.params = (const double*)h.d_params.p;
   a.tw_x = h.d_twiddle.p;
   a.tw_y = (const char*)h.d_twiddle.p + (size_t)sp.RX * sp.RX * cxs;
+  if (P.nout_site) {
+    h.d_opart.ensure((size_t)kObsSplit * nblocks * P.nout_site * P.NS * 16);
+    a.opart = h.d_opart.p;
+  }
   void* params[] = {&a};
   const unsigned xgrid = (unsigned)((size_t)total * P.N[1] / sp.XROWS);
   const unsigned sgrid = (unsigned)((size_t)total * P.F * (P.N[0] / sp.TX));
@@ -1892,8 +1925,7 @@ void launch_stream(xs_handle& h, int first_block, int nblocks, int nc, const voi
   };
   auto observe = [&](int n) {
     a.n = n;
-    xs_launch(h, XS_KERNEL_X_OBS, h.f_xobs, (unsigned)nrg, (unsigned)nblocks, 1, (unsigned)(sp.OROWS * sp.RX),
-              (unsigned)sp.osmem, st, params, "observation pass");
+    launch_observe(h, params, nrg, nblocks, st);
     if (P.nout_scalar)
       xs_launch(h, XS_KERNEL_SCALAR, h.f_scalar, (unsigned)nblocks, 1, 1, 256, 0, st, params, "scalar observables");
   };
@@ -3018,6 +3050,7 @@ void batch_prepare(xs_batch& b) {
       const Problem& P = h.P;
       h.d_field.ensure((size_t)P.E1 * P.F * P.NS * (h.fp64 ? 16 : 8));
       if (P.nred) h.d_redpart.ensure((size_t)P.E1 * (P.N[1] / h.sp.OROWS) * P.nred * 16);
+      if (P.nout_site) h.d_opart.ensure((size_t)kObsSplit * P.nout_site * P.NS * 16);
       ensure_prop(h, 1);
       ensure_prop2(h, 1);
       sitems.push_back((int)i);

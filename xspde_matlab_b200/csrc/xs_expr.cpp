@@ -1160,7 +1160,7 @@ Generated generate(const AnonFn& fn, const GenCtx& ctx) {
   Val v = g.gen(fn.body);
   Generated out;
   out.len = v.len;
-  out.is_complex = true;
+  out.is_complex = v.cplx;
   std::ostringstream code;
   code << g.os.str();
   for (int i = 0; i < v.len; ++i)

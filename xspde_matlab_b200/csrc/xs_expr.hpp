@@ -77,7 +77,7 @@ struct Reduction {
 
 struct Generated {
   int len = 1;                       // components of the result
-  bool is_complex = true;
+  bool is_complex = true;   // the result has an imaginary part (else out[i].im = 0)
   std::string code;                  // device statements; result in out[0..len)
   std::vector<Reduction> reductions; // observe only
   bool uses_k = false;               // needs k-space field (not supported: error)

@@ -447,6 +447,15 @@ def _grid(xk):
     return q
 
 
+def _kadd(s, c, x):
+    """Neumaier's compensated summation (ZAMM 54 (1974) 39-51), elementwise and in
+    place: the running sums s and corrections c together hold each total to about
+    one rounding of the exact sum; the result is s + c."""
+    t = s + x
+    c += np.where(np.abs(s) >= np.abs(x), (s - t) + x, (x - t) + s)
+    s[...] = t
+
+
 def _ensembles(inp, paths, rank=0, size=1, reduce=None, raw=None):
     """Block loop, check passes and moments (Simulator/xensemble.m:12-108) with
     all blocks of a pass integrated by one device call.  With size > 1 this
@@ -465,6 +474,7 @@ def _ensembles(inp, paths, rank=0, size=1, reduce=None, raw=None):
     for s, p in enumerate(inp):
         data.append([None] * len(p.output))
     D = {}
+    comp = {}  # compensation terms of the moment sums (_kadd)
     lo, hi = shard(nb, rank, size)
     chunk = max(1, min(nb, int(2 ** 27 // max(1, paths[0].per_block * 8))))
     for b0 in range(lo, hi, chunk):
@@ -506,10 +516,14 @@ def _ensembles(inp, paths, rank=0, size=1, reduce=None, raw=None):
                         D[(s, b, 1, o)] = d1 + (d1 - d2) / (2 ** p.order - 1.0)
                     if data[s][o] is None:
                         data[s][o] = np.zeros((D[(s, b, 1, o)].size, m1))
+                        comp[(s, o)] = np.zeros_like(data[s][o])
+                    ds, dc = data[s][o], comp[(s, o)]
                     for n1 in range(1, m + 1):
-                        data[s][o][:, n1 - 1] += D[(s, b, n1, o)] * inv
-                    data[s][o][:, m1 - 1] += D[(s, b, 1, o)] ** 2 * inv
+                        _kadd(ds[:, n1 - 1], dc[:, n1 - 1], D[(s, b, n1, o)] * inv)
+                    _kadd(ds[:, m1 - 1], dc[:, m1 - 1], D[(s, b, 1, o)] ** 2 * inv)
         D.clear()
+    for (s, o), c in comp.items():
+        data[s][o] = data[s][o] + c
     if size > 1:
         for s, p in enumerate(inp):
             for o in range(len(p.output)):
