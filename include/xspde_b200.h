@@ -112,6 +112,10 @@ typedef struct xs_problem {
                                   p.nfilter multiplies each k-space noise value by, the k lattice in FFT
                                   order (p.kx ... in propagation order, Simulator/xgrid.m) */
   const double* rfilter;       /* the same for p.rfilter and krandoms */
+  int auxfields;               /* p.auxfields: components of the auxiliary cell (Simulator/xpath.m:36-45),
+                                  0 for none; observe functions then take (a, x, p) */
+  const char* define;          /* p.define text "@(a,w,p) ...": the auxiliary cell from the field and
+                                  the step's noise, averaged over the start and end of each step */
 } xs_problem;
 
 /* Create a handle: parse, generate and compile the kernels (NVRTC, cached).

@@ -119,6 +119,8 @@ def xpreferences(inputs):
             p.checks = out[0].checks                                     # :32
         p.iterations = int(p.get("iterations", 4))                       # :59
         p.rawdata = int(p.get("rawdata", 0))                             # :85
+        p.auxfields = int(np.atleast_1d(p.get("auxfields", 0))[0])       # :46 (one auxiliary cell)
+        p.define = p.get("define", None)                                 # :93
         if "deriv" not in p:
             p.deriv = lambda a, w, p: 0 * a                              # :64
         nz = p.get("noises", None)
@@ -168,6 +170,7 @@ def xpreferences(inputs):
         p.space = space
         p.nspace = int(np.prod(space)) if space else 1
         p.ca = [p.fields] + space + [ens[0]]                              # :145
+        p.cax = [p.auxfields] + space + [ens[0]]                          # auxiliary cell
         p.dk = [2 * math.pi / (points[d] * dx[d]) for d in range(nd)]    # :165
         p.dk[0] /= p.steps[0]                                            # :166
         p.kfact = [x / math.sqrt(2 * math.pi) for x in dx]               # :167
@@ -220,10 +223,10 @@ def xpreferences(inputs):
             p.xk.append(xk)
         p.d_obs, p.d_av = [], []
         a0 = np.zeros(p.ca, dtype=complex)
+        x0 = np.zeros(p.cax, dtype=complex) if p.auxfields else None
         for n in range(len(p.observe)):
             p.nobserve = n
-            O = _transform_obs(a0, n, p)
-            O = np.asarray(p.observe[n](O, p))
+            O = _observe(a0, x0, n, p)
             sz = msize(O)
             if sz[-1] > ens[0] and sz[-1] % ens[0] == 0:                 # :269-272
                 szl = sz[-1]
@@ -814,11 +817,20 @@ def _transform_obs(a, n, p):
     return a
 
 
-def xdata(a, n, p):
-    """Ensemble mean of observe{n} at the current time (xdata.m:330-395)."""
-    p.nobserve = n
+def _observe(a, x, n, p):
+    """observe{n}(a{:}, p) on the (transformed) cells: the field, then the
+    auxiliary cell when there is one (xdata.m:24-29)."""
     a = _transform_obs(a, n, p)
-    obs = np.asarray(p.observe[n](a, p))
+    if p.auxfields:
+        return np.asarray(p.observe[n](a, _transform_obs(x, n, p), p))
+    return np.asarray(p.observe[n](a, p))
+
+
+def xdata(a, n, p, x=None):
+    """Ensemble mean of observe{n} at the current time (xdata.m:330-395); x is
+    the auxiliary cell (p.auxfields)."""
+    p.nobserve = n
+    obs = _observe(a, x, n, p)
     obs = fit(obs, p.d_obs[n])
     return np.mean(obs, axis=3)                                          # :84
 
@@ -933,6 +945,9 @@ def xpath(a, nc, p):
     aft = np.zeros((P1 * S,) + np.shape(a), dtype=complex) if spectrum else None
     # raw{l}: [fields, points(1), space, ens] (xpreferences.m:148)
     raw = np.zeros((np.shape(a)[0], P1) + np.shape(a)[1:], dtype=complex) if p.rawdata else None
+    # auxiliary cell (p.auxfields, p.define): set by xensemble at the start of the path
+    x = np.array(p.aux0, dtype=complex) if p.auxfields else None
+    aftx = np.zeros((P1 * S,) + np.shape(x), dtype=complex) if (spectrum and p.auxfields) else None
     n1 = -1
     for n in range(P1):                                                  # :137
         for step in range(S):                                            # :138
@@ -942,35 +957,60 @@ def xpath(a, nc, p):
                     p.draw += 1
                     w = p.noisegen(w, nc, p.nscale, p)                   # :142
                     if nc == 1 or checks == 1:                           # :143
+                        if p.auxfields:                                  # :36-38
+                            x = fit(np.asarray(call_cells(p.define, a, w, p), dtype=complex), p.cax)
                         a = method(a, w, p)                              # :150
+                        if p.auxfields:                                  # :42-44 (same p.t, same noise)
+                            x = 0.5 * (x + fit(np.asarray(call_cells(p.define, a, w, p), dtype=complex), p.cax))
                         if spectrum:                                     # :46-54
                             if checks == 1 and nc == 1:
                                 aft[n1] = (a + aft[n1]) / 2
+                                if p.auxfields:
+                                    aftx[n1] = (x + aftx[n1]) / 2
                             else:
                                 aft[n1] = a
+                                if p.auxfields:
+                                    aftx[n1] = x
                         w = None                                         # :164
                         p.t = p.t + p.dtr                                # :165
             elif spectrum:                                               # :64-68
                 aft[n1] = a
+                if p.auxfields:
+                    aftx[n1] = x
             if step == 0:                                                # :181
                 if p.rawdata:                                            # :72-77
                     raw[:, n] = a
                 for o in p.averages:
                     if not p.transforms[o][0]:
-                        r = xdata(a, o, p)
+                        r = xdata(a, o, p, x)
                         L = p.d_av[o][0]
                         av[o][:, n] = freshape(r, [L] + list(p.d_av[o][2:]))
     if spectrum:                                                         # :90-106
         nt = P1 * S
         f = np.fft.fftshift(np.fft.ifft(aft, axis=0) * p.fsc, axes=0)   # ifft(aft, P1 S, 2) * fsc, fftshift
+        fx = np.fft.fftshift(np.fft.ifft(aftx, axis=0) * p.fsc, axes=0) if p.auxfields else None
         sel = np.arange(P1) - P1 // 2 + nt // 2                          # specpts = plotpts + floor(S P1/2) + 1
         for n in range(P1):
             for o in p.averages:
                 if p.transforms[o][0]:
-                    r = xdata(f[sel[n]], o, p)
+                    r = xdata(f[sel[n]], o, p, fx[sel[n]] if p.auxfields else None)
                     L = p.d_av[o][0]
                     av[o][:, n] = freshape(r, [L] + list(p.d_av[o][2:]))
     return a, av, raw
+
+
+AUX_DRAW = 0xFFFFFFFF  # Philox draw index of the noise for the initial auxiliary cell
+
+
+def initial_aux(a, nc, p):
+    """Initial auxiliary cell (xensemble.m:74-77): p.define(a, w, p) on one
+    noise draw of its own (Philox draw AUX_DRAW), at the current p.t; stored
+    in p.aux0 for the path."""
+    if not p.auxfields:
+        return
+    p.draw = AUX_DRAW
+    w = p.noisegen(None, nc, p.nscale, p)
+    p.aux0 = fit(np.asarray(call_cells(p.define, a, w, p), dtype=complex), p.cax)
 
 
 def xensemble(npar, inputs):
@@ -1010,6 +1050,7 @@ def xensemble(npar, inputs):
                     p.t = p.origins[0] - 1
                     for d in range(1, p.dimensions):
                         p.boundval[d] = p.boundfun(a, 0, d, p)
+                initial_aux(a, nc, p)                                    # :74-77
                 p.t = p.origins[0]
                 b, av, r = p.path(a, nc, p)                              # :79
                 raws[s][nc - 1][j] = r

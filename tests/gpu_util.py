@@ -21,6 +21,7 @@ def oracle_block_av(pdict, block, nc):
         v = p.randomgen(p)
         p.t = p.origins[0]
         a = X.fit(np.asarray(X.call_cells(p.initial, None, v, p), dtype=complex), p.ca)
+        X.initial_aux(a, nc, p)
         b, av, raw = p.path(a, nc, p)
     if p.rawdata:
         return av, b, raw

@@ -385,3 +385,53 @@ def test_block_means_are_compensated_sums_fp64():
     a0 = np.array([[1e16, 1.0, -1e16, 1.0]], dtype=complex)
     av, _ = _gpu(g, [0], 1, a_in=a0)
     assert np.all(np.real(av[0][0]) == 0.5), av[0][0]
+
+
+def _a1(w):
+    return (w[0:1] + 1j * w[1:2]) / 2
+
+
+@pytest.mark.parametrize("method", ["MP", "RK4"])
+def test_auxiliary_fields_with_spectra_fp64(method):
+    """Auxiliary fields (p.auxfields, p.define; xpath.m:36-45, xensemble.m:74-77):
+    Examples/SDE_1D/Quantum.m form, input and output fields defined from the
+    oscillator and its noise, observed in time and as time spectra, both check passes."""
+    base = dict(points=[41], ranges=[8.0], auxfields=2, noises=2, ensembles=[16, 2, 1], method=method, checks=1,
+                transforms=[[1], [1], [1], [0]])
+    g = dict(base, initial="@(w,p) (w(1,:)+1i*w(2,:))/2", deriv="@(a,w,p) -a(1,:)+sqrt(2)*(w(1,:)+1i*w(2,:))/2",
+             define="@(a,w,p) [(w(1,:)+1i*w(2,:))/2; sqrt(2)*a(1,:)-(w(1,:)+1i*w(2,:))/2]",
+             observe=["@(a,x,p) abs(a(1,:)).^2", "@(a,x,p) abs(x(1,:)).^2", "@(a,x,p) abs(x(2,:)).^2",
+                      "@(a,x,p) x(2,:)"])
+    o = dict(base, initial=lambda w, p: _a1(w), deriv=lambda a, w, p: -a[0:1] + np.sqrt(2) * _a1(w),
+             define=lambda a, w, p: np.concatenate([_a1(w), np.sqrt(2) * a[0:1] - _a1(w)]),
+             observe=[lambda a, x, p: abs(a[0:1]) ** 2, lambda a, x, p: abs(x[0:1]) ** 2,
+                      lambda a, x, p: abs(x[1:2]) ** 2, lambda a, x, p: x[1:2]])
+    _compare(g, o, [0, 1], [1, 2], FP64_TOL)
+
+
+def test_auxiliary_field_time_dependent_define_fp64():
+    """Examples/SDE_1D/Kubodefine.m form: define = exp(5i t) a reads p.t, which
+    stays at the start of the step for both evaluations around the method."""
+    base = dict(points=[21], ranges=[4.0], auxfields=1, noises=1, ensembles=[32, 2, 1], method="RK4", checks=1,
+                transforms=[[0], [1], [1]])
+    g = dict(base, initial="@(w,p) 1+0*w", deriv="@(a,w,p) 1i*w.*a", define="@(a,w,p) exp(5*1i*p.t).*a",
+             observe=["@(a,x,p) a", "@(a,x,p) a.*conj(a)", "@(a,x,p) x.*conj(x)"])
+    o = dict(base, initial=lambda w, p: 1 + 0 * w, deriv=lambda a, w, p: 1j * w * a,
+             define=lambda a, w, p: np.exp(5j * p.t) * a,
+             observe=[lambda a, x, p: a, lambda a, x, p: a * np.conj(a), lambda a, x, p: x * np.conj(x)])
+    _compare(g, o, [0, 1], [1, 2], FP64_TOL)
+
+
+def test_auxiliary_field_on_a_lattice_fp64():
+    """An auxiliary field on a 1D lattice with noise in its definition, observed
+    per site and through an integral."""
+    base = dict(dimensions=2, points=[6, 32], ranges=[0.5, 8.0], auxfields=1, noises=2, ensembles=[4, 2, 1],
+                method="MP", checks=1)
+    g = dict(base, deriv="@(a,w,p) 1i*a.*conj(a).*a + 0.1*(w(1,:)+1i*w(2,:))", initial="@(v,p) exp(-p.x.^2)",
+             linear="@(p) 1i*p.Dx.^2", define="@(a,w,p) a.*conj(a) + w(1,:)",
+             observe=["@(a,x,p) a.*conj(a)", "@(a,x,p) Int(real(x),p)", "@(a,x,p) x"])
+    o = dict(base, deriv=lambda a, w, p: 1j * a * np.conj(a) * a + 0.1 * (w[0:1] + 1j * w[1:2]),
+             initial=lambda v, p: np.exp(-p.x ** 2), linear=lambda p: 1j * p.Dx ** 2,
+             define=lambda a, w, p: a * np.conj(a) + w[0:1],
+             observe=[lambda a, x, p: a * np.conj(a), lambda a, x, p: X.Int(np.real(x), p), lambda a, x, p: x])
+    _compare(g, o, [0, 1], [1, 2], FP64_TOL)

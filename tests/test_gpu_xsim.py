@@ -247,3 +247,38 @@ def test_gpu_xsim_planar_knoise_known_answer():
     for k in range(3):
         mean, err = np.real(dg[0][k][:, 0]), np.real(dg[0][k][:, 2])
         assert np.all(np.abs(mean - (1 + t) * 192) < 5 * err), k
+
+
+def test_gpu_xsim_quantum_auxiliary_spectra():
+    """Examples/SDE_1D/Quantum.m (shorter run) through xsim: the oscillator's
+    spectrum meets 1/(1 + w^2), the input and output fields' spectra 1/2, and
+    errors and data match the oracle's xsim."""
+    from xspde_matlab_b200 import xsim
+    T = 40.0
+
+    def a1(w):
+        return (w[0:1] + 1j * w[1:2]) / 2
+    base = dict(points=[201], ranges=[T], order=2, auxfields=2, noises=2, ensembles=[100, 1, 12],
+                transforms=[[1], [1], [1], [0]])
+    c = 2 * np.pi / T
+    g = dict(base, initial="@(w,p) (w(1,:)+1i*w(2,:))/2", deriv="@(a,w,p) -a(1,:)+sqrt(2)*(w(1,:)+1i*w(2,:))/2",
+             define="@(a,w,p) [(w(1,:)+1i*w(2,:))/2; sqrt(2)*a(1,:)-(w(1,:)+1i*w(2,:))/2]",
+             observe=["@(a,x,p) %r*abs(a(1,:)).^2" % c, "@(a,x,p) %r*abs(x(1,:)).^2" % c,
+                      "@(a,x,p) %r*abs(x(2,:)).^2" % c, "@(a,x,p) abs(a(1,:)).^2"])
+    o = dict(base, initial=lambda w, p: a1(w), deriv=lambda a, w, p: -a[0:1] + np.sqrt(2) * a1(w),
+             define=lambda a, w, p: np.concatenate([a1(w), np.sqrt(2) * a[0:1] - a1(w)]),
+             observe=[lambda a, x, p: c * abs(a[0:1]) ** 2, lambda a, x, p: c * abs(x[0:1]) ** 2,
+                      lambda a, x, p: c * abs(x[1:2]) ** 2, lambda a, x, p: abs(a[0:1]) ** 2])
+    eg, dg, ig = xsim(g)
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore", RuntimeWarning)
+        eo, do, io = X.xsim(o)
+    keep = [i for i in range(len(eo)) if i != 5]
+    assert np.allclose(np.asarray(eg)[keep], np.asarray(eo)[keep], rtol=1e-8, atol=1e-14)
+    for a, b in zip(dg[0], do[0]):
+        assert np.allclose(np.asarray(a), np.asarray(b), rtol=1e-8, atol=1e-12)
+    w = io[0].kc[0]
+    sel = np.abs(w) < 3
+    for k, exact in ((0, 1 / (1 + w ** 2)), (1, 0.5 + 0 * w), (2, 0.5 + 0 * w)):
+        mean, err = np.real(dg[0][k][:, 0]), np.real(dg[0][k][:, 2])
+        assert np.all(np.abs(mean[sel] - exact[sel]) < 5 * err[sel] + 1e-3), k

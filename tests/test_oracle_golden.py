@@ -119,3 +119,33 @@ def test_knoise_planar_known_answer():
         mean, err = np.real(data[0][k][:, 0]), np.real(data[0][k][:, 2])
         assert np.all(np.abs(mean - exact) < 5 * err + 1e-9 * exact), k
     assert np.allclose(data[0][1][:, 0], data[0][2][:, 0], rtol=1e-10)
+
+
+def test_auxiliary_fields_quantum_known_answer():
+    """Examples/SDE_1D/Quantum.m (shorter run): auxiliary fields from p.define
+    (xpath.m:36-45, xensemble.m:74-77) carry the input and output fields of a
+    damped oscillator; their spectra are flat at 1/2 and the oscillator's is
+    1/(1 + w^2), the example's comparisons, within five sampling errors."""
+    T = 40.0
+
+    def a1(w):
+        return (w[0:1] + 1j * w[1:2]) / 2
+    o = dict(points=[201], ranges=[T], order=2, auxfields=2, noises=2, ensembles=[100, 1, 12],
+             initial=lambda w, p: (w[0:1] + 1j * w[1:2]) / 2,
+             deriv=lambda a, w, p: -a[0:1] + np.sqrt(2) * a1(w),
+             define=lambda a, w, p: np.concatenate([a1(w), np.sqrt(2) * a[0:1] - a1(w)]),
+             observe=[lambda a, x, p: (2 * np.pi / T) * abs(a[0:1]) ** 2,
+                      lambda a, x, p: (2 * np.pi / T) * abs(x[0:1]) ** 2,
+                      lambda a, x, p: (2 * np.pi / T) * abs(x[1:2]) ** 2, lambda a, x, p: abs(a[0:1]) ** 2],
+             transforms=[[1], [1], [1], [0]])
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore", RuntimeWarning)
+        e, data, inp = X.xsim(o)
+    w = inp[0].kc[0]
+    sel = np.abs(w) < 3
+    for k, exact in ((0, 1 / (1 + w ** 2)), (1, 0.5 + 0 * w), (2, 0.5 + 0 * w), (3, None)):
+        mean, err = np.real(data[0][k][:, 0]), np.real(data[0][k][:, 2])
+        if exact is None:
+            assert np.all(np.abs(mean - 0.5) < 5 * err + 0.02)
+        else:
+            assert np.all(np.abs(mean[sel] - exact[sel]) < 5 * err[sel] + 1e-3), k

@@ -58,6 +58,8 @@ class XsProblem(ctypes.Structure):
         ("krandoms", ctypes.c_int),
         ("nfilter", ctypes.POINTER(ctypes.c_double)),
         ("rfilter", ctypes.POINTER(ctypes.c_double)),
+        ("auxfields", ctypes.c_int),
+        ("define", ctypes.c_char_p),
     ]
 
 

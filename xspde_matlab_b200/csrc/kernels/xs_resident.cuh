@@ -85,6 +85,12 @@ __device__ __forceinline__ cx* xs_zbuf(const XsPathArgs& P) {
 #endif
 }
 #define XS_ZIDX(k, g, s) ((size_t)((k) / XS_F) * (XS_G * XS_F * XS_NS) + ((g) * XS_F + (k) % XS_F) * XS_NS + (s))
+// auxiliary cell (p.define): XS_NAC chunks after the k-filtered arrays, indexed like XS_ZIDX
+__device__ __forceinline__ cx* xs_abuf(const XsPathArgs& P) {
+  return xs_zbuf(P) + (size_t)(2 * XS_NKC + XS_NKVC) * XS_G * XS_F * XS_NS;
+}
+// one row of the time-spectrum record: the field, then the auxiliary chunks
+#define XS_SPROW ((size_t)(1 + XS_NAC) * XS_G * XS_F * XS_NS)
 
 #define XS_STRIDE1 1
 #define XS_STRIDE2 (XS_N1)
@@ -514,6 +520,38 @@ __device__ __forceinline__ void xs_knoise(const XsPathArgs& P, cx* T, int mode, 
 #endif
 }
 
+#if XS_NA > 0
+// Auxiliary cell (Simulator/xpath.m:36-45): X = define(A, w, t), or with `avg` the
+// mean of X and define(A, w, t) (the method sits between the two evaluations,
+// with the same noise and the same p.t).
+__device__ void xs_aux(const cx* A, cx* X, const real* W, const cx* Z, double t, const XsPathArgs& P, bool avg) {
+  __syncthreads();
+  for (int i = threadIdx.x; i < XS_G * XS_NS; i += blockDim.x) {
+    const int g = i / XS_NS, s = i % XS_NS;
+    int i1, i2, i3;
+    real x, y, z;
+    xs_site(s, i1, i2, i3, x, y, z);
+    cx a[XS_F], o[XS_NA];
+    real w[XS_NWS];
+    cx zk[XS_NK > 0 ? XS_NK : 1];
+#pragma unroll
+    for (int f = 0; f < XS_F; ++f) a[f] = A[(g * XS_F + f) * XS_NS + s];
+#pragma unroll
+    for (int c = 0; c < XS_NWS; ++c) w[c] = XS_NW > 0 ? W[(g * XS_NWS + c) * XS_NS + s] : (real)0;
+#pragma unroll
+    for (int k = 0; k < XS_NK; ++k) zk[k] = Z[XS_ZIDX(k, g, s)];
+    (void)Z;
+    xs_define(a, w, zk, x, y, z, (real)t, P.params, A, g, s, o);
+#pragma unroll
+    for (int k = 0; k < XS_NA; ++k) {
+      cx& d = X[XS_ZIDX(k, g, s)];
+      d = avg ? (d + o[k]) * (real)0.5 : o[k];
+    }
+  }
+  __syncthreads();
+}
+#endif
+
 // dst = base + h * deriv(src, w, t), pointwise over sites (all components at once).
 // dst = base + h * deriv(src, w, t).  A drift with finite differences
 // (XS_STENCIL) reads neighbours of src, so an in-place update (dst == src)
@@ -728,8 +766,12 @@ __device__ __forceinline__ void xs_noise(real* W, real* Wp, int mode, int draw, 
 // T is the transform scratch, free at output times.
 // phase 0 writes the slots of observables on the field at the output time, phase 1
 // (XS_SPEC) those on its time spectrum; A is then the spectral field of output n.
-__device__ void xs_observe(const cx* A, cx* RED, int n, double t, const XsPathArgs& P, double* wsum, int cta,
-                           int nctas, cx* K, cx* T, int phase) {
+__device__ void xs_observe(const cx* A, const cx* AX, cx* RED, int n, double t, const XsPathArgs& P, double* wsum,
+                           int cta, int nctas, cx* K, cx* T, int phase) {
+  (void)AX;
+#define XS_LOAD_XA(g, s)                                                          \
+  cx xa[XS_NA > 0 ? XS_NA : 1];                                                   \
+  _Pragma("unroll") for (int k = 0; k < XS_NA; ++k) xa[k] = AX[XS_ZIDX(k, (g), (s))];
   double2* out = P.obs + ((size_t)n * nctas + cta) * XS_OBS_STRIDE;
 #if XS_KOBS
   for (int i = threadIdx.x; i < XS_G * XS_F * XS_NS; i += blockDim.x) K[i] = A[i];
@@ -760,7 +802,8 @@ __device__ void xs_observe(const cx* A, cx* RED, int n, double t, const XsPathAr
 #pragma unroll
       for (int f = 0; f < XS_F; ++f) a[f] = A[(g * XS_F + f) * XS_NS + s];
       XS_LOAD_AK(g, s)
-      xs_integrands(a, ak, A, g, s, i1, i2, i3, x, y, z, (real)t, P.params, r);
+      XS_LOAD_XA(g, s)
+      xs_integrands(a, ak, xa, A, g, s, i1, i2, i3, x, y, z, (real)t, P.params, r);
 #pragma unroll
       for (int k = 0; k < XS_NRED; ++k) { acc[2 * k] += (double)r[k].re; acc[2 * k + 1] += (double)r[k].im; }
     }
@@ -793,7 +836,8 @@ __device__ void xs_observe(const cx* A, cx* RED, int n, double t, const XsPathAr
 #pragma unroll
       for (int f = 0; f < XS_F; ++f) a[f] = A[(g * XS_F + f) * XS_NS + s];
       XS_LOAD_AK(g, s)
-      xs_obs_site(a, ak, A, g, s, RED + g * (XS_NRED > 0 ? XS_NRED : 1), x, y, z, i1, i2, i3, (real)t, P.params, o);
+      XS_LOAD_XA(g, s)
+      xs_obs_site(a, ak, xa, A, g, s, RED + g * (XS_NRED > 0 ? XS_NRED : 1), x, y, z, i1, i2, i3, (real)t, P.params, o);
 #pragma unroll
       for (int k = 0; k < XS_NOUT_SITE; ++k) {
         xs_kadd(sr[k], cr[k], (double)o[k].re);
@@ -823,6 +867,7 @@ __device__ void xs_observe(const cx* A, cx* RED, int n, double t, const XsPathAr
   }
 #endif
 #undef XS_LOAD_AK
+#undef XS_LOAD_XA
   __syncthreads();
 }
 
@@ -832,9 +877,14 @@ __device__ void xs_observe(const cx* A, cx* RED, int n, double t, const XsPathAr
 // checked run stores the mean of its two half steps.
 __device__ void xs_spec_store(const cx* A, const XsPathArgs& P, int cta, int n1, bool avg) {
   constexpr int GF = XS_G * XS_F * XS_NS;
-  cx* S = P.aft + ((size_t)cta * (P.nt + P.npoints) + n1) * GF;
+  cx* S = P.aft + ((size_t)cta * (P.nt + P.npoints) + n1) * XS_SPROW;
   __syncthreads();
   for (int i = threadIdx.x; i < GF; i += blockDim.x) S[i] = avg ? (A[i] + S[i]) * (real)0.5 : A[i];
+#if XS_NA > 0
+  const cx* X = xs_abuf(P);
+  for (size_t i = threadIdx.x; i < XS_SPROW - GF; i += blockDim.x)
+    S[GF + i] = avg ? (X[i] + S[GF + i]) * (real)0.5 : X[i];
+#endif
   __syncthreads();
 }
 
@@ -843,11 +893,11 @@ __device__ void xs_spec_store(const cx* A, const XsPathArgs& P, int cta, int n1,
 // one site of one trajectory and forms XS_SPEC_NB frequencies per pass over the record.
 #define XS_SPEC_NB 4
 __device__ void xs_spectrum(const XsPathArgs& P, int cta) {
-  constexpr int GF = XS_G * XS_F * XS_NS;
+  constexpr size_t GF = XS_SPROW;  // field and auxiliary chunks
   const int nt = P.nt, np = P.npoints;
   cx* S = P.aft + (size_t)cta * (nt + np) * GF;
   __syncthreads();
-  for (int i = threadIdx.x; i < GF; i += blockDim.x) {
+  for (size_t i = threadIdx.x; i < GF; i += blockDim.x) {
     for (int n0 = 0; n0 < np; n0 += XS_SPEC_NB) {
       double re[XS_SPEC_NB], im[XS_SPEC_NB];
       int ph[XS_SPEC_NB], dm[XS_SPEC_NB];
@@ -961,6 +1011,18 @@ __device__ void xs_resident_run(const XsPathArgs& P, int cta, int nctas) {
     for (int f = 0; f < XS_F; ++f) A[(g * XS_F + f) * XS_NS + s] = a[f];
   }
   __syncthreads();
+#if XS_NA > 0
+  // initial auxiliary cell (xensemble.m:74-77): p.define on a noise draw of its own (Philox draw
+  // 2^32 - 1), at p.t = origin, or origin - 1 when boundary values were set before it (:67-72)
+  cx* AUX = xs_abuf(P);
+  if (!P.single_step) {
+    xs_noise(W, Wp, 0, -1, g0, P);
+    if (XS_NK > 0) xs_knoise(P, T, 0, -1, g0);
+    xs_aux(A, AUX, W, xs_zbuf(P), P.t0 - ((XS_SETBOUND && XS_ND > 0) ? 1.0 : 0.0), P, false);
+  }
+#else
+  const cx* AUX = nullptr;
+#endif
 
   double t = P.t0;
   if (P.single_step) {
@@ -1007,7 +1069,13 @@ __device__ void xs_resident_run(const XsPathArgs& P, int cta, int nctas) {
           xs_noise(W, Wp, mode, draw, g0, P);
           if (P.nc == 1 || chk == 1) {
             __syncthreads();
+#if XS_NA > 0
+            xs_aux(A, AUX, W, xs_zbuf(P), t, P, false);  // xpath.m:36-38
+#endif
             xs_method(A, B1, B2, B3, T, W, P, t);
+#if XS_NA > 0
+            xs_aux(A, AUX, W, xs_zbuf(P), t, P, true);   // xpath.m:42-44
+#endif
             t += P.dtr;
 #if XS_SPEC
             xs_spec_store(A, P, cta, n * P.steps + step, P.nc == 1 && chk == 1);
@@ -1036,7 +1104,7 @@ __device__ void xs_resident_run(const XsPathArgs& P, int cta, int nctas) {
                 make_double2((double)v.re, (double)v.im);
           }
         }
-        xs_observe(A, RED, n, t, P, wsum, cta, nctas, K, T, 0);
+        xs_observe(A, AUX, RED, n, t, P, wsum, cta, nctas, K, T, 0);
       }
     }
   }
@@ -1060,8 +1128,10 @@ __device__ void xs_resident_run(const XsPathArgs& P, int cta, int nctas) {
 #if XS_SPEC
   if (!P.single_step) {
     xs_spectrum(P, cta);
-    for (int n = 0; n < P.npoints; ++n)
-      xs_observe(P.aft + ((size_t)cta * (P.nt + P.npoints) + P.nt + n) * GF, RED, n, t, P, wsum, cta, nctas, K, T, 1);
+    for (int n = 0; n < P.npoints; ++n) {
+      const cx* row = P.aft + ((size_t)cta * (P.nt + P.npoints) + P.nt + n) * XS_SPROW;
+      xs_observe(row, row + GF, RED, n, t, P, wsum, cta, nctas, K, T, 1);
+    }
   }
 #endif
 }

@@ -146,7 +146,9 @@ __device__ __forceinline__ void xs_xpass_core(const XsStreamArgs& A, int tid, si
   const int r = tid / XS_RX, t = tid % XS_RX;
   cx* buf = tw + XS_RX * XS_RX + r * XS_XLINE;
   const size_t row = cta * XS_XROWS + r;  // over ntraj * NY
-  const int e = (int)(row / XS_NY), y = (int)(row % XS_NY);
+  // XS_XROWS divides NY, so a CTA's rows share one trajectory: taking e from the CTA index lets
+  // the compiler keep the trajectory, its block and the Philox keys warp-uniform
+  const int e = (int)((cta * XS_XROWS) / XS_NY), y = (int)(row % XS_NY);
   const u32 blk = (u32)(A.block0 + e / A.ens1), el = (u32)(e % A.ens1);
   cx v[XS_F][XS_RX];
   cx* base = A.field + ((size_t)e * XS_F) * XS_NS + (size_t)y * XS_NX + t;
@@ -550,13 +552,13 @@ extern "C" __global__ void __launch_bounds__(XS_OROWS * XS_RX) xs_x_obs(const Xs
       for (int f = 0; f < XS_F; ++f) a[f] = v[f][j];
 #if XS_NRED > 0
       cx rr[XS_NRED];
-      xs_integrands(a, a, (const cx*)nullptr, 0, 0, t + XS_RX * j, y, 0, x, yy, (real)0, tt, A.params, rr);
+      xs_integrands(a, a, (const cx*)nullptr, (const cx*)nullptr, 0, 0, t + XS_RX * j, y, 0, x, yy, (real)0, tt, A.params, rr);
 #pragma unroll
       for (int k = 0; k < XS_NRED; ++k) { acc[2 * k] += (double)rr[k].re; acc[2 * k + 1] += (double)rr[k].im; }
 #endif
 #if XS_NOUT_SITE > 0
       cx o[XS_NOUT_SITE];
-      xs_obs_site(a, a, (const cx*)nullptr, 0, 0, (const cx*)nullptr, x, yy, (real)0, t + XS_RX * j, y, 0, tt, A.params, o);
+      xs_obs_site(a, a, (const cx*)nullptr, (const cx*)nullptr, 0, 0, (const cx*)nullptr, x, yy, (real)0, t + XS_RX * j, y, 0, tt, A.params, o);
 #pragma unroll
       for (int k = 0; k < XS_NOUT_SITE; ++k) {
         xs_kadd(sr[k][j], cr[k][j], (double)o[k].re);

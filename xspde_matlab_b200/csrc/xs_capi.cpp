@@ -244,6 +244,8 @@ struct Problem {
   bool bvals = false;                      // boundary values of p.boundfun supplied per pass
   bool spec = false;                       // some observable is evaluated on the time spectrum
   int NK = 0, NKV = 0;                     // k-filtered noises / initial randoms (xnoise.m:39-50, xrandom.m:24-29)
+  int NA = 0;                              // auxiliary cell components (p.auxfields, p.define)
+  std::string define;
   std::vector<double> kfilt, rfilt;        // [NK][NS] / [NKV][NS] complex filter factors (empty: identity)
   std::vector<double> runtime_defaults;
   std::vector<int> bnd;  // [D][F][2]
@@ -357,6 +359,13 @@ void setup_problem(const xs_problem* in, Problem& P) {
     if (p.rfilter && P.NKV) P.rfilt.assign(p.rfilter, p.rfilter + (size_t)2 * P.NKV * P.NS);
   }
   P.p.nfilter = P.p.rfilter = nullptr;
+  if (p.auxfields < 0 || p.auxfields > 16) raise(XS_ERR_SHAPE, "auxfields must be 0..16");
+  P.NA = p.auxfields;
+  if (P.NA) {
+    if (!p.define || !*p.define) raise(XS_ERR_ARG, "auxfields given without p.define");
+    P.define = p.define;
+  }
+  P.p.define = nullptr;
   if (p.boundary_values) {
     if (P.bnd.empty()) raise(XS_ERR_ARG, "boundary values given but every boundary is periodic");
     if (p.method != XS_METHOD_MP) raise(XS_ERR_UNSUPPORTED, "boundary values (p.boundfun) are supported with MP");
@@ -384,6 +393,7 @@ void setup_problem(const xs_problem* in, Problem& P) {
     for (int d = 0; d < 3; ++d) P.ktr[d] = k[d];
     P.kobs = true;
   }
+  if (P.kobs && P.NA) raise(XS_ERR_UNSUPPORTED, "k-space observables with auxiliary fields are not supported on the device");
   // grid constants (Simulator/xpreferences.m:133-175, spdpreferences.m:190-244)
   for (int d = 0; d < p.dimensions; ++d) {
     int n = p.points[d];
@@ -542,6 +552,7 @@ xs::GenCtx make_ctx(const Problem& P, std::vector<xs::Role> roles, bool reduce) 
   c.nrand = P.NV;
   c.nknoise = P.NK;
   c.nkrand = P.NKV;
+  c.naux = P.NA;
   c.ndim = P.D;
   c.allow_reduce = reduce;
   c.kgrid = reduce;  // observe functions may read p.kx/ky/kz
@@ -584,6 +595,30 @@ void generate_functions(Problem& P, std::ostringstream& os) {
     }
     os << "}\n";
   }
+  // define(a, w, p): the auxiliary cell (xpath.m:36-45, xensemble.m:74-77), noise cells as for deriv
+  {
+    os << "#define XS_NA " << P.NA << "\n#define XS_NAC " << (P.NA + P.F - 1) / P.F << "\n";
+    os << "__device__ __forceinline__ void xs_define(const cx* __restrict__ a, const real* __restrict__ w, const cx* __restrict__ zk, real x, real y, real z, real t, const double* __restrict__ prm, const cx* __restrict__ fld, int g, int s, cx* __restrict__ out) {\n";
+    os << "  (void)a; (void)w; (void)zk; (void)x; (void)y; (void)z; (void)t; (void)prm; (void)fld; (void)g; (void)s; (void)out;\n";
+    if (P.NA) {
+      auto fn = xs::parse_anon(P.define);
+      std::vector<Role> roles = {Role::Field};
+      if (P.NW > 0 || P.NK == 0) roles.push_back(Role::Noise);
+      if (P.NK > 0) roles.push_back(Role::KNoise);
+      roles.push_back(Role::Params);
+      auto g = xs::generate(fn, make_ctx(P, roles, false));
+      if (g.len != P.NA && g.len != 1)
+        raise(XS_ERR_SHAPE, "p.define returns " + std::to_string(g.len) + " components, auxfields = " + std::to_string(P.NA));
+      if (g.stencil) raise(XS_ERR_UNSUPPORTED, "D1/D2 in p.define are not supported on the device");
+      if (g.len == 1 && P.NA > 1) {
+        os << "  cx o1[1];\n  { cx* out = o1;\n" << g.code << "  }\n";
+        os << "  for (int f = 0; f < " << P.NA << "; ++f) out[f] = o1[0];\n";
+      } else {
+        os << g.code;
+      }
+    }
+    os << "}\n";
+  }
   // initial(v, p) (xensemble.m:60)
   {
     auto fn = xs::parse_anon(P.initial);
@@ -613,7 +648,9 @@ void generate_functions(Problem& P, std::ostringstream& os) {
     o.kspace = oi < P.obs_tr.size() && (P.obs_tr[oi][1] || P.obs_tr[oi][2] || P.obs_tr[oi][3]);
     o.tspec = oi < P.obs_tr.size() && P.obs_tr[oi][0];
     auto fn = xs::parse_anon(txt);
-    o.gen = xs::generate(fn, make_ctx(P, {Role::Field, Role::Params}, true));
+    // observe{n}(a{:}, p): the field, then the auxiliary cell when there is one (xdata.m:29)
+    o.gen = xs::generate(fn, make_ctx(P, P.NA ? std::vector<Role>{Role::Field, Role::Aux, Role::Params}
+                                              : std::vector<Role>{Role::Field, Role::Params}, true));
     o.lines = o.gen.len;
     o.spatial = o.gen.spatial;  // depends on the field or the site (0-D: one site)
     if (o.gen.stencil) P.stencil = true;
@@ -717,8 +754,8 @@ __device__ __forceinline__ cx xs_fd2(const cx* __restrict__ fld, int g, int s, i
 }
 )";
   // integrands with bounds masks and weights
-  os << "__device__ __forceinline__ void xs_integrands(const cx* __restrict__ a, const cx* __restrict__ ak, const cx* __restrict__ fld, int g, int s, int i1, int i2, int i3, real x, real y, real z, real t, const double* __restrict__ prm, cx* __restrict__ rr) {\n";
-  os << "  (void)a; (void)ak; (void)fld; (void)g; (void)s; (void)i1; (void)i2; (void)i3; (void)x; (void)y; (void)z; (void)t; (void)rr; (void)prm;\n";
+  os << "__device__ __forceinline__ void xs_integrands(const cx* __restrict__ a, const cx* __restrict__ ak, const cx* __restrict__ xa, const cx* __restrict__ fld, int g, int s, int i1, int i2, int i3, real x, real y, real z, real t, const double* __restrict__ prm, cx* __restrict__ rr) {\n";
+  os << "  (void)a; (void)ak; (void)xa; (void)fld; (void)g; (void)s; (void)i1; (void)i2; (void)i3; (void)x; (void)y; (void)z; (void)t; (void)rr; (void)prm;\n";
   int off = 0;
   for (auto& o : P.obs) {
     for (auto& r : o.gen.reductions) {
@@ -749,8 +786,8 @@ __device__ __forceinline__ cx xs_fd2(const cx* __restrict__ fld, int g, int s, i
     }
   }
   os << "}\n";
-  os << "__device__ __forceinline__ void xs_obs_site(const cx* __restrict__ a, const cx* __restrict__ ak, const cx* __restrict__ fld, int g, int s, const cx* __restrict__ redall, real x, real y, real z, int i1, int i2, int i3, real t, const double* __restrict__ prm, cx* __restrict__ outall) {\n";
-  os << "  (void)a; (void)ak; (void)fld; (void)g; (void)s; (void)redall; (void)x; (void)y; (void)z; (void)i1; (void)i2; (void)i3; (void)t; (void)outall; (void)prm;\n";
+  os << "__device__ __forceinline__ void xs_obs_site(const cx* __restrict__ a, const cx* __restrict__ ak, const cx* __restrict__ xa, const cx* __restrict__ fld, int g, int s, const cx* __restrict__ redall, real x, real y, real z, int i1, int i2, int i3, real t, const double* __restrict__ prm, cx* __restrict__ outall) {\n";
+  os << "  (void)a; (void)ak; (void)xa; (void)fld; (void)g; (void)s; (void)redall; (void)x; (void)y; (void)z; (void)i1; (void)i2; (void)i3; (void)t; (void)outall; (void)prm;\n";
   for (auto& o : P.obs)
     if (o.spatial)
       os << "  {\n    const cx* red = redall + " << o.red_off << "; (void)red;\n    cx* out = outall + " << o.out_off
@@ -758,6 +795,7 @@ __device__ __forceinline__ cx xs_fd2(const cx* __restrict__ fld, int g, int s, i
   os << "}\n";
   os << "__device__ __forceinline__ void xs_obs_scalar(const cx* __restrict__ redall, real t, const double* __restrict__ prm, cx* __restrict__ outall) {\n";
   os << "  (void)redall; (void)t; (void)outall; (void)prm; const cx* a = nullptr; const real x = 0, y = 0, z = 0; (void)a; (void)x; (void)y; (void)z;\n";
+  os << "  const cx* xa = nullptr; (void)xa;\n";
   os << "  const int i1 = 0, i2 = 0, i3 = 0; (void)i1; (void)i2; (void)i3;\n";
   os << "  const cx* fld = nullptr; const int g = 0, s = 0; (void)fld; (void)g; (void)s;\n";
   for (auto& o : P.obs)
@@ -956,8 +994,11 @@ void tile_plan(const Problem& P, bool fp64, int tl[3], int lsp[3], size_t& elems
 }
 
 // Field-sized complex arrays of the k-filtered noise: the current and the
-// first coarse draw (ceil(NK/F) chunks each), then the k-filtered randoms.
-int knarr(const Problem& P) { return 2 * ((P.NK + P.F - 1) / P.F) + (P.NKV + P.F - 1) / P.F; }
+// first coarse draw (ceil(NK/F) chunks each), then the k-filtered randoms, then
+// the auxiliary cell (ceil(NA/F) chunks).
+int knarr(const Problem& P) {
+  return 2 * ((P.NK + P.F - 1) / P.F) + (P.NKV + P.F - 1) / P.F + (P.NA + P.F - 1) / P.F;
+}
 
 bool fft_dim(const Problem& P, int d);
 
@@ -976,7 +1017,7 @@ size_t msm_reals(const Problem& P) {
 
 // MP with its midpoint iterations fused per site (noise in registers); not
 // possible when the drift reads neighbouring sites.
-bool lean_mp(const Problem& P) { return P.p.method == XS_METHOD_MP && !P.dstencil; }
+bool lean_mp(const Problem& P) { return P.p.method == XS_METHOD_MP && !P.dstencil && P.NA == 0; }
 
 size_t resident_smem(const xs_handle& h, int G, int narr) {
   const Problem& P = h.P;
@@ -1143,6 +1184,7 @@ std::string stream_blocker(const Problem& P) {
   if (P.kobs) return "k-space observables (p.transforms) are not streamed";
   if (P.spec) return "time-spectrum observables (p.transforms{n}(1)) are not streamed";
   if (P.NK || P.NKV) return "k-filtered noises are not streamed";
+  if (P.NA) return "auxiliary fields (p.define) are not streamed";
   if (P.stencil) return "observables with D1/D2 finite differences are not streamed";
   if (P.dstencil) return "drifts with D1/D2 finite differences are not streamed";
   return "";
@@ -1581,7 +1623,8 @@ void spectrum_buffers(xs_handle& h, int nctas, PathArgsHost& a) {
   const int P1 = P.p.points[0];
   const int nt = P1 * P.p.steps;
   const size_t rows = (size_t)nt + P1;
-  const size_t bytes = (size_t)nctas * rows * h.rp.G * P.F * P.NS * (h.fp64 ? 16 : 8);
+  const size_t chunks = 1 + (size_t)(P.NA + P.F - 1) / P.F;  // field, then the auxiliary cell
+  const size_t bytes = (size_t)nctas * rows * chunks * h.rp.G * P.F * P.NS * (h.fp64 ? 16 : 8);
   size_t free_b = 0, total_b = 0;
   CUDA_CHECK(cudaMemGetInfo(&free_b, &total_b));
   if (bytes > free_b + h.d_aft.bytes)
@@ -2264,6 +2307,7 @@ XS_API xs_status xs_run_path_device_noalloc(xs_handle* h, int first_block, int n
     if (h->P.bvals) raise(XS_ERR_UNSUPPORTED, "xs_run_path_device_noalloc does not take boundary values");
     if (h->P.spec) raise(XS_ERR_UNSUPPORTED, "xs_run_path_device_noalloc does not record time spectra");
     if (h->P.NK || h->P.NKV) raise(XS_ERR_UNSUPPORTED, "xs_run_path_device_noalloc does not take k-filtered noises");
+    if (h->P.NA) raise(XS_ERR_UNSUPPORTED, "xs_run_path_device_noalloc does not take auxiliary fields");
     if (nc == 2 && !P.p.checks) raise(XS_ERR_ARG, "coarse pass requested without checks");
     const int slot = nc == 2 ? 1 : 0;
     if (!h->loaded || !h->d_prop[slot].p || (P.has_linear && h->prop_dtr[slot] != pass_dtr(P, nc)))
@@ -2510,6 +2554,7 @@ XS_API xs_status xs_step(xs_handle* h, double* a_inout, const double* w, double 
     if (h->kind != 1) raise(XS_ERR_UNSUPPORTED, "xs_step covers problems on the resident path only");
     if (h->P.bvals) raise(XS_ERR_UNSUPPORTED, "xs_step does not take boundary values");
     if (h->P.NK || h->P.NKV) raise(XS_ERR_UNSUPPORTED, "xs_step does not take k-filtered noises");
+    if (h->P.NA) raise(XS_ERR_UNSUPPORTED, "xs_step does not take auxiliary fields");
     load_module(*h);
     const Problem& P = h->P;
     const size_t ntraj = (size_t)P.E1;
@@ -3137,6 +3182,7 @@ XS_API xs_status xs_batch_create(const xs_problem* items, int nitems, xs_batch**
         if (items[i].boundary_values) raise(XS_ERR_UNSUPPORTED, "batch items take no boundary values");
         if (h.P.spec) raise(XS_ERR_UNSUPPORTED, "batch items take no time-spectrum observables");
         if (h.P.NK || h.P.NKV) raise(XS_ERR_UNSUPPORTED, "batch items take no k-filtered noises");
+        if (h.P.NA) raise(XS_ERR_UNSUPPORTED, "batch items take no auxiliary fields");
         if (items[i].ensembles[1] != 1 || items[i].ensembles[2] != 1)
           raise(XS_ERR_UNSUPPORTED, "a batch item is one ensemble block (ensembles(2) = ensembles(3) = 1)");
         h.force_G = 1;

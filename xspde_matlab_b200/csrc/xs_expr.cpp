@@ -550,7 +550,7 @@ struct Gen {
   int ntmp = 0;
   std::map<std::string, std::string> memo;  // expression text -> temp
   std::vector<Reduction>* reds = nullptr;
-  std::string pname = "p", aname, wname, vname, kname, kvname;
+  std::string pname = "p", aname, wname, vname, kname, kvname, xname;
   std::vector<std::string> aux_names;
   bool in_integrand = false;
   bool stencil = false;  // D1/D2 used: the code reads neighbours through xs_fd1/xs_fd2
@@ -637,6 +637,13 @@ struct Gen {
       r.len = ctx.nnoise;
       r.spatial = true;
       for (int i = 0; i < ctx.nnoise; ++i) r.c.push_back("w[" + std::to_string(i) + "]");
+      return r;
+    }
+    if (name == xname && !xname.empty()) {  // auxiliary cell (p.define, xpath.m:36-45): complex
+      r.len = ctx.naux;
+      r.cplx = true;
+      r.spatial = true;
+      for (int i = 0; i < ctx.naux; ++i) r.c.push_back("xa[" + std::to_string(i) + "]");
       return r;
     }
     if (name == kname && !kname.empty()) {  // k-filtered noise cell (xnoise.m:39-50): complex
@@ -993,7 +1000,7 @@ struct Gen {
     // integrand code in its own generator scope
     Gen sub(ctx);
     sub.aname = aname; sub.wname = wname; sub.vname = vname; sub.pname = pname;
-    sub.kname = kname; sub.kvname = kvname;
+    sub.kname = kname; sub.kvname = kvname; sub.xname = xname;
     sub.in_integrand = true;
     Val iv = sub.gen(integrand);
     R.lines = iv.len;
@@ -1020,7 +1027,7 @@ struct Gen {
     if (base->kind == NK::Var) {
       const std::string& f = base->name;
       bool is_arg = f == aname || f == wname || f == vname || (!kname.empty() && f == kname) ||
-                    (!kvname.empty() && f == kvname);
+                    (!kvname.empty() && f == kvname) || (!xname.empty() && f == xname);
       if (!is_arg) {
         if (f == "Int") return reduction(n, false);
         if (f == "Ave") return reduction(n, true);
@@ -1152,6 +1159,7 @@ Generated generate(const AnonFn& fn, const GenCtx& ctx) {
       case Role::Random: g.vname = nm; break;
       case Role::KNoise: g.kname = nm; break;
       case Role::KRandom: g.kvname = nm; break;
+      case Role::Aux: g.xname = nm; break;
       case Role::Params: g.pname = nm; break;
       default: break;
     }

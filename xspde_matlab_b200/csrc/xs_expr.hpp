@@ -56,6 +56,7 @@ struct GenCtx {
   int nrand = 0;             // components of v
   int nknoise = 0;           // components of the k-filtered noise (complex, zk[])
   int nkrand = 0;            // components of the k-filtered randoms (complex, vk[])
+  int naux = 0;              // components of the auxiliary cell (complex, xa[]; observe only)
   int ndim = 0;              // space dimensions
   bool allow_reduce = false; // Int/Ave allowed (observe)
   bool kgrid = false;        // p.kx/ky/kz available as site values (observe): xs_kt<d>[i<d>]

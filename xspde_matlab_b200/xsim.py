@@ -87,6 +87,7 @@ def xpreferences(inputs):
             raise _lib.XsError(-9, "space-step checks (checks(2:end)) are not supported")
         p.iterations = int(p.get("iterations", 4))
         p.rawdata = int(p.get("rawdata", 0))  # xpreferences.m:85
+        p.auxfields = int(np.atleast_1d(p.get("auxfields", 0))[0])  # xpreferences.m:46, one auxiliary cell
         # noise and random cells (xpreferences.m:65-76): Gaussian x-space, then k-filtered
         nz, kz = p.get("noises", None), p.get("knoises", None)
         p.knoises = int(np.atleast_1d(kz)[0]) if kz is not None else 0
@@ -241,6 +242,9 @@ def make_problem(p, path_kind=0, runtime_params=False):
     pr.deriv = (p.get("deriv") or "@(a,w,p) 0*a").encode()
     pr.initial = (p.get("initial") or "@(v,p) 0").encode()
     pr.linear = (p.get("linear") or "").encode()
+    pr.auxfields = p.auxfields
+    if p.auxfields:
+        pr.define = (p.get("define") or "").encode()
     obs = (ctypes.c_char_p * len(p.observe))(*[o.encode() for o in p.observe])
     keep.append(obs)
     pr.nobserve = len(p.observe)
