@@ -333,6 +333,22 @@ __device__ void xs_tr_tiled(cx* X, const XsPathArgs& P, int dir) {
             __syncthreads();
           }
         }
+        // mirror-symmetric matrices (M[N-1-n][k] = (-1)^(k+p) M[n][k], XS_FOLD = 1 + p, checked on
+        // the host): fold each line into u_n = x_n + x_{N-1-n} (kept at n) and v_n = x_n - x_{N-1-n}
+        // (kept at N-1-n); outputs with k + p even sum u, the others v, over n < N/2
+        constexpr int FOLDP = D == 1 ? XS_FOLD1 : (D == 2 ? XS_FOLD2 : XS_FOLD3);
+        constexpr bool FOLD = MSH && KB == 4 && FOLDP > 0;
+        constexpr int PAR = FOLDP > 1 ? 1 : 0;
+        constexpr int NN = FOLD ? ND / 2 : ND;
+        if constexpr (FOLD) {
+          for (int i = threadIdx.x; i < (ND / 2) * TL; i += blockDim.x) {
+            const int n = i / TL, l = i % TL;
+            const cx a = S[n * LSP + l], b = S[(ND - 1 - n) * LSP + l];
+            S[n * LSP + l] = a + b;
+            S[(ND - 1 - n) * LSP + l] = a - b;
+          }
+          __syncthreads();
+        }
         for (int i = threadIdx.x; i < (ND / KB) * (TL / LB); i += blockDim.x) {
           const int l0 = (i % (TL / LB)) * LB, k0 = (i / (TL / LB)) * KB;
           real ar[KB][LB], ai[KB][LB];
@@ -341,10 +357,12 @@ __device__ void xs_tr_tiled(cx* X, const XsPathArgs& P, int dir) {
 #pragma unroll
             for (int j = 0; j < LB; ++j) ar[q][j] = ai[q][j] = 0;
 #pragma unroll 4
-          for (int n = 0; n < ND; ++n) {
-            cx v[LB], m[KB];
+          for (int n = 0; n < NN; ++n) {
+            cx v[LB], m[KB], vd[LB];
 #pragma unroll
             for (int j = 0; j < LB; ++j) v[j] = S[n * LSP + l0 + j];
+#pragma unroll
+            for (int j = 0; j < LB; ++j) vd[j] = FOLD ? S[(ND - 1 - n) * LSP + l0 + j] : v[j];
             if constexpr (MSH && KB == 4 && sizeof(real) == 4) {
               const float4 q4 = *reinterpret_cast<const float4*>(Ms + n * ND + k0);
               m[0] = mkcx((real)q4.x, (real)0);
@@ -362,8 +380,9 @@ __device__ void xs_tr_tiled(cx* X, const XsPathArgs& P, int dir) {
             for (int q = 0; q < KB; ++q)
 #pragma unroll
               for (int j = 0; j < LB; ++j) {
-                ar[q][j] += m[q].re * v[j].re;
-                ai[q][j] += m[q].re * v[j].im;
+                const cx x = (FOLD && ((q + PAR) & 1)) ? vd[j] : v[j];  // k0 is a multiple of 4
+                ar[q][j] += m[q].re * x.re;
+                ai[q][j] += m[q].re * x.im;
                 if (!RM) {
                   ar[q][j] -= m[q].im * v[j].im;
                   ai[q][j] += m[q].im * v[j].re;

@@ -1341,6 +1341,30 @@ void build_source(xs_handle& h) {
       bool real_m = d < P.D;
       for (int f = 0; f < P.F && real_m; ++f) real_m = P.type(d, f) != 0;
       os << "#define XS_REALM" << d + 1 << " " << (real_m ? 1 : 0) << "\n";
+      // mirror symmetry M[N-1-n][k] = (-1)^(k+p) M[n][k] of every matrix along d, one parity p for
+      // all (DCT-I and DCT-II: p = 0; DST-I on xSPDE's endpoint-inclusive lattice: p = 1; DCT-III
+      // has none): the tiled dense transform folds each line and halves its multiply-adds.
+      // XS_FOLD = 1 + p, or 0.
+      int fold = (real_m && h.rp.gfield && !fft_dim(P, d) && P.N[d] % 4 == 0) ? -1 : 0;
+      for (int f = 0; f < P.F && fold; ++f)
+        for (int dir = 0; dir < 2 && fold; ++dir) {
+          const int n = P.N[d];
+          const auto M = transform_matrix(P.type(d, f), dir == 1, n);
+          double mx = 0;
+          for (const auto& v : M) mx = std::max(mx, std::abs(v));
+          int found = 0;
+          for (int par = 0; par < 2 && !found; ++par) {
+            bool ok = true;
+            for (int i = 0; i < n && ok; ++i)
+              for (int k = 0; k < n && ok; ++k) {
+                const cd a = M[(size_t)(n - 1 - i) * n + k], b = M[(size_t)i * n + k] * ((k + par) % 2 ? -1.0 : 1.0);
+                if (std::abs(a - b) > 1e-12 * mx) ok = false;
+              }
+            if (ok) found = 1 + par;
+          }
+          fold = (found && (fold < 0 || fold == found)) ? found : 0;
+        }
+      os << "#define XS_FOLD" << d + 1 << " " << (fold > 0 ? fold : 0) << "\n";
     }
   }
   os << fns.str();
