@@ -287,6 +287,19 @@ template <int D> __device__ __forceinline__ cx* xs_fft_tile_d(cx* S, cx*, const 
 XS_FFT_TILE_STAGES
 
 #if XS_GFIELD
+// Asynchronous global -> shared copy of one complex element (cp.async, completion by group).
+__device__ __forceinline__ void xs_cp_async(cx* dst, const cx* src) {
+  const u32 d = (u32)__cvta_generic_to_shared(dst);
+  if constexpr (sizeof(cx) == 16)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void xs_cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void xs_cp_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+// The tile after the current one is copied into a third buffer while the current one is
+// transformed, so its loads overlap the transform.
 template <int D>
 __device__ void xs_tr_tiled(cx* X, const XsPathArgs& P, int dir) {
   constexpr int ND = D == 1 ? XS_N1 : (D == 2 ? XS_N2 : XS_N3);
@@ -303,7 +316,8 @@ __device__ void xs_tr_tiled(cx* X, const XsPathArgs& P, int dir) {
     int ms_f = -1;
     cx* S = (cx*)xs_smem + XS_MS_CX;
     cx* S2 = S + XS_TILE_ELEMS;
-    for (int tile = 0; tile < NT; ++tile) {
+    cx* SN = S2 + XS_TILE_ELEMS;  // the next tile, in flight while S is transformed
+    auto fetch = [&](int tile, cx* dst) {
       int hi0, lo0;
       if constexpr (SD == 1) { hi0 = tile * TL; lo0 = 0; }
       else { hi0 = tile / (SD / TL); lo0 = (tile % (SD / TL)) * TL; }
@@ -312,9 +326,18 @@ __device__ void xs_tr_tiled(cx* X, const XsPathArgs& P, int dir) {
         size_t gi;
         if constexpr (SD == 1) { l = i / ND; n = i % ND; gi = (size_t)(hi0 + l) * ND + n; }
         else { n = i / TL; l = i % TL; gi = (size_t)lo0 + l + (size_t)SD * (n + (size_t)ND * hi0); }
-        S[n * LSP + l] = X[gi];
+        xs_cp_async(dst + n * LSP + l, X + gi);
       }
+      xs_cp_commit();
+    };
+    fetch(0, S);
+    for (int tile = 0; tile < NT; ++tile) {
+      int hi0, lo0;
+      if constexpr (SD == 1) { hi0 = tile * TL; lo0 = 0; }
+      else { hi0 = tile / (SD / TL); lo0 = (tile % (SD / TL)) * TL; }
+      xs_cp_wait_all();  // this tile's copies (the only group in flight)
       __syncthreads();
+      if (tile + 1 < NT) fetch(tile + 1, SN);
       cx* Rb;
       if constexpr (fft) {
         Rb = xs_fft_tile_d<D>(S, S2, P.tmat + P.tmat_off[D], dir);
@@ -324,7 +347,8 @@ __device__ void xs_tr_tiled(cx* X, const XsPathArgs& P, int dir) {
         // register block: KB outputs k x LB lines per thread; real matrices
         // (every DST/DCT type) skip the imaginary part of M and are read from
         // a shared-memory copy, KB entries per vector load
-        constexpr int KB = ND % 4 == 0 ? 4 : 1, LB = TL % 2 == 0 ? 2 : 1;
+        constexpr int KB = ND % 4 == 0 ? 4 : 1;
+        constexpr int LB = (TL % 2 == 0 && (ND / KB) * (TL / 2) >= XS_THREADS) ? 2 : 1;  // every thread busy
         constexpr bool MSH = RM && (size_t)ND * ND <= (size_t)XS_MSM;
         if constexpr (MSH) {
           if (f != ms_f) {  // tiles of one component share its matrix (uniform branch)
@@ -405,6 +429,9 @@ __device__ void xs_tr_tiled(cx* X, const XsPathArgs& P, int dir) {
         X[gi] = Rb[n * LSP + l];
       }
       __syncthreads();
+      cx* const cur = S;
+      S = SN;
+      SN = cur;
     }
   }
 }
@@ -953,7 +980,7 @@ __device__ void xs_spectrum(const XsPathArgs& P, int cta) {
 // not match the layout; the CTA must then return without touching it.
 __device__ __forceinline__ bool xs_layout_ok(int* status) {
   constexpr size_t GF = (size_t)XS_G * XS_F * XS_NS;
-  constexpr size_t need = ((XS_GFIELD ? 0 : XS_NARR + XS_KARR + XS_KNARR) * GF + 2 * (size_t)XS_TILE_ELEMS + (XS_GFIELD ? XS_MS_CX : 0)) * sizeof(cx) + (size_t)XS_G * (XS_NRED > 0 ? XS_NRED : 1) * sizeof(cx) +
+  constexpr size_t need = ((XS_GFIELD ? 0 : XS_NARR + XS_KARR + XS_KNARR) * GF + 3 * (size_t)XS_TILE_ELEMS + (XS_GFIELD ? XS_MS_CX : 0)) * sizeof(cx) + (size_t)XS_G * (XS_NRED > 0 ? XS_NRED : 1) * sizeof(cx) +
                           32 * 2 * (XS_NRED > 0 ? XS_NRED : 1) * sizeof(double) +
                           (XS_GFIELD ? 0 : XS_WARR) * (size_t)XS_G * XS_NWS * XS_NS * sizeof(real);
   u32 dyn;
@@ -971,7 +998,7 @@ __device__ void xs_resident_run(const XsPathArgs& P, int cta, int nctas) {
   constexpr int GF = XS_G * XS_F * XS_NS;
 #if XS_GFIELD
   cx* A = P.gfield + (size_t)blockIdx.x * XS_GSLICE;
-  cx* RED = (cx*)xs_smem + XS_MS_CX + 2 * XS_TILE_ELEMS;  // after the matrix copy and the two tiles; [G][NRED]
+  cx* RED = (cx*)xs_smem + XS_MS_CX + 3 * XS_TILE_ELEMS;  // after the matrix copy and the three tiles; [G][NRED]
 #else
   cx* A = (cx*)xs_smem;
   cx* RED = A + (XS_NARR + XS_KARR + XS_KNARR) * GF;  // [G][NRED]

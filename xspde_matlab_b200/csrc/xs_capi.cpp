@@ -966,11 +966,11 @@ struct xs_handle {
 namespace {
 
 // Tiles of the line transforms when the field lives in device memory: lines
-// per tile TL (a divisor of the line count that keeps both tile buffers within
-// ~96 KB) and padded row stride LSP, per space dimension; elems = the larger
-// tile buffer in complex elements.
+// per tile TL (a divisor of the line count that keeps the three tile buffers -
+// current, scratch, next in flight - within ~64 KB) and padded row stride LSP,
+// per space dimension; elems = the larger tile buffer in complex elements.
 void tile_plan(const Problem& P, bool fp64, int tl[3], int lsp[3], size_t& elems) {
-  const size_t cxs = fp64 ? 16 : 8, cap = 96 * 1024;
+  const size_t cxs = fp64 ? 16 : 8, cap = 64 * 1024;
   elems = 0;
   int sd = 1;
   for (int d = 0; d < 3; ++d) {
@@ -982,7 +982,7 @@ void tile_plan(const Problem& P, bool fp64, int tl[3], int lsp[3], size_t& elems
       for (int t = 1; t <= (sd == 1 ? lines : std::min(lines, 32)); ++t) {
         if (lines % t) continue;
         const int lp = t % 2 ? t : t + 1;
-        if (2 * (size_t)nd * lp * cxs > cap) break;
+        if (3 * (size_t)nd * lp * cxs > cap) break;
         best = t;
       }
       tl[d] = best;
@@ -1035,7 +1035,7 @@ size_t resident_smem(const xs_handle& h, int G, int narr) {
     tile_plan(P, h.fp64, tl, lsp, tiles);
     ms_bytes = (msm_reals(P) * rs + 15) / 16 * 16;
   }
-  return (size_t)narr * G * P.F * P.NS * cxs + 2 * tiles * cxs + ms_bytes + (size_t)G * nred * cxs + 32 * 2 * nred * 8 +
+  return (size_t)narr * G * P.F * P.NS * cxs + 3 * tiles * cxs + ms_bytes + (size_t)G * nred * cxs + 32 * 2 * nred * 8 +
          warr * (size_t)G * nws * P.NS * rs;
 }
 
