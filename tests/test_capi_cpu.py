@@ -92,3 +92,14 @@ def test_knoise_rejections(tmp_path, monkeypatch):
     assert rc == 0, _lib.last_error()
     p.knoises = 40
     assert _lib.lib().xs_compile_check(ctypes.byref(p), None, 0) == -1
+
+
+def test_absent_noise_and_random_arguments_are_zero(tmp_path, monkeypatch):
+    """Without noise or random cells the reference passes the scalar 0 for w and v
+    (xnoise.m and xrandom.m start from w{1} = 0), so '0*w' and '1 + v' compile."""
+    monkeypatch.setenv("XSPDE_B200_CACHE", str(tmp_path))
+    p, keep = _problem(deriv="@(a,w,p) -a + 0.1*w", initial="@(v,p) 1 + v", noises=0, inrandoms=0)
+    rc = _lib.lib().xs_compile_check(ctypes.byref(p), None, 0)
+    assert rc == 0, _lib.last_error()
+    p, keep = _problem(deriv="@(a,w,p) -a + w(2,:)", noises=0)
+    assert _lib.lib().xs_compile_check(ctypes.byref(p), None, 0) == -2

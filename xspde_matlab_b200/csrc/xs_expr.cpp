@@ -633,7 +633,10 @@ struct Gen {
       return r;
     }
     if (name == wname && !wname.empty()) {
-      if (ctx.nnoise <= 0) throw GrammarError("noise '" + name + "' used but there are no noises");
+      if (ctx.nnoise <= 0) {  // no noise cell: the argument is the scalar 0 (xnoise.m:27, w{1} = 0)
+        r.c = {"(real)0"};
+        return r;
+      }
       r.len = ctx.nnoise;
       r.spatial = true;
       for (int i = 0; i < ctx.nnoise; ++i) r.c.push_back("w[" + std::to_string(i) + "]");
@@ -661,7 +664,10 @@ struct Gen {
       return r;
     }
     if (name == vname && !vname.empty()) {
-      if (ctx.nrand <= 0) throw GrammarError("random input '" + name + "' used but there are no inrandoms");
+      if (ctx.nrand <= 0) {  // no random cell: the argument is the scalar 0 (xrandom.m, w{1} = 0)
+        r.c = {"(real)0"};
+        return r;
+      }
       r.len = ctx.nrand;
       r.spatial = true;
       for (int i = 0; i < ctx.nrand; ++i) r.c.push_back("v[" + std::to_string(i) + "]");
