@@ -103,3 +103,15 @@ def test_absent_noise_and_random_arguments_are_zero(tmp_path, monkeypatch):
     assert rc == 0, _lib.last_error()
     p, keep = _problem(deriv="@(a,w,p) -a + w(2,:)", noises=0)
     assert _lib.lib().xs_compile_check(ctypes.byref(p), None, 0) == -2
+
+
+def test_zeros_with_literal_sizes(tmp_path, monkeypatch):
+    """zeros(n,1,1) / ones(n,1) give n components (Examples/SPDE_2D/Peregrine.m broadcasts its
+    initial value to four components this way); other shapes are refused."""
+    monkeypatch.setenv("XSPDE_B200_CACHE", str(tmp_path))
+    p, keep = _problem(fields=4, noises=0, initial="@(v,p) exp(-p.x.^2) + zeros(4,1,1)", deriv="@(a,w,p) -a + ones(4,1)",
+                       observe=("@(a,p) a(4,:)",), linear="")
+    rc = _lib.lib().xs_compile_check(ctypes.byref(p), None, 0)
+    assert rc == 0, _lib.last_error()
+    p, keep = _problem(initial="@(v,p) zeros(2,3)")
+    assert _lib.lib().xs_compile_check(ctypes.byref(p), None, 0) == -2

@@ -1049,6 +1049,24 @@ struct Gen {
           for (int i = 0; i < s.len; ++i) r.c.push_back(f == "zeros" ? "(real)0" : "(real)1");
           return r;
         }
+        if ((f == "zeros" || f == "ones") && n->kids.size() >= 2) {
+          // zeros(n, 1, ...) / ones(n, 1, ...) with literal sizes: n components, broadcast over the
+          // lattice and the ensemble (the other sizes must be 1)
+          std::vector<int> sz;
+          for (size_t i = 1; i < n->kids.size(); ++i) {
+            Vec d;
+            if (!try_const(n->kids[i], d) || d.size() != 1 || d[0].imag() != 0 || d[0].real() < 1 ||
+                d[0].real() != std::floor(d[0].real()) || d[0].real() > 64)
+              throw GrammarError(f + " takes size(x) or literal sizes (n, 1, ...)");
+            sz.push_back((int)d[0].real());
+          }
+          for (size_t i = 1; i < sz.size(); ++i)
+            if (sz[i] != 1) throw GrammarError(f + "(n, m, ...) with m > 1 is not supported on the device");
+          Val r;
+          r.len = sz[0];
+          for (int i = 0; i < sz[0]; ++i) r.c.push_back(f == "zeros" ? "(real)0" : "(real)1");
+          return r;
+        }
         if (f == "sum" && (n->kids.size() == 2 || n->kids.size() == 3)) {
           Val v = gen(n->kids[1]);
           if (n->kids.size() == 3) {
