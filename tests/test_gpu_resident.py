@@ -435,3 +435,29 @@ def test_auxiliary_field_on_a_lattice_fp64():
              define=lambda a, w, p: a * np.conj(a) + w[0:1],
              observe=[lambda a, x, p: a * np.conj(a), lambda a, x, p: X.Int(np.real(x), p), lambda a, x, p: x])
     _compare(g, o, [0, 1], [1, 2], FP64_TOL)
+
+
+def test_auxiliary_field_on_a_device_memory_lattice_fp64():
+    """An auxiliary cell on a 128 x 128 lattice (field, scratch, auxiliary chunks and
+    the spectrum record in device memory), observed in time and as a spectrum."""
+    base = dict(dimensions=3, points=[4, 128, 128], ranges=[0.3, 20.0, 20.0], steps=2, ensembles=[2, 1, 1],
+                noises=2, auxfields=1, method="MP", checks=1, transforms=[[0, 0, 0], [1, 0, 0]])
+    g = dict(base, deriv="@(a,w,p) 1i*abs(a).^2.*a + 0.02*(w(1,:)+1i*w(2,:))",
+             initial="@(v,p) exp(-(p.x.^2+p.y.^2)/8)", linear="@(p) 0.5i*(p.Dx.^2+p.Dy.^2)",
+             define="@(a,w,p) abs(a).^2 + 0.1*w(2,:)", observe=["@(a,x,p) Int(real(x),p)", "@(a,x,p) abs(x).^2"])
+    o = dict(base, deriv=lambda a, w, p: 1j * abs(a) ** 2 * a + 0.02 * (w[0:1] + 1j * w[1:2]),
+             initial=lambda v, p: np.exp(-(p.x ** 2 + p.y ** 2) / 8),
+             linear=lambda p: 0.5j * (p.Dx ** 2 + p.Dy ** 2), define=lambda a, w, p: abs(a) ** 2 + 0.1 * w[1:2],
+             observe=[lambda a, x, p: X.Int(np.real(x), p), lambda a, x, p: abs(x) ** 2])
+    _compare(g, o, [0], [1, 2], FP64_TOL)
+
+
+def test_noise_argument_without_noise_cells_is_zero_fp64():
+    """With noises = 0 the drift's w is the scalar 0, as xnoise.m passes it."""
+    base = dict(dimensions=2, points=[5, 32], ranges=[0.5, 8.0], steps=2, ensembles=[4, 1, 1], noises=0,
+                inrandoms=0, method="RK4", checks=1)
+    g = dict(base, deriv="@(a,w,p) 1i*abs(a).^2.*a + 3*w", initial="@(v,p) exp(-p.x.^2) + v",
+             linear="@(p) 1i*p.Dx.^2", observe=["@(a,p) abs(a).^2"])
+    o = dict(base, deriv=lambda a, w, p: 1j * abs(a) ** 2 * a + 3 * w, initial=lambda v, p: np.exp(-p.x ** 2) + v,
+             linear=lambda p: 1j * p.Dx ** 2, observe=[lambda a, p: abs(a) ** 2])
+    _compare(g, o, [0], [1, 2], FP64_TOL)
