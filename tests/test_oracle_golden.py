@@ -149,3 +149,38 @@ def test_auxiliary_fields_quantum_known_answer():
             assert np.all(np.abs(mean - 0.5) < 5 * err + 0.02)
         else:
             assert np.all(np.abs(mean[sel] - exact[sel]) < 5 * err[sel] + 1e-3), k
+
+
+def _stat_check(data, o, exact, k=3.0):
+    """Each point of the fine mean within 5 sampling errors + k step errors + 1e-3 of the exact."""
+    d = np.real(data)
+    mean, step, samp = d[:, 0], d[:, 1], d[:, 2]
+    assert np.all(np.abs(mean - exact) < 5 * samp + k * step + 1e-3), (o, np.max(np.abs(mean - exact)))
+
+
+def test_statistical_pins_kubo2_gain_wiener():
+    """The reference examples' comparisons, which hold for any random-number stream:
+    Examples/SDE_1D/Kubo2.m (RK2, <Re a> = exp(-t/2), <|a|^2> = 1), Gain.m (<|a|^2> = 1)
+    and Wiener.m (Euler; <a>, <a^2>, <a^3>, <a^4> = 0, 4 + t, 0, 3 (4 + t)^2)."""
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore", RuntimeWarning)
+        kubo = dict(ensembles=[400, 10], method="RK2", steps=5, initial=lambda w, p: 1 + 0 * w,
+                    deriv=lambda a, w, p: 1j * w * a,
+                    observe=[lambda a, p: np.real(a[0:1]), lambda a, p: a[0:1] * np.conj(a[0:1])])
+        e, d, inp = X.xsim(kubo)
+        t = inp[0].xc[0]
+        _stat_check(d[0][0], "kubo <a>", np.exp(-t / 2))
+        _stat_check(d[0][1], "kubo |a|^2", 1 + 0 * t)
+        gain = dict(ranges=[4.0], noises=2, ensembles=[2000, 1, 10],
+                    initial=lambda w, p: (w[0:1] + 1j * w[1:2]) / np.sqrt(2),
+                    deriv=lambda a, w, p: -a + w[0:1] + 1j * w[1:2], observe=[lambda a, p: a * np.conj(a)])
+        e, d, inp = X.xsim(gain)
+        _stat_check(d[0][0], "gain", 1 + 0 * inp[0].xc[0])
+        wiener = dict(method="Euler", noises=1, ensembles=[250, 4, 10], initial=lambda v, p: 2 * v,
+                      deriv=lambda a, w, p: w, observe=[lambda a, p: np.concatenate([a, a ** 2, a ** 3, a ** 4])])
+        e, d, inp = X.xsim(wiener)
+        t = inp[0].xc[0]
+        m = np.reshape(np.real(d[0][0]), (4, len(t), -1), order="F")
+        for line, exact in enumerate([0 * t, 4 + t, 0 * t, 3 * (4 + t) ** 2]):
+            mean, samp = m[line, :, 0], m[line, :, 2]
+            assert np.all(np.abs(mean - exact) < 5 * samp + 1e-3 * np.max(np.abs(exact) + 1)), line
