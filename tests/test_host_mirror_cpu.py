@@ -1,0 +1,81 @@
+"""The host mirror of xsim/xensemble (xspde_matlab_b200.xsim) on CPU: its block
+loop, moment sums, extrapolation, error columns, comparisons and axis handling
+must reproduce the oracle's xsim when the device path is replaced by one that
+returns the oracle's own block means (the device path itself is checked against
+the same oracle by the GPU parity tests)."""
+import warnings
+
+import numpy as np
+import pytest
+
+from oracle import xspde_ref as X
+from tests.gpu_util import oracle_block_av
+
+
+class OraclePath:
+    """Stands in for GpuPath: p.path of each block from the oracle's xpath."""
+
+    def __init__(self, p, odict):
+        self.p = p
+        self.o = odict
+        q = X.xpreferences([odict])[0]
+        self.shapes = [tuple(s) for s in q.d_av]
+        self.per_block = 2 * sum(int(np.prod(s)) for s in self.shapes)
+
+    def av_shapes(self):
+        return self.shapes
+
+    def run_path(self, first, nblocks, nc, a_in=None, a_out=False, raw=False):
+        av = []
+        for b in range(first, first + nblocks):
+            out = oracle_block_av(self.o, b, nc)
+            av.append([np.asarray(x, dtype=complex).reshape(s, order="F") for x, s in zip(out[0], self.shapes)])
+        return av, None
+
+
+def _run(monkeypatch, g, o):
+    import importlib
+    M = importlib.import_module("xspde_matlab_b200.xsim")  # the module (the package exports a function xsim)
+    monkeypatch.setattr(M, "GpuPath", lambda p, path_kind=0, runtime_params=False: OraclePath(p, o))
+    eg, dg, _ = M.xsim(g)
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore", RuntimeWarning)
+        eo, do, _ = X.xsim(o)
+    return np.asarray(eg), dg, np.asarray(eo), do
+
+
+def _close(eg, dg, eo, do):
+    # 1e-10: the mirror's moment sums are compensated, the oracle's plain (last-digit differences,
+    # amplified by the cancellation in the sampling-error column)
+    keep = [i for i in range(len(eo)) if i != 5]  # error(sx+2) with sx = 3 is the run time
+    assert np.allclose(eg[keep], eo[keep], rtol=1e-10, atol=1e-15), (eg, eo)
+    for a, b in zip(dg[0], do[0]):
+        assert np.allclose(np.asarray(a), np.asarray(b), rtol=1e-10, atol=1e-13)
+
+
+def test_mirror_matches_oracle_stochastic_spde_with_compare(monkeypatch):
+    base = dict(dimensions=2, points=[7, 16], ranges=[1.0, 8.0], steps=2, ensembles=[4, 3, 2], noises=2,
+                method="MP", checks=1, order=1)
+    g = dict(base, deriv="@(a,w,p) 1i*a.*conj(a).*a - 0.1*a + 0.05*(w(1,:)+1i*w(2,:))",
+             initial="@(v,p) exp(-p.x.^2) + 0.01*v(1,:)", linear="@(p) 1i*p.Dx.^2",
+             observe=["@(a,p) a.*conj(a)", "@(a,p) Int(abs(a).^2, p)"],
+             compare=[None, lambda p: np.sqrt(np.pi / 2) * np.exp(-0.2 * p.t)])
+    o = dict(base, deriv=lambda a, w, p: 1j * a * np.conj(a) * a - 0.1 * a + 0.05 * (w[0:1] + 1j * w[1:2]),
+             initial=lambda v, p: np.exp(-p.x ** 2) + 0.01 * v[0:1], linear=lambda p: 1j * p.Dx ** 2,
+             observe=[lambda a, p: a * np.conj(a), lambda a, p: X.Int(abs(a) ** 2, p)],
+             compare=[None, lambda p: np.sqrt(np.pi / 2) * np.exp(-0.2 * p.t)])
+    _close(*_run(monkeypatch, g, o))
+
+
+@pytest.mark.parametrize("order", [0, 2])
+def test_mirror_matches_oracle_kspace_and_spectrum(monkeypatch, order):
+    """k-space axes (centred, p.kc) and a time spectrum (frequency axis), with and
+    without Richardson extrapolation of the check passes."""
+    base = dict(dimensions=2, points=[9, 16], ranges=[2.0, 8.0], steps=2, ensembles=[4, 2, 1], noises=2,
+                method="RK4", checks=1, order=order, transforms=[[0, 1], [1, 0]])
+    g = dict(base, deriv="@(a,w,p) -0.3*a + 0.1*(w(1,:)+1i*w(2,:))", initial="@(v,p) exp(-p.x.^2)",
+             linear="@(p) 0.5i*p.Dx.^2", observe=["@(a,p) abs(a).^2", "@(a,p) abs(a).^2"])
+    o = dict(base, deriv=lambda a, w, p: -0.3 * a + 0.1 * (w[0:1] + 1j * w[1:2]),
+             initial=lambda v, p: np.exp(-p.x ** 2), linear=lambda p: 0.5j * p.Dx ** 2,
+             observe=[lambda a, p: abs(a) ** 2, lambda a, p: abs(a) ** 2])
+    _close(*_run(monkeypatch, g, o))
