@@ -216,7 +216,7 @@ def run_reference(args, rank, world):
     """--impl reference: the CPU restatement of the reference path on all host cores."""
     import multiprocessing as mp
     if rank != 0:
-        print(json.dumps({"impl": "reference", "rank": rank, "skipped": True}), file=sys.stderr)
+        print("reference arm: rank %d has no work (rank 0 times the CPU reference)" % rank, file=sys.stderr)
         return
     cores = os.cpu_count() or 1
     per_step = []
