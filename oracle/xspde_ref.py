@@ -281,8 +281,9 @@ def xpreferences(inputs):
     return out
 
 
-def _xobserve(a, p):
-    """Default observe: all field components as lines (xpreferences.m:427-446)."""
+def _xobserve(a, *rest):
+    """Default observe: all field components as lines (xpreferences.m:427-446); it
+    takes the field and ignores the other cells and p (varargin)."""
     return a
 
 

@@ -79,3 +79,24 @@ def test_mirror_matches_oracle_kspace_and_spectrum(monkeypatch, order):
              initial=lambda v, p: np.exp(-p.x ** 2), linear=lambda p: 0.5j * p.Dx ** 2,
              observe=[lambda a, p: abs(a) ** 2, lambda a, p: abs(a) ** 2])
     _close(*_run(monkeypatch, g, o))
+
+
+@pytest.mark.parametrize("inp", [
+    dict(dimensions=2, points=[7, 16], ranges=[1.0, 8.0], steps=2, noises=2, checks=1),
+    dict(dimensions=3, points=[5, 12, 10], ranges=[0.5, 6.0, 4.0], steps=3, knoises=2, krandoms=1, checks=0),
+    dict(points=[41], ranges=[8.0], auxfields=2, noises=2, transforms=[[1], [0]]),
+    dict(dimensions=2, points=[9, 16], ranges=[2.0, 8.0], transforms=[0, 1], inrandoms=3),
+])
+def test_mirror_preferences_match_oracle(inp):
+    """Derived constants of the host mirror's xpreferences (grids, k axes, noise
+    scales, default noise and random counts, transform flags) equal the oracle's."""
+    from xspde_matlab_b200.xsim import xpreferences as mirror
+    q = mirror([dict(inp)])[0]
+    r = X.xpreferences([dict(inp)])[0]
+    assert q.points == r.points and q.steps[0] == r.steps[0] and q.checks[0] == r.checks[0]
+    assert q.noises == r.noises and q.inrandoms == r.inrandoms
+    assert q.knoises == r.knoises and q.krandoms == r.krandoms and q.auxfields == r.auxfields
+    assert np.isclose(q.dt, r.dt) and np.allclose(q.dx, r.dx) and np.allclose(q.dk, r.dk)
+    for d in range(len(q.kc)):
+        assert np.allclose(q.kc[d], r.kc[d])
+    assert [list(t) for t in q.transforms] == [list(t)[:len(q.transforms[0])] for t in r.transforms]
