@@ -115,3 +115,44 @@ def test_zeros_with_literal_sizes(tmp_path, monkeypatch):
     assert rc == 0, _lib.last_error()
     p, keep = _problem(initial="@(v,p) zeros(2,3)")
     assert _lib.lib().xs_compile_check(ctypes.byref(p), None, 0) == -2
+
+
+# a 64 x 64 periodic lattice, which the streaming path takes unless a feature rules it out
+_LATTICE2D = dict(dimensions=3, points=(5, 64, 64), ranges=(0.5, 10.0, 10.0), ensembles=(8, 2, 1),
+                  linear="@(p) 1i*(p.Dx.^2+p.Dy.^2)")
+
+
+def _flags(vals):
+    arr = (ctypes.c_int * len(vals))(*vals)
+    return arr
+
+
+@pytest.mark.parametrize("setup,code,frag", [
+    (lambda p: setattr(p, "auxfields", 17), -1, "auxfields must be 0..16"),
+    (lambda p: setattr(p, "auxfields", 1), -7, "auxfields given without p.define"),
+    (lambda p: (setattr(p, "knoises", 1), setattr(p, "path_kind", 2)), -9, "k-filtered noises are not streamed"),
+    (lambda p: (setattr(p, "auxfields", 1), setattr(p, "define", b"@(a,w,p) a"), setattr(p, "path_kind", 2)), -9,
+     "auxiliary fields (p.define) are not streamed"),
+    (lambda p: (setattr(p, "auxfields", 2), setattr(p, "define", b"@(a,w,p) [a; a; a]")), -1,
+     "p.define returns 3 components"),
+])
+def test_feature_rejections(setup, code, frag, tmp_path, monkeypatch):
+    """Argument checks and refusals of the auxiliary-field and k-noise options (C ABI errors, no GPU)."""
+    monkeypatch.setenv("XSPDE_B200_CACHE", str(tmp_path))
+    p, keep = _problem(**_LATTICE2D)
+    setup(p)
+    rc = _lib.lib().xs_compile_check(ctypes.byref(p), None, 0)
+    assert rc == code, (rc, _lib.last_error())
+    assert frag in _lib.last_error()
+
+
+def test_time_spectrum_refused_on_streaming_path(tmp_path, monkeypatch):
+    monkeypatch.setenv("XSPDE_B200_CACHE", str(tmp_path))
+    p, keep = _problem(observe=("@(a,p) a.*conj(a)",), **_LATTICE2D)
+    flags = _flags([1, 0, 0, 0])
+    p.transforms = flags
+    p.path_kind = 2
+    rc = _lib.lib().xs_compile_check(ctypes.byref(p), None, 0)
+    assert rc == -9 and "time-spectrum observables" in _lib.last_error()
+    p.path_kind = 1
+    assert _lib.lib().xs_compile_check(ctypes.byref(p), None, 0) == 0, _lib.last_error()
