@@ -100,3 +100,19 @@ def test_mirror_preferences_match_oracle(inp):
     for d in range(len(q.kc)):
         assert np.allclose(q.kc[d], r.kc[d])
     assert [list(t) for t in q.transforms] == [list(t)[:len(q.transforms[0])] for t in r.transforms]
+
+
+def test_mirror_matches_oracle_axes_and_cutoffs(monkeypatch):
+    """Output axis selection (p.axes: all points, the middle point, the last point,
+    explicit indices; Applications/SPDE/xcompress.m) and p.cutoffs."""
+    base = dict(dimensions=3, points=[5, 8, 6], ranges=[0.5, 6.0, 4.0], steps=2, ensembles=[4, 2, 1], noises=2,
+                method="MP", checks=1, order=1, axes=[None, [0, -1, 0], [0, [2, 5], -2]], cutoffs=[0.0, 0.1, 0.0])
+    g = dict(base, deriv="@(a,w,p) -0.2*a + 0.1*w(1,:)", initial="@(v,p) exp(-(p.x.^2+p.y.^2)/4)",
+             linear="@(p) 0.3i*(p.Dx.^2+p.Dy.^2)", observe=["@(a,p) abs(a).^2", "@(a,p) real(a)", "@(a,p) imag(a)"])
+    o = dict(base, deriv=lambda a, w, p: -0.2 * a + 0.1 * w[0:1], initial=lambda v, p: np.exp(-(p.x ** 2 + p.y ** 2) / 4),
+             linear=lambda p: 0.3j * (p.Dx ** 2 + p.Dy ** 2),
+             observe=[lambda a, p: abs(a) ** 2, lambda a, p: np.real(a), lambda a, p: np.imag(a)])
+    eg, dg, eo, do = _run(monkeypatch, g, o)
+    for a, b in zip(dg[0], do[0]):
+        assert np.shape(a) == np.shape(b)
+    _close(eg, dg, eo, do)
