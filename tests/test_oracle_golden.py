@@ -184,3 +184,13 @@ def test_statistical_pins_kubo2_gain_wiener():
         for line, exact in enumerate([0 * t, 4 + t, 0 * t, 3 * (4 + t) ** 2]):
             mean, samp = m[line, :, 0], m[line, :, 2]
             assert np.all(np.abs(mean - exact) < 5 * samp + 1e-3 * np.max(np.abs(exact) + 1)), line
+
+
+def test_philox_k_stream_is_its_own_standard_normal_stream():
+    """k-space draws (bit 15 of the fourth counter word) differ from the x-space draws of the
+    same (site, trajectory, draw, component) and are standard normal."""
+    zx = philox.normals(2, 4096, 64, 5, 3, 7, 0, 1)
+    zk = philox.normals(2, 4096, 64, 5, 3, 7, 0, 1, kstream=True)
+    assert not np.any(np.isclose(zx, zk))
+    assert abs(zk.mean()) < 0.01 and abs(zk.var() - 1) < 0.01
+    assert abs(np.corrcoef(zx.ravel(), zk.ravel())[0, 1]) < 0.01
