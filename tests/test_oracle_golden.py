@@ -191,6 +191,6 @@ def test_philox_k_stream_is_its_own_standard_normal_stream():
     same (site, trajectory, draw, component) and are standard normal."""
     zx = philox.normals(2, 4096, 64, 5, 3, 7, 0, 1)
     zk = philox.normals(2, 4096, 64, 5, 3, 7, 0, 1, kstream=True)
-    assert not np.any(np.isclose(zx, zk))
+    assert np.mean(zx == zk) < 1e-4  # independent streams: equal values only by coincidence
     assert abs(zk.mean()) < 0.01 and abs(zk.var() - 1) < 0.01
     assert abs(np.corrcoef(zx.ravel(), zk.ravel())[0, 1]) < 0.01
