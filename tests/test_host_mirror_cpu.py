@@ -116,3 +116,33 @@ def test_mirror_matches_oracle_axes_and_cutoffs(monkeypatch):
     for a, b in zip(dg[0], do[0]):
         assert np.shape(a) == np.shape(b)
     _close(eg, dg, eo, do)
+
+
+def test_mirror_saves_matlab_file(monkeypatch, tmp_path):
+    """p.file: error, data, input and raw in a MATLAB file (Simulator/xsim.m:206-210)."""
+    import scipy.io
+    base = dict(dimensions=2, points=[5, 8], ranges=[0.5, 4.0], steps=2, ensembles=[4, 2, 1], noises=2,
+                method="MP", checks=1, order=1, file=str(tmp_path / "run.mat"))
+    g = dict(base, deriv="@(a,w,p) -0.2*a + 0.1*w(1,:)", initial="@(v,p) exp(-p.x.^2)",
+             linear="@(p) 0.3i*p.Dx.^2", observe=["@(a,p) abs(a).^2", "@(a,p) Int(abs(a).^2, p)"])
+    o = dict(base, deriv=lambda a, w, p: -0.2 * a + 0.1 * w[0:1], initial=lambda v, p: np.exp(-p.x ** 2),
+             linear=lambda p: 0.3j * p.Dx ** 2, observe=[lambda a, p: abs(a) ** 2, lambda a, p: X.Int(abs(a) ** 2, p)])
+    eg, dg, eo, do = _run(monkeypatch, g, o)
+    m = scipy.io.loadmat(str(tmp_path / "run.mat"))
+    assert np.array_equal(m["error"][0], eg)
+    for n in range(2):
+        assert np.allclose(m["data"][0, 0][0, n], np.asarray(dg[0][n]))
+    inp0 = m["input"][0, 0]
+    assert list(inp0["points"][0, 0][0]) == [5, 8] and inp0["method"][0, 0][0] == "MP"
+
+
+def test_save_mat_raw_cells(tmp_path):
+    """raw{s, nc, k} is saved as a cell array of the trajectories' fields."""
+    import scipy.io
+    from xspde_matlab_b200.xsim import save_mat, xpreferences
+    inp = xpreferences([dict(points=[3], ranges=[1.0], ensembles=[2, 2, 1])])
+    r = [[[np.full((1, 3, 2), k + 10 * nc + 0.5j) for k in range(2)] for nc in range(2)]]
+    save_mat(str(tmp_path / "raw.mat"), np.arange(6.0), [[np.ones((3, 3))]], inp, r)
+    m = scipy.io.loadmat(str(tmp_path / "raw.mat"))
+    assert m["raw"].shape == (1, 2, 2)
+    assert np.allclose(m["raw"][0, 1, 1], 11 + 0.5j)

@@ -631,9 +631,57 @@ def xsim(*inputs, path_kind=0):
     error[sx + 1:sx + 3] = np.sum(er[:, sx + 1:sx + 3], axis=0)
     error[sx + 1] /= 1e-20 + error[sx + 2]
     error[sx + 2] = time.perf_counter() - t0
+    fname = inp[0].get("file", None)
+    if fname and str(fname).strip():
+        save_mat(str(fname), error, data, inp, raw)
     if want_raw:
         return error, data, inp, raw
     return error, data, inp
+
+
+def _cell(items):
+    """A 1 x n MATLAB cell array (object array) of the given values."""
+    c = np.empty((1, len(items)), dtype=object)
+    for i, v in enumerate(items):
+        c[0, i] = v
+    return c
+
+
+# numeric and text input fields kept in the saved input structs (function handles are not)
+_SAVED_FIELDS = ("name", "dimensions", "fields", "noises", "knoises", "inrandoms", "krandoms", "auxfields",
+                 "points", "ranges", "origins", "steps", "checks", "ensembles", "order", "seed", "method",
+                 "iterations", "dt", "dx", "dk", "transforms")
+
+
+def save_mat(fname, error, data, inp, raw=None):
+    """xsim's MATLAB file (Simulator/xsim.m:206-210: save(file, 'error', 'data',
+    'input', 'raw')): error as a row vector, data{s}{n} as nested cells, input{s}
+    as structs of the numeric and text inputs, raw{s, nc, k} when recorded."""
+    import scipy.io
+    structs = []
+    for p in inp:
+        d = {}
+        for k in _SAVED_FIELDS:
+            v = p.get(k, None)
+            if v is None or callable(v):
+                continue
+            if k == "transforms":
+                v = _cell([np.asarray(t, dtype=float) for t in v])
+            elif not isinstance(v, str):
+                v = np.asarray(v, dtype=float)
+            d[k] = v
+        structs.append(d)
+    out = {"error": np.asarray(error, dtype=float)[None, :],
+           "data": _cell([_cell([np.asarray(x) for x in row]) for row in data]),
+           "input": _cell(structs)}
+    if raw is not None:
+        cells = np.empty((len(raw), len(raw[0]), len(raw[0][0])), dtype=object)
+        for s, per_s in enumerate(raw):
+            for nc, per_nc in enumerate(per_s):
+                for k, r in enumerate(per_nc):
+                    cells[s, nc, k] = np.zeros(0) if r is None else np.asarray(r)
+        out["raw"] = cells
+    scipy.io.savemat(fname, out, do_compression=False)
 
 
 def xspde(*inputs, **kw):
