@@ -537,7 +537,7 @@ def run_cv(args):
         "fp32_vs_fp64_traj_max_rel": d32,
         "training": {"pairs": ntrain, "data_seconds": t_data, "fit_seconds": t_fit,
                      "features": "%d coarse space-time noise projections: %s" % (CV_FEATURES, CV_SETS)},
-        "config": {"workload": "gpe_2d 256x256, 509 MP steps; sampling error from %d blocks (xsim.m:144)" % nblk},
+        "config": {"workload": "gpe_2d 256x256, 509 MP steps; sampling error from %d blocks (xsim.m:95)" % nblk},
     }
     print(json.dumps(line))
 

@@ -9,7 +9,7 @@
  *                           (noise, method, observables) runs on the GPU.
  *   xs_step       replaces  p.method(a,w,p)       Applications/SDE/MP.m:1, RK4.m:1,
  *                           Euler.m:1, RK2.m:1, Implicit.m:1, called at
- *                           Simulator/xpath.m:150.
+ *                           Simulator/xpath.m:42.
  *   xs_noise      replaces  p.noisegen(w1,nc,s,p) Simulator/xnoise.m:1 (one draw,
  *                           before the coarse average of xnoise.m:33-35).
  *   xs_random     replaces  p.randomgen(p)        Simulator/xrandom.m:1.
@@ -150,14 +150,14 @@ XS_API size_t xs_av_doubles_per_block(const xs_handle* h);
  *          device (Simulator/xensemble.m:53-64); else [fields, space, ens1*nblocks]
  *          complex FP64 (the `a` that xensemble passes to p.path).
  *   av_out per block, per observable o in order, the block mean av{o}
- *          [lines, points(1), space] complex FP64 (Simulator/xpath.m:189).
+ *          [lines, points(1), space] complex FP64 (Simulator/xpath.m:81).
  *   a_out  NULL or the final field, same layout as a_in.
  * Host pointers; copies are synchronous with respect to the caller. */
 XS_API xs_status xs_run_path(xs_handle* h, int first_block, int nblocks, int nc, const double* a_in,
                              double* av_out, double* a_out);
 
 /* xs_run_path that also returns p.path's third output `raw` when p.rawdata is
- * set (Simulator/xpath.m:72-77, stored at xensemble.m:79 and returned by
+ * set (Simulator/xpath.m:73-78, stored at xensemble.m:79 and returned by
  * xsim.m:1): raw_out is the field at every output time, [fields, points(1),
  * space, ens1*nblocks] complex FP64 (raw{l} of Simulator/xpreferences.m:148 for
  * consecutive blocks).  Resident path only (XS_ERR_UNSUPPORTED on the
@@ -262,7 +262,7 @@ enum {
 };
 
 /* Instrumentation (no counterpart in the reference, which has only tic/toc,
- * Simulator/xsim.m:77): with timing on, every launch of the handle is
+ * Simulator/xsim.m:28): with timing on, every launch of the handle is
  * bracketed by CUDA events on its stream.  xs_kernel_stats synchronises
  * that stream and returns, per kernel kind, the launches and the summed
  * device milliseconds since the last reset (arrays of XS_KERNEL_KINDS). */

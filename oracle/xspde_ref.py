@@ -288,7 +288,7 @@ def _xobserve(a, *rest):
 
 
 def _spdpreferences(p):
-    """k grids and boundary flags (Applications/SPDE/spdpreferences.m:184-247)."""
+    """k grids and boundary flags (Applications/SPDE/spdpreferences.m:1-73)."""
     nd = p.dimensions
     pts = p.points
     bnd = p.get("boundaries", None)
@@ -300,7 +300,7 @@ def _spdpreferences(p):
         bd = np.zeros((p.fields, 2), dtype=int) if bd is None else np.atleast_2d(np.asarray(bd, dtype=int))
         b.append(bd)
     p.boundaries = b
-    p.dkp = [math.pi / ((pts[d] - 1) * p.dx[d]) if pts[d] > 1 else 0.0 for d in range(nd)]  # :190
+    p.dkp = [math.pi / ((pts[d] - 1) * p.dx[d]) if pts[d] > 1 else 0.0 for d in range(nd)]  # :16
     p.points2 = [x // 2 for x in pts]
     p.setboundaries = 0
     p.setboundcell = 0
@@ -310,13 +310,13 @@ def _spdpreferences(p):
     p.boundval = [None] * nd
     zero = np.zeros([p.fields] + list(pts[1:]) + [p.ensembles[0]])
     for d in range(1, nd):
-        p.boundval[d] = _xboundfun(zero, 0, d, p)                     # :214-217
+        p.boundval[d] = _xboundfun(zero, 0, d, p)                     # :40-43
     for d in range(1, nd):
         n = pts[d]
         p0 = np.arange(n)
         p1 = np.arange(1, n)
-        p.xc[d] = p.origins[d] + p0 * p.dx[d]                           # :209
-        p.kc[d] = (p0 - p.points2[d]) * p.dk[d]                         # :210
+        p.xc[d] = p.origins[d] + p0 * p.dx[d]                           # :35
+        p.kc[d] = (p0 - p.points2[d]) * p.dk[d]                         # :36
         if np.any(b[d] != 0):
             p.setboundaries = 1
             p.setboundcell = 1
@@ -340,7 +340,7 @@ def _spdpreferences(p):
 
 
 def _xboundfun(ac, c, d, p):
-    """Default boundary values: zeros (spdpreferences.m:249-270)."""
+    """Default boundary values: zeros (spdpreferences.m:75-96)."""
     sz = list(np.shape(ac))
     s1 = sz[0]
     sz[0] = 1
@@ -356,7 +356,7 @@ def _bshape(nd, d, n):
 
 
 def _xgrid0(p):
-    """Lattice and k-space grids in propagation order (xgrid.m:288-319)."""
+    """Lattice and k-space grids in propagation order (xgrid.m:17-48)."""
     nd = p.dimensions
     pts = p.points
     p.r = [None] * max(4, nd)
@@ -375,7 +375,7 @@ def _xgrid0(p):
 
 
 def xgrid_out(n, p):
-    """Output-grid coordinate arrays for compare functions (xgrid.m:320-327)."""
+    """Output-grid coordinate arrays for compare functions (xgrid.m:49-56)."""
     q = p.copy()
     xk = p.xk[n]
     d = len(xk)
@@ -455,7 +455,7 @@ def xdst1(a, ax):
 
 
 def xdct2(a, ax):
-    """DCT-II on the first N-1 points (xdct2.m:40-69)."""
+    """DCT-II on the first N-1 points (xdct2.m:11-29)."""
     if np.iscomplexobj(a):
         return xdct2(np.real(a), ax) + 1j * xdct2(np.imag(a), ax)
     x = _swap(a, ax)
@@ -472,7 +472,7 @@ def xdct2(a, ax):
 
 
 def xdct3(a, ax):
-    """DCT-III on the first N-1 points (xdct3.m:69-102)."""
+    """DCT-III on the first N-1 points (xdct3.m:13-33)."""
     if np.iscomplexobj(a):
         return xdct3(np.real(a), ax) + 1j * xdct3(np.imag(a), ax)
     x = _swap(a, ax)
@@ -492,7 +492,7 @@ def xdct3(a, ax):
 
 
 def xdst2(a, ax):
-    """DST-II on the last N-1 points (xdst2.m:103-136)."""
+    """DST-II on the last N-1 points (xdst2.m:13-33)."""
     if np.iscomplexobj(a):
         return xdst2(np.real(a), ax) + 1j * xdst2(np.imag(a), ax)
     x = _swap(a, ax)
@@ -511,7 +511,7 @@ def xdst2(a, ax):
 
 
 def xdst3(a, ax):
-    """DST-III on the last N-1 points (xdst3.m:136-171)."""
+    """DST-III on the last N-1 points (xdst3.m:12-35)."""
     if np.iscomplexobj(a):
         return xdst3(np.real(a), ax) + 1j * xdst3(np.imag(a), ax)
     x = _swap(a, ax)
@@ -537,7 +537,7 @@ _INV = {-3: xdct1, -1: xdst2, 1: xdct2, 3: xdst1}
 
 
 def xtransform(a, inv, p):
-    """Per-component spectral transform over every space dimension (xtransform.m:125-175)."""
+    """Per-component spectral transform over every space dimension (xtransform.m:21-70)."""
     nd = p.dimensions
     a = np.array(a, dtype=complex)
     for i in range(a.shape[0]):
@@ -555,7 +555,7 @@ def xtransform(a, inv, p):
 
 
 def xpatch(ac, p):
-    """Boundary patch for non-periodic transforms (xpatch.m:86-125)."""
+    """Boundary patch for non-periodic transforms (xpatch.m:24-62)."""
     a = ac
     pa = 0.0
     lp = 0.0
@@ -619,7 +619,7 @@ def xsetbound(ac, p):
 
 
 def xprop(a, p):
-    """One interaction-picture propagation a <- T^-1[P . T a] (xprop.m:75-105)."""
+    """One interaction-picture propagation a <- T^-1[P . T a] (xprop.m:17-46)."""
     bv = 0
     if not (np.isscalar(p.propagator) and p.propagator == 1):
         pat = 0.0
@@ -672,7 +672,7 @@ def MP(a, xi, p):
 
 
 def RK4(a, xi, p):
-    """Fourth-order Runge-Kutta IP step, one noise for all stages (RK4.m:35-70)."""
+    """Fourth-order Runge-Kutta IP step, one noise for all stages (RK4.m:7-42)."""
     q = p.copy()
     dt = 0.5 * q.dtr
     if q.setboundaries:
@@ -698,14 +698,14 @@ def RK4(a, xi, p):
 
 
 def Euler(a, xi, p):
-    """Euler IP step (Euler.m:77-81)."""
+    """Euler IP step (Euler.m:6-10)."""
     a = a + _deriv(a, xi, p) * p.dtr
     a, _ = p.prop(a, p)
     return a
 
 
 def RK2(ac, xi, p):
-    """Second-order Runge-Kutta IP step (RK2.m:89-107)."""
+    """Second-order Runge-Kutta IP step (RK2.m:7-25)."""
     q = p.copy()
     dt = q.dtr
     a = ac + _deriv(ac, xi, q) * dt
@@ -722,7 +722,7 @@ def RK2(ac, xi, p):
 
 
 def Implicit(a, xi, p):
-    """Implicit (iterated Euler) IP step (Implicit.m:116-125)."""
+    """Implicit (iterated Euler) IP step (Implicit.m:8-17)."""
     q = p.copy()
     dt = q.dtr
     q.t = q.t + dt
@@ -803,7 +803,7 @@ def philox_randomgen(p):
 # ---------------------------------------------------------------------------
 
 def xnft(a, trans, p):
-    """Normalised spatial Fourier transform (xnft.m:183-202)."""
+    """Normalised spatial Fourier transform (xnft.m:23-31)."""
     a = np.array(a, dtype=complex)
     for d in range(1, min(p.dimensions, len(trans))):
         if trans[d] > 0 and a.shape[d] > 1:
@@ -820,7 +820,7 @@ def _transform_obs(a, n, p):
 
 def _observe(a, x, n, p):
     """observe{n}(a{:}, p) on the (transformed) cells: the field, then the
-    auxiliary cell when there is one (xdata.m:24-29)."""
+    auxiliary cell when there is one (xdata.m:25-30)."""
     a = _transform_obs(a, n, p)
     if p.auxfields:
         return np.asarray(p.observe[n](a, _transform_obs(x, n, p), p))
@@ -828,7 +828,7 @@ def _observe(a, x, n, p):
 
 
 def xdata(a, n, p, x=None):
-    """Ensemble mean of observe{n} at the current time (xdata.m:330-395); x is
+    """Ensemble mean of observe{n} at the current time (xdata.m:21-86); x is
     the auxiliary cell (p.auxfields)."""
     p.nobserve = n
     obs = _observe(a, x, n, p)
@@ -837,7 +837,7 @@ def xdata(a, n, p, x=None):
 
 
 def Int(o, *args):
-    """Space integral with optional bounds (Applications/SPDE/Int.m:234-282)."""
+    """Space integral with optional bounds (Applications/SPDE/Int.m:23-71)."""
     p = args[-1]
     dx = list(p.dx)
     b = np.zeros((p.dimensions, 2))
@@ -867,7 +867,7 @@ def Int(o, *args):
 
 
 def Ave(o, *args):
-    """Lattice average (Applications/SPDE/Ave.m:297-317)."""
+    """Lattice average (Applications/SPDE/Ave.m:14-34)."""
     p = args[-1]
     av = args[0] if len(args) == 2 else [1] * p.dimensions
     o = np.asarray(o)
@@ -879,7 +879,7 @@ def Ave(o, *args):
 
 
 def D2(a, d, p):
-    """Central second difference along dimension d (Applications/SPDE/D2.m:214-271),
+    """Central second difference along dimension d (Applications/SPDE/D2.m:21-77),
     cell 1, all components, propagation use (p.indext = 0)."""
     a = np.asarray(a)
     dx = p.dx[d]
@@ -909,7 +909,7 @@ def D2(a, d, p):
 
 
 def D1(a, d, p):
-    """Central first difference along dimension d (Applications/SPDE/D1.m:60-110),
+    """Central first difference along dimension d (Applications/SPDE/D1.m:62-105),
     cell 1, propagation use."""
     a = np.asarray(a)
     dx = p.dx[d]
@@ -933,7 +933,7 @@ def D1(a, d, p):
 # ---------------------------------------------------------------------------
 
 def xpath(a, nc, p):
-    """Time loop: noise, method, observe at step 1 (xpath.m:124-215).
+    """Time loop: noise, method, observe at step 1 (xpath.m:16-107).
 
     ``p.draw`` counts ``p.noisegen`` calls (the Philox draw index, from 1)."""
     P1 = p.points[0]
@@ -950,17 +950,17 @@ def xpath(a, nc, p):
     x = np.array(p.aux0, dtype=complex) if p.auxfields else None
     aftx = np.zeros((P1 * S,) + np.shape(x), dtype=complex) if (spectrum and p.auxfields) else None
     n1 = -1
-    for n in range(P1):                                                  # :137
-        for step in range(S):                                            # :138
-            n1 += 1                                                      # :27
-            if n > 0 or step > 0 or P1 == 1:                             # :140
-                for checks in range(p.checks[0] + 1):                    # :141
+    for n in range(P1):                                                  # :29
+        for step in range(S):                                            # :30
+            n1 += 1                                                      # :31
+            if n > 0 or step > 0 or P1 == 1:                             # :32
+                for checks in range(p.checks[0] + 1):                    # :33
                     p.draw += 1
-                    w = p.noisegen(w, nc, p.nscale, p)                   # :142
-                    if nc == 1 or checks == 1:                           # :143
+                    w = p.noisegen(w, nc, p.nscale, p)                   # :34
+                    if nc == 1 or checks == 1:                           # :35
                         if p.auxfields:                                  # :36-38
                             x = fit(np.asarray(call_cells(p.define, a, w, p), dtype=complex), p.cax)
-                        a = method(a, w, p)                              # :150
+                        a = method(a, w, p)                              # :42
                         if p.auxfields:                                  # :42-44 (same p.t, same noise)
                             x = 0.5 * (x + fit(np.asarray(call_cells(p.define, a, w, p), dtype=complex), p.cax))
                         if spectrum:                                     # :46-54
@@ -972,14 +972,14 @@ def xpath(a, nc, p):
                                 aft[n1] = a
                                 if p.auxfields:
                                     aftx[n1] = x
-                        w = None                                         # :164
-                        p.t = p.t + p.dtr                                # :165
+                        w = None                                         # :56
+                        p.t = p.t + p.dtr                                # :57
             elif spectrum:                                               # :64-68
                 aft[n1] = a
                 if p.auxfields:
                     aftx[n1] = x
-            if step == 0:                                                # :181
-                if p.rawdata:                                            # :72-77
+            if step == 0:                                                # :73
+                if p.rawdata:                                            # :73-78
                     raw[:, n] = a
                 for o in p.averages:
                     if not p.transforms[o][0]:
@@ -1076,7 +1076,7 @@ def xensemble(npar, inputs):
 # ---------------------------------------------------------------------------
 
 def xcompress(n, data, p, xk):
-    """Reduce output arrays to the requested axes (xcompress.m:142-194)."""
+    """Reduce output arrays to the requested axes (xcompress.m:18-70)."""
     axes = list(p.axes[n])
     x = list(xk)
     g = p.gpoints[n]
@@ -1117,7 +1117,7 @@ def xcompress(n, data, p, xk):
 
 
 def xsim(*inputs):
-    """Run ensembles and compute error columns (xsim.m:77-263).
+    """Run ensembles and compute error columns (xsim.m:28-214).
 
     Returns (error, data, input) like the reference, and raw as a fourth value
     when an input sets p.rawdata: raw[s][nc][k] is the [fields, points(1), space,
@@ -1129,14 +1129,14 @@ def xsim(*inputs):
     inp = xpreferences(list(inputs))
     p = inp[0]
     seq = len(inp)
-    ne = p.ensembles[1] * p.ensembles[2]                                 # :85
+    ne = p.ensembles[1] * p.ensembles[2]                                 # :36
     n1 = ne - 1
     nc1 = p.nchk + p.fbsw
-    sx = max(3, 1 + nc1)                                                 # :89
+    sx = max(3, 1 + nc1)                                                 # :40
     err = np.zeros(6)
     data = None
     raw = [[[None] * (p.ensembles[1] * p.ensembles[2]) for _ in range(p.nchk)] for _ in range(seq)]  # :42
-    for npar in range(1, p.ensembles[2] + 1):                            # :99-109
+    for npar in range(1, p.ensembles[2] + 1):                            # :50-60
         dp, rp = xensemble(npar, inp)
         data = dp if data is None else [[x + y for x, y in zip(a, b)] for a, b in zip(data, dp)]
         for s in range(seq):                                             # :54, :57 raw(:,:,:,npar)
@@ -1164,20 +1164,20 @@ def xsim(*inputs):
             gp = list(d.shape[:-1])
             ddata = int(np.prod(gp))
             d = freshape(d, [ddata, sx])
-            mx = np.max(np.abs(d[:, 0])) ** 2                            # :136
+            mx = np.max(np.abs(d[:, 0])) ** 2                            # :87
             if not (p.relerr and mx > p.tol):
                 mx = 1.0
             if ne > 1:
-                d[:, sx - 1] = np.abs(np.sqrt((d[:, sx - 1] - d[:, 0] ** 2 + 0j) / n1))  # :144
+                d[:, sx - 1] = np.abs(np.sqrt((d[:, sx - 1] - d[:, 0] ** 2 + 0j) / n1))  # :95
             else:
                 d[:, sx - 1] = 0
             for nc in range(2, p.nchk + p.fbsw + 1):
-                d[:, nc - 1] = np.abs(d[:, nc - 1] - d[:, 0])            # :154
+                d[:, nc - 1] = np.abs(d[:, nc - 1] - d[:, 0])            # :105
                 er[o, nc - 1] = np.mean(d[:, nc - 1] ** 2)
                 em[o, nc - 1] = math.sqrt(np.max(d[:, nc - 1] ** 2))
-            esum = np.sum(d[:, 1:sx] ** 2, axis=1) + 1e-20               # :158
+            esum = np.sum(d[:, 1:sx] ** 2, axis=1) + 1e-20               # :109
             ept = (esum > p.tol) & (np.abs(d[:, 0]) > p.cutoffs[n])
-            if p.compare[n] is not None:                                 # :168
+            if p.compare[n] is not None:                                 # :119
                 q = p.copy()
                 q.xk = list(p.xk)
                 q.xk[n] = xkn
@@ -1191,25 +1191,25 @@ def xsim(*inputs):
                 dif = np.broadcast_to(dif, shp).copy()
                 dif = freshape(dif, [ddata, 1])
                 d = np.concatenate([d, dif], axis=1)
-                ept = ept & (np.abs(d[:, sx]) > p.cutoffs[n])            # :176
+                ept = ept & (np.abs(d[:, sx]) > p.cutoffs[n])            # :127
                 mx = np.max(np.abs(d[:, sx]) ** 2)
                 if not (p.relerr and mx > p.tol):
                     mx = 1.0
-                dif2 = (d[:, 0] - d[:, sx]) ** 2                         # :185
+                dif2 = (d[:, 0] - d[:, sx]) ** 2                         # :136
                 em[o, sx] = math.sqrt(np.max(dif2) / mx)
                 er[o, sx] = np.mean(dif2) / mx
                 if ne > 1:
-                    er[o, sx + 1] = np.sum(ept * (dif2 / esum))          # :189
+                    er[o, sx + 1] = np.sum(ept * (dif2 / esum))          # :140
                 er[o, sx + 2] = np.sum(ept)
-            er[o, 1:p.nchk] = er[o, 1:p.nchk] / mx                       # :193
-            er[o, sx - 1] = np.mean(d[:, sx - 1] ** 2) / mx              # :195
+            er[o, 1:p.nchk] = er[o, 1:p.nchk] / mx                       # :144
+            er[o, sx - 1] = np.mean(d[:, sx - 1] ** 2) / mx              # :146
             em[o, sx - 1] = math.sqrt(np.max(d[:, sx - 1] ** 2) / mx)
             nz = np.sum(er[o, 1:sx + 1] > 0)
-            er[o, 0] = np.sum(er[o, 1:sx + 1]) / (1e-99 + nz)            # :197
-            er[o, 0:sx + 1] = np.sqrt(er[o, 0:sx + 1])                   # :198
+            er[o, 0] = np.sum(er[o, 1:sx + 1]) / (1e-99 + nz)            # :148
+            er[o, 0:sx + 1] = np.sqrt(er[o, 0:sx + 1])                   # :149
             data[s][n] = d
     error = np.zeros(max(6, sx + 4))
-    for c in range(1, sx + 1):                                           # :230-233
+    for c in range(1, sx + 1):                                           # :181-184
         pts = 1e-99 + np.sum(er[:, c] > p.tol)
         error[c] = math.sqrt(np.sum(er[:, c] ** 2) / pts)
     error[0] = math.sqrt(np.sum(error[1:sx + 1] ** 2) / (1e-99 + np.sum(error[1:sx + 1] > p.tol)))

@@ -1,7 +1,7 @@
 """Extract the reference's Batchtest golden error values into a fixture.
 
 Reads Examples/Batchtest.m of the xSPDE reference checkout (path given as the
-first argument, default /root/reference) as text and writes
+first argument, or in XSPDE_REFERENCE) as text and writes
 batchtest_expected.json beside this script: {name: expected e(1)} for the 42
 projects, in Batchtest order.  The reference accepts e(1) within a factor
 1.001 of these values (Examples/Batchtest.m:81).
@@ -11,7 +11,9 @@ import os
 import re
 import sys
 
-ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("XSPDE_REFERENCE")
+if not ref:
+    sys.exit("usage: make_batchtest_expected.py <xSPDE reference checkout> (or set XSPDE_REFERENCE)")
 src = open(os.path.join(ref, "Examples", "Batchtest.m")).read()
 names = re.findall(r"e\{(\d+)\}\s*=\s*\w+;\s*n\{\d+\}\s*=\s*'([^']+)'", src)
 body = src[src.index("e1 = ["):]

@@ -3,7 +3,7 @@
 Each builder returns the parameter list that the reference's example function
 passes to xsim/xspde, with the MATLAB anonymous functions rewritten as NumPy
 callables for the oracle (oracle/xspde_ref.py).  Sources, in the reference:
-Examples/SPDE_2D/Soliton.m, Characteristic.m, SolitonAv.m, SolitonDerivN.m,
+Examples/SPDE_2D/Soliton.m, Characteristic.m, SolitonAv.m, SolitonDerivS.m, SolitonDerivN.m,
 Boundaries2.m, Peregrine.m; Examples/SPDE_3D/GaussianAv2D.m,
 GaussianKinetic.m; Examples/SPDE_nD/GaussianAv4D.m, Gaussian3D.m.
 """
@@ -74,6 +74,16 @@ def soliton_deriv_n():
                  linear=lambda p: 0.5j * (p.Dx ** 2 - 1))]
 
 
+def soliton_deriv_s():
+    # D2 finite differences inside the drift on a periodic lattice, then a second
+    # sequence with twice the nonlinearity (Examples/SPDE_2D/SolitonDerivS.m:11-23)
+    p = dict(dimensions=2, order=4, points=[101, 51], steps=10, initial=lambda v, p: sech(p.x),
+             deriv=lambda a, w, p: 1j * a * (np.conj(a) * a) + 0.5j * (X.D2(a, 1, p) - a),
+             observe=[lambda a, p: a * np.conj(a), lambda a, p: X.Int(abs(X.D1(a, 1, p)) ** 2, p)])
+    p1 = dict(p, deriv=lambda a, w, p: 2 * 1j * a * (np.conj(a) * a) + 0.5j * (X.D2(a, 1, p) - a))
+    return [p, p1]
+
+
 def _heat_in(v, p):
     x = p.x
     return np.concatenate([4 * np.sin(x) + np.sin(2 * x), 5 + 4 * np.cos(x) + np.cos(2 * x),
@@ -142,6 +152,7 @@ def gaussian3d():
 
 DETERMINISTIC = {
     "Soliton": soliton, "Characteristic": characteristic, "SolitonAv": soliton_av,
-    "GaussianAv2D": gaussian_av2d, "GaussianKinetic": gaussian_kinetic, "SolitonDerivN": soliton_deriv_n,
+    "GaussianAv2D": gaussian_av2d, "GaussianKinetic": gaussian_kinetic, "SolitonDerivS": soliton_deriv_s,
+    "SolitonDerivN": soliton_deriv_n,
     "Boundaries2": boundaries2, "Peregrine": peregrine, "GaussianAv4D": gaussian_av4d, "Gaussian3D": gaussian3d,
 }

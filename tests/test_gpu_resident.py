@@ -292,7 +292,7 @@ def test_time_spectrum_field_in_device_memory_fp64():
 
 @pytest.mark.parametrize("nc", [1, 2])
 def test_raw_trajectories_two_fields_fp64(nc):
-    """p.rawdata (Simulator/xpath.m:72-77): the field of every trajectory at every
+    """p.rawdata (Simulator/xpath.m:73-78): the field of every trajectory at every
     output time, [fields, points(1), space, ens], for two blocks in one call."""
     from xspde_matlab_b200 import GpuPath, xpreferences
     base = dict(dimensions=2, fields=2, noises=2, points=[6, 16], ranges=[0.6, 6.0], steps=2, ensembles=[4, 2, 1],

@@ -81,6 +81,15 @@ GOLDEN = {
                             transforms=[0, [0, 1, 1], [0, 1, 1], 0, 0, [0, 1, 1]],
                             compare=[None, None, lambda p: 1 / (2 * 3.3 ** 2) + 1 / (2 * 0.235 ** 2),
                                      lambda p: 0.235 / np.sqrt(2), None, lambda p: 1 / (np.sqrt(2) * 0.235)]),
+    # Examples/SPDE_2D/SolitonDerivS.m: D2 finite differences inside the drift on a periodic lattice
+    # (MP runs unfused), D1 in an observable, then a second sequence with twice the nonlinearity
+    "SolitonDerivS": [
+        dict(dimensions=2, order=4, points=[101, 51], steps=10, initial="@(v,p) sech(p.x)",
+             deriv="@(a,w,p) 1i*a.*(conj(a).*a)+0.5*1i*(D2(a,p)-a)",
+             observe=["@(a,p) a.*conj(a)", "@(a,p) Int(abs(D1(a,p)).^2,p)"]),
+        dict(dimensions=2, order=4, points=[101, 51], steps=10, initial="@(v,p) sech(p.x)",
+             deriv="@(a,w,p) 2.*1i*a.*(conj(a).*a)+0.5*1i*(D2(a,p)-a)",
+             observe=["@(a,p) a.*conj(a)", "@(a,p) Int(abs(D1(a,p)).^2,p)"])],
     # Examples/SPDE_2D/SolitonDerivN.m: RK4, Neumann (DCT-I) boundaries, D1 finite differences in an observable
     "SolitonDerivN": dict(dimensions=2, points=[101, 101], method="RK4", order=4, ranges=[10, 15],
                           initial="@(v,p) sech(p.x)",

@@ -119,7 +119,7 @@ def test_mirror_matches_oracle_axes_and_cutoffs(monkeypatch):
 
 
 def test_mirror_saves_matlab_file(monkeypatch, tmp_path):
-    """p.file: error, data, input and raw in a MATLAB file (Simulator/xsim.m:206-210)."""
+    """p.file: error, data, input and raw in a MATLAB file (Simulator/xsim.m:207-210)."""
     import scipy.io
     base = dict(dimensions=2, points=[5, 8], ranges=[0.5, 4.0], steps=2, ensembles=[4, 2, 1], noises=2,
                 method="MP", checks=1, order=1, file=str(tmp_path / "run.mat"))

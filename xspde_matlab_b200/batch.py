@@ -1,6 +1,6 @@
 """Uneven batch: many independent xSPDE inputs integrated by one CUDA-graph launch.
 
-The reference runs one input at a time (Simulator/xsim.m:40-60 loops over
+The reference runs one input at a time (Simulator/xsim.m:44-60 loops over
 sequences; Simulator/xensemble.m:25-108 over blocks), so a sweep of hundreds
 of small problems pays one MATLAB time loop each.  Here every input becomes an
 item of an ``xs_batch`` (include/xspde_b200.h): items whose generated kernels

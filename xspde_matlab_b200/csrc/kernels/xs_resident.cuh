@@ -1,8 +1,8 @@
 // Resident-path kernel: every trajectory's field lives in shared memory for the
-// whole time loop of one xpath call (Simulator/xpath.m:137-194).  One CTA owns
+// whole time loop of one xpath call (Simulator/xpath.m:29-86).  One CTA owns
 // XS_G trajectories of one ensemble block; the time loop, noise draws
 // (Simulator/xnoise.m:29-38), interaction-picture steps (Applications/SDE/*.m,
-// Applications/SPDE/xprop.m) and observables (Simulator/xdata.m:339-393) run
+// Applications/SPDE/xprop.m) and observables (Simulator/xdata.m:30-84) run
 // on chip.  HBM sees only the initial/final fields and one partial-sum row of
 // observables per output time.  Transforms along each space dimension are
 // dense N x N matrices (FFT, DST-I/II/III, DCT-I/II/III alike), applied from
@@ -47,7 +47,7 @@ struct XsPathArgs {
   int nt;               // XS_SPEC: points(1) x steps(1)
   int pad4;
   double fscn;          // XS_SPEC: p.fsc / nt
-  double2* raw;         // optional raw trajectories (p.rawdata, xpath.m:72-77): the field at every
+  double2* raw;         // optional raw trajectories (p.rawdata, xpath.m:73-78): the field at every
                         // output time in MATLAB's layout [F][npoints][NS][ntraj], fastest first
   const double2* kfilt; // XS_NK: [NK][NS] factors of p.nfilter on the FFT-ordered k lattice (null: 1)
   const double2* rfilt; // XS_NKV: the same for p.rfilter
@@ -457,7 +457,7 @@ __device__ __forceinline__ void xs_tr(cx* X, cx* T, const XsPathArgs& P, int dir
   }
 }
 
-// xprop (Applications/SPDE/xprop.m:76-104): transform, multiply by exp(L dt),
+// xprop (Applications/SPDE/xprop.m:18-42): transform, multiply by exp(L dt),
 // inverse; with boundary values (XS_BVAL) the xpatch.m patch at time tb is
 // taken off before and put back (with its Neumann term) after.
 __device__ __forceinline__ void xs_prop_tab(cx* X, cx* T, const XsPathArgs& P, const double2* __restrict__ tab,
@@ -661,7 +661,7 @@ __device__ void xs_method(cx* A, cx* B1, cx* B2, cx* B3, cx* T, const real* W, c
   xs_axpby(A, (real)2, A, (real)-1, B1);
   xs_prop(A, T, P, t + dtr);
 #elif XS_METHOD == 1
-  // RK4 (Applications/SDE/RK4.m:35-70)
+  // RK4 (Applications/SDE/RK4.m:7-42)
   const real h = (real)(dtr * 0.5);
   xs_setbound(A);
   xs_deriv_update(B1, A, A, W, Z, h, t, P.params, T);
@@ -679,18 +679,18 @@ __device__ void xs_method(cx* A, cx* B1, cx* B2, cx* B3, cx* T, const real* W, c
   xs_deriv_update(A, A, B3, W, Z, (real)(dtr * 0.5 / 3.0), t + dtr, P.params, T);
   xs_setbound(A);
 #elif XS_METHOD == 2
-  // Euler (Applications/SDE/Euler.m:77-81)
+  // Euler (Applications/SDE/Euler.m:6-10)
   xs_deriv_update(A, A, A, W, Z, (real)dtr, t, P.params, T);
   xs_prop(A, T, P);
 #elif XS_METHOD == 3
-  // RK2 (Applications/SDE/RK2.m:89-107): B1 holds the predictor a.
+  // RK2 (Applications/SDE/RK2.m:7-25): B1 holds the predictor a.
   xs_deriv_update(B1, A, A, W, Z, (real)dtr, t, P.params, T);
   xs_prop(A, T, P);
   xs_prop(B1, T, P);
   xs_deriv_update(A, A, B1, W, Z, (real)dtr, t + dtr, P.params, T);
   xs_axpby(A, (real)0.5, B1, (real)0.5, A);
 #elif XS_METHOD == 4
-  // Implicit (Applications/SDE/Implicit.m:116-125)
+  // Implicit (Applications/SDE/Implicit.m:8-17)
   xs_copy(B1, A);
   for (int it = 0; it < XS_ITER; ++it) xs_deriv_update(A, B1, A, W, Z, (real)dtr, t + dtr, P.params, T);
   xs_prop(A, T, P);
@@ -1072,7 +1072,7 @@ __device__ void xs_resident_run(const XsPathArgs& P, int cta, int nctas) {
 
   double t = P.t0;
   if (P.single_step) {
-    // p.method(a, w, p) on the given noise (Simulator/xpath.m:150)
+    // p.method(a, w, p) on the given noise (Simulator/xpath.m:42)
 #if !XS_LEAN
     for (int i = threadIdx.x; i < XS_G * XS_NS; i += blockDim.x) {
       const int g = i / XS_NS, s = i % XS_NS;

@@ -1,6 +1,6 @@
 // Streaming-path kernels for 2D lattices whose field does not fit one CTA
-// (Simulator/xpath.m:137-194 with Applications/SDE/MP.m and the periodic
-// branch of Applications/SPDE/xprop.m / xtransform.m:149,164).
+// (Simulator/xpath.m:29-86 with Applications/SDE/MP.m and the periodic
+// branch of Applications/SPDE/xprop.m / xtransform.m:45,60).
 //
 // Field layout in HBM: F[e][f][y][x], x fastest, complex `real`.  Between
 // passes the field is held with the x direction Fourier transformed
@@ -538,6 +538,14 @@ extern "C" __global__ void __launch_bounds__(XS_OROWS * XS_RX) xs_x_obs(const Xs
       for (int j = 0; j < XS_RX; ++j) v[f][j] = base[(size_t)f * XS_NS + XS_RX * j];
 #pragma unroll
     for (int f = 0; f < XS_F; ++f) xs_ifft4<XS_RX, 1, 1>(v[f], t, tw, buf, ws);
+    {  // a diverged trajectory is reported (status bit 0) at every observation, not only by xs_x_final
+      bool bad = false;
+#pragma unroll
+      for (int f = 0; f < XS_F; ++f)
+#pragma unroll
+        for (int j = 0; j < XS_RX; ++j) bad |= !isfinite((double)v[f][j].re) || !isfinite((double)v[f][j].im);
+      if (bad) atomicOr(A.status, 1);
+    }
 #if XS_NRED > 0
     double acc[2 * XS_NRED];
 #pragma unroll

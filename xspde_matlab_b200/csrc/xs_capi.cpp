@@ -260,7 +260,7 @@ struct Problem {
   int Lc = 1;
   std::vector<ObsInfo> obs;
   int nred = 0, nout_site = 0, nout_scalar = 0;
-  int type(int d, int f) const {  // boundary type b1 + 2*b2 (xtransform.m:134)
+  int type(int d, int f) const {  // boundary type b1 + 2*b2 (xtransform.m:30)
     if (bnd.empty()) return 0;
     return bnd[(d * F + f) * 2] + 2 * bnd[(d * F + f) * 2 + 1];
   }
@@ -394,7 +394,7 @@ void setup_problem(const xs_problem* in, Problem& P) {
     P.kobs = true;
   }
   if (P.kobs && P.NA) raise(XS_ERR_UNSUPPORTED, "k-space observables with auxiliary fields are not supported on the device");
-  // grid constants (Simulator/xpreferences.m:133-175, spdpreferences.m:190-244)
+  // grid constants (Simulator/xpreferences.m:133-175, spdpreferences.m:16-70)
   for (int d = 0; d < p.dimensions; ++d) {
     int n = p.points[d];
     P.dx[d] = n == 1 ? 1.0 : p.ranges[d] / std::max(1, n - 1);
@@ -639,7 +639,7 @@ void generate_functions(Problem& P, std::ostringstream& os) {
     }
     os << "}\n";
   }
-  // observe{n}(a, p) (xdata.m:339)
+  // observe{n}(a, p) (xdata.m:30)
   P.obs.clear();
   P.nred = P.nout_site = P.nout_scalar = 0;
   for (size_t oi = 0; oi < P.observe.size(); ++oi) {
@@ -710,7 +710,7 @@ void generate_functions(Problem& P, std::ostringstream& os) {
       os << "};\n";
     }
   }
-  // D1/D2 of the field at site s of trajectory g (Applications/SPDE/D1.m:60-110, D2.m:214-271):
+  // D1/D2 of the field at site s of trajectory g (Applications/SPDE/D1.m:62-105, D2.m:21-77):
   // central differences with periodic wrap; at a Neumann end D1 is the boundary value and D2 the
   // one-sided form, at a Dirichlet end D2 repeats its neighbour (boundary values zero)
   os << "__device__ const int xs_btab[3][" << P.F << "][2] = {";
@@ -768,7 +768,7 @@ __device__ __forceinline__ cx xs_fd2(const cx* __restrict__ fld, int g, int s, i
         else w *= r.weight[q];
         double lo = r.lo[r.dims[q]], hi = r.hi[r.dims[q]];
         if (!r.ave && lo < hi) {
-          // Int.m:273-277: j = 1+floor((lo-x(1))/d); while x(j) <= hi
+          // Int.m:62-66: j = 1+floor((lo-x(1))/d); while x(j) <= hi
           double step = r.weight[q];
           int j0 = (int)std::floor((lo - P.xc[d][0]) / step);
           if (j0 < 0) j0 = 0;
@@ -1637,7 +1637,7 @@ int resident_grid(xs_handle& h, CUfunction f, int nctas) {
   return grid;
 }
 
-// Time spectrum (Simulator/xpath.m:26-106): the field at every step count, Nt = points(1) x steps
+// Time spectrum (Simulator/xpath.m:25-106): the field at every step count, Nt = points(1) x steps
 // rows per trajectory tile, then points(1) rows of its inverse DFT at the frequencies
 // (0..P1-1) - floor(P1/2) (ifft, fftshift and p.specpts), scaled by p.fsc / Nt with
 // p.fsc = sqrt(2 pi) / p.dw, p.dw = 2 pi / (ranges(1) + dt) (xpreferences.m:246-249).
@@ -1694,7 +1694,7 @@ void launch_resident(xs_handle& h, int first_block, int nblocks, int nc, const v
   a.seq = P.p.sequence;
   a.seed = (unsigned)(P.p.seed & 0xffffffffu);
   a.wscale = std::sqrt(P.nscale * P.noisefactor);  // xnoise.m:32
-  a.vscale = std::sqrt(P.noisefactor);              // xrandom.m:23
+  a.vscale = std::sqrt(P.noisefactor);              // xrandom.m:22
   a.dtr = pass_dtr(P, nc);
   a.t0 = P.p.origins[0];
   a.prop = ensure_prop(h, nc);
@@ -1799,7 +1799,7 @@ void launch_observe(xs_handle& h, void** prm, int nrg, int nb, cudaStream_t st) 
   }
 }
 
-// The pass sequence of one streaming p.path call (Simulator/xpath.m:137-194 with merged MP
+// The pass sequence of one streaming p.path call (Simulator/xpath.m:29-86 with merged MP
 // half steps): initial field, then per step a column pass (exp(L dt)^m, m = 2 when the previous
 // step's second half is merged in) and a row pass (drift and noise), and at output times the
 // pending half step and the observables.
@@ -1919,7 +1919,7 @@ void launch_stream_halves(xs_handle& h, const StreamArgsHost& a, int nblocks, in
   }
 }
 
-// Streaming schedule of one xpath call (Simulator/xpath.m:137-194) for MP:
+// Streaming schedule of one xpath call (Simulator/xpath.m:29-86) for MP:
 // column passes apply the pending half-step propagators, row passes do the
 // midpoint step; observations need all half steps applied first.
 void launch_stream(xs_handle& h, int first_block, int nblocks, int nc, const void* a_in_dev, void* av_dev,
@@ -2569,7 +2569,7 @@ XS_API xs_status xs_random(xs_handle* h, int block, double* v_out) {
     g_err = "null handle";
     return XS_ERR_ARG;
   }
-  return export_normals(h, true, block, 0, std::sqrt(h->P.noisefactor), v_out);  // xrandom.m:23
+  return export_normals(h, true, block, 0, std::sqrt(h->P.noisefactor), v_out);  // xrandom.m:22
 }
 
 XS_API xs_status xs_step(xs_handle* h, double* a_inout, const double* w, double t, double dtr) {
@@ -2843,7 +2843,7 @@ void variant_tables(xs_batch& b, BatchVariant& v, int steps_cap, int points_cap,
     it.block0 = 0;
     it.nunits = it.ntraj / v.G;
     it.wscale = std::sqrt(P.nscale * P.noisefactor);  // xnoise.m:32
-    it.vscale = std::sqrt(P.noisefactor);              // xrandom.m:23
+    it.vscale = std::sqrt(P.noisefactor);              // xrandom.m:22
     it.dtr = item_dtr(P);
     it.t0 = P.p.origins[0];
     it.prop = (const char*)b.d_prop.p + e.prop_off * 16;

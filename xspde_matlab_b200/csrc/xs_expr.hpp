@@ -3,7 +3,7 @@
 // xSPDE users write the drift (p.deriv), initial condition (p.initial),
 // observables (p.observe) and linear operator (p.linear) as MATLAB anonymous
 // functions, e.g. "@(a,w,p) 1i*a.*conj(a).*a + 0.01*w(1,:)".  The reference
-// evaluates them as MATLAB code (Applications/SDE/MP.m:16, Simulator/xdata.m:339,
+// evaluates them as MATLAB code (Applications/SDE/MP.m:16, Simulator/xdata.m:30,
 // Applications/SPDE/xpropfactor.m:38).  Here the same text is parsed once:
 // pointwise functions become device code inside the fused kernel; the linear
 // operator is evaluated in FP64 on the host to build exp(L dt).  Anything

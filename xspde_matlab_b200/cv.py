@@ -11,7 +11,7 @@ computed by xs_noise_features are independent N(0, 1) variables, so the M
 fresh inputs are drawn directly from N(0, 1) without integrating anything.
 The network (xs_mlp_*) is trained on pairs the solver itself produces, with
 the project's forward, backward and Adam kernels (BF16 operands, FP32
-accumulation); xSPDE's block-mean sampling error (Simulator/xsim.m:144)
+accumulation); xSPDE's block-mean sampling error (Simulator/xsim.m:95)
 judges both estimators.
 """
 import ctypes
@@ -107,7 +107,7 @@ class ControlVariateNet:
 
 
 def block_sampling_error(values, nblocks):
-    """xSPDE's sampling error of the mean from block means (Simulator/xsim.m:144):
+    """xSPDE's sampling error of the mean from block means (Simulator/xsim.m:95):
     sqrt((<D^2> - <D>^2) / (nblocks - 1)) with D the block means."""
     v = np.asarray(values, dtype=np.float64)
     n = (v.size // nblocks) * nblocks

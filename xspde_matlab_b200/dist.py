@@ -1,5 +1,5 @@
 """Multi-process ensembles: the reference's parfor over ensemble blocks
-(Simulator/xsim.m:99-106) as one process per GPU.
+(Simulator/xsim.m:50-57) as one process per GPU.
 
 Blocks are independent (each has its own Philox key), so they are split into
 contiguous ranges, one per rank, with no data exchange during integration.

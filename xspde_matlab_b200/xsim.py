@@ -8,7 +8,7 @@ return ``(error, data, input)`` as Simulator/xsim.m:1 does.  Functions that run
 on the device -- ``deriv`` (alias ``da``), ``initial``, ``observe``, ``linear``
 -- are given as the text of MATLAB anonymous functions; host-side functions
 -- ``output``, ``compare`` -- are Python callables, as in the reference where
-they run after the ensemble loop (Simulator/xensemble.m:88, xsim.m:170).
+they run after the ensemble loop (Simulator/xensemble.m:88, xsim.m:121).
 
 The ensemble loop (Simulator/xensemble.m:25-108) calls the GPU's p.path
 replacement once per check pass for a group of blocks, then accumulates
@@ -337,7 +337,7 @@ class GpuPath:
     def run_path(self, first_block, nblocks, nc, a_in=None, a_out=False, raw=False):
         """p.path for blocks [first_block, first_block+nblocks): returns
         (av, a) with av[b][o] complex arrays of shape av_shapes()[o]; with
-        raw=True (p.rawdata, Simulator/xpath.m:72-77) also the field at every
+        raw=True (p.rawdata, Simulator/xpath.m:73-78) also the field at every
         output time, [fields, points(1), space..., ens1*nblocks]: (av, a, raw)."""
         P = self.p
         if callable(P.get("boundfun", None)):
@@ -408,7 +408,7 @@ _hook_methods()
 
 
 def _xcompress(n, data, p, xk):
-    """Axis reduction of an output array (Applications/SPDE/xcompress.m:142-194)."""
+    """Axis reduction of an output array (Applications/SPDE/xcompress.m:18-70)."""
     axes = list(p.axes[n])
     x = list(xk)
     d = len(p.gpoints[n]) - 2
@@ -419,7 +419,7 @@ def _xcompress(n, data, p, xk):
         ind = axes[ax]
         if np.size(x[ax]) > 1:
             if ax + 1 <= p.dimensions and ax < len(p.ftransforms[n]) and p.ftransforms[n][ax]:
-                x[ax] = p.kc[ax]  # k axis (xcompress.m:151-153)
+                x[ax] = p.kc[ax]  # k axis (xcompress.m:40-42)
             if np.size(ind) == 1:
                 ind = int(np.atleast_1d(ind)[0])
                 ind = (list(range(1, shp[ax + 1] + 1)) if ind == 0 else [mid[ax + 1]] if ind == -1
@@ -435,7 +435,7 @@ def _xcompress(n, data, p, xk):
 
 
 def _grid(xk):
-    """Output-grid broadcast coordinates for compare functions (Applications/SPDE/xgrid.m:320-327)."""
+    """Output-grid broadcast coordinates for compare functions (Applications/SPDE/xgrid.m:49-56)."""
     q = Struct()
     d = len(xk)
     r = []
@@ -464,7 +464,7 @@ def _ensembles(inp, paths, rank=0, size=1, reduce=None, raw=None):
     """Block loop, check passes and moments (Simulator/xensemble.m:12-108) with
     all blocks of a pass integrated by one device call.  With size > 1 this
     rank integrates its own contiguous share of the blocks and `reduce` sums
-    the moment accumulators over the ranks (Simulator/xsim.m:99-106).  With
+    the moment accumulators over the ranks (Simulator/xsim.m:50-57).  With
     `raw` (nested lists [s][nc-1][k]) the blocks' raw trajectories of inputs
     with p.rawdata are stored at k = j + ens(2) (npar-1) for global block
     (npar-1) + j ens(3) (xensemble.m:26,79; xsim.m:42-57)."""
@@ -544,7 +544,7 @@ def _ensembles(inp, paths, rank=0, size=1, reduce=None, raw=None):
 
 
 def xsim(*inputs, path_kind=0):
-    """Simulate and return (error, data, input) (Simulator/xsim.m:77-263), and
+    """Simulate and return (error, data, input) (Simulator/xsim.m:28-214), and
     raw as a fourth value when an input sets p.rawdata: raw[s][nc][k] is the
     [fields, points(1), space..., ens(1)] field array of sequence s, check pass nc
     and ensemble k (xsim.m:42-57; under several ranks each rank holds its own blocks).
@@ -584,7 +584,7 @@ def xsim(*inputs, path_kind=0):
         for n in range(len(p.output)):
             d = np.reshape(np.real(data[s][n]), p.gpoints[n], order="F")
             for ax in range(1, min(p.dimensions, len(p.gpoints[n]) - 2)):
-                if p.ftransforms[n][ax]:  # k-space axes in centred order (xsim.m:117-121)
+                if p.ftransforms[n][ax]:  # k-space axes in centred order (xsim.m:77-81)
                     d = np.fft.fftshift(d, axes=ax + 1)
             d, xkn = _xcompress(n, d, p, p.xk[n])
             gp = list(d.shape[:-1])
@@ -654,7 +654,7 @@ _SAVED_FIELDS = ("name", "dimensions", "fields", "noises", "knoises", "inrandoms
 
 
 def save_mat(fname, error, data, inp, raw=None):
-    """xsim's MATLAB file (Simulator/xsim.m:206-210: save(file, 'error', 'data',
+    """xsim's MATLAB file (Simulator/xsim.m:207-210: save(file, 'error', 'data',
     'input', 'raw')): error as a row vector, data{s}{n} as nested cells, input{s}
     as structs of the numeric and text inputs, raw{s, nc, k} when recorded."""
     import scipy.io
