@@ -12,7 +12,11 @@ One "step" of this benchmark is one full p.path call over all 4096
 trajectories.  value = trajectory-steps/s with everything resident in HBM
 (field 2.1 GB > L2 every pass); e2e = the same through the host C ABI call
 xs_run_path with a pinned FP64 initial field copied in and the block means
-copied out inside the timed region.
+copied out inside the timed region.  The line also carries the same problem
+in plain FP64 (`fp64`: value, e2e and roofline, the reference's own
+precision), the oracle timed on the host (`cpu_baseline`), and each
+observable's error against the FP64 oracle on identical noise over the whole
+path at 256x256 (`precision_vs_oracle`).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -38,12 +42,12 @@ sys.path.insert(0, ROOT)
 
 METRIC = "traj-steps/s (2D 256x256 stochastic GPE, MP, 4096 trajectories)"
 HBM_FALLBACK_GBS = 6650.0
-# DRAM bytes (read + write) per launch and per trajectory of the two streaming
-# kernels, from one ncu --set full capture of the 512-trajectory case of this
-# problem (profiles/xs_stream_gpe_256x256.md); a launch's traffic grows in
-# proportion to the trajectories it processes, so bench lines scale these by
-# the trajectory count.
-NCU_TRAFFIC_PER_TRAJ = {"x_step": (268465408 + 209754880) / 512.0, "y_pass": (268470528 + 213135104) / 512.0}
+# DRAM bytes (read + write) per trajectory of the two streaming kernels in FP32
+# (keyed by kernel kind and bytes per complex value), from one ncu --set full
+# capture of a 512-trajectory case of this problem; a launch's traffic grows
+# in proportion to the trajectories it processes, so bench lines scale these
+# by the trajectory count.
+NCU_TRAFFIC_PER_TRAJ = {("x_step", 8): (268465408 + 209754880) / 512.0, ("y_pass", 8): (268470528 + 213135104) / 512.0}
 
 
 def _peaks():
@@ -126,108 +130,106 @@ def _problem(ntraj=4096):
     return p
 
 
-def _cpu_sample(seconds=12.0, ntraj=2):
-    """Oracle (FP64 NumPy restatement of the reference path, one core) on a
-    bounded sample of the workload: `ntraj` trajectories of the same 256x256
-    problem for as many integration steps as fit in about `seconds`."""
+def _oracle_gpe(npoints, ntraj, observables):
+    """The oracle's (FP64 NumPy restatement of the reference path) input for the
+    256x256 problem with `npoints` output times, 10 steps between them, one
+    block of `ntraj` trajectories; observables chosen by name."""
+    import numpy as np
+    obs = {"abs2": lambda a, q: abs(a) ** 2, "re": lambda a, q: np.real(a)}
+    return dict(dimensions=3, points=[npoints, 256, 256], ranges=[0.1 * (npoints - 1), 20.0, 20.0], steps=10,
+                ensembles=[ntraj, 1, 1], noises=2, method="MP", checks=0,
+                deriv=lambda a, w, q: (1 - abs(a) ** 2) * a - 0.5j * abs(a) ** 2 * a
+                + 0.05 * (w[0:1] + 1j * w[1:2]) / np.sqrt(2),
+                initial=lambda v, q: 1 + 0.1 * (v[0:1] + 1j * v[1:2]) / np.sqrt(2),
+                linear=lambda q: (1j + 0.1) * (q.Dx ** 2 + q.Dy ** 2), observe=[obs[k] for k in observables])
+
+
+def _oracle_path(o, block=0):
+    """One p.path call of the oracle (Simulator/xpath.m:16-107 restated): the
+    initial field, every MP step with its Philox noise and the observables at
+    every output time.  Returns (seconds, trajectory-steps, av)."""
+    import warnings
+
     import numpy as np
     from oracle import xspde_ref as X
-    p = _problem()
-    o = dict(dimensions=3, points=[2, 256, 256], ranges=[0.4, 20.0, 20.0], steps=40, ensembles=[ntraj, 1, 1],
-             noises=2, method="MP", checks=0,
-             deriv=lambda a, w, q: (1 - abs(a) ** 2) * a - 0.5j * abs(a) ** 2 * a
-             + 0.05 * (w[0:1] + 1j * w[1:2]) / np.sqrt(2),
-             initial=lambda v, q: 1 + 0.1 * (v[0:1] + 1j * v[1:2]) / np.sqrt(2),
-             linear=lambda q: (1j + 0.1) * (q.Dx ** 2 + q.Dy ** 2), observe=[lambda a, q: abs(a) ** 2])
-    inp = X.xpreferences([o])[0]
-    q = inp.copy()
-    q.block = 0
-    q.seq = 0
-    q.dtr = q.dt / q.steps[0]
-    q.propagator, q.da = q.propfactor(q)
-    v = q.randomgen(q)
-    q.t = q.origins[0]
-    a = X.fit(np.asarray(q.initial(v, q), dtype=complex), q.ca)
-    method = X.METHODS["MP"]
-    q.draw = 0
-    t0 = time.perf_counter()
-    steps = 0
-    while time.perf_counter() - t0 < seconds:
-        q.draw += 1
-        w = q.noisegen(None, 1, q.nscale, q)
-        a = method(a, w, q)
-        q.t += q.dtr
-        steps += 1
-    el = time.perf_counter() - t0
-    del p
-    return steps * ntraj / el, "%d trajectories x %d MP steps of the 256x256 problem (FP64 NumPy oracle, 1 core)" % (
-        ntraj, steps)
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore", RuntimeWarning)
+        q = X.xpreferences([o])[0].copy()
+        t0 = time.perf_counter()
+        q.block, q.seq = block, 0
+        q.dtr = q.dt / q.steps[0]
+        q.propagator, q.da = q.propfactor(q)
+        v = q.randomgen(q)
+        q.t = q.origins[0]
+        a = X.fit(np.asarray(X.call_cells(q.initial, None, v, q), dtype=complex), q.ca)
+        _, av, _ = q.path(a, 1, q)
+        el = time.perf_counter() - t0
+    steps = q.points[0] * q.steps[0] - 1
+    return el, steps * q.ensembles[0], av
 
 
-def _precision_report(ntraj_fp64):
-    """The problem as plain FP64 and as FP32 bulk (FP64 tables and moments):
-    FP64 throughput on the full workload (device timing, one step after one
-    warm-up), and the FP32 observable's error against FP64 on one block of 256
-    trajectories over all 51 output times (the FP64 device path agrees with the
-    FP64 oracle to 1e-10 in the parity tests, so it stands in for it here)."""
+def _precision_vs_oracle(npoints=51, ntraj=2):
+    """cpu_baseline and the FP64-oracle error of each observable.
+
+    The oracle integrates `ntraj` trajectories of the benchmark problem over
+    the whole path (509 MP steps, observables <|a|^2> and <Re a> at all 51
+    output times) on one host core; that run is timed as the CPU baseline.
+    The same trajectories (same Philox noise) run through the streaming
+    kernels in FP32 (the benchmark's mode) and FP64, and each observable is
+    compared with the oracle: max |GPU - oracle| / max |oracle| and the rms
+    ratio, over all sites and times."""
     import numpy as np
-    import torch
-    from xspde_matlab_b200 import GpuPath, _lib, xpreferences
-    L = _lib.lib()
-    p64 = xpreferences([dict(_problem(ntraj_fp64), precision="fp64")])[0]
-    g64 = GpuPath(p64)
-    nb = p64.ensembles[1]
-    av = torch.zeros((nb, p64.points[0], p64.nspace, 2), dtype=torch.float64, device="cuda")
-    st = torch.cuda.current_stream()
-
-    def run():
-        _lib.check(L.xs_run_path_device(g64.h, 0, nb, 1, None, ctypes.c_void_p(av.data_ptr()), None,
-                                        ctypes.c_void_p(st.cuda_stream)))
-    run()
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(st)
-    run()
-    e1.record(st)
-    e1.synchronize()
-    ms = e0.elapsed_time(e1)
-    steps = p64.points[0] * p64.steps[0] - 1
-    del g64, av
-    torch.cuda.empty_cache()
-    one = dict(_problem(256), ensembles=[256, 1, 1])
-    a64, _ = GpuPath(xpreferences([dict(one, precision="fp64")])[0]).run_path(0, 1, 1)
-    a32, _ = GpuPath(xpreferences([one])[0]).run_path(0, 1, 1)
-    x64, x32 = a64[0][0][0], a32[0][0][0]
-    err = np.abs(x32 - x64)
-    return ({"value": nb * p64.ensembles[0] * steps / (ms * 1e-3), "unit": "traj-steps/s", "ms_per_step": ms},
-            {"observable": "<|a|^2>(x,y,t), 256 trajectories, 51 times", "max_rel": float(err.max() / np.abs(x64).max()),
-             "rms_rel": float(np.sqrt(np.mean(err ** 2)) / np.sqrt(np.mean(np.abs(x64) ** 2))),
-             "reference": "FP64 device path (pinned to the FP64 oracle at 1e-10)"})
+    from xspde_matlab_b200 import GpuPath, xpreferences
+    os.environ.setdefault("OMP_NUM_THREADS", "1")
+    secs, tsteps, av_o = _oracle_path(_oracle_gpe(npoints, ntraj, ("abs2", "re")))
+    g = dict(_problem(ntraj), ensembles=[ntraj, 1, 1], points=[npoints, 256, 256],
+             ranges=[0.1 * (npoints - 1), 20.0, 20.0], observe=["@(a,p) abs(a).^2", "@(a,p) real(a)"])
+    errs = {}
+    for prec in ("fp32", "fp64"):
+        av_g, _ = GpuPath(xpreferences([dict(g, precision=prec)])[0], path_kind=2).run_path(0, 1, 1)
+        for k, name in enumerate(("<|a|^2>(x,y,t)", "<Re a>(x,y,t)")):
+            x, y = np.asarray(av_g[0][k]).ravel(), np.asarray(av_o[k]).ravel()
+            d = np.abs(x - y)
+            errs.setdefault(prec, {})[name] = {
+                "max_rel": float(d.max() / np.abs(y).max()),
+                "rms_rel": float(np.sqrt(np.mean(d ** 2)) / np.sqrt(np.mean(np.abs(y) ** 2)))}
+    cpu = {"value": tsteps / secs, "unit": "traj-steps/s", "cores": 1, "kind": "port",
+           "sample": "%d trajectories x %d MP steps of the 256x256 problem with <|a|^2> and <Re a> at %d output "
+                     "times (FP64 NumPy oracle, 1 core, %.1f s)" % (ntraj, tsteps // ntraj, npoints, secs)}
+    prec = {"reference": "FP64 oracle (CPU restatement of the reference path) on the same Philox noise",
+            "trajectories": ntraj, "output_times": npoints, "steps": tsteps // ntraj,
+            "bound_fp32": 1e-5, "fp32": errs["fp32"], "fp64": errs["fp64"]}
+    return cpu, prec
 
 
 def _reference_worker(args):
-    seconds, ntraj = args
+    npoints, ntraj = args
     os.environ.setdefault("OMP_NUM_THREADS", "1")
-    r, _ = _cpu_sample(seconds, ntraj)
-    return r
+    secs, tsteps, _ = _oracle_path(_oracle_gpe(npoints, ntraj, ("abs2",)))
+    return tsteps, secs
 
 
 def run_reference(args, rank, world):
-    """--impl reference: the CPU restatement of the reference path on all host cores."""
+    """--impl reference: the CPU restatement of the reference path on all host
+    cores.  Each step every core runs one p.path of its own trajectories (the
+    benchmark's problem, observables included) over a bounded stretch of the
+    path; the step's value is the sum over cores of trajectory-steps per
+    second of integration (process-pool dispatch excluded)."""
     import multiprocessing as mp
     if rank != 0:
         print("reference arm: rank %d has no work (rank 0 times the CPU reference)" % rank, file=sys.stderr)
         return
     cores = os.cpu_count() or 1
+    npoints, ntraj = 4, 2  # 39 MP steps and 4 observations per trajectory, as the benchmark's 509 and 51
     per_step = []
     ctx = mp.get_context("spawn")
     with ctx.Pool(cores) as pool:
         for i in range(args.warmup + args.steps):
             t0 = time.perf_counter()
-            rates = pool.map(_reference_worker, [(4.0, 2)] * cores)
+            res = pool.map(_reference_worker, [(npoints, ntraj)] * cores)
             dt = time.perf_counter() - t0
             if i >= args.warmup:
-                per_step.append((sum(rates), dt))
+                per_step.append((sum(r[0] / r[1] for r in res), dt))
     value = statistics.mean(r for r, _ in per_step)
     ms = 1000 * statistics.mean(d for _, d in per_step)
     line = {
@@ -235,48 +237,57 @@ def run_reference(args, rank, world):
         "unit": "traj-steps/s", "n_gpus": 0, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
         "config": dict(_config(4096, 1), parallelism="host processes (bounded sample per step)"),
+        "same_config": False,
+        "same_config_note": "same problem, lattice, step and observable; each core integrates %d trajectories over "
+                            "%d output times (%d MP steps, observables at every output time as the GPU arm) instead "
+                            "of 4096 trajectories over 51, so one step ends in seconds" % (
+                                ntraj, npoints, npoints * 10 - 1),
         "cpu_baseline": {"value": value, "unit": "traj-steps/s", "cores": cores, "kind": "port",
-                         "sample": "per core: 2 trajectories x ~4 s of MP steps of the 256x256 problem; MATLAB "
-                                   "reference unavailable on this box (no MATLAB/Octave)"},
+                         "sample": "per core and step: one oracle p.path of %d trajectories x %d MP steps with "
+                                   "<|a|^2> at %d output times of the 256x256 problem; MATLAB reference "
+                                   "unavailable on this box (no MATLAB/Octave)" % (ntraj, npoints * 10 - 1, npoints)},
         "e2e": {"value": value, "unit": "traj-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
 
 
-def run_ours(args, rank, world, local_rank):
-    import numpy as np
+def _measure(p, args, rank, world, local_rank, steps, warmup, cxbytes):
+    """Device-timed and end-to-end throughput of one precision mode.
+
+    value: `steps` p.path calls over all of this rank's blocks through
+    xs_run_path_device with the field resident in HBM, each followed by the
+    device-side block moments (xs_block_moments, xensemble.m:98-101) and, with
+    several ranks, their all-reduce; CUDA events on the launching stream,
+    max over ranks.  e2e: the same calls through xs_run_path with a pinned
+    FP64 host initial field copied in and the block means copied out."""
     import torch
-    from xspde_matlab_b200 import GpuPath, _lib, xpreferences
-    torch.cuda.set_device(local_rank)
+    from xspde_matlab_b200 import GpuPath, _lib
     dist = None
     if world > 1:
         import torch.distributed as dist
-    p = xpreferences([_problem(args.ntraj)])[0]
     nb = p.ensembles[1] * p.ensembles[2]
-    E = p.ensembles[0]
-    ntraj = nb * E
+    ntraj = nb * p.ensembles[0]
     steps_per_traj = p.points[0] * p.steps[0] - 1
     path = GpuPath(p)
     L = _lib.lib()
-    stride = 1 * p.nspace  # one site observable line
-    av = torch.zeros((nb, p.points[0], stride, 2), dtype=torch.float64, device="cuda")
-    moments = torch.zeros((2, p.points[0], stride), dtype=torch.float64, device="cuda")
+    n = p.points[0] * p.nspace  # complex means per block (one site observable)
+    av = torch.zeros((nb, n, 2), dtype=torch.float64, device="cuda")
+    moments = torch.zeros((2, n), dtype=torch.float64, device="cuda")
     first = rank * nb
     stream = torch.cuda.current_stream()
+    st = ctypes.c_void_p(stream.cuda_stream)
 
     def one_step():
-        _lib.check(L.xs_run_path_device(path.h, first, nb, 1, None, ctypes.c_void_p(av.data_ptr()), None,
-                                        ctypes.c_void_p(stream.cuda_stream)))
-        # block moments (xensemble.m:98-101): sum over blocks of D and D^2 / nblocks
-        re = av[..., 0]
-        moments[0].copy_(re.sum(0) / nb)
-        moments[1].copy_((re * re).sum(0) / nb)
+        _lib.check(L.xs_run_path_device(path.h, first, nb, 1, None, ctypes.c_void_p(av.data_ptr()), None, st))
+        _lib.check(L.xs_block_moments(ctypes.c_void_p(av.data_ptr()), nb, n, 1.0 / (nb * world),
+                                      ctypes.c_void_p(moments.data_ptr()), 0, st))
         if dist is not None:
             dist.all_reduce(moments)
 
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         one_step()
     torch.cuda.synchronize()
+    _lib.check(L.xs_sync(path.h))
     L.xs_set_kernel_timing(path.h, 1)
     L.xs_kernel_stats(path.h, 1, None, None)
     if dist is not None:
@@ -285,39 +296,40 @@ def run_ours(args, rank, world, local_rank):
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with Clocks(local_rank) as clk:
         ev0.record(stream)
-        for _ in range(args.steps):
+        for _ in range(steps):
             one_step()
         ev1.record(stream)
         torch.cuda.synchronize()
     if dist is not None:
         dist.barrier()
-    ms = ev0.elapsed_time(ev1) / args.steps
+    ms = ev0.elapsed_time(ev1) / steps
     nk = len(_lib.KERNEL_KINDS)
     kms = (ctypes.c_double * nk)()
     kl = (ctypes.c_longlong * nk)()
     _lib.check(L.xs_kernel_stats(path.h, 1, kms, kl))
     L.xs_set_kernel_timing(path.h, 0)
+    _lib.check(L.xs_sync(path.h))
     clocks = clk.summary()
     t_max = torch.tensor([ms], dtype=torch.float64, device="cuda")
     if dist is not None:
         dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
     ms_max = float(t_max.item())
     value = world * ntraj * steps_per_traj / (ms_max / 1000.0)
-
+    kinds = _lib.KERNEL_KINDS
+    stats = {kinds[i]: {"launches": int(kl[i]), "ms": float(kms[i])} for i in range(nk) if kl[i]}
+    # the block-moment kernel runs once per step, outside the handle's counters
+    launches = sum(int(kl[i]) for i in range(nk)) + steps
+    out = {"value": value, "ms_per_step": ms_max, "steps": steps, "warmup": warmup, "kernels": stats,
+           "gpu_launches": launches, "clocks": clocks}
     if args.quick:
-        if rank == 0:
-            print(json.dumps({"quick": True, "value": value, "ms_per_step": ms_max,
-                              "kernels": {_lib.KERNEL_KINDS[i]: {"launches": int(kl[i]), "ms": float(kms[i])}
-                                          for i in range(nk) if kl[i]}}))
-        return
+        return out
     # end to end through the host C ABI (pinned host buffers, copies inside the timed region)
     a_in = torch.empty((ntraj * p.nspace * 2,), dtype=torch.float64, pin_memory=True)
     g = torch.Generator().manual_seed(1)
     a_in.normal_(0.0, 0.1 / math.sqrt(2), generator=g)
     a_in[0::2] += 1.0
-    per_block = path.per_block
-    av_host = torch.empty((nb * per_block,), dtype=torch.float64, pin_memory=True)
-    e2e_steps = max(1, min(args.steps, 3))
+    av_host = torch.empty((nb * path.per_block,), dtype=torch.float64, pin_memory=True)
+    e2e_steps = max(1, min(steps, 3))
     _lib.check(L.xs_run_path(path.h, first, nb, 1, ctypes.c_void_p(a_in.data_ptr()),
                              ctypes.c_void_p(av_host.data_ptr()), None))
     if dist is not None:
@@ -332,52 +344,75 @@ def run_ours(args, rank, world, local_rank):
     te = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
     if dist is not None:
         dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = world * ntraj * steps_per_traj / (float(te.item()) / 1000.0)
-
-    if rank != 0:
-        return
-    kinds = _lib.KERNEL_KINDS
-    stats = {kinds[i]: {"launches": int(kl[i]), "ms": float(kms[i])} for i in range(nk) if kl[i]}
+    out["e2e"] = {"value": world * ntraj * steps_per_traj / (float(te.item()) / 1000.0), "unit": "traj-steps/s",
+                  "h2d_bytes_per_step": int(a_in.numel() * 8), "d2h_bytes_per_step": int(av_host.numel() * 8),
+                  "steps": e2e_steps}
+    # roofline of the dominant kernel and of the whole MP step
     dom = max(("x_step", "y_pass", "rc_pass"), key=lambda k: stats.get(k, {"ms": 0})["ms"])
     per_launch_ms = stats[dom]["ms"] / stats[dom]["launches"]
     if dom == "rc_pass":
         # one fused launch: the row pass of one half of the trajectories and the column pass of the
         # other half, each one read and one write of its half's field
         traj_per_launch = ntraj / 2.0
-        alg_bytes = 2.0 * 2.0 * traj_per_launch * p.fields * p.nspace * 8
+        alg_bytes = 2.0 * 2.0 * traj_per_launch * p.fields * p.nspace * cxbytes
     else:
-        # one pass over every trajectory (both halves when the schedule is not fused)
-        launches_per_pass = max(1, round(stats[dom]["launches"] / float(args.steps * steps_per_traj)))
+        launches_per_pass = max(1, round(stats[dom]["launches"] / float(steps * steps_per_traj)))
         traj_per_launch = ntraj / launches_per_pass
-        alg_bytes = 2.0 * traj_per_launch * p.fields * p.nspace * 8  # read + write of the FP32 complex field
+        alg_bytes = 2.0 * traj_per_launch * p.fields * p.nspace * cxbytes  # read + write of the complex field
     achieved = alg_bytes / (per_launch_ms / 1000.0) / 1e9
     peak, kind = _peaks()
-    tr = NCU_TRAFFIC_PER_TRAJ.get(dom)
-    gpu_launches = sum(int(kl[i]) for i in range(nk))
-    fp64_line, fp32_err = _precision_report(ntraj)
-    cpu_val, cpu_desc = _cpu_sample()
+    tr = NCU_TRAFFIC_PER_TRAJ.get((dom, cxbytes))
+    bstep = 4.0 * p.fields * p.nspace * cxbytes
+    out["roofline"] = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                       "frac": achieved / peak, "peak_kind": kind, "traffic": (tr * traj_per_launch if tr else None),
+                       "algorithmic_bytes_per_launch": alg_bytes, "trajectories_per_launch": traj_per_launch}
+    out["step_roofline"] = {"bound": "hbm", "unit": "GB/s", "peak": peak,
+                            "achieved": value / world * bstep / 1e9, "frac": value / world * bstep / 1e9 / peak,
+                            "bytes_per_traj_step": bstep,
+                            "note": "whole MP step: two passes, each one read and one write of the field"}
+    return out
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    from xspde_matlab_b200 import xpreferences
+    torch.cuda.set_device(local_rank)
+    p32 = xpreferences([_problem(args.ntraj)])[0]
+    ntraj = p32.ensembles[0] * p32.ensembles[1] * p32.ensembles[2]
+    m32 = _measure(p32, args, rank, world, local_rank, args.steps, args.warmup, 8)
+    if args.quick:
+        if rank == 0:
+            print(json.dumps({"quick": True, "value": m32["value"], "ms_per_step": m32["ms_per_step"],
+                              "kernels": m32["kernels"]}))
+        return
+    torch.cuda.empty_cache()
+    # plain FP64 (the reference's own precision, c128), fewer steps: one step takes ~4 s
+    p64 = xpreferences([dict(_problem(args.ntraj), precision="fp64")])[0]
+    m64 = _measure(p64, args, rank, world, local_rank, max(3, min(args.steps, 5)), max(3, min(args.warmup, 3)), 16)
+    torch.cuda.empty_cache()
+    if rank != 0:
+        return
+    cpu, prec = _precision_vs_oracle()
+    fp64 = {k: m64[k] for k in ("value", "ms_per_step", "steps", "warmup", "e2e", "roofline", "step_roofline",
+                                "kernels", "clocks")}
+    fp64.update(unit="traj-steps/s", dtype="c128",
+                note="plain FP64 fields, transforms, drift, tables and moments (the reference's precision)")
     line = {
         "metric": METRIC,
-        "value": value, "unit": "traj-steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64",
+        "value": m32["value"], "unit": "traj-steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": m32["ms_per_step"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "c64", "precision_mode": "FP32 fields, transforms and drift; FP64 propagator tables and moments",
         "data": "synthetic (Philox initial field and noise, seed 0)",
         "config": _config(ntraj, world),
-        "e2e": {"value": e2e_value, "unit": "traj-steps/s",
-                "h2d_bytes_per_step": int(a_in.numel() * 8), "d2h_bytes_per_step": int(av_host.numel() * 8)},
-        "gpu_launches": gpu_launches * world // max(1, world),
-        "kernels": stats,
-        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "peak_kind": kind,
-                     "traffic": (tr * traj_per_launch if tr else None),
-                     "algorithmic_bytes_per_launch": alg_bytes, "trajectories_per_launch": traj_per_launch},
-        "step_roofline": {"bound": "hbm", "unit": "GB/s", "peak": peak,
-                          "achieved": value / world * 4.0 * p.fields * p.nspace * 8 / 1e9,
-                          "frac": value / world * 4.0 * p.fields * p.nspace * 8 / 1e9 / peak,
-                          "bytes_per_traj_step": 4.0 * p.fields * p.nspace * 8,
-                          "note": "whole MP step: two passes, each one read and one write of the field"},
-        "cpu_baseline": {"value": cpu_val, "unit": "traj-steps/s", "cores": 1, "kind": "port", "sample": cpu_desc},
-        "clocks": clocks,
-        "fp64": fp64_line, "fp32_vs_fp64": fp32_err,
+        "e2e": m32["e2e"],
+        "gpu_launches": m32["gpu_launches"],
+        "kernels": m32["kernels"],
+        "roofline": m32["roofline"],
+        "step_roofline": m32["step_roofline"],
+        "cpu_baseline": cpu,
+        "clocks": m32["clocks"],
+        "fp64": fp64,
+        "precision_vs_oracle": prec,
     }
     print(json.dumps(line))
 

@@ -246,6 +246,17 @@ XS_API xs_status xs_mlp_train_grad(int batch, int in, int hidden, const float* x
 XS_API xs_status xs_mlp_adam(size_t n, float* params, const float* grad, float* m, float* v, float lr, float beta1,
                              float beta2, float eps, int step, float weight_decay, void* stream);
 
+/* Ensemble moments of block means on the device (Simulator/xensemble.m:98-101,
+ * where xSPDE accumulates data(:,1) += D*nes and data(:,m1) += D.^2*nes with
+ * D = real(output(av)) and nes = 1/(ensembles(2)*ensembles(3))): av_dev holds
+ * nblocks consecutive blocks of n complex FP64 means (as xs_run_path_device
+ * writes them); mom_dev[k] = scale * sum_b Re(av[b][k]) and
+ * mom_dev[n + k] = scale * sum_b Re(av[b][k])^2 (FP64, compensated sums over
+ * the blocks in order), added to mom_dev's contents when accumulate != 0.
+ * Asynchronous on `stream` (NULL: the default stream); allocates nothing. */
+XS_API xs_status xs_block_moments(const double* av_dev, int nblocks, long long n, double scale, double* mom_dev,
+                                  int accumulate, void* stream);
+
 /* Kernel kinds counted by xs_kernel_stats. */
 enum {
   XS_KERNEL_RESIDENT = 0, /* whole path with fields in shared memory */

@@ -19,7 +19,7 @@ EXPORTS = ["xs_create", "xs_destroy", "xs_last_error", "xs_version", "xs_observe
            "xs_set_kernel_timing", "xs_kernel_stats", "xs_run_path_device_noalloc", "xs_noise_features",
            "xs_mlp_sizes", "xs_mlp_forward", "xs_mlp_train_grad", "xs_mlp_adam", "xs_batch_create",
            "xs_batch_destroy", "xs_batch_tune", "xs_batch_run", "xs_batch_sync", "xs_batch_av_doubles",
-           "xs_batch_results", "xs_batch_info", "xs_set_boundary_values", "xs_run_path_raw"]
+           "xs_batch_results", "xs_batch_info", "xs_set_boundary_values", "xs_run_path_raw", "xs_block_moments"]
 KERNEL_KINDS = ["resident", "obs_reduce", "x_init", "x_step", "x_final", "y_pass", "x_obs", "scalar", "rc_pass"]
 
 
@@ -149,6 +149,8 @@ def lib():
         L.xs_batch_info.restype = ci
         L.xs_set_boundary_values.argtypes = [vp, ci, ci, vp]
         L.xs_set_boundary_values.restype = ci
+        L.xs_block_moments.argtypes = [vp, ci, ctypes.c_longlong, ctypes.c_double, vp, ci, vp]
+        L.xs_block_moments.restype = ci
         _ = dp
         _lib = L
     return _lib

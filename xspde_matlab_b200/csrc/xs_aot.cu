@@ -58,3 +58,42 @@ extern "C" int xs_aot_av_matlab_launch(const void* src, void* dst, const XsAvMap
   xs_aot_av_matlab<<<(unsigned)blocks, 256, 0, st>>>((const double2*)src, (double2*)dst, *m, nblocks);
   return (int)cudaGetLastError();
 }
+
+// Ensemble moments over blocks (Simulator/xensemble.m:98-101): with D_b the
+// real part of block b's means, mom[k] (+)= scale * sum_b D_b[k] and
+// mom[n + k] (+)= scale * sum_b D_b[k]^2, blocks summed in order with
+// Neumaier compensation.  One thread per element; block reads are coalesced.
+extern "C" __global__ void xs_aot_block_moments(const double2* __restrict__ av, long long n, int nblocks, double scale,
+                                                double* __restrict__ mom, int accumulate) {
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+    double s1 = 0, c1 = 0, s2 = 0, c2 = 0;
+    for (int b = 0; b < nblocks; ++b) {
+      const double d = av[(long long)b * n + k].x;
+      double t = s1 + d;
+      c1 += fabs(s1) >= fabs(d) ? (s1 - t) + d : (d - t) + s1;
+      s1 = t;
+      const double d2 = d * d;
+      t = s2 + d2;
+      c2 += fabs(s2) >= fabs(d2) ? (s2 - t) + d2 : (d2 - t) + s2;
+      s2 = t;
+    }
+    const double m1 = (s1 + c1) * scale, m2 = (s2 + c2) * scale;
+    if (accumulate) {
+      mom[k] += m1;
+      mom[n + k] += m2;
+    } else {
+      mom[k] = m1;
+      mom[n + k] = m2;
+    }
+  }
+}
+
+extern "C" int xs_aot_block_moments_launch(const void* av, long long n, int nblocks, double scale, void* mom,
+                                            int accumulate, cudaStream_t st) {
+  long long blocks = (n + 255) / 256;
+  if (blocks > 148 * 32) blocks = 148 * 32;
+  if (blocks < 1) blocks = 1;
+  xs_aot_block_moments<<<(unsigned)blocks, 256, 0, st>>>((const double2*)av, n, nblocks, scale, (double*)mom,
+                                                         accumulate);
+  return (int)cudaGetLastError();
+}

@@ -14,3 +14,5 @@ struct XsAvMap {
 extern "C" int xs_aot_reorder_launch(const void* src, void* dst, int F, int NS, long long E, int to_device,
                                       cudaStream_t st);
 extern "C" int xs_aot_av_matlab_launch(const void* src, void* dst, const XsAvMap* m, int nblocks, cudaStream_t st);
+extern "C" int xs_aot_block_moments_launch(const void* av, long long n, int nblocks, double scale, void* mom,
+                                            int accumulate, cudaStream_t st);

@@ -2530,6 +2530,17 @@ XS_API xs_status xs_kernel_stats(xs_handle* h, int reset, double* ms_out, long l
   });
 }
 
+XS_API xs_status xs_block_moments(const double* av_dev, int nblocks, long long n, double scale, double* mom_dev,
+                                  int accumulate, void* stream) {
+  return guard([&]() -> xs_status {
+    if (!av_dev || !mom_dev || nblocks < 1 || n < 0) raise(XS_ERR_ARG, "bad arguments to xs_block_moments");
+    if (n == 0) return XS_OK;
+    CUDA_CHECK((cudaError_t)xs_aot_block_moments_launch(av_dev, n, nblocks, scale, mom_dev, accumulate ? 1 : 0,
+                                                        (cudaStream_t)stream));
+    return XS_OK;
+  });
+}
+
 namespace {
 xs_status export_normals(xs_handle* h, bool random, int block, int draw, double scale, double* out) {
   return guard([&]() -> xs_status {
