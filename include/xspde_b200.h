@@ -190,7 +190,9 @@ XS_API xs_status xs_run_path_device(xs_handle* h, int first_block, int nblocks, 
  * for check pass nc: call xs_run_path or xs_run_path_device once with the
  * same nc first (those calls allocate).  The first call on each device looks
  * up the array's device address (cudaGetSymbolAddress) and should come before
- * any stream capture.  Every call shares the one array per device, so calls
+ * any stream capture; the address is kept for the life of the process, so do
+ * not call this entry point again on a device after resetting it
+ * (cudaDeviceReset).  Its launches are not counted by xs_kernel_stats.  Every call shares the one array per device, so calls
  * that overlap on the GPU race; nothing in it needs to start at zero, since
  * each call writes every element it later reads.  The initial field comes
  * from p.initial on the device; av_dev is as for xs_run_path_device. */

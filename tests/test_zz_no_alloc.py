@@ -74,3 +74,31 @@ def test_noalloc_refuses_launch_larger_than_scratch():
                                       ctypes.c_void_p(stream.cuda_stream))
     assert rc == -1
     assert "fixed scratch holds 1048576" in _lib.last_error()
+
+
+def test_noalloc_refuses_handles_it_cannot_serve():
+    """The guards that keep the entry point from reading tables it does not
+    have: a check pass the handle has not run yet (its propagator tables are
+    missing: XS_ERR_ARG), a streaming-path handle and a handle whose field
+    lives in device memory (both would need allocated buffers:
+    XS_ERR_UNSUPPORTED)."""
+    import torch
+    from xspde_matlab_b200 import GpuPath, _lib, xpreferences
+    L = _lib.lib()
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    path = _path(SMALL)
+    av = _av(path, 1)
+    _lib.check(L.xs_run_path_device(path.h, 0, 1, 1, None, ctypes.c_void_p(av.data_ptr()), None, stream))
+    torch.cuda.synchronize()
+    assert L.xs_run_path_device_noalloc(path.h, 0, 1, 2, ctypes.c_void_p(av.data_ptr()), stream) == -7
+    assert "not prepared" in _lib.last_error()
+    lattice = dict(dimensions=3, points=[3, 64, 64], ranges=[0.2, 10.0, 10.0], steps=2, ensembles=[2, 1, 1],
+                   noises=2, method="MP", checks=0, deriv="@(a,w,p) -a + 0.01*w(1,:)", initial="@(v,p) 1 + 0*v(1,:)",
+                   linear="@(p) 0.1i*(p.Dx.^2+p.Dy.^2)", observe=["@(a,p) abs(a).^2"])
+    stream_path = GpuPath(xpreferences([lattice])[0], path_kind=2)
+    assert L.xs_run_path_device_noalloc(stream_path.h, 0, 1, 1, ctypes.c_void_p(av.data_ptr()), stream) == -9
+    assert "resident path only" in _lib.last_error()
+    big = dict(lattice, points=[3, 128, 128], precision="fp64")
+    gpath = GpuPath(xpreferences([big])[0], path_kind=1)
+    assert L.xs_run_path_device_noalloc(gpath.h, 0, 1, 1, ctypes.c_void_p(av.data_ptr()), stream) == -9
+    assert "shared memory" in _lib.last_error()

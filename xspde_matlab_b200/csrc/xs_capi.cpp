@@ -2281,9 +2281,6 @@ XS_API xs_status xs_sync(xs_handle* h) {
   });
 }
 
-// Resident path with its observable partial sums in the library's fixed
-// device scratch (xs_noalloc.cu) instead of handle-owned memory.  Uses only
-// tables the handle already holds; allocates nothing.
 XS_API xs_status xs_set_boundary_values(xs_handle* h, int nc, int ntimes, const double* values) {
   return guard([&]() -> xs_status {
     if (!h || (nc != 1 && nc != 2) || ntimes < 1 || !values) raise(XS_ERR_ARG, "bad arguments to xs_set_boundary_values");
@@ -2318,6 +2315,11 @@ XS_API xs_status xs_set_boundary_values(xs_handle* h, int nc, int ntimes, const 
   });
 }
 
+// Resident path with its observable partial sums in the library's fixed
+// device scratch (xs_noalloc.cu) instead of handle-owned memory.  Uses only
+// tables the handle already holds; allocates nothing.  Its two launches go
+// straight to the driver, without the handle's timing events (creating those
+// would allocate), and are not counted by xs_kernel_stats.
 XS_API xs_status xs_run_path_device_noalloc(xs_handle* h, int first_block, int nblocks, int nc, double* av_dev,
                                             void* stream) {
   return guard([&]() -> xs_status {
@@ -2380,7 +2382,6 @@ XS_API xs_status xs_run_path_device_noalloc(xs_handle* h, int first_block, int n
     cu_check(driver().launch(h->f_resident, nctas, 1, 1, h->rp.threads, 1, 1, (unsigned)h->rp.smem, (CUstream)st,
                              params, nullptr),
              "launch xs_resident (no-alloc)");
-    h->launches[XS_KERNEL_RESIDENT]++;
     if (stride > 0) {
       const void* part = scratch;
       void* av = av_dev;
@@ -2392,7 +2393,6 @@ XS_API xs_status xs_run_path_device_noalloc(xs_handle* h, int first_block, int n
       cu_check(driver().launch(h->f_reduce, (unsigned)((stride + 127) / 128), (unsigned)npts, (unsigned)nblocks, 128,
                                1, 1, 0, (CUstream)st, rparams, nullptr),
                "launch xs_obs_reduce (no-alloc)");
-      h->launches[XS_KERNEL_OBS_REDUCE]++;
     }
     return XS_OK;
   });

@@ -19,8 +19,12 @@ void* g_addr[XS_NOALLOC_MAX_DEVICES] = {};
 
 // Device address of the scratch array on the current device.  Host code may
 // not use the array's name as a device pointer, so the address is looked up
-// once per device with that device current and cached.  Returns the CUDA
-// error of the lookup (cudaSuccess when *out is valid).
+// once per device with that device current and cached.  The cache assumes the
+// device's primary context lives as long as the process: after a
+// cudaDeviceReset (or a MATLAB gpuDevice reset) the module is loaded again and
+// the cached address is stale, so a caller that resets a device must not call
+// xs_run_path_device_noalloc on it again in the same process.  Returns the
+// CUDA error of the lookup (cudaSuccess when *out is valid).
 cudaError_t xs_noalloc_scratch_address(void** out) {
   int dev = -1;
   cudaError_t e = cudaGetDevice(&dev);
