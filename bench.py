@@ -116,16 +116,16 @@ class Clocks:
                 "samples": len(sm)}
 
 
-def _config(ntraj, world):
+def _config(ntraj, world, method="MP"):
     return {"workload": "gpe_2d: 256x256 periodic, %d trajectories per GPU (%d blocks x 256), 51 points x 10 steps"
-                        " = 509 MP steps, observable <|a|^2>(x,y,t)" % (ntraj, ntraj // 256),
+                        " = 509 %s steps, observable <|a|^2>(x,y,t)" % (ntraj, ntraj // 256, method),
             "global_batch": world * ntraj, "l2": "field 2.1 GB per pass > 126 MB L2 (no flush needed)",
             "parallelism": "dp%d (blocks per rank)" % world}
 
 
-def _problem(ntraj=4096):
+def _problem(ntraj=4096, method="MP"):
     from xspde_matlab_b200.problems import GPE_2D
-    p = dict(GPE_2D)
+    p = dict(GPE_2D, method=method)
     p["ensembles"] = [256, max(1, ntraj // 256), 1]
     return p
 
@@ -347,14 +347,20 @@ def _measure(p, args, rank, world, local_rank, steps, warmup, cxbytes):
     out["e2e"] = {"value": world * ntraj * steps_per_traj / (float(te.item()) / 1000.0), "unit": "traj-steps/s",
                   "h2d_bytes_per_step": int(a_in.numel() * 8), "d2h_bytes_per_step": int(av_host.numel() * 8),
                   "steps": e2e_steps}
-    # roofline of the dominant kernel and of the whole MP step
+    # roofline of the dominant kernel and of the whole step
+    rk4 = p.method == "RK4"
     dom = max(("x_step", "y_pass", "rc_pass"), key=lambda k: stats.get(k, {"ms": 0})["ms"])
+    if rk4:
+        dom = "y_pass"  # RK4 row passes move two to four field passes each; the column pass two
     per_launch_ms = stats[dom]["ms"] / stats[dom]["launches"]
     if dom == "rc_pass":
         # one fused launch: the row pass of one half of the trajectories and the column pass of the
         # other half, each one read and one write of its half's field
         traj_per_launch = ntraj / 2.0
         alg_bytes = 2.0 * 2.0 * traj_per_launch * p.fields * p.nspace * cxbytes
+    elif rk4:
+        traj_per_launch = float(ntraj)  # every column pass covers all trajectories of one of the two fields
+        alg_bytes = 2.0 * traj_per_launch * p.fields * p.nspace * cxbytes
     else:
         launches_per_pass = max(1, round(stats[dom]["launches"] / float(steps * steps_per_traj)))
         traj_per_launch = ntraj / launches_per_pass
@@ -362,14 +368,15 @@ def _measure(p, args, rank, world, local_rank, steps, warmup, cxbytes):
     achieved = alg_bytes / (per_launch_ms / 1000.0) / 1e9
     peak, kind = _peaks()
     tr = NCU_TRAFFIC_PER_TRAJ.get((dom, cxbytes))
-    bstep = 4.0 * p.fields * p.nspace * cxbytes
+    bstep = (16.0 if rk4 else 4.0) * p.fields * p.nspace * cxbytes
     out["roofline"] = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                        "frac": achieved / peak, "peak_kind": kind, "traffic": (tr * traj_per_launch if tr else None),
                        "algorithmic_bytes_per_launch": alg_bytes, "trajectories_per_launch": traj_per_launch}
     out["step_roofline"] = {"bound": "hbm", "unit": "GB/s", "peak": peak,
                             "achieved": value / world * bstep / 1e9, "frac": value / world * bstep / 1e9 / peak,
                             "bytes_per_traj_step": bstep,
-                            "note": "whole MP step: two passes, each one read and one write of the field"}
+                            "note": ("whole RK4 step: four passes over two fields, each one read and one write"
+                                     if rk4 else "whole MP step: two passes, each one read and one write of the field")}
     return out
 
 
@@ -377,13 +384,18 @@ def run_ours(args, rank, world, local_rank):
     import torch
     from xspde_matlab_b200 import xpreferences
     torch.cuda.set_device(local_rank)
-    p32 = xpreferences([_problem(args.ntraj)])[0]
+    p32 = xpreferences([_problem(args.ntraj, args.method)])[0]
     ntraj = p32.ensembles[0] * p32.ensembles[1] * p32.ensembles[2]
     m32 = _measure(p32, args, rank, world, local_rank, args.steps, args.warmup, 8)
-    if args.quick:
+    if args.quick or args.method != "MP":
         if rank == 0:
-            print(json.dumps({"quick": True, "value": m32["value"], "ms_per_step": m32["ms_per_step"],
-                              "kernels": m32["kernels"]}))
+            out = {"quick": args.quick, "method": args.method, "value": m32["value"], "unit": "traj-steps/s",
+                   "ms_per_step": m32["ms_per_step"], "kernels": m32["kernels"], "clocks": m32["clocks"],
+                   "config": _config(ntraj, world, args.method)}
+            for k in ("e2e", "roofline", "step_roofline"):
+                if k in m32:
+                    out[k] = m32[k]
+            print(json.dumps(out))
         return
     torch.cuda.empty_cache()
     # plain FP64 (the reference's own precision, c128), fewer steps: one step takes ~4 s
@@ -790,6 +802,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--ntraj", type=int, default=4096, help="trajectories per GPU (multiple of 256)")
     ap.add_argument("--quick", action="store_true", help="device timing only (no e2e, no CPU sample)")
+    ap.add_argument("--method", default="MP", choices=["MP", "RK4"],
+                    help="stepper of the 256x256 problem (RK4: FP32 line with e2e and roofline only)")
     ap.add_argument("--cv", action="store_true", help="second headline: time to 1e-3 sampling error, "
                                                       "plain FP64 vs FP32 + learned control variate")
     ap.add_argument("--cv-sets", default="", help="JSON list of noise-feature sets [[region6], steps, windows, gap]")

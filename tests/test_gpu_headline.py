@@ -25,11 +25,11 @@ FP64_TOL = 1e-10
 FP32_TOL = 1e-5
 
 
-def _gpe_256(precision, checks=1, ens=(2, 2, 1), points=3):
+def _gpe_256(precision, checks=1, ens=(2, 2, 1), points=3, method="MP"):
     """The benchmark's 256x256 problem with the benchmark's step (dtr = 0.01)
     over a shorter time: `points` output times, 10 steps between them."""
     base = dict(dimensions=3, points=[points, 256, 256], ranges=[0.1 * (points - 1), 20.0, 20.0], steps=10,
-                ensembles=list(ens), noises=2, method="MP", checks=checks)
+                ensembles=list(ens), noises=2, method=method, checks=checks)
     g = dict(base, precision=precision,
              deriv="@(a,w,p) (1-abs(a).^2).*a - 0.5i*abs(a).^2.*a + 0.05*(w(1,:)+1i*w(2,:))/sqrt(2)",
              initial="@(v,p) 1 + 0.1*(v(1,:)+1i*v(2,:))/sqrt(2)", linear="@(p) (1i+0.1)*(p.Dx.^2+p.Dy.^2)",
@@ -88,6 +88,15 @@ def test_gpe_256x256_streaming_fp64_longer_path():
     g, o = _gpe_256("fp64", checks=0, ens=(2, 1, 1), points=11)
     av_g, a_g = _stream(g, [3], 1)
     _check_blocks(av_g, a_g, o, [3], 1, FP64_TOL, 2)
+
+
+@pytest.mark.parametrize("nc", [1, 2])
+def test_gpe_256x256_streaming_rk4_fp64_matches_oracle(nc):
+    """RK4 (the reference's default deterministic stepper, Applications/SDE/RK4.m:7-42)
+    on the 256x256 streaming path: both check passes, observables and final field."""
+    g, o = _gpe_256("fp64", method="RK4")
+    av_g, a_g = _stream(g, [0, 1], nc)
+    _check_blocks(av_g, a_g, o, [0, 1], nc, FP64_TOL, 2)
 
 
 SNLS_FULL = dict(dimensions=2, points=[51, 64], ranges=[1.0, 10.0], steps=4, ensembles=[128, 8, 1], noises=2)

@@ -14,9 +14,9 @@ from tests.gpu_util import oracle_block_av, rel_err
 pytestmark = pytest.mark.gpu
 
 
-def _case(checks, precision="fp64", points=(5, 64, 64), ens=(4, 2, 1), obs_int=True):
+def _case(checks, precision="fp64", points=(5, 64, 64), ens=(4, 2, 1), obs_int=True, method="MP"):
     base = dict(dimensions=3, points=list(points), ranges=[0.2, 12.0, 10.0], steps=2, ensembles=list(ens), noises=2,
-                method="MP", checks=checks)
+                method=method, checks=checks)
     gobs = ["@(a,p) abs(a).^2", "@(a,p) real(a)"]
     oobs = [lambda a, p: abs(a) ** 2, lambda a, p: np.real(a)]
     if obs_int:
@@ -145,3 +145,44 @@ def test_stream_fused_halves_bit_identical(precision, monkeypatch):
         for b in range(4):
             for k in range(len(av_a[b])):
                 assert np.array_equal(av_a[b][k], av_b[b][k]), (nc, b, k)
+
+
+@pytest.mark.parametrize("checks", [0, 1])
+def test_stream_rk4_fp64_matches_oracle(checks):
+    """RK4 on the streaming kernels (Applications/SDE/RK4.m:7-42): two fields in HBM,
+    three row passes and column passes on both fields per step, one noise for all
+    stages; block means and the final field against the oracle at 1e-10, both
+    check passes (the coarse pass averages two fine draws)."""
+    g, o = _case(checks, method="RK4")
+    for nc in ([1, 2] if checks else [1]):
+        av_g, a_g = _run(g, [0, 1], nc, a_out=True)
+        for i, b in enumerate([0, 1]):
+            av_o, a_o = oracle_block_av(o, b, nc)
+            for k in range(len(av_o)):
+                e = rel_err(av_g[i][k].reshape(-1, order="F"), av_o[k].reshape(-1, order="F"))
+                assert e < 1e-10, (nc, b, k, e)
+            e = rel_err(a_g[..., 4 * i:4 * (i + 1)], a_o)
+            assert e < 1e-10, (nc, b, "field", e)
+
+
+def test_stream_rk4_fp32_bound():
+    g, o = _case(1, precision="fp32", method="RK4")
+    for nc in (1, 2):
+        av_g, _ = _run(g, [1], nc)
+        av_o, _ = oracle_block_av(o, 1, nc)
+        for k in range(len(av_o)):
+            e = rel_err(av_g[0][k].reshape(-1, order="F"), av_o[k].reshape(-1, order="F"))
+            assert e < 2e-4, (nc, k, e)
+
+
+def test_stream_rk4_single_output_time_every_step_observed():
+    """steps = 1: every step is followed by an observation, so no pass 3 is fused
+    with the next step's pass 1; with steps = 2 (above) every other one is."""
+    g, o = _case(0, points=(4, 64, 64), method="RK4", obs_int=False)
+    g = dict(g, steps=1)
+    o = dict(o, steps=1)
+    av_g, a_g = _run(g, [0], 1, a_out=True)
+    av_o, a_o = oracle_block_av(o, 0, 1)
+    assert rel_err(a_g, a_o) < 1e-10
+    for k in range(len(av_o)):
+        assert rel_err(av_g[0][k].reshape(-1, order="F"), av_o[k].reshape(-1, order="F")) < 1e-10

@@ -47,6 +47,9 @@ struct XsStreamArgs {
   const cx* tw_x;            // [RX*RX] four-step twiddles of the rows, built in FP64 on the host
   const cx* tw_y;            // [RY*RY] four-step twiddles of the columns
   double2* opart;            // [gridDim.z][nblocks][XS_NOUT_SITE * NS] per-split sums of xs_x_obs
+  cx* field2;                // RK4: the second field (a1, then a3) [ntraj][F][NS], K state
+  int ndraw0, ndraw1;        // RK4 row pass 3 fused with the next step's pass 1: that step's draws
+  int fuse;                  // RK4 row pass 3: 1 = also do the next step's pass 1
 };
 
 #define XS_RX XS_FFT_RX
@@ -304,6 +307,147 @@ __device__ __forceinline__ void xs_xpass_body(const XsStreamArgs& A) {
 extern "C" __global__ void __launch_bounds__(256) xs_x_init(const XsStreamArgs A) { xs_xpass_body<0>(A); }
 extern "C" __global__ void __launch_bounds__(256) xs_x_nl(const XsStreamArgs A) { xs_xpass_body<1>(A); }
 extern "C" __global__ void __launch_bounds__(256) xs_x_final(const XsStreamArgs A) { xs_xpass_body<3>(A); }
+
+// ---- RK4 row passes ------------------------------------------------------------
+// Interaction-picture RK4 (Applications/SDE/RK4.m:7-42) with dt = dtr/2 and P the
+// half-step propagator exp(L dtr/2) (applied by column passes on the field it
+// acts on), one noise w for every stage of a step:
+//   pass 1 (MODE 4):  a1 = a + dt D(a, t)                          -> field2
+//   column passes:    a1 = P a1, a = P a
+//   pass 2 (MODE 5):  a2 = a + dt D(a1, t + dt), a3 = a + 2 dt D(a2, t + dt),
+//                     a = (a1 + 2 a2 + a3 - a)/3 -> field, a3 -> field2
+//   column passes:    a = P a, a3 = P a3
+//   pass 3 (MODE 6):  a = a + dt/3 D(a3, t + 2 dt)                 -> field
+//                     (fuse: and the next step's pass 1 at the same time)
+// Both fields stay in the K state between passes; pass 1 reads a but does not
+// write it back.  Per step: 16 N F s bytes (four passes over two fields).
+// Shared memory per row: two stages of XS_XLINE elements (field, field2), each
+// also the transpose scratch of its field's transforms.
+#define XS_XSMEM_RK (XS_RX * XS_RX + 2 * XS_XROWS * XS_XLINE)
+
+template <int MODE>
+__device__ __forceinline__ void xs_rk4_row(const XsStreamArgs& A) {
+  if ((size_t)(blockIdx.x + 1) * XS_XROWS > (size_t)A.ntraj * XS_NY || blockDim.x != 256) {
+    if (threadIdx.x == 0) atomicOr(A.status, 2);
+    return;
+  }
+  if (!xs_smem_ok(XS_XSMEM_RK * sizeof(cx), A.status)) return;
+  cx* tw = (cx*)xs_dsmem;
+  xs_fill_twiddles<XS_RX>(tw, A.tw_x);
+  __syncthreads();
+  const int r = threadIdx.x / XS_RX, t = threadIdx.x % XS_RX;
+  cx* sa = tw + XS_RX * XS_RX + (2 * r) * XS_XLINE;  // field a: stage and transpose scratch
+  cx* sb = sa + XS_XLINE;                             // field2
+  const size_t cta = blockIdx.x;
+  const int e = (int)((cta * XS_XROWS) / XS_NY), y = (int)((cta * XS_XROWS + r) % XS_NY);
+  const u32 blk = (u32)(A.block0 + e / A.ens1), el = (u32)(e % A.ens1);
+  const size_t off = ((size_t)e * XS_F) * XS_NS + (size_t)y * XS_NX + t;
+  XsWarpSync ws;
+  // one field from HBM (K state) into its stage in x space
+  auto load_x = [&](const cx* src, cx* st) {
+    cx v[XS_F][XS_RX];
+#pragma unroll
+    for (int f = 0; f < XS_F; ++f)
+#pragma unroll
+      for (int j = 0; j < XS_RX; ++j) v[f][j] = src[off + (size_t)f * XS_NS + XS_RX * j];
+#pragma unroll
+    for (int f = 0; f < XS_F; ++f) xs_ifft4<XS_RX, 1, 1>(v[f], t, tw, st, ws);
+#pragma unroll
+    for (int f = 0; f < XS_F; ++f)
+#pragma unroll
+      for (int j = 0; j < XS_RX; ++j) st[(f * XS_RX + j) * XS_RX + t] = v[f][j];
+  };
+  // one stage back to HBM in the K state
+  auto store_k = [&](cx* st, cx* dst) {
+    cx v[XS_F][XS_RX];
+#pragma unroll
+    for (int f = 0; f < XS_F; ++f)
+#pragma unroll
+      for (int j = 0; j < XS_RX; ++j) v[f][j] = st[(f * XS_RX + j) * XS_RX + t];
+    __syncwarp();  // the transforms reuse the stage as scratch
+#pragma unroll
+    for (int f = 0; f < XS_F; ++f) xs_fft4<XS_RX, 1, 1>(v[f], t, tw, st, ws);
+#pragma unroll
+    for (int f = 0; f < XS_F; ++f)
+#pragma unroll
+      for (int j = 0; j < XS_RX; ++j) dst[off + (size_t)f * XS_NS + XS_RX * j] = v[f][j];
+  };
+  load_x(A.field, sa);
+  if (MODE != 4) load_x(A.field2, sb);
+  __syncwarp();
+  const real dt = (real)(A.dtr * 0.5);
+  const real t0 = (real)A.t, t1 = (real)(A.t + A.dtr * 0.5), t2 = (real)(A.t + A.dtr);
+  const real ws_ = (real)A.wscale;
+  // noise of element j (site t + RX j of row y) for the draws (d0, d1 >= 0: coarse average)
+  auto noise = [&](int j, int d0, int d1, real* w) {
+#if XS_NW > 0
+    const u32 s = (u32)(y * XS_NX + t + XS_RX * j);
+    xs_normals_site<XS_NW>(w, s, el, (u32)d0, (u32)A.seq, A.seed, blk);
+    if (d1 >= 0) {
+      real w2[XS_NW];
+      xs_normals_site<XS_NW>(w2, s, el, (u32)d1, (u32)A.seq, A.seed, blk);
+#pragma unroll
+      for (int c = 0; c < XS_NW; ++c) w[c] = (w[c] * ws_ + w2[c] * ws_) * (real)0.5;
+    } else {
+#pragma unroll
+      for (int c = 0; c < XS_NW; ++c) w[c] = w[c] * ws_;
+    }
+#else
+    (void)j; (void)d0; (void)d1; w[0] = (real)0;
+#endif
+  };
+#pragma unroll 1
+  for (int j = 0; j < XS_RX; ++j) {
+    real x, yy;
+    xs_row_coords(y, t, j, x, yy);
+    real w[XS_NW > 0 ? XS_NW : 1];
+    noise(j, A.draw0, A.draw1, w);
+    cx a[XS_F], b[XS_F], d[XS_F];
+#pragma unroll
+    for (int f = 0; f < XS_F; ++f) a[f] = sa[(f * XS_RX + j) * XS_RX + t];
+    if (MODE == 4) {  // a1 = a + dt D(a, t)
+      xs_deriv(a, w, (const cx*)nullptr, x, yy, (real)0, t0, A.params, (const cx*)nullptr, 0, 0, d);
+#pragma unroll
+      for (int f = 0; f < XS_F; ++f) sb[(f * XS_RX + j) * XS_RX + t] = a[f] + dt * d[f];
+    } else if (MODE == 5) {
+      cx a1[XS_F], a2[XS_F];
+#pragma unroll
+      for (int f = 0; f < XS_F; ++f) a1[f] = sb[(f * XS_RX + j) * XS_RX + t];
+      xs_deriv(a1, w, (const cx*)nullptr, x, yy, (real)0, t1, A.params, (const cx*)nullptr, 0, 0, d);
+#pragma unroll
+      for (int f = 0; f < XS_F; ++f) a2[f] = a[f] + dt * d[f];
+      xs_deriv(a2, w, (const cx*)nullptr, x, yy, (real)0, t1, A.params, (const cx*)nullptr, 0, 0, d);
+#pragma unroll
+      for (int f = 0; f < XS_F; ++f) {
+        b[f] = a[f] + (real)2 * dt * d[f];  // a3
+        sa[(f * XS_RX + j) * XS_RX + t] = (a1[f] + (real)2 * a2[f] + b[f] - a[f]) / (real)3;
+        sb[(f * XS_RX + j) * XS_RX + t] = b[f];
+      }
+    } else {  // MODE 6: a = a + dt/3 D(a3, t + 2 dt), then the next step's pass 1
+#pragma unroll
+      for (int f = 0; f < XS_F; ++f) b[f] = sb[(f * XS_RX + j) * XS_RX + t];
+      xs_deriv(b, w, (const cx*)nullptr, x, yy, (real)0, t2, A.params, (const cx*)nullptr, 0, 0, d);
+#pragma unroll
+      for (int f = 0; f < XS_F; ++f) {
+        a[f] = a[f] + d[f] * dt / (real)3;
+        sa[(f * XS_RX + j) * XS_RX + t] = a[f];
+      }
+      if (A.fuse) {
+        noise(j, A.ndraw0, A.ndraw1, w);
+        xs_deriv(a, w, (const cx*)nullptr, x, yy, (real)0, t2, A.params, (const cx*)nullptr, 0, 0, d);
+#pragma unroll
+        for (int f = 0; f < XS_F; ++f) sb[(f * XS_RX + j) * XS_RX + t] = a[f] + dt * d[f];
+      }
+    }
+  }
+  __syncwarp();
+  if (MODE != 4) store_k(sa, A.field);
+  if (MODE != 6 || A.fuse) store_k(sb, A.field2);
+}
+
+extern "C" __global__ void __launch_bounds__(256) xs_x_rk1(const XsStreamArgs A) { xs_rk4_row<4>(A); }
+extern "C" __global__ void __launch_bounds__(256) xs_x_rk2(const XsStreamArgs A) { xs_rk4_row<5>(A); }
+extern "C" __global__ void __launch_bounds__(256) xs_x_rk3(const XsStreamArgs A) { xs_rk4_row<6>(A); }
 
 // ---- column pass ------------------------------------------------------------
 // CTA = TX consecutive kx columns of one (trajectory, component); thread

@@ -900,6 +900,7 @@ struct ResidentPlan {
 struct StreamPlan {
   int RX = 0, RY = 0, XROWS = 0, TX = 0, OROWS = 0;
   size_t xsmem = 0, ssmem = 0, osmem = 0, tsmem = 0;
+  size_t rksmem = 0;  // RK4 row passes: twiddles + two stages per row
 };
 
 }  // namespace
@@ -918,6 +919,8 @@ struct xs_handle {
   CUfunction f_xcomb = nullptr;  // adds the trajectory splits of xs_x_obs
   CUfunction f_xinit = nullptr, f_xnl = nullptr, f_xfinal = nullptr, f_spass = nullptr, f_xobs = nullptr,
              f_scalar = nullptr;
+  CUfunction f_xrk[3] = {nullptr, nullptr, nullptr};  // RK4 row passes 1, 2, 3 (streaming)
+  DevBuf d_field2;                                      // RK4: second streaming field
   StreamPlan sp;
   int path_kind = 0;
   int force_G = 0, force_threads = 0;  // resident tile fixed by the caller (uneven batch)
@@ -1177,7 +1180,7 @@ std::string stream_blocker(const Problem& P) {
   if (!isqrt_pow2(P.N[0]) || !isqrt_pow2(P.N[1])) return "streaming lattices need 64, 256 or 1024 points per dimension";
   for (int v : P.bnd)
     if (v) return "the streaming path covers periodic boundaries";
-  if (P.p.method != XS_METHOD_MP) return "the streaming path integrates with MP";
+  if (P.p.method != XS_METHOD_MP && P.p.method != XS_METHOD_RK4) return "the streaming path integrates with MP or RK4";
   if (!P.has_linear) return "the streaming path needs p.linear";
   for (auto& o : P.obs)
     if (o.spatial && !o.gen.reductions.empty()) return "site observables that use Int/Ave are not streamed";
@@ -1249,6 +1252,7 @@ void plan_stream(xs_handle& h) {
   // mbarriers, alignment slack
   sp.tsmem = 2 * (size_t)P.N[1] * sp.TX * cxs + (size_t)sp.RY * sp.RY * cxs + 16 + 128;
   sp.osmem = (size_t)(sp.RX * sp.RX + sp.OROWS * sp.RX * (sp.RX + 1)) * cxs;
+  sp.rksmem = (sp.RX * sp.RX + 2 * sp.XROWS * xline) * cxs;
   if (P.N[1] % sp.XROWS || P.N[1] % sp.OROWS || P.N[0] % sp.TX)
     raise(XS_ERR_SHAPE, "internal: streaming tile sizes do not divide the lattice");
   h.sp = sp;
@@ -1402,7 +1406,7 @@ void load_module(xs_handle& h) {
       // opt-in (measured slower than the plain column pass at this tile size: 1.07 vs 0.94 ms per
       // launch at 4096 trajectories, 24 vs 32 warps per SM)
       const char* e = getenv("XSPDE_B200_TMA");
-      h.tma = h.P.N[1] <= 256 && e && *e == '1';
+      h.tma = h.P.N[1] <= 256 && e && *e == '1' && h.P.p.method == XS_METHOD_MP;
       if (h.tma) {
         cu_check(d.getfn(&h.f_spass_tma, h.mod, "xs_s_pass_tma"), "xs_s_pass_tma");
         if (h.sp.tsmem > 48 * 1024)
@@ -1414,6 +1418,14 @@ void load_module(xs_handle& h) {
         cu_check(d.occupancy(&occ, h.f_spass_tma, 256, h.sp.tsmem), "occupancy");
         if (occ < 1) raise(XS_ERR_UNSUPPORTED, "TMA column pass cannot be resident on an SM");
         h.tma_grid = sms * occ;
+      }
+    }
+    if (h.P.p.method == XS_METHOD_RK4) {
+      const char* names[3] = {"xs_x_rk1", "xs_x_rk2", "xs_x_rk3"};
+      for (int i = 0; i < 3; ++i) {
+        cu_check(d.getfn(&h.f_xrk[i], h.mod, names[i]), names[i]);
+        if (h.sp.rksmem > 48 * 1024)
+          cu_check(d.setattr(h.f_xrk[i], CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, (int)h.sp.rksmem), names[i]);
       }
     }
     cu_check(d.getfn(&h.f_feat, h.mod, "xs_noise_features"), "xs_noise_features");
@@ -1782,6 +1794,9 @@ struct StreamArgsHost {
   const void* tw_x;
   const void* tw_y;
   void* opart;
+  void* field2;
+  int ndraw0, ndraw1;
+  int fuse;
 };
 
 // Observation pass: each block's trajectories split over kObsSplit CTAs (grid z) for latency
@@ -1996,6 +2011,72 @@ void launch_stream(xs_handle& h, int first_block, int nblocks, int nc, const voi
     if (P.nout_scalar)
       xs_launch(h, XS_KERNEL_SCALAR, h.f_scalar, (unsigned)nblocks, 1, 1, 256, 0, st, params, "scalar observables");
   };
+  if (P.p.method == XS_METHOD_RK4) {
+    // RK4 (Applications/SDE/RK4.m:7-42): row passes 1, 2, 3 on the two fields with column
+    // passes P on both in between; pass 3 also does the next step's pass 1 unless the field
+    // is observed in between
+    h.d_field2.ensure((size_t)total * P.F * P.NS * cxs);
+    a.field2 = h.d_field2.p;
+    struct RkOp {
+      bool obs;
+      int n, d0, d1;
+    };
+    std::vector<RkOp> ops;
+    {
+      int draw = 0, prev = -1;
+      const int npts = P.p.points[0], S = P.p.steps, checks = P.p.checks;
+      for (int n = 0; n < npts; ++n)
+        for (int step = 0; step < S; ++step) {
+          if (n > 0 || step > 0 || npts == 1)
+            for (int chk = 0; chk <= checks; ++chk) {
+              ++draw;
+              if (nc == 2 && checks && chk == 0) {
+                prev = draw;
+                continue;
+              }
+              ops.push_back({false, 0, draw, (nc == 2 && checks) ? prev : -1});
+            }
+          if (step == 0) ops.push_back({true, n, 0, -1});
+        }
+    }
+    auto rk = [&](int i) {
+      xs_launch(h, XS_KERNEL_X_STEP, h.f_xrk[i], xgrid, 1, 1, 256, (unsigned)sp.rksmem, st, params, "RK4 row pass");
+    };
+    auto col_both = [&]() {
+      a.m = 1;
+      xs_launch(h, XS_KERNEL_Y_PASS, h.f_spass, sgrid, 1, 1, 256, (unsigned)sp.ssmem, st, params, "column pass");
+      StreamArgsHost b = a;
+      b.field = a.field2;
+      void* bp[] = {&b};
+      xs_launch(h, XS_KERNEL_Y_PASS, h.f_spass, sgrid, 1, 1, 256, (unsigned)sp.ssmem, st, bp, "column pass");
+    };
+    row(XS_KERNEL_X_INIT, h.f_xinit);
+    bool pass1_done = false;
+    for (size_t i = 0; i < ops.size(); ++i) {
+      if (ops[i].obs) {
+        observe(ops[i].n);
+        continue;
+      }
+      a.draw0 = ops[i].d0;
+      a.draw1 = ops[i].d1;
+      a.fuse = 0;
+      if (!pass1_done) rk(0);
+      col_both();
+      rk(1);
+      col_both();
+      const bool next = i + 1 < ops.size() && !ops[i + 1].obs;
+      a.fuse = next ? 1 : 0;
+      if (next) {
+        a.ndraw0 = ops[i + 1].d0;
+        a.ndraw1 = ops[i + 1].d1;
+      }
+      rk(2);
+      pass1_done = next;
+      a.t += a.dtr;
+    }
+    if (a_out_dev) row(XS_KERNEL_X_FINAL, h.f_xfinal);
+    return;
+  }
   if (h.fuse && h.f_rc && !h.tma && nblocks >= 2 && nblocks % 2 == 0) {
     launch_stream_halves(h, a, nblocks, nc, av_dev, st);
     return;
