@@ -2538,10 +2538,14 @@ XS_API xs_status xs_mlp_forward(int batch, int in, int hidden, const float* x, c
     g_err = "bad arguments to xs_mlp_forward";
     return XS_ERR_ARG;
   }
-  int e = xs_mlp_forward_impl(batch, in, hidden, x, params, work, y, (cudaStream_t)stream);
+  int e = xs_mlp_forward_impl(batch, in, hidden, x, params, work, y, (cudaStream_t)stream, false);
   if (e) {
     g_err = std::string("xs_mlp_forward: ") + cudaGetErrorString((cudaError_t)e);
     return XS_ERR_CUDA;
+  }
+  if (xs_mlp_status((cudaStream_t)stream)) {
+    g_err = "xs_mlp_forward: a tensor-core layer gave up waiting for its operands";
+    return XS_ERR_TIMEOUT;
   }
   return XS_OK;
 }
@@ -2552,11 +2556,15 @@ XS_API xs_status xs_mlp_train_grad(int batch, int in, int hidden, const float* x
     g_err = "bad arguments to xs_mlp_train_grad";
     return XS_ERR_ARG;
   }
-  int e = xs_mlp_forward_impl(batch, in, hidden, x, params, work, nullptr, (cudaStream_t)stream);
+  int e = xs_mlp_forward_impl(batch, in, hidden, x, params, work, nullptr, (cudaStream_t)stream, true);
   if (!e) e = xs_mlp_backward_impl(batch, in, hidden, x, params, work, target, grad, loss_dev, (cudaStream_t)stream);
   if (e) {
     g_err = std::string("xs_mlp_train_grad: ") + cudaGetErrorString((cudaError_t)e);
     return XS_ERR_CUDA;
+  }
+  if (xs_mlp_status((cudaStream_t)stream)) {
+    g_err = "xs_mlp_train_grad: a tensor-core layer gave up waiting for its operands";
+    return XS_ERR_TIMEOUT;
   }
   return XS_OK;
 }

@@ -2,16 +2,24 @@
 // in -> H -> H -> H -> 1 with GELU activations, BF16 operands and FP32
 // accumulation on the tensor cores, trained with hand-written forward,
 // backward, loss and Adam kernels.  Parameters are kept as an FP32 master
-// vector and rounded to BF16 when a GEMM tile is staged in shared memory.
+// vector.  The hidden layers' forward GEMMs run on the sm_100a tensor cores
+// (tcgen05.mma, accumulator in tensor memory, operand tiles brought into
+// shared memory by the Tensor Memory Accelerator) whenever in is a multiple
+// of 64 and H a multiple of 16 up to 256: the weights are converted to BF16
+// once per call and the activations travel between layers as BF16.  The
+// backward GEMMs, and other shapes, use warp-level BF16 MMA (wmma) with the
+// FP32 operands rounded to BF16 when a tile is staged in shared memory.
 //
 // Parameter vector: W1[H][in], b1[H], W2[H][H], b2[H], W3[H][H], b3[H], w4[H], b4.
 // Workspace (FP32): per hidden layer l = 1..3: Z_l[B][H] (pre-activation),
 // A_l[B][H] (GELU output); then y[B]; then two [B][H] gradient buffers.
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <mma.h>
 
 #include <cstddef>
+#include <mutex>
 
 #include "xs_mlp.hpp"
 
@@ -177,9 +185,248 @@ __global__ void adam(float* __restrict__ p, const float* __restrict__ g, float* 
   }
 }
 
+// ---- hidden layer on the tensor cores (tcgen05) ------------------------------------
+// Z[b][n] = sum_k A[b][k] W[n][k] + bias[n] for one tile of 128 rows b and all N
+// columns.  A (BF16 [B][K]) and W (BF16 [N][K]) are K-major; the Tensor Memory
+// Accelerator copies 64-column slices of both (128-byte rows, 128-byte swizzle)
+// into a two-stage shared-memory ring, one thread issues tcgen05.mma
+// (M = 128, N, K = 16, BF16 x BF16 -> FP32) into an accumulator of N tensor-memory
+// columns, and all four warps read it back (tcgen05.ld, each warp its 32 lanes =
+// rows) for the epilogue: bias, GELU, BF16 activations for the next layer, and in
+// training the FP32 pre-activation and activation for the backward pass.  Every
+// wait on an mbarrier is bounded: on a timeout the CTA sets status bit 0, waits
+// (bounded) for its copies and products in flight, frees its tensor memory and
+// returns.
+namespace tc {
+constexpr int BM = 128, BK = 64, STAGES = 2;
+constexpr int WAIT_LIMIT = 1 << 24;
+
+struct __align__(64) Tmap {
+  unsigned long long w[16];
+};
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity) {
+  for (int it = 0; it < WAIT_LIMIT; ++it) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void tma_load(const Tmap* tm, unsigned dst, unsigned bar, int x, int y) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+          dst),
+      "l"((unsigned long long)tm), "r"(x), "r"(y), "r"(bar)
+      : "memory");
+}
+
+// shared-memory matrix descriptor: K-major rows of 128 bytes with the 128-byte swizzle,
+// 8-row groups 1024 bytes apart (stride byte offset), descriptor version 1, base offset 0
+__device__ __forceinline__ unsigned long long sdesc(unsigned addr) {
+  return (unsigned long long)((addr >> 4) & 0x3FFF) | (1ull << 16) | (64ull << 32) | (1ull << 46) | (2ull << 61);
+}
+
+template <bool TRAIN>
+__global__ void __launch_bounds__(128, 1)
+    layer_tc(const __grid_constant__ Tmap tA, const __grid_constant__ Tmap tW, int B, int K, int N, int ncols,
+             const float* __restrict__ bias, float* __restrict__ Z, float* __restrict__ Af,
+             __nv_bfloat16* __restrict__ Ab, int* __restrict__ status) {
+  extern __shared__ __align__(1024) unsigned char dsm[];
+  unsigned char* base = (unsigned char*)(((size_t)dsm + 1023) & ~(size_t)1023);
+  const unsigned a_bytes = BM * BK * 2, w_bytes = (unsigned)N * BK * 2, stage_bytes = a_bytes + w_bytes;
+  unsigned long long* bars = (unsigned long long*)(base + STAGES * stage_bytes);  // full[2], empty[2], done
+  unsigned* tslot = (unsigned*)(bars + 2 * STAGES + 1);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
+                 "r"(ncols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < 2 * STAGES + 1; ++i)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bars + i)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const unsigned tmem = *tslot;
+  const int m0 = blockIdx.x * BM, nk = K / BK;
+  const unsigned full0 = smem_u32(bars), empty0 = smem_u32(bars + STAGES), done = smem_u32(bars + 2 * STAGES);
+  const unsigned sbase = smem_u32(base);
+  // instruction descriptor: FP32 accumulator, BF16 A and B, both K-major, N, M = 128
+  const unsigned idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((unsigned)(N >> 3) << 17) | ((unsigned)(BM >> 4) << 24);
+  __shared__ int s_ok;
+  bool ok = true;
+  if (threadIdx.x == 0) {
+    auto issue = [&](int kb) {
+      const int s = kb % STAGES;
+      const unsigned bar = full0 + 8u * s, dst = sbase + s * stage_bytes;
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(stage_bytes) : "memory");
+      tma_load(&tA, dst, bar, kb * BK, m0);
+      tma_load(&tW, dst + a_bytes, bar, kb * BK, 0);
+    };
+    int issued = 0;
+    for (; issued < nk && issued < STAGES; ++issued) issue(issued);
+    for (int kb = 0; kb < nk && ok; ++kb) {
+      const int s = kb % STAGES;
+      if (!mbar_wait(full0 + 8u * s, (unsigned)((kb / STAGES) & 1))) {
+        ok = false;
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const unsigned a0 = sbase + s * stage_bytes, w0 = a0 + a_bytes;
+#pragma unroll
+      for (int kk = 0; kk < BK / 16; ++kk) {
+        const unsigned long long da = sdesc(a0 + kk * 32), dw = sdesc(w0 + kk * 32);
+        const unsigned acc = (kb > 0 || kk > 0) ? 1u : 0u;
+        asm volatile(
+            "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+            " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
+            "l"(da), "l"(dw), "r"(idesc), "r"(acc)
+            : "memory");
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(empty0 + 8u * s)
+                   : "memory");
+      if (issued < nk) {  // refill this stage once its products have read it
+        if (!mbar_wait(empty0 + 8u * s, (unsigned)((kb / STAGES) & 1))) {
+          ok = false;
+          break;
+        }
+        issue(issued++);
+      }
+    }
+    // the done barrier completes when every product issued so far has finished
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(done) : "memory");
+    if (!ok) {
+      atomicOr(status, 1);
+      // copies still in flight complete on their full barriers: wait for them (bounded) before leaving
+      for (int kb = 0; kb < issued; ++kb) mbar_wait(full0 + 8u * (kb % STAGES), (unsigned)((kb / STAGES) & 1));
+    }
+    s_ok = ok ? 1 : 0;
+  }
+  __syncthreads();
+  ok = s_ok != 0;
+  const bool fin = mbar_wait(done, 0);
+  if (!fin && lane == 0) atomicOr(status, 1);
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (__all_sync(0xffffffffu, fin) && ok) {
+    const int row = m0 + 32 * warp + lane;
+    for (int c0 = 0; c0 < N; c0 += 16) {
+      unsigned r[16];
+      const unsigned taddr = tmem + ((unsigned)(32 * warp) << 16) + (unsigned)c0;
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+          "%15}, [%16];"
+          : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+            "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+          : "r"(taddr));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      if (row < B) {
+        __align__(16) float z[16], g[16];
+        __align__(16) __nv_bfloat16 gb[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          z[j] = __uint_as_float(r[j]) + bias[c0 + j];
+          g[j] = gelu(z[j]);
+          gb[j] = __float2bfloat16_rn(g[j]);
+        }
+        const size_t o = (size_t)row * N + c0;
+        if (TRAIN) {
+#pragma unroll
+          for (int j = 0; j < 16; j += 4) {
+            *(float4*)(Z + o + j) = *(const float4*)(z + j);
+            *(float4*)(Af + o + j) = *(const float4*)(g + j);
+          }
+        }
+        *(uint4*)(Ab + o) = *(const uint4*)gb;
+        *(uint4*)(Ab + o + 8) = *(const uint4*)(gb + 8);
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols) : "memory");
+  }
+}
+
+__global__ void to_bf16(const float* __restrict__ x, __nv_bfloat16* __restrict__ y, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    y[i] = __float2bfloat16_rn(x[i]);
+}
+
+// y[b] = sum_h A[b][h] w[h] + c over BF16 activations (one warp per row)
+__global__ void head_forward_bf16(const __nv_bfloat16* __restrict__ A, const float* __restrict__ w,
+                                  const float* __restrict__ c, float* __restrict__ y, int B, int H) {
+  const int row = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+  if (row >= B) return;
+  float s = 0.f;
+  for (int h = lane; h < H; h += 32)
+    s += __bfloat162float(A[(size_t)row * H + h]) * __bfloat162float(__float2bfloat16_rn(w[h]));
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (lane == 0) y[row] = s + c[0];
+}
+
+typedef CUresult (*PFN_encode)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                               const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                               CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+PFN_encode encoder() {
+  static PFN_encode fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (PFN_encode)p;
+  });
+  return fn;
+}
+
+// 2D BF16 tensor [rows][cols] (cols contiguous), box 64 columns x box_rows rows, 128-byte swizzle
+bool make_map(Tmap* m, const void* ptr, int rows, int cols, int box_rows) {
+  PFN_encode enc = encoder();
+  if (!enc) return false;
+  const cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)cols * 2};
+  const cuuint32_t box[2] = {(cuuint32_t)BK, (cuuint32_t)box_rows};
+  const cuuint32_t estr[2] = {1, 1};
+  return enc((CUtensorMap*)m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(ptr), dims, strides, box, estr,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+size_t smem_bytes(int N) { return 1024 + (size_t)STAGES * (BM * BK * 2 + (size_t)N * BK * 2) + 64; }
+
+int* status_buf() {
+  static int* p = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    if (cudaMalloc(&p, sizeof(int)) != cudaSuccess) p = nullptr;
+  });
+  return p;
+}
+}  // namespace tc
+
+bool tc_shape_ok(int in, int H) { return in % tc::BK == 0 && H % 16 == 0 && H >= 16 && H <= 256; }
+
 struct Layout {
   size_t W[4], b[4], nparams;
   size_t Z[3], A[3], y, g1, g2, nwork;
+  size_t xb, ab[3], wb[3];  // BF16 copies (offsets in floats, 256-byte aligned): x, activations, weights
 };
 
 Layout layout(int in, int H, int B) {
@@ -198,6 +445,17 @@ Layout layout(int in, int H, int B) {
   L.y = w; w += B;
   L.g1 = w; w += (size_t)B * H;
   L.g2 = w; w += (size_t)B * H;
+  auto al = [](size_t v) { return (v + 63) / 64 * 64; };
+  w = al(w);
+  L.xb = w; w = al(w + ((size_t)B * in + 1) / 2);
+  for (int l = 0; l < 3; ++l) {
+    L.ab[l] = w;
+    w = al(w + ((size_t)B * H + 1) / 2);
+  }
+  for (int l = 0; l < 3; ++l) {
+    L.wb[l] = w;
+    w = al(w + ((size_t)H * (l == 0 ? in : H) + 1) / 2);
+  }
   L.nwork = w;
   return L;
 }
@@ -215,8 +473,54 @@ size_t xs_mlp_layout(int in, int hidden, int batch, size_t* nparams) {
   return L.nwork;
 }
 
+// Forward pass on the tensor cores (tc_shape_ok): BF16 copies of x and the weights, three
+// tcgen05 layers, the head on the CUDA cores.  train: also the FP32 pre-activations and
+// activations the backward pass reads.
+int forward_tc(int B, int in, int H, const float* x, const float* P, float* work, float* y, bool train,
+               cudaStream_t st) {
+  Layout L = layout(in, H, B);
+  int* status = tc::status_buf();
+  if (!status) return (int)cudaErrorMemoryAllocation;
+  __nv_bfloat16* xb = (__nv_bfloat16*)(work + L.xb);
+  tc::to_bf16<<<grid1((size_t)B * in), 256, 0, st>>>(x, xb, (size_t)B * in);
+  for (int l = 0; l < 3; ++l) {
+    const size_t n = (size_t)H * (l == 0 ? in : H);
+    tc::to_bf16<<<grid1(n), 256, 0, st>>>(P + L.W[l], (__nv_bfloat16*)(work + L.wb[l]), n);
+  }
+  int ncols = 32;
+  while (ncols < H) ncols <<= 1;
+  const size_t smem = tc::smem_bytes(H);
+  static std::once_flag attr;
+  std::call_once(attr, [] {
+    const int mx = (int)tc::smem_bytes(256);
+    cudaFuncSetAttribute(tc::layer_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+    cudaFuncSetAttribute(tc::layer_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+  });
+  const __nv_bfloat16* a = xb;
+  int K = in;
+  const unsigned grid = (unsigned)((B + tc::BM - 1) / tc::BM);
+  for (int l = 0; l < 3; ++l) {
+    tc::Tmap tA, tW;
+    const __nv_bfloat16* wb = (const __nv_bfloat16*)(work + L.wb[l]);
+    if (!tc::make_map(&tA, a, B, K, tc::BM) || !tc::make_map(&tW, wb, H, K, H)) return (int)cudaErrorInvalidValue;
+    __nv_bfloat16* ab = (__nv_bfloat16*)(work + L.ab[l]);
+    if (train)
+      tc::layer_tc<true><<<grid, 128, smem, st>>>(tA, tW, B, K, H, ncols, P + L.b[l], work + L.Z[l], work + L.A[l],
+                                                  ab, status);
+    else
+      tc::layer_tc<false><<<grid, 128, smem, st>>>(tA, tW, B, K, H, ncols, P + L.b[l], nullptr, nullptr, ab, status);
+    a = ab;
+    K = H;
+  }
+  float* out = y ? y : work + L.y;
+  tc::head_forward_bf16<<<(B + 7) / 8, 256, 0, st>>>(a, P + L.W[3], P + L.b[3], out, B, H);
+  if (out != work + L.y) cudaMemcpyAsync(work + L.y, out, (size_t)B * 4, cudaMemcpyDeviceToDevice, st);
+  return (int)cudaGetLastError();
+}
+
 int xs_mlp_forward_impl(int B, int in, int H, const float* x, const float* P, float* work, float* y,
-                        cudaStream_t st) {
+                        cudaStream_t st, bool train) {
+  if (tc_shape_ok(in, H)) return forward_tc(B, in, H, x, P, work, y, train, st);
   Layout L = layout(in, H, B);
   dim3 blk(128);
   dim3 g((H + TN - 1) / TN, (B + TM - 1) / TM);
@@ -271,3 +575,17 @@ int xs_mlp_adam_impl(size_t n, float* P, const float* g, float* m, float* v, flo
   adam<<<grid1(n), 256, 0, st>>>(P, g, m, v, n, lr, b1, b2, eps, c1, c2, wd);
   return (int)cudaGetLastError();
 }
+
+// Status of the tensor-core layers since the last call (bit 0: a bounded wait gave up),
+// read synchronously on `st`, then cleared.
+int xs_mlp_status(cudaStream_t st) {
+  int* status = tc::status_buf();
+  if (!status) return 0;
+  int h = 0;
+  if (cudaMemcpyAsync(&h, status, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess) return 0;
+  if (cudaStreamSynchronize(st) != cudaSuccess) return 0;
+  if (h) cudaMemsetAsync(status, 0, sizeof(int), st);
+  return h;
+}
+
+int xs_mlp_uses_tensor_memory(int in, int hidden) { return tc_shape_ok(in, hidden) ? 1 : 0; }
