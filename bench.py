@@ -59,6 +59,16 @@ def _peaks():
         return HBM_FALLBACK_GBS, "fallback"
 
 
+def _bf16_peak():
+    """Dense BF16 tensor-core peak (TFLOP/s) for a kernel timed on its own: the burst figure."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["bf16_tflops"]), "measured"
+    except Exception:
+        return 1590.0, "fallback"
+
+
 class Clocks:
     """nvidia-smi clock/throttle sampling during the timed region."""
 
@@ -473,18 +483,30 @@ def _cv_solve(path, first, nb, feats=False):
 
 
 def run_cv(args):
+    """Second headline (cfg5): the learned control variate on the 256x256 GPE.
+
+    Training: 2^16 + 8192 (noise features, observable) pairs generated by the FP32
+    solver.  The control variate g is the best, on the 8192 held-out pairs, of linear
+    least squares on the features, least squares on the features and their squares,
+    and that plus the BF16 MLP (tcgen05 forward, trained by the project's kernels) on
+    the residual.  Estimators, each timed on fresh trajectories:
+      cfg5   N = 512 FP32 solves and M = 2^20 network evaluations on fresh inputs,
+             mean_N(f - g) + mean_M(g), against the plain FP64 estimator with the
+             trajectories that give it the same sampling error;
+      1e-3   both at the trajectory counts their pilot variances need for 1e-3
+             relative sampling error (xsim.m:95 block estimate).
+    Times are reported with and without generating the training pairs and fitting."""
     import numpy as np
     import torch
     global CV_SETS, CV_FEATURES
     if args.cv_sets:
         CV_SETS = tuple((tuple(r), dw, nt, gap) for r, dw, nt, gap in json.loads(args.cv_sets))
         CV_FEATURES = sum(2 * nt * r[4] * r[5] for r, dw, nt, gap in CV_SETS)
-    from xspde_matlab_b200.cv import ControlVariateNet, block_sampling_error, two_level
+    from xspde_matlab_b200.cv import ControlVariateNet, block_sampling_error, fresh_moments, two_level
     target = 1e-3
     nblk = 16
-    ntrain, nval, chunk = 1 << 16, 8192, 8192
+    ntrain, nval, chunk = args.cv_train, 8192, 8192
     p32 = _cv_path("fp32", chunk)
-    # training pairs generated by the solver itself (global blocks 0 .. 65535)
     t0 = time.perf_counter()
     fs, Xs = [], []
     for b0 in range(0, ntrain + nval, chunk):
@@ -495,20 +517,23 @@ def run_cv(args):
     t_data = time.perf_counter() - t0
     f_all, X_all = torch.cat(fs), torch.cat(Xs)
     f_tr, X_tr, f_va, X_va = f_all[:ntrain], X_all[:ntrain], f_all[ntrain:], X_all[ntrain:]
-    # control variate g = linear least squares + MLP on the residual
     t0 = time.perf_counter()
-    A = torch.cat([X_tr.double(), torch.ones(ntrain, 1, dtype=torch.float64, device="cuda")], 1)
-    coef = torch.linalg.solve(A.T @ A, A.T @ f_tr.double().unsqueeze(1))[:, 0]
 
-    w32, b0 = coef[:-1].float(), float(coef[-1])
-
-    def g_lin(X):  # the same function for the solver's inputs and the fresh ones (FP32 dot, FP64 sum)
-        return (X @ w32).double() + b0
+    def lsq(feat):
+        A = torch.cat([feat(X_tr).double(), torch.ones(ntrain, 1, dtype=torch.float64, device="cuda")], 1)
+        c = torch.linalg.solve(A.T @ A, A.T @ f_tr.double().unsqueeze(1))[:, 0]
+        w, b = c[:-1].float(), float(c[-1])
+        return lambda X: (feat(X) @ w).double() + b  # FP32 dot, FP64 sum: same for solver and fresh inputs
+    lin = lsq(lambda X: X)
+    quad = lsq(lambda X: torch.cat([X, X * X], 1))
+    var_plain = float(f_va.double().var())
+    var_lin = float((f_va.double() - lin(X_va)).var())
+    var_quad = float((f_va.double() - quad(X_va)).var())
+    base, var_base = (quad, var_quad) if var_quad < var_lin else (lin, var_lin)
     net = ControlVariateNet(CV_FEATURES, 256, seed=0)
-    r_tr = (f_tr.double() - g_lin(X_tr)).float()
-    r_va = f_va.double() - g_lin(X_va)
-    var_lin = float(r_va.var())
-    best = (var_lin, None)  # the linear fit alone
+    r_tr = (f_tr.double() - base(X_tr)).float()
+    r_va = f_va.double() - base(X_va)
+    best = (var_base, None)
     for ep in range(20):
         net.fit(X_tr, r_tr, epochs=1, batch=1024, lr=3e-4 if ep > 9 else 1e-3, seed=ep, weight_decay=1e-2)
         v = float((r_va - net.predict(X_va)).var())
@@ -522,70 +547,146 @@ def run_cv(args):
     t_fit = time.perf_counter() - t0
 
     def g(X):
-        return g_lin(X) + (net.predict(X) if use_mlp else 0.0)
-    var_plain = float(f_va.double().var())
+        return base(X) + (net.predict(X) if use_mlp else 0.0)
     var_cv = float((f_va.double() - g(X_va)).var())
     mu = float(f_va.double().mean())
-    print("cv pilot: mean %.6g var_plain %.4g var_cv %.4g mlp %s" % (mu, var_plain, var_cv, use_mlp), file=sys.stderr)
-    # plain FP64 estimator at the N that reaches the target (pilot variance)
-    n_plain = nblk * max(2, math.ceil(var_plain / (target * mu) ** 2 / nblk))
-    p64 = _cv_path("fp64", n_plain)
-    _cv_solve(p64, 1 << 19, n_plain)  # compile and warm the FP64 kernels and buffers at the timed size
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    f64, _ = _cv_solve(p64, 1 << 20, n_plain)
-    est_plain, err_plain = block_sampling_error(f64.cpu().numpy(), nblk)
-    t_plain = time.perf_counter() - t0
-    # FP32 + learned control variate at its own N, fresh trajectories and fresh network inputs
-    from xspde_matlab_b200.cv import fresh_moments
-    n_cv = nblk * max(2, math.ceil(var_cv / (target * mu) ** 2 / nblk))
+    print("cv pilot: mean %.6g var_plain %.4g lin %.4g quad %.4g cv %.4g mlp %s" % (
+        mu, var_plain, var_lin, var_quad, var_cv, use_mlp), file=sys.stderr)
+
+    def time_cv(n, m, first):
+        """N fresh FP32 solves with features + M fresh network inputs; returns (s, est, err, phases)."""
+        pcv = _cv_path("fp32", n)
+        _, Xw = _cv_solve(pcv, first + (1 << 22), n, feats=True)  # warm at the timed size
+        g(Xw)
+        gen = torch.Generator(device="cuda").manual_seed(777)
+        fresh_moments(g(torch.randn((m, CV_FEATURES), device="cuda", generator=gen)))
+        gen = torch.Generator(device="cuda").manual_seed(12345 + first)
+        torch.cuda.synchronize()
+        ta = time.perf_counter()
+        f32, Xc = _cv_solve(pcv, first, n, feats=True)
+        tb = time.perf_counter()
+        gx = g(Xc)
+        mom = fresh_moments(g(torch.randn((m, CV_FEATURES), device="cuda", generator=gen)))
+        tc_ = time.perf_counter()
+        est, err = two_level(f32.cpu().numpy(), gx.cpu().numpy(), mom, nblk)
+        te = time.perf_counter()
+        return te - ta, est, err, {"solve_and_features": tb - ta, "network_and_fresh_inputs": tc_ - tb,
+                                   "estimate": te - tc_}, f32
+
+    def time_plain(n, first):
+        p64 = _cv_path("fp64", n)
+        _cv_solve(p64, first + (1 << 22), n)  # compile and warm at the timed size
+        torch.cuda.synchronize()
+        ta = time.perf_counter()
+        f64, _ = _cv_solve(p64, first, n)
+        est, err = block_sampling_error(f64.cpu().numpy(), nblk)
+        return time.perf_counter() - ta, est, err, f64
+
     m_fresh = 1 << 20
-    pcv = _cv_path("fp32", n_cv)
-    _, Xw = _cv_solve(pcv, 1 << 22, n_cv, feats=True)  # warm at the timed size
-    g(Xw)
-    gen = torch.Generator(device="cuda").manual_seed(777)
-    fresh_moments(g(torch.randn((m_fresh, CV_FEATURES), device="cuda", generator=gen)))
-    gen = torch.Generator(device="cuda").manual_seed(12345)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    f32, Xc = _cv_solve(pcv, 1 << 21, n_cv, feats=True)
-    t1 = time.perf_counter()
-    gx = g(Xc)
-    Xf = torch.randn((m_fresh, CV_FEATURES), device="cuda", generator=gen)
-    mom = fresh_moments(g(Xf))
-    t2 = time.perf_counter()
-    est_cv, err_cv = two_level(f32.cpu().numpy(), gx.cpu().numpy(), mom, nblk)
-    t_cv = time.perf_counter() - t0
-    t_parts = {"solve_and_features": t1 - t0, "fresh_network_inputs": t2 - t1, "estimate": t_cv - (t2 - t0)}
-    # cost of the network on the 2^20 fresh inputs (BF16 tensor-core forward), whether or not it is used
-    net.predict(Xf)
-    torch.cuda.synchronize()
-    tm0 = time.perf_counter()
-    net.predict(Xf)
-    torch.cuda.synchronize()
-    t_mlp = time.perf_counter() - tm0
-    # FP32 trajectories against FP64 ones on identical noise (the FP64-oracle error of the FP32 path)
+    # cfg5: N = 512, M = 2^20; the plain FP64 estimator at the same sampling error
+    n5 = 512
+    t5, est5, err5, ph5, f5 = time_cv(n5, m_fresh, 1 << 21)
+    n5p = nblk * max(2, math.ceil(n5 * var_plain / var_cv / nblk))
+    t5p, est5p, err5p, _ = time_plain(n5p, 1 << 20)
+    # time to 1e-3 relative sampling error, each at the count its pilot variance needs
+    n_plain = nblk * max(2, math.ceil(var_plain / (target * mu) ** 2 / nblk))
+    n_cv = nblk * max(2, math.ceil(var_cv / (target * mu) ** 2 / nblk))
+    t_plain, est_plain, err_plain, f64p = time_plain(n_plain, (1 << 20) + (1 << 19))
+    t_cv, est_cv, err_cv, ph, f32c = time_cv(n_cv, m_fresh, (1 << 21) + (1 << 19))
+    # FP32 trajectories against FP64 ones on identical noise
     ncmp = min(256, n_cv)
-    p64b = _cv_path("fp64", ncmp)
-    f64b, _ = _cv_solve(p64b, 1 << 21, ncmp)
-    d32 = float(((f32[:ncmp].double() - f64b) / f64b).abs().max())
+    f64b, _ = _cv_solve(_cv_path("fp64", ncmp), (1 << 21) + (1 << 19), ncmp)
+    d32 = float(((f32c[:ncmp].double() - f64b) / f64b).abs().max())
+    train = t_data + t_fit
     line = {
         "metric": "time to 1e-3 relative sampling error on <|a|^2> (central region, t=5)", "value": t_cv,
         "unit": "s", "higher_is_better": False, "n_gpus": 1,
         "plain_fp64": {"seconds": t_plain, "trajectories": n_plain, "estimate": est_plain,
                        "rel_sampling_error": err_plain / est_plain},
-        "fp32_cv": {"seconds": t_cv, "trajectories": n_cv, "fresh_network_inputs": m_fresh, "estimate": est_cv,
-                    "rel_sampling_error": err_cv / est_cv, "mlp_used": use_mlp, "seconds_by_phase": t_parts,
-                    "mlp_forward_2p20_seconds": t_mlp},
+        "fp32_cv": {"seconds": t_cv, "seconds_with_training": t_cv + train, "trajectories": n_cv,
+                    "fresh_network_inputs": m_fresh, "estimate": est_cv, "rel_sampling_error": err_cv / est_cv,
+                    "seconds_by_phase": ph},
         "speedup_vs_plain_fp64": t_plain / t_cv,
-        "variance_ratio": {"used": var_plain / var_cv, "linear_only": var_plain / var_lin,
-                           "linear_plus_mlp_best": var_plain / best[0], "plain_var": var_plain, "cv_var": var_cv},
+        "speedup_with_training": t_plain / (t_cv + train),
+        "cfg5_N512_M2p20": {"cv_seconds": t5, "cv_seconds_with_training": t5 + train, "cv_estimate": est5,
+                            "cv_rel_sampling_error": err5 / est5, "cv_seconds_by_phase": ph5,
+                            "plain_fp64_trajectories_same_error": n5p, "plain_fp64_seconds": t5p,
+                            "plain_fp64_estimate": est5p, "plain_fp64_rel_sampling_error": err5p / est5p,
+                            "speedup": t5p / t5, "speedup_with_training": t5p / (t5 + train)},
+        "variance": {"plain": var_plain, "linear": var_lin, "linear_and_squares": var_quad,
+                     "used": var_cv, "mlp_used": use_mlp, "mlp_on_residual_best": best[0],
+                     "reduction_used": var_plain / var_cv,
+                     "mlp_gain_over_least_squares": var_base / best[0]},
         "estimates_agree_sigma": abs(est_cv - est_plain) / math.sqrt(err_cv ** 2 + err_plain ** 2),
         "fp32_vs_fp64_traj_max_rel": d32,
-        "training": {"pairs": ntrain, "data_seconds": t_data, "fit_seconds": t_fit,
+        "training": {"pairs": ntrain, "validation_pairs": nval, "data_seconds": t_data, "fit_seconds": t_fit,
                      "features": "%d coarse space-time noise projections: %s" % (CV_FEATURES, CV_SETS)},
         "config": {"workload": "gpe_2d 256x256, 509 MP steps; sampling error from %d blocks (xsim.m:95)" % nblk},
     }
+    print(json.dumps(line))
+
+
+def run_mlp(args):
+    """The control-variate network's inference on M fresh inputs (cfg5's M = 2^20 network
+    evaluations): 256 inputs -> 256 x 3 (GELU) -> 1, hidden layers on the tcgen05 tensor
+    cores with BF16 operands and FP32 accumulation.  One step = one xs_mlp_forward over
+    all M rows (FP32 inputs resident in HBM)."""
+    import numpy as np
+    import torch
+    from oracle import mlp_ref
+    from xspde_matlab_b200 import _lib
+    from xspde_matlab_b200.cv import ControlVariateNet
+    L = _lib.lib()
+    n_in, H, B = 256, 256, args.mlp_batch
+    net = ControlVariateNet(n_in, H, seed=0)
+    g = torch.Generator(device="cuda").manual_seed(5)
+    X = torch.randn((B, n_in), device="cuda", generator=g)
+    work = torch.empty(L.xs_mlp_sizes(n_in, H, B, None), dtype=torch.float32, device="cuda")
+    y = torch.empty(B, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.current_stream()
+    st = ctypes.c_void_p(stream.cuda_stream)
+
+    def fwd():
+        _lib.check(L.xs_mlp_forward(B, n_in, H, ctypes.c_void_p(X.data_ptr()), ctypes.c_void_p(net.params.data_ptr()),
+                                    ctypes.c_void_p(work.data_ptr()), ctypes.c_void_p(y.data_ptr()), st))
+    for _ in range(max(3, args.warmup)):
+        fwd()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(torch.cuda.current_device()) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            fwd()
+        e1.record(stream)
+        e1.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    flops = 2.0 * B * (n_in * H + 2 * H * H + H)
+    # HBM bytes of the forward per row: FP32 inputs read, their BF16 copy written and read,
+    # per hidden layer the BF16 activations read and written, the head's read and the output
+    bytes_row = 4 * n_in + 2 * 2 * n_in + 3 * 2 * 2 * H + 2 * H + 4
+    tf, tkind = _bf16_peak()
+    hbm, hkind = _peaks()
+    # CPU baseline: the FP64 NumPy network (oracle/mlp_ref.py) on a sample of rows
+    P = net.params.cpu().numpy()
+    Xs = X[:8192].cpu().numpy()
+    t0 = time.perf_counter()
+    ys, _, _ = mlp_ref.forward(Xs, P, n_in, H)
+    cpu_s = time.perf_counter() - t0
+    err = float(np.max(np.abs(y[:8192].cpu().numpy() - ys)) / np.max(np.abs(ys)))
+    line = {"metric": "network evaluations/s, control-variate MLP 256-256x3-1 on fresh inputs", "value": B / (ms * 1e-3),
+            "unit": "rows/s", "n_gpus": 1, "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": ms,
+            "higher_is_better": True, "dtype": "bf16 operands, f32 accumulation", "data": "synthetic N(0,1) inputs",
+            "tflops": flops / (ms * 1e-3) / 1e12,
+            "roofline": {"bound": "hbm", "achieved": bytes_row * B / (ms * 1e-3) / 1e9, "peak": hbm, "unit": "GB/s",
+                         "frac": bytes_row * B / (ms * 1e-3) / 1e9 / hbm, "peak_kind": hkind,
+                         "bytes_per_row": bytes_row, "traffic": None},
+            "tensor": {"achieved_tflops": flops / (ms * 1e-3) / 1e12, "peak_tflops": tf, "peak_kind": tkind,
+                       "frac": flops / (ms * 1e-3) / 1e12 / tf, "flops_per_row": flops / B},
+            "max_rel_vs_fp64_oracle": err,
+            "cpu_baseline": {"value": 8192 / cpu_s, "unit": "rows/s", "cores": 1, "kind": "port",
+                             "sample": "8192 rows through the FP64 NumPy network (oracle/mlp_ref.py)"},
+            "clocks": clk.summary(),
+            "config": {"workload": "mlp 256->256x3->1, M=%d rows" % B}}
     print(json.dumps(line))
 
 
@@ -807,9 +908,12 @@ def main():
     ap.add_argument("--cv", action="store_true", help="second headline: time to 1e-3 sampling error, "
                                                       "plain FP64 vs FP32 + learned control variate")
     ap.add_argument("--cv-sets", default="", help="JSON list of noise-feature sets [[region6], steps, windows, gap]")
+    ap.add_argument("--cv-train", type=int, default=1 << 16, help="solver-generated training pairs (multiple of 8192)")
     ap.add_argument("--batch", action="store_true", help="uneven batch of independent problems, one graph launch")
     ap.add_argument("--batch-items", type=int, default=512)
     ap.add_argument("--dpo", action="store_true", help="positive-P DPO, 10^6 trajectories x 2000 steps")
+    ap.add_argument("--mlp", action="store_true", help="control-variate network inference on M fresh inputs")
+    ap.add_argument("--mlp-batch", type=int, default=1 << 20)
     ap.add_argument("--ac3d", action="store_true", help="3D stochastic Allen-Cahn 64^3 with DST/DCT boundaries")
     ap.add_argument("--ac3d-traj", type=int, default=256, help="trajectories of --ac3d (multiple of 32)")
     args = ap.parse_args()
@@ -833,6 +937,11 @@ def main():
         import torch
         torch.cuda.set_device(local_rank)
         run_batch(args)
+        return
+    if args.mlp:
+        import torch
+        torch.cuda.set_device(local_rank)
+        run_mlp(args)
         return
     if args.cv:
         import torch

@@ -221,7 +221,8 @@ XS_API xs_status xs_step(xs_handle* h, double* a_inout, const double* w, double 
 /* Inputs of the learned control variate (no counterpart in the reference):
  * coarse space-time projections of the Wiener increments that p.noisegen
  * feeds the trajectories of blocks first_block .. first_block+nblocks-1
- * (fine pass).  region = {i1lo, i2lo, bw, bh, nbx, nby}: nbx x nby lattice
+ * (fine pass; lattices of up to two space dimensions, an SDE being a single
+ * site).  region = {i1lo, i2lo, bw, bh, nbx, nby}: nbx x nby lattice
  * blocks of bw x bh sites starting at x index i1lo, y index i2lo (<= 16 x 16
  * blocks); windows of draws_per_window consecutive draws starting at
  * first_draw (>= 1); within a window the draws are weighted by

@@ -2486,7 +2486,7 @@ XS_API xs_status xs_noise_features(xs_handle* h, int first_block, int nblocks, c
         first_draw < 1)
       raise(XS_ERR_ARG, "bad arguments to xs_noise_features");
     const Problem& P = h->P;
-    if (P.D < 2 || P.NW < 1) raise(XS_ERR_UNSUPPORTED, "noise features need two space dimensions and noises");
+    if (P.D > 2 || P.NW < 1) raise(XS_ERR_UNSUPPORTED, "noise features need at most two space dimensions and noises");
     const int i1lo = region[0], i2lo = region[1], bw = region[2], bh = region[3], nbx = region[4], nby = region[5];
     if (bw < 1 || bh < 1 || nbx < 1 || nby < 1 || nbx > 16 || nby > 16 || i1lo < 0 || i2lo < 0 ||
         i1lo + nbx * bw > P.N[0] || i2lo + nby * bh > P.N[1])
