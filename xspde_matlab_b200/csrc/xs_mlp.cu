@@ -191,8 +191,9 @@ __global__ void adam(float* __restrict__ p, const float* __restrict__ g, float* 
 // Accelerator copies 64-column slices of both (128-byte rows, 128-byte swizzle)
 // into a two-stage shared-memory ring, one thread issues tcgen05.mma
 // (M = 128, N, K = 16, BF16 x BF16 -> FP32) into an accumulator of N tensor-memory
-// columns, and all four warps read it back (tcgen05.ld, each warp its 32 lanes =
-// rows) for the epilogue: bias, GELU, BF16 activations for the next layer, and in
+// columns, and eight warps read it back (tcgen05.ld; a warp reaches the 32 lanes =
+// rows of its sub-partition, two warps split the columns) for the epilogue: bias,
+// GELU, BF16 activations for the next layer, and in
 // training the FP32 pre-activation and activation for the backward pass.  Every
 // wait on an mbarrier is bounded: on a timeout the CTA sets status bit 0, waits
 // (bounded) for its copies and products in flight, frees its tensor memory and
@@ -235,7 +236,7 @@ __device__ __forceinline__ unsigned long long sdesc(unsigned addr) {
 }
 
 template <bool TRAIN>
-__global__ void __launch_bounds__(128, 1)
+__global__ void __launch_bounds__(256, 1)
     layer_tc(const __grid_constant__ Tmap tA, const __grid_constant__ Tmap tW, int B, int K, int N, int ncols,
              const float* __restrict__ bias, float* __restrict__ Z, float* __restrict__ Af,
              __nv_bfloat16* __restrict__ Ab, int* __restrict__ status) {
@@ -244,7 +245,9 @@ __global__ void __launch_bounds__(128, 1)
   const unsigned a_bytes = BM * BK * 2, w_bytes = (unsigned)N * BK * 2, stage_bytes = a_bytes + w_bytes;
   unsigned long long* bars = (unsigned long long*)(base + STAGES * stage_bytes);  // full[2], empty[2], done
   unsigned* tslot = (unsigned*)(bars + 2 * STAGES + 1);
+  float* sbias = (float*)(tslot + 4);  // N bias values
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int i = threadIdx.x; i < N; i += blockDim.x) sbias[i] = bias[i];
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
                  "r"(ncols)
@@ -320,10 +323,15 @@ __global__ void __launch_bounds__(128, 1)
   if (!fin && lane == 0) atomicOr(status, 1);
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   if (__all_sync(0xffffffffu, fin) && ok) {
-    const int row = m0 + 32 * warp + lane;
-    for (int c0 = 0; c0 < N; c0 += 16) {
+    // warps w and w + 4 share the 32 accumulator lanes (rows) of sub-partition w % 4 and
+    // split the N columns in 16-column chunks
+    const int sub = warp & 3, half = warp >> 2, nch = N / 16, ch0 = half ? (nch + 1) / 2 : 0,
+              ch1 = half ? nch : (nch + 1) / 2;
+    const int row = m0 + 32 * sub + lane;
+    for (int ch = ch0; ch < ch1; ++ch) {
+      const int c0 = 16 * ch;
       unsigned r[16];
-      const unsigned taddr = tmem + ((unsigned)(32 * warp) << 16) + (unsigned)c0;
+      const unsigned taddr = tmem + ((unsigned)(32 * sub) << 16) + (unsigned)c0;
       asm volatile(
           "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
           "%15}, [%16];"
@@ -336,7 +344,7 @@ __global__ void __launch_bounds__(128, 1)
         __align__(16) __nv_bfloat16 gb[16];
 #pragma unroll
         for (int j = 0; j < 16; ++j) {
-          z[j] = __uint_as_float(r[j]) + bias[c0 + j];
+          z[j] = __uint_as_float(r[j]) + sbias[c0 + j];
           g[j] = gelu(z[j]);
           gb[j] = __float2bfloat16_rn(g[j]);
         }
@@ -409,7 +417,7 @@ bool make_map(Tmap* m, const void* ptr, int rows, int cols, int box_rows) {
              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-size_t smem_bytes(int N) { return 1024 + (size_t)STAGES * (BM * BK * 2 + (size_t)N * BK * 2) + 64; }
+size_t smem_bytes(int N) { return 1024 + (size_t)STAGES * (BM * BK * 2 + (size_t)N * BK * 2) + 64 + 4 * (size_t)N; }
 
 int* status_buf() {
   static int* p = nullptr;
@@ -505,10 +513,10 @@ int forward_tc(int B, int in, int H, const float* x, const float* P, float* work
     if (!tc::make_map(&tA, a, B, K, tc::BM) || !tc::make_map(&tW, wb, H, K, H)) return (int)cudaErrorInvalidValue;
     __nv_bfloat16* ab = (__nv_bfloat16*)(work + L.ab[l]);
     if (train)
-      tc::layer_tc<true><<<grid, 128, smem, st>>>(tA, tW, B, K, H, ncols, P + L.b[l], work + L.Z[l], work + L.A[l],
+      tc::layer_tc<true><<<grid, 256, smem, st>>>(tA, tW, B, K, H, ncols, P + L.b[l], work + L.Z[l], work + L.A[l],
                                                   ab, status);
     else
-      tc::layer_tc<false><<<grid, 128, smem, st>>>(tA, tW, B, K, H, ncols, P + L.b[l], nullptr, nullptr, ab, status);
+      tc::layer_tc<false><<<grid, 256, smem, st>>>(tA, tW, B, K, H, ncols, P + L.b[l], nullptr, nullptr, ab, status);
     a = ab;
     K = H;
   }
