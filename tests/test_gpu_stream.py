@@ -186,3 +186,22 @@ def test_stream_rk4_single_output_time_every_step_observed():
     assert rel_err(a_g, a_o) < 1e-10
     for k in range(len(av_o)):
         assert rel_err(av_g[0][k].reshape(-1, order="F"), av_o[k].reshape(-1, order="F")) < 1e-10
+
+
+def test_stream_host_copies_overlapped_equal_single_block_calls():
+    """xs_run_path on the streaming path with a host initial field runs its blocks in
+    groups, copying the next group's field in and the previous group's means out
+    while a group integrates; every trajectory does the same arithmetic as in a
+    call for its block alone, so block means and final fields are bit-identical."""
+    from xspde_matlab_b200 import GpuPath, xpreferences
+    g, _ = _case(1, ens=(8, 4, 1))
+    path = GpuPath(xpreferences([g])[0], path_kind=2)
+    rs = np.random.default_rng(11)
+    a_in = (1 + 0.1 * rs.standard_normal((1, 64, 64, 32)) + 0.1j * rs.standard_normal((1, 64, 64, 32)))
+    for nc in (1, 2):
+        av_all, a_all = path.run_path(0, 4, nc, a_in=a_in, a_out=True)
+        for b in range(4):
+            av_b, a_b = path.run_path(b, 1, nc, a_in=a_in[..., 8 * b:8 * (b + 1)], a_out=True)
+            assert np.array_equal(a_all[..., 8 * b:8 * (b + 1)], a_b), (nc, b)
+            for k in range(len(av_b[0])):
+                assert np.array_equal(av_all[b][k], av_b[0][k]), (nc, b, k)

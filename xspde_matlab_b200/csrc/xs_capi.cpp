@@ -935,6 +935,8 @@ struct xs_handle {
   bool sep = false;                    // streaming: L(kx, ky) = Lx(kx) + Ly(ky), 1D propagator tables
   CUfunction f_batch = nullptr;
   cudaStream_t stream = nullptr;
+  cudaStream_t cstream = nullptr;    // copies of the pipelined streaming xs_run_path
+  std::vector<cudaEvent_t> pipe_ev;  // its per-group events (copy in done, group done)
   DevBuf d_prop[2], d_prop2[2], d_tmat, d_obs, d_av, d_ain, d_aout, d_status, d_w, d_field, d_redpart, d_pstep,
       d_params, d_gfield, d_twiddle, d_tmp, d_avm, d_bval[2], d_bda[2], d_aft, d_twt, d_raw, d_kfilt, d_rfilt,
       d_opart;
@@ -961,8 +963,10 @@ struct xs_handle {
       cudaEventDestroy(p.b);
     }
     for (auto e : event_pool) cudaEventDestroy(e);
+    for (auto e : pipe_ev) cudaEventDestroy(e);
     if (mod && driver().unload) driver().unload(mod);
     if (stream) cudaStreamDestroy(stream);
+    if (cstream) cudaStreamDestroy(cstream);
   }
 };
 
@@ -2228,6 +2232,84 @@ struct RawScope {  // the raw-trajectory pointer belongs to one xs_run_path_raw 
   ~RawScope() { h->raw_dev = nullptr; }
 };
 
+// xs_run_path on the streaming path with the host copies overlapped: the blocks
+// run in groups (the trajectories of different blocks are independent); group g's
+// initial field is copied in on a second stream while group g - 1 integrates, and
+// group g's block means (and final field) are copied out while group g + 1
+// integrates.  Each group is the same pass sequence as one call for its blocks, so
+// the results equal those of a single call.
+void run_stream_pipelined(xs_handle* h, int first_block, int nblocks, int nc, const double* a_in, double* av_out,
+                          double* a_out) {
+  const Problem& P = h->P;
+  const int ng = std::min(nblocks, 4);
+  if (!h->cstream) CUDA_CHECK(cudaStreamCreateWithFlags(&h->cstream, cudaStreamNonBlocking));
+  while ((int)h->pipe_ev.size() < 2 * ng) {
+    cudaEvent_t e;
+    CUDA_CHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    h->pipe_ev.push_back(e);
+  }
+  const size_t ntraj = (size_t)nblocks * P.E1, per_traj = (size_t)P.F * P.NS * 16;
+  const size_t stride = av_stride(P), per_block = av_doubles_per_block(P);
+  const size_t avd = (size_t)nblocks * P.p.points[0] * stride * 2;
+  h->d_ain.ensure(ntraj * per_traj);
+  h->d_av.ensure(std::max<size_t>(avd, 1) * 8);
+  h->d_avm.ensure(std::max<size_t>((size_t)nblocks * per_block, 1) * 8);
+  if (a_out) h->d_aout.ensure(ntraj * per_traj);
+  XsAvMap m{};
+  m.nobs = (int)P.obs.size();
+  m.npts = P.p.points[0];
+  m.NS = P.NS;
+  m.nout_site = P.nout_site;
+  m.stride = (int)stride;
+  m.per_block = (long long)(per_block / 2);
+  long long off = 0;
+  for (int o = 0; o < m.nobs; ++o) {
+    m.lines[o] = P.obs[o].lines;
+    m.spatial[o] = P.obs[o].spatial ? 1 : 0;
+    m.out_off[o] = P.obs[o].out_off;
+    m.o_off[o] = off;
+    off += (long long)P.obs[o].lines * m.npts * (P.obs[o].spatial ? P.NS : 1);
+  }
+  CUDA_CHECK(cudaMemsetAsync(h->d_status.p, 0, sizeof(int), h->stream));
+  auto grp = [&](int g, int& b0, int& nb) {
+    b0 = (int)((long long)nblocks * g / ng);
+    nb = (int)((long long)nblocks * (g + 1) / ng) - b0;
+  };
+  for (int g = 0; g < ng; ++g) {  // every copy in, in order, on the copy stream
+    int b0, nb;
+    grp(g, b0, nb);
+    const size_t t0 = (size_t)b0 * P.E1;
+    CUDA_CHECK(cudaMemcpyAsync((char*)h->d_ain.p + t0 * per_traj, a_in + t0 * per_traj / 8, (size_t)nb * P.E1 * per_traj,
+                               cudaMemcpyHostToDevice, h->cstream));
+    CUDA_CHECK(cudaEventRecord(h->pipe_ev[2 * g], h->cstream));
+  }
+  for (int g = 0; g < ng; ++g) {
+    int b0, nb;
+    grp(g, b0, nb);
+    const size_t t0 = (size_t)b0 * P.E1;
+    CUDA_CHECK(cudaStreamWaitEvent(h->stream, h->pipe_ev[2 * g], 0));
+    double* avg = (double*)h->d_av.p + (size_t)b0 * P.p.points[0] * stride * 2;
+    void* dout = a_out ? (char*)h->d_aout.p + t0 * per_traj : nullptr;
+    launch_stream(*h, first_block + b0, nb, nc, (const char*)h->d_ain.p + t0 * per_traj, avg, dout, h->stream);
+    double* avm = (double*)h->d_avm.p + (size_t)b0 * per_block;
+    if (av_out && per_block) CUDA_CHECK((cudaError_t)xs_aot_av_matlab_launch(avg, avm, &m, nb, h->stream));
+    CUDA_CHECK(cudaEventRecord(h->pipe_ev[2 * g + 1], h->stream));
+    CUDA_CHECK(cudaStreamWaitEvent(h->cstream, h->pipe_ev[2 * g + 1], 0));
+    if (av_out && per_block)
+      CUDA_CHECK(cudaMemcpyAsync(av_out + (size_t)b0 * per_block, avm, (size_t)nb * per_block * 8,
+                                 cudaMemcpyDeviceToHost, h->cstream));
+    if (a_out)
+      CUDA_CHECK(cudaMemcpyAsync(a_out + t0 * per_traj / 8, dout, (size_t)nb * P.E1 * per_traj, cudaMemcpyDeviceToHost,
+                                 h->cstream));
+  }
+  int status = 0;
+  CUDA_CHECK(cudaMemcpyAsync(&status, h->d_status.p, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  CUDA_CHECK(cudaStreamSynchronize(h->stream));
+  CUDA_CHECK(cudaStreamSynchronize(h->cstream));
+  if (status & 2) raise(XS_ERR_SHAPE, "kernel refused a launch whose shared-memory layout or grid did not match");
+  if (status & 1) raise(XS_ERR_NAN, "a trajectory became non-finite (NaN/Inf) during the path");
+}
+
 xs_status run_path_impl(xs_handle* h, int first_block, int nblocks, int nc, const double* a_in, double* av_out,
                         double* a_out, double* raw_out) {
   return guard([&]() -> xs_status {
@@ -2235,6 +2317,10 @@ xs_status run_path_impl(xs_handle* h, int first_block, int nblocks, int nc, cons
     if (nc == 2 && !h->P.p.checks) raise(XS_ERR_ARG, "coarse pass requested without checks");
     load_module(*h);
     const Problem& P = h->P;
+    if (h->kind == 2 && a_in && !raw_out && nblocks >= 2 && P.F == 1 && P.obs.size() <= 32) {
+      run_stream_pipelined(h, first_block, nblocks, nc, a_in, av_out, a_out);
+      return XS_OK;
+    }
     RawScope raw_scope{h};
     size_t rbytes = 0;
     if (raw_out) {
