@@ -785,7 +785,9 @@ def _dpo_cpu_sample(seconds=10.0, ntraj=4096):
 
 def run_ac3d(args):
     """3D stochastic Allen-Cahn 64^3 (Dirichlet/Neumann/mixed), FP32, 256
-    trajectories, 100 MP steps: one p.path over all blocks per step."""
+    trajectories, 99 MP steps: one p.path over all blocks per step.  Default:
+    the 3D streaming path (plane and z-line passes over the field in HBM);
+    --ac3d-path 1: the resident path with per-CTA device-memory slices."""
     import numpy as np
     import torch
     from xspde_matlab_b200 import GpuPath, _lib, xpreferences
@@ -793,7 +795,7 @@ def run_ac3d(args):
     L = _lib.lib()
     blocks = max(1, args.ac3d_traj // AC_3D["ensembles"][0])
     p = xpreferences([dict(AC_3D, ensembles=[AC_3D["ensembles"][0], blocks, 1])])[0]
-    g = GpuPath(p)
+    g = GpuPath(p, path_kind=args.ac3d_path)
     nb = p.ensembles[1]
     av = torch.zeros((nb * g.per_block,), dtype=torch.float64, device="cuda")
     st = torch.cuda.current_stream()
@@ -801,9 +803,10 @@ def run_ac3d(args):
     def run():
         _lib.check(L.xs_run_path_device(g.h, 0, nb, 1, None, ctypes.c_void_p(av.data_ptr()), None,
                                         ctypes.c_void_p(st.cuda_stream)))
-    for _ in range(max(1, args.warmup)):
+    for _ in range(max(3, args.warmup)):
         run()
     torch.cuda.synchronize()
+    _lib.check(L.xs_sync(g.h))
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with Clocks(torch.cuda.current_device()) as clk:
         e0.record(st)
@@ -812,8 +815,38 @@ def run_ac3d(args):
         e1.record(st)
         e1.synchronize()
     ms = e0.elapsed_time(e1) / args.steps
+    _lib.check(L.xs_sync(g.h))
     steps = p.points[0] * p.steps[0] - 1
     ntraj = nb * p.ensembles[0]
+    # per-pass device times (events around every launch, one more path)
+    nk = len(_lib.KERNEL_KINDS)
+    kms = (ctypes.c_double * nk)()
+    kl = (ctypes.c_longlong * nk)()
+    L.xs_set_kernel_timing(g.h, 1)
+    L.xs_kernel_stats(g.h, 1, None, None)
+    run()
+    torch.cuda.synchronize()
+    _lib.check(L.xs_kernel_stats(g.h, 1, kms, kl))
+    L.xs_set_kernel_timing(g.h, 0)
+    kinds = _lib.KERNEL_KINDS
+    stats = {kinds[i]: {"launches": int(kl[i]), "ms": float(kms[i])} for i in range(nk) if kl[i]}
+    peak, peak_kind = _peaks()
+    field_bytes = ntraj * p.nspace * 8  # complex FP32
+    roof = None
+    if g.kind == 3:
+        # plane pass (x_step) and z-line pass (y_pass): each one read and one write of the field
+        passes = {}
+        for k in ("x_step", "y_pass"):
+            per = stats[k]["ms"] / stats[k]["launches"]
+            ach = 2.0 * field_bytes / (per * 1e-3) / 1e9
+            passes[k] = {"ms_per_launch": per, "achieved": ach, "frac": ach / peak}
+        dom = max(passes, key=lambda k: stats[k]["ms"])
+        roof = {"bound": "hbm", "kernel": dom, "achieved": passes[dom]["achieved"], "peak": peak, "unit": "GB/s",
+                "frac": passes[dom]["frac"], "peak_kind": peak_kind, "traffic": None,
+                "algorithmic_bytes_per_launch": 2.0 * field_bytes, "passes": passes,
+                "step": {"bytes_per_traj_step": 4.0 * p.nspace * 8,
+                         "achieved": ntraj * steps / (ms * 1e-3) * 4.0 * p.nspace * 8 / 1e9,
+                         "frac": ntraj * steps / (ms * 1e-3) * 4.0 * p.nspace * 8 / 1e9 / peak}}
     # oracle sample: one trajectory for a few steps
     from oracle import xspde_ref as X
     o = {k: v for k, v in AC_3D.items() if k not in ("deriv", "initial", "linear", "observe", "precision")}
@@ -833,15 +866,19 @@ def run_ac3d(args):
         a = X.METHODS["MP"](a, q.noisegen(None, 1, q.nscale, q), q)
         n += 1
     cpu = n / (time.perf_counter() - t0)
+    path = ("streaming 3D: plane passes (dense DST/DCT along x and y, MP step) and z-line passes "
+            "(dense DST/DCT along z, FP64 propagator) over the field in HBM" if g.kind == 3 else
+            "resident, field in per-CTA device-memory slices (dense DST/DCT matrices)")
     line = {"metric": "traj-steps/s, 3D stochastic Allen-Cahn 64^3 DST/DCT", "value": ntraj * steps / (ms * 1e-3),
-            "unit": "traj-steps/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "unit": "traj-steps/s", "n_gpus": 1, "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": ms,
             "higher_is_better": True, "dtype": "f32 fields, f64 tables and moments", "data": "synthetic",
-            "path": "resident, field in per-CTA device-memory slices (dense DST/DCT matrices)",
+            "path": path, "kernels": stats, "roofline": roof,
             "cpu_baseline": {"value": cpu, "unit": "traj-steps/s", "cores": 1, "kind": "port",
                              "sample": "1 trajectory x %d MP steps (FP64 NumPy oracle)" % n},
             "clocks": clk.summary(),
             "config": {"workload": "ac_3d: 64^3, x Neumann (DCT-I), y Dirichlet (DST-I), z Neumann-Dirichlet (DCT-III/II), "
-                                   "%d trajectories (%d blocks), 6 points x 20 steps = 99 MP steps" % (ntraj, nb)}}
+                                   "%d trajectories (%d blocks), 6 points x 20 steps = 99 MP steps; field %d MB "
+                                   "(larger than L2)" % (ntraj, nb, field_bytes // 2 ** 20)}}
     print(json.dumps(line))
 
 
@@ -916,6 +953,7 @@ def main():
     ap.add_argument("--mlp-batch", type=int, default=1 << 20)
     ap.add_argument("--ac3d", action="store_true", help="3D stochastic Allen-Cahn 64^3 with DST/DCT boundaries")
     ap.add_argument("--ac3d-traj", type=int, default=256, help="trajectories of --ac3d (multiple of 32)")
+    ap.add_argument("--ac3d-path", type=int, default=0, help="--ac3d device path: 0 automatic (3D streaming), 1 resident")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

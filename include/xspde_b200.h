@@ -142,6 +142,12 @@ XS_API xs_status xs_observe_info(const xs_handle* h, int o, int* lines, int* spa
  * lines*points(1)*(spatial ? nspace : 1) complex doubles, per block. */
 XS_API size_t xs_av_doubles_per_block(const xs_handle* h);
 
+/* Which device path integrates this problem: 1 resident (one CTA per group of
+ * trajectories), 2 streaming 2D (row and column passes), 3 streaming 3D
+ * (plane and z-line passes, DST/DCT in every dimension); 0 for a null handle.
+ * Chosen at xs_create (no GPU needed). */
+XS_API int xs_path_kind(const xs_handle* h);
+
 /* p.path replacement (Simulator/xpath.m): integrate ensemble blocks
  * first_block .. first_block+nblocks-1 (global block index
  * npar-1 + (j-1)*ensembles(3), Simulator/xensemble.m:26) for check pass nc
@@ -265,9 +271,9 @@ enum {
   XS_KERNEL_RESIDENT = 0, /* whole path with fields in shared memory */
   XS_KERNEL_OBS_REDUCE,   /* block means of the resident path */
   XS_KERNEL_X_INIT,       /* streaming: initial field -> K state */
-  XS_KERNEL_X_STEP,       /* streaming: row pass (IFFT_x, drift + noise, FFT_x) */
+  XS_KERNEL_X_STEP,       /* streaming: row pass (IFFT_x, drift + noise, FFT_x); 3D: plane pass */
   XS_KERNEL_X_FINAL,      /* streaming: K state -> x-space field */
-  XS_KERNEL_Y_PASS,       /* streaming: column pass (FFT_y, exp(L dt), IFFT_y) */
+  XS_KERNEL_Y_PASS,       /* streaming: column pass (FFT_y, exp(L dt), IFFT_y); 3D: z-line pass */
   XS_KERNEL_X_OBS,        /* streaming: observables */
   XS_KERNEL_SCALAR,       /* streaming: Int/Ave scalar observables */
   XS_KERNEL_RC_PASS,      /* streaming: row pass of one half of the trajectories fused with the

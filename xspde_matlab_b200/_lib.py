@@ -15,6 +15,7 @@ MAXDIM = 4
 
 # Every symbol include/xspde_b200.h declares.
 EXPORTS = ["xs_create", "xs_destroy", "xs_last_error", "xs_version", "xs_observe_info", "xs_av_doubles_per_block",
+           "xs_path_kind",
            "xs_run_path", "xs_run_path_device", "xs_sync", "xs_noise", "xs_random", "xs_step", "xs_compile_check",
            "xs_set_kernel_timing", "xs_kernel_stats", "xs_run_path_device_noalloc", "xs_noise_features",
            "xs_mlp_sizes", "xs_mlp_forward", "xs_mlp_train_grad", "xs_mlp_adam", "xs_batch_create",
@@ -92,6 +93,8 @@ def lib():
         L.xs_observe_info.restype = ctypes.c_int
         L.xs_av_doubles_per_block.argtypes = [ctypes.c_void_p]
         L.xs_av_doubles_per_block.restype = ctypes.c_size_t
+        L.xs_path_kind.argtypes = [ctypes.c_void_p]
+        L.xs_path_kind.restype = ctypes.c_int
         L.xs_run_path.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
                                   ctypes.c_void_p, ctypes.c_void_p]
         L.xs_run_path.restype = ctypes.c_int

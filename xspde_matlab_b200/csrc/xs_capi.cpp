@@ -14,6 +14,7 @@
 #include <algorithm>
 #include <cmath>
 #include <complex>
+#include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -36,6 +37,8 @@ extern const char* xs_kernel_source_prelude;
 extern const char* xs_kernel_source_noise;
 extern const char* xs_kernel_source_resident;
 extern const char* xs_kernel_source_stream;
+extern const char* xs_kernel_source_stream_common;
+extern const char* xs_kernel_source_stream3;
 
 namespace {
 
@@ -138,6 +141,27 @@ uint64_t fnv1a(const std::string& s, uint64_t h = 1469598103934665603ull) {
     h *= 1099511628211ull;
   }
   return h;
+}
+
+// XSPDE_B200_TRACE=1: one line on stderr per module load step and per kernel launch (name, grid,
+// block, dynamic shared memory), flushed before the call it describes.
+bool trace_on() {
+  static const bool on = [] {
+    const char* e = getenv("XSPDE_B200_TRACE");
+    return e && *e && *e != '0';
+  }();
+  return on;
+}
+
+void trace(const char* fmt, ...) {
+  if (!trace_on()) return;
+  va_list ap;
+  va_start(ap, fmt);
+  fputs("[xspde_b200] ", stderr);
+  vfprintf(stderr, fmt, ap);
+  fputc('\n', stderr);
+  fflush(stderr);
+  va_end(ap);
 }
 
 std::string cache_dir() {
@@ -535,6 +559,23 @@ std::vector<cd> transform_matrix(int type, bool inv, int N) {
   return M;
 }
 
+// Mirror symmetry of an n x n transform matrix: 1 + p when M[n-1-i][k] = (-1)^(k+p) M[i][k] for
+// every i, k (DCT-I and DCT-II: p = 0; DST-I on xSPDE's endpoint-inclusive lattice: p = 1), else 0.
+int fold_parity(const std::vector<cd>& M, int n) {
+  double mx = 0;
+  for (const auto& v : M) mx = std::max(mx, std::abs(v));
+  for (int par = 0; par < 2; ++par) {
+    bool ok = true;
+    for (int i = 0; i < n && ok; ++i)
+      for (int k = 0; k < n && ok; ++k) {
+        const cd x = M[(size_t)(n - 1 - i) * n + k], y = M[(size_t)i * n + k] * ((k + par) % 2 ? -1.0 : 1.0);
+        if (std::abs(x - y) > 1e-12 * mx) ok = false;
+      }
+    if (ok) return 1 + par;
+  }
+  return 0;
+}
+
 // ---------------------------------------------------------------------------
 // Code generation
 // ---------------------------------------------------------------------------
@@ -901,6 +942,12 @@ struct StreamPlan {
   int RX = 0, RY = 0, XROWS = 0, TX = 0, OROWS = 0;
   size_t xsmem = 0, ssmem = 0, osmem = 0, tsmem = 0;
   size_t rksmem = 0;  // RK4 row passes: twiddles + two stages per row
+  // 3D: z-line tile width, per matrix (x, y, z; forward, inverse) its fold (0 or 1 + parity) and
+  // offset in the matrix table, shared memory of the plane passes (to K state, step, final), the
+  // z-line pass and the observation pass
+  int QT = 0;
+  int fold3[6] = {0, 0, 0, 0, 0, 0}, moff3[6] = {0, 0, 0, 0, 0, 0};
+  size_t psmem3[3] = {0, 0, 0}, zsmem3 = 0, osmem3 = 0;
 };
 
 }  // namespace
@@ -910,7 +957,7 @@ struct xs_handle {
   std::string header;     // generated problem header
   std::string source;     // full kernel source
   bool fp64 = true;
-  int kind = 1;           // 1 resident, 2 streaming
+  int kind = 1;           // 1 resident, 2 streaming (2D), 3 streaming (3D, DST/DCT)
   ResidentPlan rp;
   // device state
   bool loaded = false;
@@ -921,6 +968,10 @@ struct xs_handle {
              f_scalar = nullptr;
   CUfunction f_xrk[3] = {nullptr, nullptr, nullptr};  // RK4 row passes 1, 2, 3 (streaming)
   DevBuf d_field2;                                      // RK4: second streaming field
+  CUfunction f_pinit = nullptr, f_ptok = nullptr, f_pnl = nullptr, f_pfinal = nullptr, f_zpass = nullptr,
+             f_pobs = nullptr;  // 3D
+  DevBuf d_mat3;                                        // 3D: real transform matrices
+  int grid_p = 0, grid_z = 0;                           // 3D: persistent grids of the plane and z-line passes
   StreamPlan sp;
   int path_kind = 0;
   int force_G = 0, force_threads = 0;  // resident tile fixed by the caller (uneven batch)
@@ -1179,12 +1230,8 @@ int isqrt_pow2(int n) {
 }
 
 // Reason why the streaming path cannot run this problem, or "" when it can.
-std::string stream_blocker(const Problem& P) {
-  if (P.D != 2) return "the streaming path covers two space dimensions";
-  if (!isqrt_pow2(P.N[0]) || !isqrt_pow2(P.N[1])) return "streaming lattices need 64, 256 or 1024 points per dimension";
-  for (int v : P.bnd)
-    if (v) return "the streaming path covers periodic boundaries";
-  if (P.p.method != XS_METHOD_MP && P.p.method != XS_METHOD_RK4) return "the streaming path integrates with MP or RK4";
+// Observables, noises and drifts the streaming passes do not cover (2D and 3D).
+std::string stream_common_blocker(const Problem& P) {
   if (!P.has_linear) return "the streaming path needs p.linear";
   for (auto& o : P.obs)
     if (o.spatial && !o.gen.reductions.empty()) return "site observables that use Int/Ave are not streamed";
@@ -1195,6 +1242,30 @@ std::string stream_blocker(const Problem& P) {
   if (P.stencil) return "observables with D1/D2 finite differences are not streamed";
   if (P.dstencil) return "drifts with D1/D2 finite differences are not streamed";
   return "";
+}
+
+std::string stream_blocker(const Problem& P) {
+  if (P.D != 2) return "the streaming path covers two space dimensions";
+  if (!isqrt_pow2(P.N[0]) || !isqrt_pow2(P.N[1])) return "streaming lattices need 64, 256 or 1024 points per dimension";
+  for (int v : P.bnd)
+    if (v) return "the streaming path covers periodic boundaries";
+  if (P.p.method != XS_METHOD_MP && P.p.method != XS_METHOD_RK4) return "the streaming path integrates with MP or RK4";
+  return stream_common_blocker(P);
+}
+
+// 3D lattices with a DST/DCT transform in every dimension (xs_stream3.cuh).
+std::string stream3_blocker(const Problem& P) {
+  if (P.D != 3) return "the 3D streaming path covers three space dimensions";
+  for (int d = 0; d < 3; ++d)
+    if (P.N[d] < 8 || P.N[d] > 64 || P.N[d] % 4)
+      return "3D streaming lattices need 8 to 64 points per dimension, a multiple of 4";
+  if ((P.N[0] * P.N[1]) % 64) return "3D streaming needs N1*N2 to be a multiple of 64";
+  if (P.F != 1) return "the 3D streaming path covers one field component";
+  for (int d = 0; d < 3; ++d)
+    if (P.type(d, 0) == 0) return "the 3D streaming path covers non-periodic (DST/DCT) boundaries in every dimension";
+  if (P.p.method != XS_METHOD_MP) return "the 3D streaming path integrates with MP";
+  if (P.bvals) return "boundary values (p.boundfun) are not streamed";
+  return stream_common_blocker(P);
 }
 
 // Straight-line radix-2 DIT DFT of R points (forward, exp(-2 pi i n k / R)),
@@ -1262,6 +1333,33 @@ void plan_stream(xs_handle& h) {
   h.sp = sp;
 }
 
+// 3D streaming plan: matrix i = 2 d + inverse (d = x, y, z) at offset moff3[i] of the table, folded
+// when it is mirror-symmetric; shared memory of each pass as xs_stream3.cuh lays it out (matrices
+// in `real`, then the plane [N2][N1 + 1] or the z-line tile [N3][QT + 1] in complex `real`).
+void plan_stream3(xs_handle& h) {
+  const Problem& P = h.P;
+  StreamPlan sp;
+  sp.QT = 64;
+  const size_t rs = h.fp64 ? 8 : 4, cxs = 2 * rs;
+  int off = 0;
+  size_t msize[6];
+  for (int i = 0; i < 6; ++i) {
+    const int d = i / 2, n = P.N[d];
+    sp.moff3[i] = off;
+    off += n * n;
+    sp.fold3[i] = fold_parity(transform_matrix(P.type(d, 0), i % 2 == 1, n), n);
+    msize[i] = (size_t)(sp.fold3[i] ? n / 2 : n) * n;
+  }
+  const size_t plane = (size_t)P.N[1] * (P.N[0] + 1) * cxs;
+  sp.psmem3[0] = (msize[0] + msize[2]) * rs + plane;
+  sp.psmem3[1] = (msize[0] + msize[1] + msize[2] + msize[3]) * rs + plane;
+  sp.psmem3[2] = (msize[1] + msize[3]) * rs + plane;
+  sp.osmem3 = sp.psmem3[2];
+  sp.zsmem3 = (msize[4] + msize[5]) * rs + (size_t)P.N[2] * (sp.QT + 1) * cxs;
+  if ((P.N[0] * P.N[1]) % sp.QT) raise(XS_ERR_SHAPE, "internal: z-line tiles do not divide the plane");
+  h.sp = sp;
+}
+
 void emit_common_header(const xs_handle& h, std::ostringstream& os) {
   const Problem& P = h.P;
   os << "// generated problem header\n";
@@ -1291,13 +1389,26 @@ void build_source(xs_handle& h) {
   if (P.bvals && (P.stencil || P.dstencil))
     raise(XS_ERR_UNSUPPORTED, "D1/D2 use zero boundary values on the device: not combined with p.boundfun values");
   const bool fits = resident_smem(h, 1, method_arrays(P)) <= 200 * 1024;
-  const std::string why = stream_blocker(P);
+  const std::string why = P.D == 3 ? stream3_blocker(P) : stream_blocker(P);
   // too large for shared memory: the streaming path when it covers the problem, else the resident
   // path with the field in device memory (MP)
   if (h.path_kind == 2 || (h.path_kind == 0 && !fits && why.empty())) {
     if (!why.empty()) {
       if (!fits) raise(XS_ERR_UNSUPPORTED, "field too large for the resident path, and " + why);
       raise(XS_ERR_UNSUPPORTED, why);
+    }
+    if (P.D == 3) {
+      h.kind = 3;
+      plan_stream3(h);
+      std::ostringstream os;
+      emit_common_header(h, os);
+      os << "#define XS3_QT " << h.sp.QT << "\n";
+      for (int i = 0; i < 6; ++i)
+        os << "#define XS3_MOFF" << i << " " << h.sp.moff3[i] << "\n#define XS3_FOLD" << i << " " << h.sp.fold3[i] << "\n";
+      os << fns.str();
+      os << xs_kernel_source_stream_common << "\n" << xs_kernel_source_stream3 << "\n";
+      h.source = os.str();
+      return;
     }
     h.kind = 2;
     plan_stream(h);
@@ -1311,7 +1422,7 @@ void build_source(xs_handle& h) {
     os << "template <int R> __device__ __forceinline__ void xs_dftR(cx (&v)[R]);\n";
     os << gen_dft(h.sp.RX);
     if (h.sp.RY != h.sp.RX) os << gen_dft(h.sp.RY);
-    os << xs_kernel_source_stream << "\n";
+    os << xs_kernel_source_stream_common << "\n" << xs_kernel_source_stream << "\n";
     h.source = os.str();
     return;
   }
@@ -1356,20 +1467,7 @@ void build_source(xs_handle& h) {
       int fold = (real_m && h.rp.gfield && !fft_dim(P, d) && P.N[d] % 4 == 0) ? -1 : 0;
       for (int f = 0; f < P.F && fold; ++f)
         for (int dir = 0; dir < 2 && fold; ++dir) {
-          const int n = P.N[d];
-          const auto M = transform_matrix(P.type(d, f), dir == 1, n);
-          double mx = 0;
-          for (const auto& v : M) mx = std::max(mx, std::abs(v));
-          int found = 0;
-          for (int par = 0; par < 2 && !found; ++par) {
-            bool ok = true;
-            for (int i = 0; i < n && ok; ++i)
-              for (int k = 0; k < n && ok; ++k) {
-                const cd a = M[(size_t)(n - 1 - i) * n + k], b = M[(size_t)i * n + k] * ((k + par) % 2 ? -1.0 : 1.0);
-                if (std::abs(a - b) > 1e-12 * mx) ok = false;
-              }
-            if (ok) found = 1 + par;
-          }
+          const int found = fold_parity(transform_matrix(P.type(d, f), dir == 1, P.N[d]), P.N[d]);
           fold = (found && (fold < 0 || fold == found)) ? found : 0;
         }
       os << "#define XS_FOLD" << d + 1 << " " << (fold > 0 ? fold : 0) << "\n";
@@ -1392,6 +1490,60 @@ void load_module(xs_handle& h) {
   if (h.loaded) return;
   ensure_device();
   upload_params(h);
+  if (h.kind == 3) {
+    trace("load: compile xs_stream3");
+    std::string cubin = nvrtc_compile(h.source, "xs_stream3", nullptr);
+    Driver& d = driver();
+    trace("load: module (%zu bytes)", cubin.size());
+    cu_check(d.load(&h.mod, cubin.data()), "cuModuleLoadData");
+    const StreamPlan& sp = h.sp;
+    struct {
+      CUfunction* f;
+      const char* name;
+      size_t smem;
+    } fns[] = {{&h.f_pinit, "xs_p_init", 0}, {&h.f_ptok, "xs_p_tok", sp.psmem3[0]}, {&h.f_pnl, "xs_p_nl", sp.psmem3[1]},
+               {&h.f_pfinal, "xs_p_final", sp.psmem3[2]}, {&h.f_zpass, "xs_z_pass", sp.zsmem3},
+               {&h.f_pobs, "xs_p_obs", sp.osmem3}, {&h.f_scalar, "xs_stream_scalar", 0},
+               {&h.f_xcomb, "xs_x_obs_combine", 0}, {&h.f_noise, "xs_export_noise", 0},
+               {&h.f_random, "xs_export_random", 0}, {&h.f_feat, "xs_noise_features", 0}};
+    for (auto& f : fns) {
+      cu_check(d.getfn(f.f, h.mod, f.name), f.name);
+      if (f.smem > 48 * 1024)
+        cu_check(d.setattr(*f.f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, (int)f.smem), f.name);
+    }
+    {  // persistent grids: every SM filled with as many CTAs as fit
+      int dev = 0, sms = 0, occ_p = 0, occ_z = 0;
+      CUDA_CHECK(cudaGetDevice(&dev));
+      CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+      trace("load: occupancy (plane pass %zu B, z-line pass %zu B of shared memory)", sp.psmem3[1], sp.zsmem3);
+      cu_check(d.occupancy(&occ_p, h.f_pnl, 256, sp.psmem3[1]), "occupancy");
+      cu_check(d.occupancy(&occ_z, h.f_zpass, 256, sp.zsmem3), "occupancy");
+      trace("load: %d SMs, %d plane-pass and %d z-line-pass CTAs per SM", sms, occ_p, occ_z);
+      if (occ_p < 1 || occ_z < 1) raise(XS_ERR_UNSUPPORTED, "3D streaming passes cannot be resident on an SM");
+      h.grid_p = sms * occ_p;
+      h.grid_z = sms * occ_z;
+    }
+    CUDA_CHECK(cudaStreamCreateWithFlags(&h.stream, cudaStreamNonBlocking));
+    {  // the reference's transforms as real matrices M[n*N + k], FP64-built (xs_stream3.cuh)
+      const Problem& P = h.P;
+      std::vector<double> all;
+      for (int i = 0; i < 6; ++i) {
+        const int dd = i / 2, n = P.N[dd];
+        for (const cd& v : transform_matrix(P.type(dd, 0), i % 2 == 1, n)) all.push_back(v.real());
+      }
+      if (h.fp64) {
+        h.d_mat3.ensure(all.size() * 8);
+        CUDA_CHECK(cudaMemcpy(h.d_mat3.p, all.data(), all.size() * 8, cudaMemcpyHostToDevice));
+      } else {
+        std::vector<float> f32(all.begin(), all.end());
+        h.d_mat3.ensure(f32.size() * 4);
+        CUDA_CHECK(cudaMemcpy(h.d_mat3.p, f32.data(), f32.size() * 4, cudaMemcpyHostToDevice));
+      }
+    }
+    h.d_status.ensure(sizeof(int));
+    h.loaded = true;
+    return;
+  }
   if (h.kind == 2) {
     std::string cubin = nvrtc_compile(h.source, "xs_stream", nullptr);
     Driver& d = driver();
@@ -1621,6 +1773,7 @@ void xs_launch(xs_handle& h, int kind, CUfunction f, unsigned gx, unsigned gy, u
     b = take_event(h);
     CUDA_CHECK(cudaEventRecord(a, st));
   }
+  trace("launch %s grid (%u, %u, %u) block %u smem %u", what, gx, gy, gz, bx, smem);
   cu_check(driver().launch(f, gx, gy, gz, bx, 1, 1, smem, (CUstream)st, params, nullptr), what);
   h.launches[kind]++;
   if (h.timing) {
@@ -1801,6 +1954,8 @@ struct StreamArgsHost {
   void* field2;
   int ndraw0, ndraw1;
   int fuse;
+  const void* mat;
+  int xspace;
 };
 
 // Observation pass: each block's trajectories split over kObsSplit CTAs (grid z) for latency
@@ -1938,11 +2093,103 @@ void launch_stream_halves(xs_handle& h, const StreamArgsHost& a, int nblocks, in
   }
 }
 
+// Streaming schedule of one xpath call on a 3D DST/DCT lattice (xs_stream3.cuh): the pass
+// sequence of the 2D path (stream_ops), z-line passes in place of the column passes and plane
+// passes in place of the row passes, on persistent grids.
+void launch_stream3(xs_handle& h, int first_block, int nblocks, int nc, const void* a_in_dev, void* av_dev,
+                    void* a_out_dev, cudaStream_t st) {
+  const Problem& P = h.P;
+  const StreamPlan& sp = h.sp;
+  const int total = nblocks * P.E1;
+  const size_t cxs = h.fp64 ? 16 : 8;
+  h.d_field.ensure((size_t)total * P.NS * cxs);
+  const int nz = P.N[2];
+  if (P.nred) h.d_redpart.ensure((size_t)total * nz * P.nred * 16);
+  StreamArgsHost a{};
+  a.ntraj = total;
+  a.ens1 = P.E1;
+  a.block0 = first_block;
+  a.seq = P.p.sequence;
+  a.seed = (unsigned)(P.p.seed & 0xffffffffu);
+  a.draw1 = -1;
+  a.npoints = P.p.points[0];
+  a.wscale = std::sqrt(P.nscale * P.noisefactor);
+  a.vscale = std::sqrt(P.noisefactor);
+  a.dtr = pass_dtr(P, nc);
+  a.field = h.d_field.p;
+  a.prop1 = ensure_prop(h, nc);
+  a.prop2 = ensure_prop2(h, nc);
+  a.a_in = a_in_dev;
+  a.a_out = a_out_dev;
+  a.av = av_dev;
+  a.redpart = h.d_redpart.p;
+  a.status = (int*)h.d_status.p;
+  a.params = (const double*)h.d_params.p;
+  a.mat = h.d_mat3.p;
+  if (P.nout_site) {
+    h.d_opart.ensure((size_t)kObsSplit * nblocks * P.nout_site * P.NS * 16);
+    a.opart = h.d_opart.p;
+  }
+  void* params[] = {&a};
+  const size_t nplanes = (size_t)total * nz, ntiles = (size_t)total * (P.N[0] * P.N[1] / sp.QT);
+  const unsigned gp = (unsigned)std::min<size_t>(nplanes, (size_t)h.grid_p);
+  const unsigned gz = (unsigned)std::min<size_t>(ntiles, (size_t)h.grid_z);
+  // the initial field stays in x space until its first observation has been taken (the
+  // transforms drop Dirichlet boundary values, which that observation still sees)
+  bool xspace = false;
+  for (const StreamOp& o : stream_ops(P, nc, a_out_dev != nullptr)) {
+    a.m = o.m;
+    a.draw0 = o.draw0;
+    a.draw1 = o.draw1;
+    a.n = o.n;
+    a.t = o.t;
+    if (xspace && (o.kind == StreamOp::ROW || o.kind == StreamOp::COL)) {
+      a.xspace = 0;
+      xs_launch(h, XS_KERNEL_X_INIT, h.f_ptok, gp, 1, 1, 256, (unsigned)sp.psmem3[0], st, params, "plane pass");
+      xspace = false;
+    }
+    a.xspace = xspace ? 1 : 0;
+    switch (o.kind) {
+      case StreamOp::INIT: {
+        const unsigned gi = (unsigned)std::min<size_t>(((size_t)total * P.NS + 255) / 256, (size_t)h.grid_p * 8);
+        xs_launch(h, XS_KERNEL_X_INIT, h.f_pinit, gi, 1, 1, 256, 0, st, params, "initial field");
+        xspace = true;
+        break;
+      }
+      case StreamOp::ROW:
+        xs_launch(h, XS_KERNEL_X_STEP, h.f_pnl, gp, 1, 1, 256, (unsigned)sp.psmem3[1], st, params, "plane pass");
+        break;
+      case StreamOp::FINAL:
+        xs_launch(h, XS_KERNEL_X_FINAL, h.f_pfinal, gp, 1, 1, 256, (unsigned)sp.psmem3[2], st, params, "plane pass");
+        break;
+      case StreamOp::COL:
+        xs_launch(h, XS_KERNEL_Y_PASS, h.f_zpass, gz, 1, 1, 256, (unsigned)sp.zsmem3, st, params, "z-line pass");
+        break;
+      case StreamOp::OBS:
+        xs_launch(h, XS_KERNEL_X_OBS, h.f_pobs, (unsigned)nz, (unsigned)nblocks, kObsSplit, 256, (unsigned)sp.osmem3, st,
+                  params, "observation pass");
+        if (P.nout_site) {
+          int nsplit = kObsSplit;
+          void* cprm[] = {params[0], &nsplit};
+          const unsigned gx = (unsigned)(((size_t)P.nout_site * P.NS + 255) / 256);
+          xs_launch(h, XS_KERNEL_X_OBS, h.f_xcomb, gx, (unsigned)nblocks, 1, 256, 0, st, cprm, "observation combine");
+        }
+        if (P.nout_scalar)
+          xs_launch(h, XS_KERNEL_SCALAR, h.f_scalar, (unsigned)nblocks, 1, 1, 256, 0, st, params, "scalar observables");
+        break;
+    }
+  }
+}
+
 // Streaming schedule of one xpath call (Simulator/xpath.m:29-86) for MP:
 // column passes apply the pending half-step propagators, row passes do the
 // midpoint step; observations need all half steps applied first.
 void launch_stream(xs_handle& h, int first_block, int nblocks, int nc, const void* a_in_dev, void* av_dev,
                    void* a_out_dev, cudaStream_t st) {
+  if (h.kind == 3) {
+    launch_stream3(h, first_block, nblocks, nc, a_in_dev, av_dev, a_out_dev, st);
+    return;
+  }
   const Problem& P = h.P;
   const StreamPlan& sp = h.sp;
   const int total = nblocks * P.E1;
@@ -2204,7 +2451,7 @@ XS_API xs_status xs_compile_check(const xs_problem* prob, char* log, size_t n) {
     xs_handle h;
     create_impl(prob, &h);
     std::string lg;
-    nvrtc_compile(h.source, h.kind == 2 ? "xs_stream" : "xs_resident", &lg);
+    nvrtc_compile(h.source, h.kind == 3 ? "xs_stream3" : h.kind == 2 ? "xs_stream" : "xs_resident", &lg);
     if (log && n) {
       size_t m = std::min(n - 1, lg.size());
       memcpy(log, lg.data(), m);
@@ -2225,6 +2472,8 @@ XS_API xs_status xs_observe_info(const xs_handle* h, int o, int* lines, int* spa
 }
 
 XS_API size_t xs_av_doubles_per_block(const xs_handle* h) { return h ? av_doubles_per_block(h->P) : 0; }
+
+XS_API int xs_path_kind(const xs_handle* h) { return h ? h->kind : 0; }
 
 namespace {
 struct RawScope {  // the raw-trajectory pointer belongs to one xs_run_path_raw call
@@ -2317,7 +2566,7 @@ xs_status run_path_impl(xs_handle* h, int first_block, int nblocks, int nc, cons
     if (nc == 2 && !h->P.p.checks) raise(XS_ERR_ARG, "coarse pass requested without checks");
     load_module(*h);
     const Problem& P = h->P;
-    if (h->kind == 2 && a_in && !raw_out && nblocks >= 2 && P.F == 1 && P.obs.size() <= 32) {
+    if (h->kind >= 2 && a_in && !raw_out && nblocks >= 2 && P.F == 1 && P.obs.size() <= 32) {
       run_stream_pipelined(h, first_block, nblocks, nc, a_in, av_out, a_out);
       return XS_OK;
     }
@@ -2359,7 +2608,7 @@ xs_status run_path_impl(xs_handle* h, int first_block, int nblocks, int nc, cons
     const size_t avd = (size_t)nblocks * P.p.points[0] * stride * 2;
     h->d_av.ensure(std::max<size_t>(avd, 1) * 8);
     CUDA_CHECK(cudaMemsetAsync(h->d_status.p, 0, sizeof(int), h->stream));
-    if (h->kind == 2) launch_stream(*h, first_block, nblocks, nc, din, h->d_av.p, dout, h->stream);
+    if (h->kind >= 2) launch_stream(*h, first_block, nblocks, nc, din, h->d_av.p, dout, h->stream);
     else launch_resident(*h, first_block, nblocks, nc, din, h->d_av.p, dout, h->stream);
     // block means into MATLAB's layout on the device, then one copy into the caller's buffer
     const size_t per_block = av_doubles_per_block(P);
@@ -2430,7 +2679,7 @@ XS_API xs_status xs_run_path_device(xs_handle* h, int first_block, int nblocks, 
     load_module(*h);
     cudaStream_t st = (cudaStream_t)stream;  // the caller's stream; NULL is the default stream
     CUDA_CHECK(cudaMemsetAsync(h->d_status.p, 0, sizeof(int), st));
-    if (h->kind == 2) launch_stream(*h, first_block, nblocks, nc, a_in_dev, av_dev, a_out_dev, st);
+    if (h->kind >= 2) launch_stream(*h, first_block, nblocks, nc, a_in_dev, av_dev, a_out_dev, st);
     else launch_resident(*h, first_block, nblocks, nc, a_in_dev, av_dev, a_out_dev, st);
     return XS_OK;
   });
@@ -3271,7 +3520,7 @@ void batch_prepare(xs_batch& b) {
     if (ep->variant < 0) raw.push_back(ep->h.get());
   {
     std::vector<xs_handle*> res, str;
-    for (auto* h : raw) (h->kind == 2 ? str : res).push_back(h);
+    for (auto* h : raw) (h->kind >= 2 ? str : res).push_back(h);
     compile_all(res);
     std::vector<std::string> errs(str.size());
     std::vector<std::thread> th;
@@ -3304,7 +3553,8 @@ void batch_prepare(xs_batch& b) {
       xs_handle& h = *b.items[i]->h;
       const Problem& P = h.P;
       h.d_field.ensure((size_t)P.E1 * P.F * P.NS * (h.fp64 ? 16 : 8));
-      if (P.nred) h.d_redpart.ensure((size_t)P.E1 * (P.N[1] / h.sp.OROWS) * P.nred * 16);
+      const int parts = h.kind == 3 ? P.N[2] : P.N[1] / h.sp.OROWS;  // reduction parts per trajectory
+      if (P.nred) h.d_redpart.ensure((size_t)P.E1 * parts * P.nred * 16);
       if (P.nout_site) h.d_opart.ensure((size_t)kObsSplit * P.nout_site * P.NS * 16);
       ensure_prop(h, 1);
       ensure_prop2(h, 1);

@@ -295,6 +295,8 @@ class GpuPath:
             _lib.check(L.xs_observe_info(h, o, ctypes.byref(ln), ctypes.byref(sp)))
             self.obs.append((ln.value, bool(sp.value)))
         self.per_block = L.xs_av_doubles_per_block(h)
+        # 1 resident, 2 streaming 2D, 3 streaming 3D (xs_path_kind)
+        self.kind = L.xs_path_kind(h)
 
     def __del__(self):
         h = getattr(self, "h", None)
