@@ -15,11 +15,19 @@
 //
 // Every transform is the reference's real matrix (built on the host in FP64 by
 // applying the reference's transform to unit vectors), applied densely from
-// shared memory: out[k] = sum_n M[n][k] in[n].  A matrix with the mirror
-// symmetry M[N-1-n][k] = (-1)^(k+p) M[n][k] (DCT-I: p = 0; DST-I on the
-// endpoint-inclusive lattice: p = 1) is applied folded, half the multiply-adds:
-// u_n = in[n] + in[N-1-n], v_n = in[n] - in[N-1-n], outputs with k + p even sum
-// M[n][k] u_n over n < N/2, the others M[n][k] v_n.
+// shared memory: out[k] = sum_n M[n][k] in[n].  Each matrix of these transforms
+// is mirror-symmetric about a centre C in N-1, N-2 or N (DCT-I and DST-I: N - 1;
+// DCT-II/III: N - 2 with row or column N - 1 zero; DST-II/III: N with row or
+// column 0 zero), which halves its multiply-adds:
+//   input fold, M[C-n][k] = (-1)^(k+p) M[n][k]: u_n = in[n] + in[C-n] and
+//     v_n = in[n] - in[C-n] over the first half of the rows; outputs with k + p
+//     even sum M[n][k] u_n, the others M[n][k] v_n (DCT-I, DST-I, DCT-II, DST-II);
+//   output fold, M[n][C-k] = (-1)^(n+p) M[n][k]: E_k sums the inputs with n + p
+//     even, O_k the others, over the first half of the outputs; out[k] = E + O,
+//     out[C-k] = E - O (DCT-III, DST-III).
+// The host packs the half of each matrix that is read (rows for an input fold,
+// columns for an output fold) and sets its entries that the symmetry makes zero
+// to exactly zero.
 //
 // Passes are persistent: gridDim.x CTAs walk the planes (or z-line tiles) with
 // stride gridDim.x, so each CTA stages its matrices in shared memory once.
@@ -29,24 +37,31 @@
 #define XS3_N2 XS_N2
 #define XS3_N3 XS_N3
 #define XS3_NP (XS_N1 * XS_N2)         // sites per plane
-#define XS3_LSX (XS_N1 + 1)            // plane row stride in shared memory (complex elements)
-#define XS3_LSQ (XS3_QT + 1)           // z-tile row stride
+// XS3_LSX, XS3_LSQ (host): row strides of the plane and of the z-line tile in shared memory, in
+// complex elements; even in FP32, so that four consecutive elements of a row are one pair of
+// 16-byte loads
 #define XS_NRG XS_N3                   // reduction parts per trajectory: one per plane
 
-// Matrix i (0 x fwd, 1 x inv, 2 y fwd, 3 y inv, 4 z fwd, 5 z inv) in A.mat: offset
-// XS3_MOFFi, N_d x N_d reals; XS3_FOLDi = 0 (applied in full) or 1 + p (folded).
+// Matrix i (0 x fwd, 1 x inv, 2 y fwd, 3 y inv, 4 z fwd, 5 z inv) in A.mat at offset
+// XS3_MOFFi; XS3_FOLDi = 0 (full N x N), 1 (input fold: N/2 packed rows of N) or 2 (output
+// fold: N rows of N/2 packed columns), about centre XS3_CENi with parity XS3_PARi.
 template <int I> struct Xs3Mat;
-template <> struct Xs3Mat<0> { static constexpr int N = XS_N1, OFF = XS3_MOFF0, FOLD = XS3_FOLD0; };
-template <> struct Xs3Mat<1> { static constexpr int N = XS_N1, OFF = XS3_MOFF1, FOLD = XS3_FOLD1; };
-template <> struct Xs3Mat<2> { static constexpr int N = XS_N2, OFF = XS3_MOFF2, FOLD = XS3_FOLD2; };
-template <> struct Xs3Mat<3> { static constexpr int N = XS_N2, OFF = XS3_MOFF3, FOLD = XS3_FOLD3; };
-template <> struct Xs3Mat<4> { static constexpr int N = XS_N3, OFF = XS3_MOFF4, FOLD = XS3_FOLD4; };
-template <> struct Xs3Mat<5> { static constexpr int N = XS_N3, OFF = XS3_MOFF5, FOLD = XS3_FOLD5; };
-// reals of shared memory a matrix occupies: the rows the transform reads (the first half when folded)
-template <int I> __host__ __device__ constexpr int xs3_mrows() { return Xs3Mat<I>::FOLD ? Xs3Mat<I>::N / 2 : Xs3Mat<I>::N; }
-template <int I> __host__ __device__ constexpr int xs3_msize() { return xs3_mrows<I>() * Xs3Mat<I>::N; }
+#define XS3_MAT(I, NN)                                                                                  \
+  template <> struct Xs3Mat<I> {                                                                       \
+    static constexpr int N = NN, OFF = XS3_MOFF##I, FOLD = XS3_FOLD##I, C = XS3_CEN##I, PAR = XS3_PAR##I; \
+  };
+XS3_MAT(0, XS_N1)
+XS3_MAT(1, XS_N1)
+XS3_MAT(2, XS_N2)
+XS3_MAT(3, XS_N2)
+XS3_MAT(4, XS_N3)
+XS3_MAT(5, XS_N3)
+// reals of shared memory a matrix occupies (the packed half when folded)
+template <int I> __host__ __device__ constexpr int xs3_msize() {
+  return Xs3Mat<I>::FOLD ? Xs3Mat<I>::N * (Xs3Mat<I>::N / 2) : Xs3Mat<I>::N * Xs3Mat<I>::N;
+}
 
-// Copy matrix I's rows into shared memory (all threads of the CTA; caller syncs).
+// Copy matrix I into shared memory (all threads of the CTA; caller syncs).
 template <int I>
 __device__ __forceinline__ void xs3_stage_matrix(real* dst, const real* __restrict__ mat) {
   const real* src = mat + Xs3Mat<I>::OFF;
@@ -71,70 +86,193 @@ __device__ __forceinline__ void xs3_load4(const real* p, real (&m)[4]) {
   }
 }
 
+// Two consecutive complex elements (16-byte aligned in FP32).
+__device__ __forceinline__ void xs3_load2(const cx* p, cx& a, cx& b) {
+  if constexpr (sizeof(real) == 4) {
+    const float4 q = *reinterpret_cast<const float4*>(p);
+    a = mkcx((real)q.x, (real)q.y);
+    b = mkcx((real)q.z, (real)q.w);
+  } else {
+    a = p[0];
+    b = p[1];
+  }
+}
+
+// Row of the folded index j: the u row (input fold) or the output (output fold), and its
+// partner C - r, or the zero row/column slot when j is its own partner.
+template <int N, int C> __device__ __forceinline__ constexpr int xs3_fr(int j) { return j + (C == N ? 1 : 0); }
+template <int N, int C> __device__ __forceinline__ constexpr int xs3_fp(int j) {
+  return C - xs3_fr<N, C>(j) != xs3_fr<N, C>(j) ? C - xs3_fr<N, C>(j) : (C == N ? 0 : N - 1);
+}
+
 // In-place dense transform of the NL lines of length ND held in `buf` by the
 // 256 threads of the CTA with the matrix I staged at Ms.  FORM_R: element n of
 // line l at buf[n*LS + l] (lines are columns); otherwise at buf[l*LS + n]
-// (lines are rows).  Thread tid < (ND/4)(NL/4) computes outputs k0..k0+3 of
-// lines l0..l0+3 in registers; a barrier separates all reads from the writes.
+// (lines are rows).  Each active thread computes 4 outputs of 4 lines in
+// registers; a barrier separates all reads from the writes.
 template <int I, int NL, int LS, bool FORM_R>
 __device__ __forceinline__ void xs3_dense(cx* buf, const real* __restrict__ Ms, int tid) {
-  constexpr int ND = Xs3Mat<I>::N, FOLD = Xs3Mat<I>::FOLD;
-  constexpr int PAR = FOLD > 1 ? 1 : 0;
-  constexpr int NN = FOLD ? ND / 2 : ND;
+  constexpr int ND = Xs3Mat<I>::N, FOLD = Xs3Mat<I>::FOLD, C = Xs3Mat<I>::C, PAR = Xs3Mat<I>::PAR;
+  constexpr int H = ND / 2;
   auto idx = [](int n, int l) { return FORM_R ? n * LS + l : l * LS + n; };
-  if constexpr (FOLD > 0) {
-    for (int i = tid; i < (ND / 2) * NL; i += 256) {
+  // four consecutive lines of element n: two 16-byte loads when the lines are columns
+  auto lines4 = [&](int n, int l0, cx (&x)[4]) {
+    if constexpr (FORM_R) {
+      xs3_load2(buf + n * LS + l0, x[0], x[1]);
+      xs3_load2(buf + n * LS + l0 + 2, x[2], x[3]);
+    } else {
+#pragma unroll
+      for (int j = 0; j < 4; ++j) x[j] = buf[(l0 + j) * LS + n];
+    }
+  };
+  if constexpr (FOLD == 1) {
+    for (int i = tid; i < H * NL; i += 256) {
       // consecutive threads take consecutive shared-memory words
-      const int n = FORM_R ? i / NL : i % (ND / 2), l = FORM_R ? i % NL : i / (ND / 2);
-      const cx a = buf[idx(n, l)], b = buf[idx(ND - 1 - n, l)];
-      buf[idx(n, l)] = a + b;
-      buf[idx(ND - 1 - n, l)] = a - b;
+      const int j = FORM_R ? i / NL : i % H, l = FORM_R ? i % NL : i / H;
+      const int r = xs3_fr<ND, C>(j), q = xs3_fp<ND, C>(j);
+      const bool self = C - r == r;  // its own partner: v is multiplied by zeros only
+      const cx a = buf[idx(r, l)], b = self ? mkcx((real)0, (real)0) : buf[idx(q, l)];
+      buf[idx(r, l)] = a + b;
+      buf[idx(q, l)] = a - b;
     }
     __syncthreads();
   }
-  constexpr int NKG = ND / 4, NT = NKG * (NL / 4);
+  constexpr int NOUT = FOLD == 2 ? H : ND;  // outputs computed per line (the first half when folded)
+  constexpr int NKG = NOUT / 4, NT = NKG * (NL / 4);
   static_assert(NT <= 256, "one output tile per thread");
   const bool act = tid < NT;
   const int k0 = 4 * (tid % NKG), l0 = 4 * (tid / NKG);
-  real ar[4][4], ai[4][4];
+  real ar[4][4], ai[4][4], br[4][4], bi[4][4];  // b: the odd-parity sums of an output fold
 #pragma unroll
   for (int q = 0; q < 4; ++q)
 #pragma unroll
-    for (int j = 0; j < 4; ++j) ar[q][j] = ai[q][j] = 0;
-  if (act) {
-#pragma unroll 4
-    for (int n = 0; n < NN; ++n) {
-      cx x[4], xd[4];
+    for (int j = 0; j < 4; ++j) ar[q][j] = ai[q][j] = br[q][j] = bi[q][j] = 0;
+  auto fma44 = [](real (&r)[4][4], real (&im)[4][4], const real (&m)[4], const cx (&x)[4]) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
-        x[j] = buf[idx(n, l0 + j)];
-        xd[j] = FOLD ? buf[idx(ND - 1 - n, l0 + j)] : x[j];
+        r[q][j] += m[q] * x[j].re;
+        im[q][j] += m[q] * x[j].im;
       }
-      real m[4];
-      xs3_load4(Ms + n * ND + k0, m);
-#pragma unroll
-      for (int q = 0; q < 4; ++q)
+  };
+  if (act) {
+    if constexpr (FOLD == 2) {
+      // E (n + PAR even) into ar/ai, O into br/bi; n runs in pairs (even n first)
+#pragma unroll 2
+      for (int n = 0; n < ND; n += 2) {
+        cx x0[4], x1[4];
+        lines4(n, l0, x0);
+        lines4(n + 1, l0, x1);
+        real m0[4], m1[4];
+        xs3_load4(Ms + n * H + k0, m0);
+        xs3_load4(Ms + (n + 1) * H + k0, m1);
+        if constexpr (PAR == 0) {
+          fma44(ar, ai, m0, x0);
+          fma44(br, bi, m1, x1);
+        } else {
+          fma44(br, bi, m0, x0);
+          fma44(ar, ai, m1, x1);
+        }
+      }
+    } else if constexpr (!FORM_R && (FOLD == 0 || C == ND - 1)) {
+      // rows are lines: two consecutive elements (and their mirror pair) per 16-byte load
+#pragma unroll 2
+      for (int n = 0; n < (FOLD ? H : ND); n += 2) {
+        cx x0[4], x1[4], d0[4], d1[4];
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-          const cx v = (FOLD && ((q + PAR) & 1)) ? xd[j] : x[j];  // k0 is a multiple of 4
-          ar[q][j] += m[q] * v.re;
-          ai[q][j] += m[q] * v.im;
+          xs3_load2(buf + (l0 + j) * LS + n, x0[j], x1[j]);
+          if constexpr (FOLD) xs3_load2(buf + (l0 + j) * LS + ND - 2 - n, d1[j], d0[j]);
         }
+        real m0[4], m1[4];
+        xs3_load4(Ms + n * ND + k0, m0);
+        xs3_load4(Ms + (n + 1) * ND + k0, m1);
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            const bool odd = FOLD && ((q + PAR) & 1);  // k0 is a multiple of 4
+            const cx v0 = odd ? d0[j] : x0[j], v1 = odd ? d1[j] : x1[j];
+            ar[q][j] += m0[q] * v0.re + m1[q] * v1.re;
+            ai[q][j] += m0[q] * v0.im + m1[q] * v1.im;
+          }
+      }
+    } else {
+#pragma unroll 4
+      for (int n = 0; n < (FOLD ? H : ND); ++n) {
+        cx x[4], xd[4];
+        if constexpr (FOLD) {
+          lines4(xs3_fr<ND, C>(n), l0, x);
+          lines4(xs3_fp<ND, C>(n), l0, xd);
+        } else {
+          lines4(n, l0, x);
+        }
+        real m[4];
+        xs3_load4(Ms + n * ND + k0, m);
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            const cx v = (FOLD && ((q + PAR) & 1)) ? xd[j] : x[j];  // k0 is a multiple of 4
+            ar[q][j] += m[q] * v.re;
+            ai[q][j] += m[q] * v.im;
+          }
+      }
     }
   }
   __syncthreads();
   if (act) {
+    if constexpr (FOLD == 2) {
 #pragma unroll
-    for (int q = 0; q < 4; ++q)
+      for (int q = 0; q < 4; ++q) {
+        const int k = xs3_fr<ND, C>(k0 + q), kp = C - k;
 #pragma unroll
-      for (int j = 0; j < 4; ++j) buf[idx(k0 + q, l0 + j)] = mkcx(ar[q][j], ai[q][j]);
+        for (int j = 0; j < 4; ++j) {
+          buf[idx(k, l0 + j)] = mkcx(ar[q][j] + br[q][j], ai[q][j] + bi[q][j]);
+          if (kp != k) buf[idx(kp, l0 + j)] = mkcx(ar[q][j] - br[q][j], ai[q][j] - bi[q][j]);
+        }
+      }
+      if (C != ND - 1 && k0 == 0)  // the zero output (row or column N-1, or 0)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) buf[idx(C == ND ? 0 : ND - 1, l0 + j)] = mkcx((real)0, (real)0);
+    } else {
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) buf[idx(k0 + q, l0 + j)] = mkcx(ar[q][j], ai[q][j]);
+    }
   }
   __syncthreads();
 }
 
+// ---- asynchronous staging ----------------------------------------------------------
+// The persistent passes copy the next plane (or z-line tile) into a second shared-memory
+// buffer with cp.async while the current one is transformed; copies of 16 bytes (two FP32 or
+// one FP64 complex element), one commit group per fetch, waited for at the top of the next
+// iteration.
+__device__ __forceinline__ void xs3_cp16(cx* dst, const cx* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((u32)__cvta_generic_to_shared(dst)), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void xs3_cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void xs3_cp_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+// ROWS rows of W complex elements, source row stride GS, into shared rows of stride LS.
+template <int ROWS, int W, size_t GS, int LS>
+__device__ __forceinline__ void xs3_fetch(cx* dst, const cx* __restrict__ src, int tid) {
+  constexpr int E = 16 / (int)sizeof(cx);  // elements per copy
+  static_assert(W % E == 0, "rows of whole 16-byte copies");
+  for (int i = tid; i < ROWS * (W / E); i += 256) {
+    const int r = i / (W / E), c = (i % (W / E)) * E;
+    xs3_cp16(dst + r * LS + c, src + (size_t)r * GS + c);
+  }
+  xs3_cp_commit();
+}
+
 // ---- plane passes ---------------------------------------------------------------
-// Shared memory: the matrices of the pass (xs3_psmem<MODE>() reals), then one
-// plane P[y][x] (row stride XS3_LSX).
+// Shared memory: the matrices of the pass (xs3_psmem<MODE>() reals), then two
+// planes P[y][x] (row stride XS3_LSX): the current one and the next, in flight.
 __device__ __forceinline__ void xs3_coords(int i1, int i2, int i3, real& x, real& y, real& z) {
   x = (real)(XS_O1 + XS_DX1 * (double)i1);
   y = (real)(XS_O2 + XS_DX2 * (double)i2);
@@ -261,14 +399,18 @@ __device__ __forceinline__ void xs3_initial_pass(const XsStreamArgs& A) {
 
 template <int MODE>
 __device__ __forceinline__ void xs3_plane_pass(const XsStreamArgs& A) {
-  constexpr size_t need = (size_t)xs3_psmem<MODE>() * sizeof(real) + (size_t)XS3_N2 * XS3_LSX * sizeof(cx);
+  constexpr size_t need = (size_t)xs3_psmem<MODE>() * sizeof(real) + 2 * (size_t)XS3_N2 * XS3_LSX * sizeof(cx);
   if (!xs_smem_ok(need, A.status)) return;
   real* sm = (real*)xs_dsmem;
   real* Mxi = sm;
   real* Myi = Mxi + (xs3_pinv<MODE>() ? xs3_msize<1>() : 0);
   real* Mxf = sm + xs3_pinv<MODE>();
   real* Myf = Mxf + ((MODE == 1 || MODE == 2) ? xs3_msize<0>() : 0);
-  cx* P = (cx*)(sm + xs3_psmem<MODE>());
+  cx* P = (cx*)(sm + xs3_psmem<MODE>());  // the plane being transformed
+  cx* Q = P + XS3_N2 * XS3_LSX;            // the next plane, in flight
+  const int tid = threadIdx.x;
+  const size_t nplanes = (size_t)A.ntraj * XS3_N3;
+  if (blockIdx.x < nplanes) xs3_fetch<XS3_N2, XS3_N1, XS3_N1, XS3_LSX>(P, A.field + blockIdx.x * XS3_NP, tid);
   if constexpr (MODE == 1 || MODE == 3) {
     xs3_stage_matrix<1>(Mxi, A.mat);
     xs3_stage_matrix<3>(Myi, A.mat);
@@ -277,14 +419,14 @@ __device__ __forceinline__ void xs3_plane_pass(const XsStreamArgs& A) {
     xs3_stage_matrix<0>(Mxf, A.mat);
     xs3_stage_matrix<2>(Myf, A.mat);
   }
-  const int tid = threadIdx.x;
-  const size_t nplanes = (size_t)A.ntraj * XS3_N3;
   bool bad = false;
   for (size_t pl = blockIdx.x; pl < nplanes; pl += gridDim.x) {
     const int e = (int)(pl / XS3_N3), z = (int)(pl % XS3_N3);
     cx* g = A.field + pl * XS3_NP;  // F = 1: plane pl of the [e][z] planes
-    for (int i = tid; i < XS3_NP; i += 256) P[(i / XS3_N1) * XS3_LSX + i % XS3_N1] = g[i];
-    __syncthreads();  // the matrices (first plane) and the plane are staged
+    xs3_cp_wait_all();
+    __syncthreads();  // this plane (and, the first time, the matrices) staged; Q free
+    if (pl + gridDim.x < nplanes)
+      xs3_fetch<XS3_N2, XS3_N1, XS3_N1, XS3_LSX>(Q, A.field + (pl + gridDim.x) * XS3_NP, tid);
     if (MODE == 1 || (MODE == 3 && !A.xspace)) {
       xs3_dense<3, XS3_N1, XS3_LSX, true>(P, Myi, tid);   // T_y^-1: lines are the x columns
       xs3_dense<1, XS3_N2, XS3_LSX, false>(P, Mxi, tid);  // T_x^-1: lines are the y rows
@@ -304,7 +446,9 @@ __device__ __forceinline__ void xs3_plane_pass(const XsStreamArgs& A) {
       xs3_dense<2, XS3_N1, XS3_LSX, true>(P, Myf, tid);   // T_y
       for (int i = tid; i < XS3_NP; i += 256) g[i] = P[(i / XS3_N1) * XS3_LSX + i % XS3_N1];
     }
-    __syncthreads();  // the plane buffer is reused by the next plane
+    cx* const t = P;  // the next iteration's barrier orders these reads before Q's refill
+    P = Q;
+    Q = t;
   }
   if (bad) atomicOr(A.status, 1);
 }
@@ -318,30 +462,31 @@ extern "C" __global__ void __launch_bounds__(256) xs_p_final(const XsStreamArgs 
 // Tile = XS3_QT consecutive (kx, ky) columns of one trajectory by N3 z points:
 // T[z][q] (row stride XS3_LSQ), each row one 8*QT-byte (FP32) run of a plane.
 // T_z, multiply by exp(L dtr/2)^m at (kx, ky, kz) (site order of the FP64
-// table), T_z^-1.  Shared memory: the two z matrices, then the tile.
+// table), T_z^-1.  Shared memory: the two z matrices, then two tiles (the current
+// one and the next, in flight).
 __host__ __device__ constexpr int xs3_zsmem() { return xs3_msize<4>() + xs3_msize<5>(); }
 
 extern "C" __global__ void __launch_bounds__(256) xs_z_pass(const XsStreamArgs A) {
-  constexpr size_t need = (size_t)xs3_zsmem() * sizeof(real) + (size_t)XS3_N3 * XS3_LSQ * sizeof(cx);
+  constexpr size_t need = (size_t)xs3_zsmem() * sizeof(real) + 2 * (size_t)XS3_N3 * XS3_LSQ * sizeof(cx);
   if (!xs_smem_ok(need, A.status)) return;
   real* Mzf = (real*)xs_dsmem;
   real* Mzi = Mzf + xs3_msize<4>();
-  cx* T = (cx*)(Mzf + xs3_zsmem());
-  xs3_stage_matrix<4>(Mzf, A.mat);
-  xs3_stage_matrix<5>(Mzi, A.mat);
+  cx* T = (cx*)(Mzf + xs3_zsmem());  // the tile being transformed
+  cx* U = T + XS3_N3 * XS3_LSQ;      // the next tile, in flight
   const int tid = threadIdx.x;
   constexpr int TPT = XS3_NP / XS3_QT;  // tiles per trajectory
   const size_t ntiles = (size_t)A.ntraj * TPT;
+  auto origin = [&](size_t tile) { return A.field + (tile / TPT) * XS_NS + (tile % TPT) * XS3_QT; };
+  if (blockIdx.x < ntiles) xs3_fetch<XS3_N3, XS3_QT, XS3_NP, XS3_LSQ>(T, origin(blockIdx.x), tid);
+  xs3_stage_matrix<4>(Mzf, A.mat);
+  xs3_stage_matrix<5>(Mzi, A.mat);
   const double2* __restrict__ tab = A.m == 2 ? A.prop2 : A.prop1;
   for (size_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    const size_t e = tile / TPT;
     const int q0 = (int)(tile % TPT) * XS3_QT;
-    cx* g = A.field + e * XS_NS + q0;
-    for (int i = tid; i < XS3_N3 * XS3_QT; i += 256) {
-      const int z = i / XS3_QT, q = i % XS3_QT;
-      T[z * XS3_LSQ + q] = g[(size_t)z * XS3_NP + q];
-    }
-    __syncthreads();
+    cx* g = origin(tile);
+    xs3_cp_wait_all();
+    __syncthreads();  // this tile (and, the first time, the matrices) staged; U free
+    if (tile + gridDim.x < ntiles) xs3_fetch<XS3_N3, XS3_QT, XS3_NP, XS3_LSQ>(U, origin(tile + gridDim.x), tid);
     xs3_dense<4, XS3_QT, XS3_LSQ, true>(T, Mzf, tid);  // T_z
 #if XS_HAS_PROP
     for (int i = tid; i < XS3_N3 * XS3_QT; i += 256) {
@@ -358,7 +503,9 @@ extern "C" __global__ void __launch_bounds__(256) xs_z_pass(const XsStreamArgs A
       const int z = i / XS3_QT, q = i % XS3_QT;
       g[(size_t)z * XS3_NP + q] = T[z * XS3_LSQ + q];
     }
-    __syncthreads();
+    cx* const t = T;  // the next iteration's barrier orders these reads before U's refill
+    T = U;
+    U = t;
   }
 }
 

@@ -576,6 +576,62 @@ int fold_parity(const std::vector<cd>& M, int n) {
   return 0;
 }
 
+// Mirror symmetry of a transform matrix about a centre c in n-1, n-2 or n (the 3D streaming
+// kernels): kind 1, input fold, M[c-i][k] = (-1)^(k+p) M[i][k] with every row whose partner lies
+// outside the matrix zero; kind 2, output fold, the same for columns; kind 0 none.
+struct FoldInfo {
+  int kind = 0, c = 0, p = 0;
+};
+
+FoldInfo fold_info(const std::vector<cd>& M, int n) {
+  double mx = 0;
+  for (const auto& v : M) mx = std::max(mx, std::abs(v));
+  auto at = [&](int i, int k, bool cols) { return cols ? M[(size_t)k * n + i] : M[(size_t)i * n + k]; };
+  for (int kind = 1; kind <= 2; ++kind)
+    for (int cc : {n - 1, n - 2, n})
+      for (int par = 0; par < 2; ++par) {
+        bool ok = true;
+        for (int i = 0; i < n && ok; ++i) {
+          const int m = cc - i;
+          for (int k = 0; k < n && ok; ++k) {
+            const cd x = at(i, k, kind == 2);
+            if (m < 0 || m >= n) {
+              if (std::abs(x) > 1e-12 * mx) ok = false;
+            } else if (std::abs(at(m, k, kind == 2) - x * ((k + par) % 2 ? -1.0 : 1.0)) > 1e-12 * mx) {
+              ok = false;
+            }
+          }
+        }
+        if (ok) return {kind, cc, par};
+      }
+  return {};
+}
+
+// The half of a folded matrix that the kernels read, M[n*N + k] convention: kind 1, rows
+// r(j) = j + (c == n) for j < n/2 ([n/2][n]); kind 2, columns r(j) ([n][n/2]).  Entries the
+// symmetry makes zero (a row or column that is its own partner, odd parity) are set to 0.
+std::vector<double> pack_folded(const std::vector<cd>& M, int n, const FoldInfo& f) {
+  if (f.kind == 0) {
+    std::vector<double> out(M.size());
+    for (size_t i = 0; i < M.size(); ++i) out[i] = M[i].real();
+    return out;
+  }
+  const int h = n / 2;
+  std::vector<double> out((size_t)n * h);
+  for (int j = 0; j < h; ++j) {
+    const int r = j + (f.c == n ? 1 : 0);
+    const bool self = f.c - r == r;
+    for (int i = 0; i < n; ++i) {
+      // kind 1: row r, column i (parity of the output i); kind 2: row i, column r (parity of the input i)
+      double v = f.kind == 1 ? M[(size_t)r * n + i].real() : M[(size_t)i * n + r].real();
+      if (self && (i + f.p) % 2) v = 0;
+      if (f.kind == 1) out[(size_t)j * n + i] = v;
+      else out[(size_t)i * h + j] = v;
+    }
+  }
+  return out;
+}
+
 // ---------------------------------------------------------------------------
 // Code generation
 // ---------------------------------------------------------------------------
@@ -945,8 +1001,9 @@ struct StreamPlan {
   // 3D: z-line tile width, per matrix (x, y, z; forward, inverse) its fold (0 or 1 + parity) and
   // offset in the matrix table, shared memory of the plane passes (to K state, step, final), the
   // z-line pass and the observation pass
-  int QT = 0;
-  int fold3[6] = {0, 0, 0, 0, 0, 0}, moff3[6] = {0, 0, 0, 0, 0, 0};
+  int QT = 0, LSX = 0, LSQ = 0;
+  int fold3[6] = {0, 0, 0, 0, 0, 0}, cen3[6] = {0, 0, 0, 0, 0, 0}, par3[6] = {0, 0, 0, 0, 0, 0};
+  int moff3[6] = {0, 0, 0, 0, 0, 0};
   size_t psmem3[3] = {0, 0, 0}, zsmem3 = 0, osmem3 = 0;
 };
 
@@ -1335,11 +1392,14 @@ void plan_stream(xs_handle& h) {
 
 // 3D streaming plan: matrix i = 2 d + inverse (d = x, y, z) at offset moff3[i] of the table, folded
 // when it is mirror-symmetric; shared memory of each pass as xs_stream3.cuh lays it out (matrices
-// in `real`, then the plane [N2][N1 + 1] or the z-line tile [N3][QT + 1] in complex `real`).
+// in `real`, then the plane [N2][LSX] or the z-line tile [N3][LSQ] in complex `real`; the row
+// strides are padded by 2 in FP32, keeping rows 16-byte aligned, and by 1 in FP64).
 void plan_stream3(xs_handle& h) {
   const Problem& P = h.P;
   StreamPlan sp;
   sp.QT = 64;
+  sp.LSX = P.N[0] + (h.fp64 ? 1 : 2);
+  sp.LSQ = sp.QT + (h.fp64 ? 1 : 2);
   const size_t rs = h.fp64 ? 8 : 4, cxs = 2 * rs;
   int off = 0;
   size_t msize[6];
@@ -1347,16 +1407,22 @@ void plan_stream3(xs_handle& h) {
     const int d = i / 2, n = P.N[d];
     sp.moff3[i] = off;
     off += n * n;
-    sp.fold3[i] = fold_parity(transform_matrix(P.type(d, 0), i % 2 == 1, n), n);
-    msize[i] = (size_t)(sp.fold3[i] ? n / 2 : n) * n;
+    const FoldInfo f = fold_info(transform_matrix(P.type(d, 0), i % 2 == 1, n), n);
+    sp.fold3[i] = f.kind;
+    sp.cen3[i] = f.c;
+    sp.par3[i] = f.p;
+    msize[i] = (size_t)(f.kind ? n / 2 : n) * n;
   }
-  const size_t plane = (size_t)P.N[1] * (P.N[0] + 1) * cxs;
-  sp.psmem3[0] = (msize[0] + msize[2]) * rs + plane;
-  sp.psmem3[1] = (msize[0] + msize[1] + msize[2] + msize[3]) * rs + plane;
-  sp.psmem3[2] = (msize[1] + msize[3]) * rs + plane;
-  sp.osmem3 = sp.psmem3[2];
-  sp.zsmem3 = (msize[4] + msize[5]) * rs + (size_t)P.N[2] * (sp.QT + 1) * cxs;
+  const size_t plane = (size_t)P.N[1] * sp.LSX * cxs;
+  // plane and z-line passes: two buffers (the current plane or tile and the next, in flight)
+  sp.psmem3[0] = (msize[0] + msize[2]) * rs + 2 * plane;
+  sp.psmem3[1] = (msize[0] + msize[1] + msize[2] + msize[3]) * rs + 2 * plane;
+  sp.psmem3[2] = (msize[1] + msize[3]) * rs + 2 * plane;
+  sp.osmem3 = (msize[1] + msize[3]) * rs + plane;
+  sp.zsmem3 = (msize[4] + msize[5]) * rs + 2 * (size_t)P.N[2] * sp.LSQ * cxs;
   if ((P.N[0] * P.N[1]) % sp.QT) raise(XS_ERR_SHAPE, "internal: z-line tiles do not divide the plane");
+  for (size_t b : {sp.psmem3[0], sp.psmem3[1], sp.psmem3[2], sp.zsmem3, sp.osmem3})
+    if (b > 227 * 1024) raise(XS_ERR_UNSUPPORTED, "3D streaming passes need more than 227 KB of shared memory");
   h.sp = sp;
 }
 
@@ -1402,9 +1468,10 @@ void build_source(xs_handle& h) {
       plan_stream3(h);
       std::ostringstream os;
       emit_common_header(h, os);
-      os << "#define XS3_QT " << h.sp.QT << "\n";
+      os << "#define XS3_QT " << h.sp.QT << "\n#define XS3_LSX " << h.sp.LSX << "\n#define XS3_LSQ " << h.sp.LSQ << "\n";
       for (int i = 0; i < 6; ++i)
-        os << "#define XS3_MOFF" << i << " " << h.sp.moff3[i] << "\n#define XS3_FOLD" << i << " " << h.sp.fold3[i] << "\n";
+        os << "#define XS3_MOFF" << i << " " << h.sp.moff3[i] << "\n#define XS3_FOLD" << i << " " << h.sp.fold3[i]
+           << "\n#define XS3_CEN" << i << " " << h.sp.cen3[i] << "\n#define XS3_PAR" << i << " " << h.sp.par3[i] << "\n";
       os << fns.str();
       os << xs_kernel_source_stream_common << "\n" << xs_kernel_source_stream3 << "\n";
       h.source = os.str();
@@ -1524,12 +1591,19 @@ void load_module(xs_handle& h) {
       h.grid_z = sms * occ_z;
     }
     CUDA_CHECK(cudaStreamCreateWithFlags(&h.stream, cudaStreamNonBlocking));
-    {  // the reference's transforms as real matrices M[n*N + k], FP64-built (xs_stream3.cuh)
+    {  // the reference's transforms as real matrices M[n*N + k], FP64-built, folded halves packed
       const Problem& P = h.P;
       std::vector<double> all;
       for (int i = 0; i < 6; ++i) {
         const int dd = i / 2, n = P.N[dd];
-        for (const cd& v : transform_matrix(P.type(dd, 0), i % 2 == 1, n)) all.push_back(v.real());
+        const auto M = transform_matrix(P.type(dd, 0), i % 2 == 1, n);
+        FoldInfo f;
+        f.kind = sp.fold3[i];
+        f.c = sp.cen3[i];
+        f.p = sp.par3[i];
+        std::vector<double> pk = pack_folded(M, n, f);
+        pk.resize((size_t)n * n, 0.0);  // each matrix keeps an N x N slot
+        all.insert(all.end(), pk.begin(), pk.end());
       }
       if (h.fp64) {
         h.d_mat3.ensure(all.size() * 8);
