@@ -882,6 +882,117 @@ def run_ac3d(args):
     print(json.dumps(line))
 
 
+def run_snls(args):
+    """1D stochastic NLS (64 points on [-5, 5], RK4, 51 x 4 = 200 steps to t = 1,
+    1024 trajectories in 8 blocks, <|a|^2> and <Re a>): one p.path over all
+    blocks per step, resident kernel (field and noise in shared memory).  FP64
+    (the reference's c128) is the line's value, FP32 a sub-line; e2e through
+    xs_run_path with a pinned host initial field; the CPU baseline is the FP64
+    oracle's p.path over one block of 128 trajectories."""
+    import numpy as np
+    import torch
+    from xspde_matlab_b200 import GpuPath, _lib, xpreferences
+    from xspde_matlab_b200.problems import SNLS_1D
+    L = _lib.lib()
+    steps = SNLS_1D["points"][0] * SNLS_1D["steps"] - 1
+    out = {}
+    for prec in ("fp64", "fp32"):
+        p = xpreferences([dict(SNLS_1D, precision=prec)])[0]
+        g = GpuPath(p)
+        nb = p.ensembles[1]
+        ntraj = nb * p.ensembles[0]
+        av = torch.zeros((nb * g.per_block,), dtype=torch.float64, device="cuda")
+        st = torch.cuda.current_stream()
+
+        def run():
+            _lib.check(L.xs_run_path_device(g.h, 0, nb, 1, None, ctypes.c_void_p(av.data_ptr()), None,
+                                            ctypes.c_void_p(st.cuda_stream)))
+        for _ in range(max(3, args.warmup)):
+            run()
+        torch.cuda.synchronize()
+        _lib.check(L.xs_sync(g.h))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        nrep = max(args.steps, 20)  # one path takes about a millisecond
+        with Clocks(torch.cuda.current_device()) as clk:
+            e0.record(st)
+            for _ in range(nrep):
+                run()
+            e1.record(st)
+            e1.synchronize()
+        ms = e0.elapsed_time(e1) / nrep
+        _lib.check(L.xs_sync(g.h))
+        nk = len(_lib.KERNEL_KINDS)
+        kms = (ctypes.c_double * nk)()
+        kl = (ctypes.c_longlong * nk)()
+        L.xs_set_kernel_timing(g.h, 1)
+        L.xs_kernel_stats(g.h, 1, None, None)
+        run()
+        torch.cuda.synchronize()
+        _lib.check(L.xs_kernel_stats(g.h, 1, kms, kl))
+        L.xs_set_kernel_timing(g.h, 0)
+        stats = {_lib.KERNEL_KINDS[i]: {"launches": int(kl[i]), "ms": float(kms[i])} for i in range(nk) if kl[i]}
+        # end to end: pinned FP64 host initial field in, block means out, inside the timed region
+        x = np.linspace(-5.0, 5.0, 64)
+        a_in = torch.empty((ntraj * 64 * 2,), dtype=torch.float64, pin_memory=True)
+        a_in.view(ntraj, 64, 2)[:, :, 0] = torch.from_numpy(np.exp(-x ** 2))[None, :]
+        a_in.view(ntraj, 64, 2)[:, :, 1] = 0.0
+        av_host = torch.empty((nb * g.per_block,), dtype=torch.float64, pin_memory=True)
+        for _ in range(2):
+            _lib.check(L.xs_run_path(g.h, 0, nb, 1, ctypes.c_void_p(a_in.data_ptr()),
+                                     ctypes.c_void_p(av_host.data_ptr()), None))
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record(st)
+        for _ in range(nrep):
+            _lib.check(L.xs_run_path(g.h, 0, nb, 1, ctypes.c_void_p(a_in.data_ptr()),
+                                     ctypes.c_void_p(av_host.data_ptr()), None))
+        t1.record(st)
+        t1.synchronize()
+        ems = t0.elapsed_time(t1) / nrep
+        cx = 16 if prec == "fp64" else 8
+        alg = ntraj * 64 * 16 + nb * g.per_block * 8  # field in (FP64), block means out
+        out[prec] = {"value": ntraj * steps / (ms * 1e-3), "ms_per_step": ms, "steps": nrep,
+                     "kernels": stats, "clocks": clk.summary(),
+                     "e2e": {"value": ntraj * steps / (ems * 1e-3), "unit": "traj-steps/s",
+                             "h2d_bytes_per_step": int(a_in.numel() * 8), "d2h_bytes_per_step": int(av_host.numel() * 8)},
+                     "roofline": {"bound": "hbm", "kernel": "resident", "unit": "GB/s",
+                                  "achieved": alg / (stats["resident"]["ms"] / stats["resident"]["launches"] * 1e-3) / 1e9,
+                                  "peak": _peaks()[0], "peak_kind": _peaks()[1],
+                                  "note": "the field (%d B per site) and noise stay in shared memory for the whole "
+                                          "path: HBM carries only the initial field and the block means, so this "
+                                          "kernel is bound by FP%d arithmetic and latency, not by HBM" % (cx, 64 if cx == 16 else 32)}}
+        out[prec]["roofline"]["frac"] = out[prec]["roofline"]["achieved"] / out[prec]["roofline"]["peak"]
+    # CPU baseline: the oracle's p.path over one block (128 trajectories, FP64 NumPy, one core)
+    from oracle import xspde_ref as X
+    os.environ.setdefault("OMP_NUM_THREADS", "1")
+    o = dict(SNLS_1D)
+    o.update(deriv=lambda a, w, q: 1j * a * np.conj(a) * a + 0.01 * (w[0:1] + 1j * w[1:2]) / np.sqrt(2),
+             initial=lambda v, q: np.exp(-q.x ** 2), linear=lambda q: 1j * q.Dx ** 2,
+             observe=[lambda a, q: a * np.conj(a), lambda a, q: np.real(a)])
+    q = X.xpreferences([o])[0].copy()
+    q.block, q.seq = 0, 0
+    q.dtr = q.dt / q.steps[0]
+    q.propagator, q.da = q.propfactor(q)
+    q.t = q.origins[0]
+    a = X.fit(np.asarray(X.call_cells(q.initial, None, q.randomgen(q), q), dtype=complex), q.ca)
+    t0 = time.perf_counter()
+    q.path(a, 1, q)
+    secs = time.perf_counter() - t0
+    m = out["fp64"]
+    line = {"metric": "traj-steps/s, 1D stochastic NLS (64 points, RK4)", "value": m["value"], "unit": "traj-steps/s",
+            "n_gpus": 1, "steps": m["steps"], "warmup": max(3, args.warmup), "ms_per_step": m["ms_per_step"],
+            "higher_is_better": True, "dtype": "c128", "data": "synthetic (Philox noise, seed 0)",
+            "path": "resident: one CTA per trajectory tile, field and noise in shared memory for all 200 RK4 steps",
+            "e2e": m["e2e"], "kernels": m["kernels"], "roofline": m["roofline"], "clocks": m["clocks"],
+            "fp32": out["fp32"],
+            "cpu_baseline": {"value": 128 * steps / secs, "unit": "traj-steps/s", "cores": 1, "kind": "port",
+                             "sample": "one block: 128 trajectories x %d RK4 steps with <|a|^2> and <Re a> at 51 "
+                                       "output times (FP64 NumPy oracle, %.1f s)" % (steps, secs)},
+            "config": {"workload": "snls_1d: 64 points on [-5, 5], RK4, 51 output times x 4 steps = 200 steps to t = 1, "
+                                   "1024 trajectories (8 blocks of 128)"}}
+    print(json.dumps(line))
+
+
 def run_dpo(args):
     """Positive-P DPO (0-D, two complex fields): 8 blocks x 125000 trajectories,
     each block its own pump eps ~ U[0.5, 2], 2000 MP steps, as one batch (one
@@ -951,6 +1062,7 @@ def main():
     ap.add_argument("--dpo", action="store_true", help="positive-P DPO, 10^6 trajectories x 2000 steps")
     ap.add_argument("--mlp", action="store_true", help="control-variate network inference on M fresh inputs")
     ap.add_argument("--mlp-batch", type=int, default=1 << 20)
+    ap.add_argument("--snls", action="store_true", help="1D stochastic NLS, 64 points, 1024 trajectories, RK4")
     ap.add_argument("--ac3d", action="store_true", help="3D stochastic Allen-Cahn 64^3 with DST/DCT boundaries")
     ap.add_argument("--ac3d-traj", type=int, default=256, help="trajectories of --ac3d (multiple of 32)")
     ap.add_argument("--ac3d-path", type=int, default=0, help="--ac3d device path: 0 automatic (3D streaming), 1 resident")
@@ -965,6 +1077,11 @@ def main():
         import torch
         torch.cuda.set_device(local_rank)
         run_ac3d(args)
+        return
+    if args.snls:
+        import torch
+        torch.cuda.set_device(local_rank)
+        run_snls(args)
         return
     if args.dpo:
         import torch
