@@ -19,6 +19,12 @@ struct __align__(2 * sizeof(real)) cx {
 };
 
 __device__ __forceinline__ cx mkcx(real r, real i) { cx z; z.re = r; z.im = i; return z; }
+// a * b + c with one rounding
+#if XS_FP64
+__device__ __forceinline__ real xs_fma(real a, real b, real c) { return fma(a, b, c); }
+#else
+__device__ __forceinline__ real xs_fma(real a, real b, real c) { return fmaf(a, b, c); }
+#endif
 __device__ __forceinline__ cx operator+(cx a, cx b) { return mkcx(a.re + b.re, a.im + b.im); }
 __device__ __forceinline__ cx operator-(cx a, cx b) { return mkcx(a.re - b.re, a.im - b.im); }
 __device__ __forceinline__ cx operator-(cx a) { return mkcx(-a.re, -a.im); }

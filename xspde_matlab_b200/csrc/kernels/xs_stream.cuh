@@ -168,12 +168,26 @@ __device__ __forceinline__ void xs_xpass_core(const XsStreamArgs& A, int tid, si
       cx a0[XS_F], a[XS_F], d[XS_F];
 #pragma unroll
       for (int f = 0; f < XS_F; ++f) a0[f] = a[f] = stage[(f * XS_RX + j) * XS_RX + t];
+#if XS_DSPLIT
+      // a = (a0 + h inv) + h dep(a): the drift's field-independent terms once per site
+      cx c0[XS_F];
+      xs_deriv_inv(a, w, (const cx*)nullptr, x, yy, (real)0, tm, A.params, (const cx*)nullptr, 0, 0, d);
+#pragma unroll
+      for (int f = 0; f < XS_F; ++f) c0[f] = a0[f] + h * d[f];
+#pragma unroll
+      for (int it = 0; it < XS_ITER; ++it) {
+        xs_deriv_dep(a, w, (const cx*)nullptr, x, yy, (real)0, tm, A.params, (const cx*)nullptr, 0, 0, d);
+#pragma unroll
+        for (int f = 0; f < XS_F; ++f) a[f] = c0[f] + h * d[f];
+      }
+#else
 #pragma unroll
       for (int it = 0; it < XS_ITER; ++it) {
         xs_deriv(a, w, (const cx*)nullptr, x, yy, (real)0, tm, A.params, (const cx*)nullptr, 0, 0, d);
 #pragma unroll
         for (int f = 0; f < XS_F; ++f) a[f] = a0[f] + h * d[f];
       }
+#endif
 #pragma unroll
       for (int f = 0; f < XS_F; ++f) stage[(f * XS_RX + j) * XS_RX + t] = (real)2 * a[f] - a0[f];
     };
@@ -263,8 +277,12 @@ __device__ __forceinline__ void xs_xpass_body(const XsStreamArgs& A) {
   xs_xpass_core<MODE>(A, threadIdx.x, blockIdx.x, (cx*)xs_dsmem, XsBlockSync());
 }
 
+// Minimum resident CTAs per SM of the MP row pass (register budget: 64 in FP32, 128 in FP64).
+#ifndef XS_XPASS_MINB
+#define XS_XPASS_MINB (XS_FP64 ? 2 : 4)
+#endif
 extern "C" __global__ void __launch_bounds__(256) xs_x_init(const XsStreamArgs A) { xs_xpass_body<0>(A); }
-extern "C" __global__ void __launch_bounds__(256) xs_x_nl(const XsStreamArgs A) { xs_xpass_body<1>(A); }
+extern "C" __global__ void __launch_bounds__(256, XS_XPASS_MINB) xs_x_nl(const XsStreamArgs A) { xs_xpass_body<1>(A); }
 extern "C" __global__ void __launch_bounds__(256) xs_x_final(const XsStreamArgs A) { xs_xpass_body<3>(A); }
 
 // ---- RK4 row passes ------------------------------------------------------------
@@ -462,7 +480,13 @@ __device__ __forceinline__ void xs_col_core(const XsStreamArgs& A, int tid, size
   for (int j = 0; j < XS_RY; ++j) base[(size_t)(t + XS_RY * j) * XS_NX] = v[j];
 }
 
-extern "C" __global__ void __launch_bounds__(256, 4) xs_s_pass(const XsStreamArgs A) {
+// Minimum resident CTAs per SM (register budget) of the column pass.  FP32: 64 registers, four
+// CTAs per SM.  FP64 lines hold 16 complex doubles per thread and spill at 64 or 80 registers, so
+// FP64 builds take 128 (two CTAs per SM).  XSPDE_B200_DEFINES="-DXS_SPASS_MINB=n" overrides it.
+#ifndef XS_SPASS_MINB
+#define XS_SPASS_MINB (XS_FP64 ? 2 : 4)
+#endif
+extern "C" __global__ void __launch_bounds__(256, XS_SPASS_MINB) xs_s_pass(const XsStreamArgs A) {
   if ((size_t)blockIdx.x >= (size_t)A.ntraj * XS_F * (XS_NX / XS_TX)) {
     if (threadIdx.x == 0) atomicOr(A.status, 2);
     return;
@@ -478,7 +502,7 @@ extern "C" __global__ void __launch_bounds__(256, 4) xs_s_pass(const XsStreamArg
 // 256 threads.  As short column CTAs finish, the block scheduler refills their
 // slots, so every SM keeps a mix of issue-bound row CTAs and HBM-bound column
 // CTAs.
-extern "C" __global__ void __launch_bounds__(256, 4) xs_rc_pass(const XsStreamArgs R, const XsStreamArgs C) {
+extern "C" __global__ void __launch_bounds__(256, XS_SPASS_MINB) xs_rc_pass(const XsStreamArgs R, const XsStreamArgs C) {
   const size_t nr = (size_t)R.ntraj * XS_NY / XS_XROWS, ncol = (size_t)C.ntraj * XS_F * (XS_NX / XS_TX);
   const size_t m = nr < ncol ? nr : ncol;
   const size_t i = blockIdx.x;

@@ -306,10 +306,20 @@ __device__ __forceinline__ void xs3_mp_sites(const XsStreamArgs& A, cx* P, int e
     xs3_coords(i1, i2, z, x, y, zz);
     cx a0[1], a[1], d[1];
     a0[0] = a[0] = P[i2 * XS3_LSX + i1];
+#if XS_DSPLIT
+    // a = (a0 + h inv) + h dep(a): the drift's field-independent terms once per site
+    xs_deriv_inv(a, w, (const cx*)nullptr, x, y, zz, tm, A.params, (const cx*)nullptr, 0, 0, d);
+    const cx c0 = a0[0] + h * d[0];
+#endif
 #pragma unroll
     for (int it = 0; it < XS_ITER; ++it) {
+#if XS_DSPLIT
+      xs_deriv_dep(a, w, (const cx*)nullptr, x, y, zz, tm, A.params, (const cx*)nullptr, 0, 0, d);
+      a[0] = c0 + h * d[0];
+#else
       xs_deriv(a, w, (const cx*)nullptr, x, y, zz, tm, A.params, (const cx*)nullptr, 0, 0, d);
       a[0] = a0[0] + h * d[0];
+#endif
 #if XS_SETBOUND
       if (xs_dirichlet(0, i1, i2, z)) a[0] = mkcx((real)0, (real)0);
 #endif

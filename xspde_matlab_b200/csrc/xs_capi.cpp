@@ -188,6 +188,14 @@ std::string nvrtc_compile(const std::string& src, const std::string& name, std::
                                    "-lineinfo", "--extra-device-vectorization", "-DXS_NVRTC=1"};
   if (const char* v = getenv("XSPDE_B200_PTXAS_VERBOSE"))
     if (*v && *v != '0') opts.push_back("--ptxas-options=-v");
+  // XSPDE_B200_DEFINES="-DNAME=value ...": extra preprocessor definitions for the generated
+  // kernels (tuning knobs such as XS_SPASS_MINB, the column pass's minimum CTAs per SM)
+  if (const char* dv = getenv("XSPDE_B200_DEFINES")) {
+    std::stringstream ds(dv);
+    std::string d;
+    while (ds >> d)
+      if (d.rfind("-D", 0) == 0) opts.push_back(d);
+  }
   int maj = 0, min = 0;
   nvrtcVersion(&maj, &min);
   std::string key = src;
@@ -684,13 +692,29 @@ void generate_functions(Problem& P, std::ostringstream& os) {
     os << "__device__ __forceinline__ cx xs_fd2(const cx* __restrict__ fld, int g, int s, int f, int d);\n";
     os << "__device__ __forceinline__ void xs_deriv(const cx* __restrict__ a, const real* __restrict__ w, const cx* __restrict__ zk, real x, real y, real z, real t, const double* __restrict__ prm, const cx* __restrict__ fld, int g, int s, cx* __restrict__ out) {\n";
     os << "  (void)a; (void)w; (void)zk; (void)x; (void)y; (void)z; (void)t; (void)prm; (void)fld; (void)g; (void)s;\n";
-    if (g.len == 1 && P.F > 1) {
-      os << "  cx o1[1];\n  { cx* out = o1;\n" << g.code << "  }\n";
-      os << "  for (int f = 0; f < " << P.F << "; ++f) out[f] = o1[0];\n";
-    } else {
-      os << g.code;
-    }
+    auto body = [&](const xs::Generated& gg) {
+      if (gg.len == 1 && P.F > 1) {
+        os << "  cx o1[1];\n  { cx* out = o1;\n" << gg.code << "  }\n";
+        os << "  for (int f = 0; f < " << P.F << "; ++f) out[f] = o1[0];\n";
+      } else {
+        os << gg.code;
+      }
+    };
+    body(g);
     os << "}\n";
+    // the drift's field-independent terms (noise, sources) apart, for MP's midpoint iterations
+    xs::Generated gd, gi;
+    const bool split = xs::generate_split(fn, make_ctx(P, roles, false), gd, gi) && gd.len == g.len && gi.len == g.len;
+    os << "#define XS_DSPLIT " << (split ? 1 : 0) << "\n";
+    if (split) {
+      const char* sig = "(const cx* __restrict__ a, const real* __restrict__ w, const cx* __restrict__ zk, real x, real y, real z, real t, const double* __restrict__ prm, const cx* __restrict__ fld, int g, int s, cx* __restrict__ out) {\n";
+      const char* unused = "  (void)a; (void)w; (void)zk; (void)x; (void)y; (void)z; (void)t; (void)prm; (void)fld; (void)g; (void)s;\n";
+      os << "__device__ __forceinline__ void xs_deriv_dep" << sig << unused;
+      body(gd);
+      os << "}\n__device__ __forceinline__ void xs_deriv_inv" << sig << unused;
+      body(gi);
+      os << "}\n";
+    }
   }
   // define(a, w, p): the auxiliary cell (xpath.m:36-45, xensemble.m:74-77), noise cells as for deriv
   {
@@ -1326,7 +1350,12 @@ std::string stream3_blocker(const Problem& P) {
 }
 
 // Straight-line radix-2 DIT DFT of R points (forward, exp(-2 pi i n k / R)),
-// emitted with literal twiddles; trivial twiddles (1, -i) cost no multiply.
+// emitted with literal twiddles; trivial twiddles (1, -i) cost no multiply.  A
+// butterfly u +- W v with a general twiddle W = c + i s is evaluated as
+// u +- c (v (1 + i s/c)) (or u +- s (v (c/s + i)) when |s| > |c|, keeping the
+// ratio within [-1, 1]): two fused multiply-adds for the scaled v and four for
+// the two outputs, instead of a complex multiply (four operations) and four
+// additions.
 std::string gen_dft(int R) {
   std::ostringstream os;
   int bits = 0;
@@ -1347,17 +1376,34 @@ std::string gen_dft(int R) {
       for (int k = 0; k < len / 2; ++k) {
         int u = i + k, w = i + k + len / 2;
         std::string tw = "q" + std::to_string(tmp++);
-        if (k == 0) {
-          os << "  const cx " << tw << " = " << cur[w] << ";\n";
-        } else if (4 * k == len) {
-          os << "  const cx " << tw << " = mkcx(" << cur[w] << ".im, -" << cur[w] << ".re);\n";
-        } else {
-          double c = std::cos(2 * M_PI * k / len), s = -std::sin(2 * M_PI * k / len);
-          os << "  const cx " << tw << " = " << cur[w] << " * mkcx((real)" << fmt(c) << ", (real)" << fmt(s) << ");\n";
-        }
         std::string a = "q" + std::to_string(tmp++), b = "q" + std::to_string(tmp++);
-        os << "  const cx " << a << " = " << cur[u] << " + " << tw << ";\n";
-        os << "  const cx " << b << " = " << cur[u] << " - " << tw << ";\n";
+        const std::string& U = cur[u];
+        const std::string& V = cur[w];
+        if (k == 0 || 4 * k == len) {
+          if (k == 0) os << "  const cx " << tw << " = " << V << ";\n";
+          else os << "  const cx " << tw << " = mkcx(" << V << ".im, -" << V << ".re);\n";
+          os << "  const cx " << a << " = " << U << " + " << tw << ";\n";
+          os << "  const cx " << b << " = " << U << " - " << tw << ";\n";
+        } else {
+          const double c = std::cos(2 * M_PI * k / len), s = -std::sin(2 * M_PI * k / len);
+          auto snap = [](double r) { return std::fabs(std::fabs(r) - 1.0) < 1e-14 ? (r > 0 ? 1.0 : -1.0) : r; };
+          double f;
+          if (std::fabs(c) >= std::fabs(s)) {  // W v = c (v (1 + i tau)), tau = s / c
+            const double tau = snap(s / c);
+            f = c;
+            os << "  const cx " << tw << " = mkcx(xs_fma((real)" << fmt(-tau) << ", " << V << ".im, " << V
+               << ".re), xs_fma((real)" << fmt(tau) << ", " << V << ".re, " << V << ".im));\n";
+          } else {  // W v = s (v (sigma + i)), sigma = c / s
+            const double sig = snap(c / s);
+            f = s;
+            os << "  const cx " << tw << " = mkcx(xs_fma((real)" << fmt(sig) << ", " << V << ".re, -" << V
+               << ".im), xs_fma((real)" << fmt(sig) << ", " << V << ".im, " << V << ".re));\n";
+          }
+          os << "  const cx " << a << " = mkcx(xs_fma((real)" << fmt(f) << ", " << tw << ".re, " << U
+             << ".re), xs_fma((real)" << fmt(f) << ", " << tw << ".im, " << U << ".im));\n";
+          os << "  const cx " << b << " = mkcx(xs_fma((real)" << fmt(-f) << ", " << tw << ".re, " << U
+             << ".re), xs_fma((real)" << fmt(-f) << ", " << tw << ".im, " << U << ".im));\n";
+        }
         nxt[u] = a;
         nxt[w] = b;
       }

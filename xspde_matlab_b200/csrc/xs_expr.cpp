@@ -1170,10 +1170,9 @@ struct Gen {
 
 }  // namespace
 
-Generated generate(const AnonFn& fn, const GenCtx& ctx) {
-  Gen g(ctx);
-  std::vector<Reduction> reds;
-  g.reds = &reds;
+namespace {
+
+void bind_params(Gen& g, const AnonFn& fn, const GenCtx& ctx) {
   for (size_t i = 0; i < fn.params.size() && i < ctx.roles.size(); ++i) {
     const std::string& nm = fn.params[i];
     if (nm == "~") continue;
@@ -1189,6 +1188,98 @@ Generated generate(const AnonFn& fn, const GenCtx& ctx) {
     }
   }
   if (fn.params.size() > ctx.roles.size()) throw GrammarError("too many arguments in '" + fn.text + "'");
+}
+
+bool reads_var(const NodeP& n, const std::string& name) {
+  if (!n) return false;
+  if (n->kind == NK::Var && n->name == name) return true;
+  for (auto& k : n->kids)
+    if (reads_var(k, name)) return true;
+  for (auto& r : n->rows)
+    for (auto& e : r)
+      if (reads_var(e, name)) return true;
+  return false;
+}
+
+// The terms of the outermost sum of n with their signs: a - (b + c) -> +a, -b, -c.
+void sum_terms(const NodeP& n, int sign, std::vector<std::pair<int, NodeP>>& out) {
+  if (n->kind == NK::Bin && (n->name == "+" || n->name == "-") && n->kids.size() == 2) {
+    sum_terms(n->kids[0], sign, out);
+    sum_terms(n->kids[1], n->name == "-" ? -sign : sign, out);
+  } else if (n->kind == NK::Un && (n->name == "-" || n->name == "+") && n->kids.size() == 1) {
+    sum_terms(n->kids[0], n->name == "-" ? -sign : sign, out);
+  } else {
+    out.push_back({sign, n});
+  }
+}
+
+}  // namespace
+
+bool generate_split(const AnonFn& fn, const GenCtx& ctx, Generated& dep, Generated& inv) {
+  Gen g(ctx);
+  bind_params(g, fn, ctx);
+  if (g.aname.empty()) return false;
+  std::vector<NodeP> rows;
+  if (fn.body->kind == NK::Concat) {
+    for (auto& row : fn.body->rows) {
+      if (row.size() != 1) return false;
+      rows.push_back(row[0]);
+    }
+  } else {
+    rows.push_back(fn.body);
+  }
+  bool any_dep = false, any_inv = false;
+  std::vector<std::string> dc, ic;  // per output component: complex expressions
+  for (auto& row : rows) {
+    std::vector<std::pair<int, NodeP>> terms;
+    sum_terms(row, 1, terms);
+    Val sd, si;
+    bool hd = false, hi = false;
+    for (auto& [sign, t] : terms) {
+      Val v = g.gen(t);
+      if (sign < 0) v = g.un("-", v);
+      const bool d = reads_var(t, g.aname);
+      Val& acc = d ? sd : si;
+      bool& has = d ? hd : hi;
+      acc = has ? g.bin("+", acc, v, nullptr) : v;
+      has = true;
+    }
+    any_dep = any_dep || hd;
+    any_inv = any_inv || hi;
+    const int len = std::max(hd ? sd.len : 1, hi ? si.len : 1);
+    if ((hd && sd.len != len && sd.len != 1) || (hi && si.len != len && si.len != 1)) return false;
+    auto comp = [&](const Val& v, bool has, int i) -> std::string {
+      if (!has) return "mkcx((real)0, (real)0)";
+      const std::string& c = v.c[v.len == 1 ? 0 : i];
+      return v.cplx ? c : "mkcx(" + c + ", (real)0)";
+    };
+    for (int i = 0; i < len; ++i) {
+      dc.push_back(comp(sd, hd, i));
+      ic.push_back(comp(si, hi, i));
+    }
+  }
+  if (!any_dep || !any_inv) return false;
+  const std::string body = g.os.str();
+  auto fill = [&](Generated& out, const std::vector<std::string>& c) {
+    out = Generated{};
+    out.len = (int)c.size();
+    out.is_complex = true;
+    std::ostringstream code;
+    code << body;
+    for (size_t i = 0; i < c.size(); ++i) code << "  out[" << i << "] = " << c[i] << ";\n";
+    out.code = code.str();
+    out.stencil = g.stencil;
+  };
+  fill(dep, dc);
+  fill(inv, ic);
+  return true;
+}
+
+Generated generate(const AnonFn& fn, const GenCtx& ctx) {
+  Gen g(ctx);
+  std::vector<Reduction> reds;
+  g.reds = &reds;
+  bind_params(g, fn, ctx);
   Val v = g.gen(fn.body);
   Generated out;
   out.len = v.len;

@@ -92,6 +92,13 @@ struct Generated {
 // For observe functions with Int/Ave, reduced values are read from `red`.
 Generated generate(const AnonFn& fn, const GenCtx& ctx);
 
+// Additive split of a drift D(a, ...) = dep(a, ...) + inv(...) along the terms of its outermost
+// sum (per component of a top-level [e1; e2; ...]): `inv` collects the terms that do not read the
+// field a, `dep` the rest, both with len components (complex).  The midpoint iterations of MP
+// evaluate D several times with the same noise: a = (a0 + h inv) + h dep(a) computes the
+// field-independent part once.  Returns false when either part would be empty (no gain).
+bool generate_split(const AnonFn& fn, const GenCtx& ctx, Generated& dep, Generated& inv);
+
 // Host FP64 evaluation of the linear operator on the propagation grid:
 // returns L per (component, site) with component count 1 or F.
 struct GridInfo {
