@@ -37,14 +37,22 @@ __device__ __forceinline__ cx xs_cj(cx a) { return mkcx(a.re, -a.im); }
 
 // W_N^(t*k) for the four-step split, N = R*R: tw[k*R + t] = exp(-2 pi i t k / N)
 // (t fastest, so the threads of a line read consecutive words), copied from
-// the host-built table (L2-resident) into the CTA's shared memory.
+// the host-built table (L2-resident) into the CTA's shared memory, followed by
+// the same table divided by N for the inverse transforms (N a power of two, so
+// the division is exact).  XS_TWN(R) elements in all.
+#define XS_TWN(R) (2 * (R) * (R))
 template <int R>
 __device__ __forceinline__ void xs_fill_twiddles(cx* tw, const cx* __restrict__ src, int tid = -1, int nthr = 0) {
   if (tid < 0) {
     tid = threadIdx.x;
     nthr = blockDim.x;
   }
-  for (int i = tid; i < R * R; i += nthr) tw[i] = src[i];
+  const real sc = (real)(1.0 / (double)(R * R));
+  for (int i = tid; i < R * R; i += nthr) {
+    const cx w = src[i];
+    tw[i] = w;
+    tw[R * R + i] = mkcx(w.re * sc, w.im * sc);
+  }
 }
 
 // Forward DFT of N = R*R points held four-step style: thread t holds v[j] =
@@ -67,14 +75,29 @@ __device__ __forceinline__ void xs_fft4(cx (&v)[R], int t, const cx* __restrict_
   xs_dftR<R>(v);
 }
 
+// Inverse DFT (exp(+2 pi i n k / N) / N) in the same layout: conj, forward, conj.  The 1/N
+// rides on the twiddle multiply (the second half of the table holds W/N; element k = 0, whose
+// twiddle is 1, is scaled on its own): N is a power of two, so the result is bit-identical to
+// scaling the output.
 template <int R, int LS, int PAD, class Sync>
 __device__ __forceinline__ void xs_ifft4(cx (&v)[R], int t, const cx* __restrict__ tw, cx* buf, Sync sync) {
 #pragma unroll
   for (int k = 0; k < R; ++k) v[k] = xs_cj(v[k]);
-  xs_fft4<R, LS, PAD>(v, t, tw, buf, sync);
+  xs_dftR<R>(v);
   const real sc = (real)(1.0 / (double)(R * R));
+  v[0] = mkcx(v[0].re * sc, v[0].im * sc);
+  const cx* tws = tw + R * R;
 #pragma unroll
-  for (int k = 0; k < R; ++k) v[k] = mkcx(v[k].re * sc, -v[k].im * sc);
+  for (int k = 1; k < R; ++k) v[k] = v[k] * tws[k * R + t];
+#pragma unroll
+  for (int k = 0; k < R; ++k) buf[(k * (R + PAD) + t) * LS] = v[k];
+  sync();
+#pragma unroll
+  for (int n = 0; n < R; ++n) v[n] = buf[(t * (R + PAD) + n) * LS];
+  sync();
+  xs_dftR<R>(v);
+#pragma unroll
+  for (int k = 0; k < R; ++k) v[k] = xs_cj(v[k]);
 }
 
 struct XsWarpSync {
@@ -88,7 +111,7 @@ struct XsBlockSync {
 // ---- row passes -------------------------------------------------------------
 // Shared memory: twiddles (RX*RX) + per-row transpose scratch (RX*(RX+1)).
 #define XS_XLINE (XS_F * XS_RX * XS_RX > XS_RX * (XS_RX + 1) ? XS_F * XS_RX * XS_RX : XS_RX * (XS_RX + 1))
-#define XS_XSMEM (XS_RX * XS_RX + XS_XROWS * XS_XLINE)
+#define XS_XSMEM (XS_TWN(XS_RX) + XS_XROWS * XS_XLINE)
 
 __device__ __forceinline__ void xs_row_coords(int y, int t, int j, real& x, real& yy) {
   x = (real)(XS_O1 + XS_DX1 * (double)(t + XS_RX * j));
@@ -106,7 +129,7 @@ __device__ __forceinline__ void xs_xpass_core(const XsStreamArgs& A, int tid, si
   xs_fill_twiddles<XS_RX>(tw, A.tw_x, tid, 256);
   bsync();
   const int r = tid / XS_RX, t = tid % XS_RX;
-  cx* buf = tw + XS_RX * XS_RX + r * XS_XLINE;
+  cx* buf = tw + XS_TWN(XS_RX) + r * XS_XLINE;
   const size_t row = cta * XS_XROWS + r;  // over ntraj * NY
   // XS_XROWS divides NY, so a CTA's rows share one trajectory: taking e from the CTA index lets
   // the compiler keep the trajectory, its block and the Philox keys warp-uniform
@@ -171,14 +194,12 @@ __device__ __forceinline__ void xs_xpass_core(const XsStreamArgs& A, int tid, si
 #if XS_DSPLIT
       // a = (a0 + h inv) + h dep(a): the drift's field-independent terms once per site
       cx c0[XS_F];
-      xs_deriv_inv(a, w, (const cx*)nullptr, x, yy, (real)0, tm, A.params, (const cx*)nullptr, 0, 0, d);
-#pragma unroll
-      for (int f = 0; f < XS_F; ++f) c0[f] = a0[f] + h * d[f];
+      xs_deriv_c0(a, a0, h, w, (const cx*)nullptr, x, yy, (real)0, tm, A.params, (const cx*)nullptr, 0, 0, c0);
 #pragma unroll
       for (int it = 0; it < XS_ITER; ++it) {
-        xs_deriv_dep(a, w, (const cx*)nullptr, x, yy, (real)0, tm, A.params, (const cx*)nullptr, 0, 0, d);
+        xs_deriv_step(a, c0, h, w, (const cx*)nullptr, x, yy, (real)0, tm, A.params, (const cx*)nullptr, 0, 0, d);
 #pragma unroll
-        for (int f = 0; f < XS_F; ++f) a[f] = c0[f] + h * d[f];
+        for (int f = 0; f < XS_F; ++f) a[f] = d[f];
       }
 #else
 #pragma unroll
@@ -300,7 +321,7 @@ extern "C" __global__ void __launch_bounds__(256) xs_x_final(const XsStreamArgs 
 // write it back.  Per step: 16 N F s bytes (four passes over two fields).
 // Shared memory per row: two stages of XS_XLINE elements (field, field2), each
 // also the transpose scratch of its field's transforms.
-#define XS_XSMEM_RK (XS_RX * XS_RX + 2 * XS_XROWS * XS_XLINE)
+#define XS_XSMEM_RK (XS_TWN(XS_RX) + 2 * XS_XROWS * XS_XLINE)
 
 template <int MODE>
 __device__ __forceinline__ void xs_rk4_row(const XsStreamArgs& A) {
@@ -313,7 +334,7 @@ __device__ __forceinline__ void xs_rk4_row(const XsStreamArgs& A) {
   xs_fill_twiddles<XS_RX>(tw, A.tw_x);
   __syncthreads();
   const int r = threadIdx.x / XS_RX, t = threadIdx.x % XS_RX;
-  cx* sa = tw + XS_RX * XS_RX + (2 * r) * XS_XLINE;  // field a: stage and transpose scratch
+  cx* sa = tw + XS_TWN(XS_RX) + (2 * r) * XS_XLINE;  // field a: stage and transpose scratch
   cx* sb = sa + XS_XLINE;                             // field2
   const size_t cta = blockIdx.x;
   const int e = (int)((cta * XS_XROWS) / XS_NY), y = (int)((cta * XS_XROWS + r) % XS_NY);
@@ -429,7 +450,7 @@ extern "C" __global__ void __launch_bounds__(256) xs_x_rk3(const XsStreamArgs A)
 // ---- column pass ------------------------------------------------------------
 // CTA = TX consecutive kx columns of one (trajectory, component); thread
 // (c = tid % TX, t = tid / TX) holds y = t + RY*j of column c.
-#define XS_SSMEM (XS_RY * XS_RY + XS_TX * XS_RY * XS_RY)
+#define XS_SSMEM (XS_TWN(XS_RY) + XS_TX * XS_RY * XS_RY)
 
 // FFT_y, x exp(L dt)^m, IFFT_y of one tile column held four-step style in v.
 template <class Sync = XsBlockSync>
@@ -445,7 +466,12 @@ __device__ __forceinline__ void xs_col_tile(cx (&v)[XS_RY], int t, int c, int x0
 #else
   const double2* P = (A.m == 2 ? A.prop2 : A.prop1) + (XS_PROP_COMPS > 1 ? (size_t)f * XS_NS : 0);
 #endif
+  // (FP32: the unroll hint of 8 keeps the 64-register pass free of spills)
+#if XS_FP64
 #pragma unroll
+#else
+#pragma unroll 8
+#endif
   for (int k = 0; k < XS_RY; ++k) {
 #if XS_SEP
     const double2 ey = __ldg(&Pt[XS_NX + t + XS_RY * k]);
@@ -466,7 +492,7 @@ __device__ __forceinline__ void xs_col_core(const XsStreamArgs& A, int tid, size
   cx* tw = smem;
   xs_fill_twiddles<XS_RY>(tw, A.tw_y, tid, 256);
   const int c = tid % XS_TX, t = tid / XS_TX;
-  cx* buf = tw + XS_RY * XS_RY + c;  // element (k, t) of column c at ((k*RY + t)*TX + c)
+  cx* buf = tw + XS_TWN(XS_RY) + c;  // element (k, t) of column c at ((k*RY + t)*TX + c)
   constexpr int TILES = XS_NX / XS_TX;
   const int x0 = (int)(tile % TILES) * XS_TX;
   const size_t ef = tile / TILES;  // e * F + f
@@ -564,7 +590,7 @@ __device__ __forceinline__ void xs_tma_load_2d(const XsTmap* tm, u32 dst, u32 ba
 }
 
 #define XS_STAGE_ELEMS (XS_NY * XS_TX)
-#define XS_TSMEM_BYTES (2 * XS_STAGE_ELEMS * sizeof(cx) + XS_RY * XS_RY * sizeof(cx) + 16 + 128)
+#define XS_TSMEM_BYTES (2 * XS_STAGE_ELEMS * sizeof(cx) + XS_TWN(XS_RY) * sizeof(cx) + 16 + 128)
 
 extern "C" __global__ void __launch_bounds__(256) xs_s_pass_tma(const XsStreamArgs A, const __grid_constant__ XsTmap tmap) {
   constexpr int TILES = XS_NX / XS_TX;
@@ -574,7 +600,7 @@ extern "C" __global__ void __launch_bounds__(256) xs_s_pass_tma(const XsStreamAr
   cx* stage = (cx*)base;                 // [2][NY][TX] (row-major tiles as the copies deliver them)
   cx* tw = stage + 2 * XS_STAGE_ELEMS;   // [RY*RY] twiddles
   const int c = threadIdx.x % XS_TX, t = threadIdx.x / XS_TX;
-  unsigned long long* bars = (unsigned long long*)(tw + XS_RY * XS_RY);
+  unsigned long long* bars = (unsigned long long*)(tw + XS_TWN(XS_RY));
   const u32 bar0 = xs_smem_u32(&bars[0]);  // stage s completes on bar0 + 8 s
   if (threadIdx.x == 0) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar0) : "memory");
@@ -626,7 +652,7 @@ extern "C" __global__ void __launch_bounds__(256) xs_s_pass_tma(const XsStreamAr
 // CTA = (row group, block): OROWS rows of every trajectory of the block.
 // Site observables: block sums in FP64 registers, written as block means.
 // Reductions (Int/Ave): per-trajectory sums over the row group -> redpart.
-#define XS_OSMEM (XS_RX * XS_RX + XS_OROWS * XS_RX * (XS_RX + 1))
+#define XS_OSMEM (XS_TWN(XS_RX) + XS_OROWS * XS_RX * (XS_RX + 1))
 
 extern "C" __global__ void __launch_bounds__(XS_OROWS * XS_RX) xs_x_obs(const XsStreamArgs A) {
   if ((int)blockIdx.x >= XS_NRG || (size_t)(blockIdx.y + 1) * A.ens1 > (size_t)A.ntraj) {
@@ -639,7 +665,7 @@ extern "C" __global__ void __launch_bounds__(XS_OROWS * XS_RX) xs_x_obs(const Xs
   xs_fill_twiddles<XS_RX>(tw, A.tw_x);
   __syncthreads();
   const int r = threadIdx.x / XS_RX, t = threadIdx.x % XS_RX;
-  cx* buf = tw + XS_RX * XS_RX + r * XS_RX * (XS_RX + 1);
+  cx* buf = tw + XS_TWN(XS_RX) + r * XS_RX * (XS_RX + 1);
   const int rg = blockIdx.x;       // row group
   const int b = blockIdx.y;        // block within the launch
   const int y = rg * XS_OROWS + r;

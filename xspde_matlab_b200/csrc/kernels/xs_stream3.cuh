@@ -308,14 +308,14 @@ __device__ __forceinline__ void xs3_mp_sites(const XsStreamArgs& A, cx* P, int e
     a0[0] = a[0] = P[i2 * XS3_LSX + i1];
 #if XS_DSPLIT
     // a = (a0 + h inv) + h dep(a): the drift's field-independent terms once per site
-    xs_deriv_inv(a, w, (const cx*)nullptr, x, y, zz, tm, A.params, (const cx*)nullptr, 0, 0, d);
-    const cx c0 = a0[0] + h * d[0];
+    cx c0;
+    xs_deriv_c0(a, a0, h, w, (const cx*)nullptr, x, y, zz, tm, A.params, (const cx*)nullptr, 0, 0, &c0);
 #endif
 #pragma unroll
     for (int it = 0; it < XS_ITER; ++it) {
 #if XS_DSPLIT
-      xs_deriv_dep(a, w, (const cx*)nullptr, x, y, zz, tm, A.params, (const cx*)nullptr, 0, 0, d);
-      a[0] = c0 + h * d[0];
+      xs_deriv_step(a, &c0, h, w, (const cx*)nullptr, x, y, zz, tm, A.params, (const cx*)nullptr, 0, 0, d);
+      a[0] = d[0];
 #else
       xs_deriv(a, w, (const cx*)nullptr, x, y, zz, tm, A.params, (const cx*)nullptr, 0, 0, d);
       a[0] = a0[0] + h * d[0];

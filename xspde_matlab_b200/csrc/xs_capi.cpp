@@ -702,17 +702,18 @@ void generate_functions(Problem& P, std::ostringstream& os) {
     };
     body(g);
     os << "}\n";
-    // the drift's field-independent terms (noise, sources) apart, for MP's midpoint iterations
-    xs::Generated gd, gi;
-    const bool split = xs::generate_split(fn, make_ctx(P, roles, false), gd, gi) && gd.len == g.len && gi.len == g.len;
+    // the drift's field-independent terms (noise, sources) apart, for MP's midpoint iterations:
+    // xs_deriv_c0: c0 = a0 + h inv once per site, then xs_deriv_step: a = c0 + h dep(a)
+    xs::Generated g0, gs;
+    const bool split = xs::generate_split(fn, make_ctx(P, roles, false), g0, gs) && g0.len == g.len && gs.len == g.len;
     os << "#define XS_DSPLIT " << (split ? 1 : 0) << "\n";
     if (split) {
-      const char* sig = "(const cx* __restrict__ a, const real* __restrict__ w, const cx* __restrict__ zk, real x, real y, real z, real t, const double* __restrict__ prm, const cx* __restrict__ fld, int g, int s, cx* __restrict__ out) {\n";
-      const char* unused = "  (void)a; (void)w; (void)zk; (void)x; (void)y; (void)z; (void)t; (void)prm; (void)fld; (void)g; (void)s;\n";
-      os << "__device__ __forceinline__ void xs_deriv_dep" << sig << unused;
-      body(gd);
-      os << "}\n__device__ __forceinline__ void xs_deriv_inv" << sig << unused;
-      body(gi);
+      const char* args = "(const cx* __restrict__ a, const cx* __restrict__ c0, real h, const real* __restrict__ w, const cx* __restrict__ zk, real x, real y, real z, real t, const double* __restrict__ prm, const cx* __restrict__ fld, int g, int s, cx* __restrict__ out) {\n";
+      const char* unused = "  (void)a; (void)c0; (void)h; (void)w; (void)zk; (void)x; (void)y; (void)z; (void)t; (void)prm; (void)fld; (void)g; (void)s;\n";
+      os << "__device__ __forceinline__ void xs_deriv_c0" << args << unused;
+      body(g0);
+      os << "}\n__device__ __forceinline__ void xs_deriv_step" << args << unused;
+      body(gs);
       os << "}\n";
     }
   }
@@ -1424,13 +1425,14 @@ void plan_stream(xs_handle& h) {
   sp.OROWS = std::max(1, 64 / sp.RX);
   size_t cxs = h.fp64 ? 16 : 8;
   const size_t xline = std::max<size_t>((size_t)P.F * sp.RX * sp.RX, (size_t)sp.RX * (sp.RX + 1));
-  sp.xsmem = (sp.RX * sp.RX + sp.XROWS * xline) * cxs;
-  sp.ssmem = (size_t)(sp.RY * sp.RY + sp.TX * sp.RY * sp.RY) * cxs;
+  // twiddle tables: W and W/N (2 R^2 elements, xs_fill_twiddles)
+  sp.xsmem = (2 * sp.RX * sp.RX + sp.XROWS * xline) * cxs;
+  sp.ssmem = (size_t)(2 * sp.RY * sp.RY + sp.TX * sp.RY * sp.RY) * cxs;
   // TMA column pass: two [NY][TX] stages (each the transpose scratch of its tile), twiddles, two
   // mbarriers, alignment slack
-  sp.tsmem = 2 * (size_t)P.N[1] * sp.TX * cxs + (size_t)sp.RY * sp.RY * cxs + 16 + 128;
-  sp.osmem = (size_t)(sp.RX * sp.RX + sp.OROWS * sp.RX * (sp.RX + 1)) * cxs;
-  sp.rksmem = (sp.RX * sp.RX + 2 * sp.XROWS * xline) * cxs;
+  sp.tsmem = 2 * (size_t)P.N[1] * sp.TX * cxs + 2 * (size_t)sp.RY * sp.RY * cxs + 16 + 128;
+  sp.osmem = (size_t)(2 * sp.RX * sp.RX + sp.OROWS * sp.RX * (sp.RX + 1)) * cxs;
+  sp.rksmem = (2 * sp.RX * sp.RX + 2 * sp.XROWS * xline) * cxs;
   if (P.N[1] % sp.XROWS || P.N[1] % sp.OROWS || P.N[0] % sp.TX)
     raise(XS_ERR_SHAPE, "internal: streaming tile sizes do not divide the lattice");
   h.sp = sp;

@@ -873,6 +873,38 @@ struct Gen {
 
   Val gen(const NodeP& n) { return mat(gen_raw(n)); }
 
+  // sv * n for a scale sv that does not depend on the site (the step h times literal factors;
+  // real, purely imaginary or complex), with the scale pushed through sums, negations and
+  // quotients, literal factors folded into it and the rest applied to one scalar (real or purely
+  // imaginary) factor of each product, so that an accumulation c0 + sv*n contracts into fused
+  // multiply-adds.  Anything else is multiplied by the scale.
+  Val gen_h(const NodeP& n, const Val& sv) {
+    Vec cv;
+    if (n->kind != NK::Colon && try_const(n, cv)) return bin("*", sv, constant(cv, true), nullptr);
+    if (n->kind == NK::Bin && (n->name == "+" || n->name == "-") && n->kids.size() == 2)
+      return bin(n->name, gen_h(n->kids[0], sv), gen_h(n->kids[1], sv), nullptr);
+    if (n->kind == NK::Un && n->name == "-" && n->kids.size() == 1) return un("-", gen_h(n->kids[0], sv));
+    if (n->kind == NK::Un && n->name == "+" && n->kids.size() == 1) return gen_h(n->kids[0], sv);
+    if (n->kind == NK::Bin && (n->name == "*" || n->name == ".*") && n->kids.size() == 2) {
+      const NodeP &ln = n->kids[0], &rn = n->kids[1];
+      Vec lc, rc;
+      const bool lk = try_const(ln, lc) && lc.size() == 1, rk = try_const(rn, rc) && rc.size() == 1;
+      if (lk) return gen_h(rn, bin("*", sv, constant(lc, true), nullptr));
+      if (rk) return gen_h(ln, bin("*", sv, constant(rc, true), nullptr));
+      const Val l = gen_raw(ln), r = gen_raw(rn);
+      auto scalar = [](const Val& v) { return v.len == 1 && !v.cplx; };
+      if (scalar(l)) return bin(n->name, gen_h(ln, sv), r, rn);
+      if (scalar(r)) return bin(n->name, l, gen_h(rn, sv), rn);
+    }
+    if (n->kind == NK::Bin && (n->name == "/" || n->name == "./") && n->kids.size() == 2) {
+      Vec dc;
+      if (try_const(n->kids[1], dc) && dc.size() == 1 && dc[0] != C(0.0) && std::isfinite(std::abs(1.0 / dc[0])))
+        return gen_h(n->kids[0], bin("*", sv, constant({C(1.0) / dc[0]}, true), nullptr));
+      return bin(n->name, gen_h(n->kids[0], sv), gen_raw(n->kids[1]), n->kids[1]);
+    }
+    return bin("*", sv, gen_raw(n), nullptr);
+  }
+
   // gen() that may return a purely imaginary value (consumed only by bin()).
   Val gen_raw(const NodeP& n) {
     Vec cv;
@@ -1215,7 +1247,7 @@ void sum_terms(const NodeP& n, int sign, std::vector<std::pair<int, NodeP>>& out
 
 }  // namespace
 
-bool generate_split(const AnonFn& fn, const GenCtx& ctx, Generated& dep, Generated& inv) {
+bool generate_split(const AnonFn& fn, const GenCtx& ctx, Generated& start, Generated& step) {
   Gen g(ctx);
   bind_params(g, fn, ctx);
   if (g.aname.empty()) return false;
@@ -1228,39 +1260,39 @@ bool generate_split(const AnonFn& fn, const GenCtx& ctx, Generated& dep, Generat
   } else {
     rows.push_back(fn.body);
   }
+  std::vector<std::vector<std::pair<int, NodeP>>> rterms(rows.size());
+  std::vector<int> rlen(rows.size(), 1);
   bool any_dep = false, any_inv = false;
-  std::vector<std::string> dc, ic;  // per output component: complex expressions
-  for (auto& row : rows) {
-    std::vector<std::pair<int, NodeP>> terms;
-    sum_terms(row, 1, terms);
-    Val sd, si;
-    bool hd = false, hi = false;
-    for (auto& [sign, t] : terms) {
-      Val v = g.gen(t);
-      if (sign < 0) v = g.un("-", v);
-      const bool d = reads_var(t, g.aname);
-      Val& acc = d ? sd : si;
-      bool& has = d ? hd : hi;
-      acc = has ? g.bin("+", acc, v, nullptr) : v;
-      has = true;
-    }
-    any_dep = any_dep || hd;
-    any_inv = any_inv || hi;
-    const int len = std::max(hd ? sd.len : 1, hi ? si.len : 1);
-    if ((hd && sd.len != len && sd.len != 1) || (hi && si.len != len && si.len != 1)) return false;
-    auto comp = [&](const Val& v, bool has, int i) -> std::string {
-      if (!has) return "mkcx((real)0, (real)0)";
-      const std::string& c = v.c[v.len == 1 ? 0 : i];
-      return v.cplx ? c : "mkcx(" + c + ", (real)0)";
-    };
-    for (int i = 0; i < len; ++i) {
-      dc.push_back(comp(sd, hd, i));
-      ic.push_back(comp(si, hi, i));
+  for (size_t r = 0; r < rows.size(); ++r) {
+    sum_terms(rows[r], 1, rterms[r]);
+    for (auto& [sign, t] : rterms[r]) rlen[r] = std::max(rlen[r], g.gen(t).len);
+    for (auto& [sign, t] : rterms[r]) {
+      if (g.gen(t).len != rlen[r] && g.gen(t).len != 1) return false;
+      (reads_var(t, g.aname) ? any_dep : any_inv) = true;
     }
   }
   if (!any_dep || !any_inv) return false;
-  const std::string body = g.os.str();
-  auto fill = [&](Generated& out, const std::vector<std::string>& c) {
+  Val hv;
+  hv.c = {"h"};
+  // c0 + h * (the terms that read the field, or those that do not), accumulated term by term
+  auto accumulate = [&](bool dep) {
+    std::vector<std::string> out;
+    for (size_t r = 0; r < rows.size(); ++r) {
+      Val acc;
+      acc.len = rlen[r];
+      acc.cplx = true;
+      acc.spatial = true;
+      for (int i = 0; i < rlen[r]; ++i) acc.c.push_back("c0[" + std::to_string((int)out.size() + i) + "]");
+      for (auto& [sign, t] : rterms[r])
+        if (reads_var(t, g.aname) == dep) acc = g.bin(sign < 0 ? "-" : "+", acc, g.gen_h(t, hv), nullptr);
+      for (int i = 0; i < rlen[r]; ++i) {
+        const std::string& c = acc.c[acc.len == 1 ? 0 : i];
+        out.push_back(acc.cplx ? c : "mkcx(" + c + ", (real)0)");
+      }
+    }
+    return out;
+  };
+  auto fill = [&](Generated& out, const std::string& body, const std::vector<std::string>& c) {
     out = Generated{};
     out.len = (int)c.size();
     out.is_complex = true;
@@ -1270,8 +1302,10 @@ bool generate_split(const AnonFn& fn, const GenCtx& ctx, Generated& dep, Generat
     out.code = code.str();
     out.stencil = g.stencil;
   };
-  fill(dep, dc);
-  fill(inv, ic);
+  const std::vector<std::string> ic = accumulate(false);
+  fill(start, g.os.str(), ic);
+  const std::vector<std::string> sc = accumulate(true);
+  fill(step, g.os.str(), sc);
   return true;
 }
 

@@ -94,10 +94,13 @@ Generated generate(const AnonFn& fn, const GenCtx& ctx);
 
 // Additive split of a drift D(a, ...) = dep(a, ...) + inv(...) along the terms of its outermost
 // sum (per component of a top-level [e1; e2; ...]): `inv` collects the terms that do not read the
-// field a, `dep` the rest, both with len components (complex).  The midpoint iterations of MP
-// evaluate D several times with the same noise: a = (a0 + h inv) + h dep(a) computes the
-// field-independent part once.  Returns false when either part would be empty (no gain).
-bool generate_split(const AnonFn& fn, const GenCtx& ctx, Generated& dep, Generated& inv);
+// field a.  The midpoint iterations of MP evaluate a = a0 + h D(a) several times with the same
+// noise; they compute `start`: out = c0 + h inv once per site (with c0 = a0), then `step`:
+// out = c0 + h dep(a) in each iteration.  In the emitted code h is a real scalar `h` and c0 a
+// complex array `c0`; h is pushed through sums and into one scalar factor of each product (with
+// literal factors folded into it) so that the updates contract into fused multiply-adds.  Both
+// have len components (complex).  Returns false when either part would be empty (no gain).
+bool generate_split(const AnonFn& fn, const GenCtx& ctx, Generated& start, Generated& step);
 
 // Host FP64 evaluation of the linear operator on the propagation grid:
 // returns L per (component, site) with component count 1 or F.
