@@ -47,7 +47,7 @@ HBM_FALLBACK_GBS = 6650.0
 # capture of a 512-trajectory case of this problem; a launch's traffic grows
 # in proportion to the trajectories it processes, so bench lines scale these
 # by the trajectory count.
-NCU_TRAFFIC_PER_TRAJ = {("x_step", 8): (268465408 + 209754880) / 512.0, ("y_pass", 8): (268470528 + 213135104) / 512.0}
+NCU_TRAFFIC_PER_TRAJ = {("x_step", 8): (268598272 + 209662208) / 512.0, ("y_pass", 8): (268474880 + 213282816) / 512.0}
 
 
 def _peaks():

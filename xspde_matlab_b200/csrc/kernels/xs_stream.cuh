@@ -41,7 +41,7 @@ __device__ __forceinline__ cx xs_cj(cx a) { return mkcx(a.re, -a.im); }
 // the same table divided by N for the inverse transforms (N a power of two, so
 // the division is exact).  XS_TWN(R) elements in all.
 #define XS_TWN(R) (2 * (R) * (R))
-template <int R>
+template <int R, bool SCALED = true>
 __device__ __forceinline__ void xs_fill_twiddles(cx* tw, const cx* __restrict__ src, int tid = -1, int nthr = 0) {
   if (tid < 0) {
     tid = threadIdx.x;
@@ -51,7 +51,7 @@ __device__ __forceinline__ void xs_fill_twiddles(cx* tw, const cx* __restrict__ 
   for (int i = tid; i < R * R; i += nthr) {
     const cx w = src[i];
     tw[i] = w;
-    tw[R * R + i] = mkcx(w.re * sc, w.im * sc);
+    if (SCALED) tw[R * R + i] = mkcx(w.re * sc, w.im * sc);
   }
 }
 
@@ -96,6 +96,17 @@ __device__ __forceinline__ void xs_ifft4(cx (&v)[R], int t, const cx* __restrict
   for (int n = 0; n < R; ++n) v[n] = buf[(t * (R + PAD) + n) * LS];
   sync();
   xs_dftR<R>(v);
+#pragma unroll
+  for (int k = 0; k < R; ++k) v[k] = xs_cj(v[k]);
+}
+
+// Unnormalised inverse DFT (exp(+2 pi i n k / N), no 1/N): conj, forward, conj.  For callers that
+// fold the 1/N into a multiply of their own.
+template <int R, int LS, int PAD, class Sync>
+__device__ __forceinline__ void xs_ifft4u(cx (&v)[R], int t, const cx* __restrict__ tw, cx* buf, Sync sync) {
+#pragma unroll
+  for (int k = 0; k < R; ++k) v[k] = xs_cj(v[k]);
+  xs_fft4<R, LS, PAD>(v, t, tw, buf, sync);
 #pragma unroll
   for (int k = 0; k < R; ++k) v[k] = xs_cj(v[k]);
 }
@@ -460,29 +471,30 @@ __device__ __forceinline__ void xs_col_tile(cx (&v)[XS_RY], int t, int c, int x0
 #if XS_SEP
   // separable L(kx, ky) = Lx(kx) + Ly(ky): exp(L dt) = ex[kx] * ey[ky] from two
   // 1D FP64 tables [NX] + [NY] (L1-resident) instead of the [NY][NX] table
+  // The inverse transform's 1/NY (a power of two: exact, bit-identical to scaling its output)
+  // rides on the FP64 propagator multiply.
+  const double sc = 1.0 / (double)XS_NY;
   const double2* Pt = A.m == 2 ? A.prop2 : A.prop1;
-  const double2 ex = __ldg(&Pt[x0 + c]);
+  const double2 ex0 = __ldg(&Pt[x0 + c]);
+  const double2 ex = make_double2(ex0.x * sc, ex0.y * sc);
   (void)f;
 #else
+  const double sc = 1.0 / (double)XS_NY;
   const double2* P = (A.m == 2 ? A.prop2 : A.prop1) + (XS_PROP_COMPS > 1 ? (size_t)f * XS_NS : 0);
 #endif
-  // (FP32: the unroll hint of 8 keeps the 64-register pass free of spills)
-#if XS_FP64
 #pragma unroll
-#else
-#pragma unroll 8
-#endif
   for (int k = 0; k < XS_RY; ++k) {
 #if XS_SEP
     const double2 ey = __ldg(&Pt[XS_NX + t + XS_RY * k]);
     const double2 pr = make_double2(ey.x * ex.x - ey.y * ex.y, ey.x * ex.y + ey.y * ex.x);
+    const double vr = (double)v[k].re, vi = (double)v[k].im;
 #else
     const double2 pr = __ldg(&P[(size_t)(t + XS_RY * k) * XS_NX + x0 + c]);
+    const double vr = (double)v[k].re * sc, vi = (double)v[k].im * sc;
 #endif
-    const double vr = (double)v[k].re, vi = (double)v[k].im;
     v[k] = mkcx((real)(vr * pr.x - vi * pr.y), (real)(vr * pr.y + vi * pr.x));
   }
-  xs_ifft4<XS_RY, XS_TX, 0>(v, t, tw, buf, bs);
+  xs_ifft4u<XS_RY, XS_TX, 0>(v, t, tw, buf, bs);
 }
 
 // Column tile `tile` (over ntraj * F * NX/TX) by 256 threads tid = 0..255 with
@@ -490,7 +502,7 @@ __device__ __forceinline__ void xs_col_tile(cx (&v)[XS_RY], int t, int c, int x0
 template <class Sync>
 __device__ __forceinline__ void xs_col_core(const XsStreamArgs& A, int tid, size_t tile, cx* smem, Sync bs) {
   cx* tw = smem;
-  xs_fill_twiddles<XS_RY>(tw, A.tw_y, tid, 256);
+  xs_fill_twiddles<XS_RY, false>(tw, A.tw_y, tid, 256);  // xs_col_tile scales through the propagator
   const int c = tid % XS_TX, t = tid / XS_TX;
   cx* buf = tw + XS_TWN(XS_RY) + c;  // element (k, t) of column c at ((k*RY + t)*TX + c)
   constexpr int TILES = XS_NX / XS_TX;
@@ -607,7 +619,7 @@ extern "C" __global__ void __launch_bounds__(256) xs_s_pass_tma(const XsStreamAr
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar0 + 8u) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  xs_fill_twiddles<XS_RY>(tw, A.tw_y);
+  xs_fill_twiddles<XS_RY, false>(tw, A.tw_y);
   __syncthreads();
   const u32 bytes = (u32)(XS_STAGE_ELEMS * sizeof(cx));
   auto issue = [&](int tile, int sidx) {
