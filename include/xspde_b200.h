@@ -290,8 +290,9 @@ XS_API xs_status xs_set_kernel_timing(xs_handle* h, int on);
 XS_API xs_status xs_kernel_stats(xs_handle* h, int reset, double* ms_out, long long* launches_out);
 
 /* Uneven batch (no counterpart in the reference): many independent problems,
- * each one ensemble block (ensembles(2) = ensembles(3) = 1, checks = 0),
- * integrated by ONE CUDA-graph launch.  Items whose generated kernels agree
+ * each one ensemble block (ensembles(2) = ensembles(3) = 1), integrated by
+ * ONE CUDA-graph launch.  An item with checks = 1 runs both check passes of
+ * xensemble.m:41-45 (fine, nc = 1, and coarse, nc = 2) inside the same graph.  Items whose generated kernels agree
  * (same lattice, fields, expressions, method, precision; set runtime_params
  * so that named scalars differ per item) share a persistent kernel that pulls
  * (item, trajectory tile) units from a longest-first queue; items too large
@@ -302,8 +303,9 @@ XS_API xs_status xs_kernel_stats(xs_handle* h, int reset, double* ms_out, long l
  *   xs_batch_run     captures the graph on first use, then launches it on
  *                    `stream` (NULL: the batch's own stream); asynchronous
  *   xs_batch_sync    waits for the device and reports kernel status
- *   xs_batch_results item means in the layout of xs_run_path's av_out
- *                    (xs_batch_av_doubles doubles)
+ *   xs_batch_results item means in the layout of xs_run_path's av_out, the
+ *                    fine pass followed (checks = 1) by the coarse pass
+ *                    (xs_batch_av_doubles doubles in all)
  *   xs_batch_info    item >= 0: {variant, path (1 resident, 2 streaming), G,
  *                    threads, CTAs, units}; item < 0: {items, variants,
  *                    streaming items, kernel launches per run} */

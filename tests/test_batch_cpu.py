@@ -49,10 +49,16 @@ def test_batch_grouping_host_only():
     assert len(names) == len({items[b.index[i]]["name"] for i in range(len(b)) if b.info(i)["path"] == 1})
 
 
-def test_batch_rejects_items_with_checks_or_blocks():
+def test_batch_checks_and_block_rules():
+    """checks = 1 items are accepted (both passes run in the graph; two pass
+    results per item), checks > 1 and several ensemble blocks are refused."""
     from xspde_matlab_b200 import _lib
     items = batch.uneven_instances(2, seed=1)
-    bad = dict(items[0], checks=1)
+    one = batch.Batch([items[0]])
+    two = batch.Batch([dict(items[0], checks=1)])
+    L = _lib.lib()
+    assert L.xs_batch_av_doubles(two.h, 0) == 2 * L.xs_batch_av_doubles(one.h, 0) > 0
+    bad = dict(items[0], checks=2)
     with pytest.raises(_lib.XsError, match="checks"):
         batch.Batch([bad])
     bad = dict(items[0], ensembles=[64, 2, 1])

@@ -126,3 +126,49 @@ def test_dpo_batch_fp64_matches_oracle():
         for k in range(2):
             e = rel_err(got[k].reshape(-1, order="F"), av_o[k].reshape(-1, order="F"))
             assert e < 1e-10, (i, k, e)
+
+
+def test_batch_checked_items_run_both_passes():
+    """Items with checks = 1 (Simulator/xensemble.m:41-45): the graph runs the
+    fine pass (nc = 1) and the coarse pass (nc = 2, twice the step, mean of two
+    fine draws) of every item, resident and streaming alike; each pass equals
+    the single-problem path's pass on the same input (1e-12), and the FP64
+    item's step error |fine - coarse| agrees with the oracle's to 1e-9
+    relative (a difference of two close means)."""
+    from xspde_matlab_b200.batch import Batch
+    items = [dict(it, checks=1) for it in _items()[:6]]
+    items[0] = dict(items[0], precision="fp64")
+    b = Batch(items)
+    s = b.summary()
+    assert s["items"] == len(items) and s["streaming"] == 1, s
+    b.run()
+    b.sync()
+    from xspde_matlab_b200 import GpuPath, xpreferences
+    from xspde_matlab_b200.batch import _named_scalars
+    for i, inp in enumerate(items):
+        fine, coarse = b.passes(i)
+        p = xpreferences([_named_scalars(inp)])[0]
+        path = GpuPath(p, 0, runtime_params=True)
+        for nc, got in ((1, fine), (2, coarse)):
+            av, _ = path.run_path(0, 1, nc)
+            ref = av[0]
+            for o in range(len(ref)):
+                e = rel_err(got[o].reshape(-1), ref[o].reshape(-1))
+                assert e < SUM_ORDER_TOL, (i, nc, o, e, b.info(i))
+        mean, err = b.results(i, step_error=True)
+        assert np.array_equal(mean[0], fine[0]) and np.allclose(err[0], np.abs(fine[0] - coarse[0]))
+    # the FP64 item against the oracle's two passes
+    inp = items[0]
+    g = inp["g"]
+    o = {k: v for k, v in inp.items() if k not in ("deriv", "linear", "initial", "observe", "g", "precision")}
+    o.update(deriv=lambda a, w, p, g=g: 1j * np.abs(a) ** 2 * a + 1j * g * a * w[0:1],
+             linear=lambda p: 0.5j * p.Dx ** 2, initial=lambda v, p: np.exp(-p.x ** 2 / 4) + 0 * v[0:1],
+             observe=[lambda a, p: np.abs(a) ** 2])
+    f_o, _ = oracle_block_av(o, 0, 1)
+    c_o, _ = oracle_block_av(o, 0, 2)
+    fine, coarse = b.passes(0)
+    assert rel_err(fine[0].reshape(-1, order="F"), f_o[0].reshape(-1, order="F")) < 1e-10
+    assert rel_err(coarse[0].reshape(-1, order="F"), c_o[0].reshape(-1, order="F")) < 1e-10
+    se = np.abs(fine[0] - coarse[0]).reshape(-1, order="F")
+    se_o = np.abs(f_o[0] - c_o[0]).reshape(-1, order="F")
+    assert np.max(se_o) > 0 and np.max(np.abs(se - se_o)) < 1e-9 * np.max(np.abs(f_o[0]))

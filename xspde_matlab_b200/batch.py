@@ -8,9 +8,12 @@ agree share a persistent kernel with a longest-first work queue, items too
 large for shared memory run their streaming launches inside the same graph,
 and the project's autotuner picks each variant's trajectory tile.
 
-An item is one ensemble block (``ensembles = [ntraj, 1, 1]``, ``checks = 0``);
-its result is the block mean of every observable, exactly what
-``GpuPath.run_path(0, 1, 1)`` returns for the same input.
+An item is one ensemble block (``ensembles = [ntraj, 1, 1]``); its result is
+the block mean of every observable, exactly what ``GpuPath.run_path(0, 1, 1)``
+returns for the same input.  With ``checks = 1`` the graph also runs the
+coarse pass (``run_path(0, 1, 2)``), and ``results`` returns the fine pass
+(Richardson-extrapolated when ``order > 0``) with the step error beside it, as
+xsim forms them (Simulator/xensemble.m:41-45, xsim.m:64-98).
 """
 import ctypes
 
@@ -143,9 +146,10 @@ class Batch:
         _lib.check(_lib.lib().xs_batch_info(self.h, i, info, 6))
         return dict(variant=info[0], path=info[1], G=info[2], threads=info[3], ctas=info[4], units=info[5])
 
-    def results(self, i):
-        """Block means of item i: one complex array per observable, shaped
-        [lines, points(1), space...] like GpuPath.run_path's av."""
+    def passes(self, i):
+        """Block means of item i per check pass: [fine] or, with checks = 1,
+        [fine, coarse]; each a list with one complex array per observable,
+        shaped [lines, points(1), space...] like GpuPath.run_path's av."""
         L = _lib.lib()
         n = L.xs_batch_av_doubles(self.h, i)
         buf = np.empty(max(n, 1), dtype=np.float64)
@@ -153,12 +157,35 @@ class Batch:
         cbuf = buf[:n].view(np.complex128)
         p = self.inputs[i]
         out, pos = [], 0
-        for o in range(len(p.observe)):
-            shp = _obs_shape(p, o)
-            m = int(np.prod(shp))
-            out.append(np.reshape(cbuf[pos:pos + m], shp, order="F"))
-            pos += m
+        for _ in range(1 + (1 if p.checks[0] else 0)):
+            one = []
+            for o in range(len(p.observe)):
+                shp = _obs_shape(p, o)
+                m = int(np.prod(shp))
+                one.append(np.reshape(cbuf[pos:pos + m], shp, order="F"))
+                pos += m
+            out.append(one)
         return out
+
+    def results(self, i, step_error=False):
+        """Block means of item i: one complex array per observable, shaped
+        [lines, points(1), space...] like GpuPath.run_path's av.  With
+        checks = 1 the fine pass, extrapolated as d1 + (d1 - d2)/(2^order - 1)
+        when order > 0 (xsim's _ensembles); step_error=True also returns the
+        step errors |mean - d2| per observable (None without checks)."""
+        ps = self.passes(i)
+        p = self.inputs[i]
+        if len(ps) == 1:
+            return (ps[0], None) if step_error else ps[0]
+        fine, coarse = ps
+        if p.order > 0:
+            mean = [d1 + (d1 - d2) / (2 ** p.order - 1.0) for d1, d2 in zip(fine, coarse)]
+            ref = fine
+        else:
+            mean, ref = fine, coarse
+        if not step_error:
+            return mean
+        return mean, [np.abs(m - r) for m, r in zip(mean, ref)]
 
 
 def _named_scalars(inp):

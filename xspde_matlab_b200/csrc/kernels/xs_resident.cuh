@@ -1205,7 +1205,7 @@ struct XsBatchItem {
   u32 seed;
   int block0;
   int nunits;
-  int pad;
+  short nc, checks;      // check pass (1 fine, 2 coarse) and p.checks of the item
   double wscale, vscale, dtr, t0;
   const double2* prop;   // [XS_PROP_COMPS][XS_NS] exp(L dtr / ipsteps) of this item
   double2* part;         // [npoints][nunits][XS_OBS_STRIDE] partial sums
@@ -1242,8 +1242,8 @@ extern "C" __global__ void __launch_bounds__(XS_THREADS) xs_batch(const XsBatchA
     P.ntraj = it.ntraj;
     P.ens1 = it.ntraj;
     P.block0 = it.block0;
-    P.nc = 1;
-    P.checks = 0;
+    P.nc = it.nc;
+    P.checks = it.checks;
     P.npoints = it.npoints;
     P.steps = it.steps;
     P.seq = it.seq;

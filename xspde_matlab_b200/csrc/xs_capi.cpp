@@ -3218,7 +3218,8 @@ namespace {
 struct BatchItemHost {  // mirrors XsBatchItem
   int ntraj, steps, npoints, seq;
   unsigned seed;
-  int block0, nunits, pad;
+  int block0, nunits;
+  short nc, checks;
   double wscale, vscale, dtr, t0;
   const void* prop;
   void* part;
@@ -3261,14 +3262,19 @@ struct BatchVariant {
 struct BatchEntry {
   std::unique_ptr<xs_handle> h;    // the item's problem; streaming items also run through it
   int variant = -1;                // resident variant, -1 = streaming path
-  size_t av_off = 0, part_off = 0, prop_off = 0, param_off = 0;  // element offsets
+  // check passes (xensemble.m:41-45): 1, or 2 with p.checks = 1 (pass 0 fine, nc = 1; pass 1
+  // coarse, nc = 2 with twice the step and the mean of two fine draws)
+  int passes = 1;
+  size_t av_off = 0, param_off = 0;        // element offsets; pass q's means at av_off + q * av_pass
+  size_t av_pass = 0;
+  size_t part_off[2] = {0, 0}, prop_off[2] = {0, 0};
+  int done_off = 0;                        // unit counter of pass q: d_done[done_off + q]
   int nunits = 0;
   double work = 0;                 // trajectory-steps x sites
 };
 
 int ntraj_of(const Problem& P) { return P.p.ensembles[0]; }
 
-double item_dtr(const Problem& P) { return P.dt / P.p.steps; }  // fine pass (xensemble.m:41-45)
 
 std::vector<cd> prop_table(const Problem& P, double dtr) {
   std::vector<cd> pr(P.L.size());
@@ -3391,34 +3397,40 @@ void variant_tables(xs_batch& b, BatchVariant& v, int steps_cap, int points_cap,
   for (size_t k = 0; k < v.items.size(); ++k) {
     BatchEntry& e = *b.items[v.items[k]];
     const Problem& P = e.h->P;
-    BatchItemHost it{};
-    it.ntraj = ntraj_of(P);
-    it.steps = steps_cap > 0 ? std::min(P.p.steps, steps_cap) : P.p.steps;
-    it.npoints = points_cap > 0 ? std::min(P.p.points[0], points_cap) : P.p.points[0];
-    it.seq = P.p.sequence;
-    it.seed = (unsigned)(P.p.seed & 0xffffffffu);
-    it.block0 = 0;
-    it.nunits = it.ntraj / v.G;
-    it.wscale = std::sqrt(P.nscale * P.noisefactor);  // xnoise.m:32
-    it.vscale = std::sqrt(P.noisefactor);              // xrandom.m:22
-    it.dtr = item_dtr(P);
-    it.t0 = P.p.origins[0];
-    it.prop = (const char*)b.d_prop.p + e.prop_off * 16;
-    it.prop2 = (const char*)b.d_prop.p + (e.prop_off + (P.has_linear ? P.L.size() : 1)) * 16;
-    const size_t stride = av_stride(P);
-    if (part_base) {
-      it.part = (char*)part_base + part * 16;
-      part += (size_t)it.npoints * it.nunits * stride;
-    } else {
-      it.part = (char*)b.d_part.p + e.part_off * 16;
+    for (int q = 0; q < e.passes; ++q) {  // one table row per check pass
+      BatchItemHost it{};
+      it.ntraj = ntraj_of(P);
+      it.steps = steps_cap > 0 ? std::min(P.p.steps, steps_cap) : P.p.steps;
+      it.npoints = points_cap > 0 ? std::min(P.p.points[0], points_cap) : P.p.points[0];
+      it.seq = P.p.sequence;
+      it.seed = (unsigned)(P.p.seed & 0xffffffffu);
+      it.block0 = 0;
+      it.nunits = it.ntraj / v.G;
+      it.nc = (short)(q + 1);
+      it.checks = (short)(e.passes - 1);
+      it.wscale = std::sqrt(P.nscale * P.noisefactor);  // xnoise.m:32
+      it.vscale = std::sqrt(P.noisefactor);              // xrandom.m:22
+      it.dtr = pass_dtr(P, q + 1);
+      it.t0 = P.p.origins[0];
+      it.prop = (const char*)b.d_prop.p + e.prop_off[q] * 16;
+      it.prop2 = (const char*)b.d_prop.p + (e.prop_off[q] + (P.has_linear ? P.L.size() : 1)) * 16;
+      const size_t stride = av_stride(P);
+      if (part_base) {
+        it.part = (char*)part_base + part * 16;
+        part += (size_t)it.npoints * it.nunits * stride;
+      } else {
+        it.part = (char*)b.d_part.p + e.part_off[q] * 16;
+      }
+      it.av = (char*)b.d_av.p + (e.av_off + q * e.av_pass) * 16;
+      it.params = P.runtime_defaults.empty() ? (const double*)b.d_params.p
+                                             : (const double*)((const char*)b.d_params.p + e.param_off * 8);
+      it.done = (int*)b.d_done.p + e.done_off + q;
+      const int row = (int)its.size();
+      its.push_back(it);
+      // the fine pass of a checked item takes two steps per coarse step
+      const double cost = (double)it.steps * it.npoints * (e.passes > 1 && q == 0 ? 2 : 1);
+      for (int u = 0; u < it.nunits; ++u) units.push_back({cost, {row, u}});
     }
-    it.av = (char*)b.d_av.p + e.av_off * 16;
-    it.params = P.runtime_defaults.empty() ? (const double*)b.d_params.p
-                                           : (const double*)((const char*)b.d_params.p + e.param_off * 8);
-    it.done = (int*)b.d_done.p + v.items[k];
-    its.push_back(it);
-    const double cost = (double)it.steps * it.npoints;
-    for (int u = 0; u < it.nunits; ++u) units.push_back({cost, {(int)k, u}});
   }
   std::stable_sort(units.begin(), units.end(), [](const auto& a, const auto& c) { return a.first > c.first; });
   std::vector<int> flat;
@@ -3462,30 +3474,38 @@ int variant_grid(BatchVariant& v) {
 
 // Device buffers shared by all items: propagators, runtime scalars, means,
 // partial sums, unit counters.
+int batch_counters(const xs_batch& b);
+
 void batch_buffers(xs_batch& b) {
   size_t prop = 0, par = 0, av = 0, part = 0;
+  int done = 0;
   for (auto& ep : b.items) {
     BatchEntry& e = *ep;
     const Problem& P = e.h->P;
     const size_t stride = av_stride(P);
     e.av_off = av;
-    av += (size_t)P.p.points[0] * stride;
+    e.av_pass = (size_t)P.p.points[0] * stride;
+    av += e.passes * e.av_pass;
+    e.done_off = done;
+    done += e.passes;
     if (e.variant < 0) continue;
     const BatchVariant& v = *b.variants[e.variant];
     e.nunits = ntraj_of(P) / std::max(v.G, 1);
-    e.prop_off = prop;  // exp(L dtr/ipsteps), then exp(2 L dtr/ipsteps)
-    prop += 2 * (P.has_linear ? P.L.size() : 1);
     e.param_off = par;
     par += P.runtime_defaults.size();
-    e.part_off = part;
-    part += (size_t)P.p.points[0] * e.nunits * stride;
+    for (int q = 0; q < e.passes; ++q) {
+      e.prop_off[q] = prop;  // exp(L dtr/ipsteps), then exp(2 L dtr/ipsteps), dtr of pass q
+      prop += 2 * (P.has_linear ? P.L.size() : 1);
+      e.part_off[q] = part;
+      part += (size_t)P.p.points[0] * e.nunits * stride;
+    }
   }
   b.av_total = av;
   b.d_av.ensure(std::max<size_t>(av, 1) * 16);
   b.d_part.ensure(std::max<size_t>(part, 1) * 16);
   b.d_prop.ensure(std::max<size_t>(prop, 1) * 16);
   b.d_params.ensure(std::max<size_t>(par, 1) * 8);
-  b.d_done.ensure(std::max<size_t>(b.items.size(), 1) * sizeof(int));
+  b.d_done.ensure(std::max<size_t>(done, 1) * sizeof(int));
   b.d_status.ensure(sizeof(int));
   std::vector<cd> hp(std::max<size_t>(prop, 1));
   std::vector<double> hpar(std::max<size_t>(par, 1));
@@ -3493,18 +3513,27 @@ void batch_buffers(xs_batch& b) {
     BatchEntry& e = *ep;
     if (e.variant < 0) continue;
     const Problem& P = e.h->P;
-    if (P.has_linear) {
-      auto pr = prop_table(P, item_dtr(P));
-      std::copy(pr.begin(), pr.end(), hp.begin() + e.prop_off);
-      auto pr2 = prop_table(P, 2 * item_dtr(P));
-      std::copy(pr2.begin(), pr2.end(), hp.begin() + e.prop_off + pr.size());
-    }
+    if (P.has_linear)
+      for (int q = 0; q < e.passes; ++q) {
+        const double dtr = pass_dtr(P, q + 1);
+        auto pr = prop_table(P, dtr);
+        std::copy(pr.begin(), pr.end(), hp.begin() + e.prop_off[q]);
+        auto pr2 = prop_table(P, 2 * dtr);
+        std::copy(pr2.begin(), pr2.end(), hp.begin() + e.prop_off[q] + pr.size());
+      }
     std::copy(P.runtime_defaults.begin(), P.runtime_defaults.end(), hpar.begin() + e.param_off);
   }
   CUDA_CHECK(cudaMemcpy(b.d_prop.p, hp.data(), hp.size() * 16, cudaMemcpyHostToDevice));
   CUDA_CHECK(cudaMemcpy(b.d_params.p, hpar.data(), hpar.size() * 8, cudaMemcpyHostToDevice));
-  CUDA_CHECK(cudaMemset(b.d_done.p, 0, b.items.size() * sizeof(int)));
+  CUDA_CHECK(cudaMemset(b.d_done.p, 0, std::max(done, 1) * sizeof(int)));
   CUDA_CHECK(cudaMemset(b.d_status.p, 0, sizeof(int)));
+}
+
+// unit counters of all items and passes (d_done)
+int batch_counters(const xs_batch& b) {
+  int n = 0;
+  for (auto& ep : b.items) n += ep->passes;
+  return std::max(n, 1);
 }
 
 void compile_all(std::vector<xs_handle*>& hs) {
@@ -3582,8 +3611,9 @@ void batch_tune(xs_batch& b, int mode) {
         double ts = 0;
         for (int i : v.items) {
           const Problem& P = b.items[i]->h->P;
-          part += (size_t)std::min(P.p.points[0], 1) * (ntraj_of(P) / v.G) * av_stride(P);
-          ts += (double)ntraj_of(P) * std::min(P.p.steps, 8);
+          const int np = b.items[i]->passes;
+          part += np * (size_t)std::min(P.p.points[0], 1) * (ntraj_of(P) / v.G) * av_stride(P);
+          ts += (double)ntraj_of(P) * std::min(P.p.steps, 8) * (np > 1 ? 3 : 1);
         }
         d_part.ensure(std::max<size_t>(part, 1) * 16);
         variant_tables(b, v, 8, 1, d_items, d_units, d_part.p);
@@ -3595,7 +3625,7 @@ void batch_tune(xs_batch& b, int mode) {
         float ms = 1e30f;
         for (int rep = 0; rep < 2; ++rep) {
           CUDA_CHECK(cudaMemsetAsync(v.d_next.p, 0, sizeof(int), b.stream));
-          CUDA_CHECK(cudaMemsetAsync(b.d_done.p, 0, b.items.size() * sizeof(int), b.stream));
+          CUDA_CHECK(cudaMemsetAsync(b.d_done.p, 0, batch_counters(b) * sizeof(int), b.stream));
           CUDA_CHECK(cudaEventRecord(e0, b.stream));
           variant_launch(b, v, d_items, d_units, b.stream);
           CUDA_CHECK(cudaEventRecord(e1, b.stream));
@@ -3678,8 +3708,10 @@ void batch_prepare(xs_batch& b) {
       const int parts = h.kind == 3 ? P.N[2] : P.N[1] / h.sp.OROWS;  // reduction parts per trajectory
       if (P.nred) h.d_redpart.ensure((size_t)P.E1 * parts * P.nred * 16);
       if (P.nout_site) h.d_opart.ensure((size_t)kObsSplit * P.nout_site * P.NS * 16);
-      ensure_prop(h, 1);
-      ensure_prop2(h, 1);
+      for (int q = 1; q <= b.items[i]->passes; ++q) {
+        ensure_prop(h, q);
+        ensure_prop2(h, q);
+      }
       sitems.push_back((int)i);
     }
   std::sort(sitems.begin(), sitems.end(), [&](int x, int y) { return b.items[x]->work > b.items[y]->work; });
@@ -3705,7 +3737,7 @@ void batch_prepare(xs_batch& b) {
   int launches = 0;
   CUDA_CHECK(cudaStreamBeginCapture(b.stream, cudaStreamCaptureModeRelaxed));
   try {
-    CUDA_CHECK(cudaMemsetAsync(b.d_done.p, 0, b.items.size() * sizeof(int), b.stream));
+    CUDA_CHECK(cudaMemsetAsync(b.d_done.p, 0, batch_counters(b) * sizeof(int), b.stream));
     CUDA_CHECK(cudaMemsetAsync(b.d_status.p, 0, sizeof(int), b.stream));
     for (auto& vp : b.variants) CUDA_CHECK(cudaMemsetAsync(vp->d_next.p, 0, sizeof(int), b.stream));
     for (int i : sitems) CUDA_CHECK(cudaMemsetAsync(b.items[i]->h->d_status.p, 0, sizeof(int), b.stream));
@@ -3722,7 +3754,9 @@ void batch_prepare(xs_batch& b) {
       BatchEntry& e = *b.items[sitems[q]];
       xs_handle& h = *e.h;
       const long long before = std::accumulate(std::begin(h.launches), std::end(h.launches), 0LL);
-      launch_stream(h, 0, 1, 1, nullptr, (char*)b.d_av.p + e.av_off * 16, nullptr, b.side[q % nside]);
+      for (int pass = 0; pass < e.passes; ++pass)
+        launch_stream(h, 0, 1, pass + 1, nullptr, (char*)b.d_av.p + (e.av_off + pass * e.av_pass) * 16, nullptr,
+                      b.side[q % nside]);
       launches += (int)(std::accumulate(std::begin(h.launches), std::end(h.launches), 0LL) - before);
     }
     for (int s = 0; s < nside; ++s) {
@@ -3760,7 +3794,7 @@ XS_API xs_status xs_batch_create(const xs_problem* items, int nitems, xs_batch**
         h.fp64 = items[i].precision != XS_PREC_FP32;
         if (items[i].path_kind < 0 || items[i].path_kind > 2) raise(XS_ERR_ARG, "path_kind must be 0, 1 or 2");
         h.path_kind = items[i].path_kind;
-        if (items[i].checks) raise(XS_ERR_UNSUPPORTED, "batch items run the fine pass only (checks = 0)");
+        if (items[i].checks < 0 || items[i].checks > 1) raise(XS_ERR_UNSUPPORTED, "batch items take checks = 0 or 1");
         if (items[i].boundary_values) raise(XS_ERR_UNSUPPORTED, "batch items take no boundary values");
         if (h.P.spec) raise(XS_ERR_UNSUPPORTED, "batch items take no time-spectrum observables");
         if (h.P.NK || h.P.NKV) raise(XS_ERR_UNSUPPORTED, "batch items take no k-filtered noises");
@@ -3774,7 +3808,8 @@ XS_API xs_status xs_batch_create(const xs_problem* items, int nitems, xs_batch**
         throw;
       }
       const Problem& P = h.P;
-      e->work = (double)ntraj_of(P) * P.p.steps * std::max(1, P.p.points[0] - 1) * P.NS;
+      e->passes = P.p.checks ? 2 : 1;
+      e->work = (double)ntraj_of(P) * P.p.steps * std::max(1, P.p.points[0] - 1) * P.NS * (P.p.checks ? 3 : 1);
       if (h.kind == 1) {
         auto it = vmap.find(h.source);
         if (it == vmap.end()) {
@@ -3836,7 +3871,7 @@ XS_API xs_status xs_batch_sync(xs_batch* b) {
 
 XS_API size_t xs_batch_av_doubles(const xs_batch* b, int item) {
   if (!b || item < 0 || item >= (int)b->items.size()) return 0;
-  return av_doubles_per_block(b->items[item]->h->P);
+  return b->items[item]->passes * av_doubles_per_block(b->items[item]->h->P);
 }
 
 XS_API xs_status xs_batch_results(xs_batch* b, int item, double* av_out) {
@@ -3848,8 +3883,12 @@ XS_API xs_status xs_batch_results(xs_batch* b, int item, double* av_out) {
     const size_t n = (size_t)P.p.points[0] * av_stride(P) * 2;
     std::vector<double> dev(std::max<size_t>(n, 1));
     CUDA_CHECK(cudaStreamSynchronize(b->stream));
-    if (n) CUDA_CHECK(cudaMemcpy(dev.data(), (const char*)b->d_av.p + e.av_off * 16, n * 8, cudaMemcpyDeviceToHost));
-    scatter_av(P, dev, 1, av_out);
+    for (int q = 0; q < e.passes; ++q) {  // fine pass, then (checks = 1) the coarse pass
+      if (n)
+        CUDA_CHECK(cudaMemcpy(dev.data(), (const char*)b->d_av.p + (e.av_off + q * e.av_pass) * 16, n * 8,
+                              cudaMemcpyDeviceToHost));
+      scatter_av(P, dev, 1, av_out + q * av_doubles_per_block(P));
+    }
     return XS_OK;
   });
 }
