@@ -97,3 +97,22 @@ def test_stream3_diverging_trajectory_reports_nan():
     with pytest.raises(_lib.XsError) as err:
         path.run_path(0, 1, 1, a_out=True)
     assert err.value.code == -5  # XS_ERR_NAN
+
+
+@pytest.mark.parametrize("boundaries", [
+    ((-1, -1), (1, 1), (-1, 1)),   # DCT-I in x, DST-I in y (the benchmark's boundaries)
+    ((1, -1), (-1, 1), (1, 1)),    # DST-III/II in x, DCT-III/II in y
+])
+def test_stream3_tensor_core_plane_pass_fp32(boundaries, monkeypatch):
+    """64 x 64 planes in FP32 take the tensor-core plane pass (xs_stream3_tc.cuh:
+    the four transforms as tcgen05 TF32 GEMMs with the three-term split): both
+    check passes, each observable and the final field within 1e-5 of the FP64
+    oracle, like the CUDA-core pass (XSPDE_B200_TC3=0); the two passes round
+    differently, so their results are not bit-identical."""
+    g, o = _ac((2, 64, 64, 8), boundaries, "fp32", ens=(2, 1, 1), steps=3, ranges=(20.0, 20.0, 5.0))
+    _check(g, o, [0], [1, 2], FP32_TOL)
+    av_tc, a_tc = _run(g, [0], 1)
+    monkeypatch.setenv("XSPDE_B200_TC3", "0")
+    av_cc, a_cc = _run(g, [0], 1)
+    assert rel_err(a_tc, a_cc) < 2 * FP32_TOL
+    assert not np.array_equal(a_tc, a_cc)

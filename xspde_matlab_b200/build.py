@@ -14,7 +14,8 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libxspde_b200.so")
 CUDA = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 KERNELS = [("prelude", "xs_prelude.cuh"), ("noise", "xs_noise.cuh"), ("resident", "xs_resident.cuh"),
-           ("stream_common", "xs_stream_common.cuh"), ("stream", "xs_stream.cuh"), ("stream3", "xs_stream3.cuh")]
+           ("stream_common", "xs_stream_common.cuh"), ("stream", "xs_stream.cuh"), ("stream3", "xs_stream3.cuh"),
+           ("stream3_tc", "xs_stream3_tc.cuh")]
 SOURCES = ["xs_capi.cpp", "xs_expr.cpp", "xs_aot.cu", "xs_noalloc.cu", "xs_mlp.cu"]
 
 

@@ -293,9 +293,10 @@ template <int MODE> __host__ __device__ constexpr int xs3_psmem() {
   return xs3_pinv<MODE>() + ((MODE == 1 || MODE == 2) ? xs3_msize<0>() + xs3_msize<2>() : 0);
 }
 
-// One MP step of the sites of plane z held in P (x space): noise, midpoint
+// One MP step of the sites of plane z held in P (x space, row stride LS; NT threads): noise, midpoint
 // iterations at t + dtr/2 with the Dirichlet mask (Applications/SDE/MP.m:13-23,
 // Simulator/xsetbound.m), 2a - a0, written back in place.
+template <int LS = XS3_LSX, int NT = 256>
 __device__ __forceinline__ void xs3_mp_sites(const XsStreamArgs& A, cx* P, int e, int z, int tid) {
   const u32 blk = (u32)(A.block0 + e / A.ens1), el = (u32)(e % A.ens1);
   const real h = (real)(A.dtr * 0.5);
@@ -305,7 +306,7 @@ __device__ __forceinline__ void xs3_mp_sites(const XsStreamArgs& A, cx* P, int e
     real x, y, zz;
     xs3_coords(i1, i2, z, x, y, zz);
     cx a0[1], a[1], d[1];
-    a0[0] = a[0] = P[i2 * XS3_LSX + i1];
+    a0[0] = a[0] = P[i2 * LS + i1];
 #if XS_DSPLIT
     // a = (a0 + h inv) + h dep(a): the drift's field-independent terms once per site
     cx c0;
@@ -324,13 +325,13 @@ __device__ __forceinline__ void xs3_mp_sites(const XsStreamArgs& A, cx* P, int e
       if (xs_dirichlet(0, i1, i2, z)) a[0] = mkcx((real)0, (real)0);
 #endif
     }
-    P[i2 * XS3_LSX + i1] = (real)2 * a[0] - a0[0];
+    P[i2 * LS + i1] = (real)2 * a[0] - a0[0];
   };
 #if XS_NW > 0 && XS_PAIRED(XS_NW)
   // one Philox call per pair of sites (x, x + N1/2) of a row
   constexpr int H = XS3_N1 / 2;
 #pragma unroll 1
-  for (int pi = tid; pi < XS3_NP / 2; pi += 256) {
+  for (int pi = tid; pi < XS3_NP / 2; pi += NT) {
     const int i2 = pi / H, xl = pi % H;
     const u32 pidx = (u32)xl + (u32)H * (u32)(i2 + XS3_N2 * z);
     real wl[XS_NW], wh[XS_NW];
@@ -355,7 +356,7 @@ __device__ __forceinline__ void xs3_mp_sites(const XsStreamArgs& A, cx* P, int e
   }
 #else
 #pragma unroll 1
-  for (int i = tid; i < XS3_NP; i += 256) {
+  for (int i = tid; i < XS3_NP; i += NT) {
     const int i2 = i / XS3_N1, i1 = i % XS3_N1;
     real w[XS_NW > 0 ? XS_NW : 1];
 #if XS_NW > 0

@@ -39,6 +39,7 @@ extern const char* xs_kernel_source_resident;
 extern const char* xs_kernel_source_stream;
 extern const char* xs_kernel_source_stream_common;
 extern const char* xs_kernel_source_stream3;
+extern const char* xs_kernel_source_stream3_tc;
 
 namespace {
 
@@ -643,6 +644,11 @@ std::vector<double> pack_folded(const std::vector<cd>& M, int n, const FoldInfo&
 // ---------------------------------------------------------------------------
 // Code generation
 // ---------------------------------------------------------------------------
+// dynamic shared memory of xs_p_nl_tc (xs_stream3_tc.cuh, tc3::SMEM_BYTES): B hi/lo of four
+// 64 x 64 TF32 matrices, A hi and lo (128 x 64), mbarrier and tensor-memory slot, alignment slack
+constexpr size_t kTc3Smem = 8 * 16384 + 2 * 32768 + 16 + 1024;
+constexpr unsigned kTc3Threads = 512;  // tc3::NTH
+
 std::string fmt(double v) {
   char b[64];
   snprintf(b, sizeof b, "%.17g", v);
@@ -1053,7 +1059,10 @@ struct xs_handle {
   CUfunction f_pinit = nullptr, f_ptok = nullptr, f_pnl = nullptr, f_pfinal = nullptr, f_zpass = nullptr,
              f_pobs = nullptr;  // 3D
   DevBuf d_mat3;                                        // 3D: real transform matrices
-  int grid_p = 0, grid_z = 0;                           // 3D: persistent grids of the plane and z-line passes
+  bool tc3 = false;                                     // 3D: plane pass on the tensor cores
+  CUfunction f_pnl_tc = nullptr;
+  DevBuf d_mat3tc;                                      // its transforms: FP32 B_m[k][n] = M[n][k]
+  int grid_p = 0, grid_z = 0, grid_tc = 0;                           // 3D: persistent grids of the plane and z-line passes
   StreamPlan sp;
   int path_kind = 0;
   int force_G = 0, force_threads = 0;  // resident tile fixed by the caller (uneven batch)
@@ -1520,8 +1529,14 @@ void build_source(xs_handle& h) {
       for (int i = 0; i < 6; ++i)
         os << "#define XS3_MOFF" << i << " " << h.sp.moff3[i] << "\n#define XS3_FOLD" << i << " " << h.sp.fold3[i]
            << "\n#define XS3_CEN" << i << " " << h.sp.cen3[i] << "\n#define XS3_PAR" << i << " " << h.sp.par3[i] << "\n";
+      // plane pass on the tensor cores (xs_stream3_tc.cuh): 64 x 64 planes, FP32 fields;
+      // XSPDE_B200_TC3=0 keeps the CUDA-core plane pass
+      const char* tce = getenv("XSPDE_B200_TC3");
+      h.tc3 = !h.fp64 && P.N[0] == 64 && P.N[1] == 64 && P.F == 1 && !(tce && *tce == '0');
+      os << "#define XS3_TC " << (h.tc3 ? 1 : 0) << "\n";
       os << fns.str();
-      os << xs_kernel_source_stream_common << "\n" << xs_kernel_source_stream3 << "\n";
+      os << xs_kernel_source_stream_common << "\n" << xs_kernel_source_stream3 << "\n" << xs_kernel_source_stream3_tc
+         << "\n";
       h.source = os.str();
       return;
     }
@@ -1661,6 +1676,27 @@ void load_module(xs_handle& h) {
         h.d_mat3.ensure(f32.size() * 4);
         CUDA_CHECK(cudaMemcpy(h.d_mat3.p, f32.data(), f32.size() * 4, cudaMemcpyHostToDevice));
       }
+    }
+    if (h.tc3) {  // x inverse, y inverse, x forward, y forward as B[k][n] = M[n][k] (xs_stream3_tc.cuh)
+      const size_t smem = kTc3Smem;
+      cu_check(d.getfn(&h.f_pnl_tc, h.mod, "xs_p_nl_tc"), "xs_p_nl_tc");
+      cu_check(d.setattr(h.f_pnl_tc, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, (int)smem), "xs_p_nl_tc");
+      int occ = 0, dev = 0, sms = 0;
+      cu_check(d.occupancy(&occ, h.f_pnl_tc, kTc3Threads, smem), "occupancy");
+      if (occ < 1) raise(XS_ERR_UNSUPPORTED, "tensor-core plane pass cannot be resident on an SM");
+      CUDA_CHECK(cudaGetDevice(&dev));
+      CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+      h.grid_tc = sms * occ;
+      const Problem& P = h.P;
+      std::vector<float> bt;
+      for (int i : {1, 3, 0, 2}) {
+        const int dd = i / 2, n = P.N[dd];
+        const auto M = transform_matrix(P.type(dd, 0), i % 2 == 1, n);
+        for (int k = 0; k < n; ++k)
+          for (int q = 0; q < n; ++q) bt.push_back((float)M[(size_t)q * n + k].real());
+      }
+      h.d_mat3tc.ensure(bt.size() * 4);
+      CUDA_CHECK(cudaMemcpy(h.d_mat3tc.p, bt.data(), bt.size() * 4, cudaMemcpyHostToDevice));
     }
     h.d_status.ensure(sizeof(int));
     h.loaded = true;
@@ -2279,7 +2315,15 @@ void launch_stream3(xs_handle& h, int first_block, int nblocks, int nc, const vo
         break;
       }
       case StreamOp::ROW:
-        xs_launch(h, XS_KERNEL_X_STEP, h.f_pnl, gp, 1, 1, 256, (unsigned)sp.psmem3[1], st, params, "plane pass");
+        if (h.tc3) {
+          const void* mt = h.d_mat3tc.p;
+          void* tparams[] = {&a, &mt};
+          const unsigned gt = (unsigned)std::min<size_t>(nplanes, (size_t)h.grid_tc);
+          xs_launch(h, XS_KERNEL_X_STEP, h.f_pnl_tc, gt, 1, 1, kTc3Threads, (unsigned)kTc3Smem, st, tparams,
+                    "plane pass (tensor cores)");
+        } else {
+          xs_launch(h, XS_KERNEL_X_STEP, h.f_pnl, gp, 1, 1, 256, (unsigned)sp.psmem3[1], st, params, "plane pass");
+        }
         break;
       case StreamOp::FINAL:
         xs_launch(h, XS_KERNEL_X_FINAL, h.f_pfinal, gp, 1, 1, 256, (unsigned)sp.psmem3[2], st, params, "plane pass");
