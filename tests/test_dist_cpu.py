@@ -104,3 +104,67 @@ def test_compensated_moment_sums():
     for x in (1e16, 1.0, -1e16, 1.0, 3.0, -3.0):
         plain += x
     assert plain != 2.0
+
+
+def _xsim_inputs():
+    """A stochastic NLS on 8 points, 4 blocks of 3 trajectories, both check passes."""
+    base = dict(dimensions=2, points=[4, 8], ranges=[0.5, 6.0], steps=2, ensembles=[3, 4, 1], noises=2,
+                method="MP", checks=1, order=1)
+    g = dict(base, deriv="@(a,w,p) 1i*a.*conj(a).*a + 0.05*(w(1,:)+1i*w(2,:))",
+             initial="@(v,p) exp(-p.x.^2)", linear="@(p) 1i*p.Dx.^2", observe=["@(a,p) a.*conj(a)"])
+    o = dict(base, deriv=lambda a, w, p: 1j * a * np.conj(a) * a + 0.05 * (w[0:1] + 1j * w[1:2]),
+             initial=lambda v, p: np.exp(-p.x ** 2), linear=lambda p: 1j * p.Dx ** 2,
+             observe=[lambda a, p: a * np.conj(a)])
+    return g, o
+
+
+def _xsim_worker(rank, size, port, out):
+    import importlib
+
+    import torch.distributed as dist
+    from tests.test_host_mirror_cpu import OraclePath
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=size)
+    try:
+        M = importlib.import_module("xspde_matlab_b200.xsim")
+        g, o = _xsim_inputs()
+        M.GpuPath = lambda p, path_kind=0, runtime_params=False: OraclePath(p, o)
+        e, d, _ = M.xsim(g)
+        if rank == 0:
+            out.put((np.asarray(e), [np.asarray(x) for x in d[0]]))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_ranks_xsim_with_oracle_blocks_matches_oracle_xsim():
+    """The whole host xsim on two gloo ranks, each integrating its half of the
+    blocks through the oracle's own p.path (Simulator/xpath.m) and one
+    all-reduce of the moment sums (xsim.m:50-57, addcell): the error vector and
+    data columns equal the oracle's single-process xsim (1e-10; the mirror's
+    sums are compensated, the oracle's plain)."""
+    import warnings
+
+    from oracle import xspde_ref as X
+    g, o = _xsim_inputs()
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore", RuntimeWarning)
+        eo, do, _ = X.xsim(o)
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_xsim_worker, args=(r, 2, port, q)) for r in range(2)]
+    for pr in procs:
+        pr.start()
+    eg, dg = q.get(timeout=300)
+    for pr in procs:
+        pr.join(timeout=120)
+        assert pr.exitcode == 0
+    eo = np.asarray(eo)
+    keep = [i for i in range(len(eo)) if i != 5]  # error(6) is the run time
+    assert np.allclose(eg[keep], eo[keep], rtol=1e-10, atol=1e-15), (eg, eo)
+    for a, b in zip(dg, do[0]):
+        assert np.allclose(a, np.asarray(b), rtol=1e-10, atol=1e-13)
