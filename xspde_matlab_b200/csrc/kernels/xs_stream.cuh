@@ -129,6 +129,14 @@ __device__ __forceinline__ void xs_row_coords(int y, int t, int j, real& x, real
   yy = (real)(XS_O2 + XS_DX2 * (double)y);
 }
 
+// XS_ROW_STAGE 1: the MP row pass stages its elements in shared memory so that the
+// per-element drift/noise loop stays rolled (one copy of the code); 0 unrolls it over the
+// registers, without the four shared-memory accesses per site: 4% faster in FP32 (1.437 against
+// 1.499 ms per launch at 4096 trajectories of 256^2); FP64 keeps the stage (128 registers).
+#ifndef XS_ROW_STAGE
+#define XS_ROW_STAGE (XS_FP64 ? 1 : 0)
+#endif
+
 // MODE 0: initial field (expression or a_in) -> K state
 // MODE 1: one MP step in x space (K state in, K state out)
 // MODE 3: K state -> x-space a_out (FP64)
@@ -189,11 +197,17 @@ __device__ __forceinline__ void xs_xpass_core(const XsStreamArgs& A, int tid, si
     // only its own elements, stage[(f*RX + j)*RX + t].
     const real h = (real)(A.dtr * 0.5);
     const real tm = (real)(A.t + A.dtr * 0.5);
+    // XS_ROW_STAGE 0: the per-element loop fully unrolled over the registers instead (no stage)
+#if XS_ROW_STAGE
     cx* stage = buf;
+#define XS_ROWEL(f, j) stage[((f) * XS_RX + (j)) * XS_RX + t]
 #pragma unroll
     for (int f = 0; f < XS_F; ++f)
 #pragma unroll
       for (int j = 0; j < XS_RX; ++j) stage[(f * XS_RX + j) * XS_RX + t] = v[f][j];
+#else
+#define XS_ROWEL(f, j) v[f][j]
+#endif
     // One element: noise w (already scaled and, on a coarse pass, averaged),
     // midpoint iterations, 2a - a0.
     auto nl_element = [&](int j, const real* w) {
@@ -201,7 +215,7 @@ __device__ __forceinline__ void xs_xpass_core(const XsStreamArgs& A, int tid, si
       xs_row_coords(y, t, j, x, yy);
       cx a0[XS_F], a[XS_F], d[XS_F];
 #pragma unroll
-      for (int f = 0; f < XS_F; ++f) a0[f] = a[f] = stage[(f * XS_RX + j) * XS_RX + t];
+      for (int f = 0; f < XS_F; ++f) a0[f] = a[f] = XS_ROWEL(f, j);
 #if XS_DSPLIT
       // a = (a0 + h inv) + h dep(a): the drift's field-independent terms once per site
       cx c0[XS_F];
@@ -221,12 +235,16 @@ __device__ __forceinline__ void xs_xpass_core(const XsStreamArgs& A, int tid, si
       }
 #endif
 #pragma unroll
-      for (int f = 0; f < XS_F; ++f) stage[(f * XS_RX + j) * XS_RX + t] = (real)2 * a[f] - a0[f];
+      for (int f = 0; f < XS_F; ++f) XS_ROWEL(f, j) = (real)2 * a[f] - a0[f];
     };
     const real ws = (real)A.wscale;
 #if XS_NW > 0 && XS_PAIRED(XS_NW)
     // one Philox call per pair of sites (x, x + NX/2) = elements (j, j + RX/2)
+#if XS_ROW_STAGE
 #pragma unroll 1
+#else
+#pragma unroll
+#endif
     for (int j = 0; j < XS_RX / 2; ++j) {
       const u32 pidx = (u32)(t + XS_RX * j) + (u32)(XS_NX / 2) * (u32)y;
       real wl[XS_NW], wh[XS_NW];
@@ -250,7 +268,11 @@ __device__ __forceinline__ void xs_xpass_core(const XsStreamArgs& A, int tid, si
       nl_element(j + XS_RX / 2, wh);
     }
 #else
+#if XS_ROW_STAGE
 #pragma unroll 1
+#else
+#pragma unroll
+#endif
     for (int j = 0; j < XS_RX; ++j) {
       const u32 s = (u32)(y * XS_NX + t + XS_RX * j);
       real w[XS_NW > 0 ? XS_NW : 1];
@@ -269,11 +291,14 @@ __device__ __forceinline__ void xs_xpass_core(const XsStreamArgs& A, int tid, si
       nl_element(j, w);
     }
 #endif
+#if XS_ROW_STAGE
 #pragma unroll
     for (int f = 0; f < XS_F; ++f)
 #pragma unroll
       for (int j = 0; j < XS_RX; ++j) v[f][j] = stage[(f * XS_RX + j) * XS_RX + t];
     __syncwarp();  // the FFT below reuses the scratch other threads may still read
+#endif
+#undef XS_ROWEL
   }
   if (MODE == 3) {
     bool bad = false;
