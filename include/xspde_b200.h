@@ -138,6 +138,15 @@ XS_API const char* xs_version(void);
  * Simulator/xpreferences.m:262-343. */
 XS_API xs_status xs_observe_info(const xs_handle* h, int o, int* lines, int* spatial);
 
+/* Space sizes of av{o} for a spatial observable: dims[d] (d = 0, 1, 2 for x, y, z)
+ * is the lattice's points, 1 for a dimension that an observable of the form
+ * Int(f, dx, [bounds,] p) or Ave(f, v, p) over a subset of the dimensions reduces
+ * (Applications/SPDE/Int.m:48-70, Ave.m), and 1 beyond the lattice's dimensions.
+ * Such an observable is evaluated per site on the device and summed over its
+ * reduced dimensions on the host when the means are copied out (xs_run_path,
+ * xs_batch_results); xs_run_path_device returns the unreduced site means. */
+XS_API xs_status xs_observe_shape(const xs_handle* h, int o, int* dims);
+
 /* Bytes of av_out for nblocks blocks: sum over observables of
  * lines*points(1)*(spatial ? nspace : 1) complex doubles, per block. */
 XS_API size_t xs_av_doubles_per_block(const xs_handle* h);

@@ -156,3 +156,32 @@ def test_time_spectrum_refused_on_streaming_path(tmp_path, monkeypatch):
     assert rc == -9 and "time-spectrum observables" in _lib.last_error()
     p.path_kind = 1
     assert _lib.lib().xs_compile_check(ctypes.byref(p), None, 0) == 0, _lib.last_error()
+
+
+def test_partial_int_observable_shape():
+    """An Int over x of a 2D lattice is the lattice with x of size 1 in av{o}
+    (Applications/SPDE/Int.m:48-70); a nonlinear function of such an Int is refused."""
+    import ctypes
+
+    from xspde_matlab_b200 import _lib, xpreferences
+    from xspde_matlab_b200.xsim import make_problem
+    base = dict(dimensions=3, points=[3, 8, 6], ranges=[1.0, 4.0, 3.0], deriv="@(a,w,p) 0*a",
+                initial="@(v,p) 1 + 0*p.x")
+    L = _lib.lib()
+    p = xpreferences([dict(base, observe=["@(a,p) Int(abs(a).^2, [0, 0.5, 0], p)", "@(a,p) a"])])[0]
+    pr, keep = make_problem(p)
+    h = ctypes.c_void_p()
+    _lib.check(L.xs_create(ctypes.byref(pr), ctypes.byref(h)))
+    try:
+        dims = (ctypes.c_int * 3)()
+        _lib.check(L.xs_observe_shape(h, 0, dims))
+        assert list(dims) == [1, 6, 1]
+        _lib.check(L.xs_observe_shape(h, 1, dims))
+        assert list(dims) == [8, 6, 1]
+        assert L.xs_av_doubles_per_block(h) == 2 * 3 * (6 + 48)
+    finally:
+        L.xs_destroy(h)
+    p = xpreferences([dict(base, observe=["@(a,p) Int(abs(a).^2, [0, 0.5, 0], p).^2"])])[0]
+    pr, keep = make_problem(p)
+    assert L.xs_create(ctypes.byref(pr), ctypes.byref(h)) != 0
+    assert "whole observable" in _lib.last_error()

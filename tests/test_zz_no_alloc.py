@@ -31,7 +31,7 @@ def _path(p):
 def _av(path, nblocks):
     import torch
     P = path.p
-    row = sum(ln * (P.nspace if sp else 1) for ln, sp in path.obs)
+    row = sum(ln * (P.nspace if sp else 1) for ln, sp, *_ in path.obs)
     return torch.zeros((nblocks, P.points[0], row, 2), dtype=torch.float64, device="cuda")
 
 

@@ -14,7 +14,8 @@ METHODS = {"MP": 0, "RK4": 1, "Euler": 2, "RK2": 3, "Implicit": 4}
 MAXDIM = 4
 
 # Every symbol include/xspde_b200.h declares.
-EXPORTS = ["xs_create", "xs_destroy", "xs_last_error", "xs_version", "xs_observe_info", "xs_av_doubles_per_block",
+EXPORTS = ["xs_create", "xs_destroy", "xs_last_error", "xs_version", "xs_observe_info", "xs_observe_shape",
+           "xs_av_doubles_per_block",
            "xs_path_kind",
            "xs_run_path", "xs_run_path_device", "xs_sync", "xs_noise", "xs_random", "xs_step", "xs_compile_check",
            "xs_set_kernel_timing", "xs_kernel_stats", "xs_run_path_device_noalloc", "xs_noise_features",
@@ -91,6 +92,8 @@ def lib():
         L.xs_version.restype = ctypes.c_char_p
         L.xs_observe_info.argtypes = [ctypes.c_void_p, ctypes.c_int, P(ctypes.c_int), P(ctypes.c_int)]
         L.xs_observe_info.restype = ctypes.c_int
+        L.xs_observe_shape.argtypes = [ctypes.c_void_p, ctypes.c_int, P(ctypes.c_int)]
+        L.xs_observe_shape.restype = ctypes.c_int
         L.xs_av_doubles_per_block.argtypes = [ctypes.c_void_p]
         L.xs_av_doubles_per_block.restype = ctypes.c_size_t
         L.xs_path_kind.argtypes = [ctypes.c_void_p]

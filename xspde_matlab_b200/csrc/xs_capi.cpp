@@ -261,6 +261,13 @@ struct ObsInfo {
   bool kspace = false;  // evaluated on the Fourier-transformed field (p.transforms{n})
   bool tspec = false;   // evaluated on the time spectrum of the field (p.transforms{n}(1))
   xs::Generated gen;
+  // Int/Ave over a subset of the space dimensions that is the whole observable (Int.m:48-70,
+  // Ave.m): the device evaluates the integrand as a site observable and the host sums the
+  // block means over the reduced dimensions (a linear map: it commutes with the ensemble mean).
+  // pw[d] > 0: dimension d reduced with weight pw[d] (Int: dx or dk; Ave: 1 / points);
+  // bounds plo[d] < phi[d] restrict an Int to the points of Int.m's rule.
+  bool partial = false;
+  double pw[3] = {0, 0, 0}, plo[3] = {0, 0, 0}, phi[3] = {0, 0, 0};
 };
 
 struct Problem {
@@ -783,11 +790,36 @@ void generate_functions(Problem& P, std::ostringstream& os) {
     o.spatial = o.gen.spatial;  // depends on the field or the site (0-D: one site)
     if (o.gen.stencil) P.stencil = true;
     o.red_off = P.nred;
-    for (auto& r : o.gen.reductions) {
-      if ((int)r.dims.size() != P.D)
-        raise(XS_ERR_UNSUPPORTED, "Int/Ave over a subset of the space dimensions is not supported on the device");
-      P.nred += r.lines;
+    bool subset = false;
+    for (auto& r : o.gen.reductions) subset = subset || (int)r.dims.size() != P.D;
+    if (subset) {
+      const xs::NodeP& body = fn.body;
+      const bool top = body->kind == xs::NK::Index && body->kids.size() >= 3 && body->kids[0]->kind == xs::NK::Var &&
+                       (body->kids[0]->name == "Int" || body->kids[0]->name == "Ave") &&
+                       o.gen.reductions.size() == 1;
+      if (!top)
+        raise(XS_ERR_UNSUPPORTED,
+              "Int/Ave over a subset of the space dimensions must be the whole observable on the device");
+      const xs::Reduction R = o.gen.reductions[0];
+      bool bounded = false;
+      for (size_t k = 0; k < R.dims.size(); ++k) {
+        const int d = R.dims[k] - 1;  // space dimension, 0 = x
+        o.pw[d] = R.ave ? 1.0 / P.N[d] : R.weight[k];
+        o.plo[d] = R.lo[d + 1];
+        o.phi[d] = R.hi[d + 1];
+        bounded = bounded || o.plo[d] < o.phi[d];
+      }
+      if (bounded && o.kspace) raise(XS_ERR_UNSUPPORTED, "Int bounds over a subset of k-space dimensions");
+      xs::AnonFn f2 = fn;
+      f2.body = body->kids[1];  // the integrand, one value per site
+      o.gen = xs::generate(f2, make_ctx(P, P.NA ? std::vector<Role>{Role::Field, Role::Aux, Role::Params}
+                                                : std::vector<Role>{Role::Field, Role::Params}, true));
+      if (!o.gen.reductions.empty()) raise(XS_ERR_UNSUPPORTED, "nested Int/Ave");
+      o.lines = o.gen.len;
+      o.spatial = true;
+      o.partial = true;
     }
+    for (auto& r : o.gen.reductions) P.nred += r.lines;
     if (o.spatial) {
       o.out_off = P.nout_site;
       P.nout_site += o.lines;
@@ -1906,9 +1938,25 @@ struct PathArgsHost {
 
 size_t av_stride(const Problem& P) { return (size_t)P.nout_site * P.NS + P.nout_scalar; }
 
+// sites of observable o in the MATLAB av{o} layout: the lattice, the lattice with its reduced
+// dimensions of size 1 (a partial Int/Ave), or one
+size_t obs_sites(const Problem& P, const ObsInfo& o) {
+  if (!o.spatial) return 1;
+  if (!o.partial) return P.NS;
+  size_t n = 1;
+  for (int d = 0; d < P.D; ++d) n *= o.pw[d] > 0 ? 1 : (size_t)P.N[d];
+  return n;
+}
+
+bool any_partial(const Problem& P) {
+  for (auto& o : P.obs)
+    if (o.partial) return true;
+  return false;
+}
+
 size_t av_doubles_per_block(const Problem& P) {
   size_t n = 0;
-  for (auto& o : P.obs) n += (size_t)2 * o.lines * P.p.points[0] * (o.spatial ? P.NS : 1);
+  for (auto& o : P.obs) n += (size_t)2 * o.lines * P.p.points[0] * obs_sites(P, o);
   return n;
 }
 
@@ -2541,6 +2589,52 @@ void scatter_av(const Problem& P, const std::vector<double>& dev, int nblocks, d
     double* ob = out + (size_t)b * per_block;
     o_off = 0;
     for (auto& o : P.obs) {
+      if (o.partial) {  // sum the block means over the reduced dimensions (Int.m:48-70, Ave.m)
+        const size_t ns = obs_sites(P, o);
+        std::vector<int> j0(3, 0), keep(3, 1);
+        for (int d = 0; d < P.D; ++d)
+          if (o.pw[d] > 0) {
+            keep[d] = 0;
+            if (o.plo[d] < o.phi[d])  // first point 1 + floor((lo - x(1)) / dx), 1-based, as Int.m
+              j0[d] = std::max(0, (int)std::floor((o.plo[d] - P.p.origins[d + 1]) / P.dx[d + 1]));
+          }
+        std::vector<double> acc((size_t)2 * o.lines * ns);
+        for (int n = 0; n < npts; ++n) {
+          std::fill(acc.begin(), acc.end(), 0.0);
+          for (size_t s = 0; s < P.NS; ++s) {
+            const int i[3] = {(int)(s % P.N[0]), P.D > 1 ? (int)((s / P.N[0]) % P.N[1]) : 0,
+                              P.D > 2 ? (int)(s / ((size_t)P.N[0] * P.N[1])) : 0};
+            double w = 1;
+            size_t r = 0, rs = 1;
+            bool in = true;
+            for (int d = 0; d < P.D; ++d) {
+              if (keep[d]) {
+                r += (size_t)i[d] * rs;
+                rs *= (size_t)P.N[d];
+                continue;
+              }
+              w *= o.pw[d];
+              if (o.plo[d] < o.phi[d])
+                in = in && i[d] >= j0[d] && P.p.origins[d + 1] + i[d] * P.dx[d + 1] <= o.phi[d];
+            }
+            if (!in) continue;
+            for (int l = 0; l < o.lines; ++l) {
+              const size_t k = (size_t)(o.out_off + l) * P.NS + s;
+              const size_t src = (((size_t)b * npts + n) * stride + k) * 2;
+              acc[2 * ((size_t)l + (size_t)o.lines * r)] += w * dev[src];
+              acc[2 * ((size_t)l + (size_t)o.lines * r) + 1] += w * dev[src + 1];
+            }
+          }
+          for (size_t r = 0; r < ns; ++r)
+            for (int l = 0; l < o.lines; ++l) {
+              const size_t dst = o_off + ((size_t)l + (size_t)o.lines * ((size_t)n + (size_t)npts * r)) * 2;
+              ob[dst] = acc[2 * ((size_t)l + (size_t)o.lines * r)];
+              ob[dst + 1] = acc[2 * ((size_t)l + (size_t)o.lines * r) + 1];
+            }
+        }
+        o_off += (size_t)2 * o.lines * npts * ns;
+        continue;
+      }
       size_t ns = o.spatial ? P.NS : 1;
       for (int n = 0; n < npts; ++n)
         for (size_t s = 0; s < ns; ++s)
@@ -2634,6 +2728,18 @@ XS_API xs_status xs_observe_info(const xs_handle* h, int o, int* lines, int* spa
   }
   if (lines) *lines = h->P.obs[o].lines;
   if (spatial) *spatial = h->P.obs[o].spatial ? 1 : 0;
+  return XS_OK;
+}
+
+XS_API xs_status xs_observe_shape(const xs_handle* h, int o, int* dims) {
+  if (!h || o < 0 || o >= (int)h->P.obs.size() || !dims) {
+    g_err = "bad handle, observable index or output pointer";
+    return XS_ERR_ARG;
+  }
+  const Problem& P = h->P;
+  const ObsInfo& ob = P.obs[o];
+  for (int d = 0; d < 3; ++d)
+    dims[d] = (d < P.D && ob.spatial && !(ob.partial && ob.pw[d] > 0)) ? P.N[d] : 1;
   return XS_OK;
 }
 
@@ -2732,7 +2838,7 @@ xs_status run_path_impl(xs_handle* h, int first_block, int nblocks, int nc, cons
     if (nc == 2 && !h->P.p.checks) raise(XS_ERR_ARG, "coarse pass requested without checks");
     load_module(*h);
     const Problem& P = h->P;
-    if (h->kind >= 2 && a_in && !raw_out && nblocks >= 2 && P.F == 1 && P.obs.size() <= 32) {
+    if (h->kind >= 2 && a_in && !raw_out && nblocks >= 2 && P.F == 1 && P.obs.size() <= 32 && !any_partial(P)) {
       run_stream_pipelined(h, first_block, nblocks, nc, a_in, av_out, a_out);
       return XS_OK;
     }
@@ -2778,7 +2884,9 @@ xs_status run_path_impl(xs_handle* h, int first_block, int nblocks, int nc, cons
     else launch_resident(*h, first_block, nblocks, nc, din, h->d_av.p, dout, h->stream);
     // block means into MATLAB's layout on the device, then one copy into the caller's buffer
     const size_t per_block = av_doubles_per_block(P);
-    const bool dev_perm = P.obs.size() <= 32;
+    // means into MATLAB's order on the device (a plain permutation), or on the host when an
+    // observable sums over reduced dimensions
+    const bool dev_perm = P.obs.size() <= 32 && !any_partial(P);
     std::vector<double> av(dev_perm ? 0 : avd);
     if (av_out && per_block) {
       if (dev_perm) {

@@ -498,8 +498,11 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
       if (xs_observe_info(e->h, o, &lines, &spatial) != XS_OK) xsm_fail("xspde:path", "xs_observe_info");
       const mxArray* pts = xsm_field(p, "points");
       size_t n = (size_t)lines * (size_t)xsm_elem(pts, 0, 1);
-      if (spatial)
-        for (int dd = 1; dd < (int)xsm_scalar(p, "dimensions", 1); ++dd) n *= (size_t)xsm_elem(pts, (size_t)dd, 1);
+      if (spatial) {  /* the lattice, with the dimensions a partial Int/Ave reduces of size 1 */
+        int shp[3] = {1, 1, 1};
+        if (xs_observe_shape(e->h, o, shp) != XS_OK) xsm_fail("xspde:path", "xs_observe_shape");
+        for (int dd = 1; dd < (int)xsm_scalar(p, "dimensions", 1) && dd <= 3; ++dd) n *= (size_t)shp[dd - 1];
+      }
       const mxArray* dims = (dav && mxIsCell(dav) && (size_t)o < mxGetNumberOfElements(dav)) ? mxGetCell(dav, (mwIndex)o) : NULL;
       mxArray* out;
       if (dims && mxIsNumeric(dims) && mxGetNumberOfElements(dims) >= 2) {

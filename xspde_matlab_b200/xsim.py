@@ -293,7 +293,10 @@ class GpuPath:
         for o in range(len(p.observe)):
             ln, sp = ctypes.c_int(), ctypes.c_int()
             _lib.check(L.xs_observe_info(h, o, ctypes.byref(ln), ctypes.byref(sp)))
-            self.obs.append((ln.value, bool(sp.value)))
+            dims = (ctypes.c_int * 3)()
+            _lib.check(L.xs_observe_shape(h, o, dims))
+            shape = tuple(dims[d] for d in range(len(p.space)))  # 1 where a partial Int/Ave reduces
+            self.obs.append((ln.value, bool(sp.value), shape))
         self.per_block = L.xs_av_doubles_per_block(h)
         # 1 resident, 2 streaming 2D, 3 streaming 3D (xs_path_kind)
         self.kind = L.xs_path_kind(h)
@@ -309,7 +312,7 @@ class GpuPath:
 
     def av_shapes(self):
         P = self.p
-        return [(ln, P.points[0]) + (tuple(P.space) if sp else ()) for ln, sp in self.obs]
+        return [(ln, P.points[0]) + (shape if sp else ()) for ln, sp, shape in self.obs]
 
     def _boundary_values(self, nc):
         """p.boundfun(a, c, d, p) tabulated at every half step t0 + k dtr/2 of check
