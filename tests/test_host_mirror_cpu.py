@@ -81,6 +81,65 @@ def test_mirror_matches_oracle_kspace_and_spectrum(monkeypatch, order):
     _close(*_run(monkeypatch, g, o))
 
 
+def _quantum():
+    """Examples/SDE_1D/Quantum.m, shorter run: the oscillator driven by its input noise
+    field, with the input and output fields as auxiliary cells and time spectra."""
+    T = 40.0
+    c = 2 * np.pi / T
+    base = dict(points=[201], ranges=[T], order=2, auxfields=2, noises=2, ensembles=[100, 1, 12],
+                transforms=[[1], [1], [1], [0]])
+    g = dict(base, initial="@(w,p) (w(1,:)+1i*w(2,:))/2", deriv="@(a,w,p) -a(1,:)+sqrt(2)*(w(1,:)+1i*w(2,:))/2",
+             define="@(a,w,p) [(w(1,:)+1i*w(2,:))/2; sqrt(2)*a(1,:)-(w(1,:)+1i*w(2,:))/2]",
+             observe=["@(a,x,p) %r*abs(a(1,:)).^2" % c, "@(a,x,p) %r*abs(x(1,:)).^2" % c,
+                      "@(a,x,p) %r*abs(x(2,:)).^2" % c, "@(a,x,p) abs(a(1,:)).^2"])
+
+    def a1(w):
+        return (w[0:1] + 1j * w[1:2]) / 2
+    o = dict(base, initial=lambda w, p: a1(w), deriv=lambda a, w, p: -a[0:1] + np.sqrt(2) * a1(w),
+             define=lambda a, w, p: np.concatenate([a1(w), np.sqrt(2) * a[0:1] - a1(w)]),
+             observe=[lambda a, x, p: c * abs(a[0:1]) ** 2, lambda a, x, p: c * abs(x[0:1]) ** 2,
+                      lambda a, x, p: c * abs(x[1:2]) ** 2, lambda a, x, p: abs(a[0:1]) ** 2])
+    return g, o
+
+
+class _CoarseUlpPath(OraclePath):
+    """The oracle's blocks with the input-field spectrum of the coarse pass moved by a
+    few units in the last place: the size of what a coarse noise formed with a fused
+    multiply-add, (z2 s + round(z1 s)) / 2, instead of two rounded products gives."""
+
+    def run_path(self, first, nblocks, nc, a_in=None, a_out=False, raw=False):
+        av, _ = super().run_path(first, nblocks, nc, a_in, a_out, raw)
+        if nc == 2:
+            for row in av:
+                row[1] = row[1] * (1 + 1e-15)
+        return av, None
+
+
+def test_mirror_quantum_step_error_counts_only_nonzero_observables(monkeypatch):
+    """The input field x(1) = w/2 has the same time spectrum in both check passes: the
+    coarse noise is the mean of the fine pass's two scaled draws bit for bit
+    (Simulator/xnoise.m:32-35) and the fine pass records the mean of its half steps.
+    Its step error is then exactly zero, and xsim.m's error vector averages the step
+    errors over the observables above p.tol = 1e-20 only: three here.  A roundoff-sized
+    difference between the passes makes it four, and the step-error entry falls by
+    sqrt(3/4) with no visible change in any data column."""
+    import importlib
+    g, o = _quantum()
+    eg, dg, eo, do = _run(monkeypatch, g, o)
+    _close(eg, dg, eo, do)
+    assert np.all(np.asarray(do[0][1])[:, 1] == 0)  # x(1) spectrum: zero step error
+    assert np.all(np.asarray(dg[0][1])[:, 1] == 0)
+    M = importlib.import_module("xspde_matlab_b200.xsim")
+    monkeypatch.setattr(M, "GpuPath", lambda p, path_kind=0, runtime_params=False: _CoarseUlpPath(p, o))
+    eu, du, _ = M.xsim(g)
+    eu = np.asarray(eu)
+    assert 0 < np.max(np.asarray(du[0][1])[:, 1]) < 1e-15
+    assert np.isclose(eu[1], eo[1] * np.sqrt(3 / 4), rtol=1e-9)
+    assert np.isclose(eu[2], eo[2], rtol=1e-12)
+    for a, b in zip(du[0], do[0]):
+        assert np.allclose(np.asarray(a)[:, 0], np.asarray(b)[:, 0], rtol=1e-12, atol=1e-15)
+
+
 @pytest.mark.parametrize("inp", [
     dict(dimensions=2, points=[7, 16], ranges=[1.0, 8.0], steps=2, noises=2, checks=1),
     dict(dimensions=3, points=[5, 12, 10], ranges=[0.5, 6.0, 4.0], steps=3, knoises=2, krandoms=1, checks=0),

@@ -25,6 +25,16 @@ __device__ __forceinline__ real xs_fma(real a, real b, real c) { return fma(a, b
 #else
 __device__ __forceinline__ real xs_fma(real a, real b, real c) { return fmaf(a, b, c); }
 #endif
+// a * b rounded on its own, never contracted into a following add.  The coarse
+// pass's noise (w1 s + w2 s) / 2 then rounds both scaled draws first, as
+// Simulator/xnoise.m:32-35 does, so it equals the mean of the fine pass's two
+// scaled draws bit for bit (a quantity that is the same in both check passes
+// then has a step error of exactly zero, as in the reference).
+#if XS_FP64
+__device__ __forceinline__ real xs_mul_rn(real a, real b) { return __dmul_rn(a, b); }
+#else
+__device__ __forceinline__ real xs_mul_rn(real a, real b) { return __fmul_rn(a, b); }
+#endif
 __device__ __forceinline__ cx operator+(cx a, cx b) { return mkcx(a.re + b.re, a.im + b.im); }
 __device__ __forceinline__ cx operator-(cx a, cx b) { return mkcx(a.re - b.re, a.im - b.im); }
 __device__ __forceinline__ cx operator-(cx a) { return mkcx(-a.re, -a.im); }

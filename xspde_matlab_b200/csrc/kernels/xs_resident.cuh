@@ -736,11 +736,11 @@ __device__ void xs_mp_lean(cx* A, cx* T, const XsPathArgs& P, double t, int g0, 
       real zz[XS_NW];
       xs_normals_site<XS_NW>(zz, (u32)s, el, (u32)draw, (u32)P.seq, P.seed, blk);
 #pragma unroll
-      for (int c = 0; c < XS_NW; ++c) w[c] = zz[c] * (real)P.wscale;
+      for (int c = 0; c < XS_NW; ++c) w[c] = xs_mul_rn(zz[c], (real)P.wscale);
       if (mode == 2) {
         xs_normals_site<XS_NW>(zz, (u32)s, el, (u32)prev, (u32)P.seq, P.seed, blk);
 #pragma unroll
-        for (int c = 0; c < XS_NW; ++c) w[c] = (w[c] + zz[c] * (real)P.wscale) * (real)0.5;
+        for (int c = 0; c < XS_NW; ++c) w[c] = (w[c] + xs_mul_rn(zz[c], (real)P.wscale)) * (real)0.5;
       }
     }
 #else
@@ -796,7 +796,7 @@ __device__ __forceinline__ void xs_noise(real* W, real* Wp, int mode, int draw, 
 #pragma unroll
     for (int c = 0; c < XS_NW; ++c) {
       const int j = (g * XS_NWS + c) * XS_NS + s;
-      const real v = z[c] * (real)P.wscale;
+      const real v = xs_mul_rn(z[c], (real)P.wscale);
       if (mode == 0) W[j] = v;                          // fine draw
       else if (mode == 1) Wp[j] = v;                    // first coarse draw
       else W[j] = (v + Wp[j]) * (real)0.5;              // averaged coarse draw

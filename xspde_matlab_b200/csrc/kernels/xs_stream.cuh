@@ -254,8 +254,8 @@ __device__ __forceinline__ void xs_xpass_core(const XsStreamArgs& A, int tid, si
         xs_normals_pair<XS_NW>(wl2, wh2, pidx, el, (u32)A.draw1, (u32)A.seq, A.seed, blk);
 #pragma unroll
         for (int c = 0; c < XS_NW; ++c) {
-          wl[c] = (wl[c] * ws + wl2[c] * ws) * (real)0.5;
-          wh[c] = (wh[c] * ws + wh2[c] * ws) * (real)0.5;
+          wl[c] = (xs_mul_rn(wl[c], ws) + xs_mul_rn(wl2[c], ws)) * (real)0.5;
+          wh[c] = (xs_mul_rn(wh[c], ws) + xs_mul_rn(wh2[c], ws)) * (real)0.5;
         }
       } else {
 #pragma unroll
@@ -282,7 +282,7 @@ __device__ __forceinline__ void xs_xpass_core(const XsStreamArgs& A, int tid, si
         real w2[XS_NW];
         xs_normals_site<XS_NW>(w2, s, el, (u32)A.draw1, (u32)A.seq, A.seed, blk);
 #pragma unroll
-        for (int c = 0; c < XS_NW; ++c) w[c] = (w[c] * ws + w2[c] * ws) * (real)0.5;
+        for (int c = 0; c < XS_NW; ++c) w[c] = (xs_mul_rn(w[c], ws) + xs_mul_rn(w2[c], ws)) * (real)0.5;
       } else {
 #pragma unroll
         for (int c = 0; c < XS_NW; ++c) w[c] = w[c] * ws;
@@ -421,7 +421,7 @@ __device__ __forceinline__ void xs_rk4_row(const XsStreamArgs& A) {
       real w2[XS_NW];
       xs_normals_site<XS_NW>(w2, s, el, (u32)d1, (u32)A.seq, A.seed, blk);
 #pragma unroll
-      for (int c = 0; c < XS_NW; ++c) w[c] = (w[c] * ws_ + w2[c] * ws_) * (real)0.5;
+      for (int c = 0; c < XS_NW; ++c) w[c] = (xs_mul_rn(w[c], ws_) + xs_mul_rn(w2[c], ws_)) * (real)0.5;
     } else {
 #pragma unroll
       for (int c = 0; c < XS_NW; ++c) w[c] = w[c] * ws_;

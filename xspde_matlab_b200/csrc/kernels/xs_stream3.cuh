@@ -341,8 +341,8 @@ __device__ __forceinline__ void xs3_mp_sites(const XsStreamArgs& A, cx* P, int e
       xs_normals_pair<XS_NW>(wl2, wh2, pidx, el, (u32)A.draw1, (u32)A.seq, A.seed, blk);
 #pragma unroll
       for (int c = 0; c < XS_NW; ++c) {
-        wl[c] = (wl[c] * ws + wl2[c] * ws) * (real)0.5;
-        wh[c] = (wh[c] * ws + wh2[c] * ws) * (real)0.5;
+        wl[c] = (xs_mul_rn(wl[c], ws) + xs_mul_rn(wl2[c], ws)) * (real)0.5;
+        wh[c] = (xs_mul_rn(wh[c], ws) + xs_mul_rn(wh2[c], ws)) * (real)0.5;
       }
     } else {
 #pragma unroll
@@ -366,7 +366,7 @@ __device__ __forceinline__ void xs3_mp_sites(const XsStreamArgs& A, cx* P, int e
       real w2[XS_NW];
       xs_normals_site<XS_NW>(w2, s, el, (u32)A.draw1, (u32)A.seq, A.seed, blk);
 #pragma unroll
-      for (int c = 0; c < XS_NW; ++c) w[c] = (w[c] * ws + w2[c] * ws) * (real)0.5;
+      for (int c = 0; c < XS_NW; ++c) w[c] = (xs_mul_rn(w[c], ws) + xs_mul_rn(w2[c], ws)) * (real)0.5;
     } else {
 #pragma unroll
       for (int c = 0; c < XS_NW; ++c) w[c] = w[c] * ws;
