@@ -168,3 +168,78 @@ def test_two_ranks_xsim_with_oracle_blocks_matches_oracle_xsim():
     assert np.allclose(eg[keep], eo[keep], rtol=1e-10, atol=1e-15), (eg, eo)
     for a, b in zip(dg, do[0]):
         assert np.allclose(a, np.asarray(b), rtol=1e-10, atol=1e-13)
+
+
+class FailingPath(FakePath):
+    """A device path whose call fails on this rank, as a C-ABI error status raised
+    by the host library does."""
+
+    def run_path(self, first, nblocks, nc, a_in=None, a_out=False):
+        raise RuntimeError("injected failure at block %d" % first)
+
+
+def _fail_worker(rank, size, port, mode, out):
+    import datetime
+    import time
+
+    import torch.distributed as dist
+    from xspde_matlab_b200.dist import allreduce_sum
+    from xspde_matlab_b200.xsim import _ensembles
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=size, timeout=datetime.timedelta(seconds=20))
+    inp = _inputs()
+    if rank == 1 and mode == "exit":
+        os._exit(3)  # leaves without reaching the reduction
+    path = FailingPath(inp[0]) if rank == 1 else FakePath(inp[0])
+    t0 = time.monotonic()
+    try:
+        _ensembles(inp, [path], rank, size, reduce=lambda a: allreduce_sum(a))
+        out.put((rank, "ok", "", time.monotonic() - t0))
+    except Exception as ex:
+        out.put((rank, type(ex).__name__, str(ex), time.monotonic() - t0))
+    if mode != "exit":
+        dist.destroy_process_group()
+
+
+def _run_failure(mode, nres):
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_fail_worker, args=(r, 2, port, mode, q)) for r in range(2)]
+    for pr in procs:
+        pr.start()
+    try:
+        res = {}
+        for _ in range(nres):
+            r, kind, msg, dt = q.get(timeout=120)
+            res[r] = (kind, msg, dt)
+    finally:
+        for pr in procs:
+            pr.join(timeout=60)
+            if pr.is_alive():
+                pr.kill()
+    return res, [pr.exitcode for pr in procs]
+
+
+def test_failing_rank_is_reported_on_every_rank():
+    """A rank whose device path raises still joins the moment reduction with a failure
+    count: it re-raises its own error and its peer raises at the reduction, at once,
+    instead of waiting there for the process-group timeout."""
+    res, codes = _run_failure("raise", 2)
+    assert res[1][0] == "RuntimeError" and "injected failure" in res[1][1]
+    assert res[0][0] == "RuntimeError" and "1 of 2 ranks failed" in res[0][1]
+    assert res[0][2] < 15
+    assert codes == [0, 0]
+
+
+def test_rank_that_leaves_ends_peers_reduction_with_error():
+    """A rank that exits before the reduction: its peer's all-reduce ends with an
+    error (closed connection or the short process-group timeout), not a hang."""
+    res, codes = _run_failure("exit", 1)
+    assert res[0][0] != "ok"
+    assert res[0][2] < 60
+    assert codes[1] == 3

@@ -486,51 +486,59 @@ def _ensembles(inp, paths, rank=0, size=1, reduce=None, raw=None):
     comp = {}  # compensation terms of the moment sums (_kadd)
     lo, hi = shard(nb, rank, size)
     chunk = max(1, min(nb, int(2 ** 27 // max(1, paths[0].per_block * 8))))
-    for b0 in range(lo, hi, chunk):
-        nbk = min(chunk, hi - b0)
-        prev = None
-        for nc in range(1, p1.nchk + 1):
+    failure = None
+    try:
+        for b0 in range(lo, hi, chunk):
+            nbk = min(chunk, hi - b0)
             prev = None
-            for s, p in enumerate(inp):
-                a_in = prev if s > 0 else None
-                if s > 0 and p.transfer is not None:
-                    # p.transfer(b, v, p) on the host between the two device paths (xensemble.m:62)
-                    if p.inrandoms > 0:
-                        v = np.concatenate([paths[s].random(b0 + b) for b in range(nbk)], axis=-1)
+            for nc in range(1, p1.nchk + 1):
+                prev = None
+                for s, p in enumerate(inp):
+                    a_in = prev if s > 0 else None
+                    if s > 0 and p.transfer is not None:
+                        # p.transfer(b, v, p) on the host between the two device paths (xensemble.m:62)
+                        if p.inrandoms > 0:
+                            v = np.concatenate([paths[s].random(b0 + b) for b in range(nbk)], axis=-1)
+                        else:
+                            v = np.zeros([0] + list(p.space) + [p.ensembles[0] * nbk])
+                        shape = [p.fields] + list(p.space) + [p.ensembles[0] * nbk]
+                        r = np.asarray(p.transfer(prev, v, p), dtype=complex)
+                        r = r.reshape(r.shape + (1,) * (len(shape) - r.ndim))
+                        a_in = np.asfortranarray(np.broadcast_to(r, shape))
+                    if raw is not None and p.rawdata:
+                        av, prev, r = paths[s].run_path(b0, nbk, nc, a_in=a_in, a_out=(s + 1 < len(inp)), raw=True)
+                        e1 = p.ensembles[0]
+                        for b in range(nbk):
+                            g = b0 + b
+                            k = g // p.ensembles[2] + p.ensembles[1] * (g % p.ensembles[2])
+                            raw[s][nc - 1][k] = r[..., b * e1:(b + 1) * e1]
                     else:
-                        v = np.zeros([0] + list(p.space) + [p.ensembles[0] * nbk])
-                    shape = [p.fields] + list(p.space) + [p.ensembles[0] * nbk]
-                    r = np.asarray(p.transfer(prev, v, p), dtype=complex)
-                    r = r.reshape(r.shape + (1,) * (len(shape) - r.ndim))
-                    a_in = np.asfortranarray(np.broadcast_to(r, shape))
-                if raw is not None and p.rawdata:
-                    av, prev, r = paths[s].run_path(b0, nbk, nc, a_in=a_in, a_out=(s + 1 < len(inp)), raw=True)
-                    e1 = p.ensembles[0]
+                        av, prev = paths[s].run_path(b0, nbk, nc, a_in=a_in, a_out=(s + 1 < len(inp)))
                     for b in range(nbk):
-                        g = b0 + b
-                        k = g // p.ensembles[2] + p.ensembles[1] * (g % p.ensembles[2])
-                        raw[s][nc - 1][k] = r[..., b * e1:(b + 1) * e1]
-                else:
-                    av, prev = paths[s].run_path(b0, nbk, nc, a_in=a_in, a_out=(s + 1 < len(inp)))
+                        for o in range(len(p.output)):
+                            Dv = np.real(np.asarray(p.output[o](av[b], p)))
+                            D[(s, b, nc, o)] = np.reshape(Dv, -1, order="F")
+            for s, p in enumerate(inp):
                 for b in range(nbk):
                     for o in range(len(p.output)):
-                        Dv = np.real(np.asarray(p.output[o](av[b], p)))
-                        D[(s, b, nc, o)] = np.reshape(Dv, -1, order="F")
-        for s, p in enumerate(inp):
-            for b in range(nbk):
-                for o in range(len(p.output)):
-                    if p1.checks[0] and p.order > 0:
-                        d1, d2 = D[(s, b, 1, o)], D[(s, b, 2, o)]
-                        D[(s, b, 2, o)] = d1
-                        D[(s, b, 1, o)] = d1 + (d1 - d2) / (2 ** p.order - 1.0)
-                    if data[s][o] is None:
-                        data[s][o] = np.zeros((D[(s, b, 1, o)].size, m1))
-                        comp[(s, o)] = np.zeros_like(data[s][o])
-                    ds, dc = data[s][o], comp[(s, o)]
-                    for n1 in range(1, m + 1):
-                        _kadd(ds[:, n1 - 1], dc[:, n1 - 1], D[(s, b, n1, o)] * inv)
-                    _kadd(ds[:, m1 - 1], dc[:, m1 - 1], D[(s, b, 1, o)] ** 2 * inv)
-        D.clear()
+                        if p1.checks[0] and p.order > 0:
+                            d1, d2 = D[(s, b, 1, o)], D[(s, b, 2, o)]
+                            D[(s, b, 2, o)] = d1
+                            D[(s, b, 1, o)] = d1 + (d1 - d2) / (2 ** p.order - 1.0)
+                        if data[s][o] is None:
+                            data[s][o] = np.zeros((D[(s, b, 1, o)].size, m1))
+                            comp[(s, o)] = np.zeros_like(data[s][o])
+                        ds, dc = data[s][o], comp[(s, o)]
+                        for n1 in range(1, m + 1):
+                            _kadd(ds[:, n1 - 1], dc[:, n1 - 1], D[(s, b, n1, o)] * inv)
+                        _kadd(ds[:, m1 - 1], dc[:, m1 - 1], D[(s, b, 1, o)] ** 2 * inv)
+            D.clear()
+    except Exception as ex:
+        # a rank that fails still takes part in the reduction below, with a failure
+        # count, so that its peers raise at once instead of waiting in the all-reduce
+        if size == 1:
+            raise
+        failure = ex
     for (s, o), c in comp.items():
         data[s][o] = data[s][o] + c
     if size > 1:
@@ -538,8 +546,14 @@ def _ensembles(inp, paths, rank=0, size=1, reduce=None, raw=None):
             for o in range(len(p.output)):
                 if data[s][o] is None:  # a rank without blocks: sizes from the output shapes
                     data[s][o] = np.zeros((int(np.prod(p.gpoints[o][:-1])), m1))
-        flat = [x for row in data for x in row]
+        flat = [x for row in data for x in row] + [np.array([0.0 if failure is None else 1.0])]
         flat = reduce(flat)
+        nfail = int(round(float(flat[-1][0])))
+        if failure is not None:
+            raise failure
+        if nfail:
+            raise RuntimeError("xsim: %d of %d ranks failed while integrating their ensemble blocks"
+                               % (nfail, size))
         pos = 0
         for s in range(len(data)):
             for o in range(len(data[s])):
