@@ -17,8 +17,18 @@ import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 CITE = re.compile(r"((?:[\w.'-]+/)*)([A-Za-z_]\w*\.m):(\d+)(?:-(\d+))?((?:,\s*\d+(?:-\d+)?)*)")
-# files that quote other documents' text (review notes, the survey) rather than cite on their own
-SKIP_PREFIX = ("VERDICT", "ADVICE", "SURVEY", "BASELINE", "GPUTEST", "BENCH", "SCALE", "MULTICHIP", "PROGRESS")
+EXT = (".py", ".md", ".h", ".hpp", ".cpp", ".cu", ".cuh", ".c", ".m")
+
+
+def _root_docs():
+    """The top-level notes that are this library's documentation: README.md and the
+    top-level .md files it names.  Other top-level .md files are records written
+    around the build (reviews, surveys, run logs) that quote other documents'
+    citations rather than make their own."""
+    docs = {"README.md"}
+    with open(os.path.join(ROOT, "README.md"), errors="replace") as f:
+        docs |= set(re.findall(r"\b([A-Za-z][\w-]*\.md)\b", f.read()))
+    return docs
 
 
 def _tracked():
@@ -28,10 +38,11 @@ def _tracked():
     except Exception:
         files = []
         for dp, dn, fn in os.walk(ROOT):
-            dn[:] = [d for d in dn if not d.startswith((".", "_work", "gpurun_out", "baseline"))]
+            # untracked trees: hidden and underscore folders, run outputs, installed packages
+            dn[:] = [d for d in dn if not d.startswith((".", "_", "baseline")) and not d.endswith("_out")]
             files += [os.path.relpath(os.path.join(dp, f), ROOT) for f in fn]
-    return [f for f in files if f.endswith((".py", ".md", ".h", ".hpp", ".cpp", ".cu", ".cuh", ".c", ".m"))
-            and not f.startswith(SKIP_PREFIX)]
+    docs = _root_docs()
+    return [f for f in files if f.endswith(EXT) and ("/" in f or not f.endswith(".md") or f in docs)]
 
 
 def _counts():
