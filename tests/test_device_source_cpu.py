@@ -281,3 +281,104 @@ def test_kernel_noise_matches_oracle_stream(tmp_path, fp64, tol):
         for s in range(0, nspace, 7):
             got = L.knormal(k, s, 2, draw, seq, seed, block)
             assert abs(got - ref[k, s, 2]) < tol * max(1.0, abs(ref[k, s, 2]))
+
+
+# Drifts of 2D periodic problems, which run on the streaming row pass.  There the midpoint
+# update a0 + h D(a) is generated as c0 + h dep(a): c0 = a0 + h inv(w, x, y, t) holds the
+# terms that do not read the field, formed once per site, and the iterations add the rest.
+SPLIT = [
+    ("-1i*(p.x.^2 + p.y.^2).*a + sin(p.t)*(w(1,:)+1i*w(2,:)) + 0.1i*a.*conj(a).*a + p.g*p.x",
+     lambda a, w1, w2, x, y, t: -1j * (x ** 2 + y ** 2) * a + np.sin(t) * (w1 + 1j * w2) + 0.1j * a * np.conj(a) * a
+     + 0.3 * x),
+    ("exp(-p.t)*a - 0.3*cos(p.x).*w(1,:) + 1i*p.y",
+     lambda a, w1, w2, x, y, t: np.exp(-t) * a - 0.3 * np.cos(x) * w1 + 1j * y),
+    ("a.^2.*w(2,:) - conj(a).*w(1,:) + 0.2", lambda a, w1, w2, x, y, t: a ** 2 * w2 - np.conj(a) * w1 + 0.2),
+    ("sqrt(abs(a)).*a + tanh(p.x - p.y).*w(1,:) - 0.5",
+     lambda a, w1, w2, x, y, t: np.sqrt(abs(a)) * a + np.tanh(x - y) * w1 - 0.5),
+    ("(1-abs(a).^2).*a - 0.5i*abs(a).^2.*a + 0.05*(w(1,:)+1i*w(2,:))/sqrt(2)",
+     lambda a, w1, w2, x, y, t: (1 - abs(a) ** 2) * a - 0.5j * abs(a) ** 2 * a + 0.05 * (w1 + 1j * w2) / np.sqrt(2)),
+    ("1i*p.g*(a - 1) + p.g^2*w(1,:).*w(2,:)",
+     lambda a, w1, w2, x, y, t: 0.3j * (a - 1) + 0.09 * w1 * w2),
+]
+
+
+def _stream_source(tmp, deriv):
+    """The 2D streaming NVRTC source the library generates for a 256 x 256 periodic problem."""
+    from xspde_matlab_b200 import _lib
+    from xspde_matlab_b200.xsim import make_problem, xpreferences
+    d = dict(dimensions=3, points=[3, 256, 256], ranges=[1.0, 20.0, 20.0], steps=1, ensembles=[4, 1, 1], noises=2,
+             method="MP", precision="fp64", params={"g": 0.3}, deriv=deriv, initial="@(v,p) 1 + 0*p.x",
+             linear="@(p) 0.5i*(p.Dx.^2+p.Dy.^2)", observe=["@(a,p) abs(a).^2"])
+    old = os.environ.get("XSPDE_B200_DUMP"), os.environ.get("XSPDE_B200_CACHE")
+    os.environ["XSPDE_B200_DUMP"] = str(tmp / "dump")
+    os.environ["XSPDE_B200_CACHE"] = str(tmp / "cache")
+    try:
+        q = xpreferences([d])[0]
+        pr, keep = make_problem(q)
+        log = ctypes.create_string_buffer(1 << 16)
+        _lib.check(_lib.lib().xs_compile_check(ctypes.byref(pr), log, len(log)))
+    finally:
+        for k, v in zip(("XSPDE_B200_DUMP", "XSPDE_B200_CACHE"), old):
+            if v is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = v
+    srcs = [open(tmp / "dump" / f).read() for f in os.listdir(tmp / "dump") if f.startswith("xs_stream")]
+    assert len(srcs) == 1
+    return srcs[0]
+
+
+def test_streaming_drift_split_matches_unsplit_update(tmp_path):
+    """For drifts with coordinates, time, named scalars, multiplicative and additive noise:
+    the generated drift equals NumPy's evaluation, and c0 + h dep(a) equals a0 + h D(a)."""
+    code = "#define XS_REAL double\n#define XS_FP64 1\n" + SHIM
+    code += open(os.path.join(KERNELS, "xs_prelude.cuh")).read().replace("#pragma once", "")
+    for k, (expr, _) in enumerate(SPLIT):
+        src = _stream_source(tmp_path / ("s%d" % k), "@(a,w,p) " + expr)
+        assert "#define XS_DSPLIT 1" in src, expr
+        for name in ("xs_deriv", "xs_deriv_c0", "xs_deriv_step"):
+            fn = _cut(src, "__device__ __forceinline__ void %s(" % name)
+            fn = fn.replace("void %s(" % name, "void %s_%d(" % (name, k))
+            code += fn
+        code += r"""
+extern "C" void update_%(k)d(int n, const double* a, const double* a0, const double* w, const double* xyt, double h,
+                            double* out) {
+  for (int i = 0; i < n; ++i) {
+    cx av[1] = {mkcx(a[2 * i], a[2 * i + 1])}, a0v[1] = {mkcx(a0[2 * i], a0[2 * i + 1])}, d[1], c0[1], s[1];
+    real wv[2] = {w[2 * i], w[2 * i + 1]};
+    const real x = xyt[3 * i], y = xyt[3 * i + 1], t = xyt[3 * i + 2];
+    xs_deriv_%(k)d(av, wv, nullptr, x, y, 0, t, nullptr, nullptr, 0, 0, d);
+    xs_deriv_c0_%(k)d(av, a0v, h, wv, nullptr, x, y, 0, t, nullptr, nullptr, 0, 0, c0);
+    xs_deriv_step_%(k)d(av, c0, h, wv, nullptr, x, y, 0, t, nullptr, nullptr, 0, 0, s);
+    out[6 * i + 0] = d[0].re; out[6 * i + 1] = d[0].im;
+    out[6 * i + 2] = a0v[0].re + h * d[0].re; out[6 * i + 3] = a0v[0].im + h * d[0].im;
+    out[6 * i + 4] = s[0].re; out[6 * i + 5] = s[0].im;
+  }
+}
+""" % dict(k=k)
+    L = _build(tmp_path, code, "split")
+    rng = np.random.default_rng(12)
+    n = 300
+    bad = []
+    for k, (expr, ref) in enumerate(SPLIT):
+        a = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+        a0 = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+        w = rng.standard_normal((n, 2))
+        xyt = np.stack([rng.uniform(-10, 10, n), rng.uniform(-10, 10, n), rng.uniform(0, 5, n)], axis=1)
+        h = 0.013
+        out = np.empty((n, 6))
+        f = getattr(L, "update_%d" % k)
+        f.argtypes = [ctypes.c_int] + [ctypes.c_void_p] * 4 + [ctypes.c_double, ctypes.c_void_p]
+        ai = np.ascontiguousarray(np.stack([a.real, a.imag], 1))
+        a0i = np.ascontiguousarray(np.stack([a0.real, a0.imag], 1))
+        f(n, ai.ctypes.data, a0i.ctypes.data, np.ascontiguousarray(w).ctypes.data, np.ascontiguousarray(xyt).ctypes.data,
+          h, out.ctypes.data)
+        d = out[:, 0] + 1j * out[:, 1]
+        full = out[:, 2] + 1j * out[:, 3]
+        split = out[:, 4] + 1j * out[:, 5]
+        want = ref(a, w[:, 0], w[:, 1], xyt[:, 0], xyt[:, 1], xyt[:, 2])
+        e1 = np.max(np.abs(d - want) / np.maximum(1.0, np.abs(want)))
+        e2 = np.max(np.abs(split - full) / np.maximum(1.0, np.abs(full)))
+        if not (e1 < 1e-12 and e2 < 1e-13):
+            bad.append("%s: drift %.2e, split %.2e" % (expr, e1, e2))
+    assert not bad, "\n".join(bad)
