@@ -1,0 +1,392 @@
+"""The resident kernel run on the CPU, without a GPU: the CUDA source the library generates
+for a problem is compiled with g++ against a host emulation of the few CUDA constructs it uses.
+Each CTA's threads are coroutines run by one OS thread and switched at every __syncthreads and
+warp-level exchange, so barriers keep their CUDA semantics; shared memory starts filled with
+garbage bytes.  The block means of whole paths (noise, check passes, steppers, auxiliary cells,
+time spectra, compensated observable sums) are compared with the oracle's p.path on the same
+Philox noise: the kernel's own arithmetic, independent of the GPU.
+"""
+import ctypes
+import math
+import os
+import re
+import subprocess
+import warnings
+
+import numpy as np
+import pytest
+
+from oracle import xspde_ref as X
+from tests.gpu_util import oracle_block_av
+
+EMU = r"""// Host emulation of the CUDA constructs the resident kernel uses: the threads of one CTA
+// are coroutines (ucontext) run by one OS thread, switched at __syncthreads and at the
+// warp-level exchanges, so a launch runs its CTAs one after another with exact barrier
+// semantics.
+#include <ucontext.h>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+#define __device__
+#define __forceinline__ inline
+#define __restrict__
+#define __global__
+#define __launch_bounds__(...)
+#define __align__(n) alignas(n)
+#define __shared__ static
+struct uint4 { unsigned x, y, z, w; };
+inline uint4 make_uint4(unsigned x, unsigned y, unsigned z, unsigned w) { return uint4{x, y, z, w}; }
+struct double2 { double x, y; };
+inline double2 make_double2(double x, double y) { return double2{x, y}; }
+struct int2 { int x, y; };
+struct xs_dim3 { unsigned x, y, z; };
+static xs_dim3 threadIdx, blockIdx, blockDim, gridDim;
+
+struct XsEmuThread {
+  ucontext_t ctx;
+  std::vector<char> stack;
+  int wait = 0;  // 0 runnable, 1 at a CTA barrier, 2 at a warp barrier
+  bool done = false;
+};
+static std::vector<XsEmuThread> xs_emu_thr;
+static ucontext_t xs_emu_sched;
+static int xs_emu_cur;
+static inline void xs_emu_yield(int why) {
+  xs_emu_thr[xs_emu_cur].wait = why;
+  swapcontext(&xs_emu_thr[xs_emu_cur].ctx, &xs_emu_sched);
+}
+inline void __syncthreads() { xs_emu_yield(1); }
+static int xs_emu_or;
+inline int __syncthreads_or(int p) {
+  if (p) xs_emu_or = 1;
+  __syncthreads();
+  const int r = xs_emu_or;
+  __syncthreads();
+  if (threadIdx.x == 0) xs_emu_or = 0;
+  __syncthreads();
+  return r;
+}
+inline void __syncwarp(unsigned = 0xffffffffu) { xs_emu_yield(2); }
+static double xs_emu_wbuf[32][32];
+inline double __shfl_xor_sync(unsigned, double v, int o) {
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  xs_emu_wbuf[w][l] = v;
+  __syncwarp();
+  const double r = xs_emu_wbuf[w][l ^ o];
+  __syncwarp();
+  return r;
+}
+inline void __threadfence() {}
+inline int atomicOr(int* p, int v) { const int o = *p; *p = o | v; return o; }
+inline int atomicAdd(int* p, int v) { const int o = *p; *p = o + v; return o; }
+inline float atomicAdd(float* p, float v) { const float o = *p; *p = o + v; return o; }
+template <class T> inline T __ldcg(const T* p) { return *p; }
+inline size_t __cvta_generic_to_shared(const void* p) { return (size_t)p; }
+inline float __int_as_float(int i) { float f; std::memcpy(&f, &i, 4); return f; }
+// separately rounded products (the device's __dmul_rn / __fmul_rn)
+inline double __dmul_rn(double a, double b) { volatile double r = a * b; return r; }
+inline float __fmul_rn(float a, float b) { volatile float r = a * b; return r; }
+inline float __logf(float x) { return std::log(x); }
+inline float __expf(float x) { return std::exp(x); }
+inline void __sincosf(float x, float* s, float* c) { *s = std::sin(x); *c = std::cos(x); }
+inline float rsqrtf(float x) { return 1.0f / std::sqrt(x); }
+inline void sincospi(double x, double* s, double* c) { *s = std::sin(M_PI * x); *c = std::cos(M_PI * x); }
+inline void sincos(float x, float* s, float* c) { *s = std::sin(x); *c = std::cos(x); }
+using std::sqrt; using std::log; using std::exp; using std::sin; using std::cos; using std::tan; using std::sinh;
+using std::cosh; using std::tanh; using std::atan; using std::atan2; using std::hypot; using std::fabs; using std::floor;
+using std::ceil; using std::round; using std::trunc; using std::erf; using std::fmin; using std::fmax; using std::pow;
+using std::copysign; using std::fma; using std::isfinite; using std::asin; using std::acos;
+"""
+
+RUNNER = r"""// One launch of xs_resident: the CTAs in turn, each as XS_THREADS coroutines.
+alignas(16) unsigned char xs_smem_storage[XS_SMEM_BYTES + 64];
+static const XsPathArgs* xs_emu_args;
+static void xs_emu_entry() {
+  xs_resident(*xs_emu_args);
+  xs_emu_thr[xs_emu_cur].done = true;
+  swapcontext(&xs_emu_thr[xs_emu_cur].ctx, &xs_emu_sched);
+}
+extern "C" int emu_run(const XsPathArgs* P, int nctas) {
+  blockDim = xs_dim3{XS_THREADS, 1, 1};
+  gridDim = xs_dim3{(unsigned)nctas, 1, 1};
+  xs_emu_args = P;
+  for (int c = 0; c < nctas; ++c) {
+    blockIdx = xs_dim3{(unsigned)c, 0, 0};
+    std::memset(xs_smem_storage, 0x7f, sizeof xs_smem_storage);  // shared memory starts as garbage
+    xs_emu_thr.assign(XS_THREADS, XsEmuThread());
+    for (int t = 0; t < XS_THREADS; ++t) {
+      XsEmuThread& th = xs_emu_thr[t];
+      th.stack.resize(1 << 18);
+      getcontext(&th.ctx);
+      th.ctx.uc_stack.ss_sp = th.stack.data();
+      th.ctx.uc_stack.ss_size = th.stack.size();
+      th.ctx.uc_link = nullptr;
+      makecontext(&th.ctx, xs_emu_entry, 0);
+    }
+    for (;;) {
+      bool any = false;
+      for (int t = 0; t < XS_THREADS; ++t) {
+        XsEmuThread& th = xs_emu_thr[t];
+        if (th.done || th.wait) continue;
+        any = true;
+        xs_emu_cur = t;
+        threadIdx = xs_dim3{(unsigned)t, 0, 0};
+        swapcontext(&xs_emu_sched, &th.ctx);
+      }
+      int live = 0, at_cta = 0;
+      for (auto& th : xs_emu_thr)
+        if (!th.done) { ++live; at_cta += th.wait == 1; }
+      if (!live) break;
+      bool released = false;
+      for (int w = 0; w * 32 < XS_THREADS; ++w) {  // warps whose live lanes all wait at a warp barrier
+        int n = 0, m = 0;
+        for (int l = w * 32; l < w * 32 + 32 && l < XS_THREADS; ++l)
+          if (!xs_emu_thr[l].done) { ++n; m += xs_emu_thr[l].wait == 2; }
+        if (n && m == n) {
+          for (int l = w * 32; l < w * 32 + 32 && l < XS_THREADS; ++l) xs_emu_thr[l].wait = 0;
+          released = true;
+        }
+      }
+      if (!released && at_cta == live) {
+        for (auto& th : xs_emu_thr) th.wait = 0;
+        released = true;
+      }
+      if (!released && !any) return -1;  // threads wait at different barriers: divergent barrier
+    }
+  }
+  return 0;
+}
+extern "C" int emu_sizes(int* out) {
+  out[0] = XS_G; out[1] = XS_THREADS; out[2] = XS_OBS_STRIDE; out[3] = (int)sizeof(XsPathArgs);
+  return 0;
+}
+"""
+
+V = ctypes.c_void_p
+
+
+class PathArgs(ctypes.Structure):
+    """XsPathArgs of csrc/kernels/xs_resident.cuh, field for field."""
+    _fields_ = [("ntraj", ctypes.c_int), ("ens1", ctypes.c_int), ("block0", ctypes.c_int), ("nc", ctypes.c_int),
+                ("checks", ctypes.c_int), ("npoints", ctypes.c_int), ("steps", ctypes.c_int), ("seq", ctypes.c_int),
+                ("seed", ctypes.c_uint), ("pad0", ctypes.c_int), ("wscale", ctypes.c_double),
+                ("vscale", ctypes.c_double), ("dtr", ctypes.c_double), ("t0", ctypes.c_double), ("prop", V),
+                ("tmat", V), ("tmat_off", ctypes.c_int * 4), ("a_in", V), ("a_out", V), ("obs", V), ("status", V),
+                ("single_step", ctypes.c_int), ("pad1", ctypes.c_int), ("w_in", V), ("params", V), ("gfield", V),
+                ("prop2", V), ("bval", V), ("bda", V), ("bval_n", ctypes.c_int), ("pad3", ctypes.c_int),
+                ("aft", V), ("twt", V), ("nt", ctypes.c_int), ("pad4", ctypes.c_int), ("fscn", ctypes.c_double),
+                ("raw", V), ("kfilt", V), ("rfilt", V), ("kwscale", ctypes.c_double), ("kvscale", ctypes.c_double)]
+
+
+class Emulated:
+    """The resident kernel of one 0-D problem (no lattice, no linear term), compiled for the host."""
+
+    def __init__(self, tmp, g, patch=None):
+        from xspde_matlab_b200 import _lib
+        from xspde_matlab_b200.xsim import make_problem, xpreferences
+        tmp.mkdir(parents=True, exist_ok=True)
+        old = os.environ.get("XSPDE_B200_DUMP"), os.environ.get("XSPDE_B200_CACHE")
+        os.environ["XSPDE_B200_DUMP"] = str(tmp / "dump")
+        os.environ["XSPDE_B200_CACHE"] = str(tmp / "cache")
+        try:
+            q = xpreferences([g])[0]
+            pr, keep = make_problem(q)
+            log = ctypes.create_string_buffer(1 << 16)
+            _lib.check(_lib.lib().xs_compile_check(ctypes.byref(pr), log, len(log)))
+        finally:
+            for k, v in zip(("XSPDE_B200_DUMP", "XSPDE_B200_CACHE"), old):
+                if v is None:
+                    os.environ.pop(k, None)
+                else:
+                    os.environ[k] = v
+        srcs = [open(tmp / "dump" / f).read() for f in os.listdir(tmp / "dump") if f.startswith("xs_resident")]
+        assert len(srcs) == 1
+        src = srcs[0]
+        self.defs = {k: v for k, v in re.findall(r"#define (XS_\w+) (-?\d+)\s*$", src, re.M)}
+        src = src.replace('asm volatile("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn));', "dyn = XS_SMEM_BYTES;")
+        src = re.sub(r'asm volatile\("cp\.async[^;]*;', ";", src)  # cp.async: device-memory lattices only
+        src = src.replace("extern __shared__ __align__(16) unsigned char xs_smem[];",
+                          "extern unsigned char xs_smem_storage[];\n#define xs_smem xs_smem_storage")
+        assert "asm" not in src
+        if patch is not None:
+            src = patch(src)
+        tmp.mkdir(parents=True, exist_ok=True)
+        cpp = tmp / "emu.cpp"
+        cpp.write_text(EMU + src + RUNNER)
+        so = tmp / "emu.so"
+        subprocess.run(["g++", "-O2", "-std=c++17", "-shared", "-fPIC", "-ffp-contract=off", "-o", str(so), str(cpp)],
+                       check=True, capture_output=True, text=True)
+        self.lib = ctypes.CDLL(str(so))
+        sz = (ctypes.c_int * 4)()
+        self.lib.emu_sizes(sz)
+        self.G, self.threads, self.stride, size = list(sz)
+        assert ctypes.sizeof(PathArgs) == size
+
+    def block_means(self, o, block, nc):
+        """Block means [points(1)][row] of one ensemble block and check pass (xs_obs_reduce's
+        sum over the block's CTAs, divided by ensembles(1))."""
+        p = X.xpreferences([o])[0]
+        P1, S, E1 = p.points[0], p.steps[0], p.ensembles[0]
+        G = self.G
+        assert E1 % G == 0
+        nctas = E1 // G
+        a = PathArgs()
+        a.ntraj, a.ens1, a.block0, a.nc, a.checks = E1, E1, block, nc, p.checks[0]
+        a.npoints, a.steps, a.seq, a.seed = P1, S, 0, p.seed & 0xFFFFFFFF
+        a.wscale, a.vscale = math.sqrt(p.nscale * p.noisefactor), math.sqrt(p.noisefactor)
+        a.dtr = p.dt / (2 * S) if (p.checks[0] and nc != 2) else p.dt / S
+        a.t0 = p.origins[0]
+        keep = []
+        prop = np.zeros((int(self.defs["XS_PROP_COMPS"]) * int(self.defs["XS_NS"]), 2))
+        prop[:, 0] = 1  # exp(L dt) with L = 0
+        a.prop = a.prop2 = prop.ctypes.data
+        obs = np.zeros((P1, nctas, self.stride, 2))
+        a.obs = obs.ctypes.data
+        status = np.zeros(1, dtype=np.int32)
+        a.status = status.ctypes.data
+        if int(self.defs.get("XS_SPEC", 0)):
+            F, NS, NA = (int(self.defs[k]) for k in ("XS_F", "XS_NS", "XS_NA"))
+            nt = P1 * S
+            row = (1 + (NA + F - 1) // F) * G * F * NS
+            real = np.float64 if int(self.defs["XS_FP64"]) else np.float32
+            aft = np.zeros((nctas * (nt + P1) * row, 2), dtype=real)
+            k = np.arange(nt)
+            twt = np.ascontiguousarray(np.stack([np.cos(2 * np.pi * k / nt), np.sin(2 * np.pi * k / nt)], 1))
+            keep += [aft, twt]
+            a.aft, a.twt, a.nt = aft.ctypes.data, twt.ctypes.data, nt
+            a.fscn = math.sqrt(2 * np.pi) / (2 * np.pi / (p.ranges[0] + p.dt)) / nt
+        assert self.lib.emu_run(ctypes.byref(a), nctas) == 0
+        assert status[0] == 0
+        m = obs[..., 0] + 1j * obs[..., 1]
+        return m.sum(axis=1) / E1
+
+
+def _rel(got, ref):
+    ref = np.asarray(ref).reshape(-1)
+    return float(np.max(np.abs(got - ref)) / max(1.0, float(np.max(np.abs(ref)))))
+
+
+def test_emulated_resident_kernel_quantum_auxiliary_spectra(tmp_path):
+    """Examples/SDE_1D/Quantum.m (auxiliary input/output fields, time spectra, step-halving
+    check with order 2): both passes of two blocks equal the oracle's block means to 1e-13,
+    and the input field's spectrum is the same in both passes bit for bit, so its step
+    error is exactly zero as in the reference."""
+    from tests.test_host_mirror_cpu import _quantum
+    g, o = _quantum()
+    emu = Emulated(tmp_path, g)
+    for b in (0, 7):
+        means = {}
+        for nc in (1, 2):
+            got = emu.block_means(o, b, nc)
+            ref, _ = oracle_block_av(o, b, nc)
+            for k in range(4):
+                assert _rel(got[:, k], ref[k]) < 1e-13, (b, nc, k)
+            means[nc] = got
+        assert np.array_equal(means[1][:, 1], means[2][:, 1])
+
+
+def test_emulated_resident_kernel_positive_p_dpo(tmp_path):
+    """The positive-P parametric oscillator (two fields, complex-sqrt multiplicative noise,
+    Stratonovich-corrected drift, MP) against the oracle to 1e-12."""
+    from xspde_matlab_b200.problems import DPO_0D
+    base = dict(DPO_0D, ensembles=[64, 2, 1], points=[4], steps=15, ranges=[0.6], precision="fp64")
+    gam, eps, chi = (base["params"][k] for k in ("gam", "eps", "chi"))
+
+    def deriv(a, w, p):
+        a1, a2 = a[0:1], a[1:2]
+        return np.concatenate([
+            -gam * a1 + eps * a2 - chi * a1 ** 2 * a2 + 0.5 * chi * a1 + np.sqrt(-chi * a1 ** 2 + 0j) * w[0:1],
+            -gam * a2 + eps * a1 - chi * a2 ** 2 * a1 + 0.5 * chi * a2 + np.sqrt(-chi * a2 ** 2 + 0j) * w[1:2]])
+
+    o = {k: v for k, v in base.items() if k not in ("deriv", "initial", "observe", "params", "precision")}
+    o.update(deriv=deriv, initial=lambda v, p: np.array([[1.0 + 0j], [1.0 + 0j]]),
+             observe=[lambda a, p: np.real(a[0:1] * a[1:2]), lambda a, p: np.real(a[0:1])])
+    emu = Emulated(tmp_path, base)
+    for b in (0, 1):
+        got = emu.block_means(o, b, 1)
+        ref, _ = oracle_block_av(o, b, 1)
+        for k in range(2):
+            assert _rel(got[:, k], ref[k]) < 1e-12, (b, k)
+
+
+@pytest.mark.parametrize("method,precision,tol", [("RK4", "fp64", 1e-13), ("RK4", "fp32", 2e-5),
+                                                  ("Euler", "fp64", 1e-13), ("RK2", "fp64", 1e-13)])
+def test_emulated_resident_kernel_steppers_with_checks(tmp_path, method, precision, tol):
+    """A driven damped oscillator with multiplicative noise through RK4, Euler and RK2 with the
+    step-halving check (both passes), FP64 at 1e-13 and FP32 within its rounding."""
+    base = dict(points=[6], ranges=[1.0], steps=4, ensembles=[32, 1, 1], noises=2, checks=1, order=1,
+                method=method)
+    g = dict(base, precision=precision, deriv="@(a,w,p) -(0.5+1i)*a + 0.3*a.*w(1,:) + 0.2i*w(2,:)",
+             initial="@(v,p) 1 + 0.1*(v(1,:) + 1i*v(2,:))", observe=["@(a,p) abs(a).^2", "@(a,p) real(a)"])
+    o = dict(base, deriv=lambda a, w, p: -(0.5 + 1j) * a + 0.3 * a * w[0:1] + 0.2j * w[1:2],
+             initial=lambda v, p: 1 + 0.1 * (v[0:1] + 1j * v[1:2]),
+             observe=[lambda a, p: abs(a) ** 2, lambda a, p: np.real(a)])
+    emu = Emulated(tmp_path, g)
+    for nc in (1, 2):
+        got = emu.block_means(o, 0, nc)
+        ref, _ = oracle_block_av(o, 0, nc)
+        for k in range(2):
+            assert _rel(got[:, k], ref[k]) < tol, (nc, k)
+
+
+class EmulatedPath:
+    """Stands in for GpuPath in the host xsim: p.path of each block from the emulated kernel
+    (0-D problems whose observables are one line each)."""
+
+    def __init__(self, emu, o):
+        self.emu, self.o = emu, o
+        q = X.xpreferences([o])[0]
+        self.shapes = [tuple(s) for s in q.d_av]
+        self.per_block = 2 * sum(int(np.prod(s)) for s in self.shapes)
+
+    def av_shapes(self):
+        return self.shapes
+
+    def run_path(self, first, nblocks, nc, a_in=None, a_out=False, raw=False):
+        av = []
+        for b in range(first, first + nblocks):
+            m = self.emu.block_means(self.o, b, nc)
+            av.append([m[:, k].reshape(s, order="F") for k, s in enumerate(self.shapes)])
+        return av, None
+
+
+def _fused(src):
+    """The coarse noise formed with a fused multiply-add, round(z2 s + round(z1 s)) / 2,
+    as a compiler that contracts the product into the add produces it."""
+    old = "W[j] = (v + Wp[j]) * (real)0.5;"
+    assert old in src
+    return src.replace(old, "W[j] = fma(z[c], (real)P.wscale, Wp[j]) * (real)0.5;")
+
+
+def test_emulated_kernel_through_xsim_matches_oracle_error_vector(monkeypatch, tmp_path):
+    """The Quantum example end to end: the host xsim over the emulated kernel's blocks gives the
+    oracle's error vector (the assertion of the GPU test).  With the coarse noise fused into a
+    multiply-add instead, the input field's spectrum differs between the passes in the last
+    bit, its step error is counted, and the step-error entry becomes sqrt(3/4) of the oracle's
+    with every data column unchanged (the GPU's result before the kernels rounded the two
+    scaled draws separately: 1.03452598e-3 against 1.19456771e-3)."""
+    import importlib
+    from tests.test_host_mirror_cpu import _quantum
+    M = importlib.import_module("xspde_matlab_b200.xsim")
+    g, o = _quantum()
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore", RuntimeWarning)
+        eo, do, _ = X.xsim(o)
+    eo = np.asarray(eo)
+    keep = [i for i in range(len(eo)) if i != 5]
+    res = {}
+    for name, patch in (("rounded", None), ("fused", _fused)):
+        emu = Emulated(tmp_path / name, g, patch)
+        monkeypatch.setattr(M, "GpuPath", lambda p, path_kind=0, runtime_params=False, emu=emu: EmulatedPath(emu, o))
+        e, d, _ = M.xsim(g)
+        res[name] = (np.asarray(e), d)
+    e, d = res["rounded"]
+    assert np.allclose(e[keep], eo[keep], rtol=1e-8, atol=1e-14)
+    assert np.all(np.asarray(d[0][1])[:, 1] == 0)
+    e, d = res["fused"]
+    assert np.isclose(e[1], eo[1] * math.sqrt(3 / 4), rtol=1e-6)
+    assert np.isclose(e[1], 1.03452598e-3, rtol=1e-6) and np.isclose(eo[1], 1.19456771e-3, rtol=1e-6)
+    assert np.isclose(e[2], eo[2], rtol=1e-10)
+    for a, b in zip(d[0], do[0]):
+        assert np.allclose(np.asarray(a)[:, 0], np.asarray(b)[:, 0], rtol=1e-9, atol=1e-12)
