@@ -273,9 +273,36 @@ class Emulated:
         a.dtr = p.dt / (2 * S) if (p.checks[0] and nc != 2) else p.dt / S
         a.t0 = p.origins[0]
         keep = []
-        prop = np.zeros((int(self.defs["XS_PROP_COMPS"]) * int(self.defs["XS_NS"]), 2))
-        prop[:, 0] = 1  # exp(L dt) with L = 0
-        a.prop = a.prop2 = prop.ctypes.data
+        NS, PC = int(self.defs["XS_NS"]), int(self.defs["XS_PROP_COMPS"])
+        if p.dimensions == 1 or not int(self.defs.get("XS_HAS_PROP", 0)):
+            prop = np.zeros((PC * NS, 2))
+            prop[:, 0] = 1  # exp(L dt) with L = 0
+            keep.append(prop)
+            a.prop = a.prop2 = prop.ctypes.data
+        else:
+            for name, mult in (("prop", 1), ("prop2", 2)):
+                # exp(mult L dtr / ipsteps) on the k lattice, [components][sites], x fastest
+                q = p.copy()
+                q.dtr = mult * a.dtr
+                pr, _ = q.propfactor(q)
+                pr = np.asarray(pr, dtype=complex).reshape(-1, order="F")
+                pr = np.broadcast_to(pr, (PC * NS,)) if pr.size == 1 else pr[:PC * NS]
+                tab = np.ascontiguousarray(np.stack([pr.real, pr.imag], 1))
+                keep.append(tab)
+                setattr(a, name, tab.ctypes.data)
+            # Stockham twiddles exp(-2 pi i m / n) of every FFT dimension, in dimension order
+            tw, off = [], [0, 0, 0, 0]
+            for d in range(p.dimensions - 1):
+                off[d + 1] = len(tw)
+                n = p.points[d + 1]
+                assert int(self.defs.get("XS_FFTD%d" % (d + 1), 0)), "dense transforms are not emulated"
+                tw += list(np.exp(-2j * np.pi * np.arange(n) / n))
+            real = np.float64 if int(self.defs["XS_FP64"]) else np.float32
+            tw = np.ascontiguousarray(np.stack([np.real(tw), np.imag(tw)], 1).astype(real))
+            keep.append(tw)
+            a.tmat = tw.ctypes.data
+            for d in range(4):
+                a.tmat_off[d] = off[d]
         obs = np.zeros((P1, nctas, self.stride, 2))
         a.obs = obs.ctypes.data
         status = np.zeros(1, dtype=np.int32)
@@ -425,3 +452,26 @@ def test_emulated_kernel_through_xsim_matches_oracle_error_vector(monkeypatch, t
     assert np.isclose(e[2], eo[2], rtol=1e-10)
     for a, b in zip(d[0], do[0]):
         assert np.allclose(np.asarray(a)[:, 0], np.asarray(b)[:, 0], rtol=1e-9, atol=1e-12)
+
+
+@pytest.mark.parametrize("method,checks", [("MP", 1), ("RK4", 1), ("RK4", 0)])
+def test_emulated_resident_kernel_snls_lattice(tmp_path, method, checks):
+    """The 1D stochastic NLS of the benchmark set (64 periodic points, i d2a/dx2 through the
+    shared-memory Stockham FFT and the FP64 propagator, MP with merged half-step propagators
+    or RK4) against the oracle: every site, output time and check pass to 1e-12."""
+    base = dict(dimensions=2, points=[4, 64], ranges=[0.3, 10.0], steps=3, ensembles=[16, 2, 1], noises=2,
+                method=method, checks=checks, order=1)
+    g = dict(base, precision="fp64", deriv="@(a,w,p) 1i*a.*conj(a).*a + 0.01*(w(1,:)+1i*w(2,:))/sqrt(2)",
+             initial="@(v,p) exp(-p.x.^2)", linear="@(p) 1i*p.Dx.^2", observe=["@(a,p) a.*conj(a)", "@(a,p) real(a)"])
+    o = dict(base, deriv=lambda a, w, p: 1j * a * np.conj(a) * a + 0.01 * (w[0:1] + 1j * w[1:2]) / np.sqrt(2),
+             initial=lambda v, p: np.exp(-p.x ** 2), linear=lambda p: 1j * p.Dx ** 2,
+             observe=[lambda a, p: a * np.conj(a), lambda a, p: np.real(a)])
+    emu = Emulated(tmp_path, g)
+    NS = 64
+    for nc in ((1, 2) if checks else (1,)):
+        for b in (0, 1):
+            got = emu.block_means(o, b, nc)
+            ref, _ = oracle_block_av(o, b, nc)
+            for k in range(2):
+                r = np.asarray(ref[k]).reshape(base["points"][0], NS, order="F")
+                assert _rel(got[:, k * NS:(k + 1) * NS].reshape(-1), r.reshape(-1)) < 1e-12, (nc, b, k)
