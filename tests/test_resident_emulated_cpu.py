@@ -50,6 +50,28 @@ struct XsEmuThread {
   bool done = false;
 };
 static std::vector<XsEmuThread> xs_emu_thr;
+// Order in which the scheduler runs the runnable threads of a CTA in each round: 0 by index,
+// 1 reversed, otherwise a fresh pseudo-random permutation every round (xorshift32).  A kernel
+// whose result depends on the order between two barriers has a race.
+static unsigned xs_emu_sched_kind = 0, xs_emu_rng = 1;
+extern "C" void emu_set_schedule(unsigned kind) {
+  xs_emu_sched_kind = kind;
+  xs_emu_rng = kind * 2654435761u + 12345u;
+}
+static void xs_emu_order(std::vector<unsigned>& ord, unsigned n) {
+  ord.resize(n);
+  for (unsigned i = 0; i < n; ++i) ord[i] = xs_emu_sched_kind == 1 ? n - 1 - i : i;
+  if (xs_emu_sched_kind > 1)
+    for (unsigned i = n - 1; i > 0; --i) {
+      xs_emu_rng ^= xs_emu_rng << 13;
+      xs_emu_rng ^= xs_emu_rng >> 17;
+      xs_emu_rng ^= xs_emu_rng << 5;
+      const unsigned j = xs_emu_rng % (i + 1);
+      const unsigned tmp = ord[i];
+      ord[i] = ord[j];
+      ord[j] = tmp;
+    }
+}
 static ucontext_t xs_emu_sched;
 static int xs_emu_cur;
 static inline void xs_emu_yield(int why) {
@@ -125,9 +147,12 @@ extern "C" int emu_run(const XsPathArgs* P, int nctas) {
       th.ctx.uc_link = nullptr;
       makecontext(&th.ctx, xs_emu_entry, 0);
     }
+    std::vector<unsigned> ord;
     for (;;) {
       bool any = false;
-      for (int t = 0; t < XS_THREADS; ++t) {
+      xs_emu_order(ord, XS_THREADS);
+      for (unsigned q = 0; q < (unsigned)XS_THREADS; ++q) {
+        const int t = (int)ord[q];
         XsEmuThread& th = xs_emu_thr[t];
         if (th.done || th.wait) continue;
         any = true;
@@ -475,3 +500,54 @@ def test_emulated_resident_kernel_snls_lattice(tmp_path, method, checks):
             for k in range(2):
                 r = np.asarray(ref[k]).reshape(base["points"][0], NS, order="F")
                 assert _rel(got[:, k * NS:(k + 1) * NS].reshape(-1), r.reshape(-1)) < 1e-12, (nc, b, k)
+
+
+def test_emulated_resident_kernel_has_no_barrier_races(tmp_path):
+    """The same launches with the threads of each CTA run in index order, reversed and in fresh
+    random orders between barriers give bit-identical block means: no result depends on an
+    order that a missing __syncthreads or __syncwarp would leave open (the Quantum example's
+    auxiliary cells, spectrum record and reductions; the 64-point lattice's Stockham FFT)."""
+    from tests.test_host_mirror_cpu import _quantum
+    g, o = _quantum()
+    cases = [(Emulated(tmp_path / "q", g), o, 1)]
+    base = dict(dimensions=2, points=[3, 64], ranges=[0.2, 10.0], steps=2, ensembles=[16, 1, 1], noises=2,
+                method="MP", checks=1, order=1)
+    gs = dict(base, precision="fp64", deriv="@(a,w,p) 1i*a.*conj(a).*a + 0.01*(w(1,:)+1i*w(2,:))/sqrt(2)",
+              initial="@(v,p) exp(-p.x.^2)", linear="@(p) 1i*p.Dx.^2", observe=["@(a,p) a.*conj(a)", "@(a,p) real(a)"])
+    os_ = dict(base, deriv=lambda a, w, p: 1j * a * np.conj(a) * a + 0.01 * (w[0:1] + 1j * w[1:2]) / np.sqrt(2),
+               initial=lambda v, p: np.exp(-p.x ** 2), linear=lambda p: 1j * p.Dx ** 2,
+               observe=[lambda a, p: a * np.conj(a), lambda a, p: np.real(a)])
+    cases.append((Emulated(tmp_path / "s", gs), os_, 2))
+    for emu, oo, nc in cases:
+        runs = []
+        for kind in (0, 1, 7, 12345):
+            emu.lib.emu_set_schedule(kind)
+            runs.append(emu.block_means(oo, 0, nc))
+        emu.lib.emu_set_schedule(0)
+        for r in runs[1:]:
+            assert np.array_equal(r, runs[0])
+
+
+def test_schedule_check_catches_a_missing_barrier(tmp_path):
+    """The check above has teeth: with the barrier before the Stockham FFT of xs_tr taken out
+    (on the CPU copy of the source only), the FFT may read elements another thread has not yet
+    written, and some thread order changes the result."""
+    old = "    __syncthreads();\n    xs_fft_d<D>(X, T, P.tmat + P.tmat_off[D], dir);"
+
+    def drop_barrier(src):
+        assert old in src
+        return src.replace(old, "    xs_fft_d<D>(X, T, P.tmat + P.tmat_off[D], dir);")
+    base = dict(dimensions=2, points=[3, 64], ranges=[0.2, 10.0], steps=2, ensembles=[16, 1, 1], noises=2,
+                method="MP", checks=1, order=1)
+    g = dict(base, precision="fp64", deriv="@(a,w,p) 1i*a.*conj(a).*a + 0.01*(w(1,:)+1i*w(2,:))/sqrt(2)",
+             initial="@(v,p) exp(-p.x.^2)", linear="@(p) 1i*p.Dx.^2", observe=["@(a,p) a.*conj(a)", "@(a,p) real(a)"])
+    o = dict(base, deriv=lambda a, w, p: 1j * a * np.conj(a) * a + 0.01 * (w[0:1] + 1j * w[1:2]) / np.sqrt(2),
+             initial=lambda v, p: np.exp(-p.x ** 2), linear=lambda p: 1j * p.Dx ** 2,
+             observe=[lambda a, p: a * np.conj(a), lambda a, p: np.real(a)])
+    emu = Emulated(tmp_path, g, drop_barrier)
+    runs = []
+    for kind in (0, 1, 7):
+        emu.lib.emu_set_schedule(kind)
+        runs.append(emu.block_means(o, 0, 1))
+    emu.lib.emu_set_schedule(0)
+    assert any(not np.array_equal(r, runs[0]) for r in runs[1:])

@@ -49,9 +49,12 @@ static int xs_emu_grid(unsigned gx, unsigned gy, unsigned gz, unsigned nthr, std
           th.ctx.uc_link = nullptr;
           makecontext(&th.ctx, xs_emu_entry, 0);
         }
+        std::vector<unsigned> ord;
         for (;;) {
           bool any = false;
-          for (unsigned t = 0; t < nthr; ++t) {
+          xs_emu_order(ord, nthr);
+          for (unsigned q = 0; q < nthr; ++q) {
+            const unsigned t = ord[q];
             XsEmuThread& th = xs_emu_thr[t];
             if (th.done || th.wait) continue;
             any = true;
@@ -305,3 +308,18 @@ def test_emulated_streaming_path_matches_oracle(tmp_path, method, precision, tol
         r1 = np.asarray(ref[1]).reshape(-1)
         assert np.max(np.abs(got[:, :NS] - r0)) / np.max(np.abs(r0)) < tol, nc
         assert np.max(np.abs(got[:, NS] - r1)) / np.max(np.abs(r1)) < tol, nc
+
+
+def test_emulated_streaming_passes_have_no_barrier_races(tmp_path):
+    """Index order, reversed and fresh random orders of each CTA's threads between barriers give
+    bit-identical block means through the row pass's warp-level transposes, the column pass and
+    the observation passes (FP32 MP, coarse pass)."""
+    g, o = _problems("MP", "fp32")
+    emu = StreamEmulated(tmp_path, g)
+    runs = []
+    for kind in (0, 1, 7):
+        emu.lib.emu_set_schedule(kind)
+        runs.append(emu.block_means(o, 0, 2))
+    emu.lib.emu_set_schedule(0)
+    for r in runs[1:]:
+        assert np.array_equal(r, runs[0])
