@@ -123,7 +123,10 @@ using std::copysign; using std::fma; using std::isfinite; using std::asin; using
 """
 
 RUNNER = r"""// One launch of xs_resident: the CTAs in turn, each as XS_THREADS coroutines.
-alignas(16) unsigned char xs_smem_storage[XS_SMEM_BYTES + 64];
+#ifndef XS_EMU_SMEM_SLACK
+#define XS_EMU_SMEM_SLACK 64
+#endif
+alignas(16) unsigned char xs_smem_storage[XS_SMEM_BYTES + XS_EMU_SMEM_SLACK];
 static const XsPathArgs* xs_emu_args;
 static void xs_emu_entry() {
   xs_resident(*xs_emu_args);
@@ -246,7 +249,7 @@ def host_source(src):
 class Emulated:
     """The resident kernel of one 0-D problem (no lattice, no linear term), compiled for the host."""
 
-    def __init__(self, tmp, g, patch=None):
+    def __init__(self, tmp, g, patch=None, asan=False):
         from xspde_matlab_b200 import _lib
         from xspde_matlab_b200.xsim import make_problem, xpreferences
         tmp.mkdir(parents=True, exist_ok=True)
@@ -275,7 +278,9 @@ class Emulated:
         cpp = tmp / "emu.cpp"
         cpp.write_text(EMU + src + RUNNER)
         so = tmp / "emu.so"
-        subprocess.run(["g++", "-O2", "-std=c++17", "-shared", "-fPIC", "-ffp-contract=off", "-o", str(so), str(cpp)],
+        # with asan: AddressSanitizer, and shared memory exactly the launch's XS_SMEM_BYTES
+        flags = ["-O1", "-g", "-fsanitize=address", "-fno-omit-frame-pointer", "-DXS_EMU_SMEM_SLACK=0"] if asan else ["-O2"]
+        subprocess.run(["g++"] + flags + ["-std=c++17", "-shared", "-fPIC", "-ffp-contract=off", "-o", str(so), str(cpp)],
                        check=True, capture_output=True, text=True)
         self.lib = ctypes.CDLL(str(so))
         sz = (ctypes.c_int * 4)()
@@ -551,3 +556,81 @@ def test_schedule_check_catches_a_missing_barrier(tmp_path):
         runs.append(emu.block_means(o, 0, 1))
     emu.lib.emu_set_schedule(0)
     assert any(not np.array_equal(r, runs[0]) for r in runs[1:])
+
+
+ASAN_RUN = r"""
+import pathlib, sys
+import numpy as np
+from tests.test_resident_emulated_cpu import Emulated, _snls
+from tests.test_host_mirror_cpu import _quantum
+tmp = pathlib.Path(sys.argv[1])
+# every problem is generated before the first emulated launch switches stacks, which the
+# sanitizer tracks only approximately
+cases = [(Emulated(tmp / name, g, asan=True), o)
+         for name, (g, o) in (("quantum", _quantum()), ("snls", _snls("MP", 1)), ("snls_rk4", _snls("RK4", 1)))]
+for emu, o in cases:
+    for nc in (1, 2):
+        emu.block_means(o, 1, nc)
+print("clean")
+"""
+
+
+def _snls(method, checks):
+    base = dict(dimensions=2, points=[3, 64], ranges=[0.2, 10.0], steps=2, ensembles=[16, 1, 1], noises=2,
+                method=method, checks=checks, order=1)
+    g = dict(base, precision="fp64", deriv="@(a,w,p) 1i*a.*conj(a).*a + 0.01*(w(1,:)+1i*w(2,:))/sqrt(2)",
+             initial="@(v,p) exp(-p.x.^2)", linear="@(p) 1i*p.Dx.^2", observe=["@(a,p) a.*conj(a)", "@(a,p) real(a)"])
+    o = dict(base, deriv=lambda a, w, p: 1j * a * np.conj(a) * a + 0.01 * (w[0:1] + 1j * w[1:2]) / np.sqrt(2),
+             initial=lambda v, p: np.exp(-p.x ** 2), linear=lambda p: 1j * p.Dx ** 2,
+             observe=[lambda a, p: a * np.conj(a), lambda a, p: np.real(a)])
+    return g, o
+
+
+def test_emulated_resident_kernel_stays_in_bounds(tmp_path):
+    """Bounds checking without a GPU (compute-sanitizer is closed on this pool): the emulated
+    kernel built with AddressSanitizer, its shared memory exactly the launch's size and every
+    launch buffer exactly the size the host allocates, runs the Quantum example (auxiliary
+    cells, spectrum record) and the 64-point lattice (MP, RK4) without an out-of-bounds access."""
+    import sys
+    libs = [subprocess.run(["g++", "-print-file-name=%s" % n], capture_output=True, text=True).stdout.strip()
+            for n in ("libasan.so", "libstdc++.so")]
+    if not all(x and os.path.exists(x) for x in libs):
+        pytest.skip("no AddressSanitizer runtime")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    # the sanitizer runtime first, and the C++ runtime with it so that its exception interceptor
+    # binds at start-up (the library throws and catches exceptions internally)
+    env = dict(os.environ, LD_PRELOAD=" ".join(os.path.realpath(x) for x in libs),
+               ASAN_OPTIONS="detect_leaks=0:halt_on_error=1", PYTHONPATH=root)
+    r = subprocess.run([sys.executable, "-c", ASAN_RUN, str(tmp_path)], cwd=root, env=env, capture_output=True,
+                       text=True, timeout=900)
+    assert "ERROR: AddressSanitizer" not in r.stderr, r.stderr[-4000:]
+    assert r.returncode == 0 and "clean" in r.stdout, r.stderr[-4000:]
+
+
+ASAN_PLANTED = r"""
+import pathlib, sys
+from tests.test_resident_emulated_cpu import Emulated
+from tests.test_host_mirror_cpu import _quantum
+old = "double2* out = P.obs + ((size_t)n * nctas + cta) * XS_OBS_STRIDE;"
+g, o = _quantum()
+emu = Emulated(pathlib.Path(sys.argv[1]), g, lambda src: src.replace(old, old[:-1] + " + 1;"), asan=True)
+emu.block_means(o, 0, 1)
+print("not caught")
+"""
+
+
+def test_bounds_check_catches_an_overrun(tmp_path):
+    """The check above has teeth: the observable rows shifted by one element (on a CPU copy
+    of the source only) make the last CTA write past the partial-sum buffer, and the
+    sanitizer stops the run with a heap-buffer-overflow."""
+    import sys
+    libs = [subprocess.run(["g++", "-print-file-name=%s" % n], capture_output=True, text=True).stdout.strip()
+            for n in ("libasan.so", "libstdc++.so")]
+    if not all(x and os.path.exists(x) for x in libs):
+        pytest.skip("no AddressSanitizer runtime")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = dict(os.environ, LD_PRELOAD=" ".join(os.path.realpath(x) for x in libs),
+               ASAN_OPTIONS="detect_leaks=0:halt_on_error=1", PYTHONPATH=root)
+    r = subprocess.run([sys.executable, "-c", ASAN_PLANTED, str(tmp_path)], cwd=root, env=env, capture_output=True,
+                       text=True, timeout=900)
+    assert r.returncode != 0 and "heap-buffer-overflow" in r.stderr, (r.returncode, r.stdout[-500:])
