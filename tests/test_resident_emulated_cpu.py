@@ -42,6 +42,7 @@ inline double2 make_double2(double x, double y) { return double2{x, y}; }
 struct int2 { int x, y; };
 struct xs_dim3 { unsigned x, y, z; };
 static xs_dim3 threadIdx, blockIdx, blockDim, gridDim;
+static unsigned xs_emu_dyn = 1u << 30;  // the launch's dynamic shared memory, as %dynamic_smem_size reads it
 
 struct XsEmuThread {
   ucontext_t ctx;
@@ -134,6 +135,7 @@ static void xs_emu_entry() {
   swapcontext(&xs_emu_thr[xs_emu_cur].ctx, &xs_emu_sched);
 }
 extern "C" int emu_run(const XsPathArgs* P, int nctas) {
+  xs_emu_dyn = XS_SMEM_BYTES;
   blockDim = xs_dim3{XS_THREADS, 1, 1};
   gridDim = xs_dim3{(unsigned)nctas, 1, 1};
   xs_emu_args = P;
@@ -237,12 +239,13 @@ def host_source(src):
             k += 1
         while src[k] != ";":
             k += 1
-        out.append("dyn = 1u << 30;" if "dynamic_smem_size" in src[j:k] else ";")
+        out.append("dyn = xs_emu_dyn;" if "dynamic_smem_size" in src[j:k] else ";")
         i = k + 1
     src = "".join(out)
-    for name in ("xs_smem", "xs_dsmem"):
-        src = src.replace("extern __shared__ __align__(16) unsigned char %s[];" % name,
-                          "extern unsigned char %s_storage[];\n#define %s %s_storage" % (name, name, name))
+    src = src.replace("extern __shared__ __align__(16) unsigned char xs_smem[];",
+                      "extern unsigned char xs_smem_storage[];\n#define xs_smem xs_smem_storage")
+    src = src.replace("extern __shared__ __align__(16) unsigned char xs_dsmem[];",
+                      "extern unsigned char* xs_dsmem_ptr;\n#define xs_dsmem xs_dsmem_ptr")
     return src.replace("__grid_constant__", "")
 
 
@@ -566,10 +569,11 @@ from tests.test_host_mirror_cpu import _quantum
 tmp = pathlib.Path(sys.argv[1])
 # every problem is generated before the first emulated launch switches stacks, which the
 # sanitizer tracks only approximately
-cases = [(Emulated(tmp / name, g, asan=True), o)
-         for name, (g, o) in (("quantum", _quantum()), ("snls", _snls("MP", 1)), ("snls_rk4", _snls("RK4", 1)))]
-for emu, o in cases:
-    for nc in (1, 2):
+cases = [(Emulated(tmp / name, g, asan=True), o, passes)
+         for name, (g, o), passes in (("quantum", _quantum(), (1, 2)), ("snls", _snls("MP", 1), (2,)),
+                                      ("snls_rk4", _snls("RK4", 1), (1,)))]
+for emu, o, passes in cases:
+    for nc in passes:
         emu.block_means(o, 1, nc)
 print("clean")
 """
@@ -590,7 +594,8 @@ def test_emulated_resident_kernel_stays_in_bounds(tmp_path):
     """Bounds checking without a GPU (compute-sanitizer is closed on this pool): the emulated
     kernel built with AddressSanitizer, its shared memory exactly the launch's size and every
     launch buffer exactly the size the host allocates, runs the Quantum example (auxiliary
-    cells, spectrum record) and the 64-point lattice (MP, RK4) without an out-of-bounds access."""
+    cells, spectrum record; both passes) and the 64-point lattice (MP coarse pass, RK4 fine pass)
+    without an out-of-bounds access."""
     import sys
     libs = [subprocess.run(["g++", "-print-file-name=%s" % n], capture_output=True, text=True).stdout.strip()
             for n in ("libasan.so", "libstdc++.so")]

@@ -21,6 +21,7 @@ RUNNER = r"""// Grid launches of the streaming kernels: the CTAs in turn, each C
 #include <functional>
 #include <string>
 alignas(16) unsigned char xs_dsmem_storage[240 * 1024];
+unsigned char* xs_dsmem_ptr = xs_dsmem_storage;
 static std::function<void()> xs_emu_fn;
 static std::vector<std::vector<char>> xs_emu_stacks;
 static void xs_emu_entry() {
@@ -28,7 +29,11 @@ static void xs_emu_entry() {
   xs_emu_thr[xs_emu_cur].done = true;
   swapcontext(&xs_emu_thr[xs_emu_cur].ctx, &xs_emu_sched);
 }
+static unsigned xs_emu_smem = 0;  // exact dynamic shared memory of this launch (0: the static buffer)
 static int xs_emu_grid(unsigned gx, unsigned gy, unsigned gz, unsigned nthr, std::function<void()> fn) {
+  std::vector<unsigned char> exact(xs_emu_smem);
+  xs_dsmem_ptr = xs_emu_smem ? exact.data() : xs_dsmem_storage;
+  xs_emu_dyn = xs_emu_smem ? xs_emu_smem : (unsigned)sizeof xs_dsmem_storage;
   blockDim = xs_dim3{nthr, 1, 1};
   gridDim = xs_dim3{gx, gy, gz};
   xs_emu_fn = fn;
@@ -39,7 +44,7 @@ static int xs_emu_grid(unsigned gx, unsigned gy, unsigned gz, unsigned nthr, std
     for (unsigned y = 0; y < gy; ++y)
       for (unsigned x = 0; x < gx; ++x) {
         blockIdx = xs_dim3{x, y, z};
-        std::memset(xs_dsmem_storage, 0x7f, sizeof xs_dsmem_storage);
+        std::memset(xs_dsmem_ptr, 0x7f, xs_emu_dyn);
         xs_emu_thr.assign(nthr, XsEmuThread());
         for (unsigned t = 0; t < nthr; ++t) {
           XsEmuThread& th = xs_emu_thr[t];
@@ -86,7 +91,8 @@ static int xs_emu_grid(unsigned gx, unsigned gy, unsigned gz, unsigned nthr, std
   return 0;
 }
 extern "C" int emu_launch(const char* name, unsigned gx, unsigned gy, unsigned gz, unsigned nthr,
-                          const XsStreamArgs* A, int extra) {
+                          const XsStreamArgs* A, int extra, unsigned smem) {
+  xs_emu_smem = smem;
   const std::string n(name);
   const XsStreamArgs a = *A;
   if (n == "xs_x_init") return xs_emu_grid(gx, gy, gz, nthr, [a] { xs_x_init(a); });
@@ -140,10 +146,11 @@ def _problems(method, precision):
 
 
 class StreamEmulated:
-    def __init__(self, tmp, g):
+    def __init__(self, tmp, g, asan=False):
         import subprocess
         from xspde_matlab_b200 import _lib
         from xspde_matlab_b200.xsim import make_problem, xpreferences
+        tmp.mkdir(parents=True, exist_ok=True)
         old = os.environ.get("XSPDE_B200_DUMP"), os.environ.get("XSPDE_B200_CACHE")
         os.environ["XSPDE_B200_DUMP"] = str(tmp / "dump")
         os.environ["XSPDE_B200_CACHE"] = str(tmp / "cache")
@@ -164,10 +171,11 @@ class StreamEmulated:
         cpp = tmp / "emu.cpp"
         cpp.write_text(EMU + host_source(srcs[0]) + RUNNER)
         so = tmp / "emu.so"
-        subprocess.run(["g++", "-O2", "-std=c++17", "-shared", "-fPIC", "-ffp-contract=off", "-o", str(so), str(cpp)],
+        flags = ["-O1", "-g", "-fsanitize=address", "-fno-omit-frame-pointer"] if asan else ["-O2"]
+        subprocess.run(["g++"] + flags + ["-std=c++17", "-shared", "-fPIC", "-ffp-contract=off", "-o", str(so), str(cpp)],
                        check=True, capture_output=True, text=True)
         self.lib = ctypes.CDLL(str(so))
-        self.lib.emu_launch.argtypes = [ctypes.c_char_p] + [ctypes.c_uint] * 4 + [V, ctypes.c_int]
+        self.lib.emu_launch.argtypes = [ctypes.c_char_p] + [ctypes.c_uint] * 4 + [V, ctypes.c_int, ctypes.c_uint]
         sz = (ctypes.c_int * 8)()
         self.lib.emu_sizes(sz)
         self.RX, self.RY, self.XROWS, self.TX, self.OROWS, self.stride, size, self.NRG = list(sz)
@@ -219,9 +227,20 @@ class StreamEmulated:
         a.tw_x, a.tw_y = tws[0].ctypes.data, tws[1].ctypes.data
         a.opart = buf((4 * NS, 2))
         xgrid, sgrid = E1 * N2 // self.XROWS, E1 * (N1 // self.TX)
+        # dynamic shared memory of each launch, as the host's StreamPlan sizes it
+        cxs = 16 if self.fp64 else 8
+        RX, RY = self.RX, self.RY
+        xline = max(RX * RX, RX * (RX + 1))
+        smem = {"xs_x_init": (2 * RX * RX + self.XROWS * xline) * cxs,
+                "xs_s_pass": (2 * RY * RY + self.TX * RY * RY) * cxs,
+                "xs_x_obs": (2 * RX * RX + self.OROWS * RX * (RX + 1)) * cxs,
+                "xs_x_rk1": (2 * RX * RX + 2 * self.XROWS * xline) * cxs}
+        smem["xs_x_nl"] = smem["xs_x_final"] = smem["xs_x_init"]
+        smem["xs_x_rk2"] = smem["xs_x_rk3"] = smem["xs_x_rk1"]
 
         def launch(name, gx, gy=1, gz=1, nthr=256, extra=0, args=a):
-            assert self.lib.emu_launch(name.encode(), gx, gy, gz, nthr, ctypes.byref(args), extra) == 0, name
+            r = self.lib.emu_launch(name.encode(), gx, gy, gz, nthr, ctypes.byref(args), extra, smem.get(name, 0))
+            assert r == 0, name
 
         def col(m):
             a.m = m
@@ -323,3 +342,35 @@ def test_emulated_streaming_passes_have_no_barrier_races(tmp_path):
     emu.lib.emu_set_schedule(0)
     for r in runs[1:]:
         assert np.array_equal(r, runs[0])
+
+
+ASAN_RUN = r"""
+import pathlib, sys
+from tests.test_stream_emulated_cpu import StreamEmulated, _problems
+tmp = pathlib.Path(sys.argv[1])
+# every problem is generated before the first emulated launch switches stacks
+cases = [(StreamEmulated(tmp / m, _problems(m, "fp64")[0], asan=True), _problems(m, "fp64")[1], nc)
+         for m, nc in (("MP", 2), ("RK4", 1))]
+for emu, o, nc in cases:
+    emu.block_means(o, 0, nc)
+print("clean")
+"""
+
+
+def test_emulated_streaming_passes_stay_in_bounds(tmp_path):
+    """Bounds checking without a GPU: the streaming kernels built with AddressSanitizer, each
+    launch's dynamic shared memory exactly the host's StreamPlan size and every buffer exactly
+    the host's, run the MP path (coarse pass) and the RK4 path (fine pass) without an out-of-bounds access."""
+    import subprocess
+    import sys
+    libs = [subprocess.run(["g++", "-print-file-name=%s" % n], capture_output=True, text=True).stdout.strip()
+            for n in ("libasan.so", "libstdc++.so")]
+    if not all(x and os.path.exists(x) for x in libs):
+        pytest.skip("no AddressSanitizer runtime")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = dict(os.environ, LD_PRELOAD=" ".join(os.path.realpath(x) for x in libs),
+               ASAN_OPTIONS="detect_leaks=0:halt_on_error=1", PYTHONPATH=root)
+    r = subprocess.run([sys.executable, "-c", ASAN_RUN, str(tmp_path)], cwd=root, env=env, capture_output=True,
+                       text=True, timeout=1200)
+    assert "ERROR: AddressSanitizer" not in r.stderr, r.stderr[-4000:]
+    assert r.returncode == 0 and "clean" in r.stdout, r.stderr[-4000:]
