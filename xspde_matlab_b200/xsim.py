@@ -465,6 +465,73 @@ def _kadd(s, c, x):
     s[...] = t
 
 
+class _Checkpoint:
+    """Block-granular checkpoint of the moment sums (p.checkpoint, a file name; no counterpart
+    in the reference, whose xsim.m:207-210 saves only at the end).  Blocks are independent and
+    their noise is keyed by the global block index, so the state after a group of blocks is the
+    index of the next block with the compensated sums and their compensation terms; a run
+    restarted with the same inputs continues from there and returns bit-identical moments.
+    Under several ranks each rank keeps its own file (name.rank<r>.npz) for its own blocks."""
+
+    def __init__(self, inp, rank, size, lo, hi, raw):
+        name = inp[0].get("checkpoint", None)
+        self.path = None
+        self.lo = lo
+        if not name or not str(name).strip():
+            return
+        if raw:
+            raise ValueError("p.checkpoint cannot be combined with p.rawdata")
+        base = str(name)
+        if base.endswith(".npz"):
+            base = base[:-4]
+        self.path = base + (".rank%d" % rank if size > 1 else "") + ".npz"
+        # what must match for a saved state to be continued: the text, numeric and list fields of
+        # every input (function handles by their text), the block range and the number of ranks
+        def plain(v):
+            if isinstance(v, (str, int, float, bool)) or v is None:
+                return v
+            if isinstance(v, (list, tuple)):
+                return [plain(x) for x in v]
+            if isinstance(v, dict):
+                return {k: plain(x) for k, x in sorted(v.items())}
+            if isinstance(v, np.ndarray):  # lattices and tables: shape and a digest of the values
+                import hashlib
+                return ("ndarray", v.shape, hashlib.sha1(np.ascontiguousarray(v).tobytes()).hexdigest()[:16])
+            return type(v).__name__
+        keys = [sorted((k, plain(v)) for k, v in dict(q).items() if k not in ("checkpoint", "checkpoint_blocks"))
+                for q in inp]
+        self.sig = repr((keys, lo, hi, size))
+
+    def resume(self, data, comp):
+        """The first block to integrate: lo, or the saved next block (restoring the sums)."""
+        import os
+        if not self.path or not os.path.exists(self.path):
+            return self.lo
+        with np.load(self.path, allow_pickle=False) as z:
+            if str(z["sig"]) != self.sig:
+                raise ValueError("p.checkpoint %s was written by a different run" % self.path)
+            for key in z.files:
+                if key.startswith("data_"):
+                    s, o = (int(x) for x in key[5:].split("_"))
+                    data[s][o] = z[key].copy()
+                    comp[(s, o)] = z["comp_%d_%d" % (s, o)].copy()
+            return int(z["next"])
+
+    def save(self, nxt, data, comp):
+        import os
+        if not self.path:
+            return
+        arrs = {"sig": np.array(self.sig), "next": np.array(nxt)}
+        for s, row in enumerate(data):
+            for o, d in enumerate(row):
+                if d is not None:
+                    arrs["data_%d_%d" % (s, o)] = d
+                    arrs["comp_%d_%d" % (s, o)] = comp[(s, o)]
+        tmp = self.path[:-4] + ".tmp.npz"
+        np.savez(tmp, **arrs)
+        os.replace(tmp, self.path)
+
+
 def _ensembles(inp, paths, rank=0, size=1, reduce=None, raw=None):
     """Block loop, check passes and moments (Simulator/xensemble.m:12-108) with
     all blocks of a pass integrated by one device call.  With size > 1 this
@@ -486,9 +553,13 @@ def _ensembles(inp, paths, rank=0, size=1, reduce=None, raw=None):
     comp = {}  # compensation terms of the moment sums (_kadd)
     lo, hi = shard(nb, rank, size)
     chunk = max(1, min(nb, int(2 ** 27 // max(1, paths[0].per_block * 8))))
+    ckpt = _Checkpoint(inp, rank, size, lo, hi, raw is not None)
+    if ckpt.path:
+        chunk = max(1, min(chunk, int(p1.get("checkpoint_blocks", chunk))))
+    start = ckpt.resume(data, comp)
     failure = None
     try:
-        for b0 in range(lo, hi, chunk):
+        for b0 in range(start, hi, chunk):
             nbk = min(chunk, hi - b0)
             prev = None
             for nc in range(1, p1.nchk + 1):
@@ -533,6 +604,7 @@ def _ensembles(inp, paths, rank=0, size=1, reduce=None, raw=None):
                             _kadd(ds[:, n1 - 1], dc[:, n1 - 1], D[(s, b, n1, o)] * inv)
                         _kadd(ds[:, m1 - 1], dc[:, m1 - 1], D[(s, b, 1, o)] ** 2 * inv)
             D.clear()
+            ckpt.save(b0 + nbk, data, comp)
     except Exception as ex:
         # a rank that fails still takes part in the reduction below, with a failure
         # count, so that its peers raise at once instead of waiting in the all-reduce
