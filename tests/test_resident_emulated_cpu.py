@@ -40,6 +40,10 @@ inline uint4 make_uint4(unsigned x, unsigned y, unsigned z, unsigned w) { return
 struct double2 { double x, y; };
 inline double2 make_double2(double x, double y) { return double2{x, y}; }
 struct int2 { int x, y; };
+struct float2 { float x, y; };
+struct alignas(16) float4 { float x, y, z, w; };
+struct alignas(32) double4 { double x, y, z, w; };
+#define __host__
 struct xs_dim3 { unsigned x, y, z; };
 static xs_dim3 threadIdx, blockIdx, blockDim, gridDim;
 static unsigned xs_emu_dyn = 1u << 30;  // the launch's dynamic shared memory, as %dynamic_smem_size reads it
@@ -211,10 +215,11 @@ class PathArgs(ctypes.Structure):
 
 
 def host_source(src):
-    """The generated CUDA source made host C++: every inline-asm statement becomes an empty
-    statement (they serve the cp.async, mbarrier and TMA paths that these tests do not take)
-    except the dynamic shared-memory size query, which reports ample room; the dynamic
-    shared-memory arrays become the emulator's buffers."""
+    """The generated CUDA source made host C++: the dynamic shared-memory size query reads the
+    emulated launch's size and every other inline-asm statement becomes an empty statement
+    (they serve the cp.async, mbarrier and TMA paths of device-memory lattices, the TMA column
+    pass and the 3D passes, which these tests do not take); the dynamic shared-memory arrays
+    become the emulator's buffers."""
     out, i = [], 0
     while True:
         j = src.find("asm volatile(", i)
@@ -239,7 +244,11 @@ def host_source(src):
             k += 1
         while src[k] != ";":
             k += 1
-        out.append("dyn = xs_emu_dyn;" if "dynamic_smem_size" in src[j:k] else ";")
+        stmt = src[j:k]
+        if "dynamic_smem_size" in stmt:
+            out.append("dyn = xs_emu_dyn;")
+        else:
+            out.append(";")
         i = k + 1
     src = "".join(out)
     src = src.replace("extern __shared__ __align__(16) unsigned char xs_smem[];",
